@@ -1,0 +1,67 @@
+"""ctypes binding of libgjxl_b200.so (the C ABI declared in include/gjxl_b200.h).
+
+The library is built in-tree by gjxl_b200.build. There is no fallback: if the
+shared library is missing or fails to load, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_char_p, c_double, c_float, c_int, c_size_t, c_uint32, c_void_p
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libgjxl_b200.so"
+
+P = c_void_p  # device or host pointer
+Z = c_size_t
+F = c_float
+I = c_int
+
+# name -> argument types; every function returns int (StatusCode numbering)
+# unless listed in _RESTYPES.
+SIGNATURES: dict[str, list] = {
+    "gjxl_b200_last_error": [],
+    "gjxl_b200_version": [],
+    "gjxl_b200_prepare_input": [P, Z, Z, Z, I, F, P, Z, Z, P, Z, Z, Z, Z, P, P],
+    "gjxl_b200_matrix_scale_stats": [P, Z, Z, Z, Z, P, P],
+}
+_RESTYPES = {"gjxl_b200_last_error": c_char_p}
+
+STATUS_NAMES = {
+    0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",
+    4: "OUT_OF_MEMORY", 5: "FAILED_PRECONDITION", 6: "SUBMISSION_FAILED",
+    7: "DEVICE_ERROR", 8: "INTERNAL",
+}
+
+
+class GjxlB200Error(RuntimeError):
+    def __init__(self, code: int, function: str, message: str):
+        super().__init__(f"{function} failed with {STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the library (once). Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise ImportError(
+                f"{LIBRARY_PATH} is missing: build it with `python -m gjxl_b200.build`")
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, c_int)
+        _lib = lib
+    return _lib
+
+
+def call(name: str, *args) -> None:
+    """Calls an entry point and raises GjxlB200Error on a nonzero status."""
+    lib = load()
+    code = getattr(lib, name)(*args)
+    if code != 0:
+        raise GjxlB200Error(code, name, lib.gjxl_b200_last_error().decode())

@@ -1,0 +1,45 @@
+"""Stage-level Python binding over the C ABI, taking torch CUDA tensors.
+
+Torch provides device memory and the current stream only; all computation is
+in libgjxl_b200.so. Images are (3, rows, stride) float32 tensors whose last
+dimension is the row stride (a multiple of 4).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def padded_extent(width: int, height: int) -> tuple[int, int]:
+    return (width + 7) // 8 * 8, (height + 7) // 8 * 8
+
+
+def _check_planes(t: torch.Tensor, rows: int, cols: int) -> None:
+    if t.dtype != torch.float32 or not t.is_cuda or t.dim() != 3 or t.shape[0] != 3:
+        raise ValueError("expected a (3, rows, stride) float32 CUDA tensor")
+    if t.shape[1] < rows or t.shape[2] < cols or not t.is_contiguous():
+        raise ValueError("plane tensor is too small or not contiguous")
+
+
+def prepare_input(pixels: torch.Tensor, width: int, height: int, row_stride: int,
+                  channels: int, linear: torch.Tensor, opsin: torch.Tensor,
+                  intensity_target: float = 255.0, device_error: torch.Tensor | None = None):
+    pw, ph = padded_extent(width, height)
+    _check_planes(linear, height, width)
+    _check_planes(opsin, ph, pw)
+    _lib.call("gjxl_b200_prepare_input", pixels.data_ptr(), width, height, row_stride,
+              channels, intensity_target, linear.data_ptr(), linear.shape[2],
+              linear.shape[1] * linear.shape[2], opsin.data_ptr(), opsin.shape[2],
+              opsin.shape[1] * opsin.shape[2], pw, ph,
+              None if device_error is None else device_error.data_ptr(), _stream())
+
+
+def matrix_scale_stats(opsin: torch.Tensor, width: int, height: int, stats: torch.Tensor):
+    _lib.call("gjxl_b200_matrix_scale_stats", opsin.data_ptr(), opsin.shape[2],
+              opsin.shape[1] * opsin.shape[2], width, height, stats.data_ptr(), _stream())

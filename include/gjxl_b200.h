@@ -1,0 +1,94 @@
+/*
+ * gjxl_b200 — C ABI of the B200 (sm_100a) perceptual-analysis backend for the
+ * gjxl JPEG XL VarDCT encoder.
+ *
+ * Conventions
+ *  - All image pointers are DEVICE pointers unless a name says "host".
+ *  - A three-plane image is one base pointer: plane c starts at
+ *    base + c * plane_pitch elements; rows are `stride` elements apart.
+ *    Strides and plane pitches are multiples of 4 elements and bases are
+ *    16-byte aligned (the kernels use 128-bit accesses).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy stream).
+ *  - Return values are the reference's StatusCode numbering
+ *    (src/core/status.h:12-22): 0 ok, 1 invalid argument, 2 unsupported,
+ *    3 unavailable, 4 out of memory, 5 failed precondition,
+ *    6 submission failed, 7 device error, 8 internal.
+ *    gjxl_b200_last_error() returns the thread's last message.
+ *  - `device_error` (may be NULL) is a device uint32 word the kernels OR
+ *    bits into: 1 non-finite input, 2 non-finite output, 4 range, 8 internal.
+ *    Callers map a nonzero word to StatusCode 7 (the reference's
+ *    ReadAndCheckDeviceError, src/gpu/cuda/cuda_aq_resident.cpp:3451).
+ */
+#ifndef GJXL_B200_H_
+#define GJXL_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GJXL_B200_API __attribute__((visibility("default")))
+#else
+#define GJXL_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GJXL_B200_OK 0
+#define GJXL_B200_INVALID_ARGUMENT 1
+#define GJXL_B200_UNSUPPORTED 2
+#define GJXL_B200_UNAVAILABLE 3
+#define GJXL_B200_OUT_OF_MEMORY 4
+#define GJXL_B200_FAILED_PRECONDITION 5
+#define GJXL_B200_SUBMISSION_FAILED 6
+#define GJXL_B200_DEVICE_ERROR 7
+#define GJXL_B200_INTERNAL 8
+
+/* Thread-local description of the last failure (empty after success). */
+GJXL_B200_API const char* gjxl_b200_last_error(void);
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+GJXL_B200_API int gjxl_b200_version(void);
+
+/*
+ * Input preparation (row a1).
+ * Replaces GpuResidentInputPreparation::PrepareResidentInput
+ * (src/gpu/ops/resident_input.h:75-80) as implemented by
+ * CudaBackend::PrepareResidentInput (src/gpu/cuda/cuda_input_preparation.cpp:299)
+ * and LinearRgbToOpsinKernel (src/gpu/cuda/cuda_aq_exact_kernels.cu:45), fused
+ * with the C API's packed sRGB decode (src/c_api/image_conversion.cpp:18-31,
+ * 116-138).
+ *
+ * Reads packed 8-bit sRGB (channels = 3 RGB or 4 opaque RGBA; alpha ignored)
+ * and writes the unpadded linear RGB planes (width x height) and the padded
+ * XYB planes (padded_width x padded_height, padded by edge replication exactly
+ * like color_transform_internal::LinearRgbToPaddedOpsin,
+ * src/codec/color_transform.cpp:365).
+ */
+GJXL_B200_API int gjxl_b200_prepare_input(const uint8_t* pixels, size_t width, size_t height,
+                            size_t row_stride_bytes, int channels,
+                            float intensity_target, float* linear,
+                            size_t linear_stride, size_t linear_plane_pitch,
+                            float* opsin, size_t opsin_stride,
+                            size_t opsin_plane_pitch, size_t padded_width,
+                            size_t padded_height, uint32_t* device_error,
+                            void* stream);
+
+/*
+ * Quantization-matrix scale statistics (row a2).
+ * Replaces OpsinMatrixScaleStatsKernel (src/gpu/cuda/cuda_aq_exact_kernels.cu:100)
+ * and ComputeQuantizationMatrixScaleStatsFromFiniteOpsin
+ * (src/codestream/workflow.cpp:1318). Writes {x_edge, b_edge, exposed_blue}
+ * as three device floats over the unpadded width x height region.
+ * `stats` is cleared by this call.
+ */
+GJXL_B200_API int gjxl_b200_matrix_scale_stats(const float* opsin, size_t opsin_stride,
+                                 size_t opsin_plane_pitch, size_t width,
+                                 size_t height, float* stats, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* GJXL_B200_H_ */

@@ -1,0 +1,178 @@
+"""numpy-facing wrapper of oracle/_ref/libgjxl_ref.so (the reference's own CPU
+analysis code built from its sources by oracle/Makefile, see ref_shim.cpp).
+
+Test infrastructure only (the checker and the timed CPU baseline).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_float, c_int, c_size_t, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "_ref" / "libgjxl_ref.so"
+
+_P, _Z, _F, _I = c_void_p, c_size_t, c_float, c_int
+_SIGNATURES = {
+    "gjxl_ref_srgb8_to_linear": [_P, _Z, _Z, _Z, _I, _P],
+    "gjxl_ref_linear_to_padded_opsin": [_P, _Z, _Z, _P, _Z, _Z, _F],
+    "gjxl_ref_opsin_to_linear": [_P, _Z, _Z, _F, _P],
+    "gjxl_ref_initial_quant_field": [_P, _Z, _Z, _F, _F, _I, _P, _P, _P],
+    "gjxl_ref_gaborish_inverse": [_P, _Z, _Z, _P, _P],
+    "gjxl_ref_gaborish": [_P, _Z, _Z, _P],
+    "gjxl_ref_initial_cfl": [_P, _Z, _Z, _I, _P, _P],
+    "gjxl_ref_ac_strategy_cost": [_P, _Z, _Z, _P, _P, _I, _Z, _Z, _F, _F, _P, _P],
+    "gjxl_ref_ac_strategy_search": [_P, _Z, _Z, _P, _P, _P, _P, _F, _I, _P],
+    "gjxl_ref_butteraugli": [_P, _P, _Z, _Z, _F, _P, _P],
+}
+
+_lib = None
+
+
+def available() -> bool:
+    return LIBRARY_PATH.exists()
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIBRARY_PATH} is missing; build it with `make -C oracle`")
+        handle = ctypes.CDLL(str(LIBRARY_PATH))
+        handle.gjxl_ref_last_error.restype = ctypes.c_char_p
+        for name, args in _SIGNATURES.items():
+            fn = getattr(handle, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = c_int
+        _lib = handle
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def _check(code: int, name: str) -> None:
+    if code != 0:
+        raise RuntimeError(f"{name}: status {code}: {lib().gjxl_ref_last_error().decode()}")
+
+
+def padded_extent(width: int, height: int) -> tuple[int, int]:
+    return (width + 7) // 8 * 8, (height + 7) // 8 * 8
+
+
+def srgb8_to_linear(pixels: np.ndarray) -> np.ndarray:
+    """(H, W, 3|4) uint8 -> (3, H, W) float32 linear RGB."""
+    pixels = np.ascontiguousarray(pixels)
+    h, w, ch = pixels.shape
+    out = np.empty((3, h, w), np.float32)
+    _check(lib().gjxl_ref_srgb8_to_linear(_ptr(pixels), w, h, w * ch, ch, _ptr(out)),
+           "srgb8_to_linear")
+    return out
+
+
+def linear_to_padded_opsin(linear: np.ndarray, intensity_target: float = 255.0) -> np.ndarray:
+    linear = np.ascontiguousarray(linear, np.float32)
+    _, h, w = linear.shape
+    pw, ph = padded_extent(w, h)
+    out = np.empty((3, ph, pw), np.float32)
+    _check(lib().gjxl_ref_linear_to_padded_opsin(_ptr(linear), w, h, _ptr(out), pw, ph,
+                                                 intensity_target), "linear_to_padded_opsin")
+    return out
+
+
+def opsin_to_linear(opsin: np.ndarray, intensity_target: float = 255.0) -> np.ndarray:
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, h, w = opsin.shape
+    out = np.empty_like(opsin)
+    _check(lib().gjxl_ref_opsin_to_linear(_ptr(opsin), w, h, intensity_target, _ptr(out)),
+           "opsin_to_linear")
+    return out
+
+
+def initial_quant_field(opsin: np.ndarray, target: float = 1.0, rescale: float = 1.0,
+                        uniform: bool = False):
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, ph, pw = opsin.shape
+    quant = np.empty((ph // 8, pw // 8), np.float32)
+    mask = np.empty_like(quant)
+    pixel_mask = np.empty((ph, pw), np.float32)
+    _check(lib().gjxl_ref_initial_quant_field(_ptr(opsin), pw, ph, target, rescale,
+                                              int(uniform), _ptr(quant), _ptr(mask),
+                                              _ptr(pixel_mask)), "initial_quant_field")
+    return quant, mask, pixel_mask
+
+
+def gaborish_inverse(opsin: np.ndarray, multipliers=(1.0, 1.0, 1.0)) -> np.ndarray:
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, h, w = opsin.shape
+    m = np.asarray(multipliers, np.float32)
+    out = np.empty_like(opsin)
+    _check(lib().gjxl_ref_gaborish_inverse(_ptr(opsin), w, h, _ptr(m), _ptr(out)),
+           "gaborish_inverse")
+    return out
+
+
+def gaborish(opsin: np.ndarray) -> np.ndarray:
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, h, w = opsin.shape
+    out = np.empty_like(opsin)
+    _check(lib().gjxl_ref_gaborish(_ptr(opsin), w, h, _ptr(out)), "gaborish")
+    return out
+
+
+def initial_cfl(opsin: np.ndarray, fast: bool = False):
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, ph, pw = opsin.shape
+    tiles = ((ph + 63) // 64, (pw + 63) // 64)
+    ytox = np.empty(tiles, np.int8)
+    ytob = np.empty(tiles, np.int8)
+    _check(lib().gjxl_ref_initial_cfl(_ptr(opsin), pw, ph, int(fast), _ptr(ytox), _ptr(ytob)),
+           "initial_cfl")
+    return ytox, ytob
+
+
+def ac_strategy_cost(opsin, quant, pixel_mask, strategy: int, bx: int, by: int,
+                     target: float, entropy_multiplier: float, cfl_factors) -> float:
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    quant = np.ascontiguousarray(quant, np.float32)
+    pixel_mask = np.ascontiguousarray(pixel_mask, np.float32)
+    _, ph, pw = opsin.shape
+    f = np.asarray(cfl_factors, np.float32)
+    cost = np.zeros(1, np.float32)
+    _check(lib().gjxl_ref_ac_strategy_cost(_ptr(opsin), pw, ph, _ptr(quant), _ptr(pixel_mask),
+                                           strategy, bx, by, target, entropy_multiplier,
+                                           _ptr(f), _ptr(cost)), "ac_strategy_cost")
+    return float(cost[0])
+
+
+def ac_strategy_search(opsin, quant, pixel_mask, ytox, ytob, target: float = 1.0,
+                       dense: bool = False) -> np.ndarray:
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    quant = np.ascontiguousarray(quant, np.float32)
+    pixel_mask = np.ascontiguousarray(pixel_mask, np.float32)
+    ytox = np.ascontiguousarray(ytox, np.int8)
+    ytob = np.ascontiguousarray(ytob, np.int8)
+    _, ph, pw = opsin.shape
+    cells = np.empty((ph // 8, pw // 8), np.uint8)
+    _check(lib().gjxl_ref_ac_strategy_search(_ptr(opsin), pw, ph, _ptr(quant), _ptr(pixel_mask),
+                                             _ptr(ytox), _ptr(ytob), target, int(dense),
+                                             _ptr(cells)), "ac_strategy_search")
+    return cells
+
+
+def butteraugli(reference: np.ndarray, distorted: np.ndarray, intensity_target: float = 80.0):
+    reference = np.ascontiguousarray(reference, np.float32)
+    distorted = np.ascontiguousarray(distorted, np.float32)
+    _, h, w = reference.shape
+    dmap = np.empty((h, w), np.float32)
+    score = np.zeros(1, np.float64)
+    _check(lib().gjxl_ref_butteraugli(_ptr(reference), _ptr(distorted), w, h, intensity_target,
+                                      _ptr(dmap), _ptr(score)), "butteraugli")
+    return dmap, float(score[0])

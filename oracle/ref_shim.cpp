@@ -1,0 +1,264 @@
+// Stage-level C entry points over the gjxl reference's own CPU analysis code.
+//
+// TEST INFRASTRUCTURE ONLY. This file is compiled together with the
+// reference's sources (src/core, src/codec, part of src/codestream) into
+// oracle/_ref/libgjxl_ref.so by oracle/Makefile. The parity tests call it as
+// the checker, and bench.py's reference arm times it as the CPU baseline.
+// The product library never links or loads it.
+//
+// Every function takes planar float images (plane-major, rows contiguous,
+// stride == width) and returns 0 on success or the reference's StatusCode
+// value on failure (the message is kept for gjxl_ref_last_error()).
+
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "c_api/image_conversion.h"
+#include "codec/ac_strategy.h"
+#include "codec/adaptive_quantization.h"
+#include "codec/butteraugli.h"
+#include "codec/chroma_from_luma.h"
+#include "codec/chroma_from_luma_internal.h"
+#include "codec/color_transform.h"
+#include "codec/color_transform_internal.h"
+#include "codec/gaborish.h"
+#include "codec/quantization_pipeline.h"
+#include "codec/quantization_pipeline_internal.h"
+#include "codec/vardct_frame.h"
+#include "core/ac_strategy.h"
+#include "core/image.h"
+#include "core/thread_budget.h"
+
+#define GJXL_REF_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+using namespace gjxl;
+
+thread_local std::string g_last_error;
+
+int Fail(const Status& status) {
+  g_last_error = std::string(status.message());
+  int code = static_cast<int>(status.code());
+  return code == 0 ? -1 : code;
+}
+
+ConstImage3FView ConstPlanar(const float* data, size_t width, size_t height) {
+  ConstImage3FView view;
+  for (size_t c = 0; c < 3; ++c) {
+    view.plane[c] = {data + c * width * height, {width, height}, width};
+  }
+  return view;
+}
+
+Image3FView Planar(float* data, size_t width, size_t height) {
+  Image3FView view;
+  for (size_t c = 0; c < 3; ++c) {
+    view.plane[c] = {data + c * width * height, {width, height}, width};
+  }
+  return view;
+}
+
+Status MakeColorCorrelation(const int8_t* y_to_x, const int8_t* y_to_b,
+                            size_t padded_width, size_t padded_height,
+                            ColorCorrelationMap* out) {
+  const Extent2D tiles = ColorTileExtent({padded_width, padded_height});
+  return chroma_from_luma_internal::CreateColorCorrelationMap(
+    {y_to_x, tiles, tiles.width}, {y_to_b, tiles, tiles.width}, out);
+}
+
+void ExportColorCorrelation(const ColorCorrelationMap& map, int8_t* y_to_x,
+                            int8_t* y_to_b) {
+  const ConstPlaneI8View x = map.y_to_x_map();
+  const ConstPlaneI8View b = map.y_to_b_map();
+  for (size_t y = 0; y < x.extent.height; ++y) {
+    std::memcpy(y_to_x + y * x.extent.width, x.Row(y), x.extent.width);
+    std::memcpy(y_to_b + y * b.extent.width, b.Row(y), b.extent.width);
+  }
+}
+
+Status ExportGrid(const AcStrategyGrid& grid, uint8_t* cells) {
+  const Extent2D extent = grid.extent();
+  for (size_t y = 0; y < extent.height; ++y) {
+    for (size_t x = 0; x < extent.width; ++x) {
+      AcStrategyCell cell;
+      Status status = grid.Get(x, y, &cell);
+      if (!status.ok()) return status;
+      cells[y * extent.width + x] = static_cast<uint8_t>(
+        (static_cast<uint8_t>(cell.strategy) << 1) | (cell.is_anchor ? 1 : 0));
+    }
+  }
+  return Status::Ok();
+}
+
+}  // namespace
+
+GJXL_REF_API const char* gjxl_ref_last_error(void) {
+  return g_last_error.c_str();
+}
+
+GJXL_REF_API int gjxl_ref_set_threads(size_t threads) {
+  (void)threads;
+  return 0;
+}
+
+// c_api/image_conversion.cpp: packed 8-bit sRGB (3 or 4 bytes per pixel) to
+// planar linear RGB through the reference's double-precision table.
+GJXL_REF_API int gjxl_ref_srgb8_to_linear(const uint8_t* pixels, size_t width,
+                                          size_t height, size_t row_stride,
+                                          int channels, float* linear) {
+  c_api_internal::PackedSrgbImageView image{};
+  image.pixels = pixels;
+  image.pixels_size = row_stride * (height - 1) + width * channels;
+  image.width = static_cast<uint32_t>(width);
+  image.height = static_cast<uint32_t>(height);
+  image.row_stride_bytes = row_stride;
+  image.format = channels == 4 ? c_api_internal::PackedPixelFormat::kRgba8Srgb
+                               : c_api_internal::PackedPixelFormat::kRgb8Srgb;
+  Status status = c_api_internal::ConvertValidatedPackedSrgbInto(
+    image, Planar(linear, width, height));
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/color_transform.cpp LinearRgbToPaddedOpsin at the workflow's
+// intensity target of 255.
+GJXL_REF_API int gjxl_ref_linear_to_padded_opsin(
+  const float* linear, size_t width, size_t height, float* opsin,
+  size_t padded_width, size_t padded_height, float intensity_target) {
+  Status status = color_transform_internal::LinearRgbToPaddedOpsin(
+    ConstPlanar(linear, width, height), intensity_target,
+    Planar(opsin, padded_width, padded_height));
+  return status.ok() ? 0 : Fail(status);
+}
+
+GJXL_REF_API int gjxl_ref_opsin_to_linear(const float* opsin, size_t width,
+                                          size_t height, float intensity_target,
+                                          float* linear) {
+  Status status = OpsinToLinearRgb(ConstPlanar(opsin, width, height),
+                                   intensity_target,
+                                   Planar(linear, width, height));
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/adaptive_quantization.cpp ComputeInitialQuantField.
+GJXL_REF_API int gjxl_ref_initial_quant_field(
+  const float* opsin, size_t padded_width, size_t padded_height,
+  float butteraugli_target, float rescale, int uniform, float* quant_field,
+  float* strategy_mask, float* pixel_mask) {
+  const Extent2D blocks{padded_width / 8, padded_height / 8};
+  const Extent2D pixels{padded_width, padded_height};
+  InitialQuantFieldOutput output{
+    .quant_field = {quant_field, blocks, blocks.width},
+    .strategy_mask = {strategy_mask, blocks, blocks.width},
+    .pixel_mask = {pixel_mask, pixels, pixels.width},
+  };
+  Status status = ComputeInitialQuantField(
+    ConstPlanar(opsin, padded_width, padded_height),
+    {.butteraugli_target = butteraugli_target,
+     .rescale = rescale,
+     .uniform = uniform != 0},
+    output);
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/gaborish.cpp ApplyGaborishInverse.
+GJXL_REF_API int gjxl_ref_gaborish_inverse(const float* input, size_t width,
+                                           size_t height,
+                                           const float* multipliers,
+                                           float* output) {
+  Status status = ApplyGaborishInverse(
+    ConstPlanar(input, width, height),
+    {multipliers[0], multipliers[1], multipliers[2]},
+    Planar(output, width, height));
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/gaborish.cpp ApplyGaborish with default weights.
+GJXL_REF_API int gjxl_ref_gaborish(const float* input, size_t width,
+                                   size_t height, float* output) {
+  Status status = ApplyGaborish(ConstPlanar(input, width, height),
+                                GaborishOptions{},
+                                Planar(output, width, height));
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/chroma_from_luma.cpp initial CfL maps (fast or regression form).
+GJXL_REF_API int gjxl_ref_initial_cfl(const float* opsin, size_t padded_width,
+                                      size_t padded_height, int fast,
+                                      int8_t* y_to_x, int8_t* y_to_b) {
+  ColorCorrelationMap map;
+  Status status =
+    fast ? chroma_from_luma_internal::ComputeInitialColorCorrelationMapFast(
+             ConstPlanar(opsin, padded_width, padded_height), &map)
+         : ComputeInitialColorCorrelationMap(
+             ConstPlanar(opsin, padded_width, padded_height), &map);
+  if (!status.ok()) return Fail(status);
+  ExportColorCorrelation(map, y_to_x, y_to_b);
+  return 0;
+}
+
+// codec/ac_strategy.cpp EstimateAcStrategyCost for one candidate.
+GJXL_REF_API int gjxl_ref_ac_strategy_cost(
+  const float* opsin, size_t padded_width, size_t padded_height,
+  const float* quant_field, const float* pixel_mask, int strategy,
+  size_t block_x, size_t block_y, float butteraugli_target,
+  float entropy_multiplier, const float* cfl_factors, float* cost) {
+  const Extent2D blocks{padded_width / 8, padded_height / 8};
+  AcStrategyCostOptions options{
+    .butteraugli_target = butteraugli_target,
+    .entropy_multiplier = entropy_multiplier,
+    .cfl_factors = {cfl_factors[0], cfl_factors[1], cfl_factors[2]},
+  };
+  Status status = EstimateAcStrategyCost(
+    static_cast<AcStrategyType>(strategy), block_x, block_y,
+    ConstPlanar(opsin, padded_width, padded_height),
+    {quant_field, blocks, blocks.width},
+    {pixel_mask, {padded_width, padded_height}, padded_width}, options, cost);
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/ac_strategy.cpp FindAcStrategyGrid. Cells use the reference's
+// encoding (strategy << 1) | anchor.
+GJXL_REF_API int gjxl_ref_ac_strategy_search(
+  const float* opsin, size_t padded_width, size_t padded_height,
+  const float* quant_field, const float* pixel_mask, const int8_t* y_to_x,
+  const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
+  uint8_t* cells) {
+  const Extent2D blocks{padded_width / 8, padded_height / 8};
+  ColorCorrelationMap cfl;
+  Status status =
+    MakeColorCorrelation(y_to_x, y_to_b, padded_width, padded_height, &cfl);
+  if (!status.ok()) return Fail(status);
+  AcStrategyGrid grid;
+  status = FindAcStrategyGrid(
+    ConstPlanar(opsin, padded_width, padded_height),
+    {quant_field, blocks, blocks.width},
+    {pixel_mask, {padded_width, padded_height}, padded_width}, cfl,
+    {.butteraugli_target = butteraugli_target,
+     .dense_dct32_search = dense_dct32 != 0},
+    &grid);
+  if (!status.ok()) return Fail(status);
+  status = ExportGrid(grid, cells);
+  return status.ok() ? 0 : Fail(status);
+}
+
+// codec/butteraugli.cpp ComputeButteraugliDistance (default options).
+GJXL_REF_API int gjxl_ref_butteraugli(const float* reference_linear,
+                                      const float* distorted_linear,
+                                      size_t width, size_t height,
+                                      float intensity_target,
+                                      float* distance_map, double* score) {
+  ButteraugliOptions options;
+  options.intensity_target = intensity_target;
+  Status status = ComputeButteraugliDistance(
+    ConstPlanar(reference_linear, width, height),
+    ConstPlanar(distorted_linear, width, height), options,
+    {distance_map, {width, height}, width}, score);
+  return status.ok() ? 0 : Fail(status);
+}
