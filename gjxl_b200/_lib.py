@@ -24,8 +24,12 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_version": [],
     "gjxl_b200_prepare_input": [P, Z, Z, Z, I, F, P, Z, Z, P, Z, Z, Z, Z, P, P],
     "gjxl_b200_matrix_scale_stats": [P, Z, Z, Z, Z, P, P],
+    "gjxl_b200_initial_quant_scratch_bytes": [Z, Z],
+    "gjxl_b200_initial_quant_field": [P, Z, Z, Z, Z, F, F, P, P, P, Z, P, Z, P, P],
+    "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
 }
-_RESTYPES = {"gjxl_b200_last_error": c_char_p}
+_RESTYPES = {"gjxl_b200_last_error": c_char_p,
+             "gjxl_b200_initial_quant_scratch_bytes": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

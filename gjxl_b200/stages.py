@@ -43,3 +43,28 @@ def prepare_input(pixels: torch.Tensor, width: int, height: int, row_stride: int
 def matrix_scale_stats(opsin: torch.Tensor, width: int, height: int, stats: torch.Tensor):
     _lib.call("gjxl_b200_matrix_scale_stats", opsin.data_ptr(), opsin.shape[2],
               opsin.shape[1] * opsin.shape[2], width, height, stats.data_ptr(), _stream())
+
+
+def initial_quant_field(opsin: torch.Tensor, padded_width: int, padded_height: int,
+                        target: float, rescale: float, quant_field: torch.Tensor,
+                        strategy_mask: torch.Tensor, pixel_mask: torch.Tensor,
+                        scratch: torch.Tensor, device_error: torch.Tensor | None = None):
+    _lib.call("gjxl_b200_initial_quant_field", opsin.data_ptr(), opsin.shape[2],
+              opsin.shape[1] * opsin.shape[2], padded_width, padded_height, target, rescale,
+              quant_field.data_ptr(), strategy_mask.data_ptr(), pixel_mask.data_ptr(),
+              pixel_mask.shape[-1], scratch.data_ptr(), scratch.numel() * scratch.element_size(),
+              None if device_error is None else device_error.data_ptr(), _stream())
+
+
+def initial_quant_scratch_bytes(padded_width: int, padded_height: int) -> int:
+    return _lib.load().gjxl_b200_initial_quant_scratch_bytes(padded_width, padded_height)
+
+
+def gaborish_inverse(src: torch.Tensor, dst: torch.Tensor, width: int, height: int,
+                     multipliers=(1.0, 1.0, 1.0), device_error: torch.Tensor | None = None):
+    import ctypes
+    m = (ctypes.c_float * 3)(*multipliers)
+    _lib.call("gjxl_b200_gaborish_inverse", src.data_ptr(), src.shape[2],
+              src.shape[1] * src.shape[2], dst.data_ptr(), dst.shape[2],
+              dst.shape[1] * dst.shape[2], width, height, ctypes.addressof(m),
+              None if device_error is None else device_error.data_ptr(), _stream())

@@ -87,6 +87,44 @@ GJXL_B200_API int gjxl_b200_matrix_scale_stats(const float* opsin, size_t opsin_
                                  size_t opsin_plane_pitch, size_t width,
                                  size_t height, float* stats, void* stream);
 
+/*
+ * Initial quantization field (row a3).
+ * Replaces ComputeInitialQuantField (src/codec/adaptive_quantization.cpp:582)
+ * as run on the GPU by InitialGradientKernel / FuzzyErosionKernel /
+ * ModulationKernel (src/gpu/cuda/cuda_aq_kernels.cu:52,174,254) behind
+ * PreparedAqEvaluation::ComputeInitialQuantization
+ * (src/gpu/ops/aq_evaluation.h:219-396).
+ *
+ * Input: padded XYB (pre-Gaborish). Outputs: quant_field and strategy_mask,
+ * one float per 8x8 block (dense, (padded_width/8) x (padded_height/8)), and
+ * the blurred pixel mask (padded_width x padded_height, row stride
+ * pixel_mask_stride). `scratch` is caller-provided device memory of at least
+ * gjxl_b200_initial_quant_scratch_bytes() bytes, 16-byte aligned.
+ */
+GJXL_B200_API size_t gjxl_b200_initial_quant_scratch_bytes(size_t padded_width,
+                                                           size_t padded_height);
+GJXL_B200_API int gjxl_b200_initial_quant_field(
+    const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+    size_t padded_width, size_t padded_height, float butteraugli_target,
+    float rescale, float* quant_field, float* strategy_mask, float* pixel_mask,
+    size_t pixel_mask_stride, void* scratch, size_t scratch_bytes,
+    uint32_t* device_error, void* stream);
+
+/*
+ * Inverse Gaborish (row a4).
+ * Replaces GaborishInverseProvider::Apply
+ * (src/codec/quantization_pipeline_internal.h:20-32) and GpuImagePrimitives'
+ * Symmetric5 convolution (src/gpu/ops/primitives.h:68-85,
+ * src/gpu/cuda/cuda_kernels.cu:1326). Three planes, mirrored borders, per-plane
+ * multipliers (the reference's ApplyGaborishInverse, src/codec/gaborish.cpp:37).
+ * `multipliers` is a HOST array of 3 floats. Input and output must not alias.
+ */
+GJXL_B200_API int gjxl_b200_gaborish_inverse(
+    const float* input, size_t input_stride, size_t input_plane_pitch,
+    float* output, size_t output_stride, size_t output_plane_pitch,
+    size_t width, size_t height, const float* multipliers,
+    uint32_t* device_error, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
