@@ -27,9 +27,14 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_initial_quant_scratch_bytes": [Z, Z],
     "gjxl_b200_initial_quant_field": [P, Z, Z, Z, Z, F, F, P, P, P, Z, P, Z, P, P],
     "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
+    "gjxl_b200_quant_matrix": [I, I, P, P, Z],
+    "gjxl_b200_ac_strategy_cost_bytes": [Z, Z],
+    "gjxl_b200_ac_strategy_costs": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P],
+    "gjxl_b200_ac_strategy_search": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P, P],
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
-             "gjxl_b200_initial_quant_scratch_bytes": c_size_t}
+             "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
+             "gjxl_b200_ac_strategy_cost_bytes": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

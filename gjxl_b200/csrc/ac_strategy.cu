@@ -1,0 +1,675 @@
+// Rows a6/a7/a8: AC-strategy candidate costs and the greedy hierarchical merge.
+//
+// Candidate cost: src/codec/ac_strategy.cpp:823-994 (EstimateAcStrategyCost)
+// with ComputeQuantNormUnchecked (:103-130) and the CPU DCT
+// (src/codec/dct.cpp:135-230). The reference transforms in double precision
+// with sequential sums and rounds to float at the end of each pass; the
+// kernel does the same (FP64 SIMT, same summation order, no FMA contraction),
+// so every cost is bit-identical to the reference's.
+//
+// Merge: src/codec/ac_strategy.cpp:340-773 (TryMerge,
+// FindBestFirstLevelDivision, SearchTile) over all 64x64 tiles. The
+// reference's CUDA path evaluates the candidates on the GPU, copies the cost
+// table to the host and merges there (src/gpu/ops/ac_strategy_search.cpp:
+// 626-740); here the merge runs on the device, one thread per tile, so the
+// strategy grid never leaves HBM.
+//
+// Work layout: one kernel instantiation per transform family <W, H>; each CTA
+// of 256 threads evaluates K = 1024 / (W*H) candidates (all three channels)
+// entirely in shared memory: pixels -> FP64 row pass -> FP64 column pass ->
+// quantize -> FP64 inverse row/column passes -> weighted loss. The reference's
+// order-dependent float sums (magnitude cost, pixel loss) are done by one
+// thread per (candidate, channel) in the reference's order.
+
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "host_util.h"
+#include "tables.h"
+
+namespace gjxl_b200 {
+namespace {
+
+// Strategy ids (reference src/core/ac_strategy.h:25-53).
+constexpr int kDct8 = 0, kDct16x16 = 4, kDct32x32 = 5, kDct16x8 = 6, kDct8x16 = 7,
+              kDct32x16 = 10, kDct16x32 = 11;
+
+// The seven searched families in the reference's candidate-stage order
+// (src/codec/ac_strategy_search_policy.h:21-29).
+constexpr int kFamilyCount = 7;
+constexpr int kFamilyStrategy[kFamilyCount] = {kDct8,     kDct16x8,  kDct8x16, kDct16x16,
+                                               kDct32x16, kDct16x32, kDct32x32};
+constexpr float kFamilyEntropy[kFamilyCount] = {1.0f, 1.21f, 1.21f, 1.34f, 1.49f, 1.49f, 1.48f};
+// Covered blocks (width, height) and anchor steps (normal search).
+constexpr int kFamilyCoveredW[kFamilyCount] = {1, 1, 2, 2, 2, 4, 4};
+constexpr int kFamilyCoveredH[kFamilyCount] = {1, 2, 1, 2, 4, 2, 4};
+constexpr int kFamilyStep[kFamilyCount] = {1, 1, 1, 1, 2, 2, 2};
+
+__host__ __device__ constexpr int FamilyOfStrategy(int s) {
+  return s == kDct8 ? 0 : s == kDct16x8 ? 1 : s == kDct8x16 ? 2 : s == kDct16x16 ? 3
+       : s == kDct32x16 ? 4 : s == kDct16x32 ? 5 : s == kDct32x32 ? 6 : -1;
+}
+
+struct CostParams {
+  const float* opsin;  // Gaborish-inverted padded XYB
+  size_t stride, pitch;
+  const float* quant_field;  // blocks_x x blocks_y, dense
+  const float* pixel_mask;
+  size_t mask_stride;
+  const int8_t* y_to_x;  // color tiles, dense
+  const int8_t* y_to_b;
+  uint32_t blocks_x, blocks_y, tiles_x, tiles_y;
+  float info_loss_multiplier, zeros_multiplier, cost_delta;
+  float entropy_multiplier;
+  int anchor_step;
+  int local_x, local_y;  // local anchors per tile along x / y (full tile)
+  const float* dequant;          // family table [3][N]
+  const float* inverse_dequant;  // family table [3][N]
+  const double* fwd_w_t;  // forward basis, width length, transposed [x][u]
+  const double* fwd_h;    // forward basis, height length, natural [v][y]
+  const double* inv_w;    // inverse basis, width length, natural [u][x]
+  const double* inv_h;    // inverse basis, height length, natural [v][y]
+  float* costs;           // family plane, blocks_x x blocks_y (anchor positions)
+  uint32_t* error;
+};
+
+template <int W, int H>
+struct Shape {
+  static constexpr int N = W * H;
+  static constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  static constexpr int CW = W / 8, CH = H / 8;
+  // AcStrategyInfo::coefficient_index (src/core/ac_strategy.h:103-113).
+  __device__ static int Index(int v, int u) { return H < W ? v * W + u : u * H + v; }
+};
+
+constexpr int kCostThreads = 256;
+
+__device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
+  return v <= 1 ? 0 : 32 - __clz(v - 1);
+}
+
+template <int W, int H>
+__global__ void __launch_bounds__(kCostThreads)
+CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_count) {
+  using S = Shape<W, H>;
+  constexpr int N = S::N, K = S::K;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* A = reinterpret_cast<float*>(smem);               // [K][3][N]
+  float* B = A + K * 3 * N;                                 // [K][3][N]
+  double* T = reinterpret_cast<double*>(B + K * 3 * N);     // [K][3][N]
+  float* Tf = reinterpret_cast<float*>(T);                  // aliases T
+  __shared__ int anchor_x[K], anchor_y[K];
+  __shared__ float quant_norm[K], cfl[K][3];
+  __shared__ float magnitude[K][3], loss_sum[K][3];
+  __shared__ uint32_t nonzero[K][3];
+
+  const int tid = threadIdx.x;
+  if (tid < K) {
+    const uint32_t cand = blockIdx.x * K + tid;
+    int ax = -1, ay = -1;
+    if (cand < candidate_count) {
+      const uint32_t per_tile = p.local_x * p.local_y;
+      const uint32_t tile = cand / per_tile, local = cand % per_tile;
+      const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+      const int lx = (local % p.local_x) * p.anchor_step;
+      const int ly = (local / p.local_x) * p.anchor_step;
+      const int tile_w = min(8, static_cast<int>(p.blocks_x) - tx * 8);
+      const int tile_h = min(8, static_cast<int>(p.blocks_y) - ty * 8);
+      if (lx + S::CW <= tile_w && ly + S::CH <= tile_h) {
+        ax = tx * 8 + lx;
+        ay = ty * 8 + ly;
+        // ComputeQuantNormUnchecked (ac_strategy.cpp:103-130).
+        const float* q = p.quant_field;
+        float qn;
+        if (S::CW * S::CH == 1) {
+          qn = q[ay * p.blocks_x + ax];
+        } else if (S::CW * S::CH == 2) {
+          qn = S::CH == 2 ? fmaxf(q[ay * p.blocks_x + ax], q[(ay + 1) * p.blocks_x + ax])
+                          : fmaxf(q[ay * p.blocks_x + ax], q[ay * p.blocks_x + ax + 1]);
+        } else {
+          float sum = 0.0f;
+          for (int dy = 0; dy < S::CH; ++dy) {
+            for (int dx = 0; dx < S::CW; ++dx) {
+              float v = q[(ay + dy) * p.blocks_x + ax + dx];
+              v *= v;
+              v *= v;
+              v *= v;
+              sum += v * v;
+            }
+          }
+          sum /= static_cast<float>(S::CW * S::CH);
+          qn = FastPow2(FastLog2(sum) * (1.0f / 16.0f));
+        }
+        if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
+        quant_norm[tid] = qn;
+        const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
+        // ColorCorrelationMap::AcFactors (chroma_from_luma.cpp:412-432).
+        cfl[tid][0] = static_cast<float>(p.y_to_x[tile_index]) / 84.0f;
+        cfl[tid][1] = 0.0f;
+        cfl[tid][2] = 1.0f + static_cast<float>(p.y_to_b[tile_index]) / 84.0f;
+      }
+    }
+    anchor_x[tid] = ax;
+    anchor_y[tid] = ay;
+    magnitude[tid][0] = magnitude[tid][1] = magnitude[tid][2] = 0.0f;
+    nonzero[tid][0] = nonzero[tid][1] = nonzero[tid][2] = 0;
+  }
+  __syncthreads();
+
+  // Pixels into A.
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    if (anchor_x[k] < 0) continue;
+    const int y = yx / W, x = yx % W;
+    A[i] = p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
+                   anchor_x[k] * 8 + x];
+  }
+  __syncthreads();
+
+  // Forward row pass: T[y][u] = sum_x (double)pixel[y][x] * basis_w[u][x].
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int kc = i / N, yu = i % N, y = yu / W, u = yu % W;
+    if (anchor_x[kc / 3] < 0) continue;
+    const float* row = A + kc * N + y * W;
+    double sum = 0.0;
+#pragma unroll 8
+    for (int x = 0; x < W; ++x) {
+      sum += static_cast<double>(row[x]) * __ldg(p.fwd_w_t + x * W + u);
+    }
+    T[i] = sum;
+  }
+  __syncthreads();
+
+  // Forward column pass into B (coefficient storage order).
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int kc = i / N, vu = i % N, v = vu / W, u = vu % W;
+    if (anchor_x[kc / 3] < 0) continue;
+    const double* col = T + kc * N + u;
+    double sum = 0.0;
+#pragma unroll 8
+    for (int y = 0; y < H; ++y) {
+      sum += __ldg(p.fwd_h + v * H + y) * col[y * W];
+    }
+    B[kc * N + S::Index(v, u)] = static_cast<float>(sum);
+  }
+  __syncthreads();
+
+  // Quantize: residual coefficients into A, sqrt terms into Tf.
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    if (anchor_x[k] < 0) continue;
+    const float* coef = B + k * 3 * N;
+    const float decorrelated = coef[c * N + j] - coef[N + j] * cfl[k][c];
+    const float scaled = decorrelated * __ldg(p.inverse_dequant + c * N + j) * quant_norm[k];
+    const float rounded = roundf(scaled);
+    const float difference = scaled - rounded;
+    A[i] = __ldg(p.dequant + c * N + j) * difference;
+    Tf[i] = sqrtf(fabsf(rounded));
+    if (rounded != 0.0f) atomicAdd(&nonzero[k][c], 1u);
+  }
+  __syncthreads();
+
+  // Ordered magnitude sums (one thread per candidate and channel).
+  if (tid < 3 * K && anchor_x[tid / 3] >= 0) {
+    const float* terms = Tf + tid * N;
+    float sum = 0.0f;
+    for (int j = 0; j < N; ++j) sum += terms[j];
+    magnitude[tid / 3][tid % 3] = sum;
+  }
+  __syncthreads();
+
+  // Inverse row pass: T[v][x] = sum_u (double)coef[index(v,u)] * inv_w[u][x].
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int kc = i / N, vx = i % N, v = vx / W, x = vx % W;
+    if (anchor_x[kc / 3] < 0) continue;
+    const float* coef = A + kc * N;
+    double sum = 0.0;
+#pragma unroll 8
+    for (int u = 0; u < W; ++u) {
+      sum += static_cast<double>(coef[S::Index(v, u)]) * __ldg(p.inv_w + u * W + x);
+    }
+    T[i] = sum;
+  }
+  __syncthreads();
+
+  // Inverse column pass into B: pixels[y][x] = sum_v inv_h[v][y] * T[v][x].
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int kc = i / N, yx = i % N, y = yx / W, x = yx % W;
+    if (anchor_x[kc / 3] < 0) continue;
+    const double* col = T + kc * N + x;
+    double sum = 0.0;
+#pragma unroll 8
+    for (int v = 0; v < H; ++v) {
+      sum += __ldg(p.inv_h + v * H + y) * col[v * W];
+    }
+    B[i] = static_cast<float>(sum);
+  }
+  __syncthreads();
+
+  // Weighted eighth powers into A.
+  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    if (anchor_x[k] < 0) continue;
+    const int y = yx / W, x = yx % W;
+    const float m = p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
+                                 anchor_x[k] * 8 + x];
+    if (!(IsFinite(m) && m > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
+    const float offset = c == 0 ? 12.0f : c == 1 ? 0.0f : 4.0f;
+    float weighted = (m + offset) * B[i];
+    weighted *= weighted;
+    weighted *= weighted;
+    weighted *= weighted;
+    A[i] = weighted;
+  }
+  __syncthreads();
+
+  if (tid < 3 * K && anchor_x[tid / 3] >= 0) {
+    const float* terms = A + tid * N;
+    float sum = 0.0f;
+    for (int j = 0; j < N; ++j) sum += terms[j];
+    loss_sum[tid / 3][tid % 3] = sum;
+  }
+  __syncthreads();
+
+  if (tid < K && anchor_x[tid] >= 0) {
+    const float kChannelMultiplier[3] = {2.0441408586549744e7f, 1.0f, 1.266770081387616f};
+    float entropy = 0.0f, loss = 0.0f;
+    for (int c = 0; c < 3; ++c) {
+      loss += loss_sum[tid][c] * kChannelMultiplier[c];
+      entropy += p.cost_delta * magnitude[tid][c];
+      const int nonzero_bits = CeilLog2Nonzero(nonzero[tid][c] + 1) + 1;
+      entropy += p.zeros_multiplier *
+                 static_cast<float>(CeilLog2Nonzero(nonzero_bits + 17) + nonzero_bits);
+      constexpr int block_count = S::CW * S::CH;
+      if (c == 0 && block_count >= 2) {
+        const float weight = 1.0f + fminf(3.0f, static_cast<float>(block_count) / 8.0f);
+        entropy *= weight;
+        loss *= weight;
+      }
+    }
+    const float normalized_loss = loss / static_cast<float>(N);
+    // std::pow(float, 1/8): evaluated in double and rounded to float.
+    const float root = static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125));
+    const float loss_cost = root * static_cast<float>(N) / quant_norm[tid];
+    const float result =
+      entropy * p.entropy_multiplier + p.info_loss_multiplier * loss_cost;
+    if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
+    p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Greedy merge (one thread per 64x64 tile).
+
+struct SearchParams {
+  const float* costs;  // [7][blocks] family planes
+  uint32_t blocks_x, blocks_y, tiles_x, tiles_y;
+  float baseline_multiplier;  // DCT8 cost multiplier
+  int dct32_step;
+  uint8_t* cells;  // blocks_x x blocks_y, (strategy << 1) | anchor
+  uint32_t* error;
+};
+
+__device__ __forceinline__ int CoveredW(int s) {
+  return s == kDct16x16 ? 2 : s == kDct32x32 ? 4 : s == kDct8x16 ? 2 : s == kDct32x16 ? 2
+       : s == kDct16x32 ? 4 : 1;
+}
+__device__ __forceinline__ int CoveredH(int s) {
+  return s == kDct16x16 ? 2 : s == kDct32x32 ? 4 : s == kDct16x8 ? 2 : s == kDct32x16 ? 4
+       : s == kDct16x32 ? 2 : 1;
+}
+
+struct TileState {
+  uint8_t cell[64];
+  float cost[64];
+  uint8_t priority[64];
+  int tile_w, tile_h;
+  int bx0, by0;
+};
+
+__device__ __forceinline__ uint8_t Encode(int s, bool anchor) {
+  return static_cast<uint8_t>((s << 1) | (anchor ? 1 : 0));
+}
+
+__device__ void SetCells(TileState& t, int lx, int ly, int s) {
+  const int cw = CoveredW(s), ch = CoveredH(s);
+  for (int dy = 0; dy < ch; ++dy)
+    for (int dx = 0; dx < cw; ++dx) t.cell[(ly + dy) * 8 + lx + dx] = Encode(s, dx == 0 && dy == 0);
+}
+
+// SearchGrid::CrossesHorizontalBoundary / CrossesVerticalBoundary
+// (ac_strategy.cpp:155-200), restricted to the tile (which they never leave).
+__device__ bool CrossesHorizontal(const TileState& t, int start_x, int y, int end_x) {
+  if (start_x >= t.tile_w || y >= t.tile_h || y % 8 == 0) return false;
+  end_x = min(end_x, t.tile_w);
+  while (start_x != 0 && !(t.cell[y * 8 + start_x] & 1)) --start_x;
+  for (int x = start_x; x < end_x;) {
+    const uint8_t c = t.cell[y * 8 + x];
+    if (!(c & 1)) return true;
+    x += CoveredW(c >> 1);
+  }
+  return false;
+}
+
+__device__ bool CrossesVertical(const TileState& t, int x, int start_y, int end_y) {
+  if (x >= t.tile_w || start_y >= t.tile_h || x % 8 == 0) return false;
+  end_y = min(end_y, t.tile_h);
+  while (start_y != 0 && !(t.cell[start_y * 8 + x] & 1)) --start_y;
+  for (int y = start_y; y < end_y;) {
+    const uint8_t c = t.cell[y * 8 + x];
+    if (!(c & 1)) return true;
+    y += CoveredH(c >> 1);
+  }
+  return false;
+}
+
+__device__ float Cost(const SearchParams& p, const TileState& t, int s, int lx, int ly) {
+  const int f = FamilyOfStrategy(s);
+  const size_t blocks = static_cast<size_t>(p.blocks_x) * p.blocks_y;
+  const float v = p.costs[f * blocks + static_cast<size_t>(t.by0 + ly) * p.blocks_x + t.bx0 + lx];
+  if (!(IsFinite(v) && v >= 0.0f)) RaiseError(p.error, kErrorInternal);
+  return v;
+}
+
+__device__ void SetCost(TileState& t, int lx, int ly, int s, float cost) {
+  const int cw = CoveredW(s), ch = CoveredH(s);
+  for (int dy = 0; dy < ch; ++dy)
+    for (int dx = 0; dx < cw; ++dx) t.cost[(ly + dy) * 8 + lx + dx] = 0.0f;
+  t.cost[ly * 8 + lx] = cost;
+}
+
+// TryMerge (ac_strategy.cpp:340-386).
+__device__ void TryMerge(const SearchParams& p, TileState& t, int s, int lx, int ly,
+                         uint8_t priority) {
+  const int cw = CoveredW(s), ch = CoveredH(s);
+  float current = 0.0f;
+  for (int dy = 0; dy < ch; ++dy) {
+    for (int dx = 0; dx < cw; ++dx) {
+      const int i = (ly + dy) * 8 + lx + dx;
+      if (t.priority[i] >= priority) return;
+      current += t.cost[i];
+    }
+  }
+  const float candidate = Cost(p, t, s, lx, ly);
+  if (!(candidate < current)) return;
+  for (int dy = 0; dy < ch; ++dy) {
+    for (int dx = 0; dx < cw; ++dx) {
+      const int i = (ly + dy) * 8 + lx + dx;
+      t.cost[i] = 0.0f;
+      t.priority[i] = priority;
+    }
+  }
+  SetCells(t, lx, ly, s);
+  t.cost[ly * 8 + lx] = candidate;
+}
+
+// FindBestFirstLevelDivision (ac_strategy.cpp:406-589).
+__device__ void FirstLevelDivision(const SearchParams& p, TileState& t, int blocks, int lx,
+                                   int ly) {
+  const int half = blocks / 2;
+  if (CrossesHorizontal(t, lx, ly, lx + blocks) ||
+      CrossesHorizontal(t, lx, ly + blocks, lx + blocks) ||
+      CrossesVertical(t, lx, ly, ly + blocks) ||
+      CrossesVertical(t, lx + blocks, ly, ly + blocks)) {
+    return;
+  }
+  const bool allow_vertical = !CrossesVertical(t, lx + half, ly, ly + blocks);
+  const bool allow_horizontal = !CrossesHorizontal(t, lx, ly + half, lx + blocks);
+  float quadrant[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+  for (int dy = 0; dy < blocks; ++dy)
+    for (int dx = 0; dx < blocks; ++dx)
+      quadrant[dy / half][dx / half] += t.cost[(ly + dy) * 8 + lx + dx];
+  const float kUnavailable = 3.40282347e+38f;
+  float vl = kUnavailable, vr = kUnavailable, ht = kUnavailable, hb = kUnavailable;
+  const int vs = blocks == 2 ? kDct16x8 : kDct32x16;
+  const int hs = blocks == 2 ? kDct8x16 : kDct16x32;
+  const int ss = blocks == 2 ? kDct16x16 : kDct32x32;
+  if (allow_vertical) {
+    if ((t.cell[ly * 8 + lx] >> 1) != vs) vl = Cost(p, t, vs, lx, ly);
+    if ((t.cell[ly * 8 + lx + half] >> 1) != vs) vr = Cost(p, t, vs, lx + half, ly);
+  }
+  if (allow_horizontal) {
+    if ((t.cell[ly * 8 + lx] >> 1) != hs) ht = Cost(p, t, hs, lx, ly);
+    if ((t.cell[(ly + half) * 8 + lx] >> 1) != hs) hb = Cost(p, t, hs, lx, ly + half);
+  }
+  const float square = Cost(p, t, ss, lx, ly);
+  const float vertical_cost = fminf(vl, quadrant[0][0] + quadrant[1][0]) +
+                              fminf(vr, quadrant[0][1] + quadrant[1][1]);
+  const float horizontal_cost = fminf(ht, quadrant[0][0] + quadrant[0][1]) +
+                                fminf(hb, quadrant[1][0] + quadrant[1][1]);
+  // ChooseFirstLevelDivision (ac_strategy_search_policy.h:69-83).
+  if (square < vertical_cost && square < horizontal_cost) {
+    SetCells(t, lx, ly, ss);
+    SetCost(t, lx, ly, ss, square);
+  } else if (vertical_cost < horizontal_cost) {
+    if (vl < quadrant[0][0] + quadrant[1][0]) {
+      SetCells(t, lx, ly, vs);
+      SetCost(t, lx, ly, vs, vl);
+    }
+    if (vr < quadrant[0][1] + quadrant[1][1]) {
+      SetCells(t, lx + half, ly, vs);
+      SetCost(t, lx + half, ly, vs, vr);
+    }
+  } else {
+    if (ht < quadrant[0][0] + quadrant[0][1]) {
+      SetCells(t, lx, ly, hs);
+      SetCost(t, lx, ly, hs, ht);
+    }
+    if (hb < quadrant[1][0] + quadrant[1][1]) {
+      SetCells(t, lx, ly + half, hs);
+      SetCost(t, lx, ly + half, hs, hb);
+    }
+  }
+}
+
+// SearchTile (ac_strategy.cpp:591-773).
+__global__ void __launch_bounds__(64) SearchTileKernel(const __grid_constant__ SearchParams p) {
+  const uint32_t tile = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tile >= p.tiles_x * p.tiles_y) return;
+  TileState t;
+  const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+  t.bx0 = tx * 8;
+  t.by0 = ty * 8;
+  t.tile_w = min(8, static_cast<int>(p.blocks_x) - t.bx0);
+  t.tile_h = min(8, static_cast<int>(p.blocks_y) - t.by0);
+  for (int i = 0; i < 64; ++i) {
+    t.cell[i] = Encode(kDct8, true);
+    t.cost[i] = 0.0f;
+    t.priority[i] = 0;
+  }
+  const int w = t.tile_w, h = t.tile_h;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) t.cost[y * 8 + x] = Cost(p, t, kDct8, x, y) * p.baseline_multiplier;
+
+  const int merge_strategy[4] = {kDct16x8, kDct8x16, kDct16x32, kDct32x16};
+  const uint8_t merge_priority[4] = {2, 2, 4, 4};
+  for (int m = 0; m < 4; ++m) {
+    const int s = merge_strategy[m];
+    const int cw = CoveredW(s), ch = CoveredH(s);
+    for (int y = 0; y + ch <= h; y += ch) {
+      for (int x = 0; x + cw <= w; x += cw) {
+        if (y + 3 < h && x + 3 < w) {
+          if (s == kDct16x32) {
+            if ((y | x) % 4 == 0) FirstLevelDivision(p, t, 4, x, y);
+            continue;
+          }
+          if (s == kDct32x16) continue;
+        }
+        if ((s == kDct16x32 && y % 4 != 0) || (s == kDct32x16 && x % 4 != 0)) continue;
+        if (y + 1 < h && x + 1 < w) {
+          if (s == kDct8x16) {
+            if ((y | x) % 2 == 0) FirstLevelDivision(p, t, 2, x, y);
+            continue;
+          }
+          if (s == kDct16x8) continue;
+        }
+        if ((s == kDct8x16 && y % 2 == 1) || (s == kDct16x8 && x % 2 == 1)) continue;
+        TryMerge(p, t, s, x, y, merge_priority[m]);
+      }
+    }
+  }
+  for (int y = 0; y + 1 < h; ++y)
+    for (int x = 0; x + 1 < w; ++x)
+      if ((y | x) % 2 != 0) FirstLevelDivision(p, t, 2, x, y);
+  for (int y = 0; y + 3 < h; y += p.dct32_step)
+    for (int x = 0; x + 3 < w; x += p.dct32_step)
+      if ((y | x) % 4 != 0) FirstLevelDivision(p, t, 4, x, y);
+
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x)
+      p.cells[static_cast<size_t>(t.by0 + y) * p.blocks_x + t.bx0 + x] = t.cell[y * 8 + x];
+}
+
+template <int W, int H>
+int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t stream) {
+  using S = Shape<W, H>;
+  const int table = StrategyTableFamily(kFamilyStrategy[family]);
+  const HostTables& h = GetHostTables();
+  p.dequant = d.dequant + h.layout.offset[table];
+  p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2;
+  const int hi = H == 8 ? 0 : H == 16 ? 1 : 2;
+  p.fwd_w_t = d.forward_t[wi];
+  p.fwd_h = d.forward[hi];
+  p.inv_w = d.inverse[wi];
+  p.inv_h = d.inverse[hi];
+  p.entropy_multiplier = kFamilyEntropy[family];
+  const int cw = kFamilyCoveredW[family], ch = kFamilyCoveredH[family];
+  p.local_x = (8 - cw) / p.anchor_step + 1;
+  p.local_y = (8 - ch) / p.anchor_step + 1;
+  const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  const size_t smem = static_cast<size_t>(S::K) * 3 * S::N * (4 + 4 + 8);
+  int status = CheckCuda(cudaFuncSetAttribute(CandidateCostKernel<W, H>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)),
+                         "ac_strategy smem attribute");
+  if (status != GJXL_B200_OK) return status;
+  const unsigned grid = (count + S::K - 1) / S::K;
+  CandidateCostKernel<W, H><<<grid, kCostThreads, smem, stream>>>(p, count);
+  return CheckLaunch("ac_strategy candidate costs");
+}
+
+}  // namespace
+
+size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y) {
+  return kFamilyCount * blocks_x * blocks_y;
+}
+
+int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
+                          const float* quant_field, const float* pixel_mask, size_t mask_stride,
+                          const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
+                          float* costs, uint32_t* error, cudaStream_t stream) {
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const size_t bx = pw / 8, by = ph / 8;
+  // Reset the table so anchors that are never evaluated read as NaN.
+  status = CheckCuda(cudaMemsetAsync(costs, 0xff, AcStrategyCostFloats(bx, by) * sizeof(float),
+                                     stream), "ac_strategy memset");
+  if (status != GJXL_B200_OK) return status;
+  CostParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.opsin = opsin;
+  p.stride = stride;
+  p.pitch = pitch;
+  p.quant_field = quant_field;
+  p.pixel_mask = pixel_mask;
+  p.mask_stride = mask_stride;
+  p.y_to_x = y_to_x;
+  p.y_to_b = y_to_b;
+  p.blocks_x = static_cast<uint32_t>(bx);
+  p.blocks_y = static_cast<uint32_t>(by);
+  p.tiles_x = static_cast<uint32_t>((bx + 7) / 8);
+  p.tiles_y = static_cast<uint32_t>((by + 7) / 8);
+  // Target-dependent constants (ac_strategy.cpp:880-888), with the host
+  // C library's powf exactly as in the reference.
+  const float kBias = 0.13731742964354549f;
+  const float ratio = (target + kBias) / (1.0f + kBias);
+  p.info_loss_multiplier = 1.2f * std::pow(ratio, 0.33677806662454718f);
+  p.zeros_multiplier = 9.3089059022677905f * std::pow(ratio, 0.50990926717963703f);
+  p.cost_delta = 10.833273317067883f * std::pow(ratio, 0.36702940662370243f);
+  p.error = error;
+  for (int f = 0; f < kFamilyCount && status == GJXL_B200_OK; ++f) {
+    CostParams q = p;
+    q.anchor_step = (dense && f >= 4) ? 1 : kFamilyStep[f];
+    q.costs = costs + f * bx * by;
+    switch (f) {
+      case 0: status = LaunchFamily<8, 8>(q, d, f, stream); break;
+      case 1: status = LaunchFamily<8, 16>(q, d, f, stream); break;
+      case 2: status = LaunchFamily<16, 8>(q, d, f, stream); break;
+      case 3: status = LaunchFamily<16, 16>(q, d, f, stream); break;
+      case 4: status = LaunchFamily<16, 32>(q, d, f, stream); break;
+      case 5: status = LaunchFamily<32, 16>(q, d, f, stream); break;
+      case 6: status = LaunchFamily<32, 32>(q, d, f, stream); break;
+    }
+  }
+  return status;
+}
+
+int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float target, bool dense,
+                           uint8_t* cells, uint32_t* error, cudaStream_t stream) {
+  SearchParams p;
+  p.costs = costs;
+  p.blocks_x = static_cast<uint32_t>(pw / 8);
+  p.blocks_y = static_cast<uint32_t>(ph / 8);
+  p.tiles_x = (p.blocks_x + 7) / 8;
+  p.tiles_y = (p.blocks_y + 7) / 8;
+  // SearchTile baseline multiplier (ac_strategy.cpp:612-617).
+  p.baseline_multiplier = 1.0f + -0.4f / (target + 1.4f);
+  p.dct32_step = dense ? 1 : 2;
+  p.cells = cells;
+  p.error = error;
+  const unsigned tiles = p.tiles_x * p.tiles_y;
+  SearchTileKernel<<<(tiles + 63) / 64, 64, 0, stream>>>(p);
+  return CheckLaunch("ac_strategy search");
+}
+
+}  // namespace gjxl_b200
+
+using namespace gjxl_b200;
+
+extern "C" size_t gjxl_b200_ac_strategy_cost_bytes(size_t padded_width, size_t padded_height) {
+  return AcStrategyCostFloats(padded_width / 8, padded_height / 8) * sizeof(float);
+}
+
+extern "C" int gjxl_b200_ac_strategy_costs(
+  const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch, size_t padded_width,
+  size_t padded_height, const float* quant_field, const float* pixel_mask,
+  size_t pixel_mask_stride, const int8_t* y_to_x, const int8_t* y_to_b,
+  float butteraugli_target, int dense_dct32, float* costs, uint32_t* device_error,
+  void* stream) {
+  ClearLastError();
+  if (opsin == nullptr || quant_field == nullptr || pixel_mask == nullptr || y_to_x == nullptr ||
+      y_to_b == nullptr || costs == nullptr || padded_width % 8 || padded_height % 8 ||
+      padded_width == 0 || padded_height == 0 || opsin_stride < padded_width ||
+      opsin_plane_pitch < opsin_stride * padded_height || pixel_mask_stride < padded_width ||
+      !std::isfinite(butteraugli_target) || butteraugli_target <= 0.0f ||
+      padded_width > (1u << 30) || padded_height > (1u << 30)) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "ac_strategy_costs: invalid arguments");
+  }
+  return LaunchAcStrategyCosts(opsin, opsin_stride, opsin_plane_pitch, padded_width,
+                               padded_height, quant_field, pixel_mask, pixel_mask_stride, y_to_x,
+                               y_to_b, butteraugli_target, dense_dct32 != 0, costs, device_error,
+                               static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gjxl_b200_ac_strategy_search(
+  const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch, size_t padded_width,
+  size_t padded_height, const float* quant_field, const float* pixel_mask,
+  size_t pixel_mask_stride, const int8_t* y_to_x, const int8_t* y_to_b,
+  float butteraugli_target, int dense_dct32, float* costs, uint8_t* cells,
+  uint32_t* device_error, void* stream) {
+  int status = gjxl_b200_ac_strategy_costs(opsin, opsin_stride, opsin_plane_pitch, padded_width,
+                                           padded_height, quant_field, pixel_mask,
+                                           pixel_mask_stride, y_to_x, y_to_b,
+                                           butteraugli_target, dense_dct32, costs, device_error,
+                                           stream);
+  if (status != GJXL_B200_OK) return status;
+  if (cells == nullptr) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "ac_strategy_search: cells is null");
+  }
+  return LaunchAcStrategySearch(costs, padded_width, padded_height, butteraugli_target,
+                                dense_dct32 != 0, cells, device_error,
+                                static_cast<cudaStream_t>(stream));
+}

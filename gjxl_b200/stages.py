@@ -68,3 +68,31 @@ def gaborish_inverse(src: torch.Tensor, dst: torch.Tensor, width: int, height: i
               src.shape[1] * src.shape[2], dst.data_ptr(), dst.shape[2],
               dst.shape[1] * dst.shape[2], width, height, ctypes.addressof(m),
               None if device_error is None else device_error.data_ptr(), _stream())
+
+
+def ac_strategy_cost_bytes(padded_width: int, padded_height: int) -> int:
+    return _lib.load().gjxl_b200_ac_strategy_cost_bytes(padded_width, padded_height)
+
+
+def _search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense):
+    return (opsin.data_ptr(), opsin.shape[2], opsin.shape[1] * opsin.shape[2], opsin.shape[2],
+            opsin.shape[1], quant_field.data_ptr(), pixel_mask.data_ptr(), pixel_mask.shape[-1],
+            y_to_x.data_ptr(), y_to_b.data_ptr(), target, int(dense))
+
+
+def ac_strategy_costs(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, target=1.0,
+                      dense=False, device_error=None):
+    """opsin: (3, PH, PW) Gaborish-inverted XYB; costs: float tensor of
+    ac_strategy_cost_bytes() bytes."""
+    _lib.call("gjxl_b200_ac_strategy_costs",
+              *_search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense),
+              costs.data_ptr(), None if device_error is None else device_error.data_ptr(),
+              _stream())
+
+
+def ac_strategy_search(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, cells,
+                       target=1.0, dense=False, device_error=None):
+    _lib.call("gjxl_b200_ac_strategy_search",
+              *_search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense),
+              costs.data_ptr(), cells.data_ptr(),
+              None if device_error is None else device_error.data_ptr(), _stream())

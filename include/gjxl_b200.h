@@ -125,6 +125,56 @@ GJXL_B200_API int gjxl_b200_gaborish_inverse(
     size_t width, size_t height, const float* multipliers,
     uint32_t* device_error, void* stream);
 
+/*
+ * Default AC quantization matrix of one searched strategy and channel, in the
+ * reference's coefficient layout (GetDefaultQuantizationMatrix,
+ * src/codec/quantization.cpp:646-703). HOST outputs of `capacity` floats.
+ */
+GJXL_B200_API int gjxl_b200_quant_matrix(int strategy, int channel,
+                                         float* dequant,
+                                         float* inverse_dequant,
+                                         size_t capacity);
+
+/*
+ * AC-strategy candidate costs (rows a6, a8).
+ * Replaces GpuAcStrategyEvaluation (src/gpu/ops/ac_strategy.h:118-170) as run
+ * by LaunchCudaAcStrategyBatch / FusedAcStrategyKernel
+ * (src/gpu/cuda/cuda_ac_strategy.cpp:500-515, src/gpu/cuda/cuda_kernels.cu:653)
+ * and the CPU EstimateAcStrategyCost (src/codec/ac_strategy.cpp:823).
+ *
+ * `opsin` is the Gaborish-inverted padded XYB image, `quant_field` the initial
+ * field (dense blocks), `pixel_mask` the blurred mask, `y_to_x`/`y_to_b` the
+ * initial CfL maps (dense 64x64 tiles). `costs` receives
+ * gjxl_b200_ac_strategy_cost_bytes() bytes: seven planes (DCT8, DCT16x8,
+ * DCT8x16, DCT16x16, DCT32x16, DCT16x32, DCT32x32) of one float per block,
+ * valid at candidate anchors and NaN elsewhere.
+ */
+GJXL_B200_API size_t gjxl_b200_ac_strategy_cost_bytes(size_t padded_width,
+                                                      size_t padded_height);
+GJXL_B200_API int gjxl_b200_ac_strategy_costs(
+    const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+    size_t padded_width, size_t padded_height, const float* quant_field,
+    const float* pixel_mask, size_t pixel_mask_stride, const int8_t* y_to_x,
+    const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
+    float* costs, uint32_t* device_error, void* stream);
+
+/*
+ * AC-strategy search (rows a6, a7, a8): candidate costs followed by the
+ * greedy hierarchical merge of every 64x64 tile on the device.
+ * Replaces AcStrategySearchProvider::Find (src/codec/quantization_pipeline.h:34-50)
+ * as implemented by FindAcStrategyGridGpuResident
+ * (src/gpu/ops/ac_strategy_search.h:130) and FindAcStrategyGrid
+ * (src/codec/ac_strategy.cpp:1103). `cells` receives one byte per block,
+ * (strategy << 1) | anchor, the reference's AcStrategyGrid encoding
+ * (src/core/ac_strategy.h:183-411). `costs` is the cost scratch above.
+ */
+GJXL_B200_API int gjxl_b200_ac_strategy_search(
+    const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+    size_t padded_width, size_t padded_height, const float* quant_field,
+    const float* pixel_mask, size_t pixel_mask_stride, const int8_t* y_to_x,
+    const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
+    float* costs, uint8_t* cells, uint32_t* device_error, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

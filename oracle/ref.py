@@ -26,6 +26,8 @@ _SIGNATURES = {
     "gjxl_ref_ac_strategy_cost": [_P, _Z, _Z, _P, _P, _I, _Z, _Z, _F, _F, _P, _P],
     "gjxl_ref_ac_strategy_search": [_P, _Z, _Z, _P, _P, _P, _P, _F, _I, _P],
     "gjxl_ref_butteraugli": [_P, _P, _Z, _Z, _F, _P, _P],
+    "gjxl_ref_quant_matrix": [_I, _I, _P, _P, _Z],
+    "gjxl_ref_ac_strategy_cost_table": [_P, _Z, _Z, _P, _P, _P, _P, _F, _I, _P],
 }
 
 _lib = None
@@ -176,3 +178,29 @@ def butteraugli(reference: np.ndarray, distorted: np.ndarray, intensity_target: 
     _check(lib().gjxl_ref_butteraugli(_ptr(reference), _ptr(distorted), w, h, intensity_target,
                                       _ptr(dmap), _ptr(score)), "butteraugli")
     return dmap, float(score[0])
+
+
+def quant_matrix(strategy: int, channel: int):
+    dq = np.zeros(1024, np.float32)
+    inv = np.zeros(1024, np.float32)
+    n = lib().gjxl_ref_quant_matrix(strategy, channel, _ptr(dq), _ptr(inv), 1024)
+    if n <= 0:
+        raise RuntimeError(f"quant_matrix({strategy}, {channel}) failed")
+    return dq[:n], inv[:n]
+
+
+def ac_strategy_cost_table(opsin, quant, pixel_mask, ytox, ytob, target: float = 1.0,
+                           dense: bool = False) -> np.ndarray:
+    """(7, blocks_y, blocks_x) costs; NaN where no candidate is anchored."""
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    quant = np.ascontiguousarray(quant, np.float32)
+    pixel_mask = np.ascontiguousarray(pixel_mask, np.float32)
+    ytox = np.ascontiguousarray(ytox, np.int8)
+    ytob = np.ascontiguousarray(ytob, np.int8)
+    _, ph, pw = opsin.shape
+    costs = np.full((7, ph // 8, pw // 8), np.nan, np.float32)
+    _check(lib().gjxl_ref_ac_strategy_cost_table(_ptr(opsin), pw, ph, _ptr(quant),
+                                                 _ptr(pixel_mask), _ptr(ytox), _ptr(ytob),
+                                                 target, int(dense), _ptr(costs)),
+           "ac_strategy_cost_table")
+    return costs

@@ -28,6 +28,7 @@
 #include "codec/color_transform.h"
 #include "codec/color_transform_internal.h"
 #include "codec/gaborish.h"
+#include "codec/quantization.h"
 #include "codec/quantization_pipeline.h"
 #include "codec/quantization_pipeline_internal.h"
 #include "codec/vardct_frame.h"
@@ -261,4 +262,63 @@ GJXL_REF_API int gjxl_ref_butteraugli(const float* reference_linear,
     ConstPlanar(distorted_linear, width, height), options,
     {distance_map, {width, height}, width}, score);
   return status.ok() ? 0 : Fail(status);
+}
+
+// codec/quantization.cpp GetDefaultQuantizationMatrix.
+GJXL_REF_API int gjxl_ref_quant_matrix(int strategy, int channel, float* dequant,
+                                       float* inverse_dequant, size_t capacity) {
+  QuantizationMatrixView view;
+  Status status = GetDefaultQuantizationMatrix(static_cast<AcStrategyType>(strategy),
+                                               static_cast<XybChannel>(channel), &view);
+  if (!status.ok()) return Fail(status);
+  if (capacity < view.dequant.size()) return -1;
+  std::memcpy(dequant, view.dequant.data(), view.dequant.size() * sizeof(float));
+  std::memcpy(inverse_dequant, view.inverse_dequant.data(),
+              view.inverse_dequant.size() * sizeof(float));
+  return static_cast<int>(view.dequant.size());
+}
+
+// Cost table of every candidate the search can ask for: for each of the seven
+// searched families (candidate-stage order DCT8, 16x8, 8x16, 16x16, 32x16,
+// 16x32, 32x32), EstimateAcStrategyCost at every anchor that fits inside its
+// 64x64 tile on the family's anchor step, with the stage's entropy multiplier
+// and the tile's CfL factors. Other entries are left untouched.
+GJXL_REF_API int gjxl_ref_ac_strategy_cost_table(
+  const float* opsin, size_t padded_width, size_t padded_height, const float* quant_field,
+  const float* pixel_mask, const int8_t* y_to_x, const int8_t* y_to_b,
+  float butteraugli_target, int dense_dct32, float* costs) {
+  const Extent2D blocks{padded_width / 8, padded_height / 8};
+  ColorCorrelationMap cfl;
+  Status status =
+    MakeColorCorrelation(y_to_x, y_to_b, padded_width, padded_height, &cfl);
+  if (!status.ok()) return Fail(status);
+  const int strategies[7] = {0, 6, 7, 4, 10, 11, 5};
+  const float entropy[7] = {1.0f, 1.21f, 1.21f, 1.34f, 1.49f, 1.49f, 1.48f};
+  const int steps[7] = {1, 1, 1, 1, 2, 2, 2};
+  for (int f = 0; f < 7; ++f) {
+    const AcStrategyInfo* info = GetAcStrategyInfo(static_cast<AcStrategyType>(strategies[f]));
+    const size_t cw = info->covered_blocks.width, ch = info->covered_blocks.height;
+    const size_t step = (dense_dct32 && f >= 4) ? 1 : steps[f];
+    for (size_t by = 0; by < blocks.height; ++by) {
+      for (size_t bx = 0; bx < blocks.width; ++bx) {
+        const size_t lx = bx % 8, ly = by % 8;
+        const size_t tile_w = std::min<size_t>(8, blocks.width - (bx - lx));
+        const size_t tile_h = std::min<size_t>(8, blocks.height - (by - ly));
+        if (lx % step || ly % step || lx + cw > tile_w || ly + ch > tile_h) continue;
+        float cost = 0.0f;
+        status = EstimateAcStrategyCost(
+          static_cast<AcStrategyType>(strategies[f]), bx, by,
+          ConstPlanar(opsin, padded_width, padded_height),
+          {quant_field, blocks, blocks.width},
+          {pixel_mask, {padded_width, padded_height}, padded_width},
+          {.butteraugli_target = butteraugli_target,
+           .entropy_multiplier = entropy[f],
+           .cfl_factors = cfl.AcFactors(bx / 8, by / 8)},
+          &cost);
+        if (!status.ok()) return Fail(status);
+        costs[f * blocks.width * blocks.height + by * blocks.width + bx] = cost;
+      }
+    }
+  }
+  return 0;
 }
