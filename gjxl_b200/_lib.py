@@ -27,10 +27,20 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_initial_quant_scratch_bytes": [Z, Z],
     "gjxl_b200_initial_quant_field": [P, Z, Z, Z, Z, F, F, P, P, P, Z, P, Z, P, P],
     "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
+    "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_quant_matrix": [I, I, P, P, Z],
     "gjxl_b200_ac_strategy_cost_bytes": [Z, Z],
     "gjxl_b200_ac_strategy_costs": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P],
     "gjxl_b200_ac_strategy_search": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P, P],
+    # Session entry points are bound with their struct types in session.py.
+    "gjxl_b200_default_options": None,
+    "gjxl_b200_session_create": None,
+    "gjxl_b200_session_destroy": None,
+    "gjxl_b200_session_analyze": None,
+    "gjxl_b200_session_analyze_host": None,
+    "gjxl_b200_session_outputs": None,
+    "gjxl_b200_session_stage_times": None,
+    "gjxl_b200_stage_name": None,
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
@@ -62,6 +72,8 @@ def load() -> ctypes.CDLL:
         lib = ctypes.CDLL(str(LIBRARY_PATH))
         for name, args in SIGNATURES.items():
             fn = getattr(lib, name)
+            if args is None:
+                continue
             fn.argtypes = args
             fn.restype = _RESTYPES.get(name, c_int)
         _lib = lib

@@ -1,0 +1,36 @@
+// Host-side analysis session: the B200 counterpart of the reference's
+// PreparedQuantizationPipeline + PreparedResidentInput
+// (src/codec/quantization_pipeline_internal.h:77-118,
+// src/gpu/ops/resident_input.h:34-57). Owns every device buffer for one image
+// extent and enqueues the analysis stages on the caller's stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "gjxl_b200.h"
+
+namespace gjxl_b200 {
+
+// Entry points of the stage translation units.
+int LaunchInitialQuantField(const float* opsin, size_t stride, size_t pitch, size_t pw,
+                            size_t ph, float target, float rescale, float* quant_field,
+                            float* strategy_mask, float* pixel_mask, size_t mask_stride,
+                            float* scratch, uint32_t* error, cudaStream_t stream);
+size_t InitialQuantScratchFloats(size_t padded_width, size_t padded_height);
+int LaunchGaborishInverse(const float* input, size_t in_stride, size_t in_pitch, float* output,
+                          size_t out_stride, size_t out_pitch, size_t width, size_t height,
+                          const float multipliers[3], uint32_t* error, cudaStream_t stream);
+int LaunchInitialCfl(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
+                     int8_t* y_to_x, int8_t* y_to_b, cudaStream_t stream);
+size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y);
+int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
+                          const float* quant_field, const float* pixel_mask, size_t mask_stride,
+                          const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
+                          float* costs, uint32_t* error, cudaStream_t stream);
+int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float target, bool dense,
+                           uint8_t* cells, uint32_t* error, cudaStream_t stream);
+
+}  // namespace gjxl_b200

@@ -1,0 +1,133 @@
+"""Python wrapper of the analysis session (gjxl_b200_session_* in the C ABI).
+
+The session owns its device buffers; analyses run on the current torch CUDA
+stream (or an explicit stream handle).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, Structure, c_float, c_int, c_size_t, c_uint8, c_void_p
+
+import numpy as np
+
+from . import _lib
+
+
+class Options(Structure):
+    _fields_ = [("struct_size", c_size_t), ("butteraugli_target", c_float), ("effort", c_int),
+                ("intensity_target", c_float), ("profile_stages", c_int)]
+
+
+class Outputs(Structure):
+    _fields_ = [(n, c_size_t) for n in ("padded_width", "padded_height", "blocks_x", "blocks_y",
+                                        "tiles_x", "tiles_y")] + [
+        ("linear", c_void_p), ("linear_stride", c_size_t), ("linear_plane_pitch", c_size_t),
+        ("opsin", c_void_p), ("preprocessed_opsin", c_void_p), ("opsin_stride", c_size_t),
+        ("opsin_plane_pitch", c_size_t), ("initial_quant_field", c_void_p),
+        ("strategy_mask", c_void_p), ("pixel_mask", c_void_p), ("y_to_x", c_void_p),
+        ("y_to_b", c_void_p), ("strategy_cells", c_void_p), ("matrix_scale_stats", c_void_p),
+        ("device_error", c_void_p), ("host_strategy_cells", c_void_p),
+        ("host_initial_quant_field", c_void_p), ("host_y_to_x", c_void_p),
+        ("host_y_to_b", c_void_p), ("host_matrix_scale_stats", c_void_p),
+        ("host_device_error", c_void_p), ("device_bytes", c_size_t)]
+
+
+_BOUND = False
+
+
+def _bind():
+    global _BOUND
+    if _BOUND:
+        return
+    lib = _lib.load()
+    lib.gjxl_b200_default_options.argtypes = [POINTER(Options)]
+    lib.gjxl_b200_default_options.restype = None
+    lib.gjxl_b200_session_create.argtypes = [c_size_t, c_size_t, POINTER(Options),
+                                             POINTER(c_void_p)]
+    lib.gjxl_b200_session_create.restype = c_int
+    lib.gjxl_b200_session_destroy.argtypes = [c_void_p]
+    lib.gjxl_b200_session_destroy.restype = None
+    lib.gjxl_b200_session_analyze.argtypes = [c_void_p, c_void_p, c_size_t, c_int, c_void_p]
+    lib.gjxl_b200_session_analyze.restype = c_int
+    lib.gjxl_b200_session_analyze_host.argtypes = [c_void_p, c_void_p, c_size_t, c_int, c_void_p]
+    lib.gjxl_b200_session_analyze_host.restype = c_int
+    lib.gjxl_b200_session_outputs.argtypes = [c_void_p, POINTER(Outputs)]
+    lib.gjxl_b200_session_outputs.restype = c_int
+    lib.gjxl_b200_session_stage_times.argtypes = [c_void_p, POINTER(c_float), c_int]
+    lib.gjxl_b200_session_stage_times.restype = c_int
+    lib.gjxl_b200_stage_name.argtypes = [c_int]
+    lib.gjxl_b200_stage_name.restype = ctypes.c_char_p
+    _BOUND = True
+
+
+def _check(code: int, name: str) -> int:
+    if code < 0 or code > 0 and name != "gjxl_b200_session_stage_times":
+        raise _lib.GjxlB200Error(code, name, _lib.load().gjxl_b200_last_error().decode())
+    return code
+
+
+class AnalysisSession:
+    """Runs the B200 analysis path for images of one extent."""
+
+    def __init__(self, width: int, height: int, butteraugli_target: float = 1.0,
+                 effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False):
+        _bind()
+        lib = _lib.load()
+        opts = Options()
+        lib.gjxl_b200_default_options(ctypes.byref(opts))
+        opts.butteraugli_target = butteraugli_target
+        opts.effort = effort
+        opts.intensity_target = intensity_target
+        opts.profile_stages = int(profile_stages)
+        handle = c_void_p()
+        _check(lib.gjxl_b200_session_create(width, height, ctypes.byref(opts),
+                                            ctypes.byref(handle)), "gjxl_b200_session_create")
+        self.handle = handle
+        self.width, self.height = width, height
+        self.outputs = Outputs()
+        _check(lib.gjxl_b200_session_outputs(handle, ctypes.byref(self.outputs)),
+               "gjxl_b200_session_outputs")
+
+    def close(self):
+        if self.handle:
+            _lib.load().gjxl_b200_session_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def analyze(self, device_pixels_ptr: int, row_stride: int, channels: int, stream: int = 0):
+        _check(_lib.load().gjxl_b200_session_analyze(self.handle, device_pixels_ptr, row_stride,
+                                                     channels, stream),
+               "gjxl_b200_session_analyze")
+
+    def analyze_host(self, host_pixels: np.ndarray, stream: int = 0):
+        assert host_pixels.dtype == np.uint8 and host_pixels.flags["C_CONTIGUOUS"]
+        h, w, ch = host_pixels.shape
+        _check(_lib.load().gjxl_b200_session_analyze_host(self.handle, host_pixels.ctypes.data,
+                                                          w * ch, ch, stream),
+               "gjxl_b200_session_analyze_host")
+
+    def stage_times(self) -> dict[str, float]:
+        lib = _lib.load()
+        buf = (c_float * 32)()
+        n = lib.gjxl_b200_session_stage_times(self.handle, buf, 32)
+        if n < 0 or n > 32:
+            raise _lib.GjxlB200Error(n, "stage_times", lib.gjxl_b200_last_error().decode())
+        if n == 0:
+            return {}
+        return {lib.gjxl_b200_stage_name(i).decode(): float(buf[i]) for i in range(n)}
+
+    # Host views of the results of analyze_host (valid after the stream completes).
+    def host_strategy_cells(self) -> np.ndarray:
+        o = self.outputs
+        return np.ctypeslib.as_array(ctypes.cast(o.host_strategy_cells, POINTER(c_uint8)),
+                                     shape=(o.blocks_y, o.blocks_x)).copy()
+
+    def host_error(self) -> int:
+        return int(np.ctypeslib.as_array(ctypes.cast(self.outputs.host_device_error,
+                                                     POINTER(ctypes.c_uint32)), shape=(1,))[0])

@@ -96,3 +96,10 @@ def ac_strategy_search(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, ce
               *_search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense),
               costs.data_ptr(), cells.data_ptr(),
               None if device_error is None else device_error.data_ptr(), _stream())
+
+
+def initial_cfl(opsin: torch.Tensor, y_to_x: torch.Tensor, y_to_b: torch.Tensor):
+    """opsin: (3, PH, PW) Gaborish-inverted XYB; outputs int8 per 64x64 tile."""
+    _lib.call("gjxl_b200_initial_cfl", opsin.data_ptr(), opsin.shape[2],
+              opsin.shape[1] * opsin.shape[2], opsin.shape[2], opsin.shape[1],
+              y_to_x.data_ptr(), y_to_b.data_ptr(), _stream())

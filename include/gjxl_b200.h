@@ -126,6 +126,22 @@ GJXL_B200_API int gjxl_b200_gaborish_inverse(
     uint32_t* device_error, void* stream);
 
 /*
+ * Initial chroma-from-luma map (row a5).
+ * Replaces the CPU path's ComputeInitialColorCorrelationMap
+ * (src/codec/chroma_from_luma.cpp:434) and the CUDA InitialCflKernel
+ * (src/gpu/cuda/cuda_aq_kernels.cu:426) behind
+ * PreparedQuantizationPipeline preprocessing
+ * (src/codec/quantization_pipeline.cpp:155-213). Input: the Gaborish-inverted
+ * padded XYB image. Outputs: int8 y_to_x and y_to_b per 64x64 tile (dense,
+ * ceil(padded_width/64) x ceil(padded_height/64)).
+ */
+GJXL_B200_API int gjxl_b200_initial_cfl(const float* opsin, size_t opsin_stride,
+                                        size_t opsin_plane_pitch,
+                                        size_t padded_width,
+                                        size_t padded_height, int8_t* y_to_x,
+                                        int8_t* y_to_b, void* stream);
+
+/*
  * Default AC quantization matrix of one searched strategy and channel, in the
  * reference's coefficient layout (GetDefaultQuantizationMatrix,
  * src/codec/quantization.cpp:646-703). HOST outputs of `capacity` floats.
@@ -174,6 +190,82 @@ GJXL_B200_API int gjxl_b200_ac_strategy_search(
     const float* pixel_mask, size_t pixel_mask_stride, const int8_t* y_to_x,
     const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
     float* costs, uint8_t* cells, uint32_t* device_error, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Analysis session: the whole analysis path for one image extent.
+ *
+ * Replaces the reference's prepared pipeline objects and their GPU providers:
+ * PrepareResidentInput + PrepareResidentQuantizationPipeline +
+ * RunPreparedGpuQuantizationPipelineForEncoding
+ * (src/gpu/ops/resident_input.h:75-95,
+ * src/codec/quantization_pipeline_internal.h:153-160,
+ * src/gpu/ops/quantization_pipeline.cpp:970). A session owns all device
+ * buffers for its extent (allocated once at creation) and enqueues every
+ * stage on the caller's stream; independent sessions may run concurrently on
+ * different streams, one session must not be used by two calls at once.
+ * ------------------------------------------------------------------------ */
+
+typedef struct gjxl_b200_options {
+  size_t struct_size;       /* sizeof(gjxl_b200_options) */
+  float butteraugli_target; /* distance; reference default 1.0 */
+  int effort;               /* 5..10 (mixed-transform search); default 7 */
+  float intensity_target;   /* XYB intensity target; the workflow uses 255 */
+  int profile_stages;       /* nonzero: record CUDA events around each stage */
+} gjxl_b200_options;
+
+typedef struct gjxl_b200_outputs {
+  size_t padded_width, padded_height, blocks_x, blocks_y, tiles_x, tiles_y;
+  /* Device views (valid until the session is destroyed). */
+  const float* linear;             /* 3 planes, unpadded */
+  size_t linear_stride, linear_plane_pitch;
+  const float* opsin;              /* padded XYB */
+  const float* preprocessed_opsin; /* Gaborish-inverted XYB */
+  size_t opsin_stride, opsin_plane_pitch;
+  const float* initial_quant_field; /* blocks */
+  const float* strategy_mask;       /* blocks */
+  const float* pixel_mask;          /* padded pixels, stride opsin_stride */
+  const int8_t* y_to_x;             /* tiles */
+  const int8_t* y_to_b;
+  const uint8_t* strategy_cells;    /* blocks, (strategy << 1) | anchor */
+  const float* matrix_scale_stats;  /* x_edge, b_edge, exposed_blue */
+  const uint32_t* device_error;
+  /* Pinned host mirrors, filled by gjxl_b200_session_analyze_host once the
+   * stream has completed. */
+  const uint8_t* host_strategy_cells;
+  const float* host_initial_quant_field;
+  const int8_t* host_y_to_x;
+  const int8_t* host_y_to_b;
+  const float* host_matrix_scale_stats;
+  const uint32_t* host_device_error;
+  size_t device_bytes;
+} gjxl_b200_outputs;
+
+typedef struct gjxl_b200_session gjxl_b200_session;
+
+GJXL_B200_API void gjxl_b200_default_options(gjxl_b200_options* options);
+GJXL_B200_API int gjxl_b200_session_create(size_t width, size_t height,
+                                           const gjxl_b200_options* options,
+                                           gjxl_b200_session** session);
+GJXL_B200_API void gjxl_b200_session_destroy(gjxl_b200_session* session);
+/* Device-resident input: packed 8-bit sRGB already in device memory. */
+GJXL_B200_API int gjxl_b200_session_analyze(gjxl_b200_session* session,
+                                            const uint8_t* pixels,
+                                            size_t row_stride_bytes,
+                                            int channels, void* stream);
+/* Host input: one host-to-device copy of the packed pixels, the analysis,
+ * and device-to-host copies of the results into the host mirrors. */
+GJXL_B200_API int gjxl_b200_session_analyze_host(gjxl_b200_session* session,
+                                                 const uint8_t* host_pixels,
+                                                 size_t row_stride_bytes,
+                                                 int channels, void* stream);
+GJXL_B200_API int gjxl_b200_session_outputs(const gjxl_b200_session* session,
+                                            gjxl_b200_outputs* outputs);
+/* Per-stage milliseconds of the last analysis (profile_stages only; call
+ * after the stream completed). Returns the number of stages written. */
+GJXL_B200_API int gjxl_b200_session_stage_times(gjxl_b200_session* session,
+                                                float* milliseconds,
+                                                int capacity);
+GJXL_B200_API const char* gjxl_b200_stage_name(int stage);
 
 #ifdef __cplusplus
 }  /* extern "C" */
