@@ -32,6 +32,10 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_ac_strategy_cost_bytes": [Z, Z],
     "gjxl_b200_ac_strategy_costs": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P],
     "gjxl_b200_ac_strategy_search": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P, P],
+    "gjxl_b200_butteraugli_create": [Z, Z, F, P],
+    "gjxl_b200_butteraugli_destroy": None,
+    "gjxl_b200_butteraugli_prepare": [P, P, Z, Z, P],
+    "gjxl_b200_butteraugli_compare": [P, P, Z, Z, P, Z, P, P, P],
     # Session entry points are bound with their struct types in session.py.
     "gjxl_b200_default_options": None,
     "gjxl_b200_session_create": None,

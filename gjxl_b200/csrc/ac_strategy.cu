@@ -167,31 +167,58 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
+  // The four FP64 passes are register-tiled: each work item produces four
+  // adjacent outputs of one row, so every shared-memory operand feeds four
+  // multiply-adds. Each output is still one sequential double sum in the
+  // reference's order.
+  constexpr int kItems = K * 3 * N / 4;
+
   // Forward row pass: T[y][u] = sum_x (double)pixel[y][x] * basis_w[u][x].
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int kc = i / N, yu = i % N, y = yu / W, u = yu % W;
+  for (int item = tid; item < kItems; item += kCostThreads) {
+    const int i = item * 4, kc = i / N, yu = i % N, y = yu / W, u0 = yu % W;
     if (anchor_x[kc / 3] < 0) continue;
     const float* row = A + kc * N + y * W;
-    double sum = 0.0;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll 8
     for (int x = 0; x < W; ++x) {
-      sum += static_cast<double>(row[x]) * __ldg(p.fwd_w_t + x * W + u);
+      const double px = static_cast<double>(row[x]);
+      const double2 b01 = __ldg(reinterpret_cast<const double2*>(p.fwd_w_t + x * W + u0));
+      const double2 b23 = __ldg(reinterpret_cast<const double2*>(p.fwd_w_t + x * W + u0 + 2));
+      s0 += px * b01.x;
+      s1 += px * b01.y;
+      s2 += px * b23.x;
+      s3 += px * b23.y;
     }
-    T[i] = sum;
+    double* out = T + i;
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
+    out[3] = s3;
   }
   __syncthreads();
 
-  // Forward column pass into B (coefficient storage order).
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int kc = i / N, vu = i % N, v = vu / W, u = vu % W;
+  // Forward column pass into B (coefficient storage order):
+  // coef[index(v, u)] = sum_y basis_h[v][y] * T[y][u].
+  for (int item = tid; item < kItems; item += kCostThreads) {
+    const int i = item * 4, kc = i / N, vu = i % N, v = vu / W, u0 = vu % W;
     if (anchor_x[kc / 3] < 0) continue;
-    const double* col = T + kc * N + u;
-    double sum = 0.0;
+    const double* col = T + kc * N + u0;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll 8
     for (int y = 0; y < H; ++y) {
-      sum += __ldg(p.fwd_h + v * H + y) * col[y * W];
+      const double b = __ldg(p.fwd_h + v * H + y);
+      const double2 t01 = *reinterpret_cast<const double2*>(col + y * W);
+      const double2 t23 = *reinterpret_cast<const double2*>(col + y * W + 2);
+      s0 += b * t01.x;
+      s1 += b * t01.y;
+      s2 += b * t23.x;
+      s3 += b * t23.y;
     }
-    B[kc * N + S::Index(v, u)] = static_cast<float>(sum);
+    float* coef = B + kc * N;
+    coef[S::Index(v, u0 + 0)] = static_cast<float>(s0);
+    coef[S::Index(v, u0 + 1)] = static_cast<float>(s1);
+    coef[S::Index(v, u0 + 2)] = static_cast<float>(s2);
+    coef[S::Index(v, u0 + 3)] = static_cast<float>(s3);
   }
   __syncthreads();
 
@@ -220,30 +247,50 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __syncthreads();
 
   // Inverse row pass: T[v][x] = sum_u (double)coef[index(v,u)] * inv_w[u][x].
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int kc = i / N, vx = i % N, v = vx / W, x = vx % W;
+  for (int item = tid; item < kItems; item += kCostThreads) {
+    const int i = item * 4, kc = i / N, vx = i % N, v = vx / W, x0 = vx % W;
     if (anchor_x[kc / 3] < 0) continue;
     const float* coef = A + kc * N;
-    double sum = 0.0;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll 8
     for (int u = 0; u < W; ++u) {
-      sum += static_cast<double>(coef[S::Index(v, u)]) * __ldg(p.inv_w + u * W + x);
+      const double c = static_cast<double>(coef[S::Index(v, u)]);
+      const double2 b01 = __ldg(reinterpret_cast<const double2*>(p.inv_w + u * W + x0));
+      const double2 b23 = __ldg(reinterpret_cast<const double2*>(p.inv_w + u * W + x0 + 2));
+      s0 += c * b01.x;
+      s1 += c * b01.y;
+      s2 += c * b23.x;
+      s3 += c * b23.y;
     }
-    T[i] = sum;
+    double* out = T + i;
+    out[0] = s0;
+    out[1] = s1;
+    out[2] = s2;
+    out[3] = s3;
   }
   __syncthreads();
 
   // Inverse column pass into B: pixels[y][x] = sum_v inv_h[v][y] * T[v][x].
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int kc = i / N, yx = i % N, y = yx / W, x = yx % W;
+  for (int item = tid; item < kItems; item += kCostThreads) {
+    const int i = item * 4, kc = i / N, yx = i % N, y = yx / W, x0 = yx % W;
     if (anchor_x[kc / 3] < 0) continue;
-    const double* col = T + kc * N + x;
-    double sum = 0.0;
+    const double* col = T + kc * N + x0;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll 8
     for (int v = 0; v < H; ++v) {
-      sum += __ldg(p.inv_h + v * H + y) * col[v * W];
+      const double b = __ldg(p.inv_h + v * H + y);
+      const double2 t01 = *reinterpret_cast<const double2*>(col + v * W);
+      const double2 t23 = *reinterpret_cast<const double2*>(col + v * W + 2);
+      s0 += b * t01.x;
+      s1 += b * t01.y;
+      s2 += b * t23.x;
+      s3 += b * t23.y;
     }
-    B[i] = static_cast<float>(sum);
+    float* out = B + i;
+    out[0] = static_cast<float>(s0);
+    out[1] = static_cast<float>(s1);
+    out[2] = static_cast<float>(s2);
+    out[3] = static_cast<float>(s3);
   }
   __syncthreads();
 

@@ -1,0 +1,990 @@
+// Rows a14/a15: Butteraugli distance map, its multiscale combination and
+// global maximum, with a prepared (cached) reference image.
+//
+// Restates the reference's scalar Butteraugli (adapted there from libjxl):
+//   src/codec/butteraugli_internal.cpp   Gaussian blurs (Separable5 :206-260,
+//     ConvolutionWithTranspose :309-423, kernel :588-621), OpsinDynamicsImage
+//     (:623-684), SeparateFrequencies (:728-856);
+//   src/codec/butteraugli_distance_internal.cpp  Malta units (:156-281),
+//     masking (:283-317, :561-628), L2 terms (:405-516), MaltaDiffMap
+//     (:518-586), ComputeDifferenceStages (:657-851), multiscale driver
+//     (:853-990), prepared reference (:992-1202).
+// Every float operation keeps the reference's association and rounding:
+// Highway's scalar MulAdd is an unfused multiply then add (--fmad=false), the
+// mixed float/double steps of the Malta scaling and the masks are done in
+// double exactly where the reference promotes, and the blur kernels come from
+// the host C library's exp() exactly as in the reference.
+//
+// The reference blurs with two "convolve rows, write transposed" passes; here
+// the second pass reads columns directly (same per-output arithmetic, no
+// transposed copy). Planes are dense float32 (stride = width).
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "host_util.h"
+
+namespace gjxl_b200 {
+namespace {
+
+constexpr int kThreads = 256;
+
+// --------------------------------------------------------------------------
+// Blur kernels.
+
+struct Kernel17 {
+  float raw[33];     // unnormalized taps, index -r..r -> 0..2r
+  float scaled[17];  // raw[i] * (1 / sum(raw)), i <= r
+  float w5[3];       // Separable5 weights (center, +-1, +-2)
+};
+
+// Mirror (butteraugli_internal.cpp:196-204): reflect with the edge repeated.
+__device__ __forceinline__ int MirrorB(int c, int size) {
+  while (c < 0 || c >= size) c = c < 0 ? -c - 1 : 2 * size - 1 - c;
+  return c;
+}
+
+__device__ __forceinline__ float HorizontalSeparable5(const float* row, int x, int w,
+                                                      const Kernel17& k) {
+  float r = row[x] * k.w5[0];
+  r = (row[MirrorB(x - 1, w)] + row[MirrorB(x + 1, w)]) * k.w5[1] + r;
+  r = (row[MirrorB(x - 2, w)] + row[MirrorB(x + 2, w)]) * k.w5[2] + r;
+  return r;
+}
+
+// Separable5 (butteraugli_internal.cpp:222-260), one output per thread.
+__global__ void __launch_bounds__(kThreads)
+Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
+            const __grid_constant__ Kernel17 k) {
+  const int plane = blockIdx.y;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  const float* base = in + plane * pitch;
+  const float center = HorizontalSeparable5(base + static_cast<size_t>(y) * w, x, w, k);
+  const float top1 = HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y - 1, h)) * w, x, w, k);
+  const float bottom1 =
+    HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y + 1, h)) * w, x, w, k);
+  const float top2 = HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y - 2, h)) * w, x, w, k);
+  const float bottom2 =
+    HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y + 2, h)) * w, x, w, k);
+  float r = center * k.w5[0];
+  r = (top1 + bottom1) * k.w5[1] + r;
+  r = (top2 + bottom2) * k.w5[2] + r;
+  out[plane * pitch + i] = r;
+}
+
+// One tap row of ConvolutionWithTranspose at position x of a line of length n
+// (samples at src[j * step]). Interior: pair sums folded round-robin into four
+// partial sums (ConvolveInterior7/13/15/33); border: renormalized direct sum
+// (ConvolveBorderColumn).
+template <int R>
+__device__ __forceinline__ float ConvolveLine(const float* src, int step, int x, int n,
+                                              const Kernel17& k) {
+  if (x >= R && x < n - R) {
+    const float* s = src + static_cast<ptrdiff_t>(x - R) * step;
+    float sums[4];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const float term = (s[i * step] + s[(2 * R - i) * step]) * k.scaled[i];
+      if (i < 4) {
+        sums[i] = term;
+      } else {
+        sums[i & 3] += term;
+      }
+    }
+    float out = s[R * step] * k.scaled[R];
+#pragma unroll
+    for (int i = 0; i < (R < 4 ? R : 4); ++i) out = out + sums[i];
+    return out;
+  }
+  const int first = x < R ? 0 : x - R;
+  const int last = min(n - 1, x + R);
+  float weight = 0.0f;
+  for (int j = first; j <= last; ++j) weight += k.raw[j + R - x];
+  const float scale = 1.0f / weight;
+  float sum = 0.0f;
+  for (int j = first; j <= last; ++j) sum += src[static_cast<ptrdiff_t>(j) * step] * k.raw[j + R - x];
+  return sum * scale;
+}
+
+template <int R>
+__global__ void __launch_bounds__(kThreads)
+BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
+               const __grid_constant__ Kernel17 k) {
+  const int plane = blockIdx.y;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  const float* row = in + plane * in_pitch + static_cast<size_t>(y) * w;
+  out[plane * out_pitch + i] = ConvolveLine<R>(row, 1, x, w, k);
+}
+
+template <int R>
+__global__ void __launch_bounds__(kThreads)
+BlurColumnsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
+                  const __grid_constant__ Kernel17 k) {
+  const int plane = blockIdx.y;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  const float* column = in + plane * in_pitch + x;
+  out[plane * out_pitch + i] = ConvolveLine<R>(column, w, y, h, k);
+}
+
+// --------------------------------------------------------------------------
+// Opsin dynamics and frequency separation.
+
+__device__ __forceinline__ float ButteraugliFastLog2(float value) {
+  const uint32_t bits = __float_as_uint(value);
+  const int32_t e = static_cast<int32_t>(bits - 0x3f2aaaabu) >> 23;
+  const float x = __uint_as_float(bits - (static_cast<uint32_t>(e) << 23)) - 1.0f;
+  float num = 0.74245873327820566f * x + 1.4287160470083755f;
+  num = num * x + -1.8503833400518310e-06f;
+  float den = 0.17409343003366853f * x + 1.0096718572241148f;
+  den = den * x + 0.99032814277590719f;
+  return num / den + static_cast<float>(e);
+}
+
+__device__ __forceinline__ float GammaB(float value) {
+  constexpr float kRetMul = 19.245013259874995f * 0.6931471805599453f;
+  value = fmaxf(value, 0.0f);
+  return kRetMul * ButteraugliFastLog2(value + 9.9710635769299145f) + -23.16046239805755f;
+}
+
+template <bool Clamp>
+__device__ __forceinline__ void OpsinAbsorbance(float r, float g, float b, float& o0, float& o1,
+                                                float& o2) {
+  constexpr float k0 = 0.29956550340058319f, k1 = 0.63373087833825936f,
+                  k2 = 0.077705617820981968f, k3 = 1.7557483643287353f,
+                  k4 = 0.22158691104574774f, k5 = 0.69391388044116142f, k6 = 0.0987313588422f,
+                  k7 = 1.7557483643287353f, k8 = 0.02f, k9 = 0.02f,
+                  k10 = 0.20480129041026129f, k11 = 12.226454707163354f;
+  o0 = k0 * r + (k1 * g + (k2 * b + k3));
+  o1 = k4 * r + (k5 * g + (k6 * b + k7));
+  o2 = k8 * r + (k9 * g + (k10 * b + k11));
+  if (Clamp) {
+    o0 = fmaxf(o0, k3);
+    o1 = fmaxf(o1, k7);
+    o2 = fmaxf(o2, k11);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+OpsinDynamicsKernel(const float* linear, size_t linear_stride, size_t linear_pitch,
+                    const float* blurred, float* xyb, int w, int h, size_t pitch,
+                    float intensity, uint32_t* error) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  float p0, p1, p2;
+  OpsinAbsorbance<true>(blurred[i] * intensity, blurred[pitch + i] * intensity,
+                        blurred[2 * pitch + i] * intensity, p0, p1, p2);
+  p0 = fmaxf(p0, 1.0e-4f);
+  p1 = fmaxf(p1, 1.0e-4f);
+  p2 = fmaxf(p2, 1.0e-4f);
+  const float s0 = fmaxf(GammaB(p0) / p0, 1.0e-4f);
+  const float s1 = fmaxf(GammaB(p1) / p1, 1.0e-4f);
+  const float s2 = fmaxf(GammaB(p2) / p2, 1.0e-4f);
+  const size_t li = static_cast<size_t>(y) * linear_stride + x;
+  float c0, c1, c2;
+  OpsinAbsorbance<false>(linear[li] * intensity, linear[linear_pitch + li] * intensity,
+                         linear[2 * linear_pitch + li] * intensity, c0, c1, c2);
+  c0 = fmaxf(c0 * s0, 1.7557483643287353f);
+  c1 = fmaxf(c1 * s1, 1.7557483643287353f);
+  c2 = fmaxf(c2 * s2, 12.226454707163354f);
+  const float ox = c0 - c1, oy = c0 + c1;
+  if (!IsFinite(ox) || !IsFinite(oy) || !IsFinite(c2)) RaiseError(error, kErrorNonFiniteOutput);
+  xyb[i] = ox;
+  xyb[pitch + i] = oy;
+  xyb[2 * pitch + i] = c2;
+}
+
+// Psycho-image plane indices (OwnedPsychoImage): LF 0-2, MF 3-5, HF 6-7,
+// UHF 8-9.
+enum : int { kLF = 0, kMF = 3, kHF = 6, kUHF = 8, kPsychoPlanes = 10 };
+
+__device__ __forceinline__ float RemoveRangeAroundZero(float v, float w) {
+  return v > w ? v - w : v < -w ? v + w : 0.0f;
+}
+__device__ __forceinline__ float AmplifyRangeAroundZero(float v, float w) {
+  return v > w ? v + w : v < -w ? v - w : v + v;
+}
+__device__ __forceinline__ float MaximumClamp(float v, float m) {
+  constexpr float kMul = 0.724216145665f;
+  if (v >= m) return (v - m) * kMul + m;
+  if (v < -m) return (v + m) * kMul + -m;
+  return v;
+}
+
+// After the 33-tap blur of all three XYB planes into psycho LF: MF = xyb - LF
+// and the LF scaling (butteraugli_internal.cpp:750-776).
+__global__ void __launch_bounds__(kThreads)
+FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  float lf[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    lf[c] = psycho[(kLF + c) * pitch + i];
+    psycho[(kMF + c) * pitch + i] = xyb[c * pitch + i] - lf[c];
+  }
+  psycho[(kLF + 2) * pitch + i] = (-0.362267051518f * lf[1] + lf[2]) * 49.87984651440f;
+  psycho[(kLF + 0) * pitch + i] = lf[0] * 33.832837186260f;
+  psycho[(kLF + 1) * pitch + i] = lf[1] * 14.458268100570f;
+}
+
+// After the 15-tap blur of MF into `blurred` (3 planes): HF = MF - blurred
+// (X, Y), MF ranges, MF_B = blurred, then X suppression by Y
+// (butteraugli_internal.cpp:778-810).
+__global__ void __launch_bounds__(kThreads)
+FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  float hf[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const float mv = blurred[c * pitch + i];
+    hf[c] = psycho[(kMF + c) * pitch + i] - mv;
+    psycho[(kMF + c) * pitch + i] =
+      c == 0 ? RemoveRangeAroundZero(mv, 0.29f) : AmplifyRangeAroundZero(mv, 0.1f);
+  }
+  psycho[(kMF + 2) * pitch + i] = blurred[2 * pitch + i];
+  constexpr float kSuppress = 46.0f, kMinimumScale = 0.653020556257f;
+  const float y = hf[1];
+  const float scaler = kSuppress / (y * y + kSuppress) * (1.0f - kMinimumScale) + kMinimumScale;
+  psycho[(kHF + 0) * pitch + i] = scaler * hf[0];
+  psycho[(kHF + 1) * pitch + i] = hf[1];
+}
+
+// After the 7-tap blur of HF into `blurred` (2 planes): UHF and final HF
+// (butteraugli_internal.cpp:812-849).
+__global__ void __launch_bounds__(kThreads)
+FrequencyUltraKernel(const float* blurred, float* psycho, int n, size_t pitch,
+                     uint32_t* error) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  {
+    const float hv = blurred[i];
+    const float ultra = psycho[(kHF + 0) * pitch + i];
+    psycho[(kUHF + 0) * pitch + i] = RemoveRangeAroundZero(ultra - hv, 0.04f);
+    psycho[(kHF + 0) * pitch + i] = RemoveRangeAroundZero(hv, 1.5f);
+  }
+  {
+    const float hv = MaximumClamp(blurred[pitch + i], 28.4691806922f);
+    const float ultra = psycho[(kHF + 1) * pitch + i];
+    float uv = ultra - hv;
+    uv = MaximumClamp(uv, 5.19175294647f);
+    psycho[(kUHF + 1) * pitch + i] = uv * 2.69313763794f;
+    psycho[(kHF + 1) * pitch + i] = AmplifyRangeAroundZero(hv * 2.155f, 0.132f);
+  }
+  for (int p = 0; p < kPsychoPlanes; ++p) {
+    if (!IsFinite(psycho[p * pitch + i])) RaiseError(error, kErrorNonFiniteOutput);
+  }
+}
+
+// --------------------------------------------------------------------------
+// Difference stages.
+
+struct MaltaParams {
+  const float* image0;
+  const float* image1;
+  float* accumulate;  // block_diff_ac plane (+= stage value)
+  int w, h;
+  float norm2_gt, norm2_lt;  // float casts of pre * norm
+  float norm;                // static_cast<float>(norm)
+  bool low_frequency;
+};
+
+__device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
+__device__ __forceinline__ float Sum5(float a, float b, float c, float d, float e) {
+  return Sum4(a, b, c, d + e);
+}
+__device__ __forceinline__ float Sum7(float a, float b, float c, float d, float e, float f,
+                                      float g) {
+  return Sum4(a, b, c, Sum4(d, e, f, g));
+}
+__device__ __forceinline__ float Sum9(float a, float b, float c, float d, float e, float f,
+                                      float g, float h, float i) {
+  return (Sum4(a, b, c, d) + Sum4(e, f, g, h)) + i;
+}
+
+// Scaled difference of MaltaDiffMap (butteraugli_distance_internal.cpp:544-575).
+__device__ __forceinline__ float MaltaScaled(const MaltaParams& p, int x, int y) {
+  if (x < 0 || y < 0 || x >= p.w || y >= p.h) return 0.0f;
+  const size_t i = static_cast<size_t>(y) * p.w + x;
+  const float v0 = p.image0[i], v1 = p.image1[i];
+  const float absolute = 0.5f * (fabsf(v0) + fabsf(v1));
+  const float difference = v0 - v1;
+  const float scaler = p.norm2_gt / (p.norm + absolute);
+  float scaled = scaler * difference;
+  const float scaler2 = p.norm2_lt / (p.norm + absolute);
+  const double magnitude = fabs(static_cast<double>(v0));
+  const double too_small = 0.55 * magnitude;
+  const double too_big = 1.05 * magnitude;
+  const double s2 = static_cast<double>(scaler2);
+  const double d1 = static_cast<double>(v1);
+  if (v0 < 0.0f) {
+    if (d1 > -too_small) {
+      scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 + too_small));
+    } else if (d1 < -too_big) {
+      scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (-d1 - too_big));
+    }
+  } else if (d1 < too_small) {
+    scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (too_small - d1));
+  } else if (d1 > too_big) {
+    scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 - too_big));
+  }
+  return scaled;
+}
+
+constexpr int kMaltaTile = 16;
+constexpr int kMaltaHalo = 4;
+constexpr int kMaltaSpan = kMaltaTile + 2 * kMaltaHalo;
+
+// Scaled differences of a 16x16 tile (+4 halo, zero outside the image) in
+// shared memory, then the Malta line sums (MaltaUnitLf / MaltaUnitFull,
+// :156-281) per pixel, added onto the accumulator.
+__global__ void __launch_bounds__(kMaltaTile * kMaltaTile)
+MaltaKernel(const __grid_constant__ MaltaParams p) {
+  __shared__ float tile[kMaltaSpan][kMaltaSpan + 1];
+  const int x0 = blockIdx.x * kMaltaTile - kMaltaHalo;
+  const int y0 = blockIdx.y * kMaltaTile - kMaltaHalo;
+  for (int i = threadIdx.x; i < kMaltaSpan * kMaltaSpan; i += blockDim.x) {
+    const int ty = i / kMaltaSpan, tx = i % kMaltaSpan;
+    tile[ty][tx] = MaltaScaled(p, x0 + tx, y0 + ty);
+  }
+  __syncthreads();
+  const int lx = threadIdx.x % kMaltaTile, ly = threadIdx.x / kMaltaTile;
+  const int x = blockIdx.x * kMaltaTile + lx, y = blockIdx.y * kMaltaTile + ly;
+  if (x >= p.w || y >= p.h) return;
+  auto P = [&](int dx, int dy) { return tile[ly + kMaltaHalo + dy][lx + kMaltaHalo + dx]; };
+  float r;
+  if (p.low_frequency) {
+    float s = Sum5(P(-4, 0), P(-2, 0), P(0, 0), P(2, 0), P(4, 0));
+    r = s * s;
+    s = Sum5(P(0, -4), P(0, -2), P(0, 0), P(0, 2), P(0, 4)); r = s * s + r;
+    s = Sum5(P(-3, -3), P(-2, -2), P(0, 0), P(2, 2), P(3, 3)); r = s * s + r;
+    s = Sum5(P(3, -3), P(2, -2), P(0, 0), P(-2, 2), P(-3, 3)); r = s * s + r;
+    s = Sum5(P(1, -4), P(1, -2), P(0, 0), P(-1, 2), P(-1, 4)); r = s * s + r;
+    s = Sum5(P(-1, -4), P(-1, -2), P(0, 0), P(1, 2), P(1, 4)); r = s * s + r;
+    s = Sum5(P(-4, -1), P(-2, -1), P(0, 0), P(2, 1), P(4, 1)); r = s * s + r;
+    s = Sum5(P(-4, 1), P(-2, 1), P(0, 0), P(2, -1), P(4, -1)); r = s * s + r;
+    s = Sum5(P(-2, -3), P(-1, -2), P(0, 0), P(1, 2), P(2, 3)); r = s * s + r;
+    s = Sum5(P(2, -3), P(1, -2), P(0, 0), P(-1, 2), P(-2, 3)); r = s * s + r;
+    s = Sum5(P(-3, -2), P(-2, -1), P(0, 0), P(2, 1), P(3, 2)); r = s * s + r;
+    s = Sum5(P(3, -2), P(2, -1), P(0, 0), P(-2, 1), P(-3, 2)); r = s * s + r;
+    s = Sum5(P(-4, 2), P(-2, 1), P(0, 0), P(2, -1), P(4, -2)); r = s * s + r;
+    s = Sum5(P(-4, -2), P(-2, -1), P(0, 0), P(2, 1), P(4, 2)); r = s * s + r;
+    s = Sum5(P(-2, -4), P(-1, -2), P(0, 0), P(1, 2), P(2, 4)); r = s * s + r;
+    s = Sum5(P(2, -4), P(1, -2), P(0, 0), P(-1, 2), P(-2, 4)); r = s * s + r;
+  } else {
+    float s = Sum9(P(-4, 0), P(-3, 0), P(-2, 0), P(-1, 0), P(0, 0), P(1, 0), P(2, 0), P(3, 0),
+                   P(4, 0));
+    r = s * s;
+    s = Sum9(P(0, -4), P(0, -3), P(0, -2), P(0, -1), P(0, 0), P(0, 1), P(0, 2), P(0, 3), P(0, 4));
+    r = s * s + r;
+    s = Sum7(P(-3, -3), P(-2, -2), P(-1, -1), P(0, 0), P(1, 1), P(2, 2), P(3, 3)); r = s * s + r;
+    s = Sum7(P(3, -3), P(2, -2), P(1, -1), P(0, 0), P(-1, 1), P(-2, 2), P(-3, 3)); r = s * s + r;
+    s = Sum9(P(1, -4), P(1, -3), P(1, -2), P(0, -1), P(0, 0), P(0, 1), P(-1, 2), P(-1, 3),
+             P(-1, 4));
+    r = s * s + r;
+    s = Sum9(P(-1, -4), P(-1, -3), P(-1, -2), P(0, -1), P(0, 0), P(0, 1), P(1, 2), P(1, 3),
+             P(1, 4));
+    r = s * s + r;
+    s = Sum9(P(-4, -1), P(-3, -1), P(-2, -1), P(-1, 0), P(0, 0), P(1, 0), P(2, 1), P(3, 1),
+             P(4, 1));
+    r = s * s + r;
+    s = Sum9(P(-4, 1), P(-3, 1), P(-2, 1), P(-1, 0), P(0, 0), P(1, 0), P(2, -1), P(3, -1),
+             P(4, -1));
+    r = s * s + r;
+    s = Sum7(P(-2, -3), P(-1, -2), P(-1, -1), P(0, 0), P(1, 1), P(1, 2), P(2, 3)); r = s * s + r;
+    s = Sum7(P(2, -3), P(1, -2), P(1, -1), P(0, 0), P(-1, 1), P(-1, 2), P(-2, 3)); r = s * s + r;
+    s = Sum7(P(-3, -2), P(-2, -1), P(-1, -1), P(0, 0), P(1, 1), P(2, 1), P(3, 2)); r = s * s + r;
+    s = Sum7(P(3, -2), P(2, -1), P(1, -1), P(0, 0), P(-1, 1), P(-2, 1), P(-3, 2)); r = s * s + r;
+    s = Sum9(P(-4, 1), P(-3, 1), P(-2, 1), P(-1, 0), P(0, 0), P(1, 0), P(2, -1), P(3, -1),
+             P(4, -1));
+    r = s * s + r;
+    s = Sum9(P(-4, -1), P(-3, -1), P(-2, -1), P(-1, 0), P(0, 0), P(1, 0), P(2, 1), P(3, 1),
+             P(4, 1));
+    r = s * s + r;
+    s = Sum9(P(-1, -4), P(-1, -3), P(-1, -2), P(0, -1), P(0, 0), P(0, 1), P(1, 2), P(1, 3),
+             P(1, 4));
+    r = s * s + r;
+    s = Sum9(P(1, -4), P(1, -3), P(1, -2), P(0, -1), P(0, 0), P(0, 1), P(-1, 2), P(-1, 3),
+             P(-1, 4));
+    r = s * s + r;
+  }
+  const size_t i = static_cast<size_t>(y) * p.w + x;
+  // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
+  p.accumulate[i] = p.accumulate[i] + (0.0f + r);
+}
+
+struct L2Params {
+  const float* ref;   // psycho planes of the reference
+  const float* dist;  // psycho planes of the distorted image
+  size_t pitch;
+  int n;
+  float* ac;  // 3 planes (X and Y already hold the Malta sums; B is 0)
+  float* dc;  // 3 planes
+  float* pre0;  // masking precompute of the reference (may be null)
+  float* pre1;  // masking precompute of the distorted image
+  float asym_gt[2], asym_lt[2];  // kL2Weights[c] * asym, / asym
+  float mf_weight[3], lf_weight[3];
+  float mask_multiplier, mask_bias, mask_sqrt_bias;
+};
+
+__device__ __forceinline__ float MaskActivity(const float* psycho, size_t pitch, int i) {
+  const float xdiff = (psycho[(kUHF + 0) * pitch + i] + psycho[(kHF + 0) * pitch + i]) * 2.5f;
+  const float ydiff = psycho[(kUHF + 1) * pitch + i] * 0.4f + psycho[(kHF + 1) * pitch + i] * 0.4f;
+  return sqrtf(xdiff * xdiff + ydiff * ydiff);
+}
+
+// L2 terms (L2DiffAsymmetric, L2Diff, SetL2Diff) and the masking inputs
+// (CombineChannelsForMasking + DiffPrecompute) in the reference's order.
+__global__ void __launch_bounds__(kThreads) L2MaskKernel(const __grid_constant__ L2Params p) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= p.n) return;
+  for (int c = 0; c < 3; ++c) {
+    float acc = c < 2 ? p.ac[c * p.pitch + i] : 0.0f;
+    if (c < 2) {
+      const float v0 = p.ref[(kHF + c) * p.pitch + i], v1 = p.dist[(kHF + c) * p.pitch + i];
+      const float primary = p.asym_gt[c] * 0.8f;
+      const float secondary_weight = p.asym_lt[c] * 0.8f;
+      const float d = v0 - v1;
+      const float total = (d * d) * primary + acc;
+      const float magnitude = fabsf(v0);
+      const float too_small = 0.4f * magnitude;
+      float secondary = 0.0f;
+      if (v0 < 0.0f) {
+        if (v1 > -too_small) {
+          secondary = v1 + too_small;
+        } else if (v1 < -magnitude) {
+          secondary = -v1 - magnitude;
+        }
+      } else if (v1 < too_small) {
+        secondary = too_small - v1;
+      } else if (v1 > magnitude) {
+        secondary = v1 - magnitude;
+      }
+      acc = secondary_weight * (secondary * secondary) + total;
+    }
+    {
+      const float d = p.ref[(kMF + c) * p.pitch + i] - p.dist[(kMF + c) * p.pitch + i];
+      acc = (d * d) * p.mf_weight[c] + acc;
+    }
+    p.ac[c * p.pitch + i] = acc;
+    const float d = p.ref[(kLF + c) * p.pitch + i] - p.dist[(kLF + c) * p.pitch + i];
+    p.dc[c * p.pitch + i] = d * d * p.lf_weight[c];
+  }
+  const float m1 = MaskActivity(p.dist, p.pitch, i);
+  p.pre1[i] = sqrtf(p.mask_multiplier * fabsf(m1) + p.mask_bias) - p.mask_sqrt_bias;
+  if (p.pre0 != nullptr) {
+    const float m0 = MaskActivity(p.ref, p.pitch, i);
+    p.pre0[i] = sqrtf(p.mask_multiplier * fabsf(m0) + p.mask_bias) - p.mask_sqrt_bias;
+  }
+}
+
+__device__ __forceinline__ void StoreMin3(float v, float& m0, float& m1, float& m2) {
+  if (v < m2) {
+    if (v < m0) {
+      m2 = m1; m1 = m0; m0 = v;
+    } else if (v < m1) {
+      m2 = m1; m1 = v;
+    } else {
+      m2 = v;
+    }
+  }
+}
+
+// FuzzyErosion of the blurred reference mask (:588-628).
+__global__ void __launch_bounds__(kThreads)
+FuzzyErosionKernel(const float* in, float* out, int w, int h) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  constexpr int kStep = 3;
+  auto at = [&](int xx, int yy) { return in[static_cast<size_t>(yy) * w + xx]; };
+  float m0 = at(x, y);
+  float m1 = 2.0f * m0;
+  float m2 = m1;
+  if (x >= kStep) {
+    StoreMin3(at(x - kStep, y), m0, m1, m2);
+    if (y >= kStep) StoreMin3(at(x - kStep, y - kStep), m0, m1, m2);
+    if (y < h - kStep) StoreMin3(at(x - kStep, y + kStep), m0, m1, m2);
+  }
+  if (x < w - kStep) {
+    StoreMin3(at(x + kStep, y), m0, m1, m2);
+    if (y >= kStep) StoreMin3(at(x + kStep, y - kStep), m0, m1, m2);
+    if (y < h - kStep) StoreMin3(at(x + kStep, y + kStep), m0, m1, m2);
+  }
+  if (y >= kStep) StoreMin3(at(x, y - kStep), m0, m1, m2);
+  if (y < h - kStep) StoreMin3(at(x, y + kStep), m0, m1, m2);
+  out[i] = 0.45f * m0 + 0.3f * m1 + 0.25f * m2;
+}
+
+__device__ __forceinline__ float MaskY(float delta) {
+  const double kNorm = 0.79079917404;
+  const double kGlobalScale = 1.0 / (17.83 * kNorm);
+  const double v = kGlobalScale * (1.0 + 2.5485944793 / (0.451936922203 * delta + 0.829591754942));
+  return static_cast<float>(v * v);
+}
+
+__device__ __forceinline__ float MaskDcY(float delta) {
+  const double kNorm = 0.79079917404;
+  const double kGlobalScale = 1.0 / (17.83 * kNorm);
+  const double v = kGlobalScale * (1.0 + 0.505054525019 / (3.87449418804 * delta + 0.20025578522));
+  return static_cast<float>(v * v);
+}
+
+// Masked Y AC term and the final composition (:805-851).
+__global__ void __launch_bounds__(kThreads)
+FinalCompositionKernel(const float* mask, const float* blurred0, const float* blurred1,
+                       const float* ac, const float* dc, size_t pitch, int n, float x_multiplier,
+                       float* final_map, uint32_t* error) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  const float difference = blurred0[i] - blurred1[i];
+  const float ac_y = ac[pitch + i] + 10.0f * difference * difference;
+  const float m = mask[i];
+  const float mask_value = MaskY(m);
+  const float dc_mask_value = MaskDcY(m);
+  const float diff_dc0 = dc[i] * x_multiplier;
+  const float diff_ac0 = ac[i] * x_multiplier;
+  const float masked_dc =
+    diff_dc0 * dc_mask_value + dc[pitch + i] * dc_mask_value + dc[2 * pitch + i] * dc_mask_value;
+  const float masked_ac = diff_ac0 * mask_value + ac_y * mask_value + ac[2 * pitch + i] * mask_value;
+  const float v = sqrtf(masked_dc + masked_ac);
+  if (!IsFinite(v)) RaiseError(error, kErrorNonFiniteOutput);
+  final_map[i] = v;
+}
+
+// Subsample2x (:338-360) of three planes.
+__global__ void __launch_bounds__(kThreads)
+Subsample2xKernel(const float* in, size_t in_stride, size_t in_pitch, int w, int h, float* out,
+                  int sw, int sh, size_t out_pitch) {
+  const int plane = blockIdx.y;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= sw * sh) return;
+  const int x = i % sw, y = i / sw;
+  const float* src = in + plane * in_pitch;
+  float v = 0.0f;
+  for (int dy = 0; dy < 2; ++dy) {
+    const int yy = 2 * y + dy;
+    if (yy >= h) continue;
+    for (int dx = 0; dx < 2; ++dx) {
+      const int xx = 2 * x + dx;
+      if (xx >= w) continue;
+      v += 0.25f * src[static_cast<size_t>(yy) * in_stride + xx];
+    }
+  }
+  if ((w & 1) && x == sw - 1) v *= 2.0f;
+  if ((h & 1) && y == sh - 1) v *= 2.0f;
+  out[plane * out_pitch + i] = v;
+}
+
+// ExpandImage (:322-336) for images narrower or shorter than 8 pixels.
+__global__ void __launch_bounds__(kThreads)
+ExpandKernel(const float* in, size_t in_stride, size_t in_pitch, int w, int h, float* out,
+             int ew, int eh, int xborder, int yborder, size_t out_pitch) {
+  const int plane = blockIdx.y;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= ew * eh) return;
+  const int x = i % ew, y = i / ew;
+  const int sy = min(h - 1, y > yborder ? y - yborder : 0);
+  const int sx = min(w - 1, x > xborder ? x - xborder : 0);
+  out[plane * out_pitch + i] = in[plane * in_pitch + static_cast<size_t>(sy) * in_stride + sx];
+}
+
+// Main/sub combination (:956-963) or the cropped copy of an expanded map,
+// with the NaN-free maximum folded into one float atomicMax per warp.
+__global__ void __launch_bounds__(kThreads)
+CombineKernel(const float* main_map, int main_w, const float* sub_map, int sub_w, int w, int h,
+              int xborder, int yborder, float* out, size_t out_stride, float* maximum,
+              uint32_t* error) {
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  float v = 0.0f;
+  if (i < w * h) {
+    const int x = i % w, y = i / w;
+    const float m = main_map[static_cast<size_t>(y + yborder) * main_w + x + xborder];
+    v = sub_map != nullptr ? m * 0.85f + 0.5f * sub_map[static_cast<size_t>(y / 2) * sub_w + x / 2]
+                           : m;
+    if (!(IsFinite(v) && v >= 0.0f)) RaiseError(error, kErrorNonFiniteOutput);
+    out[static_cast<size_t>(y) * out_stride + x] = v;
+  }
+  v = WarpMax(v);
+  if ((threadIdx.x & 31) == 0) AtomicMaxNonNegative(maximum, v);
+}
+
+__global__ void ScoreKernel(const float* maximum, double* score) {
+  *score = static_cast<double>(*maximum);
+}
+
+// --------------------------------------------------------------------------
+// Host side.
+
+Kernel17 MakeKernel(float sigma) {
+  Kernel17 k;
+  std::memset(&k, 0, sizeof(k));
+  const float scaled_radius = 2.25f * std::abs(sigma);
+  const int radius = std::max(1, static_cast<int>(scaled_radius));
+  const double exponent_scale = -1.0 / (2.0 * sigma * sigma);
+  for (int index = -radius; index <= radius; ++index) {
+    k.raw[index + radius] = static_cast<float>(std::exp(exponent_scale * index * index));
+  }
+  float full = 0.0f;
+  for (int i = 0; i < 2 * radius + 1; ++i) full += k.raw[i];
+  const float scale = 1.0f / full;
+  for (int i = 0; i <= radius && i < 17; ++i) k.scaled[i] = k.raw[i] * scale;
+  if (radius == 2) {
+    k.w5[0] = k.raw[2] * scale;
+    k.w5[1] = k.raw[1] * scale;
+    k.w5[2] = k.raw[0] * scale;
+  }
+  return k;
+}
+
+unsigned Blocks(size_t n) { return static_cast<unsigned>((n + kThreads - 1) / kThreads); }
+
+// Butteraugli sigmas (butteraugli_internal.h).
+constexpr float kOpsinSigma = 1.2f, kLowSigma = 7.15593339443f, kHighSigma = 3.22489901262f,
+                kUltraSigma = 1.56416327805f, kMaskSigma = 2.7f;
+
+struct Scale {
+  int w = 0, h = 0;
+  size_t n = 0;
+  float* ref_psycho = nullptr;   // 10 planes
+  float* dist_psycho = nullptr;  // 10 planes
+  float* ref_mask = nullptr;     // FuzzyErosion(blur13(pre0))
+  float* ref_blurred = nullptr;  // blur13(pre0)
+  float* linear_tmp = nullptr;   // 3 planes: expanded/subsampled input
+  float* blur3 = nullptr;        // 3 planes
+  float* xyb = nullptr;          // 3 planes
+  float* tmp = nullptr;          // 3 planes (row-pass outputs)
+  float* ac = nullptr;           // 3 planes
+  float* dc = nullptr;           // 3 planes
+  float* pre0 = nullptr;
+  float* pre1 = nullptr;
+  float* blurred1 = nullptr;
+  float* final_map = nullptr;
+};
+
+size_t ScaleFloats(size_t n) { return n * (10 + 10 + 1 + 1 + 3 + 3 + 3 + 3 + 3 + 3 + 1 + 1 + 1 + 1); }
+
+void AssignScale(Scale& s, float* base) {
+  float* p = base;
+  auto take = [&](size_t planes) {
+    float* r = p;
+    p += planes * s.n;
+    return r;
+  };
+  s.ref_psycho = take(10);
+  s.dist_psycho = take(10);
+  s.ref_mask = take(1);
+  s.ref_blurred = take(1);
+  s.linear_tmp = take(3);
+  s.blur3 = take(3);
+  s.xyb = take(3);
+  s.tmp = take(3);
+  s.ac = take(3);
+  s.dc = take(3);
+  s.pre0 = take(1);
+  s.pre1 = take(1);
+  s.blurred1 = take(1);
+  s.final_map = take(1);
+}
+
+}  // namespace
+
+struct ButteraugliState {
+  int width = 0, height = 0;
+  float intensity_target = 80.0f;
+  float hf_asymmetry = 1.0f, x_multiplier = 1.0f;
+  bool expanded = false, has_sub = false;
+  int xborder = 0, yborder = 0;
+  Scale main, sub;
+  float* arena = nullptr;
+  float* maximum = nullptr;
+  uint32_t* error = nullptr;
+  bool prepared = false;
+  bool reference_mask_ready = false;  // reference mask planes computed
+  Kernel17 k_opsin, k_low, k_high, k_ultra, k_mask;
+
+  ~ButteraugliState() {
+    if (arena) cudaFree(arena);
+  }
+};
+
+namespace {
+
+template <int R>
+void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pitch, int planes,
+                const Kernel17& k, cudaStream_t stream) {
+  const size_t n = static_cast<size_t>(w) * h;
+  dim3 grid(Blocks(n), planes);
+  BlurRowsKernel<R><<<grid, kThreads, 0, stream>>>(in, tmp, w, h, pitch, pitch, k);
+  BlurColumnsKernel<R><<<grid, kThreads, 0, stream>>>(tmp, out, w, h, pitch, pitch, k);
+}
+
+// Opsin dynamics + frequency separation of one image at one scale
+// (OpsinDynamicsImage + SeparateFrequencies) into `psycho`.
+void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, size_t pitch,
+            float* psycho, cudaStream_t stream) {
+  const size_t n = s.n;
+  // Dense copy of the input planes for the mirrored 5-tap blur.
+  const float* dense = linear;
+  if (stride != static_cast<size_t>(s.w) || pitch != n) {
+    cudaMemcpy2DAsync(s.linear_tmp, s.w * sizeof(float), linear, stride * sizeof(float),
+                      s.w * sizeof(float), s.h, cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpy2DAsync(s.linear_tmp + n, s.w * sizeof(float), linear + pitch,
+                      stride * sizeof(float), s.w * sizeof(float), s.h,
+                      cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpy2DAsync(s.linear_tmp + 2 * n, s.w * sizeof(float), linear + 2 * pitch,
+                      stride * sizeof(float), s.w * sizeof(float), s.h,
+                      cudaMemcpyDeviceToDevice, stream);
+    dense = s.linear_tmp;
+  }
+  Blur5Kernel<<<dim3(Blocks(n), 3), kThreads, 0, stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
+  OpsinDynamicsKernel<<<Blocks(n), kThreads, 0, stream>>>(dense, s.w, n, s.blur3, s.xyb, s.w, s.h,
+                                                          n, st.intensity_target, st.error);
+  // LF: 33-tap blur of the three XYB planes straight into the LF planes.
+  BlurPlanes<16>(s.xyb, s.tmp, psycho + kLF * n, s.w, s.h, n, 3, st.k_low, stream);
+  FrequencyLowKernel<<<Blocks(n), kThreads, 0, stream>>>(s.xyb, psycho, static_cast<int>(n), n);
+  // 15-tap blur of MF (3 planes) into blur3.
+  BlurPlanes<7>(psycho + kMF * n, s.tmp, s.blur3, s.w, s.h, n, 3, st.k_high, stream);
+  FrequencyHighKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n), n);
+  // 7-tap blur of HF (2 planes) into blur3.
+  BlurPlanes<3>(psycho + kHF * n, s.tmp, s.blur3, s.w, s.h, n, 2, st.k_ultra, stream);
+  FrequencyUltraKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n),
+                                                           n, st.error);
+}
+
+// Difference stages of one scale into s.final_map; with `reference_side`
+// the reference's mask planes are computed (prepare), otherwise reused.
+void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream_t stream) {
+  const size_t n = s.n;
+  const float asym = st.hf_asymmetry;
+  const float sqrt_asym = std::sqrt(asym);
+  // kMaltaWeights / kMaltaNorms (butteraugli_distance_internal.cpp:24-31).
+  const double kMaltaWeights[6] = {37.0819870399, 8246.75321353, 18.7237414387,
+                                   6923.99476109, 1.10039032555, 173.5};
+  const double kMaltaNorms[6] = {130262059.556, 1009002.70582, 4498534.45232,
+                                 8051.15833247, 71.7800275169, 5.0};
+  const double up[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] * sqrt_asym,
+                        kMaltaWeights[3] * sqrt_asym, kMaltaWeights[4] * asym,
+                        kMaltaWeights[5] * asym};
+  const double down[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] / sqrt_asym,
+                          kMaltaWeights[3] / sqrt_asym, kMaltaWeights[4] / asym,
+                          kMaltaWeights[5] / asym};
+  // Stage inputs: MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X.
+  const int plane_of[6] = {kMF + 1, kMF + 0, kHF + 1, kHF + 0, kUHF + 1, kUHF + 0};
+  cudaMemsetAsync(s.ac, 0, 3 * n * sizeof(float), stream);
+  const int order[6] = {4, 5, 2, 3, 0, 1};
+  dim3 tiles((s.w + kMaltaTile - 1) / kMaltaTile, (s.h + kMaltaTile - 1) / kMaltaTile);
+  for (int index : order) {
+    MaltaParams mp;
+    mp.image0 = s.ref_psycho + plane_of[index] * n;
+    mp.image1 = s.dist_psycho + plane_of[index] * n;
+    const int channel = index % 2 == 0 ? 1 : 0;
+    mp.accumulate = s.ac + channel * n;
+    mp.w = s.w;
+    mp.h = s.h;
+    const bool lf = index < 4;
+    const double multiplier = lf ? 0.611612573796 : 0.39905817637;
+    const double kLength = 3.75;
+    const double pre_gt = multiplier * std::sqrt(0.5f * up[index]) / (kLength * 2.0 + 1.0);
+    const double pre_lt = multiplier * std::sqrt(0.33f * down[index]) / (kLength * 2.0 + 1.0);
+    mp.norm2_gt = static_cast<float>(pre_gt * kMaltaNorms[index]);
+    mp.norm2_lt = static_cast<float>(pre_lt * kMaltaNorms[index]);
+    mp.norm = static_cast<float>(kMaltaNorms[index]);
+    mp.low_frequency = lf;
+    MaltaKernel<<<tiles, kMaltaTile * kMaltaTile, 0, stream>>>(mp);
+  }
+  // kL2Weights (:32-36).
+  const float kL2[9] = {400.0f, 1.50815703118f, 0.0f, 2150.0f, 10.6195433239f, 16.2176043152f,
+                        29.2353797994f, 0.844626970982f, 0.703646627719f};
+  L2Params lp;
+  lp.ref = s.ref_psycho;
+  lp.dist = s.dist_psycho;
+  lp.pitch = n;
+  lp.n = static_cast<int>(n);
+  lp.ac = s.ac;
+  lp.dc = s.dc;
+  lp.pre0 = reference_side ? s.pre0 : nullptr;
+  lp.pre1 = s.pre1;
+  for (int c = 0; c < 2; ++c) {
+    lp.asym_gt[c] = kL2[c] * asym;
+    lp.asym_lt[c] = kL2[c] / asym;
+  }
+  for (int c = 0; c < 3; ++c) {
+    lp.mf_weight[c] = kL2[3 + c];
+    lp.lf_weight[c] = kL2[6 + c];
+  }
+  lp.mask_multiplier = 6.19424080439f;
+  lp.mask_bias = 6.19424080439f * 12.61050594197f;
+  lp.mask_sqrt_bias = std::sqrt(lp.mask_bias);
+  L2MaskKernel<<<Blocks(n), kThreads, 0, stream>>>(lp);
+  if (reference_side) {
+    BlurPlanes<6>(s.pre0, s.tmp, s.ref_blurred, s.w, s.h, n, 1, st.k_mask, stream);
+    FuzzyErosionKernel<<<Blocks(n), kThreads, 0, stream>>>(s.ref_blurred, s.ref_mask, s.w, s.h);
+  }
+  BlurPlanes<6>(s.pre1, s.tmp, s.blurred1, s.w, s.h, n, 1, st.k_mask, stream);
+  FinalCompositionKernel<<<Blocks(n), kThreads, 0, stream>>>(
+    s.ref_mask, s.ref_blurred, s.blurred1, s.ac, s.dc, n, static_cast<int>(n), st.x_multiplier,
+    s.final_map, st.error);
+}
+
+void TransformScales(ButteraugliState& st, const float* linear, size_t stride, size_t pitch,
+                     bool reference, cudaStream_t stream) {
+  const float* main_in = linear;
+  size_t main_stride = stride, main_pitch = pitch;
+  if (st.expanded) {
+    ExpandKernel<<<dim3(Blocks(st.main.n), 3), kThreads, 0, stream>>>(
+      linear, stride, pitch, st.width, st.height, st.main.linear_tmp, st.main.w, st.main.h,
+      st.xborder, st.yborder, st.main.n);
+    main_in = st.main.linear_tmp;
+    main_stride = st.main.w;
+    main_pitch = st.main.n;
+  }
+  Psycho(st, st.main, main_in, main_stride, main_pitch,
+         reference ? st.main.ref_psycho : st.main.dist_psycho, stream);
+  if (st.has_sub) {
+    Subsample2xKernel<<<dim3(Blocks(st.sub.n), 3), kThreads, 0, stream>>>(
+      linear, stride, pitch, st.width, st.height, st.sub.linear_tmp, st.sub.w, st.sub.h,
+      st.sub.n);
+    Psycho(st, st.sub, st.sub.linear_tmp, st.sub.w, st.sub.n,
+           reference ? st.sub.ref_psycho : st.sub.dist_psycho, stream);
+  }
+}
+
+}  // namespace
+
+int ButteraugliCreate(size_t width, size_t height, float intensity_target, ButteraugliState** out) {
+  auto* st = new (std::nothrow) ButteraugliState();
+  if (st == nullptr) return SetError(GJXL_B200_OUT_OF_MEMORY, "butteraugli: host allocation");
+  st->width = static_cast<int>(width);
+  st->height = static_cast<int>(height);
+  st->intensity_target = intensity_target;
+  st->expanded = width < 8 || height < 8;
+  st->main.w = static_cast<int>(std::max<size_t>(8, width));
+  st->main.h = static_cast<int>(std::max<size_t>(8, height));
+  if (st->expanded) {
+    st->xborder = width < 8 ? static_cast<int>((8 - width) / 2) : 0;
+    st->yborder = height < 8 ? static_cast<int>((8 - height) / 2) : 0;
+  }
+  st->main.n = static_cast<size_t>(st->main.w) * st->main.h;
+  st->has_sub = !st->expanded && width >= 15 && height >= 15;
+  if (st->has_sub) {
+    st->sub.w = static_cast<int>((width + 1) / 2);
+    st->sub.h = static_cast<int>((height + 1) / 2);
+    st->sub.n = static_cast<size_t>(st->sub.w) * st->sub.h;
+  }
+  const size_t floats = ScaleFloats(st->main.n) + ScaleFloats(st->sub.n) + 64;
+  int status = CheckCuda(cudaMalloc(&st->arena, floats * sizeof(float)), "butteraugli: cudaMalloc");
+  if (status != GJXL_B200_OK) {
+    delete st;
+    return status;
+  }
+  AssignScale(st->main, st->arena);
+  if (st->has_sub) AssignScale(st->sub, st->arena + ScaleFloats(st->main.n));
+  st->maximum = st->arena + ScaleFloats(st->main.n) + ScaleFloats(st->sub.n);
+  st->error = reinterpret_cast<uint32_t*>(st->maximum + 32);
+  st->k_opsin = MakeKernel(kOpsinSigma);
+  st->k_low = MakeKernel(kLowSigma);
+  st->k_high = MakeKernel(kHighSigma);
+  st->k_ultra = MakeKernel(kUltraSigma);
+  st->k_mask = MakeKernel(kMaskSigma);
+  *out = st;
+  return GJXL_B200_OK;
+}
+
+int ButteraugliPrepare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
+                       cudaStream_t stream) {
+  cudaMemsetAsync(st->error, 0, sizeof(uint32_t), stream);
+  TransformScales(*st, linear, stride, pitch, true, stream);
+  st->prepared = true;
+  st->reference_mask_ready = false;
+  return CheckLaunch("butteraugli prepare");
+}
+
+int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
+                       float* map, size_t map_stride, double* score, cudaStream_t stream) {
+  if (!st->prepared) {
+    return SetError(GJXL_B200_FAILED_PRECONDITION, "butteraugli: reference not prepared");
+  }
+  TransformScales(*st, linear, stride, pitch, false, stream);
+  // The reference's mask planes depend only on the reference image; the
+  // first comparison after a prepare computes them, later ones reuse them.
+  const bool reference_side = !st->reference_mask_ready;
+  Differences(*st, st->main, reference_side, stream);
+  if (st->has_sub) Differences(*st, st->sub, reference_side, stream);
+  st->reference_mask_ready = true;
+  cudaMemsetAsync(st->maximum, 0, sizeof(float), stream);
+  const size_t n = static_cast<size_t>(st->width) * st->height;
+  CombineKernel<<<Blocks(n), kThreads, 0, stream>>>(
+    st->main.final_map, st->main.w, st->has_sub ? st->sub.final_map : nullptr, st->sub.w,
+    st->width, st->height, st->xborder, st->yborder, map, map_stride, st->maximum, st->error);
+  if (score != nullptr) ScoreKernel<<<1, 1, 0, stream>>>(st->maximum, score);
+  return CheckLaunch("butteraugli compare");
+}
+
+uint32_t* ButteraugliErrorWord(ButteraugliState* st) { return st->error; }
+float* ButteraugliMaximum(ButteraugliState* st) { return st->maximum; }
+
+}  // namespace gjxl_b200
+
+using namespace gjxl_b200;
+
+struct gjxl_b200_butteraugli : public ButteraugliState {};
+
+extern "C" int gjxl_b200_butteraugli_create(size_t width, size_t height, float intensity_target,
+                                            gjxl_b200_butteraugli** out) {
+  ClearLastError();
+  if (out == nullptr || width == 0 || height == 0 || width > (1u << 20) || height > (1u << 20) ||
+      !std::isfinite(intensity_target) || intensity_target <= 0.0f) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "butteraugli_create: invalid arguments");
+  }
+  ButteraugliState* st = nullptr;
+  const int status = ButteraugliCreate(width, height, intensity_target, &st);
+  if (status != GJXL_B200_OK) return status;
+  // The public handle type derives from the state without adding members.
+  static_assert(sizeof(gjxl_b200_butteraugli) == sizeof(ButteraugliState), "");
+  *out = static_cast<gjxl_b200_butteraugli*>(st);
+  return GJXL_B200_OK;
+}
+
+extern "C" void gjxl_b200_butteraugli_destroy(gjxl_b200_butteraugli* b) {
+  delete static_cast<ButteraugliState*>(b);
+}
+
+extern "C" int gjxl_b200_butteraugli_prepare(gjxl_b200_butteraugli* b, const float* reference,
+                                             size_t stride, size_t plane_pitch, void* stream) {
+  ClearLastError();
+  if (b == nullptr || reference == nullptr || stride < static_cast<size_t>(b->width) ||
+      plane_pitch < stride * b->height) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "butteraugli_prepare: invalid arguments");
+  }
+  return ButteraugliPrepare(b, reference, stride, plane_pitch, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gjxl_b200_butteraugli_compare(gjxl_b200_butteraugli* b, const float* distorted,
+                                             size_t stride, size_t plane_pitch,
+                                             float* distance_map, size_t map_stride,
+                                             double* score, uint32_t* device_error, void* stream) {
+  ClearLastError();
+  if (b == nullptr || distorted == nullptr || distance_map == nullptr ||
+      stride < static_cast<size_t>(b->width) || plane_pitch < stride * b->height ||
+      map_stride < static_cast<size_t>(b->width)) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "butteraugli_compare: invalid arguments");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int status = ButteraugliCompare(b, distorted, stride, plane_pitch, distance_map,
+                                        map_stride, score, s);
+  if (status == GJXL_B200_OK && device_error != nullptr) {
+    cudaMemcpyAsync(device_error, b->error, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+  }
+  return status == GJXL_B200_OK ? CheckLaunch("butteraugli compare") : status;
+}

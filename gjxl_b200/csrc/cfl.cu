@@ -11,8 +11,8 @@
 //
 // One CTA of 256 threads per tile. Phase 1: each warp transforms (block,
 // channel) pairs — lane l owns row-pass outputs l and l+32 and gathers the
-// column inputs with double shuffles. Phase 2: warp 0 solves y_to_x and warp 1
-// solves y_to_b; lanes 0..11 each own one of the 3 derivative sums x 4 lanes.
+// column inputs with double shuffles. Phase 2: warp 0 solves both maps, twelve
+// lanes per map, each lane owning one of the 3 derivative sums x 4 lanes.
 
 #include <cmath>
 #include <cstring>
@@ -56,7 +56,9 @@ __device__ __forceinline__ int8_t QuantizeMultiplier(float x) {
 }
 
 __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ CflParams p) {
-  extern __shared__ __align__(16) float values[];  // [4][kTileValues]: lx, cx, lb, cb
+  // [4][kTileValues]: per element a = luma / 84 and b = base * luma - chroma
+  // for the y_to_x problem (base 0) and the y_to_b problem (base 1).
+  extern __shared__ __align__(16) float values[];
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
   const int bx0 = tx * 8, by0 = ty * 8;
@@ -74,9 +76,7 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   for (int b = warp; b < blocks; b += 8) {
     const int bx = bx0 + b % tw, by = by0 + b / tw;
     for (int c = 1; c < 4; ++c) {
-      const int channel = c == 3 ? 0 : c;  // order: Y, B, X
-      const int ch = c == 1 ? 1 : c == 2 ? 2 : 0;
-      (void)channel;
+      const int ch = c == 1 ? 1 : c == 2 ? 2 : 0;  // order: Y, B, X
       const float* src = p.opsin + ch * p.pitch + static_cast<size_t>(by * 8) * p.stride + bx * 8;
       // Row pass: T[y][u] = sum_x pixel[y][x] * basis[u][x], outputs l, l+32.
       double t[2];
@@ -105,7 +105,6 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
           sum += __ldg(p.fwd + v * 8 + y) * value;
         }
         coef[k] = static_cast<float>(sum);
-        (void)u;
       }
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
@@ -117,13 +116,15 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
           y_coef[warp][index] = value;
         } else if (ch == 2) {
           __syncwarp();
-          const float yv = y_coef[warp][index];
-          luma_b[at] = yv * __ldg(p.inv_b + index) * 1.0f;
-          chroma_b[at] = value * __ldg(p.inv_b + index) * 1.0f;
+          const float luma = y_coef[warp][index] * __ldg(p.inv_b + index) * 1.0f;
+          const float chroma = value * __ldg(p.inv_b + index) * 1.0f;
+          luma_b[at] = luma / 84.0f;
+          chroma_b[at] = 1.0f * luma - chroma;
         } else {
-          const float yv = y_coef[warp][index];
-          luma_x[at] = yv * __ldg(p.inv_x + index) * 1.0f;
-          chroma_x[at] = value * __ldg(p.inv_x + index) * 1.0f;
+          const float luma = y_coef[warp][index] * __ldg(p.inv_x + index) * 1.0f;
+          const float chroma = value * __ldg(p.inv_x + index) * 1.0f;
+          luma_x[at] = luma / 84.0f;
+          chroma_x[at] = 0.0f * luma - chroma;
         }
       }
       __syncwarp();
@@ -131,53 +132,61 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   }
   __syncthreads();
 
-  // Phase 2: FindBestMultiplier (non-fast), warp 0 -> y_to_x, warp 1 -> y_to_b.
-  if (warp >= 2) return;
-  const float* luma = warp == 0 ? luma_x : luma_b;
-  const float* chroma = warp == 0 ? chroma_x : chroma_b;
-  const float base = warp == 0 ? 0.0f : 1.0f;
+  // Phase 2: FindBestMultiplier (non-fast) for both maps in warp 0: lanes
+  // 0..11 solve y_to_x, lanes 12..23 solve y_to_b; within a group, lane
+  // 4 * kind + slot owns derivative sum `kind` (center, +eps, -eps) over the
+  // elements i = slot (mod 4), in increasing i like the reference.
+  if (warp != 0) return;
+  const int group = lane / 12;  // 0: y_to_x, 1: y_to_b, 2: idle lanes
+  const int member = lane % 12;
+  const int kind = member / 4, slot = member % 4;
+  const float* A = group == 0 ? luma_x : luma_b;    // a = luma / 84
+  const float* Bv = group == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
   const int count = blocks * 64;
   const float kDistanceMultiplierAc = 1.0e-9f;
   const float kEpsilon = 100.0f;
-  const int kind = lane / 4, slot = lane % 4;  // kind 0 center, 1 +eps, 2 -eps
   float x = 0.0f;
+  bool done = group == 2;
   for (int iteration = 0; iteration < p.iterations; ++iteration) {
+    if (__all_sync(0xffffffffu, done)) break;
     float lane_sum = 0.0f;
-    if (lane < 12) {
+    if (!done) {
       const float offset = kind == 0 ? x : kind == 1 ? x + kEpsilon : x - kEpsilon;
+#pragma unroll 4
       for (int i = slot; i < count; i += 4) {
-        const float a = luma[i] / 84.0f;
-        const float b = base * luma[i] - chroma[i];
+        const float a = A[i], b = Bv[i];
         const float center = fmaf(a, x, b);
-        if (fabsf(center) >= 100.0f) continue;
         const float r = kind == 0 ? center : fmaf(a, offset, b);
         float d = (2.0f / 3.0f) * a * (fabsf(r) + 1.0f);
-        if (r < 0.0f) d = -d;
-        lane_sum += d;
+        d = r < 0.0f ? -d : d;
+        // Skipped elements add +0.0, which leaves the (never -0.0) sum unchanged.
+        lane_sum += fabsf(center) >= 100.0f ? 0.0f : d;
       }
     }
-    // Horizontal sums (l0 + l1) + (l2 + l3) per kind.
+    // Horizontal sums (l0 + l1) + (l2 + l3) for each kind of this group.
+    const int group_base = 12 * (group < 2 ? group : 0);
     float sums[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const float l0 = __shfl_sync(0xffffffffu, lane_sum, 4 * k + 0);
-      const float l1 = __shfl_sync(0xffffffffu, lane_sum, 4 * k + 1);
-      const float l2 = __shfl_sync(0xffffffffu, lane_sum, 4 * k + 2);
-      const float l3 = __shfl_sync(0xffffffffu, lane_sum, 4 * k + 3);
+      const float l0 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 0);
+      const float l1 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 1);
+      const float l2 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 2);
+      const float l3 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 3);
       sums[k] = (l0 + l1) + (l2 + l3);
     }
-    const float n = static_cast<float>(count);
-    const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
-    const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
-    const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
-    const float second = (plus - minus) / (2.0f * kEpsilon);
-    const float step = center / (second + 0.85f);
-    x -= fminf(fmaxf(step, -20.0f), 20.0f);
-    if (fabsf(step) < 3.0e-3f) break;
+    if (!done) {
+      const float n = static_cast<float>(count);
+      const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
+      const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
+      const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
+      const float second = (plus - minus) / (2.0f * kEpsilon);
+      const float step = center / (second + 0.85f);
+      x -= fminf(fmaxf(step, -20.0f), 20.0f);
+      if (fabsf(step) < 3.0e-3f) done = true;
+    }
   }
-  if (lane == 0) {
-    (warp == 0 ? p.y_to_x : p.y_to_b)[tile] = blocks == 0 ? 0 : QuantizeMultiplier(x);
-  }
+  if (lane == 0) p.y_to_x[tile] = QuantizeMultiplier(x);
+  if (lane == 12) p.y_to_b[tile] = QuantizeMultiplier(x);
 }
 
 }  // namespace

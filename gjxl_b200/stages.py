@@ -103,3 +103,41 @@ def initial_cfl(opsin: torch.Tensor, y_to_x: torch.Tensor, y_to_b: torch.Tensor)
     _lib.call("gjxl_b200_initial_cfl", opsin.data_ptr(), opsin.shape[2],
               opsin.shape[1] * opsin.shape[2], opsin.shape[2], opsin.shape[1],
               y_to_x.data_ptr(), y_to_b.data_ptr(), _stream())
+
+
+class Butteraugli:
+    """Prepared-reference Butteraugli on the device (gjxl_b200_butteraugli_*)."""
+
+    def __init__(self, width: int, height: int, intensity_target: float = 80.0):
+        import ctypes
+        lib = _lib.load()
+        lib.gjxl_b200_butteraugli_destroy.argtypes = [ctypes.c_void_p]
+        lib.gjxl_b200_butteraugli_destroy.restype = None
+        handle = ctypes.c_void_p()
+        _lib.call("gjxl_b200_butteraugli_create", width, height, intensity_target,
+                  ctypes.addressof(handle))
+        self.handle = handle.value
+        self.width, self.height = width, height
+
+    def prepare(self, reference: torch.Tensor):
+        _lib.call("gjxl_b200_butteraugli_prepare", self.handle, reference.data_ptr(),
+                  reference.shape[2], reference.shape[1] * reference.shape[2], _stream())
+
+    def compare(self, distorted: torch.Tensor, distance_map: torch.Tensor,
+                score: torch.Tensor | None = None, device_error: torch.Tensor | None = None):
+        _lib.call("gjxl_b200_butteraugli_compare", self.handle, distorted.data_ptr(),
+                  distorted.shape[2], distorted.shape[1] * distorted.shape[2],
+                  distance_map.data_ptr(), distance_map.shape[-1],
+                  None if score is None else score.data_ptr(),
+                  None if device_error is None else device_error.data_ptr(), _stream())
+
+    def close(self):
+        if self.handle:
+            _lib.load().gjxl_b200_butteraugli_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

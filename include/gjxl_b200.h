@@ -191,6 +191,35 @@ GJXL_B200_API int gjxl_b200_ac_strategy_search(
     const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
     float* costs, uint8_t* cells, uint32_t* device_error, void* stream);
 
+/*
+ * Butteraugli with a prepared reference image (rows a14, a15).
+ * Replaces DeviceButteraugliOperation / PreparedDeviceButteraugli
+ * (src/gpu/ops/butteraugli.h:53-150) as implemented by
+ * LaunchCudaButteraugliPrepare / LaunchButteraugliCompareImpl
+ * (src/gpu/cuda/cuda_butteraugli_kernels.cu:3927,3972), and the CPU
+ * PreparedButteraugliReference::Prepare/Compare (src/codec/butteraugli.cpp:31,60).
+ *
+ * create() allocates all working planes for one extent (both scales);
+ * prepare() transforms the reference once; compare() writes the distance map
+ * (width x height, row stride map_stride) and, if `score` is non-null, the
+ * maximum as a device double. Linear RGB inputs are 3 planes with the given
+ * row stride and plane pitch. A handle serves one stream at a time.
+ */
+typedef struct gjxl_b200_butteraugli gjxl_b200_butteraugli;
+GJXL_B200_API int gjxl_b200_butteraugli_create(size_t width, size_t height,
+                                               float intensity_target,
+                                               gjxl_b200_butteraugli** out);
+GJXL_B200_API void gjxl_b200_butteraugli_destroy(gjxl_b200_butteraugli* b);
+GJXL_B200_API int gjxl_b200_butteraugli_prepare(gjxl_b200_butteraugli* b,
+                                                const float* reference,
+                                                size_t stride,
+                                                size_t plane_pitch,
+                                                void* stream);
+GJXL_B200_API int gjxl_b200_butteraugli_compare(
+    gjxl_b200_butteraugli* b, const float* distorted, size_t stride,
+    size_t plane_pitch, float* distance_map, size_t map_stride,
+    double* score, uint32_t* device_error, void* stream);
+
 /* ------------------------------------------------------------------------
  * Analysis session: the whole analysis path for one image extent.
  *

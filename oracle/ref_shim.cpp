@@ -322,3 +322,60 @@ GJXL_REF_API int gjxl_ref_ac_strategy_cost_table(
   }
   return 0;
 }
+
+// Butteraugli golden vectors of the reference's own test suite
+// (tests/butteraugli_goldens_generated.h, generated there from libjxl
+// e8ff0976 scalar Butteraugli) and the fixture pairs they were computed on
+// (tests/butteraugli_fixtures.cpp MakeFixture).
+#include "butteraugli_fixtures.h"
+#include "butteraugli_goldens_generated.h"
+
+GJXL_REF_API int gjxl_ref_butteraugli_fixture(int kind, size_t width, size_t height,
+                                              uint32_t seed, size_t impulse_channel,
+                                              float* reference, float* distorted,
+                                              float* options3) {
+  namespace bt = gjxl::butteraugli_test;
+  bt::FixtureSpec spec;
+  spec.name = "fixture";
+  spec.extent = {width, height};
+  spec.kind = static_cast<bt::FixtureKind>(kind);
+  spec.impulse_channel = impulse_channel;
+  spec.random_seed = seed;
+  spec.options = {options3[0], options3[1], options3[2]};
+  const bt::FixturePair pair = bt::MakeFixture(spec);
+  for (size_t c = 0; c < 3; ++c) {
+    for (size_t y = 0; y < height; ++y) {
+      for (size_t x = 0; x < width; ++x) {
+        reference[(c * height + y) * width + x] =
+          pair.reference.planes()[c][y * pair.reference.stride() + x];
+        distorted[(c * height + y) * width + x] =
+          pair.distorted.planes()[c][y * pair.distorted.stride() + x];
+      }
+    }
+  }
+  return 0;
+}
+
+GJXL_REF_API int gjxl_ref_butteraugli_golden_full_map(size_t index, uint32_t* map_bits,
+                                                      uint64_t* score_bits) {
+  namespace golden = gjxl::butteraugli_test::golden;
+  if (index >= golden::kFullMapCount) return -1;
+  std::memcpy(map_bits, golden::kFullMapBits[index].data(), golden::kFullMapArea * 4);
+  *score_bits = golden::kFullMapScoreBits[index];
+  return static_cast<int>(golden::kFullMapArea);
+}
+
+// Butteraugli with explicit options (hf_asymmetry, x_multiplier, intensity).
+GJXL_REF_API int gjxl_ref_butteraugli_options(const float* reference_linear,
+                                              const float* distorted_linear, size_t width,
+                                              size_t height, const float* options3,
+                                              float* distance_map, double* score) {
+  ButteraugliOptions options;
+  options.hf_asymmetry = options3[0];
+  options.x_multiplier = options3[1];
+  options.intensity_target = options3[2];
+  Status status = ComputeButteraugliDistance(
+    ConstPlanar(reference_linear, width, height), ConstPlanar(distorted_linear, width, height),
+    options, {distance_map, {width, height}, width}, score);
+  return status.ok() ? 0 : Fail(status);
+}
