@@ -1,0 +1,1071 @@
+// Rows a9-a12: adaptive-quantization field adjustment, quantizer selection,
+// final chroma-from-luma, per-transform AC coefficient coding and
+// prediction-aware DC quantization, on the device.
+//
+// Restates, with the reference's exact float/double operation order:
+//   AdjustQuantField            src/codec/adaptive_quantization.cpp:740-830
+//   PrepareButteraugliPolicy    src/codec/adaptive_quantization.cpp:1178-1240
+//   CreateQuantizerFromField    src/codec/quantization.cpp:536-620, :59-100
+//   ComputeFinalColorCorrelationMap (fast)  src/codec/chroma_from_luma.cpp:543-650
+//   ComputeQuantizedCoefficientsImpl        src/codec/reconstruction.cpp:386-760
+//   SelectAdjustedAcQuantization / AdjustQuantForChannel /
+//   QuantizeAcBlockWithThresholds           src/codec/quantization.cpp:185-480, 740-800
+//   ConvertLowFrequenciesToDc               src/codec/dc_conversion.cpp:174-236
+//   QuantizeDcCoefficients (prediction-aware, weighted predictor)
+//                                           src/codec/vardct/dc_quantization.cpp:120-230,
+//                                           src/codec/modular/prediction.h:59-150
+//   ComputeEpfInverseSigma                  src/codec/epf.cpp:207-270
+//
+// Coefficients live in "footprint layout": the N coefficients of a transform
+// anchored at block (bx, by) occupy its own W x H pixel footprint of a padded
+// plane, coefficient i at (bx*8 + i % W, by*8 + i / W).
+
+#include <cmath>
+#include <cstring>
+
+#include "aq.h"
+#include "common.cuh"
+#include "host_util.h"
+#include "tables.h"
+#include "transform.cuh"
+
+namespace gjxl_b200 {
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Anchor lists.
+
+__global__ void AnchorListKernel(const uint8_t* cells, uint32_t blocks_x, uint32_t blocks,
+                                 int2* lists, uint32_t list_stride, uint32_t* counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= blocks) return;
+  const uint8_t cell = cells[i];
+  if (!(cell & 1)) return;
+  const int f = StrategyFamily(cell >> 1);
+  if (f < 0) return;
+  const uint32_t slot = atomicAdd(&counts[f], 1u);
+  lists[f * list_stride + slot] = make_int2(i % blocks_x, i / blocks_x);
+}
+
+// ---------------------------------------------------------------------------
+// Forward coefficients of the selected transforms (footprint layout).
+
+template <int W, int H>
+__global__ void __launch_bounds__(kThreads)
+ForwardCoefficientsKernel(const float* opsin, size_t stride, size_t pitch, const int2* anchors,
+                          const uint32_t* count, const double* bw_t, const double* bh,
+                          float* coef, size_t coef_stride, size_t coef_pitch) {
+  constexpr int N = W * H;
+  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* px = reinterpret_cast<float*>(smem);                // [K*3][N]
+  double* tmp = reinterpret_cast<double*>(px + K * 3 * N);  // [K*3][N]
+  const uint32_t first = blockIdx.x * K;
+  const uint32_t n = *count;
+  if (first >= n) return;
+  const int active = min(K, static_cast<int>(n - first));
+  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    const int2 a = anchors[first + k];
+    px[i] = opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 + yx % W];
+  }
+  __syncthreads();
+  ForwardRows<W, H>(px, tmp, bw_t, active * 3, threadIdx.x, kThreads);
+  __syncthreads();
+  ForwardColumns<W, H>(tmp, px, bh, active * 3, threadIdx.x, kThreads);
+  __syncthreads();
+  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    const int2 a = anchors[first + k];
+    coef[c * coef_pitch + static_cast<size_t>(a.y * 8 + j / W) * coef_stride + a.x * 8 + j % W] =
+      px[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field adjustment, policy bounds, quantizer selection.
+
+struct AnchorView {
+  const uint8_t* cells;
+  int blocks_x, blocks_y;
+};
+
+__device__ __forceinline__ bool AnchorAt(const AnchorView& v, int i, int* cw, int* ch, int* s) {
+  const uint8_t cell = v.cells[i];
+  if (!(cell & 1)) return false;
+  *s = cell >> 1;
+  const int f = StrategyFamily(*s);
+  *cw = FamilyCoveredW(f);
+  *ch = FamilyCoveredH(f);
+  return true;
+}
+
+// AdjustQuantField (adaptive_quantization.cpp:776-812) for every anchor.
+__global__ void AdjustFieldKernel(AnchorView v, const float* in, float* out, float mixer) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.blocks_x * v.blocks_y) return;
+  int cw, ch, s;
+  if (!AnchorAt(v, i, &cw, &ch, &s)) return;
+  const int bx = i % v.blocks_x, by = i / v.blocks_x;
+  float maximum = in[i];
+  float mean = 0.0f;
+  for (int dy = 0; dy < ch; ++dy) {
+    for (int dx = 0; dx < cw; ++dx) {
+      const float value = in[(by + dy) * v.blocks_x + bx + dx];
+      maximum = fmaxf(maximum, value);
+      mean += value;
+    }
+  }
+  const int count = cw * ch;
+  mean /= static_cast<float>(count);
+  float result = maximum;
+  if (count >= 4) result = maximum * mixer + mean * (1.0f - mixer);
+  for (int dy = 0; dy < ch; ++dy)
+    for (int dx = 0; dx < cw; ++dx) out[(by + dy) * v.blocks_x + bx + dx] = result;
+}
+
+__global__ void RangeKernel(const float* field, int n, float* range) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float lo = __int_as_float(0x7f800000), hi = 0.0f;
+  if (i < n) lo = hi = field[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(reinterpret_cast<unsigned int*>(&range[0]), __float_as_uint(lo));
+    atomicMax(reinterpret_cast<unsigned int*>(&range[1]), __float_as_uint(hi));
+  }
+}
+
+// PrepareButteraugliPolicyFromRange (adaptive_quantization.cpp:1205-1240).
+__global__ void PolicySetupKernel(const float* range, float quant_dc, AqPolicy* policy,
+                                  uint32_t* error) {
+  const float lo = range[0], hi = range[1];
+  const float initial_ratio = hi / lo;
+  const float maximum_deviation = sqrtf(250.0f / initial_ratio);
+  const float asymmetry = fminf(2.0f, maximum_deviation);
+  policy->lower_bound = lo / (asymmetry * maximum_deviation);
+  policy->upper_bound = hi * (maximum_deviation / asymmetry);
+  policy->quant_dc = quant_dc;
+  if (!(IsFinite(policy->lower_bound) && IsFinite(policy->upper_bound) &&
+        policy->lower_bound > 0.0f && policy->upper_bound >= policy->lower_bound &&
+        policy->upper_bound / policy->lower_bound < 253.0f)) {
+    RaiseError(error, kErrorRange);
+  }
+}
+
+// k-th smallest of n positive floats (or of |field - center| when use_center)
+// by four 8-bit radix passes over the ordered bit patterns.
+__device__ uint32_t RadixSelect(const float* field, int n, int k, bool use_center, float center,
+                                uint32_t* histogram) {
+  uint32_t prefix = 0, mask = 0;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) histogram[b] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float v = use_center ? fabsf(field[i] - center) : field[i];
+      const uint32_t bits = __float_as_uint(v);
+      if ((bits & mask) == prefix) atomicAdd(&histogram[(bits >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    __shared__ uint32_t chosen_bin, chosen_k;
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0;
+      for (uint32_t b = 0; b < 256; ++b) {
+        if (acc + histogram[b] > static_cast<uint32_t>(k)) {
+          chosen_bin = b;
+          chosen_k = static_cast<uint32_t>(k) - acc;
+          break;
+        }
+        acc += histogram[b];
+      }
+    }
+    __syncthreads();
+    prefix |= chosen_bin << shift;
+    mask |= 255u << shift;
+    k = static_cast<int>(chosen_k);
+    __syncthreads();
+  }
+  return prefix;
+}
+
+// CreateQuantizerFromField + ComputeQuantizerParams + Quantizer::Create.
+__global__ void __launch_bounds__(1024)
+QuantizerKernel(const float* field, int n, const AqPolicy* policy, AqQuantizer* q,
+                uint32_t* error) {
+  __shared__ uint32_t histogram[256];
+  const int k = n / 2;
+  const float median = __uint_as_float(RadixSelect(field, n, k, false, 0.0f, histogram));
+  const float mad = __uint_as_float(RadixSelect(field, n, k, true, median, histogram));
+  if (threadIdx.x != 0) return;
+  const float quant_dc = policy->quant_dc;
+  float scale = 65536.0f * (median - mad) / 5.0f;
+  scale = fminf(fmaxf(scale, 1.0f), 32768.0f);
+  int global_scale = static_cast<int>(scale);
+  const int scaled_quant_dc = static_cast<int>(static_cast<double>(quant_dc * 4096.0f) * 1.6);
+  if (global_scale > scaled_quant_dc) global_scale = max(1, scaled_quant_dc);
+  const float inverse_global_scale = 65536.0f / static_cast<float>(global_scale);
+  const float quant_dc_value = fminf(65536.0f, quant_dc * inverse_global_scale + 0.5f);
+  const uint32_t qdc = static_cast<uint32_t>(quant_dc_value);
+  q->global_scale = static_cast<uint32_t>(global_scale);
+  q->quant_dc = qdc;
+  if (global_scale < 1 || global_scale > 32768 || qdc == 0 || qdc > 65536) {
+    RaiseError(error, kErrorRange);
+  }
+  q->scale = static_cast<float>(global_scale) / 65536.0f;
+  q->inverse_global_scale = 65536.0f / static_cast<float>(global_scale);
+  const float inverse_quant_dc = q->inverse_global_scale / static_cast<float>(qdc);
+  const float kInverseDcQuant[3] = {4096.0f, 512.0f, 256.0f};
+  for (int c = 0; c < 3; ++c) {
+    q->dc_steps[c] = inverse_quant_dc / kInverseDcQuant[c];
+    q->inverse_dc_steps[c] = kInverseDcQuant[c] * q->scale * static_cast<float>(qdc);
+  }
+}
+
+__global__ void RawQuantKernel(const float* field, int n, const AqQuantizer* q, int32_t* raw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = field[i] * q->inverse_global_scale + 0.5f;
+  raw[i] = static_cast<int32_t>(fminf(fmaxf(v, 1.0f), 256.0f));
+}
+
+// ---------------------------------------------------------------------------
+// Final CfL, fast regression (one warp per 64x64 tile; lanes 0-3 solve
+// y_to_x and 4-7 y_to_b, lane i owning elements i (mod 4) in the reference's
+// order: anchors in raster order, coefficients in storage order).
+
+struct CflFinalParams {
+  AnchorView grid;
+  int tiles_x, tiles_y;
+  const float* coef;  // footprint layout, 3 planes
+  size_t coef_stride, coef_pitch;
+  const int32_t* raw;
+  const AqQuantizer* q;
+  const float* inverse_dequant;  // packed tables
+  size_t table_offset[kTableCount];
+  size_t table_count[kTableCount];
+  int8_t* y_to_x;
+  int8_t* y_to_b;
+};
+
+__device__ __forceinline__ int8_t QuantizeMultiplierF(float x) {
+  if (x >= 2.6f) {
+    x -= 2.6f;
+  } else if (x <= -2.6f) {
+    x += 2.6f;
+  } else {
+    x = 0.0f;
+  }
+  return static_cast<int8_t>(fminf(fmaxf(roundf(x), -128.0f), 127.0f));
+}
+
+__global__ void __launch_bounds__(32) FinalCflKernel(const __grid_constant__ CflFinalParams p) {
+  const int tile = blockIdx.x;
+  const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+  const int lane = threadIdx.x;
+  const int problem = lane / 4, slot = lane % 4;  // problem 0: X, 1: B
+  const int bx0 = tx * 8, by0 = ty * 8;
+  const int bx1 = min(bx0 + 8, p.grid.blocks_x), by1 = min(by0 + 8, p.grid.blocks_y);
+  float quadratic = 0.0f, linear = 0.0f;
+  int count = 0;
+  const float scale128 = p.q->scale * 128.0f;
+  if (problem < 2) {
+    const int chroma_channel = problem == 0 ? 0 : 2;
+    const float base = problem == 0 ? 0.0f : 1.0f;
+    for (int by = by0; by < by1; ++by) {
+      for (int bx = bx0; bx < bx1; ++bx) {
+        int cw, ch, s;
+        if (!AnchorAt(p.grid, by * p.grid.blocks_x + bx, &cw, &ch, &s)) continue;
+        const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
+                        : s == kStrategyDct32x32 ? kTableDct32
+                        : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
+                                                                             : kTableDct16x32;
+        const int n = static_cast<int>(p.table_count[table]);
+        const float* inv = p.inverse_dequant + p.table_offset[table] +
+                           (chroma_channel == 0 ? 0 : 2) * n;
+        const float quant_scale = scale128 * static_cast<float>(p.raw[by * p.grid.blocks_x + bx]);
+        const int w = cw * 8;
+        // LLF extent: covered blocks with the longer side first.
+        const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
+        const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
+        for (int i = slot; i < n; i += 4) {
+          const int cy = i / sw, cx = i % sw;
+          const bool llf = cy < lfh && cx < lfw;
+          const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
+          const float cy_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
+          const float cc_v = llf ? 0.0f : p.coef[chroma_channel * p.coef_pitch + at];
+          const float luma = cy_v * inv[i] * quant_scale;
+          const float chroma = cc_v * inv[i] * quant_scale;
+          const float a = luma / 84.0f;
+          const float b = base * luma - chroma;
+          quadratic = fmaf(a, a, quadratic);
+          linear = fmaf(a, b, linear);
+        }
+        count += n;
+      }
+    }
+  }
+  const int base_lane = 4 * (problem < 2 ? problem : 0);
+  const float q0 = __shfl_sync(0xffffffffu, quadratic, base_lane + 0);
+  const float q1 = __shfl_sync(0xffffffffu, quadratic, base_lane + 1);
+  const float q2 = __shfl_sync(0xffffffffu, quadratic, base_lane + 2);
+  const float q3 = __shfl_sync(0xffffffffu, quadratic, base_lane + 3);
+  const float l0 = __shfl_sync(0xffffffffu, linear, base_lane + 0);
+  const float l1 = __shfl_sync(0xffffffffu, linear, base_lane + 1);
+  const float l2 = __shfl_sync(0xffffffffu, linear, base_lane + 2);
+  const float l3 = __shfl_sync(0xffffffffu, linear, base_lane + 3);
+  if (slot == 0 && problem < 2) {
+    int8_t result = 0;
+    if (count > 0) {
+      const float x = -((l0 + l1) + (l2 + l3)) /
+                      (((q0 + q1) + (q2 + q3)) +
+                       static_cast<float>(count) * 1.0e-9f * 0.5f);
+      result = QuantizeMultiplierF(x);
+    }
+    (problem == 0 ? p.y_to_x : p.y_to_b)[tile] = result;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coefficient coding (one CTA per anchor).
+
+struct DcTables {
+  // Inverse / forward LLF bases for lengths 1, 2, 4: [len][freq][sample].
+  double inverse[3][4][4];
+  double forward[3][4][4];
+  float downsample[3][4];
+  float upsample[3][4];
+};
+__constant__ DcTables c_dc_tables;
+
+__device__ __forceinline__ int LenIndex(int len) { return len == 1 ? 0 : len == 2 ? 1 : 2; }
+
+// QuantizationThresholds for X/B (quantization.cpp:185-201).
+__device__ __forceinline__ void ChromaThresholds(int covered, float t[4]) {
+  t[0] = 0.58f;
+  t[1] = t[2] = t[3] = 0.62f;
+  if (covered >= 4) {
+    for (int i = 0; i < 4; ++i) t[i] = fmaxf(0.5f, t[i] - 0.00744f * static_cast<float>(covered));
+  }
+}
+
+// AdjustQuantForChannel (quantization.cpp:285-480) for one channel; runs on
+// one thread over the coefficients in storage order.
+template <int W, int H>
+__device__ void AdjustQuantForChannel(const AqQuantizer& q, int channel, float mm, int strategy,
+                                      const float* coef, const float* inv, float thresholds[4],
+                                      int* raw_quant) {
+  using S = TransformShape<W, H>;
+  const int xsize = S::SW / 8, ysize = S::SH / 8;
+  const float qac = q.scale * static_cast<float>(*raw_quant);
+  if (xsize > 1 || ysize > 1) {
+    const float reduction = fminf(fmaxf(0.003f * static_cast<float>(xsize * ysize), 0.0f), 0.08f);
+    for (int i = 0; i < 4; ++i) thresholds[i] = fmaxf(0.54f, thresholds[i] - reduction);
+  }
+  float border_sum = 0.0f, error_sum = 0.0f, value_sum = 0.0f;
+  float nonzeros[4] = {0, 0, 0, 0}, max_error[4] = {0, 0, 0, 0};
+  for (int y = 0; y < S::SH; ++y) {
+    for (int x = 0; x < S::SW; ++x) {
+      const int index = y * S::SW + x;
+      if (x < xsize && y < ysize) continue;
+      const int quadrant = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
+      const float value = coef[index] * (inv[index] * qac * mm);
+      const float quantized = fabsf(value) < thresholds[quadrant] ? 0.0f : rintf(value);
+      const float err = fabsf(value - quantized);
+      error_sum += err;
+      value_sum += fabsf(quantized);
+      if (channel == 1 && quantized == 0.0f) max_error[quadrant] = fmaxf(max_error[quadrant], err);
+      if (quantized != 0.0f) {
+        nonzeros[quadrant] += fabsf(quantized);
+        const bool in_corner = y >= 7 * ysize && x >= 7 * xsize;
+        const bool on_border = y + 1 == S::SH || x + 1 == S::SW;
+        const bool in_larger_corner = x >= 4 * xsize && y >= 4 * ysize;
+        if (in_corner || (on_border && in_larger_corner)) border_sum += fabsf(value);
+      }
+    }
+  }
+  if (channel == 1 && value_sum * 8.0f < static_cast<float>(xsize * ysize)) {
+    const double kLimit = 0.46, kMultiplier = 0.9999;
+    const int original = *raw_quant;
+    int new_quant = *raw_quant;
+    for (int quadrant = 1; quadrant < 4; ++quadrant) {
+      if (nonzeros[quadrant] == 0.0f && max_error[quadrant] > kLimit) {
+        new_quant = original + 1;
+        break;
+      }
+    }
+    *raw_quant = new_quant;
+    if (nonzeros[3] == 0.0f && max_error[3] > kLimit) {
+      thresholds[3] =
+        static_cast<float>(kMultiplier * max_error[3] * new_quant / original);
+    } else if ((nonzeros[1] == 0.0f && max_error[1] > kLimit) ||
+               (nonzeros[2] == 0.0f && max_error[2] > kLimit)) {
+      thresholds[1] = static_cast<float>(kMultiplier * fmaxf(max_error[1], max_error[2]) *
+                                         new_quant / original);
+      thresholds[2] = thresholds[1];
+    } else if (nonzeros[0] == 0.0f && max_error[0] > kLimit) {
+      thresholds[0] =
+        static_cast<float>(kMultiplier * max_error[0] * new_quant / original);
+    }
+  }
+  const float all_nonzeros = nonzeros[0] + nonzeros[1] + nonzeros[2] + nonzeros[3] + 1.0f;
+  const float kBorderMultiplier = channel == 0 ? 70.0f : channel == 1 ? 30.0f : 60.0f;
+  if (kBorderMultiplier * border_sum >= all_nonzeros) {
+    *raw_quant = static_cast<int>(static_cast<float>(*raw_quant) +
+                                  kBorderMultiplier * border_sum / all_nonzeros);
+    if (*raw_quant >= 256) *raw_quant = 255;
+  }
+  if (strategy == kStrategyDct8 &&
+      nonzeros[0] + nonzeros[1] + nonzeros[2] + nonzeros[3] < 11.0f) {
+    ++*raw_quant;
+    if (*raw_quant >= 256) *raw_quant = 255;
+  }
+  const double kFirst[4][3] = {
+    {0.22080615753848404, 0.45797479824262011, 0.29859235095977965},
+    {0.70109486510286834, 0.16185281305512639, 0.14387691730035473},
+    {0.114985964456218638, 0.44656840441027695, 0.10587658215149048},
+    {0.46849665264409396, 0.41239077937781954, 0.088667407767185444}};
+  const double kSecond[4][3] = {
+    {0.27450281941822197, 1.1255766549984996, 0.98950459134128388},
+    {0.4652168675598285, 0.40945807983455818, 0.36581899811751367},
+    {0.28034972424715715, 0.9182653201929738, 1.5581531543057416},
+    {0.26873118114033728, 0.68863712390392484, 1.2082185408666786}};
+  const double kQuantNormalizer = 2.2942708343284721;
+  error_sum = static_cast<float>(static_cast<double>(error_sum) * kQuantNormalizer);
+  value_sum = static_cast<float>(static_cast<double>(value_sum) * kQuantNormalizer);
+  if (strategy >= kStrategyDct16x16) {
+    int cls = 3;
+    if (strategy == kStrategyDct32x16 || strategy == kStrategyDct16x32) {
+      cls = 1;
+    } else if (strategy == kStrategyDct16x16) {
+      cls = 0;
+    } else if (strategy == kStrategyDct32x32) {
+      cls = 2;
+    }
+    const double threshold =
+      kFirst[cls][channel] * static_cast<double>(xsize) * static_cast<double>(ysize) * 8.0 * 8.0 +
+      kSecond[cls][channel] * static_cast<double>(value_sum);
+    int step = static_cast<int>(static_cast<double>(error_sum) / threshold);
+    step = min(max(step, 0), 2);
+    if (static_cast<double>(error_sum) > threshold) {
+      *raw_quant += step;
+      if (*raw_quant >= 256) *raw_quant = 255;
+    }
+  }
+  const int divisor = xsize * ysize;
+  const float minimum = fminf(fminf(nonzeros[0], nonzeros[1]), fminf(nonzeros[2], nonzeros[3]));
+  int activity = 15;
+  if (minimum < 15.0f * static_cast<float>(divisor)) {
+    activity = (static_cast<int>(minimum) + divisor / 2) / divisor;
+  }
+  int adjusted = *raw_quant - activity;
+  if (channel == 1) {
+    for (int quadrant = 1; quadrant < 4; ++quadrant)
+      thresholds[quadrant] += 0.01f * static_cast<float>(activity);
+  }
+  const int limit = max(4, *raw_quant / 2);
+  if (adjusted < limit) adjusted = limit;
+  *raw_quant = adjusted;
+}
+
+// ConvertLowFrequenciesToDc (dc_conversion.cpp:174-236) of one channel.
+template <int W, int H>
+__device__ void LowFrequenciesToDc(const float* coef, float* out) {
+  using S = TransformShape<W, H>;
+  constexpr int CW = S::CW, CH = S::CH;
+  const int lh = LenIndex(CH), lw = LenIndex(CW);
+  double scaled[16];
+  for (int v = 0; v < CH; ++v) {
+    for (int u = 0; u < CW; ++u) {
+      const int small = CH < CW ? v * CW + u : u * CH + v;
+      scaled[small] = static_cast<double>(coef[S::Index(v, u)]) *
+                      static_cast<double>(c_dc_tables.downsample[lh][v]) *
+                      static_cast<double>(c_dc_tables.downsample[lw][u]);
+    }
+  }
+  for (int y = 0; y < CH; ++y) {
+    for (int x = 0; x < CW; ++x) {
+      double value = 0.0;
+      for (int v = 0; v < CH; ++v) {
+        for (int u = 0; u < CW; ++u) {
+          const int small = CH < CW ? v * CW + u : u * CH + v;
+          value += scaled[small] * c_dc_tables.inverse[lh][v][y] * c_dc_tables.inverse[lw][u][x];
+        }
+      }
+      out[y * CW + x] = static_cast<float>(value);
+    }
+  }
+}
+
+// AdjustQuantizationBias (quantization.cpp:203-218).
+__device__ __forceinline__ float QuantBias(int32_t quantized, int channel) {
+  const float kBias[4] = {1.0f - 0.05465007330715401f, 1.0f - 0.07005449891748593f,
+                          1.0f - 0.049935103337343655f, 0.145f};
+  const float value = static_cast<float>(quantized);
+  const float absolute = fabsf(value);
+  if (absolute < 0.125f) return 0.0f;
+  if (absolute < 1.125f) return copysignf(kBias[channel], value);
+  return value - kBias[3] / value;
+}
+
+
+struct CodingParams {
+  const int2* anchors;
+  const uint32_t* count;
+  int blocks_x;
+  size_t dc_pitch;    // blocks per DC plane
+  const float* coef;  // forward coefficients, footprint layout
+  size_t stride, pitch;
+  int32_t* qac;       // quantized AC, footprint layout
+  float* dc;          // 3 planes of blocks: extracted DC
+  int32_t* raw;       // raw quant field (the anchor's entry is updated)
+  const AqQuantizer* q;
+  const int8_t* y_to_x;
+  const int8_t* y_to_b;
+  int tiles_x;
+  const float* dequant;          // this family's table, [3][N]
+  const float* inverse_dequant;  // this family's table, [3][N]
+  const float* matrix_multiplier;  // device, X / Y / B
+  uint32_t* error;
+};
+
+// ComputeQuantizedCoefficientsImpl's per-transform body
+// (reconstruction.cpp:480-700), one CTA of 64 threads per anchor.
+template <int W, int H>
+__global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ CodingParams p) {
+  using S = TransformShape<W, H>;
+  constexpr int N = S::N;
+  constexpr int strategy = W == 8 && H == 8     ? kStrategyDct8
+                         : W == 16 && H == 16   ? kStrategyDct16x16
+                         : W == 32 && H == 32   ? kStrategyDct32x32
+                         : W == 8               ? kStrategyDct16x8
+                         : H == 8               ? kStrategyDct8x16
+                         : W == 16              ? kStrategyDct32x16
+                                                : kStrategyDct16x32;
+  constexpr int covered = S::CW * S::CH;
+  __shared__ float coef[3][N];
+  __shared__ float thresholds[3][4];
+  __shared__ int candidates[3];
+  const uint32_t anchor_index = blockIdx.x;
+  if (anchor_index >= *p.count) return;
+  const int2 a = p.anchors[anchor_index];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 3 * N; i += 64) {
+    const int c = i / N, j = i % N;
+    coef[c][j] = p.coef[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride +
+                        a.x * 8 + j % W];
+  }
+  __syncthreads();
+  const AqQuantizer q = *p.q;
+  const int anchor_block = a.y * p.blocks_x + a.x;
+  const int initial_raw = p.raw[anchor_block];
+  // SelectAdjustedAcQuantization: the three channels in parallel.
+  if (tid < 3) {
+    float t[4] = {0.58f, 0.64f, 0.64f, 0.64f};
+    int candidate = initial_raw;
+    AdjustQuantForChannel<W, H>(q, tid, p.matrix_multiplier[tid], strategy, coef[tid],
+                                p.inverse_dequant + tid * N, t, &candidate);
+    for (int i = 0; i < 4; ++i) thresholds[tid][i] = t[i];
+    candidates[tid] = candidate;
+  } else if (tid == 32) {
+    // Y DC from the unquantized Y coefficients.
+    float dc[16];
+    LowFrequenciesToDc<W, H>(coef[1], dc);
+    for (int dy = 0; dy < S::CH; ++dy)
+      for (int dx = 0; dx < S::CW; ++dx)
+        p.dc[1 * p.dc_pitch + static_cast<size_t>(a.y + dy) * p.blocks_x + a.x + dx] =
+          dc[dy * S::CW + dx];
+  }
+  __syncthreads();
+  const int raw = max(candidates[0], max(candidates[1], candidates[2]));
+  if (raw < 1 || raw > 256) RaiseError(p.error, kErrorRange);
+  if (tid == 0) p.raw[anchor_block] = raw;
+  // Y: quantize with the adjusted thresholds, store, dequantize in place.
+  const float y_scale = q.scale * static_cast<float>(raw) * 1.0f;
+  const float y_dequant_scale = (q.inverse_global_scale / static_cast<float>(raw)) / 1.0f;
+  for (int j = tid; j < N; j += 64) {
+    const int x = j % S::SW, y = j / S::SW;
+    const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
+    const float value = p.inverse_dequant[N + j] * y_scale * coef[1][j];
+    const int32_t quantized =
+      fabsf(value) < thresholds[1][ti] ? 0 : static_cast<int32_t>(rintf(value));
+    p.qac[p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] = quantized;
+    coef[1][j] = QuantBias(quantized, 1) * (p.dequant[N + j] * y_dequant_scale);
+  }
+  __syncthreads();
+  // Remove the Y prediction from X and B.
+  const int tile = (a.y / 8) * p.tiles_x + (a.x / 8);
+  const float f0 = static_cast<float>(p.y_to_x[tile]) / 84.0f;
+  const float f2 = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
+  for (int j = tid; j < N; j += 64) {
+    coef[0][j] -= f0 * coef[1][j];
+    coef[2][j] -= f2 * coef[1][j];
+  }
+  __syncthreads();
+  if (tid == 0 || tid == 32) {
+    const int c = tid == 0 ? 0 : 2;
+    float dc[16];
+    LowFrequenciesToDc<W, H>(coef[c], dc);
+    for (int dy = 0; dy < S::CH; ++dy)
+      for (int dx = 0; dx < S::CW; ++dx)
+        p.dc[c * p.dc_pitch + static_cast<size_t>(a.y + dy) * p.blocks_x + a.x + dx] =
+          dc[dy * S::CW + dx];
+  }
+  float t[4];
+  ChromaThresholds(covered, t);
+  for (int i = tid; i < 2 * N; i += 64) {
+    const int c = i < N ? 0 : 2, j = i % N;
+    const int x = j % S::SW, y = j / S::SW;
+    const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
+    const float qs = q.scale * static_cast<float>(raw) * p.matrix_multiplier[c];
+    const float value = p.inverse_dequant[c * N + j] * qs * coef[c][j];
+    const int32_t quantized = fabsf(value) < t[ti] ? 0 : static_cast<int32_t>(rintf(value));
+    p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] =
+      quantized;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Prediction-aware DC quantization with the weighted predictor.
+//
+// The reference walks each 256x256-block DC group in raster order. Every
+// sample depends only on its W, N, NW, NE and NN neighbours (and on the
+// predictor's error state of those positions), so all samples on a line
+// x + 2y = t are independent: the kernel runs one CTA per group and sweeps
+// those lines, keeping the predictor state in full-resolution arrays
+// (E: signed errors, PE[4]: per-sub-predictor error sums, as the reference's
+// rolling rows would hold them when each sample is predicted).
+
+struct DcQuantParams {
+  const float* dc;  // 3 planes of blocks
+  int32_t* quantized;
+  float* reconstructed;
+  int32_t* state;  // 5 planes of blocks (E, PE0..PE3)
+  int width, height;
+  size_t pitch;
+  const AqQuantizer* q;
+  float precision;  // 1 << extra_dc_precision
+};
+
+__device__ __forceinline__ int BitWidth64(uint64_t v) { return v == 0 ? 0 : 64 - __clzll(v); }
+__device__ __forceinline__ int BitWidth32(uint32_t v) { return v == 0 ? 0 : 32 - __clz(v); }
+
+__global__ void __launch_bounds__(256) DcQuantKernel(const __grid_constant__ DcQuantParams p) {
+  const int gx0 = blockIdx.x * 256, gy0 = blockIdx.y * 256;
+  const int gw = min(256, p.width - gx0), gh = min(256, p.height - gy0);
+  const int stride = p.width;
+  __shared__ uint32_t row0[4][256];
+  int32_t* E = p.state;
+  uint32_t* PE = reinterpret_cast<uint32_t*>(p.state + p.pitch);  // [4][pitch]
+  const AqQuantizer q = *p.q;
+  float inverse_steps[3], steps[3];
+  for (int c = 0; c < 3; ++c) {
+    inverse_steps[c] = q.inverse_dc_steps[c] * p.precision;
+    steps[c] = q.dc_steps[c] / p.precision;
+  }
+  // WeightedPredictorParameters defaults (prediction.h:36-40).
+  const int64_t pcoef[7] = {16, 10, 7, 7, 7, 0, 0};
+  const uint32_t max_weights[4] = {13, 12, 12, 12};
+  const int order[3] = {1, 0, 2};
+  for (int oc = 0; oc < 3; ++oc) {
+    const int c = order[oc];
+    int32_t* plane = p.quantized + c * p.pitch;
+    const float* source = p.dc + c * p.pitch;
+    const int waves = (gw - 1) + 2 * (gh - 1) + 1;
+    for (int t = 0; t < waves; ++t) {
+      // Positions (x, y) of this group with x + 2y == t.
+      const int y_lo = max(0, (t - (gw - 1) + 1) / 2), y_hi = min(gh - 1, t / 2);
+      for (int y = y_lo + static_cast<int>(threadIdx.x); y <= y_hi; y += blockDim.x) {
+        const int x = t - 2 * y;
+        if (x < 0 || x >= gw) continue;
+        const size_t index = static_cast<size_t>(gy0 + y) * stride + gx0 + x;
+        const int64_t w = x ? plane[index - 1] : y ? plane[index - stride] : 0;
+        const int64_t n = y ? plane[index - stride] : w;
+        const int64_t nw = x && y ? plane[index - stride - 1] : w;
+        const int64_t ne = y && x + 1 < gw ? plane[index - stride + 1] : n;
+        const int64_t nn = y > 1 ? plane[index - 2 * stride] : n;
+        // Predict (prediction.h:73-119). The signed errors of row -1 read as
+        // zeros. The sub-predictor error sums of row 0 read the predictor's
+        // other rolling row, which by then holds only row 0's own "+="
+        // updates: its entry j carries the error of (j - 1, 0) once that
+        // sample is done, so north = err(x-1), northwest = err(x-2) and
+        // northeast (not yet written) = 0, or north at the right edge.
+        const int xne = x + 1 < gw ? x + 1 : x, xnw = x ? x - 1 : x;
+        const size_t up = static_cast<size_t>(gy0 + y - 1) * stride + gx0;
+        uint32_t weights[4];
+        uint32_t weight_sum = 0;
+        for (int i = 0; i < 4; ++i) {
+          uint32_t error;
+          if (y) {
+            error = PE[i * p.pitch + up + x] + PE[i * p.pitch + up + xne] +
+                    PE[i * p.pitch + up + xnw];
+          } else {
+            const uint32_t north = x ? row0[i][x - 1] : 0u;
+            const uint32_t northeast = x + 1 < gw ? 0u : north;
+            const uint32_t northwest = x >= 2 ? row0[i][x - 2] : 0u;
+            error = north + northeast + northwest;
+          }
+          const int shift = max(0, BitWidth64(static_cast<uint64_t>(error) + 1) - 6);
+          const uint32_t reciprocal = (1u << 24) / ((error >> shift) + 1);
+          weights[i] = 4 + ((max_weights[i] * reciprocal) >> shift);
+          weight_sum += weights[i];
+        }
+        const int log_weight = BitWidth32(weight_sum) - 1;
+        weight_sum = 0;
+        for (int i = 0; i < 4; ++i) {
+          weights[i] >>= log_weight - 4;
+          weight_sum += weights[i];
+        }
+        const int64_t ew = x ? E[index - 1] : 0;
+        const int64_t en = y ? E[up + x] : 0;
+        const int64_t enw = y ? E[up + xnw] : 0;
+        const int64_t ene = y ? E[up + xne] : 0;
+        const int64_t n8 = n * 8, w8 = w * 8, ne8 = ne * 8, nw8 = nw * 8, nn8 = nn * 8;
+        int64_t predictions[4];
+        predictions[0] = w8 + ne8 - n8;
+        predictions[1] = n8 - (((en + ew + ene) * pcoef[0]) >> 5);
+        predictions[2] = w8 - (((en + ew + enw) * pcoef[1]) >> 5);
+        predictions[3] = n8 - ((enw * pcoef[2] + en * pcoef[3] + ene * pcoef[4] +
+                                (nn8 - n8) * pcoef[5] + (nw8 - w8) * pcoef[6]) >> 5);
+        int64_t sum = static_cast<int64_t>(weight_sum >> 1) - 1;
+        for (int i = 0; i < 4; ++i) sum += predictions[i] * static_cast<int64_t>(weights[i]);
+        int64_t prediction =
+          (sum * static_cast<int64_t>((1u << 24) / weight_sum)) >> 24;
+        if (((en ^ ew) | (en ^ enw)) <= 0) {
+          const int64_t lo = min(w8, min(ne8, n8)), hi = max(w8, max(ne8, n8));
+          prediction = min(max(prediction, lo), hi);
+        }
+        const int64_t predicted = (prediction + 3) >> 3;
+        // Quantize the residual (dc_quantization.cpp:178-199).
+        float value = source[index];
+        if (c == 2) {
+          value = fmaf(-static_cast<float>(p.quantized[1 * p.pitch + index]), steps[1], value);
+        }
+        float residual = value * inverse_steps[c];
+        residual -= static_cast<float>(predicted);
+        if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
+        float rounded = roundf(residual);
+        if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
+        const int64_t quantized = predicted + static_cast<int64_t>(rounded);
+        plane[index] = static_cast<int32_t>(quantized);
+        // Update (prediction.h:121-141).
+        const int64_t scaled = quantized * 8;
+        E[index] = static_cast<int32_t>(prediction - scaled);
+        for (int i = 0; i < 4; ++i) {
+          const int64_t d = predictions[i] - scaled;
+          const uint32_t err = static_cast<uint32_t>(((d < 0 ? -d : d) + 3) >> 3);
+          PE[i * p.pitch + index] = err;
+          if (y && x + 1 < gw) PE[i * p.pitch + up + x + 1] += err;
+          // Row 0's errors as they were when predicted (row 1 adds to PE's).
+          if (!y) row0[i][x] = err;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // Reconstructed DC (dc_quantization.cpp:209-222).
+  for (int i = threadIdx.x; i < gw * gh; i += blockDim.x) {
+    const size_t index = static_cast<size_t>(gy0 + i / gw) * stride + gx0 + i % gw;
+    const float ry = static_cast<float>(p.quantized[p.pitch + index]) * steps[1];
+    for (int c = 0; c < 3; ++c) {
+      float r = static_cast<float>(p.quantized[c * p.pitch + index]) * steps[c];
+      if (c == 2) r = fmaf(ry, 1.0f, r);
+      p.reconstructed[c * p.pitch + index] = r;
+    }
+  }
+}
+
+// ComputeEpfInverseSigma (epf.cpp:207-270) with neutral sharpness 4.
+__global__ void SigmaKernel(AnchorView v, const int32_t* raw, const AqQuantizer* q,
+                            float* inverse_sigma) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.blocks_x * v.blocks_y) return;
+  int cw, ch, s;
+  if (!AnchorAt(v, i, &cw, &ch, &s)) return;
+  const float kInvSigmaNumerator = -1.1715728752538099024f;
+  const float sigma_quant = 0.46f / (q->scale * static_cast<float>(raw[i]) * kInvSigmaNumerator);
+  float sigma = sigma_quant * (4.0f / 7.0f);
+  sigma = fminf(-1.0e-4f, sigma);
+  const float value = 1.0f / sigma;
+  const int bx = i % v.blocks_x, by = i / v.blocks_x;
+  for (int dy = 0; dy < ch; ++dy)
+    for (int dx = 0; dx < cw; ++dx) inverse_sigma[(by + dy) * v.blocks_x + bx + dx] = value;
+}
+
+// SelectQuantizationMatrixScales (src/codestream/workflow.cpp:1435-1483) and
+// QuantizationMatrixMultiplier (src/codec/codestream.cpp:92-96) on the device,
+// so the stage chain needs no host round trip. `table[s]` = float(1.25^(s-2)).
+struct MatrixScaleTable {
+  float multiplier[16];
+};
+
+__global__ void MatrixScalesKernel(const float* stats, int have_stats, float target,
+                                   MatrixScaleTable table, float* multipliers, int* scales) {
+  const float x_edge = have_stats ? stats[0] : 0.0f;
+  const float b_edge = have_stats ? stats[1] : 0.0f;
+  const float exposed = have_stats ? stats[2] : 0.0f;
+  int x = 3, b = 2;
+  if (target > 2.5f) ++x;
+  if (target > 5.5f) ++x;
+  if (target > 9.5f) ++x;
+  const int xa = x_edge >= 0.026f ? 3 : x_edge >= 0.022f ? 2 : x_edge >= 0.015f ? 1 : 0;
+  x = max(x, 2 + xa);
+  const int eb = exposed >= 0.13f ? 1 : 0;
+  const int ba = b_edge > 0.38f ? 2 + eb : b_edge > 0.33f ? 1 + eb : b_edge > 0.28f ? eb : 0;
+  b += ba;
+  multipliers[0] = table.multiplier[x];
+  multipliers[1] = 1.0f;
+  multipliers[2] = table.multiplier[b];
+  scales[0] = x;
+  scales[1] = b;
+}
+
+unsigned Blocks(size_t n, unsigned threads = kThreads) {
+  return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+
+void UploadDcTables() {
+  static bool done = false;  // guarded by the caller's device-tables lock
+  (void)done;
+  DcTables t;
+  std::memset(&t, 0, sizeof(t));
+  const double sqrt2 = 1.41421356237309504880, pi = 3.14159265358979323846;
+  const int lengths[3] = {1, 2, 4};
+  for (int li = 0; li < 3; ++li) {
+    const int len = lengths[li];
+    for (int f = 0; f < len; ++f) {
+      const double alpha = f == 0 ? sqrt2 / 2.0 : 1.0;
+      for (int s = 0; s < len; ++s) {
+        const double angle = (static_cast<double>(s) + 0.5) * static_cast<double>(f) * pi /
+                             static_cast<double>(len);
+        t.inverse[li][f][s] = sqrt2 * alpha * std::cos(angle);
+        t.forward[li][f][s] = sqrt2 * alpha * std::cos(angle) / static_cast<double>(len);
+      }
+    }
+  }
+  // DCTTotalResampleScale tables (dc_conversion.cpp:95-158).
+  const float down[3][4] = {{1.0f, 0, 0, 0},
+                            {1.0f, 0.901764195028874394f, 0, 0},
+                            {1.0f, 0.974886821136879522f, 0.901764195028874394f,
+                             0.787054918159101335f}};
+  const float up[3][4] = {{1.0f, 0, 0, 0},
+                          {1.0f, 1.108937353592731823f, 0, 0},
+                          {1.0f, 1.025760096781116015f, 1.108937353592731823f,
+                           1.270559368765487251f}};
+  std::memcpy(t.downsample, down, sizeof(down));
+  std::memcpy(t.upsample, up, sizeof(up));
+  cudaMemcpyToSymbol(c_dc_tables, &t, sizeof(t));
+}
+
+int AqMatrixScales(const float* stats, bool have_stats, float target, float* multipliers,
+                   int* scales, cudaStream_t stream) {
+  MatrixScaleTable table;
+  for (int s = 0; s < 16; ++s) table.multiplier[s] = static_cast<float>(std::pow(1.25, s - 2));
+  MatrixScalesKernel<<<1, 1, 0, stream>>>(stats, have_stats ? 1 : 0, target, table, multipliers,
+                                          scales);
+  return CheckLaunch("aq matrix scales");
+}
+
+int AqBuildAnchors(const uint8_t* cells, size_t bx, size_t by, int2* lists, uint32_t* counts,
+                   cudaStream_t stream) {
+  const size_t blocks = bx * by;
+  cudaMemsetAsync(counts, 0, kFamilyCountT * sizeof(uint32_t), stream);
+  AnchorListKernel<<<Blocks(blocks), kThreads, 0, stream>>>(
+    cells, static_cast<uint32_t>(bx), static_cast<uint32_t>(blocks), lists,
+    static_cast<uint32_t>(blocks), counts);
+  return CheckLaunch("aq anchors");
+}
+
+template <int W, int H>
+int LaunchForward(const float* opsin, size_t stride, size_t pitch, const int2* list,
+                  const uint32_t* count, size_t max_count, const DeviceTables& d, float* coef,
+                  cudaStream_t stream) {
+  constexpr int N = W * H;
+  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  const size_t smem = static_cast<size_t>(K) * 3 * N * 12;
+  int status = CheckCuda(cudaFuncSetAttribute(ForwardCoefficientsKernel<W, H>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)),
+                         "aq forward attribute");
+  if (status != GJXL_B200_OK) return status;
+  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2, hi = H == 8 ? 0 : H == 16 ? 1 : 2;
+  const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
+  if (grid == 0) return GJXL_B200_OK;
+  ForwardCoefficientsKernel<W, H><<<grid, kThreads, smem, stream>>>(
+    opsin, stride, pitch, list, count, d.forward_t[wi], d.forward[hi], coef, stride, pitch);
+  return CheckLaunch("aq forward coefficients");
+}
+
+int AqForwardCoefficients(const float* opsin, size_t stride, size_t pitch, size_t bx, size_t by,
+                          const int2* lists, const uint32_t* counts, float* coef,
+                          cudaStream_t stream) {
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const size_t blocks = bx * by;
+  for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    const int2* list = lists + f * blocks;
+    const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
+    switch (f) {
+      case 0: status = LaunchForward<8, 8>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 1: status = LaunchForward<8, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 2: status = LaunchForward<16, 8>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 3: status = LaunchForward<16, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 4: status = LaunchForward<16, 32>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 5: status = LaunchForward<32, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 6: status = LaunchForward<32, 32>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+    }
+  }
+  return status;
+}
+
+int AqAdjustField(const uint8_t* cells, size_t bx, size_t by, const float* in, float* out,
+                  float target, cudaStream_t stream) {
+  const size_t blocks = bx * by;
+  float mixer = 1.0f;
+  const float kMixerLimit = 1.54138f, kMixerSlope = 0.56391f;
+  if (target > kMixerLimit) mixer = std::max(0.0f, mixer - (target - kMixerLimit) * kMixerSlope);
+  if (in != out) cudaMemcpyAsync(out, in, blocks * sizeof(float), cudaMemcpyDeviceToDevice, stream);
+  AnchorView v{cells, static_cast<int>(bx), static_cast<int>(by)};
+  AdjustFieldKernel<<<Blocks(blocks), kThreads, 0, stream>>>(v, in, out, mixer);
+  return CheckLaunch("aq adjust field");
+}
+
+int AqPolicySetup(const float* field, size_t blocks, float target, float* range,
+                  AqPolicy* policy, uint32_t* error, cudaStream_t stream) {
+  const float init[2] = {__builtin_huge_valf(), 0.0f};
+  cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+  RangeKernel<<<Blocks(blocks), kThreads, 0, stream>>>(field, static_cast<int>(blocks), range);
+  // ComputeInitialQuantDc (adaptive_quantization.cpp:536-560), host powf.
+  const float kDcMul = 0.3f;
+  const float nonlinear = kDcMul * std::pow(target / kDcMul, 0.83f);
+  const float target_dc = std::max(0.5f * target, std::min(target, nonlinear));
+  const float quant_dc = std::min(1.095924047623553f / target_dc, 50.0f);
+  PolicySetupKernel<<<1, 1, 0, stream>>>(range, quant_dc, policy, error);
+  return CheckLaunch("aq policy setup");
+}
+
+int AqQuantizer_(const float* field, size_t blocks, const AqPolicy* policy, AqQuantizer* q,
+                 int32_t* raw, uint32_t* error, cudaStream_t stream) {
+  QuantizerKernel<<<1, 1024, 0, stream>>>(field, static_cast<int>(blocks), policy, q, error);
+  RawQuantKernel<<<Blocks(blocks), kThreads, 0, stream>>>(field, static_cast<int>(blocks), q, raw);
+  return CheckLaunch("aq quantizer");
+}
+
+int AqFinalCfl(const uint8_t* cells, size_t bx, size_t by, const float* coef, size_t stride,
+               size_t pitch, const int32_t* raw, const AqQuantizer* q, int8_t* y_to_x,
+               int8_t* y_to_b, cudaStream_t stream) {
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const HostTables& h = GetHostTables();
+  CflFinalParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.grid = {cells, static_cast<int>(bx), static_cast<int>(by)};
+  p.tiles_x = static_cast<int>((bx + 7) / 8);
+  p.tiles_y = static_cast<int>((by + 7) / 8);
+  p.coef = coef;
+  p.coef_stride = stride;
+  p.coef_pitch = pitch;
+  p.raw = raw;
+  p.q = q;
+  p.inverse_dequant = d.inverse_dequant;
+  for (int t = 0; t < kTableCount; ++t) {
+    p.table_offset[t] = h.layout.offset[t];
+    p.table_count[t] = h.layout.count[t];
+  }
+  p.y_to_x = y_to_x;
+  p.y_to_b = y_to_b;
+  FinalCflKernel<<<p.tiles_x * p.tiles_y, 32, 0, stream>>>(p);
+  return CheckLaunch("aq final cfl");
+}
+
+template <int W, int H>
+int LaunchCoding(CodingParams p, const DeviceTables& d, int family, size_t max_count,
+                 cudaStream_t stream) {
+  const HostTables& h = GetHostTables();
+  const int table = StrategyTableFamily(FamilyStrategy(family));
+  p.dequant = d.dequant + h.layout.offset[table];
+  p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  if (max_count == 0) return GJXL_B200_OK;
+  CodingKernel<W, H><<<static_cast<unsigned>(max_count), 64, 0, stream>>>(p);
+  return CheckLaunch("aq coding");
+}
+
+int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, const float* coef,
+             size_t stride, size_t pitch, int32_t* qac, float* dc, int32_t* raw,
+             const AqQuantizer* q, const int8_t* y_to_x, const int8_t* y_to_b,
+             const float* matrix_multiplier, uint32_t* error, cudaStream_t stream) {
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const size_t blocks = bx * by;
+  CodingParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.blocks_x = static_cast<int>(bx);
+  p.dc_pitch = blocks;
+  p.coef = coef;
+  p.stride = stride;
+  p.pitch = pitch;
+  p.qac = qac;
+  p.dc = dc;
+  p.raw = raw;
+  p.q = q;
+  p.y_to_x = y_to_x;
+  p.y_to_b = y_to_b;
+  p.tiles_x = static_cast<int>((bx + 7) / 8);
+  p.matrix_multiplier = matrix_multiplier;
+  p.error = error;
+  for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    p.anchors = lists + f * blocks;
+    p.count = counts + f;
+    const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
+    switch (f) {
+      case 0: status = LaunchCoding<8, 8>(p, d, f, max_count, stream); break;
+      case 1: status = LaunchCoding<8, 16>(p, d, f, max_count, stream); break;
+      case 2: status = LaunchCoding<16, 8>(p, d, f, max_count, stream); break;
+      case 3: status = LaunchCoding<16, 16>(p, d, f, max_count, stream); break;
+      case 4: status = LaunchCoding<16, 32>(p, d, f, max_count, stream); break;
+      case 5: status = LaunchCoding<32, 16>(p, d, f, max_count, stream); break;
+      case 6: status = LaunchCoding<32, 32>(p, d, f, max_count, stream); break;
+    }
+  }
+  return status;
+}
+
+int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, int32_t* quantized,
+                 float* reconstructed, int32_t* state, int extra_precision, cudaStream_t stream) {
+  const size_t blocks = bx * by;
+  cudaMemsetAsync(state, 0, 5 * blocks * sizeof(int32_t), stream);
+  DcQuantParams p;
+  p.dc = dc;
+  p.quantized = quantized;
+  p.reconstructed = reconstructed;
+  p.state = state;
+  p.width = static_cast<int>(bx);
+  p.height = static_cast<int>(by);
+  p.pitch = blocks;
+  p.q = q;
+  p.precision = static_cast<float>(1u << extra_precision);
+  dim3 grid(static_cast<unsigned>((bx + 255) / 256), static_cast<unsigned>((by + 255) / 256));
+  DcQuantKernel<<<grid, 256, 0, stream>>>(p);
+  return CheckLaunch("aq dc quantize");
+}
+
+int AqInverseSigma(const uint8_t* cells, size_t bx, size_t by, const int32_t* raw,
+                   const AqQuantizer* q, float* inverse_sigma, cudaStream_t stream) {
+  AnchorView v{cells, static_cast<int>(bx), static_cast<int>(by)};
+  SigmaKernel<<<Blocks(bx * by), kThreads, 0, stream>>>(v, raw, q, inverse_sigma);
+  return CheckLaunch("aq inverse sigma");
+}
+
+}  // namespace gjxl_b200

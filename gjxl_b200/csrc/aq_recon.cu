@@ -1,0 +1,536 @@
+// Rows a13, a15, a16: decoder-equivalent reconstruction, loop filters,
+// XYB -> linear RGB, per-transform Butteraugli reduction and the AQ field
+// update, on the device.
+//
+// Restates, with the reference's exact operation order:
+//   SmoothDcCoefficients            src/codec/dc_smoothing.cpp:13-80
+//   ReconstructQuantizedCoefficients src/codec/reconstruction.cpp:790-936
+//   ConvertDcToLowFrequencies       src/codec/dc_conversion.cpp:238-299
+//   DequantizeAcBlock               src/codec/quantization.cpp:822-862
+//   ApplyLoopFilters / ApplyGaborish src/codec/loop_filter.cpp, src/codec/gaborish.cpp:101-185
+//   ApplyEpf (two iterations: pass 1 then pass 2)  src/codec/epf.cpp:11-160, 297-410
+//   OpsinToLinearRgb                src/codec/color_transform.cpp:433-469
+//   ReduceButteraugliDistanceMap    src/codec/butteraugli.cpp:116-199
+//   RunAdaptiveQuantizationPolicyImpl update  src/codec/adaptive_quantization.cpp:1684-1726
+
+#include <cmath>
+#include <cstring>
+
+#include "aq.h"
+#include "common.cuh"
+#include "host_util.h"
+#include "tables.h"
+#include "transform.cuh"
+
+namespace gjxl_b200 {
+
+struct DcTablesRecon {
+  double forward[3][4][4];
+  float upsample[3][4];
+};
+__constant__ DcTablesRecon c_dc_recon;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned Blocks(size_t n, unsigned threads = kThreads) {
+  return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+__global__ void SmoothDcKernel(const float* dc, int w, int h, size_t pitch, const AqQuantizer* q,
+                               float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w * h) return;
+  const int x = i % w, y = i / w;
+  if (x == 0 || y == 0 || x + 1 >= w || y + 1 >= h) {
+    for (int c = 0; c < 3; ++c) out[c * pitch + i] = dc[c * pitch + i];
+    return;
+  }
+  constexpr float side_weight = 0.20345139757231578f;
+  constexpr float corner_weight = 0.0334829185968739f;
+  constexpr float center_weight = 1.0f - 4.0f * (side_weight + corner_weight);
+  float center[3], smoothed[3];
+  float gap = 0.5f;
+  for (int c = 0; c < 3; ++c) {
+    const float* row = dc + c * pitch + static_cast<size_t>(y) * w;
+    const float* top = row - w;
+    const float* bottom = row + w;
+    const float corners = (top[x - 1] + top[x + 1]) + (bottom[x - 1] + bottom[x + 1]);
+    const float sides = (row[x - 1] + row[x + 1]) + (top[x] + bottom[x]);
+    center[c] = row[x];
+    smoothed[c] = fmaf(corners, corner_weight, fmaf(sides, side_weight, row[x] * center_weight));
+    const float normalized_gap = fabsf((row[x] - smoothed[c]) / q->dc_steps[c]);
+    gap = fmaxf(gap, normalized_gap);
+  }
+  const float factor = fmaxf(0.0f, fmaf(-4.0f, gap, 3.0f));
+  for (int c = 0; c < 3; ++c) out[c * pitch + i] = fmaf(smoothed[c] - center[c], factor, center[c]);
+}
+
+__device__ __forceinline__ float QuantBiasR(int32_t quantized, int channel) {
+  const float kBias[4] = {1.0f - 0.05465007330715401f, 1.0f - 0.07005449891748593f,
+                          1.0f - 0.049935103337343655f, 0.145f};
+  const float value = static_cast<float>(quantized);
+  const float absolute = fabsf(value);
+  if (absolute < 0.125f) return 0.0f;
+  if (absolute < 1.125f) return copysignf(kBias[channel], value);
+  return value - kBias[3] / value;
+}
+
+__device__ __forceinline__ int LenIdx(int len) { return len == 1 ? 0 : len == 2 ? 1 : 2; }
+
+// ConvertDcToLowFrequencies for one channel of one transform.
+template <int W, int H>
+__device__ void DcToLowFrequencies(const float* dc_plane, int blocks_x, int ax, int ay,
+                                   float* coef) {
+  using S = TransformShape<W, H>;
+  constexpr int CW = S::CW, CH = S::CH;
+  const int lh = LenIdx(CH), lw = LenIdx(CW);
+  float low[16];
+  for (int v = 0; v < CH; ++v) {
+    for (int u = 0; u < CW; ++u) {
+      double value = 0.0;
+      for (int y = 0; y < CH; ++y) {
+        for (int x = 0; x < CW; ++x) {
+          value += static_cast<double>(dc_plane[(ay + y) * blocks_x + ax + x]) *
+                   c_dc_recon.forward[lh][v][y] * c_dc_recon.forward[lw][u][x];
+        }
+      }
+      const int small = CH < CW ? v * CW + u : u * CH + v;
+      low[small] = static_cast<float>(value * static_cast<double>(c_dc_recon.upsample[lh][v]) *
+                                      static_cast<double>(c_dc_recon.upsample[lw][u]));
+    }
+  }
+  for (int v = 0; v < CH; ++v)
+    for (int u = 0; u < CW; ++u) coef[S::Index(v, u)] = low[CH < CW ? v * CW + u : u * CH + v];
+}
+
+struct ReconParams {
+  const int2* anchors;
+  const uint32_t* count;
+  int blocks_x;
+  size_t dc_pitch;
+  const int32_t* qac;
+  size_t stride, pitch;
+  const float* dc;  // smoothed DC, 3 planes of blocks
+  const int32_t* raw;
+  const AqQuantizer* q;
+  const int8_t* y_to_x;
+  const int8_t* y_to_b;
+  int tiles_x;
+  const float* dequant;  // family table [3][N]
+  const float* matrix_multiplier;  // device, X / Y / B
+  const double* iw;
+  const double* ih;
+  float* recon;
+};
+
+template <int W, int H>
+__global__ void __launch_bounds__(kThreads) ReconstructKernel(const __grid_constant__ ReconParams p) {
+  constexpr int N = W * H;
+  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* coef = reinterpret_cast<float*>(smem);                // [K*3][N]
+  double* tmp = reinterpret_cast<double*>(coef + K * 3 * N);  // [K*3][N]
+  __shared__ int2 anchor[K];
+  __shared__ float scales[K][3];
+  __shared__ float factors[K][2];
+  const uint32_t first = blockIdx.x * K;
+  const uint32_t n = *p.count;
+  if (first >= n) return;
+  const int active = min(K, static_cast<int>(n - first));
+  if (threadIdx.x < active) {
+    const int k = threadIdx.x;
+    const int2 a = p.anchors[first + k];
+    anchor[k] = a;
+    const int raw = p.raw[a.y * p.blocks_x + a.x];
+    for (int c = 0; c < 3; ++c) {
+      scales[k][c] = (p.q->inverse_global_scale / static_cast<float>(raw)) / p.matrix_multiplier[c];
+    }
+    const int tile = (a.y / 8) * p.tiles_x + (a.x / 8);
+    factors[k][0] = static_cast<float>(p.y_to_x[tile]) / 84.0f;
+    factors[k][1] = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
+  }
+  __syncthreads();
+  // Dequantize.
+  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    const int2 a = anchor[k];
+    const int32_t qv =
+      p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W];
+    coef[i] = QuantBiasR(qv, c) * (p.dequant[c * N + j] * scales[k][c]);
+  }
+  __syncthreads();
+  // Restore the chroma from luma.
+  for (int i = threadIdx.x; i < active * N; i += kThreads) {
+    const int k = i / N, j = i % N;
+    float* cf = coef + k * 3 * N;
+    const float y = cf[N + j];
+    cf[j] += factors[k][0] * y;
+    cf[2 * N + j] += factors[k][1] * y;
+  }
+  __syncthreads();
+  // LLF from the (smoothed) DC, one thread per transform channel.
+  if (threadIdx.x < active * 3) {
+    const int k = threadIdx.x / 3, c = threadIdx.x % 3;
+    DcToLowFrequencies<W, H>(p.dc + c * p.dc_pitch, p.blocks_x, anchor[k].x, anchor[k].y,
+                             coef + (k * 3 + c) * N);
+  }
+  __syncthreads();
+  InverseRows<W, H>(coef, tmp, p.iw, active * 3, threadIdx.x, kThreads);
+  __syncthreads();
+  InverseColumns<W, H>(tmp, coef, p.ih, active * 3, threadIdx.x, kThreads);
+  __syncthreads();
+  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    const int2 a = anchor[k];
+    p.recon[c * p.pitch + static_cast<size_t>(a.y * 8 + yx / W) * p.stride + a.x * 8 + yx % W] =
+      coef[i];
+  }
+}
+
+__device__ __forceinline__ int MirrorR(int c, int n) {
+  if (c >= 0 && c < n) return c;
+  const int period = 2 * n;
+  int phase;
+  if (c >= 0) {
+    phase = c % period;
+  } else {
+    const int r = (-c) % period;
+    phase = r == 0 ? 0 : period - r;
+  }
+  return phase < n ? phase : period - 1 - phase;
+}
+
+struct GaborishParams {
+  const float* in;
+  size_t in_stride, in_pitch;
+  float* out;  // dense width x height planes
+  int w, h;
+  float weights[3];  // center, axis, diagonal
+  uint32_t* error;
+};
+
+__global__ void GaborishForwardKernel(const __grid_constant__ GaborishParams p) {
+  const int c = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.w * p.h) return;
+  const int x = i % p.w, y = i / p.w;
+  const float* plane = p.in + c * p.in_pitch;
+  auto s = [&](int dx, int dy) {
+    return plane[static_cast<size_t>(MirrorR(y + dy, p.h)) * p.in_stride + MirrorR(x + dx, p.w)];
+  };
+  const float axes = (s(-1, 0) + s(1, 0)) + (s(0, -1) + s(0, 1));
+  const float diagonals = (s(-1, -1) + s(1, -1)) + (s(-1, 1) + s(1, 1));
+  const float value = p.weights[0] * s(0, 0) + p.weights[1] * axes + p.weights[2] * diagonals;
+  if (!IsFinite(value)) RaiseError(p.error, kErrorNonFiniteOutput);
+  p.out[static_cast<size_t>(c) * p.w * p.h + i] = value;
+}
+
+struct EpfParams {
+  const float* in;  // dense planes
+  float* out;
+  int w, h;
+  const float* inverse_sigma;
+  int blocks_x;
+  float sigma_scale;
+  int pass;  // 1: patch SAD, 2: pixel SAD (cardinal neighbours)
+};
+
+__global__ void EpfKernel(const __grid_constant__ EpfParams p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.w * p.h) return;
+  const int x = i % p.w, y = i / p.w;
+  const size_t n = static_cast<size_t>(p.w) * p.h;
+  const float block_inverse_sigma = p.inverse_sigma[(y / 8) * p.blocks_x + x / 8];
+  const float kMinInverseSigma = -1.1715728752538099024f / 0.3f;
+  if (block_inverse_sigma < kMinInverseSigma) {
+    for (int c = 0; c < 3; ++c) p.out[c * n + i] = p.in[c * n + i];
+    return;
+  }
+  const bool border = x % 8 == 0 || x % 8 == 7 || y % 8 == 0 || y % 8 == 7;
+  const float scaled = block_inverse_sigma * p.sigma_scale * (border ? 2.0f / 3.0f : 1.0f);
+  auto sample = [&](int c, int sx, int sy) {
+    return p.in[c * n + static_cast<size_t>(MirrorR(sy, p.h)) * p.w + MirrorR(sx, p.w)];
+  };
+  const float channel_scale[3] = {40.0f, 5.0f, 3.5f};
+  float sum[3] = {p.in[i], p.in[n + i], p.in[2 * n + i]};
+  float weight_sum = 1.0f;
+  const int offsets[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
+  const int plus[5][2] = {{0, 0}, {0, -1}, {-1, 0}, {0, 1}, {1, 0}};
+  for (int o = 0; o < 4; ++o) {
+    const int dx = offsets[o][0], dy = offsets[o][1];
+    float sad = 0.0f;
+    for (int c = 0; c < 3; ++c) {
+      if (p.pass == 1) {
+        float channel_sad = 0.0f;
+        for (int k = 0; k < 5; ++k) {
+          channel_sad += fabsf(sample(c, x + plus[k][0], y + plus[k][1]) -
+                               sample(c, x + dx + plus[k][0], y + dy + plus[k][1]));
+        }
+        sad = fmaf(channel_sad, channel_scale[c], sad);
+      } else {
+        sad = fmaf(fabsf(sample(c, x, y) - sample(c, x + dx, y + dy)), channel_scale[c], sad);
+      }
+    }
+    const float weight = fmaxf(0.0f, fmaf(sad, scaled, 1.0f));
+    weight_sum += weight;
+    for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, sample(c, x + dx, y + dy), sum[c]);
+  }
+  for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
+}
+
+struct LinearParams {
+  const float* opsin;
+  float* linear;
+  size_t n;
+  float bias_cuberoot;
+  float scaled_matrix[3][3];  // scale * inverse opsin matrix
+  uint32_t* error;
+};
+
+__global__ void OpsinToLinearKernel(const __grid_constant__ LinearParams p) {
+  const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+  if (i >= p.n) return;
+  const float x = p.opsin[i], y = p.opsin[p.n + i], b = p.opsin[2 * p.n + i];
+  const float kOpsinBias = 0.0037930732552754493f;
+  const float gamma[3] = {y + x + p.bias_cuberoot, y - x + p.bias_cuberoot, b + p.bias_cuberoot};
+  float mixed[3];
+  for (int c = 0; c < 3; ++c) mixed[c] = gamma[c] * gamma[c] * gamma[c] - kOpsinBias;
+  for (int r = 0; r < 3; ++r) {
+    float v = p.scaled_matrix[r][0] * mixed[0];
+    v = fmaf(p.scaled_matrix[r][1], mixed[1], v);
+    v = fmaf(p.scaled_matrix[r][2], mixed[2], v);
+    if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
+    p.linear[r * p.n + i] = v;
+  }
+}
+
+__global__ void BlockReduceKernel(const uint8_t* cells, int blocks_x, int blocks_y,
+                                  const float* map, int w, int h, float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= blocks_x * blocks_y) return;
+  const uint8_t cell = cells[i];
+  if (!(cell & 1)) return;
+  const int f = StrategyFamily(cell >> 1);
+  const int cw = FamilyCoveredW(f), ch = FamilyCoveredH(f);
+  const int bx = i % blocks_x, by = i / blocks_x;
+  const int x0 = bx * 8, y0 = by * 8;
+  const int x1 = min(w, x0 + cw * 8), y1 = min(h, y0 + ch * 8);
+  float norm = 0.0f;
+  int count = 0;
+  for (int y = y0; y < y1; ++y) {
+    for (int x = x0; x < x1; ++x) {
+      float v = map[static_cast<size_t>(y) * w + x];
+      v *= v;
+      v *= v;
+      v *= v;
+      v *= v;
+      norm += v;
+      ++count;
+    }
+  }
+  // std::pow(float, 1/16): evaluated in double and rounded to float.
+  const float mean = norm / static_cast<float>(count);
+  const float d = 1.2f * static_cast<float>(pow(static_cast<double>(mean), 0.0625));
+  for (int dy = 0; dy < ch; ++dy)
+    for (int dx = 0; dx < cw; ++dx) out[(by + dy) * blocks_x + bx + dx] = d;
+}
+
+__global__ void PolicyUpdateKernel(float* field, const float* adjusted_initial,
+                                   const float* block_distance, int n, int iteration,
+                                   float target, const AqPolicy* policy, const AqQuantizer* q,
+                                   uint32_t* error) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float lo = policy->lower_bound, hi = policy->upper_bound;
+  float value = field[i];
+  if (iteration == 1) {
+    const float clamp = 0.4f * value + 0.6f * adjusted_initial[i];
+    if (value < clamp) value = fminf(fmaxf(clamp, lo), hi);
+  }
+  const float difference = block_distance[i] / target;
+  if (!(IsFinite(difference) && difference >= 0.0f)) RaiseError(error, kErrorInternal);
+  if (difference <= 1.0f) {
+    if (iteration < 2) value *= static_cast<float>(pow(static_cast<double>(difference), 0.2));
+  } else {
+    const float old = value;
+    value *= difference;
+    const long old_raw = lroundf(old * q->inverse_global_scale);
+    const long new_raw = lroundf(value * q->inverse_global_scale);
+    if (old_raw == new_raw) value = old + q->scale;
+  }
+  field[i] = fminf(fmaxf(value, lo), hi);
+}
+
+}  // namespace
+
+void UploadDcReconTables() {
+  DcTablesRecon t;
+  std::memset(&t, 0, sizeof(t));
+  const double sqrt2 = 1.41421356237309504880, pi = 3.14159265358979323846;
+  const int lengths[3] = {1, 2, 4};
+  for (int li = 0; li < 3; ++li) {
+    const int len = lengths[li];
+    for (int f = 0; f < len; ++f) {
+      const double alpha = f == 0 ? sqrt2 / 2.0 : 1.0;
+      for (int s = 0; s < len; ++s) {
+        const double angle = (static_cast<double>(s) + 0.5) * static_cast<double>(f) * pi /
+                             static_cast<double>(len);
+        t.forward[li][f][s] = sqrt2 * alpha * std::cos(angle) / static_cast<double>(len);
+      }
+    }
+  }
+  const float up[3][4] = {{1.0f, 0, 0, 0},
+                          {1.0f, 1.108937353592731823f, 0, 0},
+                          {1.0f, 1.025760096781116015f, 1.108937353592731823f,
+                           1.270559368765487251f}};
+  std::memcpy(t.upsample, up, sizeof(up));
+  cudaMemcpyToSymbol(c_dc_recon, &t, sizeof(t));
+}
+
+int AqSmoothDc(const float* dc, size_t bx, size_t by, const AqQuantizer* q, float* out,
+               cudaStream_t stream) {
+  SmoothDcKernel<<<Blocks(bx * by), kThreads, 0, stream>>>(dc, static_cast<int>(bx),
+                                                           static_cast<int>(by), bx * by, q, out);
+  return CheckLaunch("aq smooth dc");
+}
+
+template <int W, int H>
+int LaunchReconstruct(ReconParams p, const DeviceTables& d, int family, size_t max_count,
+                      cudaStream_t stream) {
+  constexpr int N = W * H;
+  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  const HostTables& h = GetHostTables();
+  const int table = StrategyTableFamily(FamilyStrategy(family));
+  p.dequant = d.dequant + h.layout.offset[table];
+  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2, hi = H == 8 ? 0 : H == 16 ? 1 : 2;
+  p.iw = d.inverse[wi];
+  p.ih = d.inverse[hi];
+  const size_t smem = static_cast<size_t>(K) * 3 * N * 12;
+  int status = CheckCuda(cudaFuncSetAttribute(ReconstructKernel<W, H>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)),
+                         "aq reconstruct attribute");
+  if (status != GJXL_B200_OK) return status;
+  const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
+  if (grid == 0) return GJXL_B200_OK;
+  ReconstructKernel<W, H><<<grid, kThreads, smem, stream>>>(p);
+  return CheckLaunch("aq reconstruct");
+}
+
+int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t by,
+                  const int32_t* qac, size_t stride, size_t pitch, const float* dc,
+                  const int32_t* raw, const AqQuantizer* q, const int8_t* y_to_x,
+                  const int8_t* y_to_b, const float* matrix_multiplier, float* recon,
+                  cudaStream_t stream) {
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const size_t blocks = bx * by;
+  ReconParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.blocks_x = static_cast<int>(bx);
+  p.dc_pitch = blocks;
+  p.qac = qac;
+  p.stride = stride;
+  p.pitch = pitch;
+  p.dc = dc;
+  p.raw = raw;
+  p.q = q;
+  p.y_to_x = y_to_x;
+  p.y_to_b = y_to_b;
+  p.tiles_x = static_cast<int>((bx + 7) / 8);
+  p.matrix_multiplier = matrix_multiplier;
+  p.recon = recon;
+  for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    p.anchors = lists + f * blocks;
+    p.count = counts + f;
+    const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
+    switch (f) {
+      case 0: status = LaunchReconstruct<8, 8>(p, d, f, max_count, stream); break;
+      case 1: status = LaunchReconstruct<8, 16>(p, d, f, max_count, stream); break;
+      case 2: status = LaunchReconstruct<16, 8>(p, d, f, max_count, stream); break;
+      case 3: status = LaunchReconstruct<16, 16>(p, d, f, max_count, stream); break;
+      case 4: status = LaunchReconstruct<16, 32>(p, d, f, max_count, stream); break;
+      case 5: status = LaunchReconstruct<32, 16>(p, d, f, max_count, stream); break;
+      case 6: status = LaunchReconstruct<32, 32>(p, d, f, max_count, stream); break;
+    }
+  }
+  return status;
+}
+
+int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, size_t width,
+                  size_t height, const float* inverse_sigma, size_t bx, float* scratch_a,
+                  float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream) {
+  const size_t n = width * height;
+  GaborishParams g;
+  g.in = recon;
+  g.in_stride = recon_stride;
+  g.in_pitch = recon_pitch;
+  g.out = scratch_a;
+  g.w = static_cast<int>(width);
+  g.h = static_cast<int>(height);
+  // ApplyGaborish weights (gaborish.cpp:118-138).
+  const float w1 = 1.1f * 0.104699568f, w2 = 1.1f * 0.055680538f;
+  const float divisor = 1.0f + 4.0f * (w1 + w2);
+  g.weights[0] = 1.0f / divisor;
+  g.weights[1] = w1 / divisor;
+  g.weights[2] = w2 / divisor;
+  g.error = error;
+  GaborishForwardKernel<<<dim3(Blocks(n), 3), kThreads, 0, stream>>>(g);
+  EpfParams e;
+  e.w = static_cast<int>(width);
+  e.h = static_cast<int>(height);
+  e.inverse_sigma = inverse_sigma;
+  e.blocks_x = static_cast<int>(bx);
+  e.in = scratch_a;
+  e.out = scratch_b;
+  e.sigma_scale = 1.65f * 1.0f;
+  e.pass = 1;
+  EpfKernel<<<Blocks(n), kThreads, 0, stream>>>(e);
+  e.in = scratch_b;
+  e.out = filtered;
+  e.sigma_scale = 1.65f * 6.5f;
+  e.pass = 2;
+  EpfKernel<<<Blocks(n), kThreads, 0, stream>>>(e);
+  return CheckLaunch("aq loop filters");
+}
+
+int AqOpsinToLinear(const float* opsin, size_t width, size_t height, float intensity_target,
+                    float* linear, uint32_t* error, cudaStream_t stream) {
+  LinearParams p;
+  p.opsin = opsin;
+  p.linear = linear;
+  p.n = width * height;
+  p.bias_cuberoot = std::cbrt(0.0037930732552754493f);
+  const float kInverse[3][3] = {
+    {11.031566901960783f, -9.866943921568629f, -0.16462299647058826f},
+    {-3.254147380392157f, 4.418770392156863f, -0.16462299647058826f},
+    {-3.6588512862745097f, 2.7129230470588235f, 1.9459282392156863f}};
+  const float scale = 255.0f / intensity_target;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) p.scaled_matrix[r][c] = scale * kInverse[r][c];
+  p.error = error;
+  OpsinToLinearKernel<<<Blocks(p.n), kThreads, 0, stream>>>(p);
+  return CheckLaunch("aq opsin to linear");
+}
+
+int AqBlockReduce(const uint8_t* cells, size_t bx, size_t by, const float* distance_map,
+                  size_t width, size_t height, float* block_distance, cudaStream_t stream) {
+  BlockReduceKernel<<<Blocks(bx * by), kThreads, 0, stream>>>(
+    cells, static_cast<int>(bx), static_cast<int>(by), distance_map, static_cast<int>(width),
+    static_cast<int>(height), block_distance);
+  return CheckLaunch("aq block reduce");
+}
+
+int AqPolicyUpdate(float* field, const float* adjusted_initial, const float* block_distance,
+                   size_t blocks, int iteration, float target, const AqPolicy* policy,
+                   const AqQuantizer* q, uint32_t* error, cudaStream_t stream) {
+  PolicyUpdateKernel<<<Blocks(blocks), kThreads, 0, stream>>>(
+    field, adjusted_initial, block_distance, static_cast<int>(blocks), iteration, target, policy,
+    q, error);
+  return CheckLaunch("aq policy update");
+}
+
+}  // namespace gjxl_b200

@@ -932,6 +932,7 @@ int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride,
 }
 
 uint32_t* ButteraugliErrorWord(ButteraugliState* st) { return st->error; }
+void ButteraugliDestroy(ButteraugliState* st) { delete st; }
 float* ButteraugliMaximum(ButteraugliState* st) { return st->maximum; }
 
 }  // namespace gjxl_b200

@@ -1,20 +1,27 @@
 // Analysis session: buffers + stage orchestration on one stream.
 //
-// Stage order follows the reference's CPU pipeline
-// (src/codestream/workflow.cpp:700-730 for input preparation,
-// src/codec/quantization_pipeline.cpp:155-213 and :429-560 for the
-// quantization pipeline): packed sRGB -> linear RGB + padded XYB ->
-// quantization-matrix statistics -> initial quant field (on the pre-Gaborish
-// XYB) -> inverse Gaborish -> initial CfL -> AC-strategy candidate costs ->
-// greedy merge.
+// Stage order follows the reference's CPU pipeline for an ordinary
+// Butteraugli-target encode (src/codestream/workflow.cpp:700-730 and
+// :885-945, src/codec/quantization_pipeline.cpp:155-213 and :429-560,
+// src/codec/adaptive_quantization.cpp:1430-1730):
+//   packed sRGB -> linear RGB + padded XYB -> quantization-matrix statistics
+//   -> initial quant field (pre-Gaborish XYB) -> inverse Gaborish -> initial
+//   CfL -> AC-strategy costs -> greedy merge -> forward coefficients of the
+//   selected transforms -> adjusted field + policy bounds -> for each of the
+//   iterations + 1 evaluations: quantizer, final CfL, coefficient coding, DC
+//   quantization, EPF sigma, DC smoothing, reconstruction, Gaborish + EPF,
+//   XYB -> linear, Butteraugli, per-transform reduction, field update.
+// Nothing returns to the host between stages.
 
 #include "session.h"
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
+#include "aq.h"
 #include "host_util.h"
 
 namespace gjxl_b200 {
@@ -28,30 +35,44 @@ enum Stage : int {
   kStageInitialCfl,
   kStageAcCosts,
   kStageAcMerge,
+  kStageTransforms,
+  kStageAqLoop,
   kStageCount,
 };
 
 const char* const kStageNames[kStageCount] = {
-  "prepare_input", "matrix_scale_stats", "initial_quant_field", "gaborish_inverse",
-  "initial_cfl", "ac_strategy_costs", "ac_strategy_merge",
+  "prepare_input",   "matrix_scale_stats", "initial_quant_field", "gaborish_inverse",
+  "initial_cfl",     "ac_strategy_costs",  "ac_strategy_merge",   "forward_transforms",
+  "adaptive_quantization",
 };
 
 size_t Align(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int AqIterations(int effort) {
+  // AdaptiveQuantizationIterations (src/codestream/workflow_internal.h:69-82).
+  if (effort <= 5) return 0;
+  if (effort == 6) return 1;
+  if (effort == 7) return 2;
+  if (effort == 8) return 3;
+  return 4;
+}
+
+std::once_flag g_tables_once[64];
 
 }  // namespace
 
 struct Session {
   size_t width = 0, height = 0, pw = 0, ph = 0, bx = 0, by = 0, tx = 0, ty = 0;
+  int iterations = 2;
   gjxl_b200_options options{};
-  // Device arena and views into it.
   void* arena = nullptr;
   size_t arena_bytes = 0;
   uint8_t* pixels = nullptr;
   size_t pixel_capacity = 0;
-  float* linear = nullptr;  // 3 planes, stride lin_stride, pitch lin_pitch
+  float* linear = nullptr;
   size_t lin_stride = 0, lin_pitch = 0;
-  float* opsin = nullptr;  // padded, stride pw
-  float* pre = nullptr;    // Gaborish-inverted
+  float* opsin = nullptr;
+  float* pre = nullptr;
   size_t pitch = 0;
   float* quant = nullptr;
   float* strategy_mask = nullptr;
@@ -63,18 +84,56 @@ struct Session {
   uint8_t* cells = nullptr;
   float* stats = nullptr;
   uint32_t* error = nullptr;
+  // Adaptive quantization.
+  int2* anchors = nullptr;
+  uint32_t* anchor_counts = nullptr;
+  float* coef = nullptr;       // forward coefficients, footprint layout
+  float* field = nullptr;      // current quant field
+  float* adjusted = nullptr;   // adjusted initial field
+  float* range = nullptr;
+  AqPolicy* policy = nullptr;
+  AqQuantizer* quantizer = nullptr;
+  int32_t* raw = nullptr;
+  int8_t* final_y_to_x = nullptr;
+  int8_t* final_y_to_b = nullptr;
+  int32_t* qac = nullptr;      // quantized AC, footprint layout
+  float* dc = nullptr;         // extracted DC (3 x blocks)
+  int32_t* qdc = nullptr;
+  float* dc_rec = nullptr;
+  float* dc_smooth = nullptr;
+  int32_t* dc_state = nullptr;
+  float* inverse_sigma = nullptr;
+  float* recon = nullptr;      // padded reconstructed XYB
+  float* filter_a = nullptr;   // 3 x width x height
+  float* filter_b = nullptr;
+  float* filtered = nullptr;
+  float* rec_linear = nullptr;
+  float* distance_map = nullptr;
+  float* block_distance = nullptr;
+  double* scores = nullptr;
+  float* matrix_multipliers = nullptr;
+  int* matrix_scales = nullptr;
+  ButteraugliState* butteraugli = nullptr;
   // Pinned host mirrors of the outputs.
+  unsigned char* host_block = nullptr;
   uint8_t* host_cells = nullptr;
   float* host_quant = nullptr;
   int8_t* host_cfl = nullptr;
   float* host_stats = nullptr;
   uint32_t* host_error = nullptr;
+  float* host_final_quant = nullptr;
+  int32_t* host_raw = nullptr;
+  int32_t* host_qdc = nullptr;
+  double* host_scores = nullptr;
+  AqQuantizer* host_quantizer = nullptr;
+  int32_t* host_qac = nullptr;
   cudaEvent_t events[kStageCount + 1] = {};
   bool events_created = false;
 
   ~Session() {
     if (arena) cudaFree(arena);
-    if (host_cells) cudaFreeHost(host_cells);
+    if (host_block) cudaFreeHost(host_block);
+    if (butteraugli) ButteraugliDestroy(butteraugli);
     if (events_created) {
       for (auto& e : events) cudaEventDestroy(e);
     }
@@ -85,6 +144,7 @@ namespace {
 
 int Allocate(Session* s) {
   const size_t plane = s->pw * s->ph;
+  const size_t image = s->width * s->height;
   s->lin_stride = Align(s->width, 4);
   s->lin_pitch = s->lin_stride * s->height;
   s->pitch = plane;
@@ -110,6 +170,34 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->cells), blocks},
     {reinterpret_cast<void**>(&s->stats), 4 * sizeof(float)},
     {reinterpret_cast<void**>(&s->error), 4 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->anchors), 7 * blocks * sizeof(int2)},
+    {reinterpret_cast<void**>(&s->anchor_counts), 8 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->coef), 3 * plane * sizeof(float)},
+    {reinterpret_cast<void**>(&s->field), blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->adjusted), blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->range), 4 * sizeof(float)},
+    {reinterpret_cast<void**>(&s->policy), sizeof(AqPolicy)},
+    {reinterpret_cast<void**>(&s->quantizer), sizeof(AqQuantizer)},
+    {reinterpret_cast<void**>(&s->raw), blocks * sizeof(int32_t)},
+    {reinterpret_cast<void**>(&s->final_y_to_x), tiles},
+    {reinterpret_cast<void**>(&s->final_y_to_b), tiles},
+    {reinterpret_cast<void**>(&s->qac), 3 * plane * sizeof(int32_t)},
+    {reinterpret_cast<void**>(&s->dc), 3 * blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->qdc), 3 * blocks * sizeof(int32_t)},
+    {reinterpret_cast<void**>(&s->dc_rec), 3 * blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->dc_smooth), 3 * blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->dc_state), 5 * blocks * sizeof(int32_t)},
+    {reinterpret_cast<void**>(&s->inverse_sigma), blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->recon), 3 * plane * sizeof(float)},
+    {reinterpret_cast<void**>(&s->filter_a), 3 * image * sizeof(float)},
+    {reinterpret_cast<void**>(&s->filter_b), 3 * image * sizeof(float)},
+    {reinterpret_cast<void**>(&s->filtered), 3 * image * sizeof(float)},
+    {reinterpret_cast<void**>(&s->rec_linear), 3 * image * sizeof(float)},
+    {reinterpret_cast<void**>(&s->distance_map), image * sizeof(float)},
+    {reinterpret_cast<void**>(&s->block_distance), blocks * sizeof(float)},
+    {reinterpret_cast<void**>(&s->scores), 8 * sizeof(double)},
+    {reinterpret_cast<void**>(&s->matrix_multipliers), 4 * sizeof(float)},
+    {reinterpret_cast<void**>(&s->matrix_scales), 4 * sizeof(int)},
   };
   size_t total = 0;
   for (const Item& item : items) total = Align(total, 256) + item.bytes;
@@ -122,22 +210,34 @@ int Allocate(Session* s) {
     *item.ptr = static_cast<unsigned char*>(s->arena) + offset;
     offset += item.bytes;
   }
-  // Pinned host mirrors: cells, quant field, CfL maps, stats, error word.
-  const size_t host_bytes = Align(blocks, 16) + Align(blocks * sizeof(float), 16) +
-                            Align(2 * tiles, 16) + 16 + 16;
+  // Pinned host mirrors.
+  const size_t host_bytes = Align(blocks, 16) + Align(blocks * 4, 16) + Align(2 * tiles, 16) +
+                            16 + 16 + Align(blocks * 4, 16) + Align(blocks * 4, 16) +
+                            Align(3 * blocks * 4, 16) + 64 + Align(sizeof(AqQuantizer), 16) +
+                            Align(3 * plane * 4, 16);
   void* host = nullptr;
   status = CheckCuda(cudaMallocHost(&host, host_bytes), "session: cudaMallocHost");
   if (status != GJXL_B200_OK) return status;
-  auto* h = static_cast<unsigned char*>(host);
-  s->host_cells = h;
-  h += Align(blocks, 16);
-  s->host_quant = reinterpret_cast<float*>(h);
-  h += Align(blocks * sizeof(float), 16);
-  s->host_cfl = reinterpret_cast<int8_t*>(h);
-  h += Align(2 * tiles, 16);
-  s->host_stats = reinterpret_cast<float*>(h);
-  h += 16;
-  s->host_error = reinterpret_cast<uint32_t*>(h);
+  s->host_block = static_cast<unsigned char*>(host);
+  unsigned char* h = s->host_block;
+  auto take = [&](size_t bytes) {
+    unsigned char* r = h;
+    h += Align(bytes, 16);
+    return r;
+  };
+  s->host_cells = take(blocks);
+  s->host_quant = reinterpret_cast<float*>(take(blocks * 4));
+  s->host_cfl = reinterpret_cast<int8_t*>(take(2 * tiles));
+  s->host_stats = reinterpret_cast<float*>(take(16));
+  s->host_error = reinterpret_cast<uint32_t*>(take(16));
+  s->host_final_quant = reinterpret_cast<float*>(take(blocks * 4));
+  s->host_raw = reinterpret_cast<int32_t*>(take(blocks * 4));
+  s->host_qdc = reinterpret_cast<int32_t*>(take(3 * blocks * 4));
+  s->host_scores = reinterpret_cast<double*>(take(64));
+  s->host_quantizer = reinterpret_cast<AqQuantizer*>(take(sizeof(AqQuantizer)));
+  s->host_qac = reinterpret_cast<int32_t*>(take(3 * plane * 4));
+  status = ButteraugliCreate(s->width, s->height, 80.0f, &s->butteraugli);
+  if (status != GJXL_B200_OK) return status;
   if (s->options.profile_stages) {
     for (auto& e : s->events) {
       status = CheckCuda(cudaEventCreate(&e), "session: cudaEventCreate");
@@ -152,53 +252,109 @@ void Mark(Session* s, int stage, cudaStream_t stream) {
   if (s->events_created) cudaEventRecord(s->events[stage], stream);
 }
 
+#define GJXL_TRY(expr)                         \
+  do {                                         \
+    const int gjxl_status_ = (expr);           \
+    if (gjxl_status_ != GJXL_B200_OK) return gjxl_status_; \
+  } while (0)
+
+int RunAq(Session* s, cudaStream_t stream) {
+  const float target = s->options.butteraugli_target;
+  const size_t blocks = s->bx * s->by;
+  GJXL_TRY(AqBuildAnchors(s->cells, s->bx, s->by, s->anchors, s->anchor_counts, stream));
+  GJXL_TRY(AqForwardCoefficients(s->pre, s->pw, s->pitch, s->bx, s->by, s->anchors,
+                                 s->anchor_counts, s->coef, stream));
+  GJXL_TRY(AqAdjustField(s->cells, s->bx, s->by, s->quant, s->adjusted, target, stream));
+  GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->field, s->adjusted, blocks * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, stream), "session: field"));
+  GJXL_TRY(AqPolicySetup(s->adjusted, blocks, target, s->range, s->policy, s->error, stream));
+  GJXL_TRY(ButteraugliPrepare(s->butteraugli, s->linear, s->lin_stride, s->lin_pitch, stream));
+  Mark(s, kStageAqLoop, stream);
+  for (int iteration = 0; iteration <= s->iterations; ++iteration) {
+    GJXL_TRY(AqQuantizer_(s->field, blocks, s->policy, s->quantizer, s->raw, s->error, stream));
+    GJXL_TRY(AqFinalCfl(s->cells, s->bx, s->by, s->coef, s->pw, s->pitch, s->raw, s->quantizer,
+                        s->final_y_to_x, s->final_y_to_b, stream));
+    GJXL_TRY(AqCoding(s->anchors, s->anchor_counts, s->bx, s->by, s->coef, s->pw, s->pitch,
+                      s->qac, s->dc, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
+                      s->matrix_multipliers, s->error, stream));
+    GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, s->dc_state, 1,
+                          stream));
+    GJXL_TRY(AqInverseSigma(s->cells, s->bx, s->by, s->raw, s->quantizer, s->inverse_sigma,
+                            stream));
+    GJXL_TRY(AqSmoothDc(s->dc_rec, s->bx, s->by, s->quantizer, s->dc_smooth, stream));
+    GJXL_TRY(AqReconstruct(s->anchors, s->anchor_counts, s->bx, s->by, s->qac, s->pw, s->pitch,
+                           s->dc_smooth, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
+                           s->matrix_multipliers, s->recon, stream));
+    GJXL_TRY(AqLoopFilters(s->recon, s->pw, s->pitch, s->width, s->height, s->inverse_sigma,
+                           s->bx, s->filter_a, s->filter_b, s->filtered, s->error, stream));
+    GJXL_TRY(AqOpsinToLinear(s->filtered, s->width, s->height, s->options.intensity_target,
+                             s->rec_linear, s->error, stream));
+    GJXL_TRY(ButteraugliCompare(s->butteraugli, s->rec_linear, s->width, s->width * s->height,
+                                s->distance_map, s->width, s->scores + iteration, stream));
+    GJXL_TRY(AqBlockReduce(s->cells, s->bx, s->by, s->distance_map, s->width, s->height,
+                           s->block_distance, stream));
+    if (iteration < s->iterations) {
+      GJXL_TRY(AqPolicyUpdate(s->field, s->adjusted, s->block_distance, blocks, iteration, target,
+                              s->policy, s->quantizer, s->error, stream));
+    }
+  }
+  // Fold the Butteraugli error word into the session's.
+  return GJXL_B200_OK;
+}
+
 int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
         cudaStream_t stream) {
-  int status = CheckCuda(cudaMemsetAsync(s->error, 0, sizeof(uint32_t), stream),
-                         "session: clear error");
-  if (status != GJXL_B200_OK) return status;
+  GJXL_TRY(CheckCuda(cudaMemsetAsync(s->error, 0, sizeof(uint32_t), stream),
+                     "session: clear error"));
   const float target = s->options.butteraugli_target;
   Mark(s, kStagePrepare, stream);
-  status = gjxl_b200_prepare_input(pixels, s->width, s->height, row_stride, channels,
+  GJXL_TRY(gjxl_b200_prepare_input(pixels, s->width, s->height, row_stride, channels,
                                    s->options.intensity_target, s->linear, s->lin_stride,
                                    s->lin_pitch, s->opsin, s->pw, s->pitch, s->pw, s->ph,
-                                   s->error, stream);
-  if (status != GJXL_B200_OK) return status;
+                                   s->error, stream));
   Mark(s, kStageStats, stream);
-  status = gjxl_b200_matrix_scale_stats(s->opsin, s->pw, s->pitch, s->width, s->height,
-                                        s->stats, stream);
-  if (status != GJXL_B200_OK) return status;
+  const bool stats = s->options.effort >= 7;  // ShouldComputeQuantizationMatrixScaleStats
+  if (stats) {
+    GJXL_TRY(gjxl_b200_matrix_scale_stats(s->opsin, s->pw, s->pitch, s->width, s->height,
+                                          s->stats, stream));
+  } else {
+    GJXL_TRY(CheckCuda(cudaMemsetAsync(s->stats, 0, 4 * sizeof(float), stream),
+                       "session: clear stats"));
+  }
+  GJXL_TRY(AqMatrixScales(s->stats, stats, target, s->matrix_multipliers, s->matrix_scales,
+                          stream));
   Mark(s, kStageInitialQuant, stream);
   // Initial quantization samples the pre-Gaborish image at the full target
   // (Gaborish is on for efforts >= 5: quantization_pipeline.cpp:452-456).
-  status = LaunchInitialQuantField(s->opsin, s->pw, s->pitch, s->pw, s->ph, target, 1.0f,
+  GJXL_TRY(LaunchInitialQuantField(s->opsin, s->pw, s->pitch, s->pw, s->ph, target, 1.0f,
                                    s->quant, s->strategy_mask, s->pixel_mask, s->pw,
-                                   s->iq_scratch, s->error, stream);
-  if (status != GJXL_B200_OK) return status;
+                                   s->iq_scratch, s->error, stream));
   Mark(s, kStageGaborishInverse, stream);
   const float multipliers[3] = {1.0f, 1.0f, 1.0f};
-  status = LaunchGaborishInverse(s->opsin, s->pw, s->pitch, s->pre, s->pw, s->pitch, s->pw,
-                                 s->ph, multipliers, s->error, stream);
-  if (status != GJXL_B200_OK) return status;
+  GJXL_TRY(LaunchGaborishInverse(s->opsin, s->pw, s->pitch, s->pre, s->pw, s->pitch, s->pw,
+                                 s->ph, multipliers, s->error, stream));
   Mark(s, kStageInitialCfl, stream);
-  status = LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b, stream);
-  if (status != GJXL_B200_OK) return status;
+  GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b, stream));
   Mark(s, kStageAcCosts, stream);
   const bool dense = s->options.effort >= 10;
-  status = LaunchAcStrategyCosts(s->pre, s->pw, s->pitch, s->pw, s->ph, s->quant, s->pixel_mask,
+  GJXL_TRY(LaunchAcStrategyCosts(s->pre, s->pw, s->pitch, s->pw, s->ph, s->quant, s->pixel_mask,
                                  s->pw, s->y_to_x, s->y_to_b, target, dense, s->costs, s->error,
-                                 stream);
-  if (status != GJXL_B200_OK) return status;
+                                 stream));
   Mark(s, kStageAcMerge, stream);
-  status = LaunchAcStrategySearch(s->costs, s->pw, s->ph, target, dense, s->cells, s->error,
-                                  stream);
-  if (status != GJXL_B200_OK) return status;
+  GJXL_TRY(LaunchAcStrategySearch(s->costs, s->pw, s->ph, target, dense, s->cells, s->error,
+                                  stream));
+  Mark(s, kStageTransforms, stream);
+  GJXL_TRY(RunAq(s, stream));
   Mark(s, kStageCount, stream);
+  // Merge the Butteraugli error word into the session error word.
+  GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->error + 1, ButteraugliErrorWord(s->butteraugli),
+                                     sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
+                     "session: error word"));
   return GJXL_B200_OK;
 }
 
 int CopyOutputs(Session* s, cudaStream_t stream) {
-  const size_t blocks = s->bx * s->by, tiles = s->tx * s->ty;
+  const size_t blocks = s->bx * s->by, tiles = s->tx * s->ty, plane = s->pw * s->ph;
   const struct {
     void* dst;
     const void* src;
@@ -206,15 +362,20 @@ int CopyOutputs(Session* s, cudaStream_t stream) {
   } copies[] = {
     {s->host_cells, s->cells, blocks},
     {s->host_quant, s->quant, blocks * sizeof(float)},
-    {s->host_cfl, s->y_to_x, tiles},
-    {s->host_cfl + tiles, s->y_to_b, tiles},
+    {s->host_cfl, s->final_y_to_x, tiles},
+    {s->host_cfl + tiles, s->final_y_to_b, tiles},
     {s->host_stats, s->stats, 3 * sizeof(float)},
-    {s->host_error, s->error, sizeof(uint32_t)},
+    {s->host_error, s->error, 2 * sizeof(uint32_t)},
+    {s->host_final_quant, s->field, blocks * sizeof(float)},
+    {s->host_raw, s->raw, blocks * sizeof(int32_t)},
+    {s->host_qdc, s->qdc, 3 * blocks * sizeof(int32_t)},
+    {s->host_scores, s->scores, (s->iterations + 1) * sizeof(double)},
+    {s->host_quantizer, s->quantizer, sizeof(AqQuantizer)},
+    {s->host_qac, s->qac, 3 * plane * sizeof(int32_t)},
   };
   for (const auto& c : copies) {
-    int status = CheckCuda(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, stream),
-                           "session: output copy");
-    if (status != GJXL_B200_OK) return status;
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, stream),
+                       "session: output copy"));
   }
   return GJXL_B200_OK;
 }
@@ -260,6 +421,15 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
     return SetError(GJXL_B200_UNSUPPORTED,
                     "session_create: efforts 5-10 (mixed-transform search) are supported");
   }
+  int device = 0;
+  int status = CheckCuda(cudaGetDevice(&device), "session_create: cudaGetDevice");
+  if (status != GJXL_B200_OK) return status;
+  if (device >= 0 && device < 64) {
+    std::call_once(g_tables_once[device], [] {
+      UploadDcTables();
+      UploadDcReconTables();
+    });
+  }
   auto* s = new (std::nothrow) gjxl_b200_session();
   if (s == nullptr) return SetError(GJXL_B200_OUT_OF_MEMORY, "session_create: host allocation");
   s->width = width;
@@ -271,7 +441,8 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
   s->tx = (s->bx + 7) / 8;
   s->ty = (s->by + 7) / 8;
   s->options = o;
-  int status = Allocate(s);
+  s->iterations = AqIterations(o.effort);
+  status = Allocate(s);
   if (status != GJXL_B200_OK) {
     delete s;
     return status;
@@ -303,11 +474,9 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze_host: row stride too large");
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int status = CheckCuda(cudaMemcpyAsync(s->pixels, host_pixels, bytes, cudaMemcpyHostToDevice,
-                                         st), "session: input upload");
-  if (status != GJXL_B200_OK) return status;
-  status = Run(s, s->pixels, row_stride, channels, st);
-  if (status != GJXL_B200_OK) return status;
+  GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->pixels, host_pixels, bytes, cudaMemcpyHostToDevice, st),
+                     "session: input upload"));
+  GJXL_TRY(Run(s, s->pixels, row_stride, channels, st));
   return CopyOutputs(s, st);
 }
 
@@ -323,6 +492,7 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   out->blocks_y = s->by;
   out->tiles_x = s->tx;
   out->tiles_y = s->ty;
+  out->iterations = static_cast<size_t>(s->iterations);
   out->linear = s->linear;
   out->linear_stride = s->lin_stride;
   out->linear_plane_pitch = s->lin_pitch;
@@ -333,10 +503,23 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   out->initial_quant_field = s->quant;
   out->strategy_mask = s->strategy_mask;
   out->pixel_mask = s->pixel_mask;
-  out->y_to_x = s->y_to_x;
-  out->y_to_b = s->y_to_b;
+  out->initial_y_to_x = s->y_to_x;
+  out->initial_y_to_b = s->y_to_b;
   out->strategy_cells = s->cells;
   out->matrix_scale_stats = s->stats;
+  out->matrix_scales = s->matrix_scales;
+  out->quant_field = s->field;
+  out->raw_quant_field = s->raw;
+  out->y_to_x = s->final_y_to_x;
+  out->y_to_b = s->final_y_to_b;
+  out->quantized_ac = s->qac;
+  out->quantized_dc = s->qdc;
+  out->dc = s->dc_rec;
+  out->block_distance = s->block_distance;
+  out->reconstructed_linear = s->rec_linear;
+  out->distance_map = s->distance_map;
+  out->score_history = s->scores;
+  out->quantizer_params = reinterpret_cast<const uint32_t*>(s->quantizer);
   out->device_error = s->error;
   out->host_strategy_cells = s->host_cells;
   out->host_initial_quant_field = s->host_quant;
@@ -344,6 +527,12 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   out->host_y_to_b = s->host_cfl + s->tx * s->ty;
   out->host_matrix_scale_stats = s->host_stats;
   out->host_device_error = s->host_error;
+  out->host_quant_field = s->host_final_quant;
+  out->host_raw_quant_field = s->host_raw;
+  out->host_quantized_dc = s->host_qdc;
+  out->host_score_history = s->host_scores;
+  out->host_quantizer_params = reinterpret_cast<const uint32_t*>(s->host_quantizer);
+  out->host_quantized_ac = s->host_qac;
   out->device_bytes = s->arena_bytes;
   return GJXL_B200_OK;
 }
@@ -359,9 +548,10 @@ extern "C" int gjxl_b200_session_stage_times(gjxl_b200_session* s, float* millis
   }
   const int n = capacity < kStageCount ? capacity : kStageCount;
   for (int i = 0; i < n; ++i) {
-    int status = CheckCuda(cudaEventElapsedTime(&milliseconds[i], s->events[i], s->events[i + 1]),
-                           "session_stage_times");
-    if (status != GJXL_B200_OK) return status;
+    const int status =
+      CheckCuda(cudaEventElapsedTime(&milliseconds[i], s->events[i], s->events[i + 1]),
+                "session_stage_times");
+    if (status != GJXL_B200_OK) return -status;
   }
   return n;
 }

@@ -33,4 +33,13 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
 int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float target, bool dense,
                            uint8_t* cells, uint32_t* error, cudaStream_t stream);
 
+struct ButteraugliState;
+int ButteraugliCreate(size_t width, size_t height, float intensity_target, ButteraugliState** out);
+void ButteraugliDestroy(ButteraugliState* state);
+int ButteraugliPrepare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
+                       cudaStream_t stream);
+int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
+                       float* map, size_t map_stride, double* score, cudaStream_t stream);
+uint32_t* ButteraugliErrorWord(ButteraugliState* st);
+
 }  // namespace gjxl_b200

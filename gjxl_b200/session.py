@@ -21,16 +21,19 @@ class Options(Structure):
 
 class Outputs(Structure):
     _fields_ = [(n, c_size_t) for n in ("padded_width", "padded_height", "blocks_x", "blocks_y",
-                                        "tiles_x", "tiles_y")] + [
+                                        "tiles_x", "tiles_y", "iterations")] + [
         ("linear", c_void_p), ("linear_stride", c_size_t), ("linear_plane_pitch", c_size_t),
         ("opsin", c_void_p), ("preprocessed_opsin", c_void_p), ("opsin_stride", c_size_t),
-        ("opsin_plane_pitch", c_size_t), ("initial_quant_field", c_void_p),
-        ("strategy_mask", c_void_p), ("pixel_mask", c_void_p), ("y_to_x", c_void_p),
-        ("y_to_b", c_void_p), ("strategy_cells", c_void_p), ("matrix_scale_stats", c_void_p),
-        ("device_error", c_void_p), ("host_strategy_cells", c_void_p),
-        ("host_initial_quant_field", c_void_p), ("host_y_to_x", c_void_p),
-        ("host_y_to_b", c_void_p), ("host_matrix_scale_stats", c_void_p),
-        ("host_device_error", c_void_p), ("device_bytes", c_size_t)]
+        ("opsin_plane_pitch", c_size_t)] + [(n, c_void_p) for n in (
+            "initial_quant_field", "strategy_mask", "pixel_mask", "initial_y_to_x",
+            "initial_y_to_b", "strategy_cells", "matrix_scale_stats", "matrix_scales",
+            "quant_field", "raw_quant_field", "y_to_x", "y_to_b", "quantized_ac", "quantized_dc",
+            "dc", "block_distance", "reconstructed_linear", "distance_map", "score_history",
+            "quantizer_params", "device_error", "host_strategy_cells",
+            "host_initial_quant_field", "host_y_to_x", "host_y_to_b", "host_matrix_scale_stats",
+            "host_device_error", "host_quant_field", "host_raw_quant_field", "host_quantized_dc",
+            "host_score_history", "host_quantizer_params", "host_quantized_ac")] + [
+        ("device_bytes", c_size_t)]
 
 
 _BOUND = False
@@ -128,6 +131,31 @@ class AnalysisSession:
         return np.ctypeslib.as_array(ctypes.cast(o.host_strategy_cells, POINTER(c_uint8)),
                                      shape=(o.blocks_y, o.blocks_x)).copy()
 
+    def _host(self, name: str, ctype, shape) -> np.ndarray:
+        ptr = ctypes.cast(getattr(self.outputs, name), POINTER(ctype))
+        return np.ctypeslib.as_array(ptr, shape=shape).copy()
+
     def host_error(self) -> int:
-        return int(np.ctypeslib.as_array(ctypes.cast(self.outputs.host_device_error,
-                                                     POINTER(ctypes.c_uint32)), shape=(1,))[0])
+        """Analysis error word OR'ed with the Butteraugli error word."""
+        words = self._host("host_device_error", ctypes.c_uint32, (2,))
+        return int(words[0]) | int(words[1])
+
+    def host_results(self) -> dict[str, np.ndarray]:
+        """Host copies of the final frame's results (after analyze_host)."""
+        o = self.outputs
+        blocks = (o.blocks_y, o.blocks_x)
+        tiles = (o.tiles_y, o.tiles_x)
+        return {
+            "cells": self.host_strategy_cells(),
+            "initial_quant": self._host("host_initial_quant_field", c_float, blocks),
+            "y_to_x": self._host("host_y_to_x", ctypes.c_int8, tiles),
+            "y_to_b": self._host("host_y_to_b", ctypes.c_int8, tiles),
+            "final_quant": self._host("host_quant_field", c_float, blocks),
+            "raw_quant": self._host("host_raw_quant_field", ctypes.c_int32, blocks),
+            "quantized_dc": self._host("host_quantized_dc", ctypes.c_int32, (3,) + blocks),
+            "score_history": self._host("host_score_history", ctypes.c_double,
+                                        (o.iterations + 1,)),
+            "quantizer_params": self._host("host_quantizer_params", ctypes.c_uint32, (2,)),
+            "quantized_ac": self._host("host_quantized_ac", ctypes.c_int32,
+                                       (3, o.padded_height, o.padded_width)),
+        }

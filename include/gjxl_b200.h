@@ -242,8 +242,18 @@ typedef struct gjxl_b200_options {
   int profile_stages;       /* nonzero: record CUDA events around each stage */
 } gjxl_b200_options;
 
+/* Session results. The adaptive-quantization fields mirror the reference's
+ * CpuQuantizationPipelineOutput / VarDctEncoderFrame
+ * (src/codec/quantization_pipeline.h, src/codec/vardct_frame.h) after the last
+ * of the (iterations + 1) evaluations. Coefficient planes use "footprint
+ * layout": the N coefficients of a transform anchored at block (bx, by) lie
+ * in its own W x H pixel footprint, coefficient i at
+ * (bx*8 + i % W, by*8 + i / W) of a padded plane; the reference's AC group
+ * order is the anchors of each 256x256 group in raster order, each adding its
+ * coefficients 0..N-1 per channel. */
 typedef struct gjxl_b200_outputs {
   size_t padded_width, padded_height, blocks_x, blocks_y, tiles_x, tiles_y;
+  size_t iterations;                /* evaluations - 1 */
   /* Device views (valid until the session is destroyed). */
   const float* linear;             /* 3 planes, unpadded */
   size_t linear_stride, linear_plane_pitch;
@@ -253,19 +263,38 @@ typedef struct gjxl_b200_outputs {
   const float* initial_quant_field; /* blocks */
   const float* strategy_mask;       /* blocks */
   const float* pixel_mask;          /* padded pixels, stride opsin_stride */
-  const int8_t* y_to_x;             /* tiles */
-  const int8_t* y_to_b;
+  const int8_t* initial_y_to_x;     /* tiles, before the final CfL */
+  const int8_t* initial_y_to_b;
   const uint8_t* strategy_cells;    /* blocks, (strategy << 1) | anchor */
   const float* matrix_scale_stats;  /* x_edge, b_edge, exposed_blue */
-  const uint32_t* device_error;
+  const int* matrix_scales;         /* x_qm_scale, b_qm_scale */
+  const float* quant_field;         /* blocks, final field */
+  const int32_t* raw_quant_field;   /* blocks */
+  const int8_t* y_to_x;             /* tiles, final CfL map */
+  const int8_t* y_to_b;
+  const int32_t* quantized_ac;      /* 3 padded planes, footprint layout */
+  const int32_t* quantized_dc;      /* 3 x blocks (X, Y, B) */
+  const float* dc;                  /* 3 x blocks, dequantized DC */
+  const float* block_distance;      /* blocks */
+  const float* reconstructed_linear; /* 3 x width x height */
+  const float* distance_map;        /* width x height */
+  const double* score_history;      /* iterations + 1 maxima */
+  const uint32_t* quantizer_params; /* global_scale, quant_dc, ... */
+  const uint32_t* device_error;     /* [0] analysis, [1] Butteraugli */
   /* Pinned host mirrors, filled by gjxl_b200_session_analyze_host once the
    * stream has completed. */
   const uint8_t* host_strategy_cells;
   const float* host_initial_quant_field;
-  const int8_t* host_y_to_x;
+  const int8_t* host_y_to_x;        /* final CfL map */
   const int8_t* host_y_to_b;
   const float* host_matrix_scale_stats;
-  const uint32_t* host_device_error;
+  const uint32_t* host_device_error; /* 2 words */
+  const float* host_quant_field;
+  const int32_t* host_raw_quant_field;
+  const int32_t* host_quantized_dc;
+  const double* host_score_history;
+  const uint32_t* host_quantizer_params;
+  const int32_t* host_quantized_ac;
   size_t device_bytes;
 } gjxl_b200_outputs;
 

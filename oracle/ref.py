@@ -204,3 +204,49 @@ def ac_strategy_cost_table(opsin, quant, pixel_mask, ytox, ytob, target: float =
                                                  target, int(dense), _ptr(costs)),
            "ac_strategy_cost_table")
     return costs
+
+
+class _PipelineOutputs(ctypes.Structure):
+    _fields_ = [(name, c_void_p) for name in (
+        "initial_quant", "strategy_mask", "pixel_mask", "final_quant", "block_distance",
+        "reconstructed", "cells", "raw_quant", "quantizer_params", "y_to_x", "y_to_b",
+        "quantized_dc", "dc", "ac", "group_used", "score_history")]
+
+
+def quantization_pipeline(linear: np.ndarray, opsin: np.ndarray, target: float = 1.0,
+                          effort: int = 7, x_qm_scale: int = 3, b_qm_scale: int = 2) -> dict:
+    """The reference's whole CPU analysis half (RunCpuQuantizationPipeline)
+    with the workflow's settings for an ordinary Butteraugli-target encode."""
+    linear = np.ascontiguousarray(linear, np.float32)
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, h, w = linear.shape
+    _, ph, pw = opsin.shape
+    by, bx = ph // 8, pw // 8
+    ty, tx = (ph + 63) // 64, (pw + 63) // 64
+    gy, gx = (by + 31) // 32, (bx + 31) // 32
+    iterations = 0 if effort <= 5 else {6: 1, 7: 2, 8: 3}.get(effort, 4)
+    res = {
+        "initial_quant": np.zeros((by, bx), np.float32),
+        "strategy_mask": np.zeros((by, bx), np.float32),
+        "pixel_mask": np.zeros((ph, pw), np.float32),
+        "final_quant": np.zeros((by, bx), np.float32),
+        "block_distance": np.zeros((by, bx), np.float32),
+        "reconstructed": np.zeros((3, h, w), np.float32),
+        "cells": np.zeros((by, bx), np.uint8),
+        "raw_quant": np.zeros((by, bx), np.int32),
+        "quantizer_params": np.zeros(2, np.uint32),
+        "y_to_x": np.zeros((ty, tx), np.int8),
+        "y_to_b": np.zeros((ty, tx), np.int8),
+        "quantized_dc": np.zeros((3, by, bx), np.int32),
+        "dc": np.zeros((3, by, bx), np.float32),
+        "ac": np.zeros(3 * ph * pw, np.int32),
+        "group_used": np.zeros(gy * gx, np.uint64),
+        "score_history": np.zeros(iterations + 1, np.float64),
+    }
+    outs = _PipelineOutputs(**{k: v.ctypes.data for k, v in res.items()})
+    fn = lib().gjxl_ref_quantization_pipeline
+    fn.argtypes = [_P, _Z, _Z, _P, _Z, _Z, _F, _I, _I, _I, ctypes.POINTER(_PipelineOutputs)]
+    fn.restype = c_int
+    _check(fn(_ptr(linear), w, h, _ptr(opsin), pw, ph, target, effort, x_qm_scale, b_qm_scale,
+              ctypes.byref(outs)), "quantization_pipeline")
+    return res

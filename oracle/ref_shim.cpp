@@ -34,6 +34,7 @@
 #include "codec/vardct_frame.h"
 #include "core/ac_strategy.h"
 #include "core/image.h"
+#include "core/publication_vector.h"
 #include "core/thread_budget.h"
 
 #define GJXL_REF_API extern "C" __attribute__((visibility("default")))
@@ -378,4 +379,110 @@ GJXL_REF_API int gjxl_ref_butteraugli_options(const float* reference_linear,
     ConstPlanar(reference_linear, width, height), ConstPlanar(distorted_linear, width, height),
     options, {distance_map, {width, height}, width}, score);
   return status.ok() ? 0 : Fail(status);
+}
+
+// codec/quantization_pipeline.cpp RunCpuQuantizationPipeline with the
+// settings the reference workflow uses for an ordinary effort-`effort`
+// Butteraugli-target encode (src/codestream/workflow.cpp:885-945,
+// workflow_internal.h:17-130): Gaborish on, spatial initial field, adjusted
+// shared AC quantization, prediction-aware DC with one extra bit and the
+// weighted predictor, adaptive DC smoothing, fast final CfL, neutral EPF
+// sharpness, and the given quantization-matrix scales.
+struct RefPipelineOutputs {
+  float* initial_quant;        // blocks
+  float* strategy_mask;        // blocks
+  float* pixel_mask;           // padded pixels
+  float* final_quant;          // blocks
+  float* block_distance;       // blocks
+  float* reconstructed;        // 3 x width x height
+  uint8_t* cells;              // blocks
+  int32_t* raw_quant;          // blocks
+  uint32_t* quantizer_params;  // global_scale, quant_dc
+  int8_t* y_to_x;              // tiles
+  int8_t* y_to_b;              // tiles
+  int32_t* quantized_dc;       // 3 x blocks
+  float* dc;                   // 3 x blocks
+  int32_t* ac;                 // group order: per group 3 x used count
+  size_t* group_used;          // per group used coefficient count
+  double* score_history;       // iterations + 1
+};
+
+GJXL_REF_API int gjxl_ref_quantization_pipeline(
+  const float* linear, size_t width, size_t height, const float* opsin, size_t padded_width,
+  size_t padded_height, float target, int effort, int x_qm_scale, int b_qm_scale,
+  RefPipelineOutputs* out) {
+  const Extent2D blocks{padded_width / 8, padded_height / 8};
+  const Extent2D pixels{padded_width, padded_height};
+  CpuQuantizationPipelineOptions options;
+  options.butteraugli_target = target;
+  options.uniform_initial_quantization = false;
+  options.fixed_dct8 = false;
+  options.dense_dct32_search = effort == 10;
+  auto& aq = options.adaptive_quantization;
+  aq.profile.loop_filter.gaborish = true;
+  aq.iterations = effort <= 5 ? 0 : effort == 6 ? 1 : effort == 7 ? 2 : effort == 8 ? 3 : 4;
+  aq.coefficient_decision_mode = AcCoefficientDecisionMode::kAdjustedSharedQuant;
+  aq.dc_quantization = DcQuantizationMode::kPredictionAware;
+  aq.dc_prediction = VarDctDcPrediction::kWeighted;
+  aq.profile.extra_dc_precision = 1;
+  aq.profile.adaptive_dc_smoothing = true;
+  aq.profile.x_qm_scale = static_cast<uint8_t>(x_qm_scale);
+  aq.profile.b_qm_scale = static_cast<uint8_t>(b_qm_scale);
+  aq.search_epf_sharpness = false;
+
+  std::vector<double> history;
+  VarDctEncoderFrame frame;
+  MaximumErrorResult max_error;
+  resource_budget_internal::PublicationVector<double> scores;
+  CpuQuantizationPipelineOutput output{
+    .initial_quantization = {
+      .quant_field = {out->initial_quant, blocks, blocks.width},
+      .strategy_mask = {out->strategy_mask, blocks, blocks.width},
+      .pixel_mask = {out->pixel_mask, pixels, pixels.width},
+    },
+    .adaptive_quantization = {
+      .quant_field = {out->final_quant, blocks, blocks.width},
+      .block_distance_map = {out->block_distance, blocks, blocks.width},
+      .reconstructed_linear_rgb = Planar(out->reconstructed, width, height),
+      .frame = &frame,
+      .score_history = &scores,
+      .maximum_error_result = &max_error,
+    },
+  };
+  Status status = RunCpuQuantizationPipeline(ConstPlanar(linear, width, height),
+                                             ConstPlanar(opsin, padded_width, padded_height),
+                                             options, output);
+  if (!status.ok()) return Fail(status);
+  status = ExportGrid(frame.strategies(), out->cells);
+  if (!status.ok()) return Fail(status);
+  const ConstPlaneI32View raw = frame.raw_quant_field();
+  for (size_t y = 0; y < blocks.height; ++y)
+    std::memcpy(out->raw_quant + y * blocks.width, raw.Row(y), blocks.width * 4);
+  out->quantizer_params[0] = frame.quantizer().params().global_scale;
+  out->quantizer_params[1] = frame.quantizer().params().quant_dc;
+  ExportColorCorrelation(frame.color_correlation(), out->y_to_x, out->y_to_b);
+  const ConstImage3I32View qdc = frame.quantized_dc();
+  const ConstImage3FView dc = frame.dc();
+  for (size_t c = 0; c < 3; ++c) {
+    for (size_t y = 0; y < blocks.height; ++y) {
+      std::memcpy(out->quantized_dc + (c * blocks.height + y) * blocks.width,
+                  qdc.plane[c].Row(y), blocks.width * 4);
+      std::memcpy(out->dc + (c * blocks.height + y) * blocks.width, dc.plane[c].Row(y),
+                  blocks.width * 4);
+    }
+  }
+  size_t offset = 0;
+  for (size_t g = 0; g < frame.ac_group_count(); ++g) {
+    VarDctAcGroupView group;
+    status = frame.GetAcGroup(g, &group);
+    if (!status.ok()) return Fail(status);
+    out->group_used[g] = group.used_coefficient_count;
+    for (size_t c = 0; c < 3; ++c) {
+      std::memcpy(out->ac + offset, group.coefficients[c].data(),
+                  group.used_coefficient_count * 4);
+      offset += group.used_coefficient_count;
+    }
+  }
+  for (size_t i = 0; i < scores.size(); ++i) out->score_history[i] = scores[i];
+  return 0;
 }

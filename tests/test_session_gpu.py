@@ -1,6 +1,22 @@
 """The analysis session (the C-ABI entry point a caller uses) against the
-reference, through the host-input path: strategy grid, initial quant field
-and CfL maps of a whole image."""
+reference, through the host-input path: the front half (strategy grid,
+initial quant field, matrix statistics) and the adaptive-quantization
+evaluation loop (final quant field, quantizer, CfL maps, quantized DC and AC,
+Butteraugli score history, block distances, reconstruction) of whole images.
+
+The reference side is RunCpuQuantizationPipeline with the workflow's settings
+for an ordinary Butteraugli-target encode
+(src/codec/quantization_pipeline.cpp:429-560,
+src/codestream/workflow.cpp:885-945).
+
+A single evaluation (effort 5) is compared bit for bit. The one stated
+exception is the block distance: the reference takes mean^(1/16) with glibc
+powf, which is off by 1 ulp on a small fraction of inputs, while the device
+computes the correctly rounded power; check_block_distance proves that every
+difference is such a case. With field updates (efforts 6-10) a block distance
+feeds the next field, so such a case can move single field values by an ulp:
+there the quantizer must match exactly and at most 0.1% of blocks may differ,
+and runs where nothing differs are then held to the bit-exact comparison."""
 
 import ctypes
 
@@ -10,40 +26,210 @@ import torch
 
 from gjxl_b200.session import AnalysisSession
 from gjxl_b200.synthetic import generate_srgb8
+from gpu_util import (STRATEGY_COVERED, assert_bitexact, device_to_host, differing_blocks,
+                      footprint_to_group_order, group_order_to_footprint)
 from oracle import ref, restate
 
 pytestmark = pytest.mark.gpu
 
 
-def host_array(ptr, shape, ctype, dtype):
-    return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctype)), shape=shape).copy()
-
-
-@pytest.mark.parametrize("w,h", [(509, 261), (1000, 700)])
-def test_session_matches_reference(cuda, w, h):
-    img = generate_srgb8(w, h, 4000 + w)
-    s = AnalysisSession(w, h)
+def run_session(img: np.ndarray, effort: int = 7, target: float = 1.0) -> AnalysisSession:
+    h, w, _ = img.shape
+    s = AnalysisSession(w, h, butteraugli_target=target, effort=effort)
     s.analyze_host(img, torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
-    o = s.outputs
-    assert s.host_error() == 0
-    cells = s.host_strategy_cells()
-    quant = host_array(o.host_initial_quant_field, (o.blocks_y, o.blocks_x), ctypes.c_float,
-                       np.float32)
-    ytox = host_array(o.host_y_to_x, (o.tiles_y, o.tiles_x), ctypes.c_int8, np.int8)
-    ytob = host_array(o.host_y_to_b, (o.tiles_y, o.tiles_x), ctypes.c_int8, np.int8)
-    stats = host_array(o.host_matrix_scale_stats, (3,), ctypes.c_float, np.float32)
+    return s
 
-    opsin = ref.linear_to_padded_opsin(ref.srgb8_to_linear(img))
-    rq, _, rpm = ref.initial_quant_field(opsin, 1.0)
-    pre = ref.gaborish_inverse(opsin)
-    rx, rb = ref.initial_cfl(pre)
-    rcells = ref.ac_strategy_search(pre, rq, rpm, rx, rb, 1.0)
-    assert np.array_equal(quant.view(np.uint32), rq.view(np.uint32))
-    assert np.array_equal(ytox, rx) and np.array_equal(ytob, rb)
-    assert np.array_equal(stats.view(np.uint32),
-                          restate.matrix_scale_stats(opsin, w, h).view(np.uint32))
-    assert (cells != rcells).sum() <= 0.001 * cells.size
+
+def block_distances(dmap: np.ndarray, cells: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """ReduceButteraugliDistanceMap (src/codec/butteraugli.cpp:116-199) of a
+    distance map: per transform, the float32 sequential sum of v^16 over its
+    pixels in raster order, mean = sum / count, then 1.2f * mean^(1/16).
+    Returns (with the host libm's powf, as the reference calls
+    std::pow(float, float); with the correctly rounded power, as the device
+    computes it)."""
+    libm = ctypes.CDLL("libm.so.6")
+    libm.powf.restype = ctypes.c_float
+    libm.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+    h, w = dmap.shape
+    glibc = np.zeros(cells.shape, np.float32)
+    exact = np.zeros(cells.shape, np.float32)
+    ys, xs = np.nonzero(cells & 1)
+    for strategy, (cw, ch) in STRATEGY_COVERED.items():
+        sel = (cells[ys, xs] >> 1) == strategy
+        ay, ax = ys[sel], xs[sel]
+        if ay.size == 0:
+            continue
+        norm = np.zeros(ay.size, np.float32)
+        count = np.zeros(ay.size, np.int64)
+        for dy in range(ch * 8):
+            for dx in range(cw * 8):
+                py, px = ay * 8 + dy, ax * 8 + dx
+                valid = (py < h) & (px < w)
+                v = dmap[np.minimum(py, h - 1), np.minimum(px, w - 1)].astype(np.float32)
+                v = v * v
+                v = v * v
+                v = v * v
+                v = v * v
+                norm = np.where(valid, norm + v, norm).astype(np.float32)
+                count += valid
+        mean = (norm / count.astype(np.float32)).astype(np.float32)
+        g = np.array([libm.powf(float(m), 0.0625) for m in mean], np.float32)
+        e = (mean.astype(np.float64) ** 0.0625).astype(np.float32)
+        g = (np.float32(1.2) * g).astype(np.float32)
+        e = (np.float32(1.2) * e).astype(np.float32)
+        for k in range(ay.size):
+            glibc[ay[k]:ay[k] + ch, ax[k]:ax[k] + cw] = g[k]
+            exact[ay[k]:ay[k] + ch, ax[k]:ax[k] + cw] = e[k]
+    return glibc, exact
+
+
+def check_block_distance(s: AnalysisSession, got: dict, want: dict) -> None:
+    """The device's block distances are the correctly rounded reduction of its
+    own distance map, and the reference's are glibc powf of the same block
+    means: the two differ by 1 ulp only where glibc's powf is not correctly
+    rounded (a small fraction of inputs)."""
+    o = s.outputs
+    by, bx = got["cells"].shape
+    dmap = device_to_host(o.distance_map, (s.height, s.width), np.float32)
+    glibc, exact = block_distances(dmap, got["cells"])
+    bd = device_to_host(o.block_distance, (by, bx), np.float32)
+    assert_bitexact(bd, exact, "block distance (device reduction)")
+    assert_bitexact(want["block_distance"], glibc, "block distance (reference from device map)")
+
+
+def reference(img: np.ndarray, effort: int = 7, target: float = 1.0):
+    h, w, _ = img.shape
+    lin = ref.srgb8_to_linear(img)
+    opsin = ref.linear_to_padded_opsin(lin)
+    stats = restate.matrix_scale_stats(opsin, w, h)
+    # Below effort 7 the statistics are not gathered and select from zeros.
+    xs, bs = restate.select_matrix_scales(stats if effort >= 7 else np.zeros(3, np.float32),
+                                          target)
+    return opsin, stats, ref.quantization_pipeline(lin, opsin, target, effort, xs, bs)
+
+
+def compare_front_half(s: AnalysisSession, got: dict, want: dict, stats: np.ndarray,
+                       effort: int) -> None:
+    o = s.outputs
+    assert_bitexact(got["initial_quant"], want["initial_quant"], "initial quant field")
+    if effort >= 7:  # gathered from effort 7 on
+        host_stats = np.ctypeslib.as_array(
+            ctypes.cast(o.host_matrix_scale_stats, ctypes.POINTER(ctypes.c_float)), shape=(3,))
+        assert_bitexact(host_stats.copy(), stats, "matrix scale stats")
+    # The strategy search may differ in at most 0.1% of blocks (1-ulp FP64
+    # cost differences); the evaluation loop is compared when it agrees.
+    assert (got["cells"] != want["cells"]).sum() <= 0.001 * got["cells"].size
+    if not np.array_equal(got["cells"], want["cells"]):
+        pytest.skip("strategy grid differs in a tie; loop outputs not comparable")
+
+
+def compare_loop_exact(s: AnalysisSession, got: dict, want: dict) -> None:
+    """One evaluation, nothing fed back: every output bit-exact (block
+    distances per check_block_distance)."""
+    o = s.outputs
+    h, w = s.height, s.width
+    by, bx = got["cells"].shape
+    assert_bitexact(got["quantizer_params"], want["quantizer_params"], "quantizer params")
+    assert_bitexact(got["raw_quant"], want["raw_quant"], "raw quant field")
+    assert_bitexact(got["final_quant"], want["final_quant"], "final quant field")
+    assert_bitexact(got["y_to_x"], want["y_to_x"], "final y_to_x")
+    assert_bitexact(got["y_to_b"], want["y_to_b"], "final y_to_b")
+    assert_bitexact(got["quantized_dc"], want["quantized_dc"], "quantized DC")
+    ac = footprint_to_group_order(got["quantized_ac"], got["cells"])
+    assert ac.size == int(want["group_used"].sum()) * 3
+    assert_bitexact(ac, want["ac"][:ac.size], "quantized AC (group order)")
+    assert_bitexact(got["score_history"], want["score_history"], "score history")
+    dc = device_to_host(o.dc, (3, by, bx), np.float32)
+    assert_bitexact(dc, want["dc"], "dequantized DC")
+    check_block_distance(s, got, want)
+    rec = device_to_host(o.reconstructed_linear, (3, h, w), np.float32)
+    assert_bitexact(rec, want["reconstructed"], "reconstructed linear RGB")
+
+
+def compare_loop_fed_back(s: AnalysisSession, got: dict, want: dict) -> int:
+    """Several evaluations: block distances feed the field updates, so a glibc
+    powf rounding case may move single field values by an ulp. The quantizer
+    must match exactly and at most 0.1% of blocks may differ in any output;
+    returns the number of differing blocks."""
+    by, bx = got["cells"].shape
+    assert_bitexact(got["quantizer_params"], want["quantizer_params"], "quantizer params")
+    field_rel = np.abs(got["final_quant"].astype(np.float64) - want["final_quant"]) / want[
+        "final_quant"]
+    assert field_rel.max() <= 5e-7, f"final field differs by up to {field_rel.max():.3g}"
+    bad = (differing_blocks(got["final_quant"], want["final_quant"])
+           | differing_blocks(got["raw_quant"], want["raw_quant"])
+           | differing_blocks(got["quantized_dc"], want["quantized_dc"])
+           | differing_blocks(got["quantized_ac"],
+                              group_order_to_footprint(want["ac"], got["cells"]), pixels=True))
+    cfl = differing_blocks(got["y_to_x"], want["y_to_x"]) | differing_blocks(got["y_to_b"],
+                                                                                 want["y_to_b"])
+    assert bad.sum() <= 0.001 * bad.size, f"{bad.sum()} of {bad.size} blocks differ"
+    assert cfl.sum() <= max(1, 0.01 * cfl.size), f"{cfl.sum()} CfL tiles differ"
+    np.testing.assert_allclose(got["score_history"], want["score_history"], rtol=5e-3)
+    return int(bad.sum())
+
+
+SIZES = [(509, 261, 4509), (256, 256, 77), (1000, 700, 5000)]
+
+
+@pytest.mark.parametrize("w,h,seed", SIZES)
+def test_session_single_evaluation_bitexact(cuda, w, h, seed):
+    """Effort 5: the whole front half and one full evaluation (quantizer,
+    final CfL, coefficient coding, DC quantization, reconstruction, loop
+    filters, Butteraugli) bit for bit."""
+    img = generate_srgb8(w, h, seed)
+    s = run_session(img, effort=5)
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference(img, effort=5)
+    compare_front_half(s, got, want, stats, 5)
+    compare_loop_exact(s, got, want)
+    s.close()
+
+
+@pytest.mark.parametrize("w,h,seed", SIZES)
+def test_session_matches_reference(cuda, w, h, seed):
+    """Effort 7 (the headline configuration): two field updates."""
+    img = generate_srgb8(w, h, seed)
+    s = run_session(img)
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference(img)
+    compare_front_half(s, got, want, stats, 7)
+    if compare_loop_fed_back(s, got, want) == 0:
+        compare_loop_exact(s, got, want)
+    s.close()
+
+
+@pytest.mark.parametrize("effort", [6, 8, 9, 10])
+def test_session_iterations_by_effort(cuda, effort):
+    """Evaluation count follows AdaptiveQuantizationIterations
+    (src/codestream/workflow_internal.h:69-82)."""
+    img = generate_srgb8(320, 200, 600 + effort)
+    s = run_session(img, effort=effort)
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference(img, effort=effort)
+    assert got["score_history"].shape == want["score_history"].shape
+    compare_front_half(s, got, want, stats, effort)
+    if compare_loop_fed_back(s, got, want) == 0:
+        compare_loop_exact(s, got, want)
+    s.close()
+
+
+def test_session_repeated_analysis_is_stable(cuda):
+    """A session reused for a second image gives the same results as a fresh
+    one (no state leaks between analyses)."""
+    a = generate_srgb8(300, 180, 11)
+    b = generate_srgb8(300, 180, 12)
+    s = run_session(a)
+    s.analyze_host(b, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    again = s.host_results()
+    fresh = run_session(b).host_results()
+    for key in ("final_quant", "raw_quant", "quantized_dc", "quantized_ac", "score_history"):
+        assert_bitexact(again[key], fresh[key], key)
     s.close()
 
 
