@@ -65,6 +65,14 @@ def _check(code: int, name: str) -> None:
         raise RuntimeError(f"{name}: status {code}: {lib().gjxl_ref_last_error().decode()}")
 
 
+def set_threads(threads: int) -> None:
+    """CPU thread budget of the pipeline entry points (0: the caller's)."""
+    fn = lib().gjxl_ref_set_threads
+    fn.argtypes = [_Z]
+    fn.restype = c_int
+    fn(threads)
+
+
 def padded_extent(width: int, height: int) -> tuple[int, int]:
     return (width + 7) // 8 * 8, (height + 7) // 8 * 8
 

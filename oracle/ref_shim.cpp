@@ -16,6 +16,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
+#include <optional>
 #include <string>
 #include <vector>
 
@@ -105,8 +106,13 @@ GJXL_REF_API const char* gjxl_ref_last_error(void) {
   return g_last_error.c_str();
 }
 
+// CPU thread budget installed around the pipeline entry points, as the
+// workflow installs options.cpu_thread_count (src/codestream/workflow.cpp:1640).
+// 0 leaves the calling thread's budget untouched (serial outside an encode).
+static size_t g_threads = 0;
+
 GJXL_REF_API int gjxl_ref_set_threads(size_t threads) {
-  (void)threads;
+  g_threads = threads;
   return 0;
 }
 
@@ -430,6 +436,8 @@ GJXL_REF_API int gjxl_ref_quantization_pipeline(
   aq.profile.b_qm_scale = static_cast<uint8_t>(b_qm_scale);
   aq.search_epf_sharpness = false;
 
+  std::optional<thread_budget_internal::EncodeScope> budget;
+  if (g_threads != 0) budget.emplace(g_threads);
   std::vector<double> history;
   VarDctEncoderFrame frame;
   MaximumErrorResult max_error;
