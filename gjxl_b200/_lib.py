@@ -26,6 +26,7 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_matrix_scale_stats": [P, Z, Z, Z, Z, P, P],
     "gjxl_b200_initial_quant_scratch_bytes": [Z, Z],
     "gjxl_b200_initial_quant_field": [P, Z, Z, Z, Z, F, F, P, P, P, Z, P, Z, P, P],
+    "gjxl_b200_initial_quant_field_noalloc": [P, Z, Z, Z, Z, F, F, P, P, P, Z, P, P],
     "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_quant_matrix": [I, I, P, P, Z],

@@ -111,6 +111,28 @@ GJXL_B200_API int gjxl_b200_initial_quant_field(
     uint32_t* device_error, void* stream);
 
 /*
+ * Initial quantization field without any device allocation: no counterpart
+ * in the reference. Same arguments and results as
+ * gjxl_b200_initial_quant_field, but the scratch is a 16 MiB static device
+ * array owned by the library, so the call allocates nothing. For callers that
+ * cannot allocate device memory per image (a service under a fixed memory
+ * budget, where cudaMalloc/cudaFree would synchronize the device and an
+ * out-of-memory failure mid-image cannot be recovered; a plug-in host without
+ * a device allocator).
+ *  - Limit: padded images of at most 3,947,580 pixels (e.g. 2048 x 1920);
+ *    larger ones are rejected with GJXL_B200_INVALID_ARGUMENT.
+ *  - The first call on each device sets up the scratch address there
+ *    (cudaGetSymbolAddress); make it before any stream capture.
+ *  - One scratch array per device: overlapping calls on one device race.
+ *    Serialize them (for example, on one stream).
+ */
+GJXL_B200_API int gjxl_b200_initial_quant_field_noalloc(
+    const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+    size_t padded_width, size_t padded_height, float butteraugli_target,
+    float rescale, float* quant_field, float* strategy_mask, float* pixel_mask,
+    size_t pixel_mask_stride, uint32_t* device_error, void* stream);
+
+/*
  * Inverse Gaborish (row a4).
  * Replaces GaborishInverseProvider::Apply
  * (src/codec/quantization_pipeline_internal.h:20-32) and GpuImagePrimitives'
