@@ -632,149 +632,167 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
 // ---------------------------------------------------------------------------
 // Prediction-aware DC quantization with the weighted predictor.
 //
-// The reference walks each 256x256-block DC group in raster order. Every
-// sample depends only on its W, N, NW, NE and NN neighbours (and on the
-// predictor's error state of those positions), so all samples on a line
-// x + 2y = t are independent: the kernel runs one CTA per group and sweeps
-// those lines, keeping the predictor state in full-resolution arrays
-// (E: signed errors, PE[4]: per-sub-predictor error sums, as the reference's
-// rolling rows would hold them when each sample is predicted).
+// The reference walks each 256x256-block DC group in raster order, channel
+// by channel (Y, X, B), resetting the predictor per channel. A sample at
+// (x, y) depends on row y at x-1 and on row y-1 at x-1..x+1 and row y-2 at x,
+// through the quantized values and the predictor's error state. So all
+// samples on a line x + 2y = t are independent, and the kernel sweeps those
+// lines (waves). Rows y-1 and y-2 are then 2 and 4 samples ahead of row y, so
+// every value a sample reads was written within the last 4 waves. Each row
+// keeps its quantized values, signed errors and the four sub-predictor error
+// sums in an 8-slot ring (slot x & 7) in shared memory; nothing goes to
+// global memory but the quantized output.
+//
+// One CTA per DC group, one thread per (channel, row): threads 0-255 run X,
+// 256-511 Y and 512-767 B. X and Y are independent. B's residual subtracts
+// Y's quantized value at the same position, so B runs one wave behind Y and
+// reads it from Y's ring. Slot x & 7 of a row is rewritten 8 waves later, and
+// a reader needs it at most 4 waves (B: 1 wave) after it was written.
 
 struct DcQuantParams {
   const float* dc;  // 3 planes of blocks
   int32_t* quantized;
   float* reconstructed;
-  int32_t* state;  // 5 planes of blocks (E, PE0..PE3)
   int width, height;
   size_t pitch;
   const AqQuantizer* q;
   float precision;  // 1 << extra_dc_precision
 };
 
+constexpr int kDcGroup = 256;
+constexpr int kDcRing = 8;
+constexpr int kDcThreads = 3 * kDcGroup;
+
+struct DcRings {
+  int32_t q[3][kDcRing][kDcGroup];        // quantized values
+  int32_t e[3][kDcRing][kDcGroup];        // signed prediction errors (error_)
+  uint32_t pe[3][4][kDcRing][kDcGroup];   // sub-predictor errors (prediction_errors_)
+  uint32_t row0[3][4][kDcRing];           // row 0's own errors, before row 1 adds
+  uint32_t reciprocal[64];                // (1 << 24) / (i + 1)
+};
+
 __device__ __forceinline__ int BitWidth64(uint64_t v) { return v == 0 ? 0 : 64 - __clzll(v); }
 __device__ __forceinline__ int BitWidth32(uint32_t v) { return v == 0 ? 0 : 32 - __clz(v); }
 
-__global__ void __launch_bounds__(256) DcQuantKernel(const __grid_constant__ DcQuantParams p) {
-  const int gx0 = blockIdx.x * 256, gy0 = blockIdx.y * 256;
-  const int gw = min(256, p.width - gx0), gh = min(256, p.height - gy0);
+__global__ void __launch_bounds__(kDcThreads, 1)
+DcQuantKernel(const __grid_constant__ DcQuantParams p) {
+  extern __shared__ __align__(16) unsigned char dc_smem[];
+  DcRings& r = *reinterpret_cast<DcRings*>(dc_smem);
+  const int gx0 = blockIdx.x * kDcGroup, gy0 = blockIdx.y * kDcGroup;
+  const int gw = min(kDcGroup, p.width - gx0), gh = min(kDcGroup, p.height - gy0);
   const int stride = p.width;
-  __shared__ uint32_t row0[4][256];
-  int32_t* E = p.state;
-  uint32_t* PE = reinterpret_cast<uint32_t*>(p.state + p.pitch);  // [4][pitch]
+  const int c = threadIdx.x / kDcGroup;  // 0: X, 1: Y, 2: B
+  const int y = threadIdx.x % kDcGroup;
+  const int lag = c == 2 ? 1 : 0;
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) r.reciprocal[i] = (1u << 24) / (i + 1);
   const AqQuantizer q = *p.q;
-  float inverse_steps[3], steps[3];
-  for (int c = 0; c < 3; ++c) {
-    inverse_steps[c] = q.inverse_dc_steps[c] * p.precision;
-    steps[c] = q.dc_steps[c] / p.precision;
-  }
+  const float inverse_step = q.inverse_dc_steps[c] * p.precision;
+  const float step_y = q.dc_steps[1] / p.precision;
   // WeightedPredictorParameters defaults (prediction.h:36-40).
-  const int64_t pcoef[7] = {16, 10, 7, 7, 7, 0, 0};
+  constexpr int64_t kP0 = 16, kP1 = 10, kP2 = 7, kP3 = 7, kP4 = 7, kP5 = 0, kP6 = 0;
   const uint32_t max_weights[4] = {13, 12, 12, 12};
-  const int order[3] = {1, 0, 2};
-  for (int oc = 0; oc < 3; ++oc) {
-    const int c = order[oc];
-    int32_t* plane = p.quantized + c * p.pitch;
-    const float* source = p.dc + c * p.pitch;
-    const int waves = (gw - 1) + 2 * (gh - 1) + 1;
-    for (int t = 0; t < waves; ++t) {
-      // Positions (x, y) of this group with x + 2y == t.
-      const int y_lo = max(0, (t - (gw - 1) + 1) / 2), y_hi = min(gh - 1, t / 2);
-      for (int y = y_lo + static_cast<int>(threadIdx.x); y <= y_hi; y += blockDim.x) {
-        const int x = t - 2 * y;
-        if (x < 0 || x >= gw) continue;
-        const size_t index = static_cast<size_t>(gy0 + y) * stride + gx0 + x;
-        const int64_t w = x ? plane[index - 1] : y ? plane[index - stride] : 0;
-        const int64_t n = y ? plane[index - stride] : w;
-        const int64_t nw = x && y ? plane[index - stride - 1] : w;
-        const int64_t ne = y && x + 1 < gw ? plane[index - stride + 1] : n;
-        const int64_t nn = y > 1 ? plane[index - 2 * stride] : n;
-        // Predict (prediction.h:73-119). The signed errors of row -1 read as
-        // zeros. The sub-predictor error sums of row 0 read the predictor's
-        // other rolling row, which by then holds only row 0's own "+="
-        // updates: its entry j carries the error of (j - 1, 0) once that
-        // sample is done, so north = err(x-1), northwest = err(x-2) and
-        // northeast (not yet written) = 0, or north at the right edge.
-        const int xne = x + 1 < gw ? x + 1 : x, xnw = x ? x - 1 : x;
-        const size_t up = static_cast<size_t>(gy0 + y - 1) * stride + gx0;
-        uint32_t weights[4];
-        uint32_t weight_sum = 0;
-        for (int i = 0; i < 4; ++i) {
-          uint32_t error;
-          if (y) {
-            error = PE[i * p.pitch + up + x] + PE[i * p.pitch + up + xne] +
-                    PE[i * p.pitch + up + xnw];
-          } else {
-            const uint32_t north = x ? row0[i][x - 1] : 0u;
-            const uint32_t northeast = x + 1 < gw ? 0u : north;
-            const uint32_t northwest = x >= 2 ? row0[i][x - 2] : 0u;
-            error = north + northeast + northwest;
-          }
-          const int shift = max(0, BitWidth64(static_cast<uint64_t>(error) + 1) - 6);
-          const uint32_t reciprocal = (1u << 24) / ((error >> shift) + 1);
-          weights[i] = 4 + ((max_weights[i] * reciprocal) >> shift);
-          weight_sum += weights[i];
+  int32_t* plane = p.quantized + c * p.pitch;
+  const float* source = p.dc + c * p.pitch;
+  int32_t (*Q)[kDcGroup] = r.q[c];
+  int32_t (*E)[kDcGroup] = r.e[c];
+  __syncthreads();
+  const int waves = (gw - 1) + 2 * (gh - 1) + 2;
+  for (int t = 0; t < waves; ++t) {
+    const int x = t - lag - 2 * y;
+    if (y < gh && x >= 0 && x < gw) {
+      const int s = x & 7, sw = (x - 1) & 7, sne = (x + 1 < gw ? x + 1 : x) & 7;
+      const int snw = (x ? x - 1 : x) & 7;
+      const int up = y - 1, up2 = y - 2;
+      const int64_t w = x ? Q[sw][y] : y ? Q[s][up] : 0;
+      const int64_t n = y ? Q[s][up] : w;
+      const int64_t nw = x && y ? Q[sw][up] : w;
+      const int64_t ne = y && x + 1 < gw ? Q[(x + 1) & 7][up] : n;
+      const int64_t nn = y > 1 ? Q[s][up2] : n;
+      // Predict (prediction.h:73-119). The signed errors of row -1 read as
+      // zeros. The sub-predictor error sums of row 0 read the predictor's
+      // other rolling row, which by then holds only row 0's own "+="
+      // updates: its entry j carries the error of (j - 1, 0) once that
+      // sample is done, so north = err(x-1), northwest = err(x-2) and
+      // northeast (not yet written) = 0, or north at the right edge.
+      uint32_t weights[4];
+      uint32_t weight_sum = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        uint32_t error;
+        if (y) {
+          error = r.pe[c][i][s][up] + r.pe[c][i][sne][up] + r.pe[c][i][snw][up];
+        } else {
+          const uint32_t north = x ? r.row0[c][i][sw] : 0u;
+          const uint32_t northeast = x + 1 < gw ? 0u : north;
+          const uint32_t northwest = x >= 2 ? r.row0[c][i][(x - 2) & 7] : 0u;
+          error = north + northeast + northwest;
         }
-        const int log_weight = BitWidth32(weight_sum) - 1;
-        weight_sum = 0;
-        for (int i = 0; i < 4; ++i) {
-          weights[i] >>= log_weight - 4;
-          weight_sum += weights[i];
-        }
-        const int64_t ew = x ? E[index - 1] : 0;
-        const int64_t en = y ? E[up + x] : 0;
-        const int64_t enw = y ? E[up + xnw] : 0;
-        const int64_t ene = y ? E[up + xne] : 0;
-        const int64_t n8 = n * 8, w8 = w * 8, ne8 = ne * 8, nw8 = nw * 8, nn8 = nn * 8;
-        int64_t predictions[4];
-        predictions[0] = w8 + ne8 - n8;
-        predictions[1] = n8 - (((en + ew + ene) * pcoef[0]) >> 5);
-        predictions[2] = w8 - (((en + ew + enw) * pcoef[1]) >> 5);
-        predictions[3] = n8 - ((enw * pcoef[2] + en * pcoef[3] + ene * pcoef[4] +
-                                (nn8 - n8) * pcoef[5] + (nw8 - w8) * pcoef[6]) >> 5);
-        int64_t sum = static_cast<int64_t>(weight_sum >> 1) - 1;
-        for (int i = 0; i < 4; ++i) sum += predictions[i] * static_cast<int64_t>(weights[i]);
-        int64_t prediction =
-          (sum * static_cast<int64_t>((1u << 24) / weight_sum)) >> 24;
-        if (((en ^ ew) | (en ^ enw)) <= 0) {
-          const int64_t lo = min(w8, min(ne8, n8)), hi = max(w8, max(ne8, n8));
-          prediction = min(max(prediction, lo), hi);
-        }
-        const int64_t predicted = (prediction + 3) >> 3;
-        // Quantize the residual (dc_quantization.cpp:178-199).
-        float value = source[index];
-        if (c == 2) {
-          value = fmaf(-static_cast<float>(p.quantized[1 * p.pitch + index]), steps[1], value);
-        }
-        float residual = value * inverse_steps[c];
-        residual -= static_cast<float>(predicted);
-        if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
-        float rounded = roundf(residual);
-        if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
-        const int64_t quantized = predicted + static_cast<int64_t>(rounded);
-        plane[index] = static_cast<int32_t>(quantized);
-        // Update (prediction.h:121-141).
-        const int64_t scaled = quantized * 8;
-        E[index] = static_cast<int32_t>(prediction - scaled);
-        for (int i = 0; i < 4; ++i) {
-          const int64_t d = predictions[i] - scaled;
-          const uint32_t err = static_cast<uint32_t>(((d < 0 ? -d : d) + 3) >> 3);
-          PE[i * p.pitch + index] = err;
-          if (y && x + 1 < gw) PE[i * p.pitch + up + x + 1] += err;
-          // Row 0's errors as they were when predicted (row 1 adds to PE's).
-          if (!y) row0[i][x] = err;
-        }
+        const int shift = max(0, BitWidth64(static_cast<uint64_t>(error) + 1) - 6);
+        weights[i] = 4 + ((max_weights[i] * r.reciprocal[error >> shift]) >> shift);
+        weight_sum += weights[i];
       }
-      __syncthreads();
+      const int log_weight = BitWidth32(weight_sum) - 1;
+      weight_sum = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        weights[i] >>= log_weight - 4;
+        weight_sum += weights[i];
+      }
+      const int64_t ew = x ? E[sw][y] : 0;
+      const int64_t en = y ? E[s][up] : 0;
+      const int64_t enw = y ? E[snw][up] : 0;
+      const int64_t ene = y ? E[sne][up] : 0;
+      const int64_t n8 = n * 8, w8 = w * 8, ne8 = ne * 8, nw8 = nw * 8, nn8 = nn * 8;
+      int64_t predictions[4];
+      predictions[0] = w8 + ne8 - n8;
+      predictions[1] = n8 - (((en + ew + ene) * kP0) >> 5);
+      predictions[2] = w8 - (((en + ew + enw) * kP1) >> 5);
+      predictions[3] = n8 - ((enw * kP2 + en * kP3 + ene * kP4 + (nn8 - n8) * kP5 +
+                              (nw8 - w8) * kP6) >> 5);
+      int64_t sum = static_cast<int64_t>(weight_sum >> 1) - 1;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) sum += predictions[i] * static_cast<int64_t>(weights[i]);
+      int64_t prediction = (sum * static_cast<int64_t>(r.reciprocal[weight_sum - 1])) >> 24;
+      if (((en ^ ew) | (en ^ enw)) <= 0) {
+        const int64_t lo = min(w8, min(ne8, n8)), hi = max(w8, max(ne8, n8));
+        prediction = min(max(prediction, lo), hi);
+      }
+      const int64_t predicted = (prediction + 3) >> 3;
+      // Quantize the residual (dc_quantization.cpp:178-199).
+      const size_t index = static_cast<size_t>(gy0 + y) * stride + gx0 + x;
+      float value = source[index];
+      if (c == 2) value = fmaf(-static_cast<float>(r.q[1][s][y]), step_y, value);
+      float residual = value * inverse_step;
+      residual -= static_cast<float>(predicted);
+      if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
+      float rounded = roundf(residual);
+      if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
+      const int64_t quantized = predicted + static_cast<int64_t>(rounded);
+      plane[index] = static_cast<int32_t>(quantized);
+      Q[s][y] = static_cast<int32_t>(quantized);
+      // Update (prediction.h:121-141).
+      const int64_t scaled = quantized * 8;
+      E[s][y] = static_cast<int32_t>(prediction - scaled);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int64_t d = predictions[i] - scaled;
+        const uint32_t err = static_cast<uint32_t>(((d < 0 ? -d : d) + 3) >> 3);
+        r.pe[c][i][s][y] = err;
+        if (y && x + 1 < gw) r.pe[c][i][(x + 1) & 7][up] += err;
+        if (!y) r.row0[c][i][s] = err;
+      }
     }
+    __syncthreads();
   }
   // Reconstructed DC (dc_quantization.cpp:209-222).
+  const float steps[3] = {q.dc_steps[0] / p.precision, step_y, q.dc_steps[2] / p.precision};
   for (int i = threadIdx.x; i < gw * gh; i += blockDim.x) {
     const size_t index = static_cast<size_t>(gy0 + i / gw) * stride + gx0 + i % gw;
     const float ry = static_cast<float>(p.quantized[p.pitch + index]) * steps[1];
-    for (int c = 0; c < 3; ++c) {
-      float r = static_cast<float>(p.quantized[c * p.pitch + index]) * steps[c];
-      if (c == 2) r = fmaf(ry, 1.0f, r);
-      p.reconstructed[c * p.pitch + index] = r;
+    for (int ch = 0; ch < 3; ++ch) {
+      float v = static_cast<float>(p.quantized[ch * p.pitch + index]) * steps[ch];
+      if (ch == 2) v = fmaf(ry, 1.0f, v);
+      p.reconstructed[ch * p.pitch + index] = v;
     }
   }
 }
@@ -1043,21 +1061,24 @@ int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, co
 }
 
 int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, int32_t* quantized,
-                 float* reconstructed, int32_t* state, int extra_precision, cudaStream_t stream) {
-  const size_t blocks = bx * by;
-  cudaMemsetAsync(state, 0, 5 * blocks * sizeof(int32_t), stream);
+                 float* reconstructed, int extra_precision, cudaStream_t stream) {
   DcQuantParams p;
   p.dc = dc;
   p.quantized = quantized;
   p.reconstructed = reconstructed;
-  p.state = state;
   p.width = static_cast<int>(bx);
   p.height = static_cast<int>(by);
-  p.pitch = blocks;
+  p.pitch = bx * by;
   p.q = q;
   p.precision = static_cast<float>(1u << extra_precision);
-  dim3 grid(static_cast<unsigned>((bx + 255) / 256), static_cast<unsigned>((by + 255) / 256));
-  DcQuantKernel<<<grid, 256, 0, stream>>>(p);
+  const int smem = static_cast<int>(sizeof(DcRings));
+  int status = CheckCuda(cudaFuncSetAttribute(DcQuantKernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                         "aq dc quantize attribute");
+  if (status != GJXL_B200_OK) return status;
+  dim3 grid(static_cast<unsigned>((bx + kDcGroup - 1) / kDcGroup),
+            static_cast<unsigned>((by + kDcGroup - 1) / kDcGroup));
+  DcQuantKernel<<<grid, kDcThreads, smem, stream>>>(p);
   return CheckLaunch("aq dc quantize");
 }
 

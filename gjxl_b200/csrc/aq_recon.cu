@@ -202,6 +202,25 @@ __device__ __forceinline__ int MirrorR(int c, int n) {
   return phase < n ? phase : period - 1 - phase;
 }
 
+// Loop filters on a shared-memory tile: each CTA computes a kTileW x kTileH
+// output tile and first stages its input window (tile + halo, every
+// coordinate mirrored at the image border as the reference's filters read
+// it) for all three planes, so the filter taps read shared memory only.
+constexpr int kTileW = 32, kTileH = 8;
+
+template <int Halo>
+__device__ __forceinline__ void StageWindow(const float* in, size_t stride, size_t pitch, int w,
+                                            int h, int x0, int y0,
+                                            float (*tile)[kTileH + 2 * Halo][kTileW + 2 * Halo]) {
+  constexpr int TW = kTileW + 2 * Halo, TH = kTileH + 2 * Halo;
+  const int tid = threadIdx.y * kTileW + threadIdx.x;
+  for (int i = tid; i < 3 * TW * TH; i += kTileW * kTileH) {
+    const int c = i / (TW * TH), r = i % (TW * TH), ty = r / TW, tx = r % TW;
+    const int gy = MirrorR(y0 + ty - Halo, h), gx = MirrorR(x0 + tx - Halo, w);
+    tile[c][ty][tx] = in[c * pitch + static_cast<size_t>(gy) * stride + gx];
+  }
+}
+
 struct GaborishParams {
   const float* in;
   size_t in_stride, in_pitch;
@@ -211,20 +230,25 @@ struct GaborishParams {
   uint32_t* error;
 };
 
-__global__ void GaborishForwardKernel(const __grid_constant__ GaborishParams p) {
-  const int c = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.w * p.h) return;
-  const int x = i % p.w, y = i / p.w;
-  const float* plane = p.in + c * p.in_pitch;
-  auto s = [&](int dx, int dy) {
-    return plane[static_cast<size_t>(MirrorR(y + dy, p.h)) * p.in_stride + MirrorR(x + dx, p.w)];
-  };
-  const float axes = (s(-1, 0) + s(1, 0)) + (s(0, -1) + s(0, 1));
-  const float diagonals = (s(-1, -1) + s(1, -1)) + (s(-1, 1) + s(1, 1));
-  const float value = p.weights[0] * s(0, 0) + p.weights[1] * axes + p.weights[2] * diagonals;
-  if (!IsFinite(value)) RaiseError(p.error, kErrorNonFiniteOutput);
-  p.out[static_cast<size_t>(c) * p.w * p.h + i] = value;
+__global__ void __launch_bounds__(kTileW * kTileH)
+GaborishForwardKernel(const __grid_constant__ GaborishParams p) {
+  __shared__ float tile[3][kTileH + 2][kTileW + 2];
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
+  StageWindow<1>(p.in, p.in_stride, p.in_pitch, p.w, p.h, x0, y0, tile);
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= p.w || y >= p.h) return;
+  const int tx = threadIdx.x + 1, ty = threadIdx.y + 1;
+  const size_t n = static_cast<size_t>(p.w) * p.h;
+  for (int c = 0; c < 3; ++c) {
+    const auto& t = tile[c];
+    const float axes = (t[ty][tx - 1] + t[ty][tx + 1]) + (t[ty - 1][tx] + t[ty + 1][tx]);
+    const float diagonals =
+      (t[ty - 1][tx - 1] + t[ty - 1][tx + 1]) + (t[ty + 1][tx - 1] + t[ty + 1][tx + 1]);
+    const float value = p.weights[0] * t[ty][tx] + p.weights[1] * axes + p.weights[2] * diagonals;
+    if (!IsFinite(value)) RaiseError(p.error, kErrorNonFiniteOutput);
+    p.out[c * n + static_cast<size_t>(y) * p.w + x] = value;
+  }
 }
 
 struct EpfParams {
@@ -234,48 +258,58 @@ struct EpfParams {
   const float* inverse_sigma;
   int blocks_x;
   float sigma_scale;
-  int pass;  // 1: patch SAD, 2: pixel SAD (cardinal neighbours)
 };
 
-__global__ void EpfKernel(const __grid_constant__ EpfParams p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.w * p.h) return;
-  const int x = i % p.w, y = i / p.w;
+// One EPF iteration (epf.cpp:92-160). Pass 1 compares 5-pixel plus-shaped
+// patches (halo 2); pass 2 compares single pixels (halo 1).
+template <int Pass>
+__global__ void __launch_bounds__(kTileW * kTileH) EpfKernel(const __grid_constant__ EpfParams p) {
+  constexpr int Halo = Pass == 1 ? 2 : 1;
+  __shared__ float tile[3][kTileH + 2 * Halo][kTileW + 2 * Halo];
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
+  StageWindow<Halo>(p.in, p.w, static_cast<size_t>(p.w) * p.h, p.w, p.h, x0, y0, tile);
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= p.w || y >= p.h) return;
   const size_t n = static_cast<size_t>(p.w) * p.h;
+  const size_t i = static_cast<size_t>(y) * p.w + x;
+  const int tx = threadIdx.x + Halo, ty = threadIdx.y + Halo;
   const float block_inverse_sigma = p.inverse_sigma[(y / 8) * p.blocks_x + x / 8];
   const float kMinInverseSigma = -1.1715728752538099024f / 0.3f;
   if (block_inverse_sigma < kMinInverseSigma) {
-    for (int c = 0; c < 3; ++c) p.out[c * n + i] = p.in[c * n + i];
+    for (int c = 0; c < 3; ++c) p.out[c * n + i] = tile[c][ty][tx];
     return;
   }
   const bool border = x % 8 == 0 || x % 8 == 7 || y % 8 == 0 || y % 8 == 7;
   const float scaled = block_inverse_sigma * p.sigma_scale * (border ? 2.0f / 3.0f : 1.0f);
-  auto sample = [&](int c, int sx, int sy) {
-    return p.in[c * n + static_cast<size_t>(MirrorR(sy, p.h)) * p.w + MirrorR(sx, p.w)];
-  };
   const float channel_scale[3] = {40.0f, 5.0f, 3.5f};
-  float sum[3] = {p.in[i], p.in[n + i], p.in[2 * n + i]};
+  float sum[3] = {tile[0][ty][tx], tile[1][ty][tx], tile[2][ty][tx]};
   float weight_sum = 1.0f;
   const int offsets[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
   const int plus[5][2] = {{0, 0}, {0, -1}, {-1, 0}, {0, 1}, {1, 0}};
+#pragma unroll
   for (int o = 0; o < 4; ++o) {
     const int dx = offsets[o][0], dy = offsets[o][1];
     float sad = 0.0f;
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (p.pass == 1) {
+      const auto& t = tile[c];
+      if (Pass == 1) {
         float channel_sad = 0.0f;
+#pragma unroll
         for (int k = 0; k < 5; ++k) {
-          channel_sad += fabsf(sample(c, x + plus[k][0], y + plus[k][1]) -
-                               sample(c, x + dx + plus[k][0], y + dy + plus[k][1]));
+          channel_sad += fabsf(t[ty + plus[k][1]][tx + plus[k][0]] -
+                               t[ty + dy + plus[k][1]][tx + dx + plus[k][0]]);
         }
         sad = fmaf(channel_sad, channel_scale[c], sad);
       } else {
-        sad = fmaf(fabsf(sample(c, x, y) - sample(c, x + dx, y + dy)), channel_scale[c], sad);
+        sad = fmaf(fabsf(t[ty][tx] - t[ty + dy][tx + dx]), channel_scale[c], sad);
       }
     }
     const float weight = fmaxf(0.0f, fmaf(sad, scaled, 1.0f));
     weight_sum += weight;
-    for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, sample(c, x + dx, y + dy), sum[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, tile[c][ty + dy][tx + dx], sum[c]);
   }
   for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
 }
@@ -463,7 +497,6 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
 int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, size_t width,
                   size_t height, const float* inverse_sigma, size_t bx, float* scratch_a,
                   float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream) {
-  const size_t n = width * height;
   GaborishParams g;
   g.in = recon;
   g.in_stride = recon_stride;
@@ -478,7 +511,10 @@ int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, s
   g.weights[1] = w1 / divisor;
   g.weights[2] = w2 / divisor;
   g.error = error;
-  GaborishForwardKernel<<<dim3(Blocks(n), 3), kThreads, 0, stream>>>(g);
+  const dim3 tiles(static_cast<unsigned>((width + kTileW - 1) / kTileW),
+                   static_cast<unsigned>((height + kTileH - 1) / kTileH));
+  const dim3 threads(kTileW, kTileH);
+  GaborishForwardKernel<<<tiles, threads, 0, stream>>>(g);
   EpfParams e;
   e.w = static_cast<int>(width);
   e.h = static_cast<int>(height);
@@ -487,13 +523,11 @@ int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, s
   e.in = scratch_a;
   e.out = scratch_b;
   e.sigma_scale = 1.65f * 1.0f;
-  e.pass = 1;
-  EpfKernel<<<Blocks(n), kThreads, 0, stream>>>(e);
+  EpfKernel<1><<<tiles, threads, 0, stream>>>(e);
   e.in = scratch_b;
   e.out = filtered;
   e.sigma_scale = 1.65f * 6.5f;
-  e.pass = 2;
-  EpfKernel<<<Blocks(n), kThreads, 0, stream>>>(e);
+  EpfKernel<2><<<tiles, threads, 0, stream>>>(e);
   return CheckLaunch("aq loop filters");
 }
 

@@ -101,7 +101,6 @@ struct Session {
   int32_t* qdc = nullptr;
   float* dc_rec = nullptr;
   float* dc_smooth = nullptr;
-  int32_t* dc_state = nullptr;
   float* inverse_sigma = nullptr;
   float* recon = nullptr;      // padded reconstructed XYB
   float* filter_a = nullptr;   // 3 x width x height
@@ -186,7 +185,6 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->qdc), 3 * blocks * sizeof(int32_t)},
     {reinterpret_cast<void**>(&s->dc_rec), 3 * blocks * sizeof(float)},
     {reinterpret_cast<void**>(&s->dc_smooth), 3 * blocks * sizeof(float)},
-    {reinterpret_cast<void**>(&s->dc_state), 5 * blocks * sizeof(int32_t)},
     {reinterpret_cast<void**>(&s->inverse_sigma), blocks * sizeof(float)},
     {reinterpret_cast<void**>(&s->recon), 3 * plane * sizeof(float)},
     {reinterpret_cast<void**>(&s->filter_a), 3 * image * sizeof(float)},
@@ -277,8 +275,7 @@ int RunAq(Session* s, cudaStream_t stream) {
     GJXL_TRY(AqCoding(s->anchors, s->anchor_counts, s->bx, s->by, s->coef, s->pw, s->pitch,
                       s->qac, s->dc, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
                       s->matrix_multipliers, s->error, stream));
-    GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, s->dc_state, 1,
-                          stream));
+    GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, 1, stream));
     GJXL_TRY(AqInverseSigma(s->cells, s->bx, s->by, s->raw, s->quantizer, s->inverse_sigma,
                             stream));
     GJXL_TRY(AqSmoothDc(s->dc_rec, s->bx, s->by, s->quantizer, s->dc_smooth, stream));
