@@ -37,6 +37,10 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_butteraugli_destroy": None,
     "gjxl_b200_butteraugli_prepare": [P, P, Z, Z, P],
     "gjxl_b200_butteraugli_compare": [P, P, Z, Z, P, Z, P, P, P],
+    "gjxl_b200_ac_token_capacity": [Z, Z],
+    "gjxl_b200_ac_tokens_create": [Z, Z, P],
+    "gjxl_b200_ac_tokens_destroy": None,
+    "gjxl_b200_ac_tokenize": [P, P, P, P, Z, Z, P, I, P, P],
     # Session entry points are bound with their struct types in session.py.
     "gjxl_b200_default_options": None,
     "gjxl_b200_session_create": None,
@@ -49,7 +53,8 @@ SIGNATURES: dict[str, list] = {
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
-             "gjxl_b200_ac_strategy_cost_bytes": c_size_t}
+             "gjxl_b200_ac_strategy_cost_bytes": c_size_t,
+             "gjxl_b200_ac_token_capacity": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

@@ -7,6 +7,8 @@ dimension is the row stride (a multiple of 4).
 
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
 from . import _lib
@@ -141,3 +143,92 @@ class Butteraugli:
             self.close()
         except Exception:
             pass
+
+
+class BlockContextMap(ctypes.Structure):
+    """gjxl_b200_block_context_map."""
+    _fields_ = [("threshold_count", ctypes.c_uint32), ("qf_thresholds", ctypes.c_uint32 * 15),
+                ("num_contexts", ctypes.c_uint32), ("context_map", ctypes.c_uint8 * (3 * 13 * 16))]
+
+    @classmethod
+    def make(cls, thresholds, context_map: bytes, num_contexts: int) -> "BlockContextMap":
+        m = cls()
+        m.threshold_count = len(thresholds)
+        for i, t in enumerate(thresholds):
+            m.qf_thresholds[i] = t
+        m.num_contexts = num_contexts
+        for i, v in enumerate(context_map):
+            m.context_map[i] = v
+        return m
+
+
+class AcTokenOutputs(ctypes.Structure):
+    """gjxl_b200_ac_token_outputs."""
+    _fields_ = [("token_values", ctypes.c_void_p), ("token_contexts", ctypes.c_void_p),
+                ("token_capacity", ctypes.c_size_t), ("group_offsets", ctypes.c_void_p),
+                ("histogram", ctypes.c_void_p), ("packed_ac", ctypes.c_void_p),
+                ("group_coef_offsets", ctypes.c_void_p), ("order_population", ctypes.c_void_p),
+                ("present_mask", ctypes.c_void_p), ("used_order_mask", ctypes.c_void_p),
+                ("orders", ctypes.c_void_p), ("device_error", ctypes.c_void_p)]
+
+
+class AcTokens:
+    """AC group packing, coefficient-order populations and AC tokenization
+    for one block extent (gjxl_b200_ac_tokens_*)."""
+
+    def __init__(self, blocks_x: int, blocks_y: int):
+        self.bx, self.by = blocks_x, blocks_y
+        handle = ctypes.c_void_p()
+        _lib.call("gjxl_b200_ac_tokens_create", blocks_x, blocks_y, ctypes.byref(handle))
+        self.handle = handle
+        self.capacity = _lib.load().gjxl_b200_ac_token_capacity(blocks_x, blocks_y)
+        self.groups = ((blocks_x + 31) // 32) * ((blocks_y + 31) // 32)
+
+    def close(self):
+        if self.handle:
+            _lib.load().gjxl_b200_ac_tokens_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tokenize(self, cells: torch.Tensor, raw_quant: torch.Tensor, quantized_ac: torch.Tensor,
+                 block_context_map: BlockContextMap, order_mode: int = 0,
+                 histogram: bool = True, packed: bool = True) -> dict:
+        """Returns device tensors: values, contexts, group_offsets, histogram,
+        packed_ac, group_coef_offsets, order_population, masks (present, used),
+        orders and the error word. `quantized_ac` is (3, padded_h, padded_w)
+        int32 in footprint layout."""
+        dev = quantized_ac.device
+        u32 = torch.int32
+        res = {
+            "values": torch.empty(self.capacity, dtype=u32, device=dev),
+            "contexts": torch.empty(self.capacity, dtype=torch.int16, device=dev),
+            "group_offsets": torch.zeros(self.groups + 1, dtype=u32, device=dev),
+            "group_coef_offsets": torch.zeros(self.groups + 1, dtype=u32, device=dev),
+            "order_population": torch.zeros(6144, dtype=u32, device=dev),
+            "masks": torch.zeros(2, dtype=u32, device=dev),
+            "orders": torch.zeros((13, 3, 1024), dtype=u32, device=dev),
+            "error": torch.zeros(1, dtype=u32, device=dev),
+        }
+        if histogram:
+            res["histogram"] = torch.zeros((block_context_map.num_contexts * 495, 128), dtype=u32,
+                                           device=dev)
+        if packed:
+            res["packed_ac"] = torch.zeros(3 * 64 * self.bx * self.by, dtype=u32, device=dev)
+        out = AcTokenOutputs(
+            res["values"].data_ptr(), res["contexts"].data_ptr(), self.capacity,
+            res["group_offsets"].data_ptr(),
+            res["histogram"].data_ptr() if histogram else None,
+            res["packed_ac"].data_ptr() if packed else None,
+            res["group_coef_offsets"].data_ptr(), res["order_population"].data_ptr(),
+            res["masks"].data_ptr(), res["masks"].data_ptr() + 4, res["orders"].data_ptr(),
+            res["error"].data_ptr())
+        _, ph, pw = quantized_ac.shape
+        _lib.call("gjxl_b200_ac_tokenize", self.handle, cells.data_ptr(), raw_quant.data_ptr(),
+                  quantized_ac.data_ptr(), pw, ph * pw, ctypes.byref(block_context_map),
+                  order_mode, ctypes.byref(out), _stream())
+        return res

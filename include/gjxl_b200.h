@@ -243,6 +243,63 @@ GJXL_B200_API int gjxl_b200_butteraugli_compare(
     double* score, uint32_t* device_error, void* stream);
 
 /* ------------------------------------------------------------------------
+ * AC group packing, coefficient-order populations and AC tokenization
+ * (rows a17, a18).
+ *
+ * Replaces the reference's AC-group packing and order-population kernels
+ * (PackAcGroupsKernel cuda_ac_group_kernels.cu:13,
+ * CoefficientOrderPopulationKernel cuda_coefficient_order_kernels.cu:29) and
+ * the AcTokenizationProvider seam
+ * (src/codestream/ac_tokenization_provider_internal.h:20-31) with the CPU
+ * semantics of TokenizeSimpleAcGroupDirectValidated
+ * (src/codestream/ac_group.cpp:740) and ComputeSimpleCoefficientOrdersForEncoder
+ * (src/codestream/coefficient_order.cpp:568-830).
+ *
+ * Inputs: the strategy grid, the raw quant field (blocks) and quantized AC in
+ * footprint layout (gjxl_b200_outputs). Tokens of every 256x256 group are
+ * written back to back in row-major group order; group g's tokens are
+ * token_values/contexts[group_offsets[g] .. group_offsets[g+1]). Within a
+ * group: anchors in raster order, channels Y, X, B, each a nonzero-count token
+ * followed by its coefficient tokens in scan order. order_mode: 0 natural
+ * scans, 1 custom scans from full zero counts, 2 the effort-7 behaviour (DCT8
+ * populations sampled when the frame holds DCT8 only).
+ * ------------------------------------------------------------------------ */
+
+typedef struct gjxl_b200_block_context_map {
+  uint32_t threshold_count;          /* raw-quant thresholds, 0..15 */
+  uint32_t qf_thresholds[15];
+  uint32_t num_contexts;             /* 1..16 */
+  /* [(channel_row * 13 + order_family) * (threshold_count + 1) + segment] */
+  uint8_t context_map[3 * 13 * 16];
+} gjxl_b200_block_context_map;
+
+typedef struct gjxl_b200_ac_token_outputs {
+  uint32_t* token_values;        /* required, token_capacity entries */
+  uint16_t* token_contexts;      /* required, token_capacity entries */
+  size_t token_capacity;         /* >= gjxl_b200_ac_token_capacity() */
+  uint32_t* group_offsets;       /* required, groups + 1 */
+  uint32_t* histogram;           /* optional: [num_contexts * 495][128] counts */
+  int32_t* packed_ac;            /* optional: group order, 3 x 64 x blocks */
+  uint32_t* group_coef_offsets;  /* optional: groups + 1 offsets into packed_ac */
+  uint32_t* order_population;    /* optional: 6144 zero counts (3 x 1984 + 3 x 64) */
+  uint32_t* present_mask;        /* optional device word: order families present */
+  uint32_t* used_order_mask;     /* optional device word: families with custom scans */
+  uint32_t* orders;              /* optional: [13][3][1024] scans in use */
+  uint32_t* device_error;        /* optional */
+} gjxl_b200_ac_token_outputs;
+
+typedef struct gjxl_b200_ac_tokens gjxl_b200_ac_tokens;
+GJXL_B200_API size_t gjxl_b200_ac_token_capacity(size_t blocks_x, size_t blocks_y);
+GJXL_B200_API int gjxl_b200_ac_tokens_create(size_t blocks_x, size_t blocks_y,
+                                             gjxl_b200_ac_tokens** out);
+GJXL_B200_API void gjxl_b200_ac_tokens_destroy(gjxl_b200_ac_tokens* tokens);
+GJXL_B200_API int gjxl_b200_ac_tokenize(
+    gjxl_b200_ac_tokens* tokens, const uint8_t* strategy_cells,
+    const int32_t* raw_quant_field, const int32_t* quantized_ac, size_t stride,
+    size_t plane_pitch, const gjxl_b200_block_context_map* map, int order_mode,
+    const gjxl_b200_ac_token_outputs* outputs, void* stream);
+
+/* ------------------------------------------------------------------------
  * Analysis session: the whole analysis path for one image extent.
  *
  * Replaces the reference's prepared pipeline objects and their GPU providers:

@@ -258,3 +258,89 @@ def quantization_pipeline(linear: np.ndarray, opsin: np.ndarray, target: float =
     _check(fn(_ptr(linear), w, h, _ptr(opsin), pw, ph, target, effort, x_qm_scale, b_qm_scale,
               ctypes.byref(outs)), "quantization_pipeline")
     return res
+
+
+# Block-context maps of the reference (src/codestream/simple_ac_context.h:27-31,
+# src/codestream/block_context_map.cpp:35-39): (qf thresholds, 3x13 map rows
+# per threshold segment, number of contexts).
+SIMPLE_BLOCK_CONTEXT_MAP = ((), bytes([0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1,
+                                      2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 3,
+                                      2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 3]), 4)
+JXL_DEFAULT_BLOCK_CONTEXT_MAP = ((), bytes([0, 1, 2, 2, 3, 3, 4, 5, 6, 6, 6, 6, 6,
+                                           7, 8, 9, 9, 10, 11, 12, 13, 14, 14, 14, 14, 14,
+                                           7, 8, 9, 9, 10, 11, 12, 13, 14, 14, 14, 14, 14]), 15)
+
+
+class _TokenRequest(ctypes.Structure):
+    _fields_ = [("qf_thresholds", c_void_p), ("threshold_count", c_size_t),
+                ("context_map", c_void_p), ("num_contexts", ctypes.c_uint32),
+                ("order_mode", c_int), ("orders", c_void_p), ("used_order_mask", c_void_p),
+                ("group_tokens", c_void_p), ("values", c_void_p), ("contexts", c_void_p),
+                ("capacity", c_size_t), ("histogram", c_void_p), ("fixed_dct8", c_int)]
+
+
+def pipeline_tokens(linear: np.ndarray, opsin: np.ndarray, target: float = 1.0, effort: int = 7,
+                    x_qm_scale: int = 3, b_qm_scale: int = 2,
+                    block_context_map=SIMPLE_BLOCK_CONTEXT_MAP, order_mode: int = 0,
+                    fixed_dct8: bool = False) -> dict:
+    """quantization_pipeline, then the reference's coefficient orders
+    (order_mode 0 natural, 1 full counts, 2 effort-7 sampled DCT8) and AC
+    tokens of every group with the given block-context map
+    (TokenizeSimpleAcGroupForEncoder, populations collected)."""
+    linear = np.ascontiguousarray(linear, np.float32)
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, h, w = linear.shape
+    _, ph, pw = opsin.shape
+    by, bx = ph // 8, pw // 8
+    ty, tx = (ph + 63) // 64, (pw + 63) // 64
+    gy, gx = (by + 31) // 32, (bx + 31) // 32
+    iterations = 0 if effort <= 5 else {6: 1, 7: 2, 8: 3}.get(effort, 4)
+    res = {
+        "initial_quant": np.zeros((by, bx), np.float32),
+        "strategy_mask": np.zeros((by, bx), np.float32),
+        "pixel_mask": np.zeros((ph, pw), np.float32),
+        "final_quant": np.zeros((by, bx), np.float32),
+        "block_distance": np.zeros((by, bx), np.float32),
+        "reconstructed": np.zeros((3, h, w), np.float32),
+        "cells": np.zeros((by, bx), np.uint8),
+        "raw_quant": np.zeros((by, bx), np.int32),
+        "quantizer_params": np.zeros(2, np.uint32),
+        "y_to_x": np.zeros((ty, tx), np.int8),
+        "y_to_b": np.zeros((ty, tx), np.int8),
+        "quantized_dc": np.zeros((3, by, bx), np.int32),
+        "dc": np.zeros((3, by, bx), np.float32),
+        "ac": np.zeros(3 * ph * pw, np.int32),
+        "group_used": np.zeros(gy * gx, np.uint64),
+        "score_history": np.zeros(iterations + 1, np.float64),
+    }
+    outs = _PipelineOutputs(**{k: v.ctypes.data for k, v in res.items()})
+    thresholds, cmap, num_contexts = block_context_map
+    thresholds = np.ascontiguousarray(np.array(thresholds, np.uint32))
+    cmap = np.frombuffer(bytes(cmap), np.uint8).copy()
+    assert cmap.size == 39 * (thresholds.size + 1)
+    capacity = 3 * ph * pw + 3 * by * bx
+    tok = {
+        "orders": np.zeros((13, 3, 1024), np.uint32),
+        "used_order_mask": np.zeros(1, np.uint32),
+        "group_tokens": np.zeros(gy * gx, np.uint64),
+        "values": np.zeros(capacity, np.uint32),
+        "contexts": np.zeros(capacity, np.uint16),
+        "histogram": np.zeros((num_contexts * 495, 128), np.uint32),
+    }
+    req = _TokenRequest(thresholds.ctypes.data if thresholds.size else None, thresholds.size,
+                        cmap.ctypes.data, num_contexts, order_mode, tok["orders"].ctypes.data,
+                        tok["used_order_mask"].ctypes.data, tok["group_tokens"].ctypes.data,
+                        tok["values"].ctypes.data, tok["contexts"].ctypes.data, capacity,
+                        tok["histogram"].ctypes.data, int(fixed_dct8))
+    fn = lib().gjxl_ref_pipeline_tokens
+    fn.argtypes = [_P, _Z, _Z, _P, _Z, _Z, _F, _I, _I, _I, ctypes.POINTER(_PipelineOutputs),
+                   ctypes.POINTER(_TokenRequest)]
+    fn.restype = c_int
+    _check(fn(_ptr(linear), w, h, _ptr(opsin), pw, ph, target, effort, x_qm_scale, b_qm_scale,
+              ctypes.byref(outs), ctypes.byref(req)), "pipeline_tokens")
+    total = int(tok["group_tokens"].sum())
+    tok["values"] = tok["values"][:total]
+    tok["contexts"] = tok["contexts"][:total]
+    tok["used_order_mask"] = int(tok["used_order_mask"][0])
+    res.update(tok)
+    return res

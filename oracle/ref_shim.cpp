@@ -33,6 +33,11 @@
 #include "codec/quantization_pipeline.h"
 #include "codec/quantization_pipeline_internal.h"
 #include "codec/vardct_frame.h"
+#include "codestream/ac_group.h"
+#include "codestream/block_context_map.h"
+#include "codestream/coefficient_order.h"
+#include "codestream/encoder.h"
+#include "codec/vardct_frame_view_internal.h"
 #include "core/ac_strategy.h"
 #include "core/image.h"
 #include "core/publication_vector.h"
@@ -413,16 +418,37 @@ struct RefPipelineOutputs {
   double* score_history;       // iterations + 1
 };
 
-GJXL_REF_API int gjxl_ref_quantization_pipeline(
+// Token request for the frame the pipeline produced: the coefficient orders
+// (codestream/coefficient_order.cpp ComputeSimpleCoefficientOrdersForEncoder;
+// order_mode 0 = natural scans, 1 = full counts, 2 = effort-7 sampled DCT8),
+// then TokenizeSimpleAcGroupForEncoder (codestream/ac_group.cpp:1245) for every
+// group with the given block-context map, collecting fixed populations.
+struct RefTokenRequest {
+  const uint32_t* qf_thresholds;   // threshold_count entries
+  size_t threshold_count;
+  const uint8_t* context_map;      // 3 * 13 * (threshold_count + 1)
+  uint32_t num_contexts;
+  int order_mode;
+  uint32_t* orders;                // [13][3][1024]: scan used per family/channel
+  uint32_t* used_order_mask;
+  size_t* group_tokens;            // per group token count
+  uint32_t* values;                // capacity entries, groups back to back
+  uint16_t* contexts;
+  size_t capacity;
+  uint32_t* histogram;             // [num_contexts * 495][128] symbol counts
+  int fixed_dct8;                  // pipeline option: DCT8 everywhere
+};
+
+static int RunPipeline(
   const float* linear, size_t width, size_t height, const float* opsin, size_t padded_width,
   size_t padded_height, float target, int effort, int x_qm_scale, int b_qm_scale,
-  RefPipelineOutputs* out) {
+  RefPipelineOutputs* out, const RefTokenRequest* tokens) {
   const Extent2D blocks{padded_width / 8, padded_height / 8};
   const Extent2D pixels{padded_width, padded_height};
   CpuQuantizationPipelineOptions options;
   options.butteraugli_target = target;
   options.uniform_initial_quantization = false;
-  options.fixed_dct8 = false;
+  options.fixed_dct8 = tokens != nullptr && tokens->fixed_dct8 != 0;
   options.dense_dct32_search = effort == 10;
   auto& aq = options.adaptive_quantization;
   aq.profile.loop_filter.gaborish = true;
@@ -492,5 +518,86 @@ GJXL_REF_API int gjxl_ref_quantization_pipeline(
     }
   }
   for (size_t i = 0; i < scores.size(); ++i) out->score_history[i] = scores[i];
+  if (tokens == nullptr) return 0;
+
+  SimpleCoefficientOrders orders;
+  if (tokens->order_mode != 0) {
+    status = codestream_internal::ComputeSimpleCoefficientOrdersForEncoder(
+      vardct_frame_internal::BorrowFrame(frame),
+      tokens->order_mode == 2 ? VarDctCoefficientOrderBehavior::kEffort7Dct8Sampled
+                              : VarDctCoefficientOrderBehavior::kFull,
+      &orders);
+    if (!status.ok()) return Fail(status);
+  }
+  codestream_internal::SimpleAcNaturalOrders natural;
+  status = codestream_internal::PrepareSimpleAcNaturalOrders(&natural);
+  if (!status.ok()) return Fail(status);
+  *tokens->used_order_mask = orders.used_order_mask;
+  // Scan per order family and channel: custom where used, else the natural
+  // scan of the family's representative strategy.
+  const AcStrategyType representative[13] = {
+    AcStrategyType::kDct8, AcStrategyType::kCount, AcStrategyType::kDct16x16,
+    AcStrategyType::kDct32x32, AcStrategyType::kDct16x8, AcStrategyType::kCount,
+    AcStrategyType::kDct32x16, AcStrategyType::kCount, AcStrategyType::kCount,
+    AcStrategyType::kCount, AcStrategyType::kCount, AcStrategyType::kCount,
+    AcStrategyType::kCount};
+  for (size_t family = 0; family < 13; ++family) {
+    for (size_t c = 0; c < 3; ++c) {
+      uint32_t* dst = tokens->orders + (family * 3 + c) * 1024;
+      if (orders.used_order_mask & (1u << family)) {
+        const auto& o = orders.orders[family][c];
+        std::copy(o.begin(), o.end(), dst);
+      } else if (representative[family] != AcStrategyType::kCount) {
+        const auto& o = natural.orders[static_cast<size_t>(representative[family])];
+        std::copy(o.begin(), o.end(), dst);
+      }
+    }
+  }
+  SimpleBlockContextMap map;
+  map.qf_thresholds.assign(tokens->qf_thresholds, tokens->qf_thresholds + tokens->threshold_count);
+  map.context_map.assign(tokens->context_map,
+                         tokens->context_map + 3 * 13 * (tokens->threshold_count + 1));
+  map.num_contexts = static_cast<uint8_t>(tokens->num_contexts);
+  const auto view = vardct_frame_internal::BorrowFrame(frame);
+  codestream_internal::SimpleAcTokenizationScratch scratch;
+  size_t written = 0;
+  for (size_t g = 0; g < frame.ac_group_count(); ++g) {
+    codestream_internal::SimpleAcGroupTokenData data;
+    status = codestream_internal::TokenizeSimpleAcGroupForEncoder(
+      view, orders, natural, map, g, /*collect_fixed_populations=*/true, &scratch, &data);
+    if (!status.ok()) return Fail(status);
+    if (written + data.values.size() > tokens->capacity) {
+      g_last_error = "token capacity exceeded";
+      return -1;
+    }
+    std::copy(data.values.begin(), data.values.end(), tokens->values + written);
+    std::copy(data.contexts.begin(), data.contexts.end(), tokens->contexts + written);
+    tokens->group_tokens[g] = data.values.size();
+    written += data.values.size();
+    for (const auto& population : data.context_populations) {
+      for (size_t k = 0; k < population.symbol_count; ++k) {
+        const auto& symbol = data.symbol_populations[population.symbol_offset + k];
+        tokens->histogram[static_cast<size_t>(population.context) * 128 + symbol.symbol] +=
+          symbol.count;
+      }
+    }
+  }
   return 0;
 }
+
+GJXL_REF_API int gjxl_ref_quantization_pipeline(
+  const float* linear, size_t width, size_t height, const float* opsin, size_t padded_width,
+  size_t padded_height, float target, int effort, int x_qm_scale, int b_qm_scale,
+  RefPipelineOutputs* out) {
+  return RunPipeline(linear, width, height, opsin, padded_width, padded_height, target, effort,
+                     x_qm_scale, b_qm_scale, out, nullptr);
+}
+
+GJXL_REF_API int gjxl_ref_pipeline_tokens(
+  const float* linear, size_t width, size_t height, const float* opsin, size_t padded_width,
+  size_t padded_height, float target, int effort, int x_qm_scale, int b_qm_scale,
+  RefPipelineOutputs* out, const RefTokenRequest* tokens) {
+  return RunPipeline(linear, width, height, opsin, padded_width, padded_height, target, effort,
+                     x_qm_scale, b_qm_scale, out, tokens);
+}
+
