@@ -10,7 +10,9 @@ Gaborish, initial CfL, AC-strategy costs and greedy merge, forward
 transforms, and the adaptive-quantization loop (three evaluations, each with
 quantizer, final CfL, AC/DC quantization, decoder-equivalent
 reconstruction, Gaborish + EPF, Butteraugli and per-transform reduction, and
-two field updates). The metric is megapixels per second (source pixels).
+two field updates), then the coefficient-order populations and scans and the
+AC tokens with their histogram. The metric is megapixels per second (source
+pixels).
 
 `value` is measured with the input already in device memory (CUDA events on
 the launching stream around K steps). `e2e` runs the same steps through
@@ -56,7 +58,7 @@ WORKLOAD = ("analysis half of one 4032x3024 synthetic sRGB image at d1.0 e7: sRG
             "matrix stats, initial AQ field, inverse Gaborish, initial CfL, AC-strategy costs "
             "+ greedy merge, forward transforms, 3 AQ evaluations (quantizer, final CfL, AC/DC "
             "quantization, reconstruction, Gaborish+EPF, Butteraugli, block reduction) with 2 "
-            "field updates")
+            "field updates, then coefficient-order populations/scans and AC tokens")
 
 
 def load_peaks() -> dict:
@@ -150,6 +152,17 @@ FP64_MAC_PER_TILE = 3 * 1_990_656
 KERNELS_PER_STEP = 15
 
 
+def d2h_bytes(session) -> int:
+    """Bytes the host-input entry point copies back per analysis: block maps
+    (strategy cells, initial and final quant fields, raw quant field, DC), CfL
+    maps, statistics, error words, score history, quantizer, group offsets and
+    the AC tokens (4-byte values, 2-byte contexts)."""
+    o = session.outputs
+    blocks, tiles = o.blocks_x * o.blocks_y, o.tiles_x * o.tiles_y
+    return (blocks * (1 + 4 + 4 + 4 + 12) + 2 * tiles + 12 + 12 + 8 * (o.iterations + 1) + 40
+            + 4 * (o.groups + 1) + 6 * o.host_token_count)
+
+
 def run_gpu(args) -> dict:
     import torch
     from gjxl_b200.session import AnalysisSession
@@ -229,8 +242,7 @@ def run_gpu(args) -> dict:
         "e2e": {"value": round(world * mp / (e2e_ms / 1e3), 3), "unit": "MP/s",
                 "ms_per_step": round(e2e_ms, 4),
                 "h2d_bytes_per_step": WIDTH * HEIGHT * 3,
-                "d2h_bytes_per_step": session.outputs.blocks_x * session.outputs.blocks_y * 5
-                + 2 * tiles + 16},
+                "d2h_bytes_per_step": d2h_bytes(session)},
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "gpu_launches": args.steps * KERNELS_PER_STEP,
         "roofline": {

@@ -37,13 +37,14 @@ enum Stage : int {
   kStageAcMerge,
   kStageTransforms,
   kStageAqLoop,
+  kStageTokenize,
   kStageCount,
 };
 
 const char* const kStageNames[kStageCount] = {
   "prepare_input",   "matrix_scale_stats", "initial_quant_field", "gaborish_inverse",
   "initial_cfl",     "ac_strategy_costs",  "ac_strategy_merge",   "forward_transforms",
-  "adaptive_quantization",
+  "adaptive_quantization", "ac_tokenize",
 };
 
 size_t Align(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -58,6 +59,27 @@ int AqIterations(int effort) {
 }
 
 std::once_flag g_tables_once[64];
+
+// The reference's initial block-context map (src/codestream/simple_ac_context.h:
+// 27-31; DefaultSimpleBlockContextMap, block_context_map.cpp:245-252): no
+// raw-quant thresholds, four contexts.
+gjxl_b200_block_context_map DefaultBlockContextMap() {
+  gjxl_b200_block_context_map m;
+  std::memset(&m, 0, sizeof(m));
+  const uint8_t rows[3][13] = {{0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1},
+                               {2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 3},
+                               {2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 3}};
+  std::memcpy(m.context_map, rows, sizeof(rows));
+  m.num_contexts = 4;
+  return m;
+}
+
+// ResolveCoefficientOrderBehavior (src/codestream/workflow.cpp:2064-2072) for
+// the default density and compression modes.
+int OrderMode(const gjxl_b200_options& o) {
+  if (o.order_mode >= 0) return o.order_mode;
+  return o.effort == 7 ? 2 : 1;
+}
 
 }  // namespace
 
@@ -113,6 +135,19 @@ struct Session {
   float* matrix_multipliers = nullptr;
   int* matrix_scales = nullptr;
   ButteraugliState* butteraugli = nullptr;
+  // AC tokens.
+  gjxl_b200_ac_tokens* tokens = nullptr;
+  size_t token_capacity = 0, groups = 0;
+  uint32_t* tok_values = nullptr;
+  uint16_t* tok_contexts = nullptr;
+  uint32_t* group_offsets = nullptr;
+  uint32_t* histogram = nullptr;
+  uint32_t* scans = nullptr;
+  uint32_t* order_masks = nullptr;
+  uint32_t* host_tok_values = nullptr;
+  uint16_t* host_tok_contexts = nullptr;
+  uint32_t* host_group_offsets = nullptr;
+  size_t host_token_count = 0;
   // Pinned host mirrors of the outputs.
   unsigned char* host_block = nullptr;
   uint8_t* host_cells = nullptr;
@@ -133,6 +168,8 @@ struct Session {
     if (arena) cudaFree(arena);
     if (host_block) cudaFreeHost(host_block);
     if (butteraugli) ButteraugliDestroy(butteraugli);
+    if (tokens) gjxl_b200_ac_tokens_destroy(tokens);
+    if (host_tok_values) cudaFreeHost(host_tok_values);
     if (events_created) {
       for (auto& e : events) cudaEventDestroy(e);
     }
@@ -196,6 +233,12 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->scores), 8 * sizeof(double)},
     {reinterpret_cast<void**>(&s->matrix_multipliers), 4 * sizeof(float)},
     {reinterpret_cast<void**>(&s->matrix_scales), 4 * sizeof(int)},
+    {reinterpret_cast<void**>(&s->tok_values), s->token_capacity * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->tok_contexts), s->token_capacity * sizeof(uint16_t)},
+    {reinterpret_cast<void**>(&s->group_offsets), (s->groups + 1) * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->histogram), (s->token_capacity ? 4 * 495 * 128 : 0) * 4},
+    {reinterpret_cast<void**>(&s->scans), 13 * 3 * 1024 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->order_masks), 4 * sizeof(uint32_t)},
   };
   size_t total = 0;
   for (const Item& item : items) total = Align(total, 256) + item.bytes;
@@ -236,6 +279,18 @@ int Allocate(Session* s) {
   s->host_qac = reinterpret_cast<int32_t*>(take(3 * plane * 4));
   status = ButteraugliCreate(s->width, s->height, 80.0f, &s->butteraugli);
   if (status != GJXL_B200_OK) return status;
+  if (s->options.tokenize) {
+    status = gjxl_b200_ac_tokens_create(s->bx, s->by, &s->tokens);
+    if (status != GJXL_B200_OK) return status;
+    void* mirror = nullptr;
+    status = CheckCuda(cudaMallocHost(&mirror, s->token_capacity * 6 + (s->groups + 1) * 4 + 64),
+                       "session: token mirrors");
+    if (status != GJXL_B200_OK) return status;
+    s->host_tok_values = static_cast<uint32_t*>(mirror);
+    s->host_tok_contexts = reinterpret_cast<uint16_t*>(s->host_tok_values + s->token_capacity);
+    s->host_group_offsets = reinterpret_cast<uint32_t*>(
+      reinterpret_cast<unsigned char*>(mirror) + Align(s->token_capacity * 6, 16));
+  }
   if (s->options.profile_stages) {
     for (auto& e : s->events) {
       status = CheckCuda(cudaEventCreate(&e), "session: cudaEventCreate");
@@ -301,7 +356,7 @@ int RunAq(Session* s, cudaStream_t stream) {
 
 int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
         cudaStream_t stream) {
-  GJXL_TRY(CheckCuda(cudaMemsetAsync(s->error, 0, sizeof(uint32_t), stream),
+  GJXL_TRY(CheckCuda(cudaMemsetAsync(s->error, 0, 4 * sizeof(uint32_t), stream),
                      "session: clear error"));
   const float target = s->options.butteraugli_target;
   Mark(s, kStagePrepare, stream);
@@ -342,6 +397,23 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
                                   stream));
   Mark(s, kStageTransforms, stream);
   GJXL_TRY(RunAq(s, stream));
+  Mark(s, kStageTokenize, stream);
+  if (s->tokens != nullptr) {
+    const gjxl_b200_block_context_map map = DefaultBlockContextMap();
+    gjxl_b200_ac_token_outputs outs;
+    std::memset(&outs, 0, sizeof(outs));
+    outs.token_values = s->tok_values;
+    outs.token_contexts = s->tok_contexts;
+    outs.token_capacity = s->token_capacity;
+    outs.group_offsets = s->group_offsets;
+    outs.histogram = s->histogram;
+    outs.orders = s->scans;
+    outs.present_mask = s->order_masks;
+    outs.used_order_mask = s->order_masks + 1;
+    outs.device_error = s->error + 2;
+    GJXL_TRY(gjxl_b200_ac_tokenize(s->tokens, s->cells, s->raw, s->qac, s->pw, s->pitch, &map,
+                                   OrderMode(s->options), &outs, stream));
+  }
   Mark(s, kStageCount, stream);
   // Merge the Butteraugli error word into the session error word.
   GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->error + 1, ButteraugliErrorWord(s->butteraugli),
@@ -362,15 +434,18 @@ int CopyOutputs(Session* s, cudaStream_t stream) {
     {s->host_cfl, s->final_y_to_x, tiles},
     {s->host_cfl + tiles, s->final_y_to_b, tiles},
     {s->host_stats, s->stats, 3 * sizeof(float)},
-    {s->host_error, s->error, 2 * sizeof(uint32_t)},
+    {s->host_error, s->error, 3 * sizeof(uint32_t)},
     {s->host_final_quant, s->field, blocks * sizeof(float)},
     {s->host_raw, s->raw, blocks * sizeof(int32_t)},
     {s->host_qdc, s->qdc, 3 * blocks * sizeof(int32_t)},
     {s->host_scores, s->scores, (s->iterations + 1) * sizeof(double)},
     {s->host_quantizer, s->quantizer, sizeof(AqQuantizer)},
-    {s->host_qac, s->qac, 3 * plane * sizeof(int32_t)},
+    // Quantized AC returns to the host only without tokenization (the tokens
+    // carry it otherwise).
+    {s->host_qac, s->qac, s->tokens != nullptr ? 0 : 3 * plane * sizeof(int32_t)},
   };
   for (const auto& c : copies) {
+    if (c.bytes == 0) continue;
     GJXL_TRY(CheckCuda(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, stream),
                        "session: output copy"));
   }
@@ -392,6 +467,8 @@ extern "C" void gjxl_b200_default_options(gjxl_b200_options* options) {
   options->effort = 7;
   options->intensity_target = 255.0f;
   options->profile_stages = 0;
+  options->tokenize = 1;
+  options->order_mode = -1;
 }
 
 extern "C" int gjxl_b200_session_create(size_t width, size_t height,
@@ -413,6 +490,9 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
   if (!std::isfinite(o.butteraugli_target) || o.butteraugli_target <= 0.0f ||
       !std::isfinite(o.intensity_target) || o.intensity_target <= 0.0f) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: invalid options");
+  }
+  if (o.order_mode < -1 || o.order_mode > 2) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: order_mode is -1..2");
   }
   if (o.effort < 5 || o.effort > 10) {
     return SetError(GJXL_B200_UNSUPPORTED,
@@ -439,6 +519,8 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
   s->ty = (s->by + 7) / 8;
   s->options = o;
   s->iterations = AqIterations(o.effort);
+  s->groups = ((s->bx + 31) / 32) * ((s->by + 31) / 32);
+  s->token_capacity = o.tokenize ? gjxl_b200_ac_token_capacity(s->bx, s->by) : 0;
   status = Allocate(s);
   if (status != GJXL_B200_OK) {
     delete s;
@@ -474,7 +556,27 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
   GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->pixels, host_pixels, bytes, cudaMemcpyHostToDevice, st),
                      "session: input upload"));
   GJXL_TRY(Run(s, s->pixels, row_stride, channels, st));
-  return CopyOutputs(s, st);
+  GJXL_TRY(CopyOutputs(s, st));
+  s->host_token_count = 0;
+  if (s->tokens != nullptr) {
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_group_offsets, s->group_offsets,
+                                       (s->groups + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                       st),
+                       "session: group offsets"));
+    GJXL_TRY(CheckCuda(cudaStreamSynchronize(st), "session: analysis"));
+    const size_t total = s->host_group_offsets[s->groups];
+    if (total > s->token_capacity) {
+      return SetError(GJXL_B200_INTERNAL, "session_analyze_host: token count exceeds capacity");
+    }
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_tok_values, s->tok_values, total * 4,
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: token values"));
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_tok_contexts, s->tok_contexts, total * 2,
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: token contexts"));
+    s->host_token_count = total;
+  }
+  return CheckCuda(cudaStreamSynchronize(st), "session: analysis");
 }
 
 extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_outputs* out) {
@@ -530,6 +632,19 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   out->host_score_history = s->host_scores;
   out->host_quantizer_params = reinterpret_cast<const uint32_t*>(s->host_quantizer);
   out->host_quantized_ac = s->host_qac;
+  out->groups = s->groups;
+  if (s->tokens != nullptr) {
+    out->token_values = s->tok_values;
+    out->token_contexts = s->tok_contexts;
+    out->group_offsets = s->group_offsets;
+    out->token_histogram = s->histogram;
+    out->scans = s->scans;
+    out->order_masks = s->order_masks;
+    out->host_token_values = s->host_tok_values;
+    out->host_token_contexts = s->host_tok_contexts;
+    out->host_group_offsets = s->host_group_offsets;
+  }
+  out->host_token_count = s->host_token_count;
   out->device_bytes = s->arena_bytes;
   return GJXL_B200_OK;
 }

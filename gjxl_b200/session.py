@@ -16,7 +16,8 @@ from . import _lib
 
 class Options(Structure):
     _fields_ = [("struct_size", c_size_t), ("butteraugli_target", c_float), ("effort", c_int),
-                ("intensity_target", c_float), ("profile_stages", c_int)]
+                ("intensity_target", c_float), ("profile_stages", c_int), ("tokenize", c_int),
+                ("order_mode", c_int)]
 
 
 class Outputs(Structure):
@@ -33,7 +34,10 @@ class Outputs(Structure):
             "host_initial_quant_field", "host_y_to_x", "host_y_to_b", "host_matrix_scale_stats",
             "host_device_error", "host_quant_field", "host_raw_quant_field", "host_quantized_dc",
             "host_score_history", "host_quantizer_params", "host_quantized_ac")] + [
-        ("device_bytes", c_size_t)]
+        ("groups", c_size_t)] + [(n, c_void_p) for n in (
+            "token_values", "token_contexts", "group_offsets", "token_histogram", "scans",
+            "order_masks", "host_token_values", "host_token_contexts", "host_group_offsets")] + [
+        ("host_token_count", c_size_t), ("device_bytes", c_size_t)]
 
 
 _BOUND = False
@@ -74,7 +78,8 @@ class AnalysisSession:
     """Runs the B200 analysis path for images of one extent."""
 
     def __init__(self, width: int, height: int, butteraugli_target: float = 1.0,
-                 effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False):
+                 effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False,
+                 tokenize: bool = True, order_mode: int = -1):
         _bind()
         lib = _lib.load()
         opts = Options()
@@ -83,6 +88,8 @@ class AnalysisSession:
         opts.effort = effort
         opts.intensity_target = intensity_target
         opts.profile_stages = int(profile_stages)
+        opts.tokenize = int(tokenize)
+        opts.order_mode = order_mode
         handle = c_void_p()
         _check(lib.gjxl_b200_session_create(width, height, ctypes.byref(opts),
                                             ctypes.byref(handle)), "gjxl_b200_session_create")
@@ -111,9 +118,12 @@ class AnalysisSession:
     def analyze_host(self, host_pixels: np.ndarray, stream: int = 0):
         assert host_pixels.dtype == np.uint8 and host_pixels.flags["C_CONTIGUOUS"]
         h, w, ch = host_pixels.shape
-        _check(_lib.load().gjxl_b200_session_analyze_host(self.handle, host_pixels.ctypes.data,
-                                                          w * ch, ch, stream),
+        lib = _lib.load()
+        _check(lib.gjxl_b200_session_analyze_host(self.handle, host_pixels.ctypes.data,
+                                                  w * ch, ch, stream),
                "gjxl_b200_session_analyze_host")
+        _check(lib.gjxl_b200_session_outputs(self.handle, ctypes.byref(self.outputs)),
+               "gjxl_b200_session_outputs")
 
     def stage_times(self) -> dict[str, float]:
         lib = _lib.load()
@@ -137,8 +147,8 @@ class AnalysisSession:
 
     def host_error(self) -> int:
         """Analysis error word OR'ed with the Butteraugli error word."""
-        words = self._host("host_device_error", ctypes.c_uint32, (2,))
-        return int(words[0]) | int(words[1])
+        words = self._host("host_device_error", ctypes.c_uint32, (3,))
+        return int(words[0]) | int(words[1]) | int(words[2])
 
     def host_results(self) -> dict[str, np.ndarray]:
         """Host copies of the final frame's results (after analyze_host)."""
@@ -156,6 +166,18 @@ class AnalysisSession:
             "score_history": self._host("host_score_history", ctypes.c_double,
                                         (o.iterations + 1,)),
             "quantizer_params": self._host("host_quantizer_params", ctypes.c_uint32, (2,)),
+        } | self.host_tokens() | ({} if o.host_token_values else {
             "quantized_ac": self._host("host_quantized_ac", ctypes.c_int32,
-                                       (3, o.padded_height, o.padded_width)),
+                                       (3, o.padded_height, o.padded_width))})
+
+    def host_tokens(self) -> dict[str, np.ndarray]:
+        """AC tokens of the last analyze_host (empty without tokenization)."""
+        o = self.outputs
+        if not o.host_token_values:
+            return {}
+        n = o.host_token_count
+        return {
+            "token_values": self._host("host_token_values", ctypes.c_uint32, (n,)),
+            "token_contexts": self._host("host_token_contexts", ctypes.c_uint16, (n,)),
+            "group_offsets": self._host("host_group_offsets", ctypes.c_uint32, (o.groups + 1,)),
         }

@@ -319,6 +319,10 @@ typedef struct gjxl_b200_options {
   int effort;               /* 5..10 (mixed-transform search); default 7 */
   float intensity_target;   /* XYB intensity target; the workflow uses 255 */
   int profile_stages;       /* nonzero: record CUDA events around each stage */
+  int tokenize;             /* nonzero (default): AC tokens after the last evaluation */
+  int order_mode;           /* -1 (default): by effort, as the reference resolves it
+                               (effort 7: 2, else 1); or 0/1/2 as for
+                               gjxl_b200_ac_tokenize */
 } gjxl_b200_options;
 
 /* Session results. The adaptive-quantization fields mirror the reference's
@@ -359,7 +363,7 @@ typedef struct gjxl_b200_outputs {
   const float* distance_map;        /* width x height */
   const double* score_history;      /* iterations + 1 maxima */
   const uint32_t* quantizer_params; /* global_scale, quant_dc, ... */
-  const uint32_t* device_error;     /* [0] analysis, [1] Butteraugli */
+  const uint32_t* device_error;     /* [0] analysis, [1] Butteraugli, [2] tokens */
   /* Pinned host mirrors, filled by gjxl_b200_session_analyze_host once the
    * stream has completed. */
   const uint8_t* host_strategy_cells;
@@ -367,13 +371,28 @@ typedef struct gjxl_b200_outputs {
   const int8_t* host_y_to_x;        /* final CfL map */
   const int8_t* host_y_to_b;
   const float* host_matrix_scale_stats;
-  const uint32_t* host_device_error; /* 2 words */
+  const uint32_t* host_device_error; /* 3 words */
   const float* host_quant_field;
   const int32_t* host_raw_quant_field;
   const int32_t* host_quantized_dc;
   const double* host_score_history;
   const uint32_t* host_quantizer_params;
   const int32_t* host_quantized_ac;
+  /* AC tokens (tokenize != 0), with the reference's initial block-context
+   * map (src/codestream/simple_ac_context.h:27-31): device views, then host
+   * mirrors holding host_token_count tokens after
+   * gjxl_b200_session_analyze_host. */
+  size_t groups;
+  const uint32_t* token_values;
+  const uint16_t* token_contexts;
+  const uint32_t* group_offsets;      /* groups + 1 */
+  const uint32_t* token_histogram;    /* [4 * 495][128] */
+  const uint32_t* scans;              /* [13][3][1024] coefficient scans in use */
+  const uint32_t* order_masks;        /* present families, families with custom scans */
+  const uint32_t* host_token_values;
+  const uint16_t* host_token_contexts;
+  const uint32_t* host_group_offsets;
+  size_t host_token_count;
   size_t device_bytes;
 } gjxl_b200_outputs;
 
@@ -390,7 +409,9 @@ GJXL_B200_API int gjxl_b200_session_analyze(gjxl_b200_session* session,
                                             size_t row_stride_bytes,
                                             int channels, void* stream);
 /* Host input: one host-to-device copy of the packed pixels, the analysis,
- * and device-to-host copies of the results into the host mirrors. */
+ * and device-to-host copies of the results into the host mirrors. Returns
+ * once the stream has completed and the mirrors are filled (the token count
+ * is known only then). */
 GJXL_B200_API int gjxl_b200_session_analyze_host(gjxl_b200_session* session,
                                                  const uint8_t* host_pixels,
                                                  size_t row_stride_bytes,

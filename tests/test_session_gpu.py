@@ -99,6 +99,9 @@ def check_block_distance(s: AnalysisSession, got: dict, want: dict) -> None:
 
 
 def reference(img: np.ndarray, effort: int = 7, target: float = 1.0):
+    """The reference pipeline, then its coefficient orders (effort 7: the
+    sampled behaviour, else full counts) and AC tokens with the initial
+    block-context map, as the session tokenizes by default."""
     h, w, _ = img.shape
     lin = ref.srgb8_to_linear(img)
     opsin = ref.linear_to_padded_opsin(lin)
@@ -106,7 +109,14 @@ def reference(img: np.ndarray, effort: int = 7, target: float = 1.0):
     # Below effort 7 the statistics are not gathered and select from zeros.
     xs, bs = restate.select_matrix_scales(stats if effort >= 7 else np.zeros(3, np.float32),
                                           target)
-    return opsin, stats, ref.quantization_pipeline(lin, opsin, target, effort, xs, bs)
+    return opsin, stats, ref.pipeline_tokens(lin, opsin, target, effort, xs, bs,
+                                             ref.SIMPLE_BLOCK_CONTEXT_MAP,
+                                             2 if effort == 7 else 1)
+
+
+def device_quantized_ac(s: AnalysisSession) -> np.ndarray:
+    o = s.outputs
+    return device_to_host(o.quantized_ac, (3, o.padded_height, o.padded_width), np.int32)
 
 
 def compare_front_half(s: AnalysisSession, got: dict, want: dict, stats: np.ndarray,
@@ -136,9 +146,13 @@ def compare_loop_exact(s: AnalysisSession, got: dict, want: dict) -> None:
     assert_bitexact(got["y_to_x"], want["y_to_x"], "final y_to_x")
     assert_bitexact(got["y_to_b"], want["y_to_b"], "final y_to_b")
     assert_bitexact(got["quantized_dc"], want["quantized_dc"], "quantized DC")
-    ac = footprint_to_group_order(got["quantized_ac"], got["cells"])
+    ac = footprint_to_group_order(device_quantized_ac(s), got["cells"])
     assert ac.size == int(want["group_used"].sum()) * 3
     assert_bitexact(ac, want["ac"][:ac.size], "quantized AC (group order)")
+    offsets = got["group_offsets"].astype(np.int64)
+    assert_bitexact(np.diff(offsets), want["group_tokens"].astype(np.int64), "group tokens")
+    assert_bitexact(got["token_values"], want["values"], "token values")
+    assert_bitexact(got["token_contexts"], want["contexts"], "token contexts")
     assert_bitexact(got["score_history"], want["score_history"], "score history")
     dc = device_to_host(o.dc, (3, by, bx), np.float32)
     assert_bitexact(dc, want["dc"], "dequantized DC")
@@ -160,7 +174,7 @@ def compare_loop_fed_back(s: AnalysisSession, got: dict, want: dict) -> int:
     bad = (differing_blocks(got["final_quant"], want["final_quant"])
            | differing_blocks(got["raw_quant"], want["raw_quant"])
            | differing_blocks(got["quantized_dc"], want["quantized_dc"])
-           | differing_blocks(got["quantized_ac"],
+           | differing_blocks(device_quantized_ac(s),
                               group_order_to_footprint(want["ac"], got["cells"]), pixels=True))
     cfl = differing_blocks(got["y_to_x"], want["y_to_x"]) | differing_blocks(got["y_to_b"],
                                                                                  want["y_to_b"])
@@ -228,7 +242,8 @@ def test_session_repeated_analysis_is_stable(cuda):
     torch.cuda.synchronize()
     again = s.host_results()
     fresh = run_session(b).host_results()
-    for key in ("final_quant", "raw_quant", "quantized_dc", "quantized_ac", "score_history"):
+    for key in ("final_quant", "raw_quant", "quantized_dc", "score_history", "token_values",
+                "token_contexts", "group_offsets"):
         assert_bitexact(again[key], fresh[key], key)
     s.close()
 
