@@ -217,31 +217,57 @@ struct PopulationParams {
   uint32_t* present_mask;
 };
 
+// One CTA per group. The group's anchors are first listed per family; then,
+// family by family and channel by channel, each thread owns one physical
+// index (and a share of the anchors when the family has fewer than 256
+// indices) and counts zeros in a register, so shared-memory atomics happen
+// once per thread and index, not once per coefficient.
 __global__ void __launch_bounds__(256) PopulationKernel(const __grid_constant__ PopulationParams p) {
   __shared__ uint32_t counts[kPopulationCount];
+  __shared__ short2 anchors[5][kGroupBlocks * kGroupBlocks];
+  __shared__ uint8_t sampled[kGroupBlocks * kGroupBlocks];
+  __shared__ int anchor_count[5];
   __shared__ uint32_t present;
   for (int i = threadIdx.x; i < kPopulationCount; i += blockDim.x) counts[i] = 0;
+  if (threadIdx.x < 5) anchor_count[threadIdx.x] = 0;
   if (threadIdx.x == 0) present = 0;
   __syncthreads();
   const int x0 = (blockIdx.x % p.groups_x) * kGroupBlocks;
   const int y0 = (blockIdx.x / p.groups_x) * kGroupBlocks;
   const int w = min(kGroupBlocks, p.blocks_x - x0), h = min(kGroupBlocks, p.blocks_y - y0);
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  // One warp per anchor: lanes own physical indices i = lane + 32k.
-  for (int b = warp; b < w * h; b += blockDim.x / 32) {
+  for (int b = threadIdx.x; b < w * h; b += blockDim.x) {
     const int bx = x0 + b % w, by = y0 + b / w;
     const TaskShape t = ShapeAt(p.cells, by * p.blocks_x + bx);
     if (t.family < 0) continue;
-    if (lane == 0) atomicOr(&present, 1u << t.family);
-    const bool sampled = t.family == 0 && p.sample[by * p.blocks_x + bx];
+    const int fi = t.family == 0 ? 0 : t.family == 2 ? 1 : t.family == 3 ? 2 : t.family == 4 ? 3 : 4;
+    const int slot = atomicAdd(&anchor_count[fi], 1);
+    anchors[fi][slot] = make_short2(static_cast<short>(bx), static_cast<short>(by));
+    if (fi == 0) sampled[slot] = p.sample[by * p.blocks_x + bx];
+    atomicOr(&present, 1u << t.family);
+  }
+  __syncthreads();
+  for (int fi = 0; fi < 5; ++fi) {
+    const int count = anchor_count[fi];
+    if (count == 0) continue;
+    const int family = FamilyOfIndex(fi), n = FamilySize(family);
+    const int shares = n >= static_cast<int>(blockDim.x) ? 1 : static_cast<int>(blockDim.x) / n;
+    const int share = static_cast<int>(threadIdx.x) / (n >= static_cast<int>(blockDim.x) ? static_cast<int>(blockDim.x) : n);
+    if (share >= shares) continue;
     for (int c = 0; c < 3; ++c) {
-      uint32_t* full = counts + c * kPopulationStride + PopulationOffset(t.family);
-      for (int i = lane; i < t.n; i += 32) {
-        const bool zero = Coefficient(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_w, i) == 0;
-        if (zero) {
-          atomicAdd(full + i, 1u);
-          if (sampled) atomicAdd(counts + kPopulationFull + c * 64 + i, 1u);
+      for (int i = static_cast<int>(threadIdx.x) % n; i < n; i += blockDim.x) {
+        uint32_t zeros = 0, zeros_sampled = 0;
+        for (int a = share; a < count; a += shares) {
+          const short2 anchor = anchors[fi][a];
+          // Both orientations of a rectangular family share physical indices;
+          // the footprint width of this anchor decides where index i lies.
+          const TaskShape t = ShapeAt(p.cells, anchor.y * p.blocks_x + anchor.x);
+          const bool zero = Coefficient(p.qac, p.stride, p.pitch, c, anchor.x, anchor.y,
+                                        t.footprint_w, i) == 0;
+          zeros += zero;
+          if (fi == 0 && sampled[a]) zeros_sampled += zero;
         }
+        if (zeros) atomicAdd(counts + c * kPopulationStride + PopulationOffset(family) + i, zeros);
+        if (zeros_sampled) atomicAdd(counts + kPopulationFull + c * 64 + i, zeros_sampled);
       }
     }
   }

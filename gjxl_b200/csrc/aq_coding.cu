@@ -696,10 +696,16 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   int32_t (*Q)[kDcGroup] = r.q[c];
   int32_t (*E)[kDcGroup] = r.e[c];
   __syncthreads();
+  // The DC sample of the next position is loaded one wave ahead, so its
+  // global-memory latency overlaps this wave's work and barrier.
+  const size_t row_index = static_cast<size_t>(gy0 + min(y, gh - 1)) * stride + gx0;
+  float pending = y < gh ? source[row_index] : 0.0f;
   const int waves = (gw - 1) + 2 * (gh - 1) + 2;
   for (int t = 0; t < waves; ++t) {
     const int x = t - lag - 2 * y;
     if (y < gh && x >= 0 && x < gw) {
+      const float dc_value = pending;
+      if (x + 1 < gw) pending = source[row_index + x + 1];
       const int s = x & 7, sw = (x - 1) & 7, sne = (x + 1 < gw ? x + 1 : x) & 7;
       const int snw = (x ? x - 1 : x) & 7;
       const int up = y - 1, up2 = y - 2;
@@ -759,8 +765,8 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
       }
       const int64_t predicted = (prediction + 3) >> 3;
       // Quantize the residual (dc_quantization.cpp:178-199).
-      const size_t index = static_cast<size_t>(gy0 + y) * stride + gx0 + x;
-      float value = source[index];
+      const size_t index = row_index + x;
+      float value = dc_value;
       if (c == 2) value = fmaf(-static_cast<float>(r.q[1][s][y]), step_y, value);
       float residual = value * inverse_step;
       residual -= static_cast<float>(predicted);

@@ -47,34 +47,42 @@ __device__ __forceinline__ int MirrorB(int c, int size) {
   return c;
 }
 
-__device__ __forceinline__ float HorizontalSeparable5(const float* row, int x, int w,
-                                                      const Kernel17& k) {
-  float r = row[x] * k.w5[0];
-  r = (row[MirrorB(x - 1, w)] + row[MirrorB(x + 1, w)]) * k.w5[1] + r;
-  r = (row[MirrorB(x - 2, w)] + row[MirrorB(x + 2, w)]) * k.w5[2] + r;
-  return r;
-}
+// Separable5 (butteraugli_internal.cpp:222-260) on a 32x8 output tile: the
+// mirrored input window (tile + 2 on each side) is staged in shared memory,
+// the horizontal 5-tap pass runs over the window's 12 rows, then the vertical
+// pass, with the reference's operation order for every output.
+constexpr int kB5W = 32, kB5H = 8;
 
-// Separable5 (butteraugli_internal.cpp:222-260), one output per thread.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kB5W * kB5H)
 Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
             const __grid_constant__ Kernel17 k) {
-  const int plane = blockIdx.y;
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= w * h) return;
-  const int x = i % w, y = i / w;
+  __shared__ float window[kB5H + 4][kB5W + 4];
+  __shared__ float horizontal[kB5H + 4][kB5W];
+  const int plane = blockIdx.z;
+  const int x0 = blockIdx.x * kB5W, y0 = blockIdx.y * kB5H;
   const float* base = in + plane * pitch;
-  const float center = HorizontalSeparable5(base + static_cast<size_t>(y) * w, x, w, k);
-  const float top1 = HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y - 1, h)) * w, x, w, k);
-  const float bottom1 =
-    HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y + 1, h)) * w, x, w, k);
-  const float top2 = HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y - 2, h)) * w, x, w, k);
-  const float bottom2 =
-    HorizontalSeparable5(base + static_cast<size_t>(MirrorB(y + 2, h)) * w, x, w, k);
-  float r = center * k.w5[0];
-  r = (top1 + bottom1) * k.w5[1] + r;
-  r = (top2 + bottom2) * k.w5[2] + r;
-  out[plane * pitch + i] = r;
+  const int tid = threadIdx.y * kB5W + threadIdx.x;
+  for (int i = tid; i < (kB5H + 4) * (kB5W + 4); i += kB5W * kB5H) {
+    const int ty = i / (kB5W + 4), tx = i % (kB5W + 4);
+    window[ty][tx] = base[static_cast<size_t>(MirrorB(y0 + ty - 2, h)) * w + MirrorB(x0 + tx - 2, w)];
+  }
+  __syncthreads();
+  for (int i = tid; i < (kB5H + 4) * kB5W; i += kB5W * kB5H) {
+    const int ty = i / kB5W, tx = i % kB5W;
+    const float* row = window[ty] + tx + 2;
+    float r = row[0] * k.w5[0];
+    r = (row[-1] + row[1]) * k.w5[1] + r;
+    r = (row[-2] + row[2]) * k.w5[2] + r;
+    horizontal[ty][tx] = r;
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const int ty = threadIdx.y + 2, tx = threadIdx.x;
+  float r = horizontal[ty][tx] * k.w5[0];
+  r = (horizontal[ty - 1][tx] + horizontal[ty + 1][tx]) * k.w5[1] + r;
+  r = (horizontal[ty - 2][tx] + horizontal[ty + 2][tx]) * k.w5[2] + r;
+  out[plane * pitch + static_cast<size_t>(y) * w + x] = r;
 }
 
 // One tap row of ConvolutionWithTranspose at position x of a line of length n
@@ -111,16 +119,57 @@ __device__ __forceinline__ float ConvolveLine(const float* src, int step, int x,
   return sum * scale;
 }
 
+// Register-blocked blur along one axis: each thread computes kRun
+// consecutive outputs of one line from a window of kRun + 2R samples held in
+// registers (the interior pair-sum order of ConvolveLine for every output),
+// and falls back to ConvolveLine for outputs within R of either end.
+constexpr int kRun = 8;
+
+template <int R>
+__device__ __forceinline__ void ConvolveRun(const float* src, int step, int first, int n,
+                                            const Kernel17& k, float* out, int out_step,
+                                            int count) {
+  if (first >= R && first + kRun - 1 < n - R) {
+    float v[kRun + 2 * R];
+    const float* s = src + static_cast<ptrdiff_t>(first - R) * step;
+#pragma unroll
+    for (int j = 0; j < kRun + 2 * R; ++j) v[j] = s[static_cast<ptrdiff_t>(j) * step];
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) {
+      float sums[4];
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const float term = (v[o + i] + v[o + 2 * R - i]) * k.scaled[i];
+        if (i < 4) {
+          sums[i] = term;
+        } else {
+          sums[i & 3] += term;
+        }
+      }
+      float r = v[o + R] * k.scaled[R];
+#pragma unroll
+      for (int i = 0; i < (R < 4 ? R : 4); ++i) r = r + sums[i];
+      out[static_cast<ptrdiff_t>(o) * out_step] = r;
+    }
+    return;
+  }
+  for (int o = 0; o < count; ++o) {
+    out[static_cast<ptrdiff_t>(o) * out_step] = ConvolveLine<R>(src, step, first + o, n, k);
+  }
+}
+
 template <int R>
 __global__ void __launch_bounds__(kThreads)
 BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
                const __grid_constant__ Kernel17 k) {
   const int plane = blockIdx.y;
+  const int runs = (w + kRun - 1) / kRun;
   const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= w * h) return;
-  const int x = i % w, y = i / w;
+  if (i >= runs * h) return;
+  const int x = (i % runs) * kRun, y = i / runs;
   const float* row = in + plane * in_pitch + static_cast<size_t>(y) * w;
-  out[plane * out_pitch + i] = ConvolveLine<R>(row, 1, x, w, k);
+  ConvolveRun<R>(row, 1, x, w, k, out + plane * out_pitch + static_cast<size_t>(y) * w + x, 1,
+                 min(kRun, w - x));
 }
 
 template <int R>
@@ -128,11 +177,15 @@ __global__ void __launch_bounds__(kThreads)
 BlurColumnsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
                   const __grid_constant__ Kernel17 k) {
   const int plane = blockIdx.y;
+  const int runs = (h + kRun - 1) / kRun;
   const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= w * h) return;
-  const int x = i % w, y = i / w;
+  if (i >= w * runs) return;
+  // Consecutive threads take consecutive columns of one run of rows, so the
+  // window loads are coalesced across the warp.
+  const int x = i % w, y = (i / w) * kRun;
   const float* column = in + plane * in_pitch + x;
-  out[plane * out_pitch + i] = ConvolveLine<R>(column, w, y, h, k);
+  ConvolveRun<R>(column, w, y, h, k, out + plane * out_pitch + static_cast<size_t>(y) * w + x, w,
+                 min(kRun, h - y));
 }
 
 // --------------------------------------------------------------------------
@@ -723,10 +776,12 @@ namespace {
 template <int R>
 void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pitch, int planes,
                 const Kernel17& k, cudaStream_t stream) {
-  const size_t n = static_cast<size_t>(w) * h;
-  dim3 grid(Blocks(n), planes);
-  BlurRowsKernel<R><<<grid, kThreads, 0, stream>>>(in, tmp, w, h, pitch, pitch, k);
-  BlurColumnsKernel<R><<<grid, kThreads, 0, stream>>>(tmp, out, w, h, pitch, pitch, k);
+  const size_t row_runs = static_cast<size_t>((w + kRun - 1) / kRun) * h;
+  const size_t column_runs = static_cast<size_t>(w) * ((h + kRun - 1) / kRun);
+  BlurRowsKernel<R><<<dim3(Blocks(row_runs), planes), kThreads, 0, stream>>>(in, tmp, w, h, pitch,
+                                                                          pitch, k);
+  BlurColumnsKernel<R><<<dim3(Blocks(column_runs), planes), kThreads, 0, stream>>>(
+    tmp, out, w, h, pitch, pitch, k);
 }
 
 // Opsin dynamics + frequency separation of one image at one scale
@@ -747,7 +802,8 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
                       cudaMemcpyDeviceToDevice, stream);
     dense = s.linear_tmp;
   }
-  Blur5Kernel<<<dim3(Blocks(n), 3), kThreads, 0, stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
+  Blur5Kernel<<<dim3((s.w + kB5W - 1) / kB5W, (s.h + kB5H - 1) / kB5H, 3), dim3(kB5W, kB5H), 0,
+                stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
   OpsinDynamicsKernel<<<Blocks(n), kThreads, 0, stream>>>(dense, s.w, n, s.blur3, s.xyb, s.w, s.h,
                                                           n, st.intensity_target, st.error);
   // LF: 33-tap blur of the three XYB planes straight into the LF planes.
