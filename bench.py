@@ -140,16 +140,46 @@ def barrier(world: int):
         dist.barrier()
 
 
-# Algorithmic work of the dominant kernel family (AC-strategy candidate costs):
-# per 64x64 tile 52,480 coefficient evaluations per channel; each forward and
-# inverse separable DCT costs (W + H) double-precision multiply-adds per
-# coefficient -> 1,990,656 MACs per tile per channel (x3 channels).
-FP64_MAC_PER_TILE = 3 * 1_990_656
+# Families searched per 64x64 tile (ac_strategy_search_policy.h:21-29): pixel
+# extent (W, H), covered blocks and anchor step.
+FAMILIES = [(8, 8, 1, 1, 1), (8, 16, 1, 2, 1), (16, 8, 2, 1, 1), (16, 16, 2, 2, 1),
+            (16, 32, 2, 4, 2), (32, 16, 4, 2, 2), (32, 32, 4, 4, 2)]
 
-# Kernels of this library launched per analysis step: prepare_input,
-# matrix_scale_stats, 3 initial-quant kernels, inverse Gaborish, initial CfL,
-# 7 candidate-cost families, greedy merge.
-KERNELS_PER_STEP = 15
+
+def candidate_cost_fp64_ops(blocks_x: int, blocks_y: int) -> int:
+    """Algorithmic FP64 operations of the candidate-cost kernels for one
+    image: every candidate transforms 3 channels forward and back, each
+    separable DCT costs (W + H) multiply-adds per coefficient, and the
+    bit-exact restatement rounds every multiply and every add separately
+    (2 FP64 operations per multiply-add)."""
+    total = 0
+    for w, h, cw, ch, step in FAMILIES:
+        anchors = 0
+        for ty in range(0, blocks_y, 8):
+            for tx in range(0, blocks_x, 8):
+                tw, th = min(8, blocks_x - tx), min(8, blocks_y - ty)
+                nx = len([x for x in range(0, 8 - cw + 1, step) if x + cw <= tw])
+                ny = len([y for y in range(0, 8 - ch + 1, step) if y + ch <= th])
+                anchors += nx * ny
+        total += anchors * 3 * 2 * (w * h) * (w + h) * 2
+    return total
+
+
+# DRAM traffic of the seven candidate-cost launches for one analysis of the
+# workload, from an ncu capture (None until captured).
+COST_KERNEL_DRAM_BYTES = None
+
+
+def fp64_peak_tflops(stream: int) -> float:
+    """FP64 multiply/add throughput of this GPU (TFLOP/s, one DMUL or DADD =
+    one operation), measured by the library's calibration kernel."""
+    import ctypes
+    import torch
+    from gjxl_b200 import _lib
+    sink = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ops = ctypes.c_double()
+    _lib.call("gjxl_b200_fp64_throughput", sink.data_ptr(), ctypes.byref(ops), stream)
+    return ops.value / 1e12
 
 
 def d2h_bytes(session) -> int:
@@ -227,10 +257,12 @@ def run_gpu(args) -> dict:
             stage_ms[k] = stage_ms.get(k, 0.0) + v / reps
     prof.close()
 
-    tiles = prof.outputs.tiles_x * prof.outputs.tiles_y
+    o = prof.outputs
     cost_ms = stage_ms.get("ac_strategy_costs", float("nan"))
-    fp64_tflops = FP64_MAC_PER_TILE * tiles * 2 / (cost_ms / 1e3) / 1e12
-    peaks = load_peaks()
+    fp64_ops = candidate_cost_fp64_ops(o.blocks_x, o.blocks_y)
+    achieved = fp64_ops / (cost_ms / 1e3) / 1e12
+    peak = fp64_peak_tflops(stream)
+    launches = session.kernel_count(d_img.data_ptr(), row, 3)
     result = {
         "metric": METRIC, "value": round(value, 3), "unit": "MP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
@@ -244,19 +276,23 @@ def run_gpu(args) -> dict:
                 "h2d_bytes_per_step": WIDTH * HEIGHT * 3,
                 "d2h_bytes_per_step": d2h_bytes(session)},
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-        "gpu_launches": args.steps * KERNELS_PER_STEP,
+        "gpu_launches": args.steps * launches,
         "roofline": {
-            "kernel": "CandidateCostKernel<W,H> (7 transform families)",
+            "kernel": "CandidateCostKernel<W,H> (7 transform families, one launch each)",
             "bound": "fp64",
-            "achieved": round(fp64_tflops, 3),
-            "unit": "TFLOP/s (FP64 multiply + add, counted as 2 flops per MAC)",
-            "peak": None, "frac": None, "traffic": None,
-            "note": ("the dominant kernel is FP64-pipe bound (bit-exact double-precision "
-                     "DCTs); MEASURED_PEAKS.json has no FP64 figure"),
+            "achieved": round(achieved, 3),
+            "peak": round(peak, 3),
+            "unit": "TFLOP/s (FP64, multiply and add rounded and counted separately)",
+            "frac": round(achieved / peak, 4),
+            "traffic": COST_KERNEL_DRAM_BYTES,
+            "algorithmic_ops": fp64_ops,
+            "peak_source": ("measured live: gjxl_b200_fp64_throughput (independent DMUL/DADD "
+                            "chains on every SM); MEASURED_PEAKS.json has no FP64 figure"),
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over "
+                               "the 7 family launches of one analysis of this workload"),
         },
         "clocks": clocks,
     }
-    del peaks
     session.close()
     if world > 1:
         import torch.distributed as dist
@@ -360,7 +396,12 @@ def main():
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--launch-list", action="store_true")
+    parser.add_argument("--size", default=None,
+                        help="WxH of a smaller image of the same generator (profiling only)")
     args = parser.parse_args()
+    if args.size:
+        global WIDTH, HEIGHT
+        WIDTH, HEIGHT = (int(v) for v in args.size.lower().split("x"))
     if args.impl == "reference":
         out = run_reference(args)
         if out:

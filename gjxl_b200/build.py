@@ -31,7 +31,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC
 
 
 def _headers_mtime() -> float:
-    paths = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    paths = (list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.inc"))
+             + list(INCLUDE.glob("*.h")))
     return max((p.stat().st_mtime for p in paths), default=0.0)
 
 

@@ -15,9 +15,11 @@
 // strategy grid never leaves HBM.
 //
 // Work layout: one kernel instantiation per transform family <W, H>; each CTA
-// of 256 threads evaluates K = 1024 / (W*H) candidates (all three channels)
+// of 384 threads evaluates K = 1024 / (W*H) candidates (all three channels)
 // entirely in shared memory: pixels -> FP64 row pass -> FP64 column pass ->
-// quantize -> FP64 inverse row/column passes -> weighted loss. The reference's
+// quantize -> FP64 inverse row/column passes -> weighted loss. Each FP64
+// pass gives every thread one 8-output chunk of one line, with the DCT basis
+// in constant memory (line_dct.cuh). The reference's
 // order-dependent float sums (magnitude cost, pixel loss) are done by one
 // thread per (candidate, channel) in the reference's order.
 
@@ -26,6 +28,7 @@
 
 #include "common.cuh"
 #include "host_util.h"
+#include "line_dct.cuh"
 #include "tables.h"
 
 namespace gjxl_b200 {
@@ -66,10 +69,6 @@ struct CostParams {
   int local_x, local_y;  // local anchors per tile along x / y (full tile)
   const float* dequant;          // family table [3][N]
   const float* inverse_dequant;  // family table [3][N]
-  const double* fwd_w_t;  // forward basis, width length, transposed [x][u]
-  const double* fwd_h;    // forward basis, height length, natural [v][y]
-  const double* inv_w;    // inverse basis, width length, natural [u][x]
-  const double* inv_h;    // inverse basis, height length, natural [v][y]
   float* costs;           // family plane, blocks_x x blocks_y (anchor positions)
   uint32_t* error;
 };
@@ -83,22 +82,68 @@ struct Shape {
   __device__ static int Index(int v, int u) { return H < W ? v * W + u : u * H + v; }
 };
 
-constexpr int kCostThreads = 256;
+// One CTA evaluates K = 1024 / N candidates, 3 channels each, with
+// 3 * K * N / 8 = 384 threads: in each of the four transform passes every
+// thread computes one 8-output chunk of one line (line_dct.cuh). Shared
+// planes are [candidate * 3 + channel][row][column] with rows padded to
+// W + 1 elements, so that threads on consecutive rows and threads on
+// consecutive columns both hit distinct banks.
+constexpr int kCostThreads = 384;
+
+template <int W, int H>
+struct CostLayout {
+  static constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
+  static constexpr int RowPitch = W + 1;
+  static constexpr int PlanePitch = H * RowPitch;
+  static constexpr int Planes = KC * PlanePitch;  // elements per padded buffer
+  static constexpr size_t SharedBytes =
+    static_cast<size_t>(Planes) * (4 + 4 + 8) + static_cast<size_t>(KC) * N * 4;
+  static_assert(KC * N / 8 == kCostThreads, "one chunk per thread and pass");
+  static_assert((KC * H) % 32 == 0 && (KC * W) % 32 == 0, "warp-uniform chunks");
+};
 
 __device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
   return v <= 1 ? 0 : 32 - __clz(v - 1);
 }
 
+// Row pass over all KC * H rows: chunk `tid / (KC * H)` of row `tid % (KC * H)`.
+template <int W, int H, bool kForward, typename In>
+__device__ __forceinline__ void RowPass(const In* in, double* out, const int* anchor_x, int tid) {
+  using Lay = CostLayout<W, H>;
+  constexpr int kLines = Lay::KC * H;
+  const int chunk = tid / kLines, line = tid % kLines;
+  if (anchor_x[line / H / 3] < 0) return;
+  LineChunkAt<W, kForward, 1, 1>(chunk, in + line * Lay::RowPitch,
+                                 out + line * Lay::RowPitch + chunk * 8);
+}
+
+// Column pass over all KC * W columns: chunk `tid / (KC * W)` of column
+// `tid % (KC * W)`.
+template <int W, int H, bool kForward>
+__device__ __forceinline__ void ColumnPass(const double* in, float* out, const int* anchor_x,
+                                           int tid) {
+  using Lay = CostLayout<W, H>;
+  constexpr int kLines = Lay::KC * W;
+  const int chunk = tid / kLines, line = tid % kLines;
+  const int kc = line / W, u = line % W;
+  if (anchor_x[kc / 3] < 0) return;
+  const int base = kc * Lay::PlanePitch + u;
+  LineChunkAt<H, kForward, Lay::RowPitch, Lay::RowPitch>(
+    chunk, in + base, out + base + chunk * 8 * Lay::RowPitch);
+}
+
 template <int W, int H>
-__global__ void __launch_bounds__(kCostThreads)
+__global__ void __launch_bounds__(kCostThreads, 3)
 CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_count) {
   using S = Shape<W, H>;
-  constexpr int N = S::N, K = S::K;
+  using Lay = CostLayout<W, H>;
+  constexpr int N = S::N, K = Lay::K, KC = Lay::KC;
+  static_assert(K == S::K, "candidates per CTA");
   extern __shared__ __align__(16) unsigned char smem[];
-  float* A = reinterpret_cast<float*>(smem);               // [K][3][N]
-  float* B = A + K * 3 * N;                                 // [K][3][N]
-  double* T = reinterpret_cast<double*>(B + K * 3 * N);     // [K][3][N]
-  float* Tf = reinterpret_cast<float*>(T);                  // aliases T
+  double* T = reinterpret_cast<double*>(smem);             // [KC][H][W+1] row-pass results
+  float* A = reinterpret_cast<float*>(T + Lay::Planes);    // [KC][H][W+1] pixels, residuals
+  float* B = A + Lay::Planes;                              // [KC][H][W+1] coefficients, pixels
+  float* terms = B + Lay::Planes;                          // [KC][N] ordered sum terms
   __shared__ int anchor_x[K], anchor_y[K];
   __shared__ float quant_norm[K], cfl[K][3];
   __shared__ float magnitude[K][3], loss_sum[K][3];
@@ -157,164 +202,74 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
-  // Pixels into A.
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+  // Pixels into A (one W-float run of the source per row).
+  for (int i = tid; i < KC * N; i += kCostThreads) {
+    const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
-    const int y = yx / W, x = yx % W;
-    A[i] = p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
-                   anchor_x[k] * 8 + x];
+    A[kc * Lay::PlanePitch + y * Lay::RowPitch + x] =
+      p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
+              anchor_x[k] * 8 + x];
   }
   __syncthreads();
 
-  // The four FP64 passes are register-tiled: each work item produces four
-  // adjacent outputs of one row, so every shared-memory operand feeds four
-  // multiply-adds. Each output is still one sequential double sum in the
-  // reference's order.
-  constexpr int kItems = K * 3 * N / 4;
-
-  // Forward row pass: T[y][u] = sum_x (double)pixel[y][x] * basis_w[u][x].
-  for (int item = tid; item < kItems; item += kCostThreads) {
-    const int i = item * 4, kc = i / N, yu = i % N, y = yu / W, u0 = yu % W;
-    if (anchor_x[kc / 3] < 0) continue;
-    const float* row = A + kc * N + y * W;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 8
-    for (int x = 0; x < W; ++x) {
-      const double px = static_cast<double>(row[x]);
-      const double2 b01 = __ldg(reinterpret_cast<const double2*>(p.fwd_w_t + x * W + u0));
-      const double2 b23 = __ldg(reinterpret_cast<const double2*>(p.fwd_w_t + x * W + u0 + 2));
-      s0 += px * b01.x;
-      s1 += px * b01.y;
-      s2 += px * b23.x;
-      s3 += px * b23.y;
-    }
-    double* out = T + i;
-    out[0] = s0;
-    out[1] = s1;
-    out[2] = s2;
-    out[3] = s3;
-  }
+  // Forward DCT (ForwardDctCpu): rows into T, then columns into B.
+  RowPass<W, H, true>(A, T, anchor_x, tid);
+  __syncthreads();
+  ColumnPass<W, H, true>(T, B, anchor_x, tid);
   __syncthreads();
 
-  // Forward column pass into B (coefficient storage order):
-  // coef[index(v, u)] = sum_y basis_h[v][y] * T[y][u].
-  for (int item = tid; item < kItems; item += kCostThreads) {
-    const int i = item * 4, kc = i / N, vu = i % N, v = vu / W, u0 = vu % W;
-    if (anchor_x[kc / 3] < 0) continue;
-    const double* col = T + kc * N + u0;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 8
-    for (int y = 0; y < H; ++y) {
-      const double b = __ldg(p.fwd_h + v * H + y);
-      const double2 t01 = *reinterpret_cast<const double2*>(col + y * W);
-      const double2 t23 = *reinterpret_cast<const double2*>(col + y * W + 2);
-      s0 += b * t01.x;
-      s1 += b * t01.y;
-      s2 += b * t23.x;
-      s3 += b * t23.y;
-    }
-    float* coef = B + kc * N;
-    coef[S::Index(v, u0 + 0)] = static_cast<float>(s0);
-    coef[S::Index(v, u0 + 1)] = static_cast<float>(s1);
-    coef[S::Index(v, u0 + 2)] = static_cast<float>(s2);
-    coef[S::Index(v, u0 + 3)] = static_cast<float>(s3);
-  }
-  __syncthreads();
-
-  // Quantize: residual coefficients into A, sqrt terms into Tf.
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+  // Quantize in the reference's coefficient order j = coefficient_index(v, u):
+  // residual coefficients into A at (v, u), sqrt terms into terms[j].
+  for (int i = tid; i < KC * N; i += kCostThreads) {
+    const int kc = i / N, r = i % N, v = r / W, u = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
-    const float* coef = B + k * 3 * N;
-    const float decorrelated = coef[c * N + j] - coef[N + j] * cfl[k][c];
+    const int at = v * Lay::RowPitch + u, j = S::Index(v, u);
+    const float decorrelated =
+      B[kc * Lay::PlanePitch + at] - B[(k * 3 + 1) * Lay::PlanePitch + at] * cfl[k][c];
     const float scaled = decorrelated * __ldg(p.inverse_dequant + c * N + j) * quant_norm[k];
     const float rounded = roundf(scaled);
     const float difference = scaled - rounded;
-    A[i] = __ldg(p.dequant + c * N + j) * difference;
-    Tf[i] = sqrtf(fabsf(rounded));
+    A[kc * Lay::PlanePitch + at] = __ldg(p.dequant + c * N + j) * difference;
+    terms[kc * N + j] = sqrtf(fabsf(rounded));
     if (rounded != 0.0f) atomicAdd(&nonzero[k][c], 1u);
   }
   __syncthreads();
 
-  // Ordered magnitude sums (one thread per candidate and channel).
-  if (tid < 3 * K && anchor_x[tid / 3] >= 0) {
-    const float* terms = Tf + tid * N;
+  // Ordered magnitude sums (one thread per candidate and channel); these
+  // threads then join the inverse row pass, which does not touch `terms`.
+  if (tid < KC && anchor_x[tid / 3] >= 0) {
+    const float* t = terms + tid * N;
     float sum = 0.0f;
-    for (int j = 0; j < N; ++j) sum += terms[j];
+    for (int j = 0; j < N; ++j) sum += t[j];
     magnitude[tid / 3][tid % 3] = sum;
   }
+
+  // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
+  RowPass<W, H, false>(A, T, anchor_x, tid);
+  __syncthreads();
+  ColumnPass<W, H, false>(T, B, anchor_x, tid);
   __syncthreads();
 
-  // Inverse row pass: T[v][x] = sum_u (double)coef[index(v,u)] * inv_w[u][x].
-  for (int item = tid; item < kItems; item += kCostThreads) {
-    const int i = item * 4, kc = i / N, vx = i % N, v = vx / W, x0 = vx % W;
-    if (anchor_x[kc / 3] < 0) continue;
-    const float* coef = A + kc * N;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 8
-    for (int u = 0; u < W; ++u) {
-      const double c = static_cast<double>(coef[S::Index(v, u)]);
-      const double2 b01 = __ldg(reinterpret_cast<const double2*>(p.inv_w + u * W + x0));
-      const double2 b23 = __ldg(reinterpret_cast<const double2*>(p.inv_w + u * W + x0 + 2));
-      s0 += c * b01.x;
-      s1 += c * b01.y;
-      s2 += c * b23.x;
-      s3 += c * b23.y;
-    }
-    double* out = T + i;
-    out[0] = s0;
-    out[1] = s1;
-    out[2] = s2;
-    out[3] = s3;
-  }
-  __syncthreads();
-
-  // Inverse column pass into B: pixels[y][x] = sum_v inv_h[v][y] * T[v][x].
-  for (int item = tid; item < kItems; item += kCostThreads) {
-    const int i = item * 4, kc = i / N, yx = i % N, y = yx / W, x0 = yx % W;
-    if (anchor_x[kc / 3] < 0) continue;
-    const double* col = T + kc * N + x0;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 8
-    for (int v = 0; v < H; ++v) {
-      const double b = __ldg(p.inv_h + v * H + y);
-      const double2 t01 = *reinterpret_cast<const double2*>(col + v * W);
-      const double2 t23 = *reinterpret_cast<const double2*>(col + v * W + 2);
-      s0 += b * t01.x;
-      s1 += b * t01.y;
-      s2 += b * t23.x;
-      s3 += b * t23.y;
-    }
-    float* out = B + i;
-    out[0] = static_cast<float>(s0);
-    out[1] = static_cast<float>(s1);
-    out[2] = static_cast<float>(s2);
-    out[3] = static_cast<float>(s3);
-  }
-  __syncthreads();
-
-  // Weighted eighth powers into A.
-  for (int i = tid; i < K * 3 * N; i += kCostThreads) {
-    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+  // Weighted eighth powers in pixel order.
+  for (int i = tid; i < KC * N; i += kCostThreads) {
+    const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
-    const int y = yx / W, x = yx % W;
     const float m = p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
                                  anchor_x[k] * 8 + x];
     if (!(IsFinite(m) && m > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
     const float offset = c == 0 ? 12.0f : c == 1 ? 0.0f : 4.0f;
-    float weighted = (m + offset) * B[i];
+    float weighted = (m + offset) * B[kc * Lay::PlanePitch + y * Lay::RowPitch + x];
     weighted *= weighted;
     weighted *= weighted;
     weighted *= weighted;
-    A[i] = weighted;
+    terms[kc * N + r] = weighted;
   }
   __syncthreads();
 
-  if (tid < 3 * K && anchor_x[tid / 3] >= 0) {
-    const float* terms = A + tid * N;
+  if (tid < KC && anchor_x[tid / 3] >= 0) {
+    const float* t = terms + tid * N;
     float sum = 0.0f;
-    for (int j = 0; j < N; ++j) sum += terms[j];
+    for (int j = 0; j < N; ++j) sum += t[j];
     loss_sum[tid / 3][tid % 3] = sum;
   }
   __syncthreads();
@@ -575,18 +530,12 @@ int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t s
   const HostTables& h = GetHostTables();
   p.dequant = d.dequant + h.layout.offset[table];
   p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
-  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2;
-  const int hi = H == 8 ? 0 : H == 16 ? 1 : 2;
-  p.fwd_w_t = d.forward_t[wi];
-  p.fwd_h = d.forward[hi];
-  p.inv_w = d.inverse[wi];
-  p.inv_h = d.inverse[hi];
   p.entropy_multiplier = kFamilyEntropy[family];
   const int cw = kFamilyCoveredW[family], ch = kFamilyCoveredH[family];
   p.local_x = (8 - cw) / p.anchor_step + 1;
   p.local_y = (8 - ch) / p.anchor_step + 1;
   const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
-  const size_t smem = static_cast<size_t>(S::K) * 3 * S::N * (4 + 4 + 8);
+  const size_t smem = CostLayout<W, H>::SharedBytes;
   int status = CheckCuda(cudaFuncSetAttribute(CandidateCostKernel<W, H>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(smem)),

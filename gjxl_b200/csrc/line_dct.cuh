@@ -1,0 +1,84 @@
+// Line passes of the reference CPU DCT (src/codec/dct.cpp:135-230) for the
+// FP64 transform kernels.
+//
+// The reference transforms one W x H block as two 1-D passes of dense matrix
+// products in double precision, each output one sequential sum
+// `sum += sample[s] * basis[...]` over s = 0..L-1 (multiply and add rounded
+// separately; the device code is built with --fmad=false). A *line* is the L
+// samples one output depends on (a row of W for the row pass, a column of H
+// for the column pass); a *chunk* is 8 consecutive outputs of one line.
+//
+// One thread computes one chunk: it streams the line's samples once from
+// shared memory and keeps 8 independent double accumulators, so every sample
+// load feeds 8 multiply-adds and the 8 chains give the FP64 pipe enough
+// independent work. The chunk index is a template parameter, so after full
+// unrolling every basis value is a compile-time offset into constant memory
+// and enters the multiply as a constant-bank operand: the basis costs no load
+// instruction. Callers map warps to chunks so that the chunk is warp-uniform.
+#pragma once
+
+#include "dct_basis.inc"
+
+namespace gjxl_b200 {
+
+// basis[frequency * L + sample] of the forward (DCT-II, 1/L scaled) or inverse
+// (DCT-III) transform of length L.
+template <int L, bool kForward>
+__device__ __forceinline__ double DctBasis(int index) {
+  if constexpr (kForward) {
+    if constexpr (L == 8) return kDctForward8[index];
+    if constexpr (L == 16) return kDctForward16[index];
+    if constexpr (L == 32) return kDctForward32[index];
+  } else {
+    if constexpr (L == 8) return kDctInverse8[index];
+    if constexpr (L == 16) return kDctInverse16[index];
+    if constexpr (L == 32) return kDctInverse32[index];
+  }
+  return 0.0;
+}
+
+// Outputs k = C*8 .. C*8+7 of one line of length L:
+//   forward: out[k] = sum_s in[s] * basis[k * L + s]   (k = frequency)
+//   inverse: out[k] = sum_s in[s] * basis[s * L + k]   (k = sample, s = frequency)
+// `in` advances by InStep elements per sample, `out` by OutStep per output.
+template <int L, bool kForward, int C, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunk(const In* __restrict__ in, Out* __restrict__ out) {
+  double acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    const double v = static_cast<double>(in[s * InStep]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = C * 8 + j;
+      acc[j] += v * DctBasis<L, kForward>(kForward ? k * L + s : s * L + k);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
+}
+
+// Runtime chunk index (warp-uniform) to the compile-time instantiation.
+template <int L, bool kForward, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunkAt(int chunk, const In* __restrict__ in,
+                                            Out* __restrict__ out) {
+  switch (chunk) {
+    case 0:
+      LineChunk<L, kForward, 0, InStep, OutStep>(in, out);
+      break;
+    case 1:
+      if constexpr (L > 8) LineChunk<L, kForward, 1, InStep, OutStep>(in, out);
+      break;
+    case 2:
+      if constexpr (L > 16) LineChunk<L, kForward, 2, InStep, OutStep>(in, out);
+      break;
+    case 3:
+      if constexpr (L > 16) LineChunk<L, kForward, 3, InStep, OutStep>(in, out);
+      break;
+    default:
+      break;
+  }
+}
+
+}  // namespace gjxl_b200

@@ -671,3 +671,49 @@ extern "C" int gjxl_b200_session_stage_times(gjxl_b200_session* s, float* millis
 extern "C" const char* gjxl_b200_stage_name(int stage) {
   return stage >= 0 && stage < kStageCount ? kStageNames[stage] : nullptr;
 }
+
+extern "C" int gjxl_b200_session_kernel_count(gjxl_b200_session* s, const uint8_t* pixels,
+                                              size_t row_stride, int channels,
+                                              size_t* kernels) {
+  ClearLastError();
+  if (s == nullptr || pixels == nullptr || kernels == nullptr) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_kernel_count: null argument");
+  }
+  if (s->events_created) {
+    return SetError(GJXL_B200_FAILED_PRECONDITION,
+                    "session_kernel_count: needs a session without stage profiling");
+  }
+  // Capture one analysis into a graph (nothing executes) and count its
+  // kernel nodes.
+  cudaStream_t st = nullptr;
+  GJXL_TRY(CheckCuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking),
+                     "session_kernel_count: stream"));
+  int status = CheckCuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed),
+                         "session_kernel_count: begin capture");
+  const int run_status = status == GJXL_B200_OK ? Run(s, pixels, row_stride, channels, st)
+                                                : status;
+  cudaGraph_t graph = nullptr;
+  if (status == GJXL_B200_OK) {
+    status = CheckCuda(cudaStreamEndCapture(st, &graph), "session_kernel_count: end capture");
+  }
+  if (status == GJXL_B200_OK) status = run_status;
+  size_t count = 0;
+  if (status == GJXL_B200_OK) {
+    size_t nodes = 0;
+    status = CheckCuda(cudaGraphGetNodes(graph, nullptr, &nodes), "session_kernel_count: nodes");
+    std::vector<cudaGraphNode_t> list(nodes);
+    if (status == GJXL_B200_OK && nodes > 0) {
+      status = CheckCuda(cudaGraphGetNodes(graph, list.data(), &nodes),
+                         "session_kernel_count: nodes");
+    }
+    for (size_t i = 0; status == GJXL_B200_OK && i < nodes; ++i) {
+      cudaGraphNodeType type;
+      status = CheckCuda(cudaGraphNodeGetType(list[i], &type), "session_kernel_count: type");
+      if (status == GJXL_B200_OK && type == cudaGraphNodeTypeKernel) ++count;
+    }
+  }
+  if (graph != nullptr) cudaGraphDestroy(graph);
+  cudaStreamDestroy(st);
+  if (status == GJXL_B200_OK) *kernels = count;
+  return status;
+}

@@ -65,6 +65,9 @@ def _bind():
     lib.gjxl_b200_session_stage_times.restype = c_int
     lib.gjxl_b200_stage_name.argtypes = [c_int]
     lib.gjxl_b200_stage_name.restype = ctypes.c_char_p
+    lib.gjxl_b200_session_kernel_count.argtypes = [c_void_p, c_void_p, c_size_t, c_int,
+                                                   POINTER(c_size_t)]
+    lib.gjxl_b200_session_kernel_count.restype = c_int
     _BOUND = True
 
 
@@ -114,6 +117,16 @@ class AnalysisSession:
         _check(_lib.load().gjxl_b200_session_analyze(self.handle, device_pixels_ptr, row_stride,
                                                      channels, stream),
                "gjxl_b200_session_analyze")
+
+    def kernel_count(self, device_pixels_ptr: int, row_stride: int, channels: int) -> int:
+        """Kernels one analyze() call on these arguments launches (counted
+        from a captured graph; nothing executes)."""
+        count = c_size_t()
+        _check(_lib.load().gjxl_b200_session_kernel_count(self.handle, device_pixels_ptr,
+                                                          row_stride, channels,
+                                                          ctypes.byref(count)),
+               "gjxl_b200_session_kernel_count")
+        return int(count.value)
 
     def analyze_host(self, host_pixels: np.ndarray, stream: int = 0):
         assert host_pixels.dtype == np.uint8 and host_pixels.flags["C_CONTIGUOUS"]

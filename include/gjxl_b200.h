@@ -424,6 +424,25 @@ GJXL_B200_API int gjxl_b200_session_stage_times(gjxl_b200_session* session,
                                                 float* milliseconds,
                                                 int capacity);
 GJXL_B200_API const char* gjxl_b200_stage_name(int stage);
+/* Number of kernels one gjxl_b200_session_analyze call on these arguments
+ * launches: the analysis is captured into a CUDA graph on a private stream
+ * (nothing executes) and its kernel nodes are counted. Needs a session
+ * created with profile_stages off. No counterpart in the reference. */
+GJXL_B200_API int gjxl_b200_session_kernel_count(gjxl_b200_session* session,
+                                                 const uint8_t* pixels,
+                                                 size_t row_stride_bytes, int channels,
+                                                 size_t* kernels);
+
+/*
+ * Measurement (no counterpart in the reference).
+ * FP64 multiply/add throughput of the current device in operations per
+ * second (one DMUL or DADD = one operation), measured with independent
+ * separately rounded multiply-add chains: the ceiling of the bit-exact
+ * double-precision transform kernels. `device_sink` is 8 bytes of device
+ * memory (never written in practice). Synchronizes `stream`.
+ */
+GJXL_B200_API int gjxl_b200_fp64_throughput(double* device_sink, double* ops_per_second,
+                                            void* stream);
 
 #ifdef __cplusplus
 }  /* extern "C" */
