@@ -126,6 +126,13 @@ __global__ void AdjustFieldKernel(AnchorView v, const float* in, float* out, flo
     for (int dx = 0; dx < cw; ++dx) out[(by + dy) * v.blocks_x + bx + dx] = result;
 }
 
+// The field is positive, so its extremes reduce as unsigned bit patterns
+// from {+inf, 0}.
+__global__ void RangeInitKernel(float* range) {
+  range[0] = __int_as_float(0x7f800000);
+  range[1] = 0.0f;
+}
+
 __global__ void RangeKernel(const float* field, int n, float* range) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float lo = __int_as_float(0x7f800000), hi = 0.0f;
@@ -166,10 +173,20 @@ __device__ uint32_t RadixSelect(const float* field, int n, int k, bool use_cente
   for (int shift = 24; shift >= 0; shift -= 8) {
     for (int b = threadIdx.x; b < 256; b += blockDim.x) histogram[b] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float v = use_center ? fabsf(field[i] - center) : field[i];
-      const uint32_t bits = __float_as_uint(v);
-      if ((bits & mask) == prefix) atomicAdd(&histogram[(bits >> shift) & 255u], 1u);
+    // Field values cluster in a few bins, so lanes of a warp that share a
+    // bin add their count with one atomic (all lanes run every iteration).
+    for (int base = 0; base < n; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      int bin = -1;
+      if (i < n) {
+        const float v = use_center ? fabsf(field[i] - center) : field[i];
+        const uint32_t bits = __float_as_uint(v);
+        if ((bits & mask) == prefix) bin = static_cast<int>((bits >> shift) & 255u);
+      }
+      const uint32_t same = __match_any_sync(0xffffffffu, bin);
+      if (bin >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) {
+        atomicAdd(&histogram[bin], static_cast<uint32_t>(__popc(same)));
+      }
     }
     __syncthreads();
     __shared__ uint32_t chosen_bin, chosen_k;
@@ -234,9 +251,9 @@ __global__ void RawQuantKernel(const float* field, int n, const AqQuantizer* q, 
 }
 
 // ---------------------------------------------------------------------------
-// Final CfL, fast regression (one warp per 64x64 tile; lanes 0-3 solve
-// y_to_x and 4-7 y_to_b, lane i owning elements i (mod 4) in the reference's
-// order: anchors in raster order, coefficients in storage order).
+// Final CfL, fast regression (one CTA per 64x64 tile; lane i of the solving
+// lanes owns elements i (mod 4) in the reference's order: anchors in raster
+// order, coefficients in storage order).
 
 struct CflFinalParams {
   AnchorView grid;
@@ -263,50 +280,91 @@ __device__ __forceinline__ int8_t QuantizeMultiplierF(float x) {
   return static_cast<int8_t>(fminf(fmaxf(roundf(x), -128.0f), 127.0f));
 }
 
-__global__ void __launch_bounds__(32) FinalCflKernel(const __grid_constant__ CflFinalParams p) {
+// Per tile, all threads first write the regression terms a = luma / 84 and
+// b = base * luma - chroma of both problems into shared memory in the
+// reference's element order (anchors in raster order, coefficients in
+// storage order); then lanes 0-3 (y_to_x) and 4-7 (y_to_b) of warp 0 run the
+// four ordered fused multiply-add chains per problem from shared memory.
+constexpr int kFinalCflThreads = 128;
+constexpr int kFinalCflTerms = 64 * 64;  // coefficients of one 64x64 tile
+
+__global__ void __launch_bounds__(kFinalCflThreads)
+FinalCflKernel(const __grid_constant__ CflFinalParams p) {
+  extern __shared__ __align__(16) float terms[];  // [a_x, b_x, a_b, b_b][kFinalCflTerms]
+  __shared__ int block_terms[64], offsets[64], total_terms;
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
-  const int lane = threadIdx.x;
-  const int problem = lane / 4, slot = lane % 4;  // problem 0: X, 1: B
   const int bx0 = tx * 8, by0 = ty * 8;
-  const int bx1 = min(bx0 + 8, p.grid.blocks_x), by1 = min(by0 + 8, p.grid.blocks_y);
-  float quadratic = 0.0f, linear = 0.0f;
-  int count = 0;
+  const int tw = min(8, p.grid.blocks_x - bx0), th = min(8, p.grid.blocks_y - by0);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x < 64) {
+    int n = 0, cw, ch, s;
+    const int b = threadIdx.x;
+    if (b < tw * th && AnchorAt(p.grid, (by0 + b / tw) * p.grid.blocks_x + bx0 + b % tw, &cw,
+                                &ch, &s)) {
+      n = cw * ch * 64;
+    }
+    block_terms[b] = n;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int running = 0;
+    for (int b = 0; b < 64; ++b) {
+      offsets[b] = running;
+      running += block_terms[b];
+    }
+    total_terms = running;
+  }
+  __syncthreads();
   const float scale128 = p.q->scale * 128.0f;
+  for (int b = warp; b < tw * th; b += kFinalCflThreads / 32) {
+    const int n = block_terms[b];
+    if (n == 0) continue;
+    const int bx = bx0 + b % tw, by = by0 + b / tw;
+    int cw, ch, s;
+    AnchorAt(p.grid, by * p.grid.blocks_x + bx, &cw, &ch, &s);
+    const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
+                    : s == kStrategyDct32x32 ? kTableDct32
+                    : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
+                                                                         : kTableDct16x32;
+    const float* inv_x = p.inverse_dequant + p.table_offset[table];
+    const float* inv_b = inv_x + 2 * n;
+    const float quant_scale = scale128 * static_cast<float>(p.raw[by * p.grid.blocks_x + bx]);
+    const int w = cw * 8;
+    // LLF extent: covered blocks with the longer side first.
+    const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
+    const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
+    float* out = terms + offsets[b];
+    for (int i = lane; i < n; i += 32) {
+      const int cy = i / sw, cx = i % sw;
+      const bool llf = cy < lfh && cx < lfw;
+      const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
+      const float luma_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
+      const float x_v = llf ? 0.0f : p.coef[at];
+      const float b_v = llf ? 0.0f : p.coef[2 * p.coef_pitch + at];
+      const float base_x = 0.0f, base_b = 1.0f;
+      const float luma_x = luma_v * inv_x[i] * quant_scale;
+      const float chroma_x = x_v * inv_x[i] * quant_scale;
+      const float luma_b = luma_v * inv_b[i] * quant_scale;
+      const float chroma_b = b_v * inv_b[i] * quant_scale;
+      out[i] = luma_x / 84.0f;
+      out[kFinalCflTerms + i] = base_x * luma_x - chroma_x;
+      out[2 * kFinalCflTerms + i] = luma_b / 84.0f;
+      out[3 * kFinalCflTerms + i] = base_b * luma_b - chroma_b;
+    }
+  }
+  __syncthreads();
+  if (warp != 0) return;
+  const int problem = lane / 4, slot = lane % 4;  // problem 0: X, 1: B
+  const int count = total_terms;
+  float quadratic = 0.0f, linear = 0.0f;
   if (problem < 2) {
-    const int chroma_channel = problem == 0 ? 0 : 2;
-    const float base = problem == 0 ? 0.0f : 1.0f;
-    for (int by = by0; by < by1; ++by) {
-      for (int bx = bx0; bx < bx1; ++bx) {
-        int cw, ch, s;
-        if (!AnchorAt(p.grid, by * p.grid.blocks_x + bx, &cw, &ch, &s)) continue;
-        const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
-                        : s == kStrategyDct32x32 ? kTableDct32
-                        : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
-                                                                             : kTableDct16x32;
-        const int n = static_cast<int>(p.table_count[table]);
-        const float* inv = p.inverse_dequant + p.table_offset[table] +
-                           (chroma_channel == 0 ? 0 : 2) * n;
-        const float quant_scale = scale128 * static_cast<float>(p.raw[by * p.grid.blocks_x + bx]);
-        const int w = cw * 8;
-        // LLF extent: covered blocks with the longer side first.
-        const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
-        const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
-        for (int i = slot; i < n; i += 4) {
-          const int cy = i / sw, cx = i % sw;
-          const bool llf = cy < lfh && cx < lfw;
-          const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
-          const float cy_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
-          const float cc_v = llf ? 0.0f : p.coef[chroma_channel * p.coef_pitch + at];
-          const float luma = cy_v * inv[i] * quant_scale;
-          const float chroma = cc_v * inv[i] * quant_scale;
-          const float a = luma / 84.0f;
-          const float b = base * luma - chroma;
-          quadratic = fmaf(a, a, quadratic);
-          linear = fmaf(a, b, linear);
-        }
-        count += n;
-      }
+    const float* A = terms + 2 * problem * kFinalCflTerms;
+    const float* B = A + kFinalCflTerms;
+    for (int e = slot; e < count; e += 4) {
+      const float a = A[e], b = B[e];
+      quadratic = fmaf(a, a, quadratic);
+      linear = fmaf(a, b, linear);
     }
   }
   const int base_lane = 4 * (problem < 2 ? problem : 0);
@@ -966,8 +1024,7 @@ int AqAdjustField(const uint8_t* cells, size_t bx, size_t by, const float* in, f
 
 int AqPolicySetup(const float* field, size_t blocks, float target, float* range,
                   AqPolicy* policy, uint32_t* error, cudaStream_t stream) {
-  const float init[2] = {__builtin_huge_valf(), 0.0f};
-  cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+  RangeInitKernel<<<1, 1, 0, stream>>>(range);
   RangeKernel<<<Blocks(blocks), kThreads, 0, stream>>>(field, static_cast<int>(blocks), range);
   // ComputeInitialQuantDc (adaptive_quantization.cpp:536-560), host powf.
   const float kDcMul = 0.3f;
@@ -1009,7 +1066,13 @@ int AqFinalCfl(const uint8_t* cells, size_t bx, size_t by, const float* coef, si
   }
   p.y_to_x = y_to_x;
   p.y_to_b = y_to_b;
-  FinalCflKernel<<<p.tiles_x * p.tiles_y, 32, 0, stream>>>(p);
+  const size_t smem = 4 * kFinalCflTerms * sizeof(float);
+  status = CheckCuda(cudaFuncSetAttribute(FinalCflKernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)),
+                     "final cfl smem attribute");
+  if (status != GJXL_B200_OK) return status;
+  FinalCflKernel<<<p.tiles_x * p.tiles_y, kFinalCflThreads, smem, stream>>>(p);
   return CheckLaunch("aq final cfl");
 }
 
