@@ -93,43 +93,22 @@ constexpr int kCostThreads = 384;
 template <int W, int H>
 struct CostLayout {
   static constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
-  static constexpr int RowPitch = W + 1;
-  static constexpr int PlanePitch = H * RowPitch;
-  static constexpr int Planes = KC * PlanePitch;  // elements per padded buffer
-  static constexpr size_t SharedBytes =
-    static_cast<size_t>(Planes) * (4 + 4 + 8) + static_cast<size_t>(KC) * N * 4;
-  static_assert(KC * N / 8 == kCostThreads, "one chunk per thread and pass");
-  static_assert((KC * H) % 32 == 0 && (KC * W) % 32 == 0, "warp-uniform chunks");
+  using Batch = PlaneBatch<W, H, KC>;
+  static constexpr int RowPitch = Batch::RowPitch;
+  static constexpr int PlanePitch = Batch::PlanePitch;
+  static constexpr int Planes = Batch::Elements;  // elements per padded buffer
+  // Ordered-sum terms: one plane of N + 1 floats per (candidate, channel), so
+  // the summing threads (one per plane, same index at the same time) hit
+  // distinct banks.
+  static constexpr int TermPitch = N + 1;
+  static constexpr size_t SharedBytes = static_cast<size_t>(Planes) * (4 + 4 + 8) +
+                                        static_cast<size_t>(KC) * TermPitch * 4 +
+                                        static_cast<size_t>(K) * N * 4;
+  static_assert(Batch::Items == kCostThreads, "one chunk per thread and pass");
 };
 
 __device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
   return v <= 1 ? 0 : 32 - __clz(v - 1);
-}
-
-// Row pass over all KC * H rows: chunk `tid / (KC * H)` of row `tid % (KC * H)`.
-template <int W, int H, bool kForward, typename In>
-__device__ __forceinline__ void RowPass(const In* in, double* out, const int* anchor_x, int tid) {
-  using Lay = CostLayout<W, H>;
-  constexpr int kLines = Lay::KC * H;
-  const int chunk = tid / kLines, line = tid % kLines;
-  if (anchor_x[line / H / 3] < 0) return;
-  LineChunkAt<W, kForward, 1, 1>(chunk, in + line * Lay::RowPitch,
-                                 out + line * Lay::RowPitch + chunk * 8);
-}
-
-// Column pass over all KC * W columns: chunk `tid / (KC * W)` of column
-// `tid % (KC * W)`.
-template <int W, int H, bool kForward>
-__device__ __forceinline__ void ColumnPass(const double* in, float* out, const int* anchor_x,
-                                           int tid) {
-  using Lay = CostLayout<W, H>;
-  constexpr int kLines = Lay::KC * W;
-  const int chunk = tid / kLines, line = tid % kLines;
-  const int kc = line / W, u = line % W;
-  if (anchor_x[kc / 3] < 0) return;
-  const int base = kc * Lay::PlanePitch + u;
-  LineChunkAt<H, kForward, Lay::RowPitch, Lay::RowPitch>(
-    chunk, in + base, out + base + chunk * 8 * Lay::RowPitch);
 }
 
 template <int W, int H>
@@ -143,7 +122,8 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   double* T = reinterpret_cast<double*>(smem);             // [KC][H][W+1] row-pass results
   float* A = reinterpret_cast<float*>(T + Lay::Planes);    // [KC][H][W+1] pixels, residuals
   float* B = A + Lay::Planes;                              // [KC][H][W+1] coefficients, pixels
-  float* terms = B + Lay::Planes;                          // [KC][N] ordered sum terms
+  float* terms = B + Lay::Planes;                          // [KC][N + 1] ordered sum terms
+  float* mask = terms + KC * Lay::TermPitch;               // [K][H][W] pixel mask
   __shared__ int anchor_x[K], anchor_y[K];
   __shared__ float quant_norm[K], cfl[K][3];
   __shared__ float magnitude[K][3], loss_sum[K][3];
@@ -202,7 +182,8 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
-  // Pixels into A (one W-float run of the source per row).
+  // Pixels into A and the pixel mask into `mask` (one W-float run of the
+  // source per row), all loads issued before the first use.
   for (int i = tid; i < KC * N; i += kCostThreads) {
     const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
@@ -210,27 +191,35 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
       p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
               anchor_x[k] * 8 + x];
   }
+  for (int i = tid; i < K * N; i += kCostThreads) {
+    const int k = i / N, r = i % N, y = r / W, x = r % W;
+    if (anchor_x[k] < 0) continue;
+    mask[i] = p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
+                           anchor_x[k] * 8 + x];
+  }
   __syncthreads();
 
   // Forward DCT (ForwardDctCpu): rows into T, then columns into B.
-  RowPass<W, H, true>(A, T, anchor_x, tid);
+  const auto present = [&](int plane) { return anchor_x[plane / 3] >= 0; };
+  BatchRowPass<W, H, KC, true>(A, T, tid, kCostThreads, present);
   __syncthreads();
-  ColumnPass<W, H, true>(T, B, anchor_x, tid);
+  BatchColumnPass<W, H, KC, true>(T, B, tid, kCostThreads, present);
   __syncthreads();
 
-  // Quantize in the reference's coefficient order j = coefficient_index(v, u):
+  // Quantize, coefficient j = coefficient_index(v, u) by coefficient:
   // residual coefficients into A at (v, u), sqrt terms into terms[j].
   for (int i = tid; i < KC * N; i += kCostThreads) {
-    const int kc = i / N, r = i % N, v = r / W, u = r % W, k = kc / 3, c = kc % 3;
+    const int kc = i / N, j = i % N, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
-    const int at = v * Lay::RowPitch + u, j = S::Index(v, u);
+    const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
+    const int at = v * Lay::RowPitch + u;
     const float decorrelated =
       B[kc * Lay::PlanePitch + at] - B[(k * 3 + 1) * Lay::PlanePitch + at] * cfl[k][c];
     const float scaled = decorrelated * __ldg(p.inverse_dequant + c * N + j) * quant_norm[k];
     const float rounded = roundf(scaled);
     const float difference = scaled - rounded;
     A[kc * Lay::PlanePitch + at] = __ldg(p.dequant + c * N + j) * difference;
-    terms[kc * N + j] = sqrtf(fabsf(rounded));
+    terms[kc * Lay::TermPitch + j] = sqrtf(fabsf(rounded));
     if (rounded != 0.0f) atomicAdd(&nonzero[k][c], 1u);
   }
   __syncthreads();
@@ -238,36 +227,35 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   // Ordered magnitude sums (one thread per candidate and channel); these
   // threads then join the inverse row pass, which does not touch `terms`.
   if (tid < KC && anchor_x[tid / 3] >= 0) {
-    const float* t = terms + tid * N;
+    const float* t = terms + tid * Lay::TermPitch;
     float sum = 0.0f;
     for (int j = 0; j < N; ++j) sum += t[j];
     magnitude[tid / 3][tid % 3] = sum;
   }
 
   // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
-  RowPass<W, H, false>(A, T, anchor_x, tid);
+  BatchRowPass<W, H, KC, false>(A, T, tid, kCostThreads, present);
   __syncthreads();
-  ColumnPass<W, H, false>(T, B, anchor_x, tid);
+  BatchColumnPass<W, H, KC, false>(T, B, tid, kCostThreads, present);
   __syncthreads();
 
   // Weighted eighth powers in pixel order.
   for (int i = tid; i < KC * N; i += kCostThreads) {
     const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
-    const float m = p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
-                                 anchor_x[k] * 8 + x];
+    const float m = mask[k * N + r];
     if (!(IsFinite(m) && m > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
     const float offset = c == 0 ? 12.0f : c == 1 ? 0.0f : 4.0f;
     float weighted = (m + offset) * B[kc * Lay::PlanePitch + y * Lay::RowPitch + x];
     weighted *= weighted;
     weighted *= weighted;
     weighted *= weighted;
-    terms[kc * N + r] = weighted;
+    terms[kc * Lay::TermPitch + r] = weighted;
   }
   __syncthreads();
 
   if (tid < KC && anchor_x[tid / 3] >= 0) {
-    const float* t = terms + tid * N;
+    const float* t = terms + tid * Lay::TermPitch;
     float sum = 0.0f;
     for (int j = 0; j < N; ++j) sum += t[j];
     loss_sum[tid / 3][tid % 3] = sum;

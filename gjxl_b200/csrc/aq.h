@@ -39,8 +39,10 @@ int AqAdjustField(const uint8_t* cells, size_t bx, size_t by, const float* in, f
                   float target, cudaStream_t stream);
 int AqPolicySetup(const float* field, size_t blocks, float target, float* range,
                   AqPolicy* policy, uint32_t* error, cudaStream_t stream);
+// Device state of the quantizer's median / deviation selection.
+size_t AqSelectStateBytes();
 int AqQuantizer_(const float* field, size_t blocks, const AqPolicy* policy, AqQuantizer* q,
-                 int32_t* raw, uint32_t* error, cudaStream_t stream);
+                 int32_t* raw, void* select_state, uint32_t* error, cudaStream_t stream);
 int AqFinalCfl(const uint8_t* cells, size_t bx, size_t by, const float* coef, size_t stride,
                size_t pitch, const int32_t* raw, const AqQuantizer* q, int8_t* y_to_x,
                int8_t* y_to_b, cudaStream_t stream);

@@ -20,12 +20,14 @@
 // anchored at block (bx, by) occupy its own W x H pixel footprint of a padded
 // plane, coefficient i at (bx*8 + i % W, by*8 + i / W).
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
 #include "aq.h"
 #include "common.cuh"
 #include "host_util.h"
+#include "line_dct.cuh"
 #include "tables.h"
 #include "transform.cuh"
 
@@ -52,36 +54,47 @@ __global__ void AnchorListKernel(const uint8_t* cells, uint32_t blocks_x, uint32
 // ---------------------------------------------------------------------------
 // Forward coefficients of the selected transforms (footprint layout).
 
+// K = 1024 / N transforms (3 channels each) per CTA of 384 threads, one
+// 8-output chunk of one line per thread and pass (line_dct.cuh).
+constexpr int kTransformThreads = 384;
+
 template <int W, int H>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kTransformThreads)
 ForwardCoefficientsKernel(const float* opsin, size_t stride, size_t pitch, const int2* anchors,
-                          const uint32_t* count, const double* bw_t, const double* bh,
-                          float* coef, size_t coef_stride, size_t coef_pitch) {
-  constexpr int N = W * H;
-  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+                          const uint32_t* count, float* coef, size_t coef_stride,
+                          size_t coef_pitch) {
+  using S = TransformShape<W, H>;
+  constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
+  using Batch = PlaneBatch<W, H, KC>;
+  static_assert(Batch::Items == kTransformThreads, "one chunk per thread and pass");
   extern __shared__ __align__(16) unsigned char smem[];
-  float* px = reinterpret_cast<float*>(smem);                // [K*3][N]
-  double* tmp = reinterpret_cast<double*>(px + K * 3 * N);  // [K*3][N]
+  double* tmp = reinterpret_cast<double*>(smem);                  // [KC] padded planes
+  float* px = reinterpret_cast<float*>(tmp + Batch::Elements);    // [KC] padded planes
   const uint32_t first = blockIdx.x * K;
   const uint32_t n = *count;
   if (first >= n) return;
   const int active = min(K, static_cast<int>(n - first));
-  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+  for (int i = threadIdx.x; i < active * 3 * N; i += kTransformThreads) {
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
     const int2 a = anchors[first + k];
-    px[i] = opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 + yx % W];
+    px[Batch::At(k * 3 + c, yx / W, yx % W)] =
+      opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 + yx % W];
   }
   __syncthreads();
-  ForwardRows<W, H>(px, tmp, bw_t, active * 3, threadIdx.x, kThreads);
+  const auto present = [&](int plane) { return plane < 3 * active; };
+  BatchRowPass<W, H, KC, true>(px, tmp, threadIdx.x, kTransformThreads, present);
   __syncthreads();
-  ForwardColumns<W, H>(tmp, px, bh, active * 3, threadIdx.x, kThreads);
+  BatchColumnPass<W, H, KC, true>(tmp, px, threadIdx.x, kTransformThreads, present);
   __syncthreads();
-  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+  // Coefficient j = coefficient_index(v, u) goes to footprint (j % W, j / W).
+  for (int i = threadIdx.x; i < active * 3 * N; i += kTransformThreads) {
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
     const int2 a = anchors[first + k];
     coef[c * coef_pitch + static_cast<size_t>(a.y * 8 + j / W) * coef_stride + a.x * 8 + j % W] =
-      px[i];
+      px[Batch::At(k * 3 + c, v, u)];
   }
+  static_assert(S::N == N, "shape");
 }
 
 // ---------------------------------------------------------------------------
@@ -165,60 +178,120 @@ __global__ void PolicySetupKernel(const float* range, float quant_dc, AqPolicy* 
   }
 }
 
-// k-th smallest of n positive floats (or of |field - center| when use_center)
-// by four 8-bit radix passes over the ordered bit patterns.
-__device__ uint32_t RadixSelect(const float* field, int n, int k, bool use_center, float center,
-                                uint32_t* histogram) {
-  uint32_t prefix = 0, mask = 0;
-  for (int shift = 24; shift >= 0; shift -= 8) {
-    for (int b = threadIdx.x; b < 256; b += blockDim.x) histogram[b] = 0;
-    __syncthreads();
-    // Field values cluster in a few bins, so lanes of a warp that share a
-    // bin add their count with one atomic (all lanes run every iteration).
-    for (int base = 0; base < n; base += blockDim.x) {
-      const int i = base + threadIdx.x;
-      int bin = -1;
-      if (i < n) {
-        const float v = use_center ? fabsf(field[i] - center) : field[i];
-        const uint32_t bits = __float_as_uint(v);
-        if ((bits & mask) == prefix) bin = static_cast<int>((bits >> shift) & 255u);
-      }
-      const uint32_t same = __match_any_sync(0xffffffffu, bin);
-      if (bin >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) {
-        atomicAdd(&histogram[bin], static_cast<uint32_t>(__popc(same)));
-      }
-    }
-    __syncthreads();
-    __shared__ uint32_t chosen_bin, chosen_k;
-    if (threadIdx.x == 0) {
-      uint32_t acc = 0;
-      for (uint32_t b = 0; b < 256; ++b) {
-        if (acc + histogram[b] > static_cast<uint32_t>(k)) {
-          chosen_bin = b;
-          chosen_k = static_cast<uint32_t>(k) - acc;
-          break;
-        }
-        acc += histogram[b];
-      }
-    }
-    __syncthreads();
-    prefix |= chosen_bin << shift;
-    mask |= 255u << shift;
-    k = static_cast<int>(chosen_k);
-    __syncthreads();
+// k-th smallest of n positive floats (or of |field - center|) by radix
+// selection over the ordered bit patterns in three digit passes (bits 21-31,
+// 10-20, 0-9). Each pass is a grid-wide histogram of the elements that match
+// the prefix chosen so far (SelectHistogramKernel) and a one-CTA scan that
+// picks the digit holding the k-th element (SelectDigitKernel). The median
+// of the field is selected first, then the median absolute deviation.
+constexpr int kSelectBins = 2048;
+constexpr int kSelectPasses = 3;
+__host__ __device__ constexpr int SelectShift(int pass) { return pass == 0 ? 21 : pass == 1 ? 10 : 0; }
+__host__ __device__ constexpr int SelectBits(int pass) { return pass == 2 ? 10 : 11; }
+
+struct SelectState {
+  uint32_t prefix, mask, k;
+  uint32_t median_bits, mad_bits;
+  uint32_t pad[3];
+  uint32_t histogram[kSelectBins];
+};
+
+__global__ void SelectInitKernel(SelectState* st, int n) {
+  for (int b = threadIdx.x; b < kSelectBins; b += blockDim.x) st->histogram[b] = 0;
+  if (threadIdx.x == 0) {
+    st->prefix = 0;
+    st->mask = 0;
+    st->k = static_cast<uint32_t>(n / 2);
   }
-  return prefix;
+}
+
+__device__ __forceinline__ uint32_t SelectKey(const float* field, int i, bool use_center,
+                                              float center) {
+  return __float_as_uint(use_center ? fabsf(field[i] - center) : field[i]);
+}
+
+__global__ void __launch_bounds__(256)
+SelectHistogramKernel(const float* field, int n, bool use_center, int pass, SelectState* st) {
+  __shared__ uint32_t histogram[kSelectBins];
+  for (int b = threadIdx.x; b < kSelectBins; b += blockDim.x) histogram[b] = 0;
+  __syncthreads();
+  const uint32_t prefix = st->prefix, mask = st->mask;
+  const float center = __uint_as_float(st->median_bits);
+  const int shift = SelectShift(pass);
+  const uint32_t digit_mask = (1u << SelectBits(pass)) - 1u;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t bits = SelectKey(field, i, use_center, center);
+    if ((bits & mask) == prefix) atomicAdd(&histogram[(bits >> shift) & digit_mask], 1u);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < kSelectBins; b += blockDim.x) {
+    if (histogram[b] != 0) atomicAdd(&st->histogram[b], histogram[b]);
+  }
+}
+
+// One CTA of 1024 threads: inclusive scan of the histogram (two bins per
+// thread), the digit whose range holds rank k, and the histogram cleared for
+// the next pass. After the last pass the selected value is stored and the
+// state rearmed for the next selection.
+__global__ void __launch_bounds__(1024) SelectDigitKernel(int pass, int n, bool mad,
+                                                          SelectState* st) {
+  __shared__ uint32_t warp_sums[32];
+  const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+  const uint32_t h0 = st->histogram[2 * t], h1 = st->histogram[2 * t + 1];
+  uint32_t inclusive = h0 + h1;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, inclusive, o);
+    if (lane >= o) inclusive += v;
+  }
+  if (lane == 31) warp_sums[warp] = inclusive;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    warp_sums[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t before = inclusive - (h0 + h1) + (warp ? warp_sums[warp - 1] : 0u);
+  const uint32_t k = st->k;
+  __syncthreads();
+  const int shift = SelectShift(pass);
+  const uint32_t digit_mask = (1u << SelectBits(pass)) - 1u;
+  // Exactly one (thread, bin) has before_bin <= k < before_bin + count.
+  if (k >= before && k < before + h0) {
+    st->prefix |= static_cast<uint32_t>(2 * t) << shift;
+    st->k = k - before;
+  } else if (k >= before + h0 && k < before + h0 + h1) {
+    st->prefix |= static_cast<uint32_t>(2 * t + 1) << shift;
+    st->k = k - before - h0;
+  }
+  st->histogram[2 * t] = 0;
+  st->histogram[2 * t + 1] = 0;
+  __syncthreads();
+  if (t == 0) {
+    st->mask |= digit_mask << shift;
+    if (pass == kSelectPasses - 1) {
+      if (mad) {
+        st->mad_bits = st->prefix;
+      } else {
+        st->median_bits = st->prefix;
+      }
+      st->prefix = 0;
+      st->mask = 0;
+      st->k = static_cast<uint32_t>(n / 2);
+    }
+  }
 }
 
 // CreateQuantizerFromField + ComputeQuantizerParams + Quantizer::Create.
-__global__ void __launch_bounds__(1024)
-QuantizerKernel(const float* field, int n, const AqPolicy* policy, AqQuantizer* q,
-                uint32_t* error) {
-  __shared__ uint32_t histogram[256];
-  const int k = n / 2;
-  const float median = __uint_as_float(RadixSelect(field, n, k, false, 0.0f, histogram));
-  const float mad = __uint_as_float(RadixSelect(field, n, k, true, median, histogram));
-  if (threadIdx.x != 0) return;
+__global__ void QuantizerKernel(const SelectState* st, const AqPolicy* policy, AqQuantizer* q,
+                                uint32_t* error) {
+  const float median = __uint_as_float(st->median_bits);
+  const float mad = __uint_as_float(st->mad_bits);
   const float quant_dc = policy->quant_dc;
   float scale = 65536.0f * (median - mad) / 5.0f;
   scale = fminf(fmaxf(scale, 1.0f), 32768.0f);
@@ -335,6 +408,7 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
     const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
     const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
     float* out = terms + offsets[b];
+#pragma unroll 4
     for (int i = lane; i < n; i += 32) {
       const int cy = i / sw, cx = i % sw;
       const bool llf = cy < lfh && cx < lfw;
@@ -361,10 +435,20 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   if (problem < 2) {
     const float* A = terms + 2 * problem * kFinalCflTerms;
     const float* B = A + kFinalCflTerms;
-    for (int e = slot; e < count; e += 4) {
-      const float a = A[e], b = B[e];
-      quadratic = fmaf(a, a, quadratic);
-      linear = fmaf(a, b, linear);
+    // count is a multiple of 64: batches of 8 elements per lane, loaded
+    // before the ordered multiply-adds.
+    for (int e0 = slot; e0 < count; e0 += 32) {
+      float a[8], b[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        a[j] = A[e0 + 4 * j];
+        b[j] = B[e0 + 4 * j];
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        quadratic = fmaf(a[j], a[j], quadratic);
+        linear = fmaf(a[j], b[j], linear);
+      }
     }
   }
   const int base_lane = 4 * (problem < 2 ? problem : 0);
@@ -916,8 +1000,6 @@ unsigned Blocks(size_t n, unsigned threads = kThreads) {
 // Host launchers.
 
 void UploadDcTables() {
-  static bool done = false;  // guarded by the caller's device-tables lock
-  (void)done;
   DcTables t;
   std::memset(&t, 0, sizeof(t));
   const double sqrt2 = 1.41421356237309504880, pi = 3.14159265358979323846;
@@ -969,42 +1051,37 @@ int AqBuildAnchors(const uint8_t* cells, size_t bx, size_t by, int2* lists, uint
 
 template <int W, int H>
 int LaunchForward(const float* opsin, size_t stride, size_t pitch, const int2* list,
-                  const uint32_t* count, size_t max_count, const DeviceTables& d, float* coef,
-                  cudaStream_t stream) {
-  constexpr int N = W * H;
-  constexpr int K = N >= 1024 ? 1 : 1024 / N;
-  const size_t smem = static_cast<size_t>(K) * 3 * N * 12;
+                  const uint32_t* count, size_t max_count, float* coef, cudaStream_t stream) {
+  constexpr int N = W * H, K = 1024 / N;
+  const size_t smem = static_cast<size_t>(PlaneBatch<W, H, 3 * K>::Elements) * 12;
   int status = CheckCuda(cudaFuncSetAttribute(ForwardCoefficientsKernel<W, H>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(smem)),
                          "aq forward attribute");
   if (status != GJXL_B200_OK) return status;
-  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2, hi = H == 8 ? 0 : H == 16 ? 1 : 2;
   const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
   if (grid == 0) return GJXL_B200_OK;
-  ForwardCoefficientsKernel<W, H><<<grid, kThreads, smem, stream>>>(
-    opsin, stride, pitch, list, count, d.forward_t[wi], d.forward[hi], coef, stride, pitch);
+  ForwardCoefficientsKernel<W, H><<<grid, kTransformThreads, smem, stream>>>(
+    opsin, stride, pitch, list, count, coef, stride, pitch);
   return CheckLaunch("aq forward coefficients");
 }
 
 int AqForwardCoefficients(const float* opsin, size_t stride, size_t pitch, size_t bx, size_t by,
                           const int2* lists, const uint32_t* counts, float* coef,
                           cudaStream_t stream) {
-  DeviceTables d;
-  int status = GetDeviceTables(&d);
-  if (status != GJXL_B200_OK) return status;
+  int status = GJXL_B200_OK;
   const size_t blocks = bx * by;
   for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
     const int2* list = lists + f * blocks;
     const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
     switch (f) {
-      case 0: status = LaunchForward<8, 8>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 1: status = LaunchForward<8, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 2: status = LaunchForward<16, 8>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 3: status = LaunchForward<16, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 4: status = LaunchForward<16, 32>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 5: status = LaunchForward<32, 16>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
-      case 6: status = LaunchForward<32, 32>(opsin, stride, pitch, list, counts + f, max_count, d, coef, stream); break;
+      case 0: status = LaunchForward<8, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 1: status = LaunchForward<8, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 2: status = LaunchForward<16, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 3: status = LaunchForward<16, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 4: status = LaunchForward<16, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 5: status = LaunchForward<32, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 6: status = LaunchForward<32, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
     }
   }
   return status;
@@ -1035,10 +1112,22 @@ int AqPolicySetup(const float* field, size_t blocks, float target, float* range,
   return CheckLaunch("aq policy setup");
 }
 
+size_t AqSelectStateBytes() { return sizeof(SelectState); }
+
 int AqQuantizer_(const float* field, size_t blocks, const AqPolicy* policy, AqQuantizer* q,
-                 int32_t* raw, uint32_t* error, cudaStream_t stream) {
-  QuantizerKernel<<<1, 1024, 0, stream>>>(field, static_cast<int>(blocks), policy, q, error);
-  RawQuantKernel<<<Blocks(blocks), kThreads, 0, stream>>>(field, static_cast<int>(blocks), q, raw);
+                 int32_t* raw, void* select_state, uint32_t* error, cudaStream_t stream) {
+  SelectState* st = static_cast<SelectState*>(select_state);
+  const int n = static_cast<int>(blocks);
+  const unsigned grid = static_cast<unsigned>(std::min<size_t>(Blocks(blocks), 4 * 148));
+  SelectInitKernel<<<1, 1024, 0, stream>>>(st, n);
+  for (int selection = 0; selection < 2; ++selection) {
+    for (int pass = 0; pass < kSelectPasses; ++pass) {
+      SelectHistogramKernel<<<grid, kThreads, 0, stream>>>(field, n, selection == 1, pass, st);
+      SelectDigitKernel<<<1, 1024, 0, stream>>>(pass, n, selection == 1, st);
+    }
+  }
+  QuantizerKernel<<<1, 1, 0, stream>>>(st, policy, q, error);
+  RawQuantKernel<<<Blocks(blocks), kThreads, 0, stream>>>(field, n, q, raw);
   return CheckLaunch("aq quantizer");
 }
 

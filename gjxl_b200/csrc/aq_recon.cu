@@ -19,6 +19,7 @@
 #include "aq.h"
 #include "common.cuh"
 #include "host_util.h"
+#include "line_dct.cuh"
 #include "tables.h"
 #include "transform.cuh"
 
@@ -82,11 +83,11 @@ __device__ __forceinline__ int LenIdx(int len) { return len == 1 ? 0 : len == 2 
 // ConvertDcToLowFrequencies for one channel of one transform.
 template <int W, int H>
 __device__ void DcToLowFrequencies(const float* dc_plane, int blocks_x, int ax, int ay,
-                                   float* coef) {
+                                   float* plane, int row_pitch) {
   using S = TransformShape<W, H>;
   constexpr int CW = S::CW, CH = S::CH;
   const int lh = LenIdx(CH), lw = LenIdx(CW);
-  float low[16];
+  // LLF coefficient (v, u) lands at row v, column u of the natural plane.
   for (int v = 0; v < CH; ++v) {
     for (int u = 0; u < CW; ++u) {
       double value = 0.0;
@@ -96,13 +97,11 @@ __device__ void DcToLowFrequencies(const float* dc_plane, int blocks_x, int ax, 
                    c_dc_recon.forward[lh][v][y] * c_dc_recon.forward[lw][u][x];
         }
       }
-      const int small = CH < CW ? v * CW + u : u * CH + v;
-      low[small] = static_cast<float>(value * static_cast<double>(c_dc_recon.upsample[lh][v]) *
-                                      static_cast<double>(c_dc_recon.upsample[lw][u]));
+      plane[v * row_pitch + u] =
+        static_cast<float>(value * static_cast<double>(c_dc_recon.upsample[lh][v]) *
+                           static_cast<double>(c_dc_recon.upsample[lw][u]));
     }
   }
-  for (int v = 0; v < CH; ++v)
-    for (int u = 0; u < CW; ++u) coef[S::Index(v, u)] = low[CH < CW ? v * CW + u : u * CH + v];
 }
 
 struct ReconParams {
@@ -120,18 +119,23 @@ struct ReconParams {
   int tiles_x;
   const float* dequant;  // family table [3][N]
   const float* matrix_multiplier;  // device, X / Y / B
-  const double* iw;
-  const double* ih;
   float* recon;
 };
 
+// K = 1024 / N transforms (3 channels each) per CTA of 384 threads; the
+// inverse DCT gives every thread one 8-output chunk of one line per pass
+// (line_dct.cuh). Coefficients sit at their natural (v, u) position of a
+// padded plane.
+constexpr int kReconThreads = 384;
+
 template <int W, int H>
-__global__ void __launch_bounds__(kThreads) ReconstructKernel(const __grid_constant__ ReconParams p) {
-  constexpr int N = W * H;
-  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+__global__ void __launch_bounds__(kReconThreads, 2) ReconstructKernel(const __grid_constant__ ReconParams p) {
+  constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
+  using Batch = PlaneBatch<W, H, KC>;
+  static_assert(Batch::Items == kReconThreads, "one chunk per thread and pass");
   extern __shared__ __align__(16) unsigned char smem[];
-  float* coef = reinterpret_cast<float*>(smem);                // [K*3][N]
-  double* tmp = reinterpret_cast<double*>(coef + K * 3 * N);  // [K*3][N]
+  double* tmp = reinterpret_cast<double*>(smem);                  // [KC] padded planes
+  float* coef = reinterpret_cast<float*>(tmp + Batch::Elements);  // [KC] padded planes
   __shared__ int2 anchor[K];
   __shared__ float scales[K][3];
   __shared__ float factors[K][2];
@@ -152,40 +156,42 @@ __global__ void __launch_bounds__(kThreads) ReconstructKernel(const __grid_const
     factors[k][1] = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
   }
   __syncthreads();
-  // Dequantize.
-  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+  // Dequantize coefficient j = coefficient_index(v, u) (footprint (j % W, j / W))
+  // into (v, u).
+  for (int i = threadIdx.x; i < active * 3 * N; i += kReconThreads) {
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
     const int2 a = anchor[k];
     const int32_t qv =
       p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W];
-    coef[i] = QuantBiasR(qv, c) * (p.dequant[c * N + j] * scales[k][c]);
+    coef[Batch::At(k * 3 + c, v, u)] = QuantBiasR(qv, c) * (p.dequant[c * N + j] * scales[k][c]);
   }
   __syncthreads();
   // Restore the chroma from luma.
-  for (int i = threadIdx.x; i < active * N; i += kThreads) {
-    const int k = i / N, j = i % N;
-    float* cf = coef + k * 3 * N;
-    const float y = cf[N + j];
-    cf[j] += factors[k][0] * y;
-    cf[2 * N + j] += factors[k][1] * y;
+  for (int i = threadIdx.x; i < active * N; i += kReconThreads) {
+    const int k = i / N, r = i % N, v = r / W, u = r % W;
+    const float y = coef[Batch::At(k * 3 + 1, v, u)];
+    coef[Batch::At(k * 3 + 0, v, u)] += factors[k][0] * y;
+    coef[Batch::At(k * 3 + 2, v, u)] += factors[k][1] * y;
   }
   __syncthreads();
   // LLF from the (smoothed) DC, one thread per transform channel.
   if (threadIdx.x < active * 3) {
     const int k = threadIdx.x / 3, c = threadIdx.x % 3;
     DcToLowFrequencies<W, H>(p.dc + c * p.dc_pitch, p.blocks_x, anchor[k].x, anchor[k].y,
-                             coef + (k * 3 + c) * N);
+                             coef + Batch::At(k * 3 + c, 0, 0), Batch::RowPitch);
   }
   __syncthreads();
-  InverseRows<W, H>(coef, tmp, p.iw, active * 3, threadIdx.x, kThreads);
+  const auto present = [&](int plane) { return plane < 3 * active; };
+  BatchRowPass<W, H, KC, false>(coef, tmp, threadIdx.x, kReconThreads, present);
   __syncthreads();
-  InverseColumns<W, H>(tmp, coef, p.ih, active * 3, threadIdx.x, kThreads);
+  BatchColumnPass<W, H, KC, false>(tmp, coef, threadIdx.x, kReconThreads, present);
   __syncthreads();
-  for (int i = threadIdx.x; i < active * 3 * N; i += kThreads) {
+  for (int i = threadIdx.x; i < active * 3 * N; i += kReconThreads) {
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
     const int2 a = anchor[k];
     p.recon[c * p.pitch + static_cast<size_t>(a.y * 8 + yx / W) * p.stride + a.x * 8 + yx % W] =
-      coef[i];
+      coef[Batch::At(k * 3 + c, yx / W, yx % W)];
   }
 }
 
@@ -433,15 +439,11 @@ int AqSmoothDc(const float* dc, size_t bx, size_t by, const AqQuantizer* q, floa
 template <int W, int H>
 int LaunchReconstruct(ReconParams p, const DeviceTables& d, int family, size_t max_count,
                       cudaStream_t stream) {
-  constexpr int N = W * H;
-  constexpr int K = N >= 1024 ? 1 : 1024 / N;
+  constexpr int N = W * H, K = 1024 / N;
   const HostTables& h = GetHostTables();
   const int table = StrategyTableFamily(FamilyStrategy(family));
   p.dequant = d.dequant + h.layout.offset[table];
-  const int wi = W == 8 ? 0 : W == 16 ? 1 : 2, hi = H == 8 ? 0 : H == 16 ? 1 : 2;
-  p.iw = d.inverse[wi];
-  p.ih = d.inverse[hi];
-  const size_t smem = static_cast<size_t>(K) * 3 * N * 12;
+  const size_t smem = static_cast<size_t>(PlaneBatch<W, H, 3 * K>::Elements) * 12;
   int status = CheckCuda(cudaFuncSetAttribute(ReconstructKernel<W, H>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(smem)),
@@ -449,7 +451,7 @@ int LaunchReconstruct(ReconParams p, const DeviceTables& d, int family, size_t m
   if (status != GJXL_B200_OK) return status;
   const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
   if (grid == 0) return GJXL_B200_OK;
-  ReconstructKernel<W, H><<<grid, kThreads, smem, stream>>>(p);
+  ReconstructKernel<W, H><<<grid, kReconThreads, smem, stream>>>(p);
   return CheckLaunch("aq reconstruct");
 }
 

@@ -349,7 +349,6 @@ struct MaltaParams {
   int w, h;
   float norm2_gt, norm2_lt;  // float casts of pre * norm
   float norm;                // static_cast<float>(norm)
-  bool low_frequency;
 };
 
 __device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
@@ -365,11 +364,9 @@ __device__ __forceinline__ float Sum9(float a, float b, float c, float d, float 
   return (Sum4(a, b, c, d) + Sum4(e, f, g, h)) + i;
 }
 
-// Scaled difference of MaltaDiffMap (butteraugli_distance_internal.cpp:544-575).
-__device__ __forceinline__ float MaltaScaled(const MaltaParams& p, int x, int y) {
-  if (x < 0 || y < 0 || x >= p.w || y >= p.h) return 0.0f;
-  const size_t i = static_cast<size_t>(y) * p.w + x;
-  const float v0 = p.image0[i], v1 = p.image1[i];
+// Scaled difference of MaltaDiffMap (butteraugli_distance_internal.cpp:544-575)
+// of the samples v0 (reference side) and v1 at one position.
+__device__ __forceinline__ float MaltaScaledValue(const MaltaParams& p, float v0, float v1) {
   const float absolute = 0.5f * (fabsf(v0) + fabsf(v1));
   const float difference = v0 - v1;
   const float scaler = p.norm2_gt / (p.norm + absolute);
@@ -394,30 +391,28 @@ __device__ __forceinline__ float MaltaScaled(const MaltaParams& p, int x, int y)
   return scaled;
 }
 
-constexpr int kMaltaTile = 16;
+// Output tile of one CTA: 64 x 16 pixels, each of the 256 threads computing
+// kMaltaRun = 4 horizontally adjacent outputs. The scaled differences of the
+// tile plus a 4-pixel halo (zero outside the image) are staged in shared
+// memory; every thread then copies the 9 x 12 window its four outputs read
+// into registers with 128-bit loads, so each staged value is loaded once per
+// thread instead of once per tap.
+constexpr int kMaltaRun = 4;
+constexpr int kMaltaTileW = 64, kMaltaTileH = 16;
 constexpr int kMaltaHalo = 4;
-constexpr int kMaltaSpan = kMaltaTile + 2 * kMaltaHalo;
+constexpr int kMaltaSpanW = kMaltaTileW + 2 * kMaltaHalo;  // 72 (16-byte rows)
+constexpr int kMaltaSpanH = kMaltaTileH + 2 * kMaltaHalo;  // 24
+constexpr int kMaltaWindowW = kMaltaRun + 2 * kMaltaHalo;   // 12
+constexpr int kMaltaThreads = (kMaltaTileW / kMaltaRun) * kMaltaTileH;
 
-// Scaled differences of a 16x16 tile (+4 halo, zero outside the image) in
-// shared memory, then the Malta line sums (MaltaUnitLf / MaltaUnitFull,
-// :156-281) per pixel, added onto the accumulator.
-__global__ void __launch_bounds__(kMaltaTile * kMaltaTile)
-MaltaKernel(const __grid_constant__ MaltaParams p) {
-  __shared__ float tile[kMaltaSpan][kMaltaSpan + 1];
-  const int x0 = blockIdx.x * kMaltaTile - kMaltaHalo;
-  const int y0 = blockIdx.y * kMaltaTile - kMaltaHalo;
-  for (int i = threadIdx.x; i < kMaltaSpan * kMaltaSpan; i += blockDim.x) {
-    const int ty = i / kMaltaSpan, tx = i % kMaltaSpan;
-    tile[ty][tx] = MaltaScaled(p, x0 + tx, y0 + ty);
-  }
-  __syncthreads();
-  const int lx = threadIdx.x % kMaltaTile, ly = threadIdx.x / kMaltaTile;
-  const int x = blockIdx.x * kMaltaTile + lx, y = blockIdx.y * kMaltaTile + ly;
-  if (x >= p.w || y >= p.h) return;
-  auto P = [&](int dx, int dy) { return tile[ly + kMaltaHalo + dy][lx + kMaltaHalo + dx]; };
-  float r;
-  if (p.low_frequency) {
-    float s = Sum5(P(-4, 0), P(-2, 0), P(0, 0), P(2, 0), P(4, 0));
+// MaltaUnitLf / MaltaUnitFull (butteraugli_distance_internal.cpp:156-281) at
+// output k of the window: the 16 line sums with the reference's association.
+template <bool kLowFrequency, int K>
+__device__ __forceinline__ float MaltaUnit(const float (&v)[2 * kMaltaHalo + 1][kMaltaWindowW]) {
+#define P(dx, dy) v[(dy) + kMaltaHalo][K + kMaltaHalo + (dx)]
+  float r, s;
+  if constexpr (kLowFrequency) {
+    s = Sum5(P(-4, 0), P(-2, 0), P(0, 0), P(2, 0), P(4, 0));
     r = s * s;
     s = Sum5(P(0, -4), P(0, -2), P(0, 0), P(0, 2), P(0, 4)); r = s * s + r;
     s = Sum5(P(-3, -3), P(-2, -2), P(0, 0), P(2, 2), P(3, 3)); r = s * s + r;
@@ -435,8 +430,8 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
     s = Sum5(P(-2, -4), P(-1, -2), P(0, 0), P(1, 2), P(2, 4)); r = s * s + r;
     s = Sum5(P(2, -4), P(1, -2), P(0, 0), P(-1, 2), P(-2, 4)); r = s * s + r;
   } else {
-    float s = Sum9(P(-4, 0), P(-3, 0), P(-2, 0), P(-1, 0), P(0, 0), P(1, 0), P(2, 0), P(3, 0),
-                   P(4, 0));
+    s = Sum9(P(-4, 0), P(-3, 0), P(-2, 0), P(-1, 0), P(0, 0), P(1, 0), P(2, 0), P(3, 0),
+             P(4, 0));
     r = s * s;
     s = Sum9(P(0, -4), P(0, -3), P(0, -2), P(0, -1), P(0, 0), P(0, 1), P(0, 2), P(0, 3), P(0, 4));
     r = s * s + r;
@@ -471,9 +466,64 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
              P(-1, 4));
     r = s * s + r;
   }
-  const size_t i = static_cast<size_t>(y) * p.w + x;
-  // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
-  p.accumulate[i] = p.accumulate[i] + (0.0f + r);
+#undef P
+  return r;
+}
+
+// Scaled differences of the tile in shared memory, then the Malta line sums
+// of four outputs per thread, added onto the accumulator.
+template <bool kLowFrequency>
+__global__ void __launch_bounds__(kMaltaThreads, 3)
+MaltaKernel(const __grid_constant__ MaltaParams p) {
+  __shared__ __align__(16) float tile[kMaltaSpanH][kMaltaSpanW];
+  const int x0 = blockIdx.x * kMaltaTileW - kMaltaHalo;
+  const int y0 = blockIdx.y * kMaltaTileH - kMaltaHalo;
+  // Staging: both planes' samples are loaded first (all in flight at once),
+  // then scaled.
+  constexpr int kStage = (kMaltaSpanW * kMaltaSpanH + kMaltaThreads - 1) / kMaltaThreads;
+  float v0[kStage], v1[kStage];
+#pragma unroll
+  for (int j = 0; j < kStage; ++j) {
+    const int i = threadIdx.x + j * kMaltaThreads;
+    const int ty = i / kMaltaSpanW, tx = i % kMaltaSpanW, x = x0 + tx, y = y0 + ty;
+    const bool inside = i < kMaltaSpanW * kMaltaSpanH && x >= 0 && y >= 0 && x < p.w && y < p.h;
+    const size_t at = inside ? static_cast<size_t>(y) * p.w + x : 0;
+    v0[j] = inside ? p.image0[at] : 0.0f;
+    v1[j] = inside ? p.image1[at] : 0.0f;
+  }
+#pragma unroll
+  for (int j = 0; j < kStage; ++j) {
+    const int i = threadIdx.x + j * kMaltaThreads;
+    if (i >= kMaltaSpanW * kMaltaSpanH) break;
+    const int ty = i / kMaltaSpanW, tx = i % kMaltaSpanW, x = x0 + tx, y = y0 + ty;
+    const bool inside = x >= 0 && y >= 0 && x < p.w && y < p.h;
+    tile[ty][tx] = inside ? MaltaScaledValue(p, v0[j], v1[j]) : 0.0f;
+  }
+  __syncthreads();
+  const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
+  const int ly = threadIdx.x / (kMaltaTileW / kMaltaRun);
+  float v[2 * kMaltaHalo + 1][kMaltaWindowW];
+#pragma unroll
+  for (int dy = 0; dy < 2 * kMaltaHalo + 1; ++dy) {
+#pragma unroll
+    for (int q = 0; q < kMaltaWindowW / 4; ++q) {
+      const float4 f = *reinterpret_cast<const float4*>(&tile[ly + dy][lx + 4 * q]);
+      v[dy][4 * q + 0] = f.x;
+      v[dy][4 * q + 1] = f.y;
+      v[dy][4 * q + 2] = f.z;
+      v[dy][4 * q + 3] = f.w;
+    }
+  }
+  const float r[kMaltaRun] = {MaltaUnit<kLowFrequency, 0>(v), MaltaUnit<kLowFrequency, 1>(v),
+                              MaltaUnit<kLowFrequency, 2>(v), MaltaUnit<kLowFrequency, 3>(v)};
+  const int x = blockIdx.x * kMaltaTileW + lx, y = blockIdx.y * kMaltaTileH + ly;
+  if (y >= p.h) return;
+  float* out = p.accumulate + static_cast<size_t>(y) * p.w + x;
+#pragma unroll
+  for (int k = 0; k < kMaltaRun; ++k) {
+    // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
+    if (x + k < p.w) out[k] = out[k] + (0.0f + r[k]);
+  }
 }
 
 struct L2Params {
@@ -839,7 +889,7 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
   const int plane_of[6] = {kMF + 1, kMF + 0, kHF + 1, kHF + 0, kUHF + 1, kUHF + 0};
   cudaMemsetAsync(s.ac, 0, 3 * n * sizeof(float), stream);
   const int order[6] = {4, 5, 2, 3, 0, 1};
-  dim3 tiles((s.w + kMaltaTile - 1) / kMaltaTile, (s.h + kMaltaTile - 1) / kMaltaTile);
+  dim3 tiles((s.w + kMaltaTileW - 1) / kMaltaTileW, (s.h + kMaltaTileH - 1) / kMaltaTileH);
   for (int index : order) {
     MaltaParams mp;
     mp.image0 = s.ref_psycho + plane_of[index] * n;
@@ -856,8 +906,11 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
     mp.norm2_gt = static_cast<float>(pre_gt * kMaltaNorms[index]);
     mp.norm2_lt = static_cast<float>(pre_lt * kMaltaNorms[index]);
     mp.norm = static_cast<float>(kMaltaNorms[index]);
-    mp.low_frequency = lf;
-    MaltaKernel<<<tiles, kMaltaTile * kMaltaTile, 0, stream>>>(mp);
+    if (lf) {
+      MaltaKernel<true><<<tiles, kMaltaThreads, 0, stream>>>(mp);
+    } else {
+      MaltaKernel<false><<<tiles, kMaltaThreads, 0, stream>>>(mp);
+    }
   }
   // kL2Weights (:32-36).
   const float kL2[9] = {400.0f, 1.50815703118f, 0.0f, 2150.0f, 10.6195433239f, 16.2176043152f,

@@ -11,8 +11,9 @@
 //
 // One CTA of 256 threads per tile. Phase 1: each warp transforms (block,
 // channel) pairs — lane l owns row-pass outputs l and l+32 and gathers the
-// column inputs with double shuffles. Phase 2: warp 0 solves both maps, twelve
-// lanes per map, each lane owning one of the 3 derivative sums x 4 lanes.
+// column inputs with double shuffles. Phase 2: per Newton iteration all
+// threads evaluate the derivative terms chunk by chunk and warp 0 adds them
+// in order, twelve lanes per map, each owning one of the 3 sums x 4 lanes.
 
 #include <cmath>
 #include <cstring>
@@ -25,6 +26,7 @@ namespace gjxl_b200 {
 namespace {
 
 constexpr int kTileValues = 64 * 64;  // up to 64 blocks of 64 coefficients
+constexpr int kCflChunk = 256;        // elements per shared term chunk (divides kTileValues)
 
 struct CflParams {
   const float* opsin;  // Gaborish-inverted padded XYB
@@ -132,61 +134,90 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   }
   __syncthreads();
 
-  // Phase 2: FindBestMultiplier (non-fast) for both maps in warp 0: lanes
-  // 0..11 solve y_to_x, lanes 12..23 solve y_to_b; within a group, lane
-  // 4 * kind + slot owns derivative sum `kind` (center, +eps, -eps) over the
-  // elements i = slot (mod 4), in increasing i like the reference.
-  if (warp != 0) return;
-  const int group = lane / 12;  // 0: y_to_x, 1: y_to_b, 2: idle lanes
-  const int member = lane % 12;
-  const int kind = member / 4, slot = member % 4;
-  const float* A = group == 0 ? luma_x : luma_b;    // a = luma / 84
-  const float* Bv = group == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
+  // Phase 2: FindBestMultiplier (non-fast) for both maps. Per iteration the
+  // element terms of the three derivative sums (center, +eps, -eps) are
+  // computed by all threads, a chunk of kCflChunk elements at a time, into
+  // shared memory; then warp 0 adds them in the reference's order: lanes
+  // 0..11 solve y_to_x and 12..23 y_to_b, lane 4 * kind + slot of a group
+  // owning derivative sum `kind` over the elements i = slot (mod 4), in
+  // increasing i. Elements skipped by the reference contribute +0.0, which
+  // leaves the (never -0.0) sum unchanged.
+  // Rows padded by 4 floats: the 24 summing lanes read 24 distinct banks.
+  __shared__ float terms[2][3][kCflChunk + 4];
+  __shared__ float solution[2];
+  __shared__ int solved[2];
   const int count = blocks * 64;
   const float kDistanceMultiplierAc = 1.0e-9f;
   const float kEpsilon = 100.0f;
-  float x = 0.0f;
-  bool done = group == 2;
+  if (threadIdx.x < 2) {
+    solution[threadIdx.x] = 0.0f;
+    solved[threadIdx.x] = 0;
+  }
+  const int group = lane / 12;  // warp 0: 0 y_to_x, 1 y_to_b, 2 idle lanes
+  const int member = lane % 12;
+  const int kind = member / 4, slot = member % 4;
+  float lane_sum = 0.0f;
+  __syncthreads();
   for (int iteration = 0; iteration < p.iterations; ++iteration) {
-    if (__all_sync(0xffffffffu, done)) break;
-    float lane_sum = 0.0f;
-    if (!done) {
-      const float offset = kind == 0 ? x : kind == 1 ? x + kEpsilon : x - kEpsilon;
-#pragma unroll 4
-      for (int i = slot; i < count; i += 4) {
-        const float a = A[i], b = Bv[i];
+    if (solved[0] && solved[1]) break;
+    const float x_map[2] = {solution[0], solution[1]};
+    const int done_map[2] = {solved[0], solved[1]};
+    lane_sum = 0.0f;
+    for (int chunk = 0; chunk < count; chunk += kCflChunk) {
+      for (int t = threadIdx.x; t < 2 * kCflChunk; t += blockDim.x) {
+        const int map = t / kCflChunk, e = t % kCflChunk, i = chunk + e;
+        if (done_map[map] || i >= count) continue;
+        const float* A = map == 0 ? luma_x : luma_b;    // a = luma / 84
+        const float* Bv = map == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
+        const float a = A[i], b = Bv[i], x = x_map[map];
         const float center = fmaf(a, x, b);
-        const float r = kind == 0 ? center : fmaf(a, offset, b);
-        float d = (2.0f / 3.0f) * a * (fabsf(r) + 1.0f);
-        d = r < 0.0f ? -d : d;
-        // Skipped elements add +0.0, which leaves the (never -0.0) sum unchanged.
-        lane_sum += fabsf(center) >= 100.0f ? 0.0f : d;
+        const bool skip = fabsf(center) >= 100.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float offset = k == 0 ? x : k == 1 ? x + kEpsilon : x - kEpsilon;
+          const float r = k == 0 ? center : fmaf(a, offset, b);
+          float d = (2.0f / 3.0f) * a * (fabsf(r) + 1.0f);
+          d = r < 0.0f ? -d : d;
+          terms[map][k][e] = skip ? 0.0f : d;
+        }
+      }
+      __syncthreads();
+      if (warp == 0 && group < 2 && !done_map[group]) {
+        const float* t = terms[group][kind];
+        const int limit = min(kCflChunk, count - chunk);
+#pragma unroll 8
+        for (int e = slot; e < limit; e += 4) lane_sum += t[e];
+      }
+      __syncthreads();
+    }
+    if (warp == 0) {
+      // Horizontal sums (l0 + l1) + (l2 + l3) for each kind of this group.
+      const int group_base = 12 * (group < 2 ? group : 0);
+      float sums[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float l0 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 0);
+        const float l1 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 1);
+        const float l2 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 2);
+        const float l3 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 3);
+        sums[k] = (l0 + l1) + (l2 + l3);
+      }
+      if (group < 2 && member == 0 && !done_map[group]) {
+        const float x = x_map[group];
+        const float n = static_cast<float>(count);
+        const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
+        const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
+        const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
+        const float second = (plus - minus) / (2.0f * kEpsilon);
+        const float step = center / (second + 0.85f);
+        solution[group] = x - fminf(fmaxf(step, -20.0f), 20.0f);
+        if (fabsf(step) < 3.0e-3f) solved[group] = 1;
       }
     }
-    // Horizontal sums (l0 + l1) + (l2 + l3) for each kind of this group.
-    const int group_base = 12 * (group < 2 ? group : 0);
-    float sums[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float l0 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 0);
-      const float l1 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 1);
-      const float l2 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 2);
-      const float l3 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 3);
-      sums[k] = (l0 + l1) + (l2 + l3);
-    }
-    if (!done) {
-      const float n = static_cast<float>(count);
-      const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
-      const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
-      const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
-      const float second = (plus - minus) / (2.0f * kEpsilon);
-      const float step = center / (second + 0.85f);
-      x -= fminf(fmaxf(step, -20.0f), 20.0f);
-      if (fabsf(step) < 3.0e-3f) done = true;
-    }
+    __syncthreads();
   }
-  if (lane == 0) p.y_to_x[tile] = QuantizeMultiplier(x);
-  if (lane == 12) p.y_to_b[tile] = QuantizeMultiplier(x);
+  if (threadIdx.x == 0) p.y_to_x[tile] = QuantizeMultiplier(solution[0]);
+  if (threadIdx.x == 1) p.y_to_b[tile] = QuantizeMultiplier(solution[1]);
 }
 
 }  // namespace

@@ -82,3 +82,58 @@ __device__ __forceinline__ void LineChunkAt(int chunk, const In* __restrict__ in
 }
 
 }  // namespace gjxl_b200
+
+namespace gjxl_b200 {
+
+// A batch of KC = transforms x channels W x H planes in shared memory,
+// [plane][row][column] with rows padded to W + 1 elements: threads on
+// consecutive rows (row passes) and threads on consecutive columns (column
+// passes) then hit distinct banks. Items = one 8-output chunk of one line,
+// KC * W * H / 8 per pass.
+template <int W, int H, int KC>
+struct PlaneBatch {
+  static constexpr int N = W * H;
+  static constexpr int RowPitch = W + 1;
+  static constexpr int PlanePitch = H * RowPitch;
+  static constexpr int Elements = KC * PlanePitch;
+  static constexpr int Items = KC * N / 8;
+  static_assert((KC * H) % 32 == 0 && (KC * W) % 32 == 0, "warp-uniform chunks");
+  __device__ static int At(int plane, int row, int column) {
+    return plane * PlanePitch + row * RowPitch + column;
+  }
+};
+
+// Row pass over all KC * H rows of `in` into `out` (same layout): item
+// `item` is chunk item / (KC * H) of row item % (KC * H). `valid(plane)`
+// skips planes of absent transforms.
+template <int W, int H, int KC, bool kForward, typename In, typename Valid>
+__device__ __forceinline__ void BatchRowPass(const In* in, double* out, int tid, int threads,
+                                             Valid valid) {
+  using B = PlaneBatch<W, H, KC>;
+  constexpr int kLines = KC * H;
+  for (int item = tid; item < B::Items; item += threads) {
+    const int chunk = item / kLines, line = item % kLines;
+    if (!valid(line / H)) continue;
+    LineChunkAt<W, kForward, 1, 1>(chunk, in + line * B::RowPitch,
+                                   out + line * B::RowPitch + chunk * 8);
+  }
+}
+
+// Column pass over all KC * W columns: item `item` is chunk item / (KC * W)
+// of column item % (KC * W).
+template <int W, int H, int KC, bool kForward, typename Out, typename Valid>
+__device__ __forceinline__ void BatchColumnPass(const double* in, Out* out, int tid, int threads,
+                                                Valid valid) {
+  using B = PlaneBatch<W, H, KC>;
+  constexpr int kLines = KC * W;
+  for (int item = tid; item < B::Items; item += threads) {
+    const int chunk = item / kLines, line = item % kLines;
+    const int plane = line / W, u = line % W;
+    if (!valid(plane)) continue;
+    const int base = plane * B::PlanePitch + u;
+    LineChunkAt<H, kForward, B::RowPitch, B::RowPitch>(chunk, in + base,
+                                                       out + base + chunk * 8 * B::RowPitch);
+  }
+}
+
+}  // namespace gjxl_b200

@@ -115,6 +115,7 @@ struct Session {
   float* range = nullptr;
   AqPolicy* policy = nullptr;
   AqQuantizer* quantizer = nullptr;
+  void* select_state = nullptr;
   int32_t* raw = nullptr;
   int8_t* final_y_to_x = nullptr;
   int8_t* final_y_to_b = nullptr;
@@ -163,8 +164,18 @@ struct Session {
   int32_t* host_qac = nullptr;
   cudaEvent_t events[kStageCount + 1] = {};
   bool events_created = false;
+  // The analysis as one CUDA graph, captured on the first analyze() call for
+  // a given input pointer / stride / channel count and replayed afterwards.
+  cudaStream_t capture_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  const uint8_t* graph_pixels = nullptr;
+  size_t graph_stride = 0;
+  int graph_channels = 0;
+  bool graph_disabled = false;
 
   ~Session() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
     if (arena) cudaFree(arena);
     if (host_block) cudaFreeHost(host_block);
     if (butteraugli) ButteraugliDestroy(butteraugli);
@@ -214,6 +225,7 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->range), 4 * sizeof(float)},
     {reinterpret_cast<void**>(&s->policy), sizeof(AqPolicy)},
     {reinterpret_cast<void**>(&s->quantizer), sizeof(AqQuantizer)},
+    {reinterpret_cast<void**>(&s->select_state), AqSelectStateBytes()},
     {reinterpret_cast<void**>(&s->raw), blocks * sizeof(int32_t)},
     {reinterpret_cast<void**>(&s->final_y_to_x), tiles},
     {reinterpret_cast<void**>(&s->final_y_to_b), tiles},
@@ -324,7 +336,8 @@ int RunAq(Session* s, cudaStream_t stream) {
   GJXL_TRY(ButteraugliPrepare(s->butteraugli, s->linear, s->lin_stride, s->lin_pitch, stream));
   Mark(s, kStageAqLoop, stream);
   for (int iteration = 0; iteration <= s->iterations; ++iteration) {
-    GJXL_TRY(AqQuantizer_(s->field, blocks, s->policy, s->quantizer, s->raw, s->error, stream));
+    GJXL_TRY(AqQuantizer_(s->field, blocks, s->policy, s->quantizer, s->raw, s->select_state,
+                          s->error, stream));
     GJXL_TRY(AqFinalCfl(s->cells, s->bx, s->by, s->coef, s->pw, s->pitch, s->raw, s->quantizer,
                         s->final_y_to_x, s->final_y_to_b, stream));
     GJXL_TRY(AqCoding(s->anchors, s->anchor_counts, s->bx, s->by, s->coef, s->pw, s->pitch,
@@ -420,6 +433,52 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
                                      sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
                      "session: error word"));
   return GJXL_B200_OK;
+}
+
+// Runs the analysis as a replay of its captured graph: one launch instead of
+// ~280, with the same kernels and arguments. Stage profiling, a caller stream
+// that is itself being captured, or a failed capture run the stages directly.
+int RunReplay(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
+              cudaStream_t stream) {
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  if (s->events_created || s->graph_disabled ||
+      cudaStreamIsCapturing(stream, &capturing) != cudaSuccess ||
+      capturing != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return Run(s, pixels, row_stride, channels, stream);
+  }
+  if (s->graph == nullptr || s->graph_pixels != pixels || s->graph_stride != row_stride ||
+      s->graph_channels != channels) {
+    if (s->graph != nullptr) {
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    if (s->capture_stream == nullptr) {
+      GJXL_TRY(CheckCuda(cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking),
+                         "session: capture stream"));
+    }
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeRelaxed) ==
+              cudaSuccess;
+    if (ok) {
+      const int run_status = Run(s, pixels, row_stride, channels, s->capture_stream);
+      ok = cudaStreamEndCapture(s->capture_stream, &graph) == cudaSuccess &&
+           run_status == GJXL_B200_OK;
+    }
+    if (ok) ok = cudaGraphInstantiate(&s->graph, graph, 0) == cudaSuccess;
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    if (!ok) {
+      cudaGetLastError();
+      ClearLastError();
+      s->graph = nullptr;
+      s->graph_disabled = true;
+      return Run(s, pixels, row_stride, channels, stream);
+    }
+    s->graph_pixels = pixels;
+    s->graph_stride = row_stride;
+    s->graph_channels = channels;
+  }
+  return CheckCuda(cudaGraphLaunch(s->graph, stream), "session: graph launch");
 }
 
 int CopyOutputs(Session* s, cudaStream_t stream) {
@@ -538,7 +597,7 @@ extern "C" int gjxl_b200_session_analyze(gjxl_b200_session* s, const uint8_t* pi
   if (s == nullptr || pixels == nullptr) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze: null argument");
   }
-  return Run(s, pixels, row_stride, channels, static_cast<cudaStream_t>(stream));
+  return RunReplay(s, pixels, row_stride, channels, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_t* host_pixels,
@@ -555,7 +614,7 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->pixels, host_pixels, bytes, cudaMemcpyHostToDevice, st),
                      "session: input upload"));
-  GJXL_TRY(Run(s, s->pixels, row_stride, channels, st));
+  GJXL_TRY(RunReplay(s, s->pixels, row_stride, channels, st));
   GJXL_TRY(CopyOutputs(s, st));
   s->host_token_count = 0;
   if (s->tokens != nullptr) {
