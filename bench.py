@@ -165,9 +165,12 @@ def candidate_cost_fp64_ops(blocks_x: int, blocks_y: int) -> int:
     return total
 
 
-# DRAM traffic of the seven candidate-cost launches for one analysis of the
-# workload, from an ncu capture (None until captured).
-COST_KERNEL_DRAM_BYTES = None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the seven
+# candidate-cost launches of one analysis: 354.57 MB measured by ncu on the
+# 2048x1536 image of the same generator, scaled by the pixel ratio to
+# 4032x3024 (each launch reads the three XYB planes and the pixel mask once,
+# 16 B per pixel, so traffic grows with the image area).
+COST_KERNEL_DRAM_BYTES = round(354_570_240 * (4032 * 3024) / (2048 * 1536))
 
 
 def fp64_peak_tflops(stream: int) -> float:
@@ -289,7 +292,9 @@ def run_gpu(args) -> dict:
             "peak_source": ("measured live: gjxl_b200_fp64_throughput (independent DMUL/DADD "
                             "chains on every SM); MEASURED_PEAKS.json has no FP64 figure"),
             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum summed over "
-                               "the 7 family launches of one analysis of this workload"),
+                               "the 7 family launches, captured at 2048x1536 and scaled by "
+                               "the pixel ratio; algorithmic bytes are 16 B/px per launch "
+                               "(1.366 GB)"),
         },
         "clocks": clocks,
     }

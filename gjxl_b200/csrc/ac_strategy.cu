@@ -97,15 +97,32 @@ struct CostLayout {
   static constexpr int RowPitch = Batch::RowPitch;
   static constexpr int PlanePitch = Batch::PlanePitch;
   static constexpr int Planes = Batch::Elements;  // elements per padded buffer
-  // Ordered-sum terms: one plane of N + 1 floats per (candidate, channel), so
-  // the summing threads (one per plane, same index at the same time) hit
-  // distinct banks.
-  static constexpr int TermPitch = N + 1;
+  // Ordered-sum terms: one plane of N + 4 floats per (candidate, channel):
+  // 16-byte aligned rows for 128-bit loads, and the summing threads (one per
+  // plane, same index at the same time) of each quarter warp hit distinct
+  // banks.
+  static constexpr int TermPitch = N + 4;
   static constexpr size_t SharedBytes = static_cast<size_t>(Planes) * (4 + 4 + 8) +
                                         static_cast<size_t>(KC) * TermPitch * 4 +
                                         static_cast<size_t>(K) * N * 4;
   static_assert(Batch::Items == kCostThreads, "one chunk per thread and pass");
 };
+
+// Sequential float sum t[0] + t[1] + ... + t[n-1] (the reference's loop
+// order), read four terms at a time.
+template <int kCount>
+__device__ __forceinline__ float OrderedSum(const float* t) {
+  float sum = 0.0f;
+#pragma unroll 4
+  for (int j = 0; j < kCount; j += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(t + j);
+    sum += v.x;
+    sum += v.y;
+    sum += v.z;
+    sum += v.w;
+  }
+  return sum;
+}
 
 __device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
   return v <= 1 ? 0 : 32 - __clz(v - 1);
@@ -122,7 +139,7 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   double* T = reinterpret_cast<double*>(smem);             // [KC][H][W+1] row-pass results
   float* A = reinterpret_cast<float*>(T + Lay::Planes);    // [KC][H][W+1] pixels, residuals
   float* B = A + Lay::Planes;                              // [KC][H][W+1] coefficients, pixels
-  float* terms = B + Lay::Planes;                          // [KC][N + 1] ordered sum terms
+  float* terms = B + Lay::Planes;                          // [KC][N + 4] ordered sum terms
   float* mask = terms + KC * Lay::TermPitch;               // [K][H][W] pixel mask
   __shared__ int anchor_x[K], anchor_y[K];
   __shared__ float quant_norm[K], cfl[K][3];
@@ -220,17 +237,17 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     const float difference = scaled - rounded;
     A[kc * Lay::PlanePitch + at] = __ldg(p.dequant + c * N + j) * difference;
     terms[kc * Lay::TermPitch + j] = sqrtf(fabsf(rounded));
-    if (rounded != 0.0f) atomicAdd(&nonzero[k][c], 1u);
+    // A warp's 32 consecutive coefficients share (k, c) (N is a multiple of
+    // 32 and every thread runs the same trip count): one count per warp.
+    const unsigned nz = __ballot_sync(0xffffffffu, rounded != 0.0f);
+    if ((tid & 31) == 0 && nz != 0u) atomicAdd(&nonzero[k][c], static_cast<uint32_t>(__popc(nz)));
   }
   __syncthreads();
 
   // Ordered magnitude sums (one thread per candidate and channel); these
   // threads then join the inverse row pass, which does not touch `terms`.
   if (tid < KC && anchor_x[tid / 3] >= 0) {
-    const float* t = terms + tid * Lay::TermPitch;
-    float sum = 0.0f;
-    for (int j = 0; j < N; ++j) sum += t[j];
-    magnitude[tid / 3][tid % 3] = sum;
+    magnitude[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
   }
 
   // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
@@ -255,10 +272,7 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __syncthreads();
 
   if (tid < KC && anchor_x[tid / 3] >= 0) {
-    const float* t = terms + tid * Lay::TermPitch;
-    float sum = 0.0f;
-    for (int j = 0; j < N; ++j) sum += t[j];
-    loss_sum[tid / 3][tid % 3] = sum;
+    loss_sum[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
   }
   __syncthreads();
 

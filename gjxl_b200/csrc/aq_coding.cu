@@ -365,6 +365,7 @@ __global__ void __launch_bounds__(kFinalCflThreads)
 FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   extern __shared__ __align__(16) float terms[];  // [a_x, b_x, a_b, b_b][kFinalCflTerms]
   __shared__ int block_terms[64], offsets[64], total_terms;
+  __shared__ uint8_t group_block[64];  // anchor block of each 64-term group
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
   const int bx0 = tx * 8, by0 = ty * 8;
@@ -384,18 +385,25 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
     int running = 0;
     for (int b = 0; b < 64; ++b) {
       offsets[b] = running;
+      for (int g = running / 64; g < (running + block_terms[b]) / 64; ++g) {
+        group_block[g] = static_cast<uint8_t>(b);
+      }
       running += block_terms[b];
     }
     total_terms = running;
   }
   __syncthreads();
+  // Every thread takes terms e = tid, tid + 128, ... of the tile; every
+  // anchor's term count is a multiple of 64, so term e belongs to the anchor
+  // of group e / 64.
   const float scale128 = p.q->scale * 128.0f;
-  for (int b = warp; b < tw * th; b += kFinalCflThreads / 32) {
-    const int n = block_terms[b];
-    if (n == 0) continue;
+  const int count = total_terms;
+  for (int e = threadIdx.x; e < count; e += kFinalCflThreads) {
+    const int b = group_block[e / 64], i = e - offsets[b];
     const int bx = bx0 + b % tw, by = by0 + b / tw;
     int cw, ch, s;
     AnchorAt(p.grid, by * p.grid.blocks_x + bx, &cw, &ch, &s);
+    const int n = cw * ch * 64;
     const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
                     : s == kStrategyDct32x32 ? kTableDct32
                     : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
@@ -407,30 +415,25 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
     // LLF extent: covered blocks with the longer side first.
     const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
     const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
-    float* out = terms + offsets[b];
-#pragma unroll 4
-    for (int i = lane; i < n; i += 32) {
-      const int cy = i / sw, cx = i % sw;
-      const bool llf = cy < lfh && cx < lfw;
-      const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
-      const float luma_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
-      const float x_v = llf ? 0.0f : p.coef[at];
-      const float b_v = llf ? 0.0f : p.coef[2 * p.coef_pitch + at];
-      const float base_x = 0.0f, base_b = 1.0f;
-      const float luma_x = luma_v * inv_x[i] * quant_scale;
-      const float chroma_x = x_v * inv_x[i] * quant_scale;
-      const float luma_b = luma_v * inv_b[i] * quant_scale;
-      const float chroma_b = b_v * inv_b[i] * quant_scale;
-      out[i] = luma_x / 84.0f;
-      out[kFinalCflTerms + i] = base_x * luma_x - chroma_x;
-      out[2 * kFinalCflTerms + i] = luma_b / 84.0f;
-      out[3 * kFinalCflTerms + i] = base_b * luma_b - chroma_b;
-    }
+    const int cy = i / sw, cx = i % sw;
+    const bool llf = cy < lfh && cx < lfw;
+    const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
+    const float luma_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
+    const float x_v = llf ? 0.0f : p.coef[at];
+    const float b_v = llf ? 0.0f : p.coef[2 * p.coef_pitch + at];
+    const float base_x = 0.0f, base_b = 1.0f;
+    const float luma_x = luma_v * inv_x[i] * quant_scale;
+    const float chroma_x = x_v * inv_x[i] * quant_scale;
+    const float luma_b = luma_v * inv_b[i] * quant_scale;
+    const float chroma_b = b_v * inv_b[i] * quant_scale;
+    terms[e] = luma_x / 84.0f;
+    terms[kFinalCflTerms + e] = base_x * luma_x - chroma_x;
+    terms[2 * kFinalCflTerms + e] = luma_b / 84.0f;
+    terms[3 * kFinalCflTerms + e] = base_b * luma_b - chroma_b;
   }
   __syncthreads();
   if (warp != 0) return;
   const int problem = lane / 4, slot = lane % 4;  // problem 0: X, 1: B
-  const int count = total_terms;
   float quadratic = 0.0f, linear = 0.0f;
   if (problem < 2) {
     const float* A = terms + 2 * problem * kFinalCflTerms;
@@ -785,10 +788,10 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
 // sums in an 8-slot ring (slot x & 7) in shared memory; nothing goes to
 // global memory but the quantized output.
 //
-// One CTA per DC group, one thread per (channel, row): threads 0-255 run X,
-// 256-511 Y and 512-767 B. X and Y are independent. B's residual subtracts
-// Y's quantized value at the same position, so B runs one wave behind Y and
-// reads it from Y's ring. Slot x & 7 of a row is rewritten 8 waves later, and
+// Two CTAs per DC group, one thread per (channel, row): one CTA runs X, the
+// other Y (threads 0-255) and B (256-511). X and Y are independent. B's
+// residual subtracts Y's quantized value at the same position, so B runs one
+// wave behind Y and reads it from Y's ring. Slot x & 7 of a row is rewritten 8 waves later, and
 // a reader needs it at most 4 waves (B: 1 wave) after it was written.
 
 struct DcQuantParams {
@@ -803,7 +806,10 @@ struct DcQuantParams {
 
 constexpr int kDcGroup = 256;
 constexpr int kDcRing = 8;
-constexpr int kDcThreads = 3 * kDcGroup;
+// Two CTAs per DC group on different SMs: blockIdx.z == 0 runs X (threads
+// 0-255; 256-511 idle), blockIdx.z == 1 runs Y (0-255) and B (256-511), which
+// reads Y's ring.
+constexpr int kDcThreads = 2 * kDcGroup;
 
 struct DcRings {
   int32_t q[3][kDcRing][kDcGroup];        // quantized values
@@ -823,8 +829,9 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   const int gx0 = blockIdx.x * kDcGroup, gy0 = blockIdx.y * kDcGroup;
   const int gw = min(kDcGroup, p.width - gx0), gh = min(kDcGroup, p.height - gy0);
   const int stride = p.width;
-  const int c = threadIdx.x / kDcGroup;  // 0: X, 1: Y, 2: B
-  const int y = threadIdx.x % kDcGroup;
+  const bool idle = blockIdx.z == 0 && threadIdx.x >= kDcGroup;
+  const int c = blockIdx.z == 0 ? 0 : 1 + static_cast<int>(threadIdx.x) / kDcGroup;  // X, Y, B
+  const int y = idle ? kDcGroup : static_cast<int>(threadIdx.x) % kDcGroup;
   const int lag = c == 2 ? 1 : 0;
   for (int i = threadIdx.x; i < 64; i += blockDim.x) r.reciprocal[i] = (1u << 24) / (i + 1);
   const AqQuantizer q = *p.q;
@@ -841,7 +848,7 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   // The DC sample of the next position is loaded one wave ahead, so its
   // global-memory latency overlaps this wave's work and barrier.
   const size_t row_index = static_cast<size_t>(gy0 + min(y, gh - 1)) * stride + gx0;
-  float pending = y < gh ? source[row_index] : 0.0f;
+  float pending = y < gh ? source[row_index] : 0.0f;  // idle threads have y >= gh
   const int waves = (gw - 1) + 2 * (gh - 1) + 2;
   for (int t = 0; t < waves; ++t) {
     const int x = t - lag - 2 * y;
@@ -932,16 +939,21 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
     }
     __syncthreads();
   }
-  // Reconstructed DC (dc_quantization.cpp:209-222).
-  const float steps[3] = {q.dc_steps[0] / p.precision, step_y, q.dc_steps[2] / p.precision};
-  for (int i = threadIdx.x; i < gw * gh; i += blockDim.x) {
-    const size_t index = static_cast<size_t>(gy0 + i / gw) * stride + gx0 + i % gw;
-    const float ry = static_cast<float>(p.quantized[p.pitch + index]) * steps[1];
-    for (int ch = 0; ch < 3; ++ch) {
-      float v = static_cast<float>(p.quantized[ch * p.pitch + index]) * steps[ch];
-      if (ch == 2) v = fmaf(ry, 1.0f, v);
-      p.reconstructed[ch * p.pitch + index] = v;
-    }
+}
+
+// Reconstructed DC (dc_quantization.cpp:209-222), once both channel CTAs of
+// every group are done.
+__global__ void DcDequantKernel(const int32_t* quantized, float* reconstructed, int n,
+                                size_t pitch, const AqQuantizer* q, float precision) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float steps[3] = {q->dc_steps[0] / precision, q->dc_steps[1] / precision,
+                          q->dc_steps[2] / precision};
+  const float ry = static_cast<float>(quantized[pitch + i]) * steps[1];
+  for (int ch = 0; ch < 3; ++ch) {
+    float v = static_cast<float>(quantized[ch * pitch + i]) * steps[ch];
+    if (ch == 2) v = fmaf(ry, 1.0f, v);
+    reconstructed[ch * pitch + i] = v;
   }
 }
 
@@ -1235,8 +1247,10 @@ int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, in
                          "aq dc quantize attribute");
   if (status != GJXL_B200_OK) return status;
   dim3 grid(static_cast<unsigned>((bx + kDcGroup - 1) / kDcGroup),
-            static_cast<unsigned>((by + kDcGroup - 1) / kDcGroup));
+            static_cast<unsigned>((by + kDcGroup - 1) / kDcGroup), 2);
   DcQuantKernel<<<grid, kDcThreads, smem, stream>>>(p);
+  DcDequantKernel<<<Blocks(bx * by), kThreads, 0, stream>>>(
+    quantized, reconstructed, static_cast<int>(bx * by), bx * by, q, p.precision);
   return CheckLaunch("aq dc quantize");
 }
 

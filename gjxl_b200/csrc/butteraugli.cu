@@ -19,6 +19,7 @@
 // the second pass reads columns directly (same per-output arithmetic, no
 // transposed copy). Planes are dense float32 (stride = width).
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -158,18 +159,84 @@ __device__ __forceinline__ void ConvolveRun(const float* src, int step, int firs
   }
 }
 
+// Interior outputs o = 0..kOut-1 of a register window v[kOut + 2R] (output o
+// centred on v[o + R]), in ConvolveLine's pair-sum order.
+template <int R, int kOut>
+__device__ __forceinline__ void ConvolveWindow(const float (&v)[kOut + 2 * R], const Kernel17& k,
+                                               float (&r)[kOut]) {
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) {
+    float sums[4];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const float term = (v[o + i] + v[o + 2 * R - i]) * k.scaled[i];
+      if (i < 4) {
+        sums[i] = term;
+      } else {
+        sums[i & 3] += term;
+      }
+    }
+    float out = v[o + R] * k.scaled[R];
+#pragma unroll
+    for (int i = 0; i < (R < 4 ? R : 4); ++i) out = out + sums[i];
+    r[o] = out;
+  }
+}
+
+// Row blur: one CTA per 1024-sample segment of one row. The segment and its
+// R-sample halo are loaded into shared memory with coalesced loads; each
+// thread then reads the window of its 4 outputs with 128-bit (and, for odd
+// R, one 64-bit) shared loads. Outputs within R of the row ends use
+// ConvolveLine's renormalized border sum.
+constexpr int kRowRun = 4;
+constexpr int kRowSegment = kThreads * kRowRun;
+
 template <int R>
 __global__ void __launch_bounds__(kThreads)
 BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
                const __grid_constant__ Kernel17 k) {
-  const int plane = blockIdx.y;
-  const int runs = (w + kRun - 1) / kRun;
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= runs * h) return;
-  const int x = (i % runs) * kRun, y = i / runs;
+  constexpr int kWindow = kRowRun + 2 * R;
+  __shared__ __align__(16) float segment[kRowSegment + 2 * R + 4];
+  const int plane = blockIdx.z;
+  const int x0 = blockIdx.x * kRowSegment;
+  // Rows beyond the grid's y extent (65535) are taken in further rounds.
+  for (int y = blockIdx.y; y < h; y += gridDim.y) {
   const float* row = in + plane * in_pitch + static_cast<size_t>(y) * w;
-  ConvolveRun<R>(row, 1, x, w, k, out + plane * out_pitch + static_cast<size_t>(y) * w + x, 1,
-                 min(kRun, w - x));
+  __syncthreads();
+  // segment[j] holds sample x0 - R + j.
+  for (int j = threadIdx.x; j < kRowSegment + 2 * R; j += kThreads) {
+    const int x = x0 - R + j;
+    segment[j] = x >= 0 && x < w ? row[x] : 0.0f;
+  }
+  __syncthreads();
+  const int first = x0 + threadIdx.x * kRowRun;
+  if (first >= w) continue;
+  float* dst = out + plane * out_pitch + static_cast<size_t>(y) * w + first;
+  if (first >= R && first + kRowRun - 1 < w - R) {
+    float v[kWindow];
+    const float* s = segment + threadIdx.x * kRowRun;
+#pragma unroll
+    for (int j = 0; j + 4 <= kWindow; j += 4) {
+      const float4 f = *reinterpret_cast<const float4*>(s + j);
+      v[j] = f.x;
+      v[j + 1] = f.y;
+      v[j + 2] = f.z;
+      v[j + 3] = f.w;
+    }
+    if constexpr (kWindow % 4 == 2) {
+      const float2 f = *reinterpret_cast<const float2*>(s + kWindow - 2);
+      v[kWindow - 2] = f.x;
+      v[kWindow - 1] = f.y;
+    }
+    float r[kRowRun];
+    ConvolveWindow<R, kRowRun>(v, k, r);
+#pragma unroll
+    for (int o = 0; o < kRowRun; ++o) dst[o] = r[o];
+    continue;
+  }
+  const int count = min(kRowRun, w - first);
+  for (int o = 0; o < count; ++o) dst[o] = ConvolveLine<R>(row, 1, first + o, w, k);
+  }
 }
 
 template <int R>
@@ -826,10 +893,9 @@ namespace {
 template <int R>
 void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pitch, int planes,
                 const Kernel17& k, cudaStream_t stream) {
-  const size_t row_runs = static_cast<size_t>((w + kRun - 1) / kRun) * h;
   const size_t column_runs = static_cast<size_t>(w) * ((h + kRun - 1) / kRun);
-  BlurRowsKernel<R><<<dim3(Blocks(row_runs), planes), kThreads, 0, stream>>>(in, tmp, w, h, pitch,
-                                                                          pitch, k);
+  BlurRowsKernel<R><<<dim3((w + kRowSegment - 1) / kRowSegment, std::min(h, 65535), planes),
+                      kThreads, 0, stream>>>(in, tmp, w, h, pitch, pitch, k);
   BlurColumnsKernel<R><<<dim3(Blocks(column_runs), planes), kThreads, 0, stream>>>(
     tmp, out, w, h, pitch, pitch, k);
 }

@@ -11,10 +11,13 @@
 // One thread computes one chunk: it streams the line's samples once from
 // shared memory and keeps 8 independent double accumulators, so every sample
 // load feeds 8 multiply-adds and the 8 chains give the FP64 pipe enough
-// independent work. The chunk index is a template parameter, so after full
-// unrolling every basis value is a compile-time offset into constant memory
-// and enters the multiply as a constant-bank operand: the basis costs no load
-// instruction. Callers map warps to chunks so that the chunk is warp-uniform.
+// independent work. Callers map warps to chunks so that the chunk is
+// warp-uniform. For lengths 8 and 16 the chunk is a template parameter and,
+// fully unrolled, every basis value is a compile-time offset into constant
+// memory that enters the multiply as a constant-bank operand. Length 32 reads
+// the basis from constant memory with a runtime index (warp-uniform, so the
+// constant cache broadcasts it), because its fully unrolled code thrashes the
+// instruction cache.
 #pragma once
 
 #include "dct_basis.inc"
@@ -59,25 +62,61 @@ __device__ __forceinline__ void LineChunk(const In* __restrict__ in, Out* __rest
   for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
 }
 
-// Runtime chunk index (warp-uniform) to the compile-time instantiation.
+// basis table laid out [s][k]: the transposed forward basis, or the inverse
+// basis as stored.
+template <int L, bool kForward>
+__device__ __forceinline__ double DctTable(int index) {
+  if constexpr (kForward) {
+    if constexpr (L == 8) return kDctForwardT8[index];
+    if constexpr (L == 16) return kDctForwardT16[index];
+    if constexpr (L == 32) return kDctForwardT32[index];
+  } else {
+    if constexpr (L == 8) return kDctInverse8[index];
+    if constexpr (L == 16) return kDctInverse16[index];
+    if constexpr (L == 32) return kDctInverse32[index];
+  }
+  return 0.0;
+}
+
+// Outputs k = chunk*8 .. chunk*8+7 of one line of length L, reading the basis
+// from constant memory with a runtime (warp-uniform) index:
+// out[k] = sum_s in[s] * table[s * L + k]. The sample loop is only partly
+// unrolled, so the code stays small.
+template <int L, bool kForward, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunkTable(int chunk, const In* __restrict__ in,
+                                               Out* __restrict__ out) {
+  double acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+#pragma unroll 2
+  for (int s = 0; s < L; ++s) {
+    const double v = static_cast<double>(in[s * InStep]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] += v * DctTable<L, kForward>(s * L + chunk * 8 + j);
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
+}
+
+// Runtime chunk index (warp-uniform). Lengths 8 and 16 use the unrolled form
+// with compile-time basis offsets; length 32 uses the table form, because
+// the fully unrolled length-32 passes outgrow the instruction cache.
 template <int L, bool kForward, int InStep, int OutStep, typename In, typename Out>
 __device__ __forceinline__ void LineChunkAt(int chunk, const In* __restrict__ in,
                                             Out* __restrict__ out) {
-  switch (chunk) {
-    case 0:
-      LineChunk<L, kForward, 0, InStep, OutStep>(in, out);
-      break;
-    case 1:
-      if constexpr (L > 8) LineChunk<L, kForward, 1, InStep, OutStep>(in, out);
-      break;
-    case 2:
-      if constexpr (L > 16) LineChunk<L, kForward, 2, InStep, OutStep>(in, out);
-      break;
-    case 3:
-      if constexpr (L > 16) LineChunk<L, kForward, 3, InStep, OutStep>(in, out);
-      break;
-    default:
-      break;
+  if constexpr (L == 32) {
+    LineChunkTable<L, kForward, InStep, OutStep>(chunk, in, out);
+  } else {
+    switch (chunk) {
+      case 0:
+        LineChunk<L, kForward, 0, InStep, OutStep>(in, out);
+        break;
+      case 1:
+        if constexpr (L > 8) LineChunk<L, kForward, 1, InStep, OutStep>(in, out);
+        break;
+      default:
+        break;
+    }
   }
 }
 

@@ -40,3 +40,10 @@ def test_bases_are_inverse_pairs():
         # X[f] = sum_s x[s] forward[f][s] and x[s] = sum_f X[f] inverse[f][s].
         product = inverse.T @ forward
         assert np.abs(product - np.eye(n)).max() < 1e-14
+
+
+def test_transposed_forward_tables():
+    tables = committed_tables()
+    for n in (8, 16, 32):
+        forward = tables[f"Forward{n}"].reshape(n, n)
+        assert np.array_equal(tables[f"ForwardT{n}"].reshape(n, n), forward.T)
