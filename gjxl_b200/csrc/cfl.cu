@@ -11,9 +11,10 @@
 //
 // One CTA of 256 threads per tile. Phase 1: each warp transforms (block,
 // channel) pairs — lane l owns row-pass outputs l and l+32 and gathers the
-// column inputs with double shuffles. Phase 2: per Newton iteration all
-// threads evaluate the derivative terms chunk by chunk and warp 0 adds them
-// in order, twelve lanes per map, each owning one of the 3 sums x 4 lanes.
+// column inputs with double shuffles. Phase 2: per Newton iteration warps
+// 1-7 evaluate the derivative terms of the next chunk while warp 0 adds the
+// current one in order, twelve lanes per map, each owning one of the 3 sums
+// x 4 lanes.
 
 #include <cmath>
 #include <cstring>
@@ -26,7 +27,7 @@ namespace gjxl_b200 {
 namespace {
 
 constexpr int kTileValues = 64 * 64;  // up to 64 blocks of 64 coefficients
-constexpr int kCflChunk = 256;        // elements per shared term chunk (divides kTileValues)
+constexpr int kCflChunk = 128;        // elements per shared term chunk (divides kTileValues)
 
 struct CflParams {
   const float* opsin;  // Gaborish-inverted padded XYB
@@ -134,19 +135,20 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   }
   __syncthreads();
 
-  // Phase 2: FindBestMultiplier (non-fast) for both maps. Per iteration the
-  // element terms of the three derivative sums (center, +eps, -eps) are
-  // computed by all threads, a chunk of kCflChunk elements at a time, into
-  // shared memory; then warp 0 adds them in the reference's order: lanes
-  // 0..11 solve y_to_x and 12..23 y_to_b, lane 4 * kind + slot of a group
-  // owning derivative sum `kind` over the elements i = slot (mod 4), in
-  // increasing i. Elements skipped by the reference contribute +0.0, which
-  // leaves the (never -0.0) sum unchanged.
+  // Phase 2: FindBestMultiplier (non-fast) for both maps. The element terms
+  // of the three derivative sums (center, +eps, -eps) are computed a chunk of
+  // kCflChunk elements at a time into one of two shared buffers while warp 0
+  // adds the previous chunk in the reference's order: lanes 0..11 solve
+  // y_to_x and 12..23 y_to_b, lane 4 * kind + slot of a group owning
+  // derivative sum `kind` over the elements i = slot (mod 4), in increasing
+  // i. One barrier per chunk. Elements skipped by the reference contribute
+  // +0.0, which leaves the (never -0.0) sum unchanged.
   // Rows padded by 4 floats: the 24 summing lanes read 24 distinct banks.
-  __shared__ float terms[2][3][kCflChunk + 4];
+  __shared__ float terms[2][2][3][kCflChunk + 4];
   __shared__ float solution[2];
   __shared__ int solved[2];
   const int count = blocks * 64;
+  const int chunks = (count + kCflChunk - 1) / kCflChunk;
   const float kDistanceMultiplierAc = 1.0e-9f;
   const float kEpsilon = 100.0f;
   if (threadIdx.x < 2) {
@@ -156,37 +158,47 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   const int group = lane / 12;  // warp 0: 0 y_to_x, 1 y_to_b, 2 idle lanes
   const int member = lane % 12;
   const int kind = member / 4, slot = member % 4;
-  float lane_sum = 0.0f;
   __syncthreads();
+  // Terms of chunk `chunk` into buffer `buffer`, by the threads first..255.
+  const auto produce = [&](int chunk, int buffer, int first, const float (&x_map)[2],
+                           const int (&done_map)[2]) {
+    for (int t = static_cast<int>(threadIdx.x) - first; t < 2 * kCflChunk;
+         t += blockDim.x - first) {
+      const int map = t / kCflChunk, e = t % kCflChunk, i = chunk * kCflChunk + e;
+      if (done_map[map] || i >= count) continue;
+      const float* A = map == 0 ? luma_x : luma_b;       // a = luma / 84
+      const float* Bv = map == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
+      const float a = A[i], b = Bv[i], x = x_map[map];
+      const float center = fmaf(a, x, b);
+      const bool skip = fabsf(center) >= 100.0f;
+      const float scale = (2.0f / 3.0f) * a;
+      float* out = terms[buffer][map][0] + e;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float r = k == 0 ? center : fmaf(a, k == 1 ? x + kEpsilon : x - kEpsilon, b);
+        float d = scale * (fabsf(r) + 1.0f);
+        d = r < 0.0f ? -d : d;
+        out[k * (kCflChunk + 4)] = skip ? 0.0f : d;
+      }
+    }
+  };
   for (int iteration = 0; iteration < p.iterations; ++iteration) {
     if (solved[0] && solved[1]) break;
     const float x_map[2] = {solution[0], solution[1]};
     const int done_map[2] = {solved[0], solved[1]};
-    lane_sum = 0.0f;
-    for (int chunk = 0; chunk < count; chunk += kCflChunk) {
-      for (int t = threadIdx.x; t < 2 * kCflChunk; t += blockDim.x) {
-        const int map = t / kCflChunk, e = t % kCflChunk, i = chunk + e;
-        if (done_map[map] || i >= count) continue;
-        const float* A = map == 0 ? luma_x : luma_b;    // a = luma / 84
-        const float* Bv = map == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
-        const float a = A[i], b = Bv[i], x = x_map[map];
-        const float center = fmaf(a, x, b);
-        const bool skip = fabsf(center) >= 100.0f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float offset = k == 0 ? x : k == 1 ? x + kEpsilon : x - kEpsilon;
-          const float r = k == 0 ? center : fmaf(a, offset, b);
-          float d = (2.0f / 3.0f) * a * (fabsf(r) + 1.0f);
-          d = r < 0.0f ? -d : d;
-          terms[map][k][e] = skip ? 0.0f : d;
-        }
-      }
-      __syncthreads();
-      if (warp == 0 && group < 2 && !done_map[group]) {
-        const float* t = terms[group][kind];
-        const int limit = min(kCflChunk, count - chunk);
+    float lane_sum = 0.0f;
+    produce(0, 0, 0, x_map, done_map);
+    __syncthreads();
+    for (int chunk = 0; chunk < chunks; ++chunk) {
+      if (warp == 0) {
+        if (group < 2 && !done_map[group]) {
+          const float* t = terms[chunk & 1][group][kind];
+          const int limit = min(kCflChunk, count - chunk * kCflChunk);
 #pragma unroll 8
-        for (int e = slot; e < limit; e += 4) lane_sum += t[e];
+          for (int e = slot; e < limit; e += 4) lane_sum += t[e];
+        }
+      } else if (chunk + 1 < chunks) {
+        produce(chunk + 1, (chunk + 1) & 1, 32, x_map, done_map);
       }
       __syncthreads();
     }

@@ -14,7 +14,7 @@
 //   ErosionModulationKernel one thread per 8x8 block: fuzzy erosion (2x2 of
 //                          pre-erosion cells), strategy mask, gamma / HF /
 //                          blue modulations, FastPow2.
-//   Symmetric5Kernel       4 outputs per thread, 5x8 window from L1.
+//   Symmetric5Kernel       32x8 output tile from a mirrored halo tile in shared memory.
 
 #include <cmath>
 #include <cstring>
@@ -264,34 +264,44 @@ struct Symmetric5Params {
   uint32_t* error;
 };
 
-// WeightedRow (src/codec/convolution.cpp:14-30): far + (near + center).
-__device__ __forceinline__ float WeightedRow(const float* row, int x, int width, float c,
-                                             float n, float f) {
-  const float far = f * (row[Mirror(x - 2, width)] + row[Mirror(x + 2, width)]);
-  const float near = n * (row[Mirror(x - 1, width)] + row[Mirror(x + 1, width)]);
-  const float center = c * row[x];
+
+// One CTA per 32x8 output tile: the tile with a mirrored 2-pixel halo is
+// staged in shared memory (coalesced rows), then every output reads its 5x5
+// neighbourhood from there.
+constexpr int kS5W = 32, kS5H = 8;
+
+// WeightedRow (src/codec/convolution.cpp:14-30): far + (near + center), on a
+// staged row (the halo is already mirrored).
+__device__ __forceinline__ float WeightedTileRow(const float* row, float c, float n, float f) {
+  const float far = f * (row[-2] + row[2]);
+  const float near = n * (row[-1] + row[1]);
+  const float center = c * row[0];
   return far + (near + center);
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kS5W * kS5H)
 Symmetric5Kernel(const __grid_constant__ Symmetric5Params p) {
-  const uint32_t plane = blockIdx.y;
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  if (index >= p.width * p.height) return;
-  const int x = index % p.width, y = index / p.width;
-  const float* in = p.input + plane * p.in_pitch;
-  const float* w = p.w[plane];
+  __shared__ float tile[kS5H + 4][kS5W + 4];
+  const uint32_t plane = blockIdx.z;
+  const int x0 = blockIdx.x * kS5W, y0 = blockIdx.y * kS5H;
   const int h = p.height, wd = p.width;
-  const float* r0 = in + static_cast<size_t>(y) * p.in_stride;
-  const float* rm2 = in + static_cast<size_t>(Mirror(y - 2, h)) * p.in_stride;
-  const float* rp2 = in + static_cast<size_t>(Mirror(y + 2, h)) * p.in_stride;
-  const float* rm1 = in + static_cast<size_t>(Mirror(y - 1, h)) * p.in_stride;
-  const float* rp1 = in + static_cast<size_t>(Mirror(y + 1, h)) * p.in_stride;
-  float sum0 = WeightedRow(r0, x, wd, w[0], w[1], w[2]);
-  sum0 += WeightedRow(rm2, x, wd, w[2], w[5], w[4]);
-  float sum1 = WeightedRow(rp2, x, wd, w[2], w[5], w[4]);
-  sum0 += WeightedRow(rm1, x, wd, w[1], w[3], w[5]);
-  sum1 += WeightedRow(rp1, x, wd, w[1], w[3], w[5]);
+  const float* in = p.input + plane * p.in_pitch;
+  const int tid = threadIdx.y * kS5W + threadIdx.x;
+  for (int i = tid; i < (kS5H + 4) * (kS5W + 4); i += kS5W * kS5H) {
+    const int ty = i / (kS5W + 4), tx = i % (kS5W + 4);
+    tile[ty][tx] = in[static_cast<size_t>(Mirror(y0 + ty - 2, h)) * p.in_stride +
+                      Mirror(x0 + tx - 2, wd)];
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= wd || y >= h) return;
+  const float* w = p.w[plane];
+  const int cx = threadIdx.x + 2, cy = threadIdx.y + 2;
+  float sum0 = WeightedTileRow(&tile[cy][cx], w[0], w[1], w[2]);
+  sum0 += WeightedTileRow(&tile[cy - 2][cx], w[2], w[5], w[4]);
+  float sum1 = WeightedTileRow(&tile[cy + 2][cx], w[2], w[5], w[4]);
+  sum0 += WeightedTileRow(&tile[cy - 1][cx], w[1], w[3], w[5]);
+  sum1 += WeightedTileRow(&tile[cy + 1][cx], w[1], w[3], w[5]);
   const float v = sum0 + sum1;
   if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
   p.output[plane * p.out_pitch + static_cast<size_t>(y) * p.out_stride + x] = v;
@@ -345,9 +355,12 @@ int LaunchSymmetric5(const float* input, size_t in_stride, size_t in_pitch, floa
   p.planes = planes;
   for (uint32_t c = 0; c < planes; ++c) std::memcpy(p.w[c], weights[c], sizeof(p.w[c]));
   p.error = error;
-  const uint64_t n = static_cast<uint64_t>(width) * height;
-  dim3 grid(static_cast<unsigned>((n + 255) / 256), planes);
-  Symmetric5Kernel<<<grid, 256, 0, stream>>>(p);
+  if ((height + kS5H - 1) / kS5H > 65535) {
+    return SetError(GJXL_B200_UNSUPPORTED, "symmetric5: image taller than 524,280 rows");
+  }
+  dim3 grid(static_cast<unsigned>((width + kS5W - 1) / kS5W),
+            static_cast<unsigned>((height + kS5H - 1) / kS5H), planes);
+  Symmetric5Kernel<<<grid, dim3(kS5W, kS5H), 0, stream>>>(p);
   return CheckLaunch("symmetric5");
 }
 

@@ -14,6 +14,7 @@
 // HBM layout: planar float32, stride a multiple of 4 floats, so each thread
 // writes one float4 per plane (4 pixels) — 128-bit coalesced stores.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -140,39 +141,53 @@ struct StatsParams {
   float* stats;
 };
 
-// One thread per pixel (x >= 1, y >= 1) of the unpadded region; block-level
-// max reduction through warp shuffles, then one atomicMax per warp.
-__global__ void __launch_bounds__(256)
+// Grid-stride over the pixels (x >= 1, y >= 1) of the unpadded region; each
+// thread keeps running maxima, then warp shuffles and shared memory reduce
+// them per CTA, and one atomicMax per CTA and statistic publishes the result
+// (a max is order-independent, so the result is exact).
+constexpr int kStatsThreads = 256;
+
+__global__ void __launch_bounds__(kStatsThreads)
 MatrixScaleStatsKernel(const __grid_constant__ StatsParams p) {
-  const uint64_t index = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+  __shared__ float partial[3][kStatsThreads / 32];
   const uint32_t w1 = p.width - 1;
+  const uint64_t n = p.width > 1 && p.height > 1 ? static_cast<uint64_t>(w1) * (p.height - 1) : 0;
   float x_edge = 0.0f, b_edge = 0.0f, exposed = 0.0f;
-  if (p.width > 1 && p.height > 1 && index < static_cast<uint64_t>(w1) * (p.height - 1)) {
+  const float* X = p.opsin;
+  const float* Y = p.opsin + p.pitch;
+  const float* B = p.opsin + 2 * p.pitch;
+  for (uint64_t index = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; index < n;
+       index += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     const uint32_t y = 1 + static_cast<uint32_t>(index / w1);
     const uint32_t x = 1 + static_cast<uint32_t>(index % w1);
-    const float* X = p.opsin;
-    const float* Y = p.opsin + p.pitch;
-    const float* B = p.opsin + 2 * p.pitch;
     const size_t at = static_cast<size_t>(y) * p.stride + x;
     const size_t left = at - 1, up = at - p.stride;
     const float cx = X[at];
-    x_edge = fmaxf(fabsf(cx - X[left]), fabsf(cx - X[up]));
+    x_edge = fmaxf(x_edge, fmaxf(fabsf(cx - X[left]), fabsf(cx - X[up])));
     const float cy = Y[at], cb = B[at];
     const float diff = cb - cy;
-    b_edge = fmaxf(fabsf(diff - (B[left] - Y[left])), fabsf(diff - (B[up] - Y[up])));
+    b_edge = fmaxf(b_edge,
+                   fmaxf(fabsf(diff - (B[left] - Y[left])), fabsf(diff - (B[up] - Y[up]))));
     float e = cb - 1.2f * cy;
     if (e >= 0.0f) {
       e *= fabsf(cb - B[left]) + fabsf(cb - B[up]);
-      exposed = e;
+      exposed = fmaxf(exposed, e);
     }
   }
   x_edge = WarpMax(x_edge);
   b_edge = WarpMax(b_edge);
   exposed = WarpMax(exposed);
+  const int warp = threadIdx.x / 32;
   if ((threadIdx.x & 31) == 0) {
-    AtomicMaxNonNegative(&p.stats[0], x_edge);
-    AtomicMaxNonNegative(&p.stats[1], b_edge);
-    AtomicMaxNonNegative(&p.stats[2], exposed);
+    partial[0][warp] = x_edge;
+    partial[1][warp] = b_edge;
+    partial[2][warp] = exposed;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    float m = 0.0f;
+    for (int w = 0; w < kStatsThreads / 32; ++w) m = fmaxf(m, partial[threadIdx.x][w]);
+    AtomicMaxNonNegative(&p.stats[threadIdx.x], m);
   }
 }
 
@@ -254,7 +269,9 @@ extern "C" int gjxl_b200_matrix_scale_stats(const float* opsin, size_t opsin_str
                 static_cast<uint32_t>(height), stats};
   const uint64_t n = width > 1 && height > 1 ? (width - 1) * (height - 1) : 0;
   if (n == 0) return GJXL_B200_OK;
-  const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
-  MatrixScaleStatsKernel<<<blocks, 256, 0, s>>>(p);
+  // Eight CTAs per SM of a B200, fewer for small images.
+  const unsigned blocks =
+    static_cast<unsigned>(std::min<uint64_t>((n + kStatsThreads - 1) / kStatsThreads, 148 * 8));
+  MatrixScaleStatsKernel<<<blocks, kStatsThreads, 0, s>>>(p);
   return CheckLaunch("matrix_scale_stats");
 }
