@@ -693,6 +693,9 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
                                                 : kStrategyDct16x32;
   constexpr int covered = S::CW * S::CH;
   __shared__ float coef[3][N];
+  // The family's inverse-dequant weights, staged so that the serial
+  // threshold passes below read shared memory instead of waiting on L2.
+  __shared__ float inverse_dequant[3][N];
   __shared__ float thresholds[3][4];
   __shared__ int candidates[3];
   const uint32_t anchor_index = blockIdx.x;
@@ -703,6 +706,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
     const int c = i / N, j = i % N;
     coef[c][j] = p.coef[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride +
                         a.x * 8 + j % W];
+    inverse_dequant[c][j] = p.inverse_dequant[i];
   }
   __syncthreads();
   const AqQuantizer q = *p.q;
@@ -713,7 +717,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
     float t[4] = {0.58f, 0.64f, 0.64f, 0.64f};
     int candidate = initial_raw;
     AdjustQuantForChannel<W, H>(q, tid, p.matrix_multiplier[tid], strategy, coef[tid],
-                                p.inverse_dequant + tid * N, t, &candidate);
+                                inverse_dequant[tid], t, &candidate);
     for (int i = 0; i < 4; ++i) thresholds[tid][i] = t[i];
     candidates[tid] = candidate;
   } else if (tid == 32) {
@@ -735,7 +739,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
   for (int j = tid; j < N; j += 64) {
     const int x = j % S::SW, y = j / S::SW;
     const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
-    const float value = p.inverse_dequant[N + j] * y_scale * coef[1][j];
+    const float value = inverse_dequant[1][j] * y_scale * coef[1][j];
     const int32_t quantized =
       fabsf(value) < thresholds[1][ti] ? 0 : static_cast<int32_t>(rintf(value));
     p.qac[p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] = quantized;
@@ -767,7 +771,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
     const int x = j % S::SW, y = j / S::SW;
     const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
     const float qs = q.scale * static_cast<float>(raw) * p.matrix_multiplier[c];
-    const float value = p.inverse_dequant[c * N + j] * qs * coef[c][j];
+    const float value = inverse_dequant[c][j] * qs * coef[c][j];
     const int32_t quantized = fabsf(value) < t[ti] ? 0 : static_cast<int32_t>(rintf(value));
     p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] =
       quantized;

@@ -159,26 +159,35 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   const int member = lane % 12;
   const int kind = member / 4, slot = member % 4;
   __syncthreads();
-  // Terms of chunk `chunk` into buffer `buffer`, by the threads first..255.
+  // Terms of chunk `chunk` into buffer `buffer`, by the threads first..255,
+  // two adjacent elements per item (count is a multiple of 64, so pairs
+  // never straddle its end).
   const auto produce = [&](int chunk, int buffer, int first, const float (&x_map)[2],
                            const int (&done_map)[2]) {
-    for (int t = static_cast<int>(threadIdx.x) - first; t < 2 * kCflChunk;
+    for (int t = static_cast<int>(threadIdx.x) - first; t < kCflChunk;
          t += blockDim.x - first) {
-      const int map = t / kCflChunk, e = t % kCflChunk, i = chunk * kCflChunk + e;
+      const int map = t / (kCflChunk / 2), e = 2 * (t % (kCflChunk / 2));
+      const int i = chunk * kCflChunk + e;
       if (done_map[map] || i >= count) continue;
       const float* A = map == 0 ? luma_x : luma_b;       // a = luma / 84
       const float* Bv = map == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
-      const float a = A[i], b = Bv[i], x = x_map[map];
-      const float center = fmaf(a, x, b);
-      const bool skip = fabsf(center) >= 100.0f;
-      const float scale = (2.0f / 3.0f) * a;
+      const float2 a2 = *reinterpret_cast<const float2*>(A + i);
+      const float2 b2 = *reinterpret_cast<const float2*>(Bv + i);
+      const float x = x_map[map], xp = x + kEpsilon, xm = x - kEpsilon;
       float* out = terms[buffer][map][0] + e;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float r = k == 0 ? center : fmaf(a, k == 1 ? x + kEpsilon : x - kEpsilon, b);
-        float d = scale * (fabsf(r) + 1.0f);
-        d = r < 0.0f ? -d : d;
-        out[k * (kCflChunk + 4)] = skip ? 0.0f : d;
+      for (int q = 0; q < 2; ++q) {
+        const float a = q == 0 ? a2.x : a2.y, b = q == 0 ? b2.x : b2.y;
+        const float center = fmaf(a, x, b);
+        const bool skip = fabsf(center) >= 100.0f;
+        const float scale = (2.0f / 3.0f) * a;
+        const float r[3] = {center, fmaf(a, xp, b), fmaf(a, xm, b)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          float d = scale * (fabsf(r[k]) + 1.0f);
+          d = r[k] < 0.0f ? -d : d;
+          out[k * (kCflChunk + 4) + q] = skip ? 0.0f : d;
+        }
       }
     }
   };
