@@ -343,7 +343,7 @@ __device__ __forceinline__ float MaximumClamp(float v, float m) {
 // After the 33-tap blur of all three XYB planes into psycho LF: MF = xyb - LF
 // and the LF scaling (butteraugli_internal.cpp:750-776).
 __global__ void __launch_bounds__(kThreads)
-FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch) {
+FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch, uint32_t* error) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
   float lf[3];
@@ -352,32 +352,38 @@ FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch) {
     lf[c] = psycho[(kLF + c) * pitch + i];
     psycho[(kMF + c) * pitch + i] = xyb[c * pitch + i] - lf[c];
   }
-  psycho[(kLF + 2) * pitch + i] = (-0.362267051518f * lf[1] + lf[2]) * 49.87984651440f;
-  psycho[(kLF + 0) * pitch + i] = lf[0] * 33.832837186260f;
-  psycho[(kLF + 1) * pitch + i] = lf[1] * 14.458268100570f;
+  const float l2 = (-0.362267051518f * lf[1] + lf[2]) * 49.87984651440f;
+  const float l0 = lf[0] * 33.832837186260f;
+  const float l1 = lf[1] * 14.458268100570f;
+  psycho[(kLF + 2) * pitch + i] = l2;
+  psycho[(kLF + 0) * pitch + i] = l0;
+  psycho[(kLF + 1) * pitch + i] = l1;
+  if (!(IsFinite(l0) && IsFinite(l1) && IsFinite(l2))) RaiseError(error, kErrorNonFiniteOutput);
 }
 
 // After the 15-tap blur of MF into `blurred` (3 planes): HF = MF - blurred
 // (X, Y), MF ranges, MF_B = blurred, then X suppression by Y
 // (butteraugli_internal.cpp:778-810).
 __global__ void __launch_bounds__(kThreads)
-FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch) {
+FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch, uint32_t* error) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
-  float hf[2];
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    const float mv = blurred[c * pitch + i];
-    hf[c] = psycho[(kMF + c) * pitch + i] - mv;
-    psycho[(kMF + c) * pitch + i] =
-      c == 0 ? RemoveRangeAroundZero(mv, 0.29f) : AmplifyRangeAroundZero(mv, 0.1f);
-  }
-  psycho[(kMF + 2) * pitch + i] = blurred[2 * pitch + i];
+  const float mv0 = blurred[i], mv1 = blurred[pitch + i], mf_b = blurred[2 * pitch + i];
+  const float hf0 = psycho[(kMF + 0) * pitch + i] - mv0;
+  const float hf1 = psycho[(kMF + 1) * pitch + i] - mv1;
+  const float mf0 = RemoveRangeAroundZero(mv0, 0.29f);
+  const float mf1 = AmplifyRangeAroundZero(mv1, 0.1f);
+  psycho[(kMF + 0) * pitch + i] = mf0;
+  psycho[(kMF + 1) * pitch + i] = mf1;
+  psycho[(kMF + 2) * pitch + i] = mf_b;
   constexpr float kSuppress = 46.0f, kMinimumScale = 0.653020556257f;
-  const float y = hf[1];
-  const float scaler = kSuppress / (y * y + kSuppress) * (1.0f - kMinimumScale) + kMinimumScale;
-  psycho[(kHF + 0) * pitch + i] = scaler * hf[0];
-  psycho[(kHF + 1) * pitch + i] = hf[1];
+  const float scaler =
+    kSuppress / (hf1 * hf1 + kSuppress) * (1.0f - kMinimumScale) + kMinimumScale;
+  psycho[(kHF + 0) * pitch + i] = scaler * hf0;
+  psycho[(kHF + 1) * pitch + i] = hf1;
+  // Finiteness of the final MF planes (the HF planes are rewritten, and
+  // checked, by FrequencyUltraKernel).
+  if (!(IsFinite(mf0) & IsFinite(mf1) & IsFinite(mf_b))) RaiseError(error, kErrorNonFiniteOutput);
 }
 
 // After the 7-tap blur of HF into `blurred` (2 planes): UHF and final HF
@@ -387,22 +393,23 @@ FrequencyUltraKernel(const float* blurred, float* psycho, int n, size_t pitch,
                      uint32_t* error) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
-  {
-    const float hv = blurred[i];
-    const float ultra = psycho[(kHF + 0) * pitch + i];
-    psycho[(kUHF + 0) * pitch + i] = RemoveRangeAroundZero(ultra - hv, 0.04f);
-    psycho[(kHF + 0) * pitch + i] = RemoveRangeAroundZero(hv, 1.5f);
-  }
-  {
-    const float hv = MaximumClamp(blurred[pitch + i], 28.4691806922f);
-    const float ultra = psycho[(kHF + 1) * pitch + i];
-    float uv = ultra - hv;
-    uv = MaximumClamp(uv, 5.19175294647f);
-    psycho[(kUHF + 1) * pitch + i] = uv * 2.69313763794f;
-    psycho[(kHF + 1) * pitch + i] = AmplifyRangeAroundZero(hv * 2.155f, 0.132f);
-  }
-  for (int p = 0; p < kPsychoPlanes; ++p) {
-    if (!IsFinite(psycho[p * pitch + i])) RaiseError(error, kErrorNonFiniteOutput);
+  const float hv0 = blurred[i];
+  const float ultra0 = psycho[(kHF + 0) * pitch + i];
+  const float uhf0 = RemoveRangeAroundZero(ultra0 - hv0, 0.04f);
+  const float hf0 = RemoveRangeAroundZero(hv0, 1.5f);
+  const float hv1 = MaximumClamp(blurred[pitch + i], 28.4691806922f);
+  const float ultra1 = psycho[(kHF + 1) * pitch + i];
+  const float uv1 = MaximumClamp(ultra1 - hv1, 5.19175294647f);
+  const float uhf1 = uv1 * 2.69313763794f;
+  const float hf1 = AmplifyRangeAroundZero(hv1 * 2.155f, 0.132f);
+  psycho[(kUHF + 0) * pitch + i] = uhf0;
+  psycho[(kHF + 0) * pitch + i] = hf0;
+  psycho[(kUHF + 1) * pitch + i] = uhf1;
+  psycho[(kHF + 1) * pitch + i] = hf1;
+  // Finiteness of the final HF and UHF planes; FrequencyLowKernel and
+  // FrequencyHighKernel check the final LF and MF planes as they write them.
+  if (!(IsFinite(uhf0) && IsFinite(hf0) && IsFinite(uhf1) && IsFinite(hf1))) {
+    RaiseError(error, kErrorNonFiniteOutput);
   }
 }
 
@@ -769,24 +776,35 @@ ExpandKernel(const float* in, size_t in_stride, size_t in_pitch, int w, int h, f
   out[plane * out_pitch + i] = in[plane * in_pitch + static_cast<size_t>(sy) * in_stride + sx];
 }
 
-// Main/sub combination (:956-963) or the cropped copy of an expanded map,
-// with the NaN-free maximum folded into one float atomicMax per warp.
+// Main/sub combination (:956-963) or the cropped copy of an expanded map.
+// Grid-stride over the pixels; the NaN-free maximum is reduced per CTA
+// (warp shuffles, then shared memory) and published with one float atomicMax
+// per CTA (a max is order-independent).
 __global__ void __launch_bounds__(kThreads)
 CombineKernel(const float* main_map, int main_w, const float* sub_map, int sub_w, int w, int h,
               int xborder, int yborder, float* out, size_t out_stride, float* maximum,
               uint32_t* error) {
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  float v = 0.0f;
-  if (i < w * h) {
-    const int x = i % w, y = i / w;
+  __shared__ float warp_max[kThreads / 32];
+  float best = 0.0f;
+  const size_t n = static_cast<size_t>(w) * h;
+  for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * kThreads) {
+    const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
     const float m = main_map[static_cast<size_t>(y + yborder) * main_w + x + xborder];
-    v = sub_map != nullptr ? m * 0.85f + 0.5f * sub_map[static_cast<size_t>(y / 2) * sub_w + x / 2]
-                           : m;
+    const float v =
+      sub_map != nullptr ? m * 0.85f + 0.5f * sub_map[static_cast<size_t>(y / 2) * sub_w + x / 2]
+                         : m;
     if (!(IsFinite(v) && v >= 0.0f)) RaiseError(error, kErrorNonFiniteOutput);
     out[static_cast<size_t>(y) * out_stride + x] = v;
+    best = fmaxf(best, v);
   }
-  v = WarpMax(v);
-  if ((threadIdx.x & 31) == 0) AtomicMaxNonNegative(maximum, v);
+  best = WarpMax(best);
+  if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x / 32] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kThreads / 32; ++k) best = fmaxf(best, warp_max[k]);
+    AtomicMaxNonNegative(maximum, best);
+  }
 }
 
 __global__ void ScoreKernel(const float* maximum, double* score) {
@@ -924,10 +942,12 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
                                                           n, st.intensity_target, st.error);
   // LF: 33-tap blur of the three XYB planes straight into the LF planes.
   BlurPlanes<16>(s.xyb, s.tmp, psycho + kLF * n, s.w, s.h, n, 3, st.k_low, stream);
-  FrequencyLowKernel<<<Blocks(n), kThreads, 0, stream>>>(s.xyb, psycho, static_cast<int>(n), n);
+  FrequencyLowKernel<<<Blocks(n), kThreads, 0, stream>>>(s.xyb, psycho, static_cast<int>(n), n,
+                                                         st.error);
   // 15-tap blur of MF (3 planes) into blur3.
   BlurPlanes<7>(psycho + kMF * n, s.tmp, s.blur3, s.w, s.h, n, 3, st.k_high, stream);
-  FrequencyHighKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n), n);
+  FrequencyHighKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n), n,
+                                                          st.error);
   // 7-tap blur of HF (2 planes) into blur3.
   BlurPlanes<3>(psycho + kHF * n, s.tmp, s.blur3, s.w, s.h, n, 2, st.k_ultra, stream);
   FrequencyUltraKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n),
@@ -1099,7 +1119,7 @@ int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride,
   st->reference_mask_ready = true;
   cudaMemsetAsync(st->maximum, 0, sizeof(float), stream);
   const size_t n = static_cast<size_t>(st->width) * st->height;
-  CombineKernel<<<Blocks(n), kThreads, 0, stream>>>(
+  CombineKernel<<<std::min<unsigned>(Blocks(n), 148 * 8), kThreads, 0, stream>>>(
     st->main.final_map, st->main.w, st->has_sub ? st->sub.final_map : nullptr, st->sub.w,
     st->width, st->height, st->xborder, st->yborder, map, map_stride, st->maximum, st->error);
   if (score != nullptr) ScoreKernel<<<1, 1, 0, stream>>>(st->maximum, score);
