@@ -147,6 +147,8 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __shared__ uint32_t nonzero[K][3];
 
   const int tid = threadIdx.x;
+  // Anchors first (integer arithmetic only), so that the pixel loads can
+  // start before the quant norms and CfL factors arrive.
   if (tid < K) {
     const uint32_t cand = blockIdx.x * K + tid;
     int ax = -1, ay = -1;
@@ -161,35 +163,6 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
       if (lx + S::CW <= tile_w && ly + S::CH <= tile_h) {
         ax = tx * 8 + lx;
         ay = ty * 8 + ly;
-        // ComputeQuantNormUnchecked (ac_strategy.cpp:103-130).
-        const float* q = p.quant_field;
-        float qn;
-        if (S::CW * S::CH == 1) {
-          qn = q[ay * p.blocks_x + ax];
-        } else if (S::CW * S::CH == 2) {
-          qn = S::CH == 2 ? fmaxf(q[ay * p.blocks_x + ax], q[(ay + 1) * p.blocks_x + ax])
-                          : fmaxf(q[ay * p.blocks_x + ax], q[ay * p.blocks_x + ax + 1]);
-        } else {
-          float sum = 0.0f;
-          for (int dy = 0; dy < S::CH; ++dy) {
-            for (int dx = 0; dx < S::CW; ++dx) {
-              float v = q[(ay + dy) * p.blocks_x + ax + dx];
-              v *= v;
-              v *= v;
-              v *= v;
-              sum += v * v;
-            }
-          }
-          sum /= static_cast<float>(S::CW * S::CH);
-          qn = FastPow2(FastLog2(sum) * (1.0f / 16.0f));
-        }
-        if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
-        quant_norm[tid] = qn;
-        const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
-        // ColorCorrelationMap::AcFactors (chroma_from_luma.cpp:412-432).
-        cfl[tid][0] = static_cast<float>(p.y_to_x[tile_index]) / 84.0f;
-        cfl[tid][1] = 0.0f;
-        cfl[tid][2] = 1.0f + static_cast<float>(p.y_to_b[tile_index]) / 84.0f;
       }
     }
     anchor_x[tid] = ax;
@@ -200,19 +173,72 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __syncthreads();
 
   // Pixels into A and the pixel mask into `mask` (one W-float run of the
-  // source per row), all loads issued before the first use.
-  for (int i = tid; i < KC * N; i += kCostThreads) {
-    const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
-    if (anchor_x[k] < 0) continue;
-    A[kc * Lay::PlanePitch + y * Lay::RowPitch + x] =
-      p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
-              anchor_x[k] * 8 + x];
-  }
-  for (int i = tid; i < K * N; i += kCostThreads) {
-    const int k = i / N, r = i % N, y = r / W, x = r % W;
-    if (anchor_x[k] < 0) continue;
-    mask[i] = p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
-                           anchor_x[k] * 8 + x];
+  // source per row): every load of a thread is issued before the first
+  // store, so their latencies overlap.
+  {
+    constexpr int kPixelLoads = KC * N / kCostThreads;
+    constexpr int kMaskLoads = (K * N + kCostThreads - 1) / kCostThreads;
+    float pixel[kPixelLoads], pmask[kMaskLoads];
+#pragma unroll
+    for (int q = 0; q < kPixelLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
+      pixel[q] = anchor_x[k] < 0 ? 0.0f
+               : p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
+                         anchor_x[k] * 8 + x];
+    }
+#pragma unroll
+    for (int q = 0; q < kMaskLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      const int k = i / N, r = i % N, y = r / W, x = r % W;
+      pmask[q] = i >= K * N || anchor_x[k] < 0 ? 1.0f
+               : p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
+                              anchor_x[k] * 8 + x];
+    }
+    // ComputeQuantNormUnchecked (ac_strategy.cpp:103-130) and the CfL
+    // factors, while the loads above are in flight.
+    if (tid < K && anchor_x[tid] >= 0) {
+      const int ax = anchor_x[tid], ay = anchor_y[tid];
+      const float* q = p.quant_field;
+      float qn;
+      if (S::CW * S::CH == 1) {
+        qn = q[ay * p.blocks_x + ax];
+      } else if (S::CW * S::CH == 2) {
+        qn = S::CH == 2 ? fmaxf(q[ay * p.blocks_x + ax], q[(ay + 1) * p.blocks_x + ax])
+                        : fmaxf(q[ay * p.blocks_x + ax], q[ay * p.blocks_x + ax + 1]);
+      } else {
+        float sum = 0.0f;
+        for (int dy = 0; dy < S::CH; ++dy) {
+          for (int dx = 0; dx < S::CW; ++dx) {
+            float v = q[(ay + dy) * p.blocks_x + ax + dx];
+            v *= v;
+            v *= v;
+            v *= v;
+            sum += v * v;
+          }
+        }
+        sum /= static_cast<float>(S::CW * S::CH);
+        qn = FastPow2(FastLog2(sum) * (1.0f / 16.0f));
+      }
+      if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
+      quant_norm[tid] = qn;
+      const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
+      // ColorCorrelationMap::AcFactors (chroma_from_luma.cpp:412-432).
+      cfl[tid][0] = static_cast<float>(p.y_to_x[tile_index]) / 84.0f;
+      cfl[tid][1] = 0.0f;
+      cfl[tid][2] = 1.0f + static_cast<float>(p.y_to_b[tile_index]) / 84.0f;
+    }
+#pragma unroll
+    for (int q = 0; q < kPixelLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      const int kc = i / N, r = i % N, y = r / W, x = r % W;
+      if (anchor_x[kc / 3] >= 0) A[kc * Lay::PlanePitch + y * Lay::RowPitch + x] = pixel[q];
+    }
+#pragma unroll
+    for (int q = 0; q < kMaskLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      if (i < K * N && anchor_x[i / N] >= 0) mask[i] = pmask[q];
+    }
   }
   __syncthreads();
 
@@ -224,23 +250,39 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __syncthreads();
 
   // Quantize, coefficient j = coefficient_index(v, u) by coefficient:
-  // residual coefficients into A at (v, u), sqrt terms into terms[j].
-  for (int i = tid; i < KC * N; i += kCostThreads) {
-    const int kc = i / N, j = i % N, k = kc / 3, c = kc % 3;
-    if (anchor_x[k] < 0) continue;
-    const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
-    const int at = v * Lay::RowPitch + u;
-    const float decorrelated =
-      B[kc * Lay::PlanePitch + at] - B[(k * 3 + 1) * Lay::PlanePitch + at] * cfl[k][c];
-    const float scaled = decorrelated * __ldg(p.inverse_dequant + c * N + j) * quant_norm[k];
-    const float rounded = roundf(scaled);
-    const float difference = scaled - rounded;
-    A[kc * Lay::PlanePitch + at] = __ldg(p.dequant + c * N + j) * difference;
-    terms[kc * Lay::TermPitch + j] = sqrtf(fabsf(rounded));
-    // A warp's 32 consecutive coefficients share (k, c) (N is a multiple of
-    // 32 and every thread runs the same trip count): one count per warp.
-    const unsigned nz = __ballot_sync(0xffffffffu, rounded != 0.0f);
-    if ((tid & 31) == 0 && nz != 0u) atomicAdd(&nonzero[k][c], static_cast<uint32_t>(__popc(nz)));
+  // residual coefficients into A at (v, u), sqrt terms into terms[j]. The
+  // quantization weights of all of a thread's coefficients are loaded first.
+  {
+    constexpr int kPerThread = KC * N / kCostThreads;
+    float inv[kPerThread], dq[kPerThread];
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+      const int i = tid + q * kCostThreads;
+      const int c = (i / N) % 3, j = i % N;
+      inv[q] = __ldg(p.inverse_dequant + c * N + j);
+      dq[q] = __ldg(p.dequant + c * N + j);
+    }
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+      const int i = tid + q * kCostThreads;
+      const int kc = i / N, j = i % N, k = kc / 3, c = kc % 3;
+      if (anchor_x[k] < 0) continue;
+      const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
+      const int at = v * Lay::RowPitch + u;
+      const float decorrelated =
+        B[kc * Lay::PlanePitch + at] - B[(k * 3 + 1) * Lay::PlanePitch + at] * cfl[k][c];
+      const float scaled = decorrelated * inv[q] * quant_norm[k];
+      const float rounded = roundf(scaled);
+      const float difference = scaled - rounded;
+      A[kc * Lay::PlanePitch + at] = dq[q] * difference;
+      terms[kc * Lay::TermPitch + j] = sqrtf(fabsf(rounded));
+      // A warp's 32 consecutive coefficients share (k, c) (N is a multiple
+      // of 32 and every thread runs the same trip count): one count per warp.
+      const unsigned nz = __ballot_sync(0xffffffffu, rounded != 0.0f);
+      if ((tid & 31) == 0 && nz != 0u) {
+        atomicAdd(&nonzero[k][c], static_cast<uint32_t>(__popc(nz)));
+      }
+    }
   }
   __syncthreads();
 
