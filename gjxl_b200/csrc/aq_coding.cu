@@ -74,11 +74,25 @@ ForwardCoefficientsKernel(const float* opsin, size_t stride, size_t pitch, const
   const uint32_t n = *count;
   if (first >= n) return;
   const int active = min(K, static_cast<int>(n - first));
-  for (int i = threadIdx.x; i < active * 3 * N; i += kTransformThreads) {
+  // All of a thread's loads are issued before the first store.
+  constexpr int kPerThread = KC * N / kTransformThreads;
+  float value[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kTransformThreads;
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
-    const int2 a = anchors[first + k];
-    px[Batch::At(k * 3 + c, yx / W, yx % W)] =
-      opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 + yx % W];
+    const bool live = i < active * 3 * N;
+    const int2 a = anchors[first + (live ? k : 0)];
+    value[q] = live ? opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 +
+                            yx % W]
+                    : 0.0f;
+  }
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kTransformThreads;
+    if (i >= active * 3 * N) break;
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    px[Batch::At(k * 3 + c, yx / W, yx % W)] = value[q];
   }
   __syncthreads();
   const auto present = [&](int plane) { return plane < 3 * active; };
@@ -680,8 +694,14 @@ struct CodingParams {
 
 // ComputeQuantizedCoefficientsImpl's per-transform body
 // (reconstruction.cpp:480-700), one CTA of 64 threads per anchor.
+// Threads per anchor.
 template <int W, int H>
-__global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ CodingParams p) {
+__host__ __device__ constexpr int CodingThreads() {
+  return 64;
+}
+
+template <int W, int H>
+__global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __grid_constant__ CodingParams p) {
   using S = TransformShape<W, H>;
   constexpr int N = S::N;
   constexpr int strategy = W == 8 && H == 8     ? kStrategyDct8
@@ -692,6 +712,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
                          : W == 16              ? kStrategyDct32x16
                                                 : kStrategyDct16x32;
   constexpr int covered = S::CW * S::CH;
+  constexpr int kT = CodingThreads<W, H>();
   __shared__ float coef[3][N];
   // The family's inverse-dequant weights, staged so that the serial
   // threshold passes below read shared memory instead of waiting on L2.
@@ -702,7 +723,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
   if (anchor_index >= *p.count) return;
   const int2 a = p.anchors[anchor_index];
   const int tid = threadIdx.x;
-  for (int i = tid; i < 3 * N; i += 64) {
+  for (int i = tid; i < 3 * N; i += kT) {
     const int c = i / N, j = i % N;
     coef[c][j] = p.coef[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride +
                         a.x * 8 + j % W];
@@ -736,7 +757,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
   // Y: quantize with the adjusted thresholds, store, dequantize in place.
   const float y_scale = q.scale * static_cast<float>(raw) * 1.0f;
   const float y_dequant_scale = (q.inverse_global_scale / static_cast<float>(raw)) / 1.0f;
-  for (int j = tid; j < N; j += 64) {
+  for (int j = tid; j < N; j += kT) {
     const int x = j % S::SW, y = j / S::SW;
     const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
     const float value = inverse_dequant[1][j] * y_scale * coef[1][j];
@@ -750,7 +771,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
   const int tile = (a.y / 8) * p.tiles_x + (a.x / 8);
   const float f0 = static_cast<float>(p.y_to_x[tile]) / 84.0f;
   const float f2 = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
-  for (int j = tid; j < N; j += 64) {
+  for (int j = tid; j < N; j += kT) {
     coef[0][j] -= f0 * coef[1][j];
     coef[2][j] -= f2 * coef[1][j];
   }
@@ -766,7 +787,7 @@ __global__ void __launch_bounds__(64) CodingKernel(const __grid_constant__ Codin
   }
   float t[4];
   ChromaThresholds(covered, t);
-  for (int i = tid; i < 2 * N; i += 64) {
+  for (int i = tid; i < 2 * N; i += kT) {
     const int c = i < N ? 0 : 2, j = i % N;
     const int x = j % S::SW, y = j / S::SW;
     const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
@@ -1189,7 +1210,7 @@ int LaunchCoding(CodingParams p, const DeviceTables& d, int family, size_t max_c
   p.dequant = d.dequant + h.layout.offset[table];
   p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
   if (max_count == 0) return GJXL_B200_OK;
-  CodingKernel<W, H><<<static_cast<unsigned>(max_count), 64, 0, stream>>>(p);
+  CodingKernel<W, H><<<static_cast<unsigned>(max_count), CodingThreads<W, H>(), 0, stream>>>(p);
   return CheckLaunch("aq coding");
 }
 

@@ -158,13 +158,28 @@ __global__ void __launch_bounds__(kReconThreads, 2) ReconstructKernel(const __gr
   __syncthreads();
   // Dequantize coefficient j = coefficient_index(v, u) (footprint (j % W, j / W))
   // into (v, u).
-  for (int i = threadIdx.x; i < active * 3 * N; i += kReconThreads) {
+  // All of a thread's loads are issued before the first store.
+  constexpr int kPerThread = KC * N / kReconThreads;
+  int32_t qv[kPerThread];
+  float dq[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kReconThreads;
+    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
+    const bool live = i < active * 3 * N;
+    const int2 a = anchor[live ? k : 0];
+    qv[q] = live ? p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 +
+                         j % W]
+                 : 0;
+    dq[q] = p.dequant[c * N + j];
+  }
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kReconThreads;
+    if (i >= active * 3 * N) break;
     const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
     const int v = H < W ? j / W : j % H, u = H < W ? j % W : j / H;
-    const int2 a = anchor[k];
-    const int32_t qv =
-      p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W];
-    coef[Batch::At(k * 3 + c, v, u)] = QuantBiasR(qv, c) * (p.dequant[c * N + j] * scales[k][c]);
+    coef[Batch::At(k * 3 + c, v, u)] = QuantBiasR(qv[q], c) * (dq[q] * scales[k][c]);
   }
   __syncthreads();
   // Restore the chroma from luma.

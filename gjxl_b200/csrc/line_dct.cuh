@@ -88,7 +88,7 @@ __device__ __forceinline__ void LineChunkTable(int chunk, const In* __restrict__
   double acc[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) acc[j] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
   for (int s = 0; s < L; ++s) {
     const double v = static_cast<double>(in[s * InStep]);
 #pragma unroll
