@@ -28,6 +28,7 @@
 
 #include "common.cuh"
 #include "host_util.h"
+#include "fan.h"
 #include "line_dct.cuh"
 #include "tables.h"
 
@@ -599,7 +600,8 @@ size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y) {
 int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
                           const float* quant_field, const float* pixel_mask, size_t mask_stride,
                           const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
-                          float* costs, uint32_t* error, cudaStream_t stream) {
+                          float* costs, uint32_t* error, cudaStream_t stream,
+                          const StreamFan* fan) {
   DeviceTables d;
   int status = GetDeviceTables(&d);
   if (status != GJXL_B200_OK) return status;
@@ -630,20 +632,25 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
   p.zeros_multiplier = 9.3089059022677905f * std::pow(ratio, 0.50990926717963703f);
   p.cost_delta = 10.833273317067883f * std::pow(ratio, 0.36702940662370243f);
   p.error = error;
+  // The families are independent: with a fan they run side by side.
+  if (status == GJXL_B200_OK) status = CheckCuda(FanFork(fan), "ac_strategy fork");
   for (int f = 0; f < kFamilyCount && status == GJXL_B200_OK; ++f) {
+    const cudaStream_t fs = fan != nullptr ? fan->For(f) : stream;
     CostParams q = p;
     q.anchor_step = (dense && f >= 4) ? 1 : kFamilyStep[f];
     q.costs = costs + f * bx * by;
     switch (f) {
-      case 0: status = LaunchFamily<8, 8>(q, d, f, stream); break;
-      case 1: status = LaunchFamily<8, 16>(q, d, f, stream); break;
-      case 2: status = LaunchFamily<16, 8>(q, d, f, stream); break;
-      case 3: status = LaunchFamily<16, 16>(q, d, f, stream); break;
-      case 4: status = LaunchFamily<16, 32>(q, d, f, stream); break;
-      case 5: status = LaunchFamily<32, 16>(q, d, f, stream); break;
-      case 6: status = LaunchFamily<32, 32>(q, d, f, stream); break;
+      case 0: status = LaunchFamily<8, 8>(q, d, f, fs); break;
+      case 1: status = LaunchFamily<8, 16>(q, d, f, fs); break;
+      case 2: status = LaunchFamily<16, 8>(q, d, f, fs); break;
+      case 3: status = LaunchFamily<16, 16>(q, d, f, fs); break;
+      case 4: status = LaunchFamily<16, 32>(q, d, f, fs); break;
+      case 5: status = LaunchFamily<32, 16>(q, d, f, fs); break;
+      case 6: status = LaunchFamily<32, 32>(q, d, f, fs); break;
     }
   }
+  const cudaError_t joined = FanJoin(fan);
+  if (status == GJXL_B200_OK) status = CheckCuda(joined, "ac_strategy join");
   return status;
 }
 
@@ -691,7 +698,7 @@ extern "C" int gjxl_b200_ac_strategy_costs(
   return LaunchAcStrategyCosts(opsin, opsin_stride, opsin_plane_pitch, padded_width,
                                padded_height, quant_field, pixel_mask, pixel_mask_stride, y_to_x,
                                y_to_b, butteraugli_target, dense_dct32 != 0, costs, device_error,
-                               static_cast<cudaStream_t>(stream));
+                               static_cast<cudaStream_t>(stream), nullptr);
 }
 
 extern "C" int gjxl_b200_ac_strategy_search(

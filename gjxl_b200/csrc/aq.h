@@ -6,6 +6,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "fan.h"
+
 namespace gjxl_b200 {
 
 // Device copy of the reference's Quantizer (src/core/quantizer.h:24-120).
@@ -34,7 +36,7 @@ int AqBuildAnchors(const uint8_t* cells, size_t bx, size_t by, int2* lists, uint
                    cudaStream_t stream);
 int AqForwardCoefficients(const float* opsin, size_t stride, size_t pitch, size_t bx, size_t by,
                           const int2* lists, const uint32_t* counts, float* coef,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const StreamFan* fan = nullptr);
 int AqAdjustField(const uint8_t* cells, size_t bx, size_t by, const float* in, float* out,
                   float target, cudaStream_t stream);
 int AqPolicySetup(const float* field, size_t blocks, float target, float* range,
@@ -49,7 +51,8 @@ int AqFinalCfl(const uint8_t* cells, size_t bx, size_t by, const float* coef, si
 int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, const float* coef,
              size_t stride, size_t pitch, int32_t* qac, float* dc, int32_t* raw,
              const AqQuantizer* q, const int8_t* y_to_x, const int8_t* y_to_b,
-             const float* matrix_multiplier, uint32_t* error, cudaStream_t stream);
+             const float* matrix_multiplier, uint32_t* error, cudaStream_t stream,
+             const StreamFan* fan = nullptr);
 int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, int32_t* quantized,
                  float* reconstructed, int extra_precision, cudaStream_t stream);
 int AqInverseSigma(const uint8_t* cells, size_t bx, size_t by, const int32_t* raw,
@@ -62,7 +65,7 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
                   const int32_t* qac, size_t stride, size_t pitch, const float* dc,
                   const int32_t* raw, const AqQuantizer* q, const int8_t* y_to_x,
                   const int8_t* y_to_b, const float* matrix_multiplier, float* recon,
-                  cudaStream_t stream);
+                  cudaStream_t stream, const StreamFan* fan = nullptr);
 int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, size_t width,
                   size_t height, const float* inverse_sigma, size_t bx, float* scratch_a,
                   float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream);

@@ -1105,22 +1105,27 @@ int LaunchForward(const float* opsin, size_t stride, size_t pitch, const int2* l
 
 int AqForwardCoefficients(const float* opsin, size_t stride, size_t pitch, size_t bx, size_t by,
                           const int2* lists, const uint32_t* counts, float* coef,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, const StreamFan* fan) {
   int status = GJXL_B200_OK;
   const size_t blocks = bx * by;
+  // The families are independent: with a fan they run side by side.
+  if (status == GJXL_B200_OK) status = CheckCuda(FanFork(fan), "fork");
   for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    const cudaStream_t fs = fan != nullptr ? fan->For(f) : stream;
     const int2* list = lists + f * blocks;
     const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
     switch (f) {
-      case 0: status = LaunchForward<8, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 1: status = LaunchForward<8, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 2: status = LaunchForward<16, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 3: status = LaunchForward<16, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 4: status = LaunchForward<16, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 5: status = LaunchForward<32, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
-      case 6: status = LaunchForward<32, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, stream); break;
+      case 0: status = LaunchForward<8, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 1: status = LaunchForward<8, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 2: status = LaunchForward<16, 8>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 3: status = LaunchForward<16, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 4: status = LaunchForward<16, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 5: status = LaunchForward<32, 16>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
+      case 6: status = LaunchForward<32, 32>(opsin, stride, pitch, list, counts + f, max_count, coef, fs); break;
     }
   }
+  const cudaError_t joined = FanJoin(fan);
+  if (status == GJXL_B200_OK) status = CheckCuda(joined, "join");
   return status;
 }
 
@@ -1217,7 +1222,8 @@ int LaunchCoding(CodingParams p, const DeviceTables& d, int family, size_t max_c
 int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, const float* coef,
              size_t stride, size_t pitch, int32_t* qac, float* dc, int32_t* raw,
              const AqQuantizer* q, const int8_t* y_to_x, const int8_t* y_to_b,
-             const float* matrix_multiplier, uint32_t* error, cudaStream_t stream) {
+             const float* matrix_multiplier, uint32_t* error, cudaStream_t stream,
+             const StreamFan* fan) {
   DeviceTables d;
   int status = GetDeviceTables(&d);
   if (status != GJXL_B200_OK) return status;
@@ -1238,20 +1244,25 @@ int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, co
   p.tiles_x = static_cast<int>((bx + 7) / 8);
   p.matrix_multiplier = matrix_multiplier;
   p.error = error;
+  // The families are independent: with a fan they run side by side.
+  if (status == GJXL_B200_OK) status = CheckCuda(FanFork(fan), "fork");
   for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    const cudaStream_t fs = fan != nullptr ? fan->For(f) : stream;
     p.anchors = lists + f * blocks;
     p.count = counts + f;
     const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
     switch (f) {
-      case 0: status = LaunchCoding<8, 8>(p, d, f, max_count, stream); break;
-      case 1: status = LaunchCoding<8, 16>(p, d, f, max_count, stream); break;
-      case 2: status = LaunchCoding<16, 8>(p, d, f, max_count, stream); break;
-      case 3: status = LaunchCoding<16, 16>(p, d, f, max_count, stream); break;
-      case 4: status = LaunchCoding<16, 32>(p, d, f, max_count, stream); break;
-      case 5: status = LaunchCoding<32, 16>(p, d, f, max_count, stream); break;
-      case 6: status = LaunchCoding<32, 32>(p, d, f, max_count, stream); break;
+      case 0: status = LaunchCoding<8, 8>(p, d, f, max_count, fs); break;
+      case 1: status = LaunchCoding<8, 16>(p, d, f, max_count, fs); break;
+      case 2: status = LaunchCoding<16, 8>(p, d, f, max_count, fs); break;
+      case 3: status = LaunchCoding<16, 16>(p, d, f, max_count, fs); break;
+      case 4: status = LaunchCoding<16, 32>(p, d, f, max_count, fs); break;
+      case 5: status = LaunchCoding<32, 16>(p, d, f, max_count, fs); break;
+      case 6: status = LaunchCoding<32, 32>(p, d, f, max_count, fs); break;
     }
   }
+  const cudaError_t joined = FanJoin(fan);
+  if (status == GJXL_B200_OK) status = CheckCuda(joined, "join");
   return status;
 }
 

@@ -474,7 +474,7 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
                   const int32_t* qac, size_t stride, size_t pitch, const float* dc,
                   const int32_t* raw, const AqQuantizer* q, const int8_t* y_to_x,
                   const int8_t* y_to_b, const float* matrix_multiplier, float* recon,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, const StreamFan* fan) {
   DeviceTables d;
   int status = GetDeviceTables(&d);
   if (status != GJXL_B200_OK) return status;
@@ -494,20 +494,25 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
   p.tiles_x = static_cast<int>((bx + 7) / 8);
   p.matrix_multiplier = matrix_multiplier;
   p.recon = recon;
+  // The families are independent: with a fan they run side by side.
+  if (status == GJXL_B200_OK) status = CheckCuda(FanFork(fan), "fork");
   for (int f = 0; f < kFamilyCountT && status == GJXL_B200_OK; ++f) {
+    const cudaStream_t fs = fan != nullptr ? fan->For(f) : stream;
     p.anchors = lists + f * blocks;
     p.count = counts + f;
     const size_t max_count = blocks / (FamilyCoveredW(f) * FamilyCoveredH(f));
     switch (f) {
-      case 0: status = LaunchReconstruct<8, 8>(p, d, f, max_count, stream); break;
-      case 1: status = LaunchReconstruct<8, 16>(p, d, f, max_count, stream); break;
-      case 2: status = LaunchReconstruct<16, 8>(p, d, f, max_count, stream); break;
-      case 3: status = LaunchReconstruct<16, 16>(p, d, f, max_count, stream); break;
-      case 4: status = LaunchReconstruct<16, 32>(p, d, f, max_count, stream); break;
-      case 5: status = LaunchReconstruct<32, 16>(p, d, f, max_count, stream); break;
-      case 6: status = LaunchReconstruct<32, 32>(p, d, f, max_count, stream); break;
+      case 0: status = LaunchReconstruct<8, 8>(p, d, f, max_count, fs); break;
+      case 1: status = LaunchReconstruct<8, 16>(p, d, f, max_count, fs); break;
+      case 2: status = LaunchReconstruct<16, 8>(p, d, f, max_count, fs); break;
+      case 3: status = LaunchReconstruct<16, 16>(p, d, f, max_count, fs); break;
+      case 4: status = LaunchReconstruct<16, 32>(p, d, f, max_count, fs); break;
+      case 5: status = LaunchReconstruct<32, 16>(p, d, f, max_count, fs); break;
+      case 6: status = LaunchReconstruct<32, 32>(p, d, f, max_count, fs); break;
     }
   }
+  const cudaError_t joined = FanJoin(fan);
+  if (status == GJXL_B200_OK) status = CheckCuda(joined, "join");
   return status;
 }
 

@@ -167,6 +167,13 @@ struct Session {
   // The analysis as one CUDA graph, captured on the first analyze() call for
   // a given input pointer / stride / channel count and replayed afterwards.
   cudaStream_t capture_stream = nullptr;
+  // Side streams: the fan for the per-family stages, and one stream for the
+  // Butteraugli reference preparation, which only needs the input and runs
+  // beside the whole front half.
+  cudaStream_t fan_side[StreamFan::kSide] = {};
+  cudaEvent_t fan_fork = nullptr, fan_join[StreamFan::kSide] = {};
+  cudaStream_t prepare_stream = nullptr;
+  cudaEvent_t prepare_fork = nullptr, prepare_join = nullptr;
   cudaGraphExec_t graph = nullptr;
   const uint8_t* graph_pixels = nullptr;
   size_t graph_stride = 0;
@@ -176,6 +183,16 @@ struct Session {
   ~Session() {
     if (graph) cudaGraphExecDestroy(graph);
     if (capture_stream) cudaStreamDestroy(capture_stream);
+    for (auto& side : fan_side) {
+      if (side) cudaStreamDestroy(side);
+    }
+    for (auto& e : fan_join) {
+      if (e) cudaEventDestroy(e);
+    }
+    if (fan_fork) cudaEventDestroy(fan_fork);
+    if (prepare_stream) cudaStreamDestroy(prepare_stream);
+    if (prepare_fork) cudaEventDestroy(prepare_fork);
+    if (prepare_join) cudaEventDestroy(prepare_join);
     if (arena) cudaFree(arena);
     if (host_block) cudaFreeHost(host_block);
     if (butteraugli) ButteraugliDestroy(butteraugli);
@@ -303,6 +320,19 @@ int Allocate(Session* s) {
     s->host_group_offsets = reinterpret_cast<uint32_t*>(
       reinterpret_cast<unsigned char*>(mirror) + Align(s->token_capacity * 6, 16));
   }
+  for (auto& side : s->fan_side) {
+    status = CheckCuda(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking),
+                       "session: side stream");
+    if (status != GJXL_B200_OK) return status;
+  }
+  for (cudaEvent_t* e : {&s->fan_fork, &s->fan_join[0], &s->fan_join[1], &s->fan_join[2],
+                         &s->prepare_fork, &s->prepare_join}) {
+    status = CheckCuda(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "session: event");
+    if (status != GJXL_B200_OK) return status;
+  }
+  status = CheckCuda(cudaStreamCreateWithFlags(&s->prepare_stream, cudaStreamNonBlocking),
+                     "session: prepare stream");
+  if (status != GJXL_B200_OK) return status;
   if (s->options.profile_stages) {
     for (auto& e : s->events) {
       status = CheckCuda(cudaEventCreate(&e), "session: cudaEventCreate");
@@ -323,17 +353,31 @@ void Mark(Session* s, int stage, cudaStream_t stream) {
     if (gjxl_status_ != GJXL_B200_OK) return gjxl_status_; \
   } while (0)
 
+StreamFan MakeFan(const Session* s, cudaStream_t stream) {
+  StreamFan fan;
+  fan.main = stream;
+  for (int i = 0; i < StreamFan::kSide; ++i) {
+    fan.side[i] = s->fan_side[i];
+    fan.join[i] = s->fan_join[i];
+  }
+  fan.fork = s->fan_fork;
+  return fan;
+}
+
 int RunAq(Session* s, cudaStream_t stream) {
   const float target = s->options.butteraugli_target;
   const size_t blocks = s->bx * s->by;
   GJXL_TRY(AqBuildAnchors(s->cells, s->bx, s->by, s->anchors, s->anchor_counts, stream));
+  const StreamFan fan = MakeFan(s, stream);
   GJXL_TRY(AqForwardCoefficients(s->pre, s->pw, s->pitch, s->bx, s->by, s->anchors,
-                                 s->anchor_counts, s->coef, stream));
+                                 s->anchor_counts, s->coef, stream, &fan));
   GJXL_TRY(AqAdjustField(s->cells, s->bx, s->by, s->quant, s->adjusted, target, stream));
   GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->field, s->adjusted, blocks * sizeof(float),
                                      cudaMemcpyDeviceToDevice, stream), "session: field"));
   GJXL_TRY(AqPolicySetup(s->adjusted, blocks, target, s->range, s->policy, s->error, stream));
-  GJXL_TRY(ButteraugliPrepare(s->butteraugli, s->linear, s->lin_stride, s->lin_pitch, stream));
+  // The reference preparation (queued on its own stream after the input)
+  // must be done before the first comparison.
+  GJXL_TRY(CheckCuda(cudaStreamWaitEvent(stream, s->prepare_join, 0), "session: prepare join"));
   Mark(s, kStageAqLoop, stream);
   for (int iteration = 0; iteration <= s->iterations; ++iteration) {
     GJXL_TRY(AqQuantizer_(s->field, blocks, s->policy, s->quantizer, s->raw, s->select_state,
@@ -342,14 +386,14 @@ int RunAq(Session* s, cudaStream_t stream) {
                         s->final_y_to_x, s->final_y_to_b, stream));
     GJXL_TRY(AqCoding(s->anchors, s->anchor_counts, s->bx, s->by, s->coef, s->pw, s->pitch,
                       s->qac, s->dc, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
-                      s->matrix_multipliers, s->error, stream));
+                      s->matrix_multipliers, s->error, stream, &fan));
     GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, 1, stream));
     GJXL_TRY(AqInverseSigma(s->cells, s->bx, s->by, s->raw, s->quantizer, s->inverse_sigma,
                             stream));
     GJXL_TRY(AqSmoothDc(s->dc_rec, s->bx, s->by, s->quantizer, s->dc_smooth, stream));
     GJXL_TRY(AqReconstruct(s->anchors, s->anchor_counts, s->bx, s->by, s->qac, s->pw, s->pitch,
                            s->dc_smooth, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
-                           s->matrix_multipliers, s->recon, stream));
+                           s->matrix_multipliers, s->recon, stream, &fan));
     GJXL_TRY(AqLoopFilters(s->recon, s->pw, s->pitch, s->width, s->height, s->inverse_sigma,
                            s->bx, s->filter_a, s->filter_b, s->filtered, s->error, stream));
     GJXL_TRY(AqOpsinToLinear(s->filtered, s->width, s->height, s->options.intensity_target,
@@ -377,6 +421,14 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
                                    s->options.intensity_target, s->linear, s->lin_stride,
                                    s->lin_pitch, s->opsin, s->pw, s->pitch, s->pw, s->ph,
                                    s->error, stream));
+  // Butteraugli reference preparation beside the front half.
+  GJXL_TRY(CheckCuda(cudaEventRecord(s->prepare_fork, stream), "session: prepare fork"));
+  GJXL_TRY(CheckCuda(cudaStreamWaitEvent(s->prepare_stream, s->prepare_fork, 0),
+                     "session: prepare fork"));
+  GJXL_TRY(ButteraugliPrepare(s->butteraugli, s->linear, s->lin_stride, s->lin_pitch,
+                              s->prepare_stream));
+  GJXL_TRY(CheckCuda(cudaEventRecord(s->prepare_join, s->prepare_stream),
+                     "session: prepare join"));
   Mark(s, kStageStats, stream);
   const bool stats = s->options.effort >= 7;  // ShouldComputeQuantizationMatrixScaleStats
   if (stats) {
@@ -401,10 +453,11 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
   Mark(s, kStageInitialCfl, stream);
   GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b, stream));
   Mark(s, kStageAcCosts, stream);
+  const StreamFan fan = MakeFan(s, stream);
   const bool dense = s->options.effort >= 10;
   GJXL_TRY(LaunchAcStrategyCosts(s->pre, s->pw, s->pitch, s->pw, s->ph, s->quant, s->pixel_mask,
                                  s->pw, s->y_to_x, s->y_to_b, target, dense, s->costs, s->error,
-                                 stream));
+                                 stream, &fan));
   Mark(s, kStageAcMerge, stream);
   GJXL_TRY(LaunchAcStrategySearch(s->costs, s->pw, s->ph, target, dense, s->cells, s->error,
                                   stream));
