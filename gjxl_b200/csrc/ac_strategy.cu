@@ -18,8 +18,9 @@
 // of 384 threads evaluates K = 1024 / (W*H) candidates (all three channels)
 // entirely in shared memory: pixels -> FP64 row pass -> FP64 column pass ->
 // quantize -> FP64 inverse row/column passes -> weighted loss. Each FP64
-// pass gives every thread one 8-output chunk of one line, with the DCT basis
-// in constant memory (line_dct.cuh). The reference's
+// pass gives every thread one 8-output chunk of one line, with the length-8
+// and length-16 bases in constant memory and the length-32 basis staged in
+// shared memory (line_dct.cuh). The reference's
 // order-dependent float sums (magnitude cost, pixel loss) are done by one
 // thread per (candidate, channel) in the reference's order.
 
@@ -103,9 +104,14 @@ struct CostLayout {
   // plane, same index at the same time) of each quarter warp hit distinct
   // banks.
   static constexpr int TermPitch = N + 4;
-  static constexpr size_t SharedBytes = static_cast<size_t>(Planes) * (4 + 4 + 8) +
-                                        static_cast<size_t>(KC) * TermPitch * 4 +
-                                        static_cast<size_t>(K) * N * 4;
+  // Families with a length-32 side read that pass's basis from a shared copy
+  // (the forward table through the forward passes, then the inverse table).
+  static constexpr bool kStagedBasis = W == 32 || H == 32;
+  static constexpr int BasisDoubles = kStagedBasis ? 32 * 32 : 0;
+  static constexpr size_t SharedBytes = static_cast<size_t>(BasisDoubles) * 8 +
+                                        static_cast<size_t>(Planes) * (4 + 4 + 8) +
+                                        static_cast<size_t>(KC) * TermPitch * 4;
+  static_assert(K * N <= Planes, "the pixel mask fits the residual buffer");
   static_assert(Batch::Items == kCostThreads, "one chunk per thread and pass");
 };
 
@@ -137,11 +143,12 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   constexpr int N = S::N, K = Lay::K, KC = Lay::KC;
   static_assert(K == S::K, "candidates per CTA");
   extern __shared__ __align__(16) unsigned char smem[];
-  double* T = reinterpret_cast<double*>(smem);             // [KC][H][W+1] row-pass results
+  double* basis = reinterpret_cast<double*>(smem);         // [32][32] staged length-32 basis
+  double* T = basis + Lay::BasisDoubles;                   // [KC][H][W+1] row-pass results
   float* A = reinterpret_cast<float*>(T + Lay::Planes);    // [KC][H][W+1] pixels, residuals
   float* B = A + Lay::Planes;                              // [KC][H][W+1] coefficients, pixels
   float* terms = B + Lay::Planes;                          // [KC][N + 4] ordered sum terms
-  float* mask = terms + KC * Lay::TermPitch;               // [K][H][W] pixel mask
+  float* mask = A;  // [K][H][W] pixel mask, once the inverse row pass has read A
   __shared__ int anchor_x[K], anchor_y[K];
   __shared__ float quant_norm[K], cfl[K][3];
   __shared__ float magnitude[K][3], loss_sum[K][3];
@@ -173,13 +180,22 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
-  // Pixels into A and the pixel mask into `mask` (one W-float run of the
-  // source per row): every load of a thread is issued before the first
-  // store, so their latencies overlap.
+  // Pixels into A (one W-float run of the source per row) and the forward
+  // length-32 basis into `basis`: every load of a thread is issued before the
+  // first store, so their latencies overlap.
+  constexpr int kBasisLoads = (Lay::BasisDoubles / 2 + kCostThreads - 1) / kCostThreads;
+  const double2* staged_forward = reinterpret_cast<const double2*>(kDctStagedForwardT32);
+  const double2* staged_inverse = reinterpret_cast<const double2*>(kDctStagedInverse32);
+  double2* basis2 = reinterpret_cast<double2*>(basis);
   {
     constexpr int kPixelLoads = KC * N / kCostThreads;
-    constexpr int kMaskLoads = (K * N + kCostThreads - 1) / kCostThreads;
-    float pixel[kPixelLoads], pmask[kMaskLoads];
+    float pixel[kPixelLoads];
+    double2 table[kBasisLoads > 0 ? kBasisLoads : 1];
+#pragma unroll
+    for (int q = 0; q < kBasisLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      if (i < Lay::BasisDoubles / 2) table[q] = __ldg(staged_forward + i);
+    }
 #pragma unroll
     for (int q = 0; q < kPixelLoads; ++q) {
       const int i = tid + q * kCostThreads;
@@ -187,14 +203,6 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
       pixel[q] = anchor_x[k] < 0 ? 0.0f
                : p.opsin[c * p.pitch + static_cast<size_t>(anchor_y[k] * 8 + y) * p.stride +
                          anchor_x[k] * 8 + x];
-    }
-#pragma unroll
-    for (int q = 0; q < kMaskLoads; ++q) {
-      const int i = tid + q * kCostThreads;
-      const int k = i / N, r = i % N, y = r / W, x = r % W;
-      pmask[q] = i >= K * N || anchor_x[k] < 0 ? 1.0f
-               : p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
-                              anchor_x[k] * 8 + x];
     }
     // ComputeQuantNormUnchecked (ac_strategy.cpp:103-130) and the CfL
     // factors, while the loads above are in flight.
@@ -236,26 +244,34 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
       if (anchor_x[kc / 3] >= 0) A[kc * Lay::PlanePitch + y * Lay::RowPitch + x] = pixel[q];
     }
 #pragma unroll
-    for (int q = 0; q < kMaskLoads; ++q) {
+    for (int q = 0; q < kBasisLoads; ++q) {
       const int i = tid + q * kCostThreads;
-      if (i < K * N && anchor_x[i / N] >= 0) mask[i] = pmask[q];
+      if (i < Lay::BasisDoubles / 2) basis2[i] = table[q];
     }
   }
   __syncthreads();
 
   // Forward DCT (ForwardDctCpu): rows into T, then columns into B.
   const auto present = [&](int plane) { return anchor_x[plane / 3] >= 0; };
-  BatchRowPass<W, H, KC, true>(A, T, tid, kCostThreads, present);
+  const double* staged = Lay::kStagedBasis ? basis : nullptr;
+  BatchRowPass<W, H, KC, true>(A, T, tid, kCostThreads, present, staged);
   __syncthreads();
-  BatchColumnPass<W, H, KC, true>(T, B, tid, kCostThreads, present);
+  BatchColumnPass<W, H, KC, true>(T, B, tid, kCostThreads, present, staged);
   __syncthreads();
 
   // Quantize, coefficient j = coefficient_index(v, u) by coefficient:
   // residual coefficients into A at (v, u), sqrt terms into terms[j]. The
-  // quantization weights of all of a thread's coefficients are loaded first.
+  // quantization weights of all of a thread's coefficients (and the inverse
+  // length-32 basis, which replaces the forward one) are loaded first.
   {
     constexpr int kPerThread = KC * N / kCostThreads;
     float inv[kPerThread], dq[kPerThread];
+    double2 table[kBasisLoads > 0 ? kBasisLoads : 1];
+#pragma unroll
+    for (int q = 0; q < kBasisLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      if (i < Lay::BasisDoubles / 2) table[q] = __ldg(staged_inverse + i);
+    }
 #pragma unroll
     for (int q = 0; q < kPerThread; ++q) {
       const int i = tid + q * kCostThreads;
@@ -284,8 +300,26 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
         atomicAdd(&nonzero[k][c], static_cast<uint32_t>(__popc(nz)));
       }
     }
+#pragma unroll
+    for (int q = 0; q < kBasisLoads; ++q) {
+      const int i = tid + q * kCostThreads;
+      if (i < Lay::BasisDoubles / 2) basis2[i] = table[q];
+    }
   }
   __syncthreads();
+
+  // The pixel mask is loaded now and kept in registers until the inverse
+  // row pass has read the residual out of A, where it then goes.
+  constexpr int kMaskLoads = (K * N + kCostThreads - 1) / kCostThreads;
+  float pmask[kMaskLoads];
+#pragma unroll
+  for (int q = 0; q < kMaskLoads; ++q) {
+    const int i = tid + q * kCostThreads;
+    const int k = i / N, r = i % N, y = r / W, x = r % W;
+    pmask[q] = i >= K * N || anchor_x[k] < 0 ? 1.0f
+             : p.pixel_mask[static_cast<size_t>(anchor_y[k] * 8 + y) * p.mask_stride +
+                            anchor_x[k] * 8 + x];
+  }
 
   // Ordered magnitude sums (one thread per candidate and channel); these
   // threads then join the inverse row pass, which does not touch `terms`.
@@ -294,9 +328,14 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
 
   // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
-  BatchRowPass<W, H, KC, false>(A, T, tid, kCostThreads, present);
+  BatchRowPass<W, H, KC, false>(A, T, tid, kCostThreads, present, staged);
   __syncthreads();
-  BatchColumnPass<W, H, KC, false>(T, B, tid, kCostThreads, present);
+#pragma unroll
+  for (int q = 0; q < kMaskLoads; ++q) {
+    const int i = tid + q * kCostThreads;
+    if (i < K * N && anchor_x[i / N] >= 0) mask[i] = pmask[q];
+  }
+  BatchColumnPass<W, H, KC, false>(T, B, tid, kCostThreads, present, staged);
   __syncthreads();
 
   // Weighted eighth powers in pixel order.

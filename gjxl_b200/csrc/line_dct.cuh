@@ -14,10 +14,11 @@
 // independent work. Callers map warps to chunks so that the chunk is
 // warp-uniform. For lengths 8 and 16 the chunk is a template parameter and,
 // fully unrolled, every basis value is a compile-time offset into constant
-// memory that enters the multiply as a constant-bank operand. Length 32 reads
-// the basis from constant memory with a runtime index (warp-uniform, so the
-// constant cache broadcasts it), because its fully unrolled code thrashes the
-// instruction cache.
+// memory that enters the multiply as a constant-bank operand. Length 32 keeps
+// the sample loop rolled, because its fully unrolled code thrashes the
+// instruction cache, and reads the basis with a runtime (warp-uniform) index:
+// from a copy that the caller staged in shared memory, four 128-bit broadcast
+// loads per sample, or else from constant memory.
 #pragma once
 
 #include "dct_basis.inc"
@@ -98,15 +99,47 @@ __device__ __forceinline__ void LineChunkTable(int chunk, const In* __restrict__
   for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
 }
 
+// As LineChunkTable, with the basis table staged in shared memory by the
+// caller (laid out [s][k], 16-byte aligned): every lane of the warp reads the
+// same eight entries per sample, four 128-bit broadcast loads.
+template <int L, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunkShared(int chunk, const double* __restrict__ table,
+                                                const In* __restrict__ in,
+                                                Out* __restrict__ out) {
+  double acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+  const double2* row = reinterpret_cast<const double2*>(table + chunk * 8);
+#pragma unroll 4
+  for (int s = 0; s < L; ++s) {
+    const double v = static_cast<double>(in[s * InStep]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 b = row[s * (L / 2) + q];
+      acc[2 * q] += v * b.x;
+      acc[2 * q + 1] += v * b.y;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
+}
+
 // Runtime chunk index (warp-uniform). Lengths 8 and 16 use the unrolled form
-// with compile-time basis offsets; length 32 uses the table form, because
-// the fully unrolled length-32 passes outgrow the instruction cache.
+// with compile-time basis offsets; length 32 reads its basis from a shared
+// table when the caller staged one (`table`), else from constant memory,
+// because the fully unrolled length-32 passes outgrow the instruction cache.
 template <int L, bool kForward, int InStep, int OutStep, typename In, typename Out>
 __device__ __forceinline__ void LineChunkAt(int chunk, const In* __restrict__ in,
-                                            Out* __restrict__ out) {
+                                            Out* __restrict__ out,
+                                            const double* table = nullptr) {
   if constexpr (L == 32) {
-    LineChunkTable<L, kForward, InStep, OutStep>(chunk, in, out);
+    if (table != nullptr) {
+      LineChunkShared<L, InStep, OutStep>(chunk, table, in, out);
+    } else {
+      LineChunkTable<L, kForward, InStep, OutStep>(chunk, in, out);
+    }
   } else {
+    (void)table;
     switch (chunk) {
       case 0:
         LineChunk<L, kForward, 0, InStep, OutStep>(in, out);
@@ -145,24 +178,25 @@ struct PlaneBatch {
 // Row pass over all KC * H rows of `in` into `out` (same layout): item
 // `item` is chunk item / (KC * H) of row item % (KC * H). `valid(plane)`
 // skips planes of absent transforms.
+// `table`: a shared copy of the width-length basis laid out [s][k], or null.
 template <int W, int H, int KC, bool kForward, typename In, typename Valid>
 __device__ __forceinline__ void BatchRowPass(const In* in, double* out, int tid, int threads,
-                                             Valid valid) {
+                                             Valid valid, const double* table = nullptr) {
   using B = PlaneBatch<W, H, KC>;
   constexpr int kLines = KC * H;
   for (int item = tid; item < B::Items; item += threads) {
     const int chunk = item / kLines, line = item % kLines;
     if (!valid(line / H)) continue;
     LineChunkAt<W, kForward, 1, 1>(chunk, in + line * B::RowPitch,
-                                   out + line * B::RowPitch + chunk * 8);
+                                   out + line * B::RowPitch + chunk * 8, table);
   }
 }
 
 // Column pass over all KC * W columns: item `item` is chunk item / (KC * W)
-// of column item % (KC * W).
+// of column item % (KC * W). `table`: as for the row pass, height-length.
 template <int W, int H, int KC, bool kForward, typename Out, typename Valid>
 __device__ __forceinline__ void BatchColumnPass(const double* in, Out* out, int tid, int threads,
-                                                Valid valid) {
+                                                Valid valid, const double* table = nullptr) {
   using B = PlaneBatch<W, H, KC>;
   constexpr int kLines = KC * W;
   for (int item = tid; item < B::Items; item += threads) {
@@ -171,7 +205,8 @@ __device__ __forceinline__ void BatchColumnPass(const double* in, Out* out, int 
     if (!valid(plane)) continue;
     const int base = plane * B::PlanePitch + u;
     LineChunkAt<H, kForward, B::RowPitch, B::RowPitch>(chunk, in + base,
-                                                       out + base + chunk * 8 * B::RowPitch);
+                                                       out + base + chunk * 8 * B::RowPitch,
+                                                       table);
   }
 }
 

@@ -47,3 +47,9 @@ def test_transposed_forward_tables():
     for n in (8, 16, 32):
         forward = tables[f"Forward{n}"].reshape(n, n)
         assert np.array_equal(tables[f"ForwardT{n}"].reshape(n, n), forward.T)
+
+
+def test_staged_tables_equal_constant_tables():
+    tables = committed_tables()
+    assert np.array_equal(tables["StagedForwardT32"], tables["ForwardT32"])
+    assert np.array_equal(tables["StagedInverse32"], tables["Inverse32"])
