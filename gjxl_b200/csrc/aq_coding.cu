@@ -380,18 +380,33 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   extern __shared__ __align__(16) float terms[];  // [a_x, b_x, a_b, b_b][kFinalCflTerms]
   __shared__ int block_terms[64], offsets[64], total_terms;
   __shared__ uint8_t group_block[64];  // anchor block of each 64-term group
+  // Per anchor block: covered width and height, inverse-dequant table
+  // offset, and the quantization scale of its raw quant.
+  __shared__ uint8_t block_cw[64], block_ch[64];
+  __shared__ int block_table[64];
+  __shared__ float block_scale[64];
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
   const int bx0 = tx * 8, by0 = ty * 8;
   const int tw = min(8, p.grid.blocks_x - bx0), th = min(8, p.grid.blocks_y - by0);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x < 64) {
-    int n = 0, cw, ch, s;
+    int n = 0, cw = 1, ch = 1, s = kStrategyDct8;
     const int b = threadIdx.x;
-    if (b < tw * th && AnchorAt(p.grid, (by0 + b / tw) * p.grid.blocks_x + bx0 + b % tw, &cw,
-                                &ch, &s)) {
-      n = cw * ch * 64;
+    if (b < tw * th) {
+      const int block = (by0 + b / tw) * p.grid.blocks_x + bx0 + b % tw;
+      if (AnchorAt(p.grid, block, &cw, &ch, &s)) {
+        n = cw * ch * 64;
+        const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
+                        : s == kStrategyDct32x32 ? kTableDct32
+                        : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
+                                                                             : kTableDct16x32;
+        block_table[b] = static_cast<int>(p.table_offset[table]);
+        block_scale[b] = p.q->scale * 128.0f * static_cast<float>(p.raw[block]);
+      }
     }
+    block_cw[b] = static_cast<uint8_t>(cw);
+    block_ch[b] = static_cast<uint8_t>(ch);
     block_terms[b] = n;
   }
   __syncthreads();
@@ -409,41 +424,51 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   __syncthreads();
   // Every thread takes terms e = tid, tid + 128, ... of the tile; every
   // anchor's term count is a multiple of 64, so term e belongs to the anchor
-  // of group e / 64.
-  const float scale128 = p.q->scale * 128.0f;
+  // of group e / 64. Batches of kBatch terms: all their global loads are
+  // issued before the first term is computed.
+  constexpr int kBatch = 8;
   const int count = total_terms;
-  for (int e = threadIdx.x; e < count; e += kFinalCflThreads) {
-    const int b = group_block[e / 64], i = e - offsets[b];
-    const int bx = bx0 + b % tw, by = by0 + b / tw;
-    int cw, ch, s;
-    AnchorAt(p.grid, by * p.grid.blocks_x + bx, &cw, &ch, &s);
-    const int n = cw * ch * 64;
-    const int table = s == kStrategyDct8 ? kTableDct8 : s == kStrategyDct16x16 ? kTableDct16
-                    : s == kStrategyDct32x32 ? kTableDct32
-                    : (s == kStrategyDct16x8 || s == kStrategyDct8x16) ? kTableDct8x16
-                                                                         : kTableDct16x32;
-    const float* inv_x = p.inverse_dequant + p.table_offset[table];
-    const float* inv_b = inv_x + 2 * n;
-    const float quant_scale = scale128 * static_cast<float>(p.raw[by * p.grid.blocks_x + bx]);
-    const int w = cw * 8;
-    // LLF extent: covered blocks with the longer side first.
-    const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
-    const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
-    const int cy = i / sw, cx = i % sw;
-    const bool llf = cy < lfh && cx < lfw;
-    const size_t at = static_cast<size_t>(by * 8 + i / w) * p.coef_stride + bx * 8 + i % w;
-    const float luma_v = llf ? 0.0f : p.coef[p.coef_pitch + at];
-    const float x_v = llf ? 0.0f : p.coef[at];
-    const float b_v = llf ? 0.0f : p.coef[2 * p.coef_pitch + at];
-    const float base_x = 0.0f, base_b = 1.0f;
-    const float luma_x = luma_v * inv_x[i] * quant_scale;
-    const float chroma_x = x_v * inv_x[i] * quant_scale;
-    const float luma_b = luma_v * inv_b[i] * quant_scale;
-    const float chroma_b = b_v * inv_b[i] * quant_scale;
-    terms[e] = luma_x / 84.0f;
-    terms[kFinalCflTerms + e] = base_x * luma_x - chroma_x;
-    terms[2 * kFinalCflTerms + e] = luma_b / 84.0f;
-    terms[3 * kFinalCflTerms + e] = base_b * luma_b - chroma_b;
+  for (int e0 = threadIdx.x; e0 < count; e0 += kBatch * kFinalCflThreads) {
+    float luma_v[kBatch], x_v[kBatch], b_v[kBatch], inv_x[kBatch], inv_b[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      const int e = e0 + j * kFinalCflThreads;
+      luma_v[j] = x_v[j] = b_v[j] = inv_x[j] = inv_b[j] = 0.0f;
+      if (e >= count) continue;
+      const int b = group_block[e / 64], i = e - offsets[b];
+      const int cw = block_cw[b], ch = block_ch[b];
+      const int w = cw * 8;
+      // LLF extent: covered blocks with the longer side first.
+      const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
+      const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
+      const int cy = i / sw, cx = i % sw;
+      const bool llf = cy < lfh && cx < lfw;
+      const float* inv = p.inverse_dequant + block_table[b];
+      inv_x[j] = inv[i];
+      inv_b[j] = inv[2 * cw * ch * 64 + i];
+      if (!llf) {
+        const size_t at = static_cast<size_t>((by0 + b / tw) * 8 + i / w) * p.coef_stride +
+                          (bx0 + b % tw) * 8 + i % w;
+        luma_v[j] = p.coef[p.coef_pitch + at];
+        x_v[j] = p.coef[at];
+        b_v[j] = p.coef[2 * p.coef_pitch + at];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      const int e = e0 + j * kFinalCflThreads;
+      if (e >= count) continue;
+      const float quant_scale = block_scale[group_block[e / 64]];
+      const float base_x = 0.0f, base_b = 1.0f;
+      const float luma_x = luma_v[j] * inv_x[j] * quant_scale;
+      const float chroma_x = x_v[j] * inv_x[j] * quant_scale;
+      const float luma_b = luma_v[j] * inv_b[j] * quant_scale;
+      const float chroma_b = b_v[j] * inv_b[j] * quant_scale;
+      terms[e] = luma_x / 84.0f;
+      terms[kFinalCflTerms + e] = base_x * luma_x - chroma_x;
+      terms[2 * kFinalCflTerms + e] = luma_b / 84.0f;
+      terms[3 * kFinalCflTerms + e] = base_b * luma_b - chroma_b;
+    }
   }
   __syncthreads();
   if (warp != 0) return;

@@ -11,10 +11,10 @@
 //
 // One CTA of 256 threads per tile. Phase 1: each warp transforms (block,
 // channel) pairs — lane l owns row-pass outputs l and l+32 and gathers the
-// column inputs with double shuffles. Phase 2: per Newton iteration warps
-// 1-7 evaluate the derivative terms of the next chunk while warp 0 adds the
-// current one in order, twelve lanes per map, each owning one of the 3 sums
-// x 4 lanes.
+// column inputs with double shuffles. Phase 2: warp 0 alone runs the Newton
+// iterations, twelve lanes per map, each owning one of the 3 sums x 4 lanes
+// and evaluating its terms as it adds them (no barriers); the other warps
+// leave, so that the SM's other tiles take their issue slots.
 
 #include <cmath>
 #include <cstring>
@@ -27,7 +27,7 @@ namespace gjxl_b200 {
 namespace {
 
 constexpr int kTileValues = 64 * 64;  // up to 64 blocks of 64 coefficients
-constexpr int kCflChunk = 128;        // elements per shared term chunk (divides kTileValues)
+constexpr int kMapPad = 4;            // pairs between the two maps' arrays
 
 struct CflParams {
   const float* opsin;  // Gaborish-inverted padded XYB
@@ -59,9 +59,11 @@ __device__ __forceinline__ int8_t QuantizeMultiplier(float x) {
 }
 
 __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ CflParams p) {
-  // [4][kTileValues]: per element a = luma / 84 and b = base * luma - chroma
-  // for the y_to_x problem (base 0) and the y_to_b problem (base 1).
-  extern __shared__ __align__(16) float values[];
+  // Per map (0: y_to_x, 1: y_to_b) and element the pair {a, b}:
+  // a = luma / 84 and b = base * luma - chroma (base 0 for y_to_x, 1 for
+  // y_to_b). Map 1 starts kMapPad pairs further on, so that the two maps'
+  // elements of one index fall in different banks.
+  extern __shared__ __align__(16) float2 pairs[];
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
   const int bx0 = tx * 8, by0 = ty * 8;
@@ -69,10 +71,8 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
   const int th = min(8, static_cast<int>(p.blocks_y) - by0);
   const int blocks = tw * th;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* luma_x = values;
-  float* chroma_x = values + kTileValues;
-  float* luma_b = values + 2 * kTileValues;
-  float* chroma_b = values + 3 * kTileValues;
+  float2* pairs_x = pairs;
+  float2* pairs_b = pairs + kTileValues + kMapPad;
   __shared__ float y_coef[8][64];  // per warp: Y coefficients of the current block
 
   // Phase 1: DCT8 of every block, Y first so X/B can pair with it.
@@ -121,124 +121,78 @@ __global__ void __launch_bounds__(256) InitialCflKernel(const __grid_constant__ 
           __syncwarp();
           const float luma = y_coef[warp][index] * __ldg(p.inv_b + index) * 1.0f;
           const float chroma = value * __ldg(p.inv_b + index) * 1.0f;
-          luma_b[at] = luma / 84.0f;
-          chroma_b[at] = 1.0f * luma - chroma;
+          pairs_b[at] = make_float2(luma / 84.0f, 1.0f * luma - chroma);
         } else {
           const float luma = y_coef[warp][index] * __ldg(p.inv_x + index) * 1.0f;
           const float chroma = value * __ldg(p.inv_x + index) * 1.0f;
-          luma_x[at] = luma / 84.0f;
-          chroma_x[at] = 0.0f * luma - chroma;
+          pairs_x[at] = make_float2(luma / 84.0f, 0.0f * luma - chroma);
         }
       }
       __syncwarp();
     }
   }
   __syncthreads();
+  if (warp != 0) return;
 
-  // Phase 2: FindBestMultiplier (non-fast) for both maps. The element terms
-  // of the three derivative sums (center, +eps, -eps) are computed a chunk of
-  // kCflChunk elements at a time into one of two shared buffers while warp 0
-  // adds the previous chunk in the reference's order: lanes 0..11 solve
-  // y_to_x and 12..23 y_to_b, lane 4 * kind + slot of a group owning
-  // derivative sum `kind` over the elements i = slot (mod 4), in increasing
-  // i. One barrier per chunk. Elements skipped by the reference contribute
-  // +0.0, which leaves the (never -0.0) sum unchanged.
-  // Rows padded by 4 floats: the 24 summing lanes read 24 distinct banks.
-  __shared__ float terms[2][2][3][kCflChunk + 4];
-  __shared__ float solution[2];
-  __shared__ int solved[2];
+  // Phase 2: FindBestMultiplier (non-fast) for both maps, by warp 0 alone.
+  // Lanes 0..11 solve y_to_x and 12..23 y_to_b; lane 4 * kind + slot of a
+  // map owns derivative sum `kind` (center, +eps, -eps) over the elements
+  // i = slot (mod 4), in increasing i, the reference's four-lane order. Each
+  // lane evaluates its terms as it adds them: the dependent adds of the 24
+  // chains run back to back, with the term arithmetic between them. Elements
+  // skipped by the reference contribute +0.0, which leaves the (never -0.0)
+  // sum unchanged.
   const int count = blocks * 64;
-  const int chunks = (count + kCflChunk - 1) / kCflChunk;
   const float kDistanceMultiplierAc = 1.0e-9f;
   const float kEpsilon = 100.0f;
-  if (threadIdx.x < 2) {
-    solution[threadIdx.x] = 0.0f;
-    solved[threadIdx.x] = 0;
-  }
-  const int group = lane / 12;  // warp 0: 0 y_to_x, 1 y_to_b, 2 idle lanes
+  const bool active = lane < 24;
+  const int map = active ? lane / 12 : 0;
   const int member = lane % 12;
   const int kind = member / 4, slot = member % 4;
-  __syncthreads();
-  // Terms of chunk `chunk` into buffer `buffer`, by the threads first..255,
-  // two adjacent elements per item (count is a multiple of 64, so pairs
-  // never straddle its end).
-  const auto produce = [&](int chunk, int buffer, int first, const float (&x_map)[2],
-                           const int (&done_map)[2]) {
-    for (int t = static_cast<int>(threadIdx.x) - first; t < kCflChunk;
-         t += blockDim.x - first) {
-      const int map = t / (kCflChunk / 2), e = 2 * (t % (kCflChunk / 2));
-      const int i = chunk * kCflChunk + e;
-      if (done_map[map] || i >= count) continue;
-      const float* A = map == 0 ? luma_x : luma_b;       // a = luma / 84
-      const float* Bv = map == 0 ? chroma_x : chroma_b;  // b = base * luma - chroma
-      const float2 a2 = *reinterpret_cast<const float2*>(A + i);
-      const float2 b2 = *reinterpret_cast<const float2*>(Bv + i);
-      const float x = x_map[map], xp = x + kEpsilon, xm = x - kEpsilon;
-      float* out = terms[buffer][map][0] + e;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const float a = q == 0 ? a2.x : a2.y, b = q == 0 ? b2.x : b2.y;
-        const float center = fmaf(a, x, b);
-        const bool skip = fabsf(center) >= 100.0f;
-        const float scale = (2.0f / 3.0f) * a;
-        const float r[3] = {center, fmaf(a, xp, b), fmaf(a, xm, b)};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          float d = scale * (fabsf(r[k]) + 1.0f);
-          d = r[k] < 0.0f ? -d : d;
-          out[k * (kCflChunk + 4) + q] = skip ? 0.0f : d;
-        }
-      }
-    }
-  };
+  const float2* ab = map == 0 ? pairs_x : pairs_b;
+  float x = 0.0f;
+  bool done = false;
   for (int iteration = 0; iteration < p.iterations; ++iteration) {
-    if (solved[0] && solved[1]) break;
-    const float x_map[2] = {solution[0], solution[1]};
-    const int done_map[2] = {solved[0], solved[1]};
+    const bool done_x = __shfl_sync(0xffffffffu, done, 0);
+    const bool done_b = __shfl_sync(0xffffffffu, done, 12);
+    if (done_x && done_b) break;
+    const float xk = kind == 0 ? x : kind == 1 ? x + kEpsilon : x - kEpsilon;
     float lane_sum = 0.0f;
-    produce(0, 0, 0, x_map, done_map);
-    __syncthreads();
-    for (int chunk = 0; chunk < chunks; ++chunk) {
-      if (warp == 0) {
-        if (group < 2 && !done_map[group]) {
-          const float* t = terms[chunk & 1][group][kind];
-          const int limit = min(kCflChunk, count - chunk * kCflChunk);
+    if (active && !done) {
 #pragma unroll 8
-          for (int e = slot; e < limit; e += 4) lane_sum += t[e];
-        }
-      } else if (chunk + 1 < chunks) {
-        produce(chunk + 1, (chunk + 1) & 1, 32, x_map, done_map);
+      for (int i = slot; i < count; i += 4) {
+        const float2 v = ab[i];
+        const float center = fmaf(v.x, x, v.y);
+        const float r = fmaf(v.x, xk, v.y);
+        float d = ((2.0f / 3.0f) * v.x) * (fabsf(r) + 1.0f);
+        d = r < 0.0f ? -d : d;
+        lane_sum += fabsf(center) >= 100.0f ? 0.0f : d;
       }
-      __syncthreads();
     }
-    if (warp == 0) {
-      // Horizontal sums (l0 + l1) + (l2 + l3) for each kind of this group.
-      const int group_base = 12 * (group < 2 ? group : 0);
-      float sums[3];
+    // Horizontal sums (l0 + l1) + (l2 + l3) for each kind of this map.
+    const int map_base = 12 * map;
+    float sums[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float l0 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 0);
-        const float l1 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 1);
-        const float l2 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 2);
-        const float l3 = __shfl_sync(0xffffffffu, lane_sum, group_base + 4 * k + 3);
-        sums[k] = (l0 + l1) + (l2 + l3);
-      }
-      if (group < 2 && member == 0 && !done_map[group]) {
-        const float x = x_map[group];
-        const float n = static_cast<float>(count);
-        const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
-        const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
-        const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
-        const float second = (plus - minus) / (2.0f * kEpsilon);
-        const float step = center / (second + 0.85f);
-        solution[group] = x - fminf(fmaxf(step, -20.0f), 20.0f);
-        if (fabsf(step) < 3.0e-3f) solved[group] = 1;
-      }
+    for (int k = 0; k < 3; ++k) {
+      const float l0 = __shfl_sync(0xffffffffu, lane_sum, map_base + 4 * k + 0);
+      const float l1 = __shfl_sync(0xffffffffu, lane_sum, map_base + 4 * k + 1);
+      const float l2 = __shfl_sync(0xffffffffu, lane_sum, map_base + 4 * k + 2);
+      const float l3 = __shfl_sync(0xffffffffu, lane_sum, map_base + 4 * k + 3);
+      sums[k] = (l0 + l1) + (l2 + l3);
     }
-    __syncthreads();
+    if (active && !done) {
+      const float n = static_cast<float>(count);
+      const float center = 2.0f * kDistanceMultiplierAc * n * x + sums[0];
+      const float plus = 2.0f * kDistanceMultiplierAc * n * (x + kEpsilon) + sums[1];
+      const float minus = 2.0f * kDistanceMultiplierAc * n * (x - kEpsilon) + sums[2];
+      const float second = (plus - minus) / (2.0f * kEpsilon);
+      const float step = center / (second + 0.85f);
+      x = x - fminf(fmaxf(step, -20.0f), 20.0f);
+      if (fabsf(step) < 3.0e-3f) done = true;
+    }
   }
-  if (threadIdx.x == 0) p.y_to_x[tile] = QuantizeMultiplier(solution[0]);
-  if (threadIdx.x == 1) p.y_to_b[tile] = QuantizeMultiplier(solution[1]);
+  if (lane == 0) p.y_to_x[tile] = QuantizeMultiplier(x);
+  if (lane == 12) p.y_to_b[tile] = QuantizeMultiplier(x);
 }
 
 }  // namespace
@@ -265,7 +219,7 @@ int LaunchInitialCfl(const float* opsin, size_t stride, size_t pitch, size_t pw,
   p.iterations = 20;
   p.y_to_x = y_to_x;
   p.y_to_b = y_to_b;
-  const size_t smem = 4 * kTileValues * sizeof(float);
+  const size_t smem = (2 * kTileValues + kMapPad) * sizeof(float2);
   status = CheckCuda(cudaFuncSetAttribute(InitialCflKernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(smem)),
