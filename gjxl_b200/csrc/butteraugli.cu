@@ -48,28 +48,53 @@ __device__ __forceinline__ int MirrorB(int c, int size) {
   return c;
 }
 
-// Separable5 (butteraugli_internal.cpp:222-260) on a 32x8 output tile: the
-// mirrored input window (tile + 2 on each side) is staged in shared memory,
-// the horizontal 5-tap pass runs over the window's 12 rows, then the vertical
-// pass, with the reference's operation order for every output.
-constexpr int kB5W = 32, kB5H = 8;
+// Separable5 (butteraugli_internal.cpp:222-260) on a 32x32 output tile of
+// 32x8 threads (four output rows each): the mirrored input window (tile + 2
+// on each side) is staged in shared memory, all of a thread's loads issued
+// before its first store; tiles whose window lies inside the image skip the
+// mirroring. The horizontal 5-tap pass runs over the window's 36 rows, then
+// the vertical pass, with the reference's operation order for every output.
+constexpr int kB5W = 32, kB5H = 32, kB5Rows = 8;
 
-__global__ void __launch_bounds__(kB5W * kB5H)
+__global__ void __launch_bounds__(kB5W * kB5Rows)
 Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
             const __grid_constant__ Kernel17 k) {
-  __shared__ float window[kB5H + 4][kB5W + 4];
-  __shared__ float horizontal[kB5H + 4][kB5W];
+  constexpr int kSpanW = kB5W + 4, kSpanH = kB5H + 4, kSpan = kSpanW * kSpanH;
+  constexpr int kThreadsB5 = kB5W * kB5Rows;
+  constexpr int kLoads = (kSpan + kThreadsB5 - 1) / kThreadsB5;
+  __shared__ float window[kSpanH][kSpanW];
+  __shared__ float horizontal[kSpanH][kB5W];
   const int plane = blockIdx.z;
   const int x0 = blockIdx.x * kB5W, y0 = blockIdx.y * kB5H;
   const float* base = in + plane * pitch;
   const int tid = threadIdx.y * kB5W + threadIdx.x;
-  for (int i = tid; i < (kB5H + 4) * (kB5W + 4); i += kB5W * kB5H) {
-    const int ty = i / (kB5W + 4), tx = i % (kB5W + 4);
-    window[ty][tx] = base[static_cast<size_t>(MirrorB(y0 + ty - 2, h)) * w + MirrorB(x0 + tx - 2, w)];
+  const bool interior = x0 >= 2 && y0 >= 2 && x0 + kSpanW - 2 <= w && y0 + kSpanH - 2 <= h;
+  float staged[kLoads];
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) {
+    const int i = tid + q * kThreadsB5;
+    if (i < kSpan) {
+      const int ty = i / kSpanW, tx = i - ty * kSpanW;
+      int gy = y0 + ty - 2, gx = x0 + tx - 2;
+      if (!interior) {
+        gy = MirrorB(gy, h);
+        gx = MirrorB(gx, w);
+      }
+      staged[q] = base[static_cast<size_t>(gy) * w + gx];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) {
+    const int i = tid + q * kThreadsB5;
+    if (i < kSpan) {
+      const int ty = i / kSpanW, tx = i - ty * kSpanW;
+      window[ty][tx] = staged[q];
+    }
   }
   __syncthreads();
-  for (int i = tid; i < (kB5H + 4) * kB5W; i += kB5W * kB5H) {
-    const int ty = i / kB5W, tx = i % kB5W;
+  const int tx = threadIdx.x;
+#pragma unroll
+  for (int ty = threadIdx.y; ty < kSpanH; ty += kB5Rows) {
     const float* row = window[ty] + tx + 2;
     float r = row[0] * k.w5[0];
     r = (row[-1] + row[1]) * k.w5[1] + r;
@@ -77,13 +102,18 @@ Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
     horizontal[ty][tx] = r;
   }
   __syncthreads();
-  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const int ty = threadIdx.y + 2, tx = threadIdx.x;
-  float r = horizontal[ty][tx] * k.w5[0];
-  r = (horizontal[ty - 1][tx] + horizontal[ty + 1][tx]) * k.w5[1] + r;
-  r = (horizontal[ty - 2][tx] + horizontal[ty + 2][tx]) * k.w5[2] + r;
-  out[plane * pitch + static_cast<size_t>(y) * w + x] = r;
+  const int x = x0 + tx;
+  if (x >= w) return;
+#pragma unroll
+  for (int q = 0; q < kB5H / kB5Rows; ++q) {
+    const int oy = threadIdx.y + q * kB5Rows, y = y0 + oy;
+    if (y >= h) break;
+    const int ty = oy + 2;
+    float r = horizontal[ty][tx] * k.w5[0];
+    r = (horizontal[ty - 1][tx] + horizontal[ty + 1][tx]) * k.w5[1] + r;
+    r = (horizontal[ty - 2][tx] + horizontal[ty + 2][tx]) * k.w5[2] + r;
+    out[plane * pitch + static_cast<size_t>(y) * w + x] = r;
+  }
 }
 
 // One tap row of ConvolutionWithTranspose at position x of a line of length n
@@ -936,8 +966,8 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
                       cudaMemcpyDeviceToDevice, stream);
     dense = s.linear_tmp;
   }
-  Blur5Kernel<<<dim3((s.w + kB5W - 1) / kB5W, (s.h + kB5H - 1) / kB5H, 3), dim3(kB5W, kB5H), 0,
-                stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
+  Blur5Kernel<<<dim3((s.w + kB5W - 1) / kB5W, (s.h + kB5H - 1) / kB5H, 3), dim3(kB5W, kB5Rows),
+                0, stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
   OpsinDynamicsKernel<<<Blocks(n), kThreads, 0, stream>>>(dense, s.w, n, s.blur3, s.xyb, s.w, s.h,
                                                           n, st.intensity_target, st.error);
   // LF: 33-tap blur of the three XYB planes straight into the LF planes.
