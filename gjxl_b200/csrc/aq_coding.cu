@@ -867,10 +867,89 @@ struct DcRings {
   uint32_t pe[3][4][kDcRing][kDcGroup];   // sub-predictor errors (prediction_errors_)
   uint32_t row0[3][4][kDcRing];           // row 0's own errors, before row 1 adds
   uint32_t reciprocal[64];                // (1 << 24) / (i + 1)
+  int wide;  // set once a stored value leaves the 32-bit bounds below
 };
 
 __device__ __forceinline__ int BitWidth64(uint64_t v) { return v == 0 ? 0 : 64 - __clzll(v); }
 __device__ __forceinline__ int BitWidth32(uint32_t v) { return v == 0 ? 0 : 32 - __clz(v); }
+
+// Bounds under which every intermediate of one predictor step fits in 32
+// bits: |quantized| <= 2^21 and |signed error| <= 2^23 for every stored
+// value the step reads, and |value * inverse step| < 2^21 for its own
+// sample. Then |8 q| <= 2^24, every sub-prediction is below 2^26 in
+// magnitude, their weighted sum (weights adding up to at most 31) below
+// 2^31, and the sub-predictor error sums below 2^28. The reference computes
+// in 64 bits; within these bounds the 32-bit step gives the same values.
+constexpr int32_t kDcNarrowQuantized = 1 << 21;
+constexpr int32_t kDcNarrowError = 1 << 23;
+constexpr float kDcNarrowScaled = 2097152.0f;  // 2^21
+
+// One step of the weighted predictor (prediction.h:73-141) and the residual
+// quantization (dc_quantization.cpp:178-199) in integer type Int: the
+// neighbours' quantized values and signed errors, the four sub-predictor
+// error sums and value * inverse step in; the quantized value, its signed
+// error and the four sub-predictor errors out.
+template <typename Int, bool kWide>
+__device__ __forceinline__ void WeightedPredictorStep(Int w, Int n, Int nw, Int ne, Int nn, Int ew,
+                                                      Int en, Int enw, Int ene,
+                                                      const uint32_t (&errors)[4],
+                                                      const uint32_t* reciprocal,
+                                                      float scaled_value, int32_t* quantized_out,
+                                                      int32_t* error_out,
+                                                      uint32_t (&sub_errors)[4]) {
+  // WeightedPredictorParameters defaults (prediction.h:36-40).
+  constexpr int kP0 = 16, kP1 = 10, kP2 = 7, kP3 = 7, kP4 = 7, kP5 = 0, kP6 = 0;
+  const uint32_t max_weights[4] = {13, 12, 12, 12};
+  uint32_t weights[4];
+  uint32_t weight_sum = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int bits = kWide ? BitWidth64(static_cast<uint64_t>(errors[i]) + 1)
+                           : BitWidth32(errors[i] + 1u);
+    const int shift = max(0, bits - 6);
+    weights[i] = 4 + ((max_weights[i] * reciprocal[errors[i] >> shift]) >> shift);
+    weight_sum += weights[i];
+  }
+  const int log_weight = BitWidth32(weight_sum) - 1;
+  weight_sum = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    weights[i] >>= log_weight - 4;
+    weight_sum += weights[i];
+  }
+  const Int n8 = n * 8, w8 = w * 8, ne8 = ne * 8, nw8 = nw * 8, nn8 = nn * 8;
+  Int predictions[4];
+  predictions[0] = w8 + ne8 - n8;
+  predictions[1] = n8 - (((en + ew + ene) * Int(kP0)) >> 5);
+  predictions[2] = w8 - (((en + ew + enw) * Int(kP1)) >> 5);
+  predictions[3] = n8 - ((enw * Int(kP2) + en * Int(kP3) + ene * Int(kP4) + (nn8 - n8) * Int(kP5) +
+                          (nw8 - w8) * Int(kP6)) >> 5);
+  Int sum = static_cast<Int>(weight_sum >> 1) - 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) sum += predictions[i] * static_cast<Int>(weights[i]);
+  Int prediction = static_cast<Int>(
+    (static_cast<int64_t>(sum) * static_cast<int64_t>(reciprocal[weight_sum - 1])) >> 24);
+  if (((en ^ ew) | (en ^ enw)) <= 0) {
+    const Int lo = min(w8, min(ne8, n8)), hi = max(w8, max(ne8, n8));
+    prediction = min(max(prediction, lo), hi);
+  }
+  const Int predicted = (prediction + 3) >> 3;
+  float residual = scaled_value;
+  residual -= static_cast<float>(predicted);
+  if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
+  float rounded = roundf(residual);
+  if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
+  const Int quantized = predicted + static_cast<Int>(rounded);
+  *quantized_out = static_cast<int32_t>(quantized);
+  // Update (prediction.h:121-141).
+  const Int scaled = quantized * 8;
+  *error_out = static_cast<int32_t>(prediction - scaled);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const Int d = predictions[i] - scaled;
+    sub_errors[i] = static_cast<uint32_t>(((d < 0 ? -d : d) + 3) >> 3);
+  }
+}
 
 __global__ void __launch_bounds__(kDcThreads, 1)
 DcQuantKernel(const __grid_constant__ DcQuantParams p) {
@@ -884,12 +963,10 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   const int y = idle ? kDcGroup : static_cast<int>(threadIdx.x) % kDcGroup;
   const int lag = c == 2 ? 1 : 0;
   for (int i = threadIdx.x; i < 64; i += blockDim.x) r.reciprocal[i] = (1u << 24) / (i + 1);
+  if (threadIdx.x == 0) r.wide = 0;
   const AqQuantizer q = *p.q;
   const float inverse_step = q.inverse_dc_steps[c] * p.precision;
   const float step_y = q.dc_steps[1] / p.precision;
-  // WeightedPredictorParameters defaults (prediction.h:36-40).
-  constexpr int64_t kP0 = 16, kP1 = 10, kP2 = 7, kP3 = 7, kP4 = 7, kP5 = 0, kP6 = 0;
-  const uint32_t max_weights[4] = {13, 12, 12, 12};
   int32_t* plane = p.quantized + c * p.pitch;
   const float* source = p.dc + c * p.pitch;
   int32_t (*Q)[kDcGroup] = r.q[c];
@@ -899,92 +976,78 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   // global-memory latency overlaps this wave's work and barrier.
   const size_t row_index = static_cast<size_t>(gy0 + min(y, gh - 1)) * stride + gx0;
   float pending = y < gh ? source[row_index] : 0.0f;  // idle threads have y >= gh
+  // This row's previous quantized value and signed error (its west
+  // neighbour), kept in registers.
+  int32_t own_q = 0, own_e = 0;
   const int waves = (gw - 1) + 2 * (gh - 1) + 2;
   for (int t = 0; t < waves; ++t) {
     const int x = t - lag - 2 * y;
+    const int wide = r.wide;
     if (y < gh && x >= 0 && x < gw) {
       const float dc_value = pending;
       if (x + 1 < gw) pending = source[row_index + x + 1];
       const int s = x & 7, sw = (x - 1) & 7, sne = (x + 1 < gw ? x + 1 : x) & 7;
       const int snw = (x ? x - 1 : x) & 7;
       const int up = y - 1, up2 = y - 2;
-      const int64_t w = x ? Q[sw][y] : y ? Q[s][up] : 0;
-      const int64_t n = y ? Q[s][up] : w;
-      const int64_t nw = x && y ? Q[sw][up] : w;
-      const int64_t ne = y && x + 1 < gw ? Q[(x + 1) & 7][up] : n;
-      const int64_t nn = y > 1 ? Q[s][up2] : n;
-      // Predict (prediction.h:73-119). The signed errors of row -1 read as
-      // zeros. The sub-predictor error sums of row 0 read the predictor's
+      const int32_t w = x ? own_q : y ? Q[s][up] : 0;
+      const int32_t n = y ? Q[s][up] : w;
+      const int32_t nw = x && y ? Q[sw][up] : w;
+      const int32_t ne = y && x + 1 < gw ? Q[(x + 1) & 7][up] : n;
+      const int32_t nn = y > 1 ? Q[s][up2] : n;
+      const int32_t ew = x ? own_e : 0;
+      const int32_t en = y ? E[s][up] : 0;
+      const int32_t enw = y ? E[snw][up] : 0;
+      const int32_t ene = y ? E[sne][up] : 0;
+      // Sub-predictor error sums (prediction.h:73-90). The signed errors of
+      // row -1 read as zeros. The error sums of row 0 read the predictor's
       // other rolling row, which by then holds only row 0's own "+="
       // updates: its entry j carries the error of (j - 1, 0) once that
       // sample is done, so north = err(x-1), northwest = err(x-2) and
       // northeast (not yet written) = 0, or north at the right edge.
-      uint32_t weights[4];
-      uint32_t weight_sum = 0;
+      uint32_t errors[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        uint32_t error;
         if (y) {
-          error = r.pe[c][i][s][up] + r.pe[c][i][sne][up] + r.pe[c][i][snw][up];
+          errors[i] = r.pe[c][i][s][up] + r.pe[c][i][sne][up] + r.pe[c][i][snw][up];
         } else {
           const uint32_t north = x ? r.row0[c][i][sw] : 0u;
           const uint32_t northeast = x + 1 < gw ? 0u : north;
           const uint32_t northwest = x >= 2 ? r.row0[c][i][(x - 2) & 7] : 0u;
-          error = north + northeast + northwest;
+          errors[i] = north + northeast + northwest;
         }
-        const int shift = max(0, BitWidth64(static_cast<uint64_t>(error) + 1) - 6);
-        weights[i] = 4 + ((max_weights[i] * r.reciprocal[error >> shift]) >> shift);
-        weight_sum += weights[i];
       }
-      const int log_weight = BitWidth32(weight_sum) - 1;
-      weight_sum = 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        weights[i] >>= log_weight - 4;
-        weight_sum += weights[i];
-      }
-      const int64_t ew = x ? E[sw][y] : 0;
-      const int64_t en = y ? E[s][up] : 0;
-      const int64_t enw = y ? E[snw][up] : 0;
-      const int64_t ene = y ? E[sne][up] : 0;
-      const int64_t n8 = n * 8, w8 = w * 8, ne8 = ne * 8, nw8 = nw * 8, nn8 = nn * 8;
-      int64_t predictions[4];
-      predictions[0] = w8 + ne8 - n8;
-      predictions[1] = n8 - (((en + ew + ene) * kP0) >> 5);
-      predictions[2] = w8 - (((en + ew + enw) * kP1) >> 5);
-      predictions[3] = n8 - ((enw * kP2 + en * kP3 + ene * kP4 + (nn8 - n8) * kP5 +
-                              (nw8 - w8) * kP6) >> 5);
-      int64_t sum = static_cast<int64_t>(weight_sum >> 1) - 1;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) sum += predictions[i] * static_cast<int64_t>(weights[i]);
-      int64_t prediction = (sum * static_cast<int64_t>(r.reciprocal[weight_sum - 1])) >> 24;
-      if (((en ^ ew) | (en ^ enw)) <= 0) {
-        const int64_t lo = min(w8, min(ne8, n8)), hi = max(w8, max(ne8, n8));
-        prediction = min(max(prediction, lo), hi);
-      }
-      const int64_t predicted = (prediction + 3) >> 3;
-      // Quantize the residual (dc_quantization.cpp:178-199).
-      const size_t index = row_index + x;
       float value = dc_value;
       if (c == 2) value = fmaf(-static_cast<float>(r.q[1][s][y]), step_y, value);
-      float residual = value * inverse_step;
-      residual -= static_cast<float>(predicted);
-      if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
-      float rounded = roundf(residual);
-      if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
-      const int64_t quantized = predicted + static_cast<int64_t>(rounded);
-      plane[index] = static_cast<int32_t>(quantized);
-      Q[s][y] = static_cast<int32_t>(quantized);
-      // Update (prediction.h:121-141).
-      const int64_t scaled = quantized * 8;
-      E[s][y] = static_cast<int32_t>(prediction - scaled);
+      const float scaled_value = value * inverse_step;
+      int32_t quantized, error_value;
+      uint32_t sub[4];
+      if (!wide && fabsf(scaled_value) < kDcNarrowScaled) {
+        WeightedPredictorStep<int32_t, false>(w, n, nw, ne, nn, ew, en, enw, ene, errors,
+                                              r.reciprocal, scaled_value, &quantized,
+                                              &error_value, sub);
+      } else {
+        WeightedPredictorStep<int64_t, true>(w, n, nw, ne, nn, ew, en, enw, ene, errors,
+                                             r.reciprocal, scaled_value, &quantized,
+                                             &error_value, sub);
+      }
+      // Later steps read this value: past the 32-bit bounds, every later
+      // step of the CTA takes the 64-bit form.
+      if (static_cast<uint32_t>(quantized) + static_cast<uint32_t>(kDcNarrowQuantized) >
+            static_cast<uint32_t>(2 * kDcNarrowQuantized) ||
+          static_cast<uint32_t>(error_value) + static_cast<uint32_t>(kDcNarrowError) >
+            static_cast<uint32_t>(2 * kDcNarrowError)) {
+        r.wide = 1;
+      }
+      plane[row_index + x] = quantized;
+      Q[s][y] = quantized;
+      E[s][y] = error_value;
+      own_q = quantized;
+      own_e = error_value;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int64_t d = predictions[i] - scaled;
-        const uint32_t err = static_cast<uint32_t>(((d < 0 ? -d : d) + 3) >> 3);
-        r.pe[c][i][s][y] = err;
-        if (y && x + 1 < gw) r.pe[c][i][(x + 1) & 7][up] += err;
-        if (!y) r.row0[c][i][s] = err;
+        r.pe[c][i][s][y] = sub[i];
+        if (y && x + 1 < gw) r.pe[c][i][(x + 1) & 7][up] += sub[i];
+        if (!y) r.row0[c][i][s] = sub[i];
       }
     }
     __syncthreads();
