@@ -213,59 +213,85 @@ __device__ __forceinline__ void ConvolveWindow(const float (&v)[kOut + 2 * R], c
   }
 }
 
-// Row blur: one CTA per 1024-sample segment of one row. The segment and its
-// R-sample halo are loaded into shared memory with coalesced loads; each
+// Row blur: one CTA per 1024-sample segment of kBlurRows consecutive rows.
+// The segments and their R-sample halos are loaded with coalesced loads, all
+// rows' loads in flight at once (more bytes in flight per SM than one row per
+// CTA gives), into shared rows whose pitch is a multiple of 4 floats. Each
 // thread then reads the window of its 4 outputs with 128-bit (and, for odd
 // R, one 64-bit) shared loads. Outputs within R of the row ends use
 // ConvolveLine's renormalized border sum.
 constexpr int kRowRun = 4;
 constexpr int kRowSegment = kThreads * kRowRun;
+constexpr int kBlurRows = 2;
 
 template <int R>
 __global__ void __launch_bounds__(kThreads)
 BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_t out_pitch,
                const __grid_constant__ Kernel17 k) {
   constexpr int kWindow = kRowRun + 2 * R;
-  __shared__ __align__(16) float segment[kRowSegment + 2 * R + 4];
+  constexpr int kSpan = kRowSegment + 2 * R;
+  constexpr int kLoads = (kSpan + kThreads - 1) / kThreads;
+  constexpr int kPitch = (kSpan + 4 + 3) / 4 * 4;  // 16-byte aligned rows
+  __shared__ __align__(16) float segment[kBlurRows][kPitch];
   const int plane = blockIdx.z;
   const int x0 = blockIdx.x * kRowSegment;
-  // Rows beyond the grid's y extent (65535) are taken in further rounds.
-  for (int y = blockIdx.y; y < h; y += gridDim.y) {
-  const float* row = in + plane * in_pitch + static_cast<size_t>(y) * w;
-  __syncthreads();
-  // segment[j] holds sample x0 - R + j.
-  for (int j = threadIdx.x; j < kRowSegment + 2 * R; j += kThreads) {
-    const int x = x0 - R + j;
-    segment[j] = x >= 0 && x < w ? row[x] : 0.0f;
-  }
-  __syncthreads();
-  const int first = x0 + threadIdx.x * kRowRun;
-  if (first >= w) continue;
-  float* dst = out + plane * out_pitch + static_cast<size_t>(y) * w + first;
-  if (first >= R && first + kRowRun - 1 < w - R) {
-    float v[kWindow];
-    const float* s = segment + threadIdx.x * kRowRun;
+  const float* base = in + plane * in_pitch;
+  // Rows beyond the grid's y extent (65535 row groups) are taken in further
+  // rounds.
+  for (int y0 = blockIdx.y * kBlurRows; y0 < h; y0 += gridDim.y * kBlurRows) {
+    __syncthreads();
+    // segment[r][j] holds sample x0 - R + j of row y0 + r.
+    float staged[kBlurRows][kLoads];
 #pragma unroll
-    for (int j = 0; j + 4 <= kWindow; j += 4) {
-      const float4 f = *reinterpret_cast<const float4*>(s + j);
-      v[j] = f.x;
-      v[j + 1] = f.y;
-      v[j + 2] = f.z;
-      v[j + 3] = f.w;
-    }
-    if constexpr (kWindow % 4 == 2) {
-      const float2 f = *reinterpret_cast<const float2*>(s + kWindow - 2);
-      v[kWindow - 2] = f.x;
-      v[kWindow - 1] = f.y;
-    }
-    float r[kRowRun];
-    ConvolveWindow<R, kRowRun>(v, k, r);
+    for (int r = 0; r < kBlurRows; ++r) {
+      const float* row = base + static_cast<size_t>(min(y0 + r, h - 1)) * w;
 #pragma unroll
-    for (int o = 0; o < kRowRun; ++o) dst[o] = r[o];
-    continue;
-  }
-  const int count = min(kRowRun, w - first);
-  for (int o = 0; o < count; ++o) dst[o] = ConvolveLine<R>(row, 1, first + o, w, k);
+      for (int q = 0; q < kLoads; ++q) {
+        const int j = threadIdx.x + q * kThreads, x = x0 - R + j;
+        staged[r][q] = j < kSpan && x >= 0 && x < w ? row[x] : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kBlurRows; ++r) {
+#pragma unroll
+      for (int q = 0; q < kLoads; ++q) {
+        const int j = threadIdx.x + q * kThreads;
+        if (j < kSpan) segment[r][j] = staged[r][q];
+      }
+    }
+    __syncthreads();
+    const int first = x0 + threadIdx.x * kRowRun;
+    if (first >= w) continue;
+#pragma unroll 1
+    for (int r = 0; r < kBlurRows && y0 + r < h; ++r) {
+      const int y = y0 + r;
+      float* dst = out + plane * out_pitch + static_cast<size_t>(y) * w + first;
+      if (first >= R && first + kRowRun - 1 < w - R) {
+        float v[kWindow];
+        const float* s = segment[r] + threadIdx.x * kRowRun;
+#pragma unroll
+        for (int j = 0; j + 4 <= kWindow; j += 4) {
+          const float4 f = *reinterpret_cast<const float4*>(s + j);
+          v[j] = f.x;
+          v[j + 1] = f.y;
+          v[j + 2] = f.z;
+          v[j + 3] = f.w;
+        }
+        if constexpr (kWindow % 4 == 2) {
+          const float2 f = *reinterpret_cast<const float2*>(s + kWindow - 2);
+          v[kWindow - 2] = f.x;
+          v[kWindow - 1] = f.y;
+        }
+        float o4[kRowRun];
+        ConvolveWindow<R, kRowRun>(v, k, o4);
+#pragma unroll
+        for (int o = 0; o < kRowRun; ++o) dst[o] = o4[o];
+        continue;
+      }
+      const float* row = base + static_cast<size_t>(y) * w;
+      const int count = min(kRowRun, w - first);
+      for (int o = 0; o < count; ++o) dst[o] = ConvolveLine<R>(row, 1, first + o, w, k);
+    }
   }
 }
 
@@ -942,8 +968,9 @@ template <int R>
 void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pitch, int planes,
                 const Kernel17& k, cudaStream_t stream) {
   const size_t column_runs = static_cast<size_t>(w) * ((h + kRun - 1) / kRun);
-  BlurRowsKernel<R><<<dim3((w + kRowSegment - 1) / kRowSegment, std::min(h, 65535), planes),
-                      kThreads, 0, stream>>>(in, tmp, w, h, pitch, pitch, k);
+  const int row_groups = std::min((h + kBlurRows - 1) / kBlurRows, 65535);
+  BlurRowsKernel<R><<<dim3((w + kRowSegment - 1) / kRowSegment, row_groups, planes), kThreads, 0,
+                      stream>>>(in, tmp, w, h, pitch, pitch, k);
   BlurColumnsKernel<R><<<dim3(Blocks(column_runs), planes), kThreads, 0, stream>>>(
     tmp, out, w, h, pitch, pitch, k);
 }
