@@ -402,12 +402,16 @@ __global__ void __launch_bounds__(kThreads)
 FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch, uint32_t* error) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
-  float lf[3];
+  // All loads first: `psycho` is read and written, so loads after a store
+  // could not be moved ahead of it.
+  float lf[3], v[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     lf[c] = psycho[(kLF + c) * pitch + i];
-    psycho[(kMF + c) * pitch + i] = xyb[c * pitch + i] - lf[c];
+    v[c] = xyb[c * pitch + i];
   }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) psycho[(kMF + c) * pitch + i] = v[c] - lf[c];
   const float l2 = (-0.362267051518f * lf[1] + lf[2]) * 49.87984651440f;
   const float l0 = lf[0] * 33.832837186260f;
   const float l1 = lf[1] * 14.458268100570f;
@@ -670,21 +674,44 @@ struct L2Params {
   float mask_multiplier, mask_bias, mask_sqrt_bias;
 };
 
-__device__ __forceinline__ float MaskActivity(const float* psycho, size_t pitch, int i) {
-  const float xdiff = (psycho[(kUHF + 0) * pitch + i] + psycho[(kHF + 0) * pitch + i]) * 2.5f;
-  const float ydiff = psycho[(kUHF + 1) * pitch + i] * 0.4f + psycho[(kHF + 1) * pitch + i] * 0.4f;
+// CombineChannelsForMasking of one position from its HF and UHF values.
+__device__ __forceinline__ float MaskActivity(float uhf0, float hf0, float uhf1, float hf1) {
+  const float xdiff = (uhf0 + hf0) * 2.5f;
+  const float ydiff = uhf1 * 0.4f + hf1 * 0.4f;
   return sqrtf(xdiff * xdiff + ydiff * ydiff);
 }
 
 // L2 terms (L2DiffAsymmetric, L2Diff, SetL2Diff) and the masking inputs
-// (CombineChannelsForMasking + DiffPrecompute) in the reference's order.
+// (CombineChannelsForMasking + DiffPrecompute) in the reference's order. All
+// of a thread's loads are issued before its first store (the output planes
+// are written through other pointers, which the compiler cannot tell apart
+// from the inputs).
 __global__ void __launch_bounds__(kThreads) L2MaskKernel(const __grid_constant__ L2Params p) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= p.n) return;
+  const size_t pitch = p.pitch;
+  float ac_in[2], hf_ref[2], hf_dist[2], uhf_ref[2], uhf_dist[2];
+  float mf_ref[3], mf_dist[3], lf_ref[3], lf_dist[3];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    ac_in[c] = p.ac[c * pitch + i];
+    hf_ref[c] = p.ref[(kHF + c) * pitch + i];
+    hf_dist[c] = p.dist[(kHF + c) * pitch + i];
+    uhf_dist[c] = p.dist[(kUHF + c) * pitch + i];
+    uhf_ref[c] = p.pre0 != nullptr ? p.ref[(kUHF + c) * pitch + i] : 0.0f;
+  }
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
-    float acc = c < 2 ? p.ac[c * p.pitch + i] : 0.0f;
+    mf_ref[c] = p.ref[(kMF + c) * pitch + i];
+    mf_dist[c] = p.dist[(kMF + c) * pitch + i];
+    lf_ref[c] = p.ref[(kLF + c) * pitch + i];
+    lf_dist[c] = p.dist[(kLF + c) * pitch + i];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float acc = c < 2 ? ac_in[c] : 0.0f;
     if (c < 2) {
-      const float v0 = p.ref[(kHF + c) * p.pitch + i], v1 = p.dist[(kHF + c) * p.pitch + i];
+      const float v0 = hf_ref[c], v1 = hf_dist[c];
       const float primary = p.asym_gt[c] * 0.8f;
       const float secondary_weight = p.asym_lt[c] * 0.8f;
       const float d = v0 - v1;
@@ -706,17 +733,17 @@ __global__ void __launch_bounds__(kThreads) L2MaskKernel(const __grid_constant__
       acc = secondary_weight * (secondary * secondary) + total;
     }
     {
-      const float d = p.ref[(kMF + c) * p.pitch + i] - p.dist[(kMF + c) * p.pitch + i];
+      const float d = mf_ref[c] - mf_dist[c];
       acc = (d * d) * p.mf_weight[c] + acc;
     }
-    p.ac[c * p.pitch + i] = acc;
-    const float d = p.ref[(kLF + c) * p.pitch + i] - p.dist[(kLF + c) * p.pitch + i];
-    p.dc[c * p.pitch + i] = d * d * p.lf_weight[c];
+    p.ac[c * pitch + i] = acc;
+    const float d = lf_ref[c] - lf_dist[c];
+    p.dc[c * pitch + i] = d * d * p.lf_weight[c];
   }
-  const float m1 = MaskActivity(p.dist, p.pitch, i);
+  const float m1 = MaskActivity(uhf_dist[0], hf_dist[0], uhf_dist[1], hf_dist[1]);
   p.pre1[i] = sqrtf(p.mask_multiplier * fabsf(m1) + p.mask_bias) - p.mask_sqrt_bias;
   if (p.pre0 != nullptr) {
-    const float m0 = MaskActivity(p.ref, p.pitch, i);
+    const float m0 = MaskActivity(uhf_ref[0], hf_ref[0], uhf_ref[1], hf_ref[1]);
     p.pre0[i] = sqrtf(p.mask_multiplier * fabsf(m0) + p.mask_bias) - p.mask_sqrt_bias;
   }
 }
