@@ -537,19 +537,33 @@ __device__ __forceinline__ void ChromaThresholds(int covered, float t[4]) {
   }
 }
 
-// AdjustQuantForChannel (quantization.cpp:285-480) for one channel; runs on
-// one thread over the coefficients in storage order.
+// AdjustQuantForChannel (quantization.cpp:285-480) for one channel, in two
+// parts: the sums over the coefficients, and the decisions taken from them.
+struct AdjustSums {
+  float border_sum, error_sum, value_sum;
+  float nonzeros[4], max_error[4];
+};
+
+// Initial thresholds of a channel: the reference's defaults, lowered for
+// multi-block transforms.
 template <int W, int H>
-__device__ void AdjustQuantForChannel(const AqQuantizer& q, int channel, float mm, int strategy,
-                                      const float* coef, const float* inv, float thresholds[4],
-                                      int* raw_quant) {
+__device__ __forceinline__ void AdjustThresholds(float thresholds[4]) {
   using S = TransformShape<W, H>;
-  const int xsize = S::SW / 8, ysize = S::SH / 8;
-  const float qac = q.scale * static_cast<float>(*raw_quant);
+  constexpr int xsize = S::SW / 8, ysize = S::SH / 8;
+  thresholds[0] = 0.58f;
+  thresholds[1] = thresholds[2] = thresholds[3] = 0.64f;
   if (xsize > 1 || ysize > 1) {
     const float reduction = fminf(fmaxf(0.003f * static_cast<float>(xsize * ysize), 0.0f), 0.08f);
     for (int i = 0; i < 4; ++i) thresholds[i] = fmaxf(0.54f, thresholds[i] - reduction);
   }
+}
+
+// The sums, on one thread over the coefficients in storage order.
+template <int W, int H>
+__device__ void AdjustSumsSerial(float qac, int channel, float mm, const float* coef,
+                                 const float* inv, const float thresholds[4], AdjustSums* out) {
+  using S = TransformShape<W, H>;
+  const int xsize = S::SW / 8, ysize = S::SH / 8;
   float border_sum = 0.0f, error_sum = 0.0f, value_sum = 0.0f;
   float nonzeros[4] = {0, 0, 0, 0}, max_error[4] = {0, 0, 0, 0};
   for (int y = 0; y < S::SH; ++y) {
@@ -571,6 +585,27 @@ __device__ void AdjustQuantForChannel(const AqQuantizer& q, int channel, float m
         if (in_corner || (on_border && in_larger_corner)) border_sum += fabsf(value);
       }
     }
+  }
+  out->border_sum = border_sum;
+  out->error_sum = error_sum;
+  out->value_sum = value_sum;
+  for (int i = 0; i < 4; ++i) {
+    out->nonzeros[i] = nonzeros[i];
+    out->max_error[i] = max_error[i];
+  }
+}
+
+// The decisions: raw quant and thresholds from the sums.
+template <int W, int H>
+__device__ void AdjustFinish(int channel, int strategy, const AdjustSums& sums,
+                             float thresholds[4], int* raw_quant) {
+  using S = TransformShape<W, H>;
+  const int xsize = S::SW / 8, ysize = S::SH / 8;
+  float border_sum = sums.border_sum, error_sum = sums.error_sum, value_sum = sums.value_sum;
+  float nonzeros[4], max_error[4];
+  for (int i = 0; i < 4; ++i) {
+    nonzeros[i] = sums.nonzeros[i];
+    max_error[i] = sums.max_error[i];
   }
   if (channel == 1 && value_sum * 8.0f < static_cast<float>(xsize * ysize)) {
     const double kLimit = 0.46, kMultiplier = 0.9999;
@@ -744,6 +779,11 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
   __shared__ float inverse_dequant[3][N];
   __shared__ float thresholds[3][4];
   __shared__ int candidates[3];
+  __shared__ float adjust_err[3][N];   // per coefficient |value - quantized|, 0 on the LLF
+  __shared__ uint32_t adjust_sum[2][3][5];  // per warp and channel: sum |q|, per quadrant
+  __shared__ uint32_t adjust_max[2][4];     // per warp: Y max error per quadrant (float bits)
+  __shared__ int adjust_big[2];             // per warp: a |q| sum reached 2^24
+  static_assert(kT == 64, "two warps");
   const uint32_t anchor_index = blockIdx.x;
   if (anchor_index >= *p.count) return;
   const int2 a = p.anchors[anchor_index];
@@ -758,14 +798,113 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
   const AqQuantizer q = *p.q;
   const int anchor_block = a.y * p.blocks_x + a.x;
   const int initial_raw = p.raw[anchor_block];
-  // SelectAdjustedAcQuantization: the three channels in parallel.
+  // SelectAdjustedAcQuantization, the sums in parallel: every thread takes
+  // coefficients of all three channels, storing each error term for the
+  // ordered error sum and adding |quantized| into integer sums. Those sums are
+  // the reference's float sums exactly while they stay below 2^24 (every
+  // partial sum is then an integer the float holds exactly); past that, the
+  // channel threads redo the sums serially.
+  using Sh = TransformShape<W, H>;
+  constexpr int xsize = Sh::SW / 8, ysize = Sh::SH / 8;
+  const float qac = q.scale * static_cast<float>(initial_raw);
+  float t0[4];
+  AdjustThresholds<W, H>(t0);
+  {
+    uint32_t sums[3][5];
+    uint32_t max_bits[4] = {0, 0, 0, 0};
+    bool big = false;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float mm = p.matrix_multiplier[c];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) sums[c][k] = 0;
+      for (int index = tid; index < N; index += kT) {
+        const int y = index / Sh::SW, x = index % Sh::SW;
+        if (x < xsize && y < ysize) {
+          adjust_err[c][index] = 0.0f;
+          continue;
+        }
+        const int quadrant = (y >= Sh::SH / 2) * 2 + (x >= Sh::SW / 2);
+        const float value = coef[c][index] * (inverse_dequant[c][index] * qac * mm);
+        const float quantized = fabsf(value) < t0[quadrant] ? 0.0f : rintf(value);
+        const float err = fabsf(value - quantized);
+        adjust_err[c][index] = err;
+        const float magnitude = fabsf(quantized);
+        if (magnitude < 16777216.0f) {
+          const uint32_t m = static_cast<uint32_t>(magnitude);
+          sums[c][0] += m;
+          sums[c][1 + quadrant] += m;
+        } else {
+          big = true;
+        }
+        if (c == 1 && quantized == 0.0f) {
+          // Non-negative floats order like their bit patterns; NaN errors are
+          // skipped, as fmaxf skips them.
+          if (err == err) max_bits[quadrant] = max(max_bits[quadrant], __float_as_uint(err));
+        }
+      }
+      if (sums[c][0] >= (1u << 24)) big = true;
+    }
+    const int warp = tid / 32, lane = tid % 32;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const uint32_t total = __reduce_add_sync(0xffffffffu, big ? 0u : sums[c][k]);
+        if (lane == 0) adjust_sum[warp][c][k] = total;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t m = __reduce_max_sync(0xffffffffu, max_bits[k]);
+      if (lane == 0) adjust_max[warp][k] = m;
+    }
+    const bool any_big = __any_sync(0xffffffffu, big);
+    if (lane == 0) adjust_big[warp] = any_big ? 1 : 0;
+  }
+  __syncthreads();
   if (tid < 3) {
-    float t[4] = {0.58f, 0.64f, 0.64f, 0.64f};
+    const int c = tid;
+    float t[4] = {t0[0], t0[1], t0[2], t0[3]};
     int candidate = initial_raw;
-    AdjustQuantForChannel<W, H>(q, tid, p.matrix_multiplier[tid], strategy, coef[tid],
-                                inverse_dequant[tid], t, &candidate);
-    for (int i = 0; i < 4; ++i) thresholds[tid][i] = t[i];
-    candidates[tid] = candidate;
+    AdjustSums sums;
+    const uint32_t total = adjust_sum[0][c][0] + adjust_sum[1][c][0];
+    if (adjust_big[0] | adjust_big[1] || total >= (1u << 24)) {
+      AdjustSumsSerial<W, H>(qac, c, p.matrix_multiplier[c], coef[c], inverse_dequant[c], t,
+                             &sums);
+    } else {
+      // The ordered sums: error terms in storage order (+0.0 on the LLF
+      // leaves the never -0.0 sum unchanged), and the border terms, which
+      // all lie in the larger corner, in storage order.
+      float error_sum = 0.0f;
+#pragma unroll 8
+      for (int index = 0; index < N; ++index) error_sum += adjust_err[c][index];
+      float border_sum = 0.0f;
+      const float mm = p.matrix_multiplier[c];
+      for (int y = 4 * ysize; y < Sh::SH; ++y) {
+        for (int x = 4 * xsize; x < Sh::SW; ++x) {
+          const bool in_corner = y >= 7 * ysize && x >= 7 * xsize;
+          const bool on_border = y + 1 == Sh::SH || x + 1 == Sh::SW;
+          if (!(in_corner || on_border)) continue;
+          const int index = y * Sh::SW + x;
+          const int quadrant = (y >= Sh::SH / 2) * 2 + (x >= Sh::SW / 2);
+          const float value = coef[c][index] * (inverse_dequant[c][index] * qac * mm);
+          const float quantized = fabsf(value) < t[quadrant] ? 0.0f : rintf(value);
+          if (quantized != 0.0f) border_sum += fabsf(value);
+        }
+      }
+      sums.error_sum = error_sum;
+      sums.border_sum = border_sum;
+      sums.value_sum = static_cast<float>(total);
+      for (int k = 0; k < 4; ++k) {
+        sums.nonzeros[k] = static_cast<float>(adjust_sum[0][c][1 + k] + adjust_sum[1][c][1 + k]);
+        sums.max_error[k] =
+          c == 1 ? __uint_as_float(max(adjust_max[0][k], adjust_max[1][k])) : 0.0f;
+      }
+    }
+    AdjustFinish<W, H>(c, strategy, sums, t, &candidate);
+    for (int i = 0; i < 4; ++i) thresholds[c][i] = t[i];
+    candidates[c] = candidate;
   } else if (tid == 32) {
     // Y DC from the unquantized Y coefficients.
     float dc[16];
