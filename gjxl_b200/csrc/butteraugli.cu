@@ -396,6 +396,39 @@ __device__ __forceinline__ float MaximumClamp(float v, float m) {
   return v;
 }
 
+// Constants of one MaltaDiffMap stage: float casts of pre * norm (for
+// differences above and below the reference) and of the norm.
+struct MaltaScale {
+  float norm2_gt, norm2_lt, norm;
+};
+
+// Scaled difference of MaltaDiffMap (butteraugli_distance_internal.cpp:544-575)
+// of the samples v0 (reference side) and v1 at one position.
+__device__ __forceinline__ float MaltaScaledValue(const MaltaScale& p, float v0, float v1) {
+  const float absolute = 0.5f * (fabsf(v0) + fabsf(v1));
+  const float difference = v0 - v1;
+  const float scaler = p.norm2_gt / (p.norm + absolute);
+  float scaled = scaler * difference;
+  const float scaler2 = p.norm2_lt / (p.norm + absolute);
+  const double magnitude = fabs(static_cast<double>(v0));
+  const double too_small = 0.55 * magnitude;
+  const double too_big = 1.05 * magnitude;
+  const double s2 = static_cast<double>(scaler2);
+  const double d1 = static_cast<double>(v1);
+  if (v0 < 0.0f) {
+    if (d1 > -too_small) {
+      scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 + too_small));
+    } else if (d1 < -too_big) {
+      scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (-d1 - too_big));
+    }
+  } else if (d1 < too_small) {
+    scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (too_small - d1));
+  } else if (d1 > too_big) {
+    scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 - too_big));
+  }
+  return scaled;
+}
+
 // After the 33-tap blur of all three XYB planes into psycho LF: MF = xyb - LF
 // and the LF scaling (butteraugli_internal.cpp:750-776).
 __global__ void __launch_bounds__(kThreads)
@@ -424,11 +457,27 @@ FrequencyLowKernel(const float* xyb, float* psycho, int n, size_t pitch, uint32_
 // After the 15-tap blur of MF into `blurred` (3 planes): HF = MF - blurred
 // (X, Y), MF ranges, MF_B = blurred, then X suppression by Y
 // (butteraugli_internal.cpp:778-810).
+// The Malta stages' scaled differences of the distorted image against the
+// reference, written beside the final planes they are taken from (plane k of
+// `malta` for stage k: MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X), so that each
+// is computed once per pixel instead of once per Malta tile that reads it.
+struct MaltaPlanes {
+  const float* ref;  // reference psycho planes; null: the reference itself
+  float* malta;      // 6 planes
+  MaltaScale scale[6];
+};
+
 __global__ void __launch_bounds__(kThreads)
-FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch, uint32_t* error) {
+FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch, uint32_t* error,
+                    const __grid_constant__ MaltaPlanes m) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
   const float mv0 = blurred[i], mv1 = blurred[pitch + i], mf_b = blurred[2 * pitch + i];
+  float ref_mf0 = 0.0f, ref_mf1 = 0.0f;
+  if (m.ref != nullptr) {
+    ref_mf0 = m.ref[(kMF + 0) * pitch + i];
+    ref_mf1 = m.ref[(kMF + 1) * pitch + i];
+  }
   const float hf0 = psycho[(kMF + 0) * pitch + i] - mv0;
   const float hf1 = psycho[(kMF + 1) * pitch + i] - mv1;
   const float mf0 = RemoveRangeAroundZero(mv0, 0.29f);
@@ -441,6 +490,10 @@ FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch, ui
     kSuppress / (hf1 * hf1 + kSuppress) * (1.0f - kMinimumScale) + kMinimumScale;
   psycho[(kHF + 0) * pitch + i] = scaler * hf0;
   psycho[(kHF + 1) * pitch + i] = hf1;
+  if (m.ref != nullptr) {
+    m.malta[0 * pitch + i] = MaltaScaledValue(m.scale[0], ref_mf1, mf1);
+    m.malta[1 * pitch + i] = MaltaScaledValue(m.scale[1], ref_mf0, mf0);
+  }
   // Finiteness of the final MF planes (the HF planes are rewritten, and
   // checked, by FrequencyUltraKernel).
   if (!(IsFinite(mf0) & IsFinite(mf1) & IsFinite(mf_b))) RaiseError(error, kErrorNonFiniteOutput);
@@ -450,9 +503,16 @@ FrequencyHighKernel(const float* blurred, float* psycho, int n, size_t pitch, ui
 // (butteraugli_internal.cpp:812-849).
 __global__ void __launch_bounds__(kThreads)
 FrequencyUltraKernel(const float* blurred, float* psycho, int n, size_t pitch,
-                     uint32_t* error) {
+                     uint32_t* error, const __grid_constant__ MaltaPlanes m) {
   const int i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
+  float ref_hf0 = 0.0f, ref_hf1 = 0.0f, ref_uhf0 = 0.0f, ref_uhf1 = 0.0f;
+  if (m.ref != nullptr) {
+    ref_hf0 = m.ref[(kHF + 0) * pitch + i];
+    ref_hf1 = m.ref[(kHF + 1) * pitch + i];
+    ref_uhf0 = m.ref[(kUHF + 0) * pitch + i];
+    ref_uhf1 = m.ref[(kUHF + 1) * pitch + i];
+  }
   const float hv0 = blurred[i];
   const float ultra0 = psycho[(kHF + 0) * pitch + i];
   const float uhf0 = RemoveRangeAroundZero(ultra0 - hv0, 0.04f);
@@ -466,6 +526,12 @@ FrequencyUltraKernel(const float* blurred, float* psycho, int n, size_t pitch,
   psycho[(kHF + 0) * pitch + i] = hf0;
   psycho[(kUHF + 1) * pitch + i] = uhf1;
   psycho[(kHF + 1) * pitch + i] = hf1;
+  if (m.ref != nullptr) {
+    m.malta[2 * pitch + i] = MaltaScaledValue(m.scale[2], ref_hf1, hf1);
+    m.malta[3 * pitch + i] = MaltaScaledValue(m.scale[3], ref_hf0, hf0);
+    m.malta[4 * pitch + i] = MaltaScaledValue(m.scale[4], ref_uhf1, uhf1);
+    m.malta[5 * pitch + i] = MaltaScaledValue(m.scale[5], ref_uhf0, uhf0);
+  }
   // Finiteness of the final HF and UHF planes; FrequencyLowKernel and
   // FrequencyHighKernel check the final LF and MF planes as they write them.
   if (!(IsFinite(uhf0) && IsFinite(hf0) && IsFinite(uhf1) && IsFinite(hf1))) {
@@ -477,12 +543,9 @@ FrequencyUltraKernel(const float* blurred, float* psycho, int n, size_t pitch,
 // Difference stages.
 
 struct MaltaParams {
-  const float* image0;
-  const float* image1;
-  float* accumulate;  // block_diff_ac plane (+= stage value)
+  const float* scaled;  // the stage's scaled differences (MaltaPlanes)
+  float* accumulate;    // block_diff_ac plane (+= stage value)
   int w, h;
-  float norm2_gt, norm2_lt;  // float casts of pre * norm
-  float norm;                // static_cast<float>(norm)
 };
 
 __device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
@@ -498,37 +561,10 @@ __device__ __forceinline__ float Sum9(float a, float b, float c, float d, float 
   return (Sum4(a, b, c, d) + Sum4(e, f, g, h)) + i;
 }
 
-// Scaled difference of MaltaDiffMap (butteraugli_distance_internal.cpp:544-575)
-// of the samples v0 (reference side) and v1 at one position.
-__device__ __forceinline__ float MaltaScaledValue(const MaltaParams& p, float v0, float v1) {
-  const float absolute = 0.5f * (fabsf(v0) + fabsf(v1));
-  const float difference = v0 - v1;
-  const float scaler = p.norm2_gt / (p.norm + absolute);
-  float scaled = scaler * difference;
-  const float scaler2 = p.norm2_lt / (p.norm + absolute);
-  const double magnitude = fabs(static_cast<double>(v0));
-  const double too_small = 0.55 * magnitude;
-  const double too_big = 1.05 * magnitude;
-  const double s2 = static_cast<double>(scaler2);
-  const double d1 = static_cast<double>(v1);
-  if (v0 < 0.0f) {
-    if (d1 > -too_small) {
-      scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 + too_small));
-    } else if (d1 < -too_big) {
-      scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (-d1 - too_big));
-    }
-  } else if (d1 < too_small) {
-    scaled = static_cast<float>(static_cast<double>(scaled) + s2 * (too_small - d1));
-  } else if (d1 > too_big) {
-    scaled = static_cast<float>(static_cast<double>(scaled) - s2 * (d1 - too_big));
-  }
-  return scaled;
-}
-
 // Output tile of one CTA: 64 x 16 pixels, each of the 256 threads computing
 // kMaltaRun = 4 horizontally adjacent outputs. The scaled differences of the
 // tile plus a 4-pixel halo (zero outside the image) are staged in shared
-// memory; every thread then copies the 9 x 12 window its four outputs read
+// memory from the stage's precomputed plane; every thread then copies the 9 x 12 window its four outputs read
 // into registers with 128-bit loads, so each staged value is loaded once per
 // thread instead of once per tap.
 constexpr int kMaltaRun = 4;
@@ -612,26 +648,21 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
   __shared__ __align__(16) float tile[kMaltaSpanH][kMaltaSpanW];
   const int x0 = blockIdx.x * kMaltaTileW - kMaltaHalo;
   const int y0 = blockIdx.y * kMaltaTileH - kMaltaHalo;
-  // Staging: both planes' samples are loaded first (all in flight at once),
-  // then scaled.
+  // Staging: all of a thread's samples are loaded before the first store.
   constexpr int kStage = (kMaltaSpanW * kMaltaSpanH + kMaltaThreads - 1) / kMaltaThreads;
-  float v0[kStage], v1[kStage];
+  float staged[kStage];
 #pragma unroll
   for (int j = 0; j < kStage; ++j) {
     const int i = threadIdx.x + j * kMaltaThreads;
     const int ty = i / kMaltaSpanW, tx = i % kMaltaSpanW, x = x0 + tx, y = y0 + ty;
     const bool inside = i < kMaltaSpanW * kMaltaSpanH && x >= 0 && y >= 0 && x < p.w && y < p.h;
-    const size_t at = inside ? static_cast<size_t>(y) * p.w + x : 0;
-    v0[j] = inside ? p.image0[at] : 0.0f;
-    v1[j] = inside ? p.image1[at] : 0.0f;
+    staged[j] = inside ? p.scaled[static_cast<size_t>(y) * p.w + x] : 0.0f;
   }
 #pragma unroll
   for (int j = 0; j < kStage; ++j) {
     const int i = threadIdx.x + j * kMaltaThreads;
     if (i >= kMaltaSpanW * kMaltaSpanH) break;
-    const int ty = i / kMaltaSpanW, tx = i % kMaltaSpanW, x = x0 + tx, y = y0 + ty;
-    const bool inside = x >= 0 && y >= 0 && x < p.w && y < p.h;
-    tile[ty][tx] = inside ? MaltaScaledValue(p, v0[j], v1[j]) : 0.0f;
+    tile[i / kMaltaSpanW][i % kMaltaSpanW] = staged[j];
   }
   __syncthreads();
   const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
@@ -941,9 +972,12 @@ struct Scale {
   float* pre1 = nullptr;
   float* blurred1 = nullptr;
   float* final_map = nullptr;
+  float* malta = nullptr;        // 6 planes: Malta stage inputs (MaltaPlanes)
 };
 
-size_t ScaleFloats(size_t n) { return n * (10 + 10 + 1 + 1 + 3 + 3 + 3 + 3 + 3 + 3 + 1 + 1 + 1 + 1); }
+size_t ScaleFloats(size_t n) {
+  return n * (10 + 10 + 1 + 1 + 3 + 3 + 3 + 3 + 3 + 3 + 1 + 1 + 1 + 1 + 6);
+}
 
 void AssignScale(Scale& s, float* base) {
   float* p = base;
@@ -966,6 +1000,7 @@ void AssignScale(Scale& s, float* base) {
   s.pre1 = take(1);
   s.blurred1 = take(1);
   s.final_map = take(1);
+  s.malta = take(6);
 }
 
 }  // namespace
@@ -1002,10 +1037,44 @@ void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pi
     tmp, out, w, h, pitch, pitch, k);
 }
 
+// Constants of the six Malta stages (MaltaDiffMap calls of
+// butteraugli_distance_internal.cpp:659-674): MF_Y, MF_X, HF_Y, HF_X, UHF_Y,
+// UHF_X, with kMaltaWeights / kMaltaNorms (:24-31).
+void MaltaStageScales(float hf_asymmetry, MaltaScale out[6]) {
+  const float asym = hf_asymmetry;
+  const float sqrt_asym = std::sqrt(asym);
+  const double kMaltaWeights[6] = {37.0819870399, 8246.75321353, 18.7237414387,
+                                   6923.99476109, 1.10039032555, 173.5};
+  const double kMaltaNorms[6] = {130262059.556, 1009002.70582, 4498534.45232,
+                                 8051.15833247, 71.7800275169, 5.0};
+  const double up[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] * sqrt_asym,
+                        kMaltaWeights[3] * sqrt_asym, kMaltaWeights[4] * asym,
+                        kMaltaWeights[5] * asym};
+  const double down[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] / sqrt_asym,
+                          kMaltaWeights[3] / sqrt_asym, kMaltaWeights[4] / asym,
+                          kMaltaWeights[5] / asym};
+  for (int index = 0; index < 6; ++index) {
+    const bool lf = index < 4;
+    const double multiplier = lf ? 0.611612573796 : 0.39905817637;
+    const double kLength = 3.75;
+    const double pre_gt = multiplier * std::sqrt(0.5f * up[index]) / (kLength * 2.0 + 1.0);
+    const double pre_lt = multiplier * std::sqrt(0.33f * down[index]) / (kLength * 2.0 + 1.0);
+    out[index].norm2_gt = static_cast<float>(pre_gt * kMaltaNorms[index]);
+    out[index].norm2_lt = static_cast<float>(pre_lt * kMaltaNorms[index]);
+    out[index].norm = static_cast<float>(kMaltaNorms[index]);
+  }
+}
+
 // Opsin dynamics + frequency separation of one image at one scale
 // (OpsinDynamicsImage + SeparateFrequencies) into `psycho`.
+// For the distorted image (`ref_psycho` set: the reference's final planes)
+// the frequency kernels also write the Malta stage inputs into s.malta.
 void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, size_t pitch,
-            float* psycho, cudaStream_t stream) {
+            float* psycho, const float* ref_psycho, cudaStream_t stream) {
+  MaltaPlanes mp;
+  mp.ref = ref_psycho;
+  mp.malta = s.malta;
+  MaltaStageScales(st.hf_asymmetry, mp.scale);
   const size_t n = s.n;
   // Dense copy of the input planes for the mirrored 5-tap blur.
   const float* dense = linear;
@@ -1031,11 +1100,11 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
   // 15-tap blur of MF (3 planes) into blur3.
   BlurPlanes<7>(psycho + kMF * n, s.tmp, s.blur3, s.w, s.h, n, 3, st.k_high, stream);
   FrequencyHighKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n), n,
-                                                          st.error);
+                                                          st.error, mp);
   // 7-tap blur of HF (2 planes) into blur3.
   BlurPlanes<3>(psycho + kHF * n, s.tmp, s.blur3, s.w, s.h, n, 2, st.k_ultra, stream);
   FrequencyUltraKernel<<<Blocks(n), kThreads, 0, stream>>>(s.blur3, psycho, static_cast<int>(n),
-                                                           n, st.error);
+                                                           n, st.error, mp);
 }
 
 // Difference stages of one scale into s.final_map; with `reference_side`
@@ -1043,40 +1112,19 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
 void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream_t stream) {
   const size_t n = s.n;
   const float asym = st.hf_asymmetry;
-  const float sqrt_asym = std::sqrt(asym);
-  // kMaltaWeights / kMaltaNorms (butteraugli_distance_internal.cpp:24-31).
-  const double kMaltaWeights[6] = {37.0819870399, 8246.75321353, 18.7237414387,
-                                   6923.99476109, 1.10039032555, 173.5};
-  const double kMaltaNorms[6] = {130262059.556, 1009002.70582, 4498534.45232,
-                                 8051.15833247, 71.7800275169, 5.0};
-  const double up[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] * sqrt_asym,
-                        kMaltaWeights[3] * sqrt_asym, kMaltaWeights[4] * asym,
-                        kMaltaWeights[5] * asym};
-  const double down[6] = {kMaltaWeights[0], kMaltaWeights[1], kMaltaWeights[2] / sqrt_asym,
-                          kMaltaWeights[3] / sqrt_asym, kMaltaWeights[4] / asym,
-                          kMaltaWeights[5] / asym};
-  // Stage inputs: MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X.
-  const int plane_of[6] = {kMF + 1, kMF + 0, kHF + 1, kHF + 0, kUHF + 1, kUHF + 0};
+  // Stage inputs (computed beside the distorted image's final planes):
+  // MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X.
   cudaMemsetAsync(s.ac, 0, 3 * n * sizeof(float), stream);
   const int order[6] = {4, 5, 2, 3, 0, 1};
   dim3 tiles((s.w + kMaltaTileW - 1) / kMaltaTileW, (s.h + kMaltaTileH - 1) / kMaltaTileH);
   for (int index : order) {
     MaltaParams mp;
-    mp.image0 = s.ref_psycho + plane_of[index] * n;
-    mp.image1 = s.dist_psycho + plane_of[index] * n;
+    mp.scaled = s.malta + index * n;
     const int channel = index % 2 == 0 ? 1 : 0;
     mp.accumulate = s.ac + channel * n;
     mp.w = s.w;
     mp.h = s.h;
-    const bool lf = index < 4;
-    const double multiplier = lf ? 0.611612573796 : 0.39905817637;
-    const double kLength = 3.75;
-    const double pre_gt = multiplier * std::sqrt(0.5f * up[index]) / (kLength * 2.0 + 1.0);
-    const double pre_lt = multiplier * std::sqrt(0.33f * down[index]) / (kLength * 2.0 + 1.0);
-    mp.norm2_gt = static_cast<float>(pre_gt * kMaltaNorms[index]);
-    mp.norm2_lt = static_cast<float>(pre_lt * kMaltaNorms[index]);
-    mp.norm = static_cast<float>(kMaltaNorms[index]);
-    if (lf) {
+    if (index < 4) {
       MaltaKernel<true><<<tiles, kMaltaThreads, 0, stream>>>(mp);
     } else {
       MaltaKernel<false><<<tiles, kMaltaThreads, 0, stream>>>(mp);
@@ -1129,13 +1177,15 @@ void TransformScales(ButteraugliState& st, const float* linear, size_t stride, s
     main_pitch = st.main.n;
   }
   Psycho(st, st.main, main_in, main_stride, main_pitch,
-         reference ? st.main.ref_psycho : st.main.dist_psycho, stream);
+         reference ? st.main.ref_psycho : st.main.dist_psycho,
+         reference ? nullptr : st.main.ref_psycho, stream);
   if (st.has_sub) {
     Subsample2xKernel<<<dim3(Blocks(st.sub.n), 3), kThreads, 0, stream>>>(
       linear, stride, pitch, st.width, st.height, st.sub.linear_tmp, st.sub.w, st.sub.h,
       st.sub.n);
     Psycho(st, st.sub, st.sub.linear_tmp, st.sub.w, st.sub.n,
-           reference ? st.sub.ref_psycho : st.sub.dist_psycho, stream);
+           reference ? st.sub.ref_psycho : st.sub.dist_psycho,
+           reference ? nullptr : st.sub.ref_psycho, stream);
   }
 }
 
