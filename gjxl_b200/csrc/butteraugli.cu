@@ -648,21 +648,40 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
   __shared__ __align__(16) float tile[kMaltaSpanH][kMaltaSpanW];
   const int x0 = blockIdx.x * kMaltaTileW - kMaltaHalo;
   const int y0 = blockIdx.y * kMaltaTileH - kMaltaHalo;
-  // Staging: all of a thread's samples are loaded before the first store.
-  constexpr int kStage = (kMaltaSpanW * kMaltaSpanH + kMaltaThreads - 1) / kMaltaThreads;
-  float staged[kStage];
+  // Staging, four samples per load: x0 is a multiple of 4, so with the row
+  // length a multiple of 4 every aligned group of 4 lies wholly inside or
+  // wholly outside the image and is 16-byte aligned; other widths take
+  // scalar loads. All of a thread's loads are issued before its first store.
+  constexpr int kQuads = kMaltaSpanW / 4 * kMaltaSpanH;
+  constexpr int kStage = (kQuads + kMaltaThreads - 1) / kMaltaThreads;
+  static_assert(kMaltaSpanW % 4 == 0 && kMaltaHalo % 4 == 0, "aligned quads");
+  float4 staged[kStage];
+  const bool aligned = p.w % 4 == 0;
 #pragma unroll
   for (int j = 0; j < kStage; ++j) {
     const int i = threadIdx.x + j * kMaltaThreads;
-    const int ty = i / kMaltaSpanW, tx = i % kMaltaSpanW, x = x0 + tx, y = y0 + ty;
-    const bool inside = i < kMaltaSpanW * kMaltaSpanH && x >= 0 && y >= 0 && x < p.w && y < p.h;
-    staged[j] = inside ? p.scaled[static_cast<size_t>(y) * p.w + x] : 0.0f;
+    const int ty = i / (kMaltaSpanW / 4), tx = (i % (kMaltaSpanW / 4)) * 4;
+    const int x = x0 + tx, y = y0 + ty;
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (i < kQuads && y >= 0 && y < p.h) {
+      const float* row = p.scaled + static_cast<size_t>(y) * p.w;
+      if (aligned) {
+        if (x >= 0 && x < p.w) v = *reinterpret_cast<const float4*>(row + x);
+      } else {
+        v.x = x >= 0 && x < p.w ? row[x] : 0.0f;
+        v.y = x + 1 >= 0 && x + 1 < p.w ? row[x + 1] : 0.0f;
+        v.z = x + 2 >= 0 && x + 2 < p.w ? row[x + 2] : 0.0f;
+        v.w = x + 3 >= 0 && x + 3 < p.w ? row[x + 3] : 0.0f;
+      }
+    }
+    staged[j] = v;
   }
 #pragma unroll
   for (int j = 0; j < kStage; ++j) {
     const int i = threadIdx.x + j * kMaltaThreads;
-    if (i >= kMaltaSpanW * kMaltaSpanH) break;
-    tile[i / kMaltaSpanW][i % kMaltaSpanW] = staged[j];
+    if (i >= kQuads) break;
+    *reinterpret_cast<float4*>(&tile[i / (kMaltaSpanW / 4)][(i % (kMaltaSpanW / 4)) * 4]) =
+      staged[j];
   }
   __syncthreads();
   const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
