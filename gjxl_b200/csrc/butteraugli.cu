@@ -650,13 +650,15 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
   const int y0 = blockIdx.y * kMaltaTileH - kMaltaHalo;
   // Staging, four samples per load: x0 is a multiple of 4, so with the row
   // length a multiple of 4 every aligned group of 4 lies wholly inside or
-  // wholly outside the image and is 16-byte aligned; other widths take
-  // scalar loads. All of a thread's loads are issued before its first store.
+  // wholly outside the image, and with a 16-byte aligned plane it is 16-byte
+  // aligned; other planes take scalar loads (the half-scale planes follow the
+  // full-scale ones in the arena, so their alignment depends on the image
+  // size). All of a thread's loads are issued before its first store.
   constexpr int kQuads = kMaltaSpanW / 4 * kMaltaSpanH;
   constexpr int kStage = (kQuads + kMaltaThreads - 1) / kMaltaThreads;
   static_assert(kMaltaSpanW % 4 == 0 && kMaltaHalo % 4 == 0, "aligned quads");
   float4 staged[kStage];
-  const bool aligned = p.w % 4 == 0;
+  const bool aligned = p.w % 4 == 0 && reinterpret_cast<uintptr_t>(p.scaled) % 16 == 0;
 #pragma unroll
   for (int j = 0; j < kStage; ++j) {
     const int i = threadIdx.x + j * kMaltaThreads;
