@@ -223,22 +223,53 @@ __device__ __forceinline__ int MirrorR(int c, int n) {
   return phase < n ? phase : period - 1 - phase;
 }
 
-// Loop filters on a shared-memory tile: each CTA computes a kTileW x kTileH
-// output tile and first stages its input window (tile + halo, every
+// Loop filters on a shared-memory tile: each CTA of kTileW x kTileRows
+// threads computes a kTileW x kTileH output tile (each thread kTileH /
+// kTileRows rows) and first stages its input window (tile + halo, every
 // coordinate mirrored at the image border as the reference's filters read
 // it) for all three planes, so the filter taps read shared memory only.
-constexpr int kTileW = 32, kTileH = 8;
+constexpr int kTileW = 32, kTileH = 32, kTileRows = 8;
+constexpr int kRowsPerThread = kTileH / kTileRows;
 
+// The window is loaded with a 2D thread mapping (no index division), all of
+// a thread's loads issued before its first store; windows that lie inside
+// the image skip the mirroring.
 template <int Halo>
 __device__ __forceinline__ void StageWindow(const float* in, size_t stride, size_t pitch, int w,
                                             int h, int x0, int y0,
                                             float (*tile)[kTileH + 2 * Halo][kTileW + 2 * Halo]) {
   constexpr int TW = kTileW + 2 * Halo, TH = kTileH + 2 * Halo;
-  const int tid = threadIdx.y * kTileW + threadIdx.x;
-  for (int i = tid; i < 3 * TW * TH; i += kTileW * kTileH) {
-    const int c = i / (TW * TH), r = i % (TW * TH), ty = r / TW, tx = r % TW;
-    const int gy = MirrorR(y0 + ty - Halo, h), gx = MirrorR(x0 + tx - Halo, w);
-    tile[c][ty][tx] = in[c * pitch + static_cast<size_t>(gy) * stride + gx];
+  constexpr int kCols = (TW + kTileW - 1) / kTileW, kRows = (TH + kTileRows - 1) / kTileRows;
+  const bool interior = x0 >= Halo && y0 >= Halo && x0 + kTileW + Halo <= w &&
+                        y0 + kTileH + Halo <= h;
+  float v[3][kRows][kCols];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int ty = threadIdx.y + r * kTileRows, tx = threadIdx.x + k * kTileW;
+      if (ty < TH && tx < TW) {
+        int gy = y0 + ty - Halo, gx = x0 + tx - Halo;
+        if (!interior) {
+          gy = MirrorR(gy, h);
+          gx = MirrorR(gx, w);
+        }
+        const float* src = in + static_cast<size_t>(gy) * stride + gx;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c][r][k] = src[c * pitch];
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int ty = threadIdx.y + r * kTileRows, tx = threadIdx.x + k * kTileW;
+      if (ty < TH && tx < TW) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tile[c][ty][tx] = v[c][r][k];
+      }
+    }
   }
 }
 
@@ -251,24 +282,32 @@ struct GaborishParams {
   uint32_t* error;
 };
 
-__global__ void __launch_bounds__(kTileW * kTileH)
+__global__ void __launch_bounds__(kTileW * kTileRows)
 GaborishForwardKernel(const __grid_constant__ GaborishParams p) {
   __shared__ float tile[3][kTileH + 2][kTileW + 2];
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
   StageWindow<1>(p.in, p.in_stride, p.in_pitch, p.w, p.h, x0, y0, tile);
   __syncthreads();
-  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= p.w || y >= p.h) return;
-  const int tx = threadIdx.x + 1, ty = threadIdx.y + 1;
+  const int x = x0 + threadIdx.x;
+  if (x >= p.w) return;
+  const int tx = threadIdx.x + 1;
   const size_t n = static_cast<size_t>(p.w) * p.h;
-  for (int c = 0; c < 3; ++c) {
-    const auto& t = tile[c];
-    const float axes = (t[ty][tx - 1] + t[ty][tx + 1]) + (t[ty - 1][tx] + t[ty + 1][tx]);
-    const float diagonals =
-      (t[ty - 1][tx - 1] + t[ty - 1][tx + 1]) + (t[ty + 1][tx - 1] + t[ty + 1][tx + 1]);
-    const float value = p.weights[0] * t[ty][tx] + p.weights[1] * axes + p.weights[2] * diagonals;
-    if (!IsFinite(value)) RaiseError(p.error, kErrorNonFiniteOutput);
-    p.out[c * n + static_cast<size_t>(y) * p.w + x] = value;
+#pragma unroll
+  for (int row = 0; row < kRowsPerThread; ++row) {
+    const int oy = threadIdx.y + row * kTileRows, y = y0 + oy;
+    if (y >= p.h) break;
+    const int ty = oy + 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const auto& t = tile[c];
+      const float axes = (t[ty][tx - 1] + t[ty][tx + 1]) + (t[ty - 1][tx] + t[ty + 1][tx]);
+      const float diagonals =
+        (t[ty - 1][tx - 1] + t[ty - 1][tx + 1]) + (t[ty + 1][tx - 1] + t[ty + 1][tx + 1]);
+      const float value =
+        p.weights[0] * t[ty][tx] + p.weights[1] * axes + p.weights[2] * diagonals;
+      if (!IsFinite(value)) RaiseError(p.error, kErrorNonFiniteOutput);
+      p.out[c * n + static_cast<size_t>(y) * p.w + x] = value;
+    }
   }
 }
 
@@ -282,57 +321,90 @@ struct EpfParams {
 };
 
 // One EPF iteration (epf.cpp:92-160). Pass 1 compares 5-pixel plus-shaped
-// patches (halo 2); pass 2 compares single pixels (halo 1).
+// patches (halo 2); pass 2 compares single pixels (halo 1). For pass 1 the
+// absolute differences of horizontal and vertical neighbours are taken once
+// per window position: the patch distance for offset d at p adds
+// |t[p + k] - t[p + d + k]| over the patch in the reference's order, and that
+// term is the horizontal (vertical) difference at p + k for d = +1 and at
+// p - 1 + k for d = -1 (|a - b| = |b - a| exactly).
 template <int Pass>
-__global__ void __launch_bounds__(kTileW * kTileH) EpfKernel(const __grid_constant__ EpfParams p) {
+__global__ void __launch_bounds__(kTileW * kTileRows) EpfKernel(const __grid_constant__ EpfParams p) {
   constexpr int Halo = Pass == 1 ? 2 : 1;
-  __shared__ float tile[3][kTileH + 2 * Halo][kTileW + 2 * Halo];
+  constexpr int TW = kTileW + 2 * Halo, TH = kTileH + 2 * Halo;
+  __shared__ float tile[3][TH][TW];
+  // Pass 1: [0] horizontal |t[y][x] - t[y][x+1]|, [1] vertical |t[y][x] - t[y+1][x]|.
+  __shared__ float diff[Pass == 1 ? 2 : 1][Pass == 1 ? 3 : 1][Pass == 1 ? TH : 1]
+                       [Pass == 1 ? TW : 1];
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * kTileH;
   StageWindow<Halo>(p.in, p.w, static_cast<size_t>(p.w) * p.h, p.w, p.h, x0, y0, tile);
   __syncthreads();
-  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= p.w || y >= p.h) return;
-  const size_t n = static_cast<size_t>(p.w) * p.h;
-  const size_t i = static_cast<size_t>(y) * p.w + x;
-  const int tx = threadIdx.x + Halo, ty = threadIdx.y + Halo;
-  const float block_inverse_sigma = p.inverse_sigma[(y / 8) * p.blocks_x + x / 8];
-  const float kMinInverseSigma = -1.1715728752538099024f / 0.3f;
-  if (block_inverse_sigma < kMinInverseSigma) {
-    for (int c = 0; c < 3; ++c) p.out[c * n + i] = tile[c][ty][tx];
-    return;
-  }
-  const bool border = x % 8 == 0 || x % 8 == 7 || y % 8 == 0 || y % 8 == 7;
-  const float scaled = block_inverse_sigma * p.sigma_scale * (border ? 2.0f / 3.0f : 1.0f);
-  const float channel_scale[3] = {40.0f, 5.0f, 3.5f};
-  float sum[3] = {tile[0][ty][tx], tile[1][ty][tx], tile[2][ty][tx]};
-  float weight_sum = 1.0f;
-  const int offsets[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
-  const int plus[5][2] = {{0, 0}, {0, -1}, {-1, 0}, {0, 1}, {1, 0}};
+  if constexpr (Pass == 1) {
+    constexpr int kCols = (TW + kTileW - 1) / kTileW, kRows = (TH + kTileRows - 1) / kTileRows;
 #pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const int dx = offsets[o][0], dy = offsets[o][1];
-    float sad = 0.0f;
+    for (int r = 0; r < kRows; ++r) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const auto& t = tile[c];
-      if (Pass == 1) {
-        float channel_sad = 0.0f;
+      for (int k = 0; k < kCols; ++k) {
+        const int ty = threadIdx.y + r * kTileRows, tx = threadIdx.x + k * kTileW;
+        if (ty >= TH || tx >= TW) continue;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          channel_sad += fabsf(t[ty + plus[k][1]][tx + plus[k][0]] -
-                               t[ty + dy + plus[k][1]][tx + dx + plus[k][0]]);
+        for (int c = 0; c < 3; ++c) {
+          if (tx + 1 < TW) diff[0][c][ty][tx] = fabsf(tile[c][ty][tx] - tile[c][ty][tx + 1]);
+          if (ty + 1 < TH) diff[1][c][ty][tx] = fabsf(tile[c][ty][tx] - tile[c][ty + 1][tx]);
         }
-        sad = fmaf(channel_sad, channel_scale[c], sad);
-      } else {
-        sad = fmaf(fabsf(t[ty][tx] - t[ty + dy][tx + dx]), channel_scale[c], sad);
       }
     }
-    const float weight = fmaxf(0.0f, fmaf(sad, scaled, 1.0f));
-    weight_sum += weight;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, tile[c][ty + dy][tx + dx], sum[c]);
+    __syncthreads();
   }
-  for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
+  const int x = x0 + threadIdx.x;
+  if (x >= p.w) return;
+  const size_t n = static_cast<size_t>(p.w) * p.h;
+  const int tx = threadIdx.x + Halo;
+  const float kMinInverseSigma = -1.1715728752538099024f / 0.3f;
+  const float channel_scale[3] = {40.0f, 5.0f, 3.5f};
+  const int offsets[4][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}};
+  const int plus[5][2] = {{0, 0}, {0, -1}, {-1, 0}, {0, 1}, {1, 0}};
+#pragma unroll 1
+  for (int row = 0; row < kRowsPerThread; ++row) {
+    const int oy = threadIdx.y + row * kTileRows, y = y0 + oy;
+    if (y >= p.h) break;
+    const size_t i = static_cast<size_t>(y) * p.w + x;
+    const int ty = oy + Halo;
+    const float block_inverse_sigma = p.inverse_sigma[(y / 8) * p.blocks_x + x / 8];
+    if (block_inverse_sigma < kMinInverseSigma) {
+      for (int c = 0; c < 3; ++c) p.out[c * n + i] = tile[c][ty][tx];
+      continue;
+    }
+    const bool border = x % 8 == 0 || x % 8 == 7 || y % 8 == 0 || y % 8 == 7;
+    const float scaled = block_inverse_sigma * p.sigma_scale * (border ? 2.0f / 3.0f : 1.0f);
+    float sum[3] = {tile[0][ty][tx], tile[1][ty][tx], tile[2][ty][tx]};
+    float weight_sum = 1.0f;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const int dx = offsets[o][0], dy = offsets[o][1];
+      float sad = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if constexpr (Pass == 1) {
+          // Differences along the offset's axis, based at p (d = +1) or at
+          // p + d (d = -1).
+          const auto& d = diff[dy != 0 ? 1 : 0][c];
+          const int bx = tx + (dx < 0 ? dx : 0), by = ty + (dy < 0 ? dy : 0);
+          float channel_sad = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) channel_sad += d[by + plus[k][1]][bx + plus[k][0]];
+          sad = fmaf(channel_sad, channel_scale[c], sad);
+        } else {
+          const auto& t = tile[c];
+          sad = fmaf(fabsf(t[ty][tx] - t[ty + dy][tx + dx]), channel_scale[c], sad);
+        }
+      }
+      const float weight = fmaxf(0.0f, fmaf(sad, scaled, 1.0f));
+      weight_sum += weight;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, tile[c][ty + dy][tx + dx], sum[c]);
+    }
+    for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
+  }
 }
 
 struct LinearParams {
@@ -535,7 +607,7 @@ int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, s
   g.error = error;
   const dim3 tiles(static_cast<unsigned>((width + kTileW - 1) / kTileW),
                    static_cast<unsigned>((height + kTileH - 1) / kTileH));
-  const dim3 threads(kTileW, kTileH);
+  const dim3 threads(kTileW, kTileRows);
   GaborishForwardKernel<<<tiles, threads, 0, stream>>>(g);
   EpfParams e;
   e.w = static_cast<int>(width);
