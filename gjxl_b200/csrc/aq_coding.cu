@@ -783,21 +783,30 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
   __shared__ uint32_t adjust_sum[2][3][5];  // per warp and channel: sum |q|, per quadrant
   __shared__ uint32_t adjust_max[2][4];     // per warp: Y max error per quadrant (float bits)
   __shared__ int adjust_big[2];             // per warp: a |q| sum reached 2^24
+  __shared__ float dequant_y[N];            // the family's Y dequant weights
   static_assert(kT == 64, "two warps");
   const uint32_t anchor_index = blockIdx.x;
   if (anchor_index >= *p.count) return;
   const int2 a = p.anchors[anchor_index];
   const int tid = threadIdx.x;
+  // Every global value the CTA reads is requested here, before the first
+  // barrier (loads are not moved across barriers), so that one round trip
+  // covers them all.
+  const AqQuantizer q = *p.q;
+  const int anchor_block = a.y * p.blocks_x + a.x;
+  const int initial_raw = p.raw[anchor_block];
+  const float mm0 = p.matrix_multiplier[0], mm1 = p.matrix_multiplier[1],
+              mm2 = p.matrix_multiplier[2];
+  const int tile = (a.y / 8) * p.tiles_x + (a.x / 8);
+  const int8_t y_to_x = p.y_to_x[tile], y_to_b = p.y_to_b[tile];
   for (int i = tid; i < 3 * N; i += kT) {
     const int c = i / N, j = i % N;
     coef[c][j] = p.coef[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride +
                         a.x * 8 + j % W];
     inverse_dequant[c][j] = p.inverse_dequant[i];
+    if (c == 1) dequant_y[j] = p.dequant[N + j];
   }
   __syncthreads();
-  const AqQuantizer q = *p.q;
-  const int anchor_block = a.y * p.blocks_x + a.x;
-  const int initial_raw = p.raw[anchor_block];
   // SelectAdjustedAcQuantization, the sums in parallel: every thread takes
   // coefficients of all three channels, storing each error term for the
   // ordered error sum and adding |quantized| into integer sums. Those sums are
@@ -815,7 +824,7 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
     bool big = false;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float mm = p.matrix_multiplier[c];
+      const float mm = c == 0 ? mm0 : c == 1 ? mm1 : mm2;
 #pragma unroll
       for (int k = 0; k < 5; ++k) sums[c][k] = 0;
       for (int index = tid; index < N; index += kT) {
@@ -870,8 +879,8 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
     AdjustSums sums;
     const uint32_t total = adjust_sum[0][c][0] + adjust_sum[1][c][0];
     if (adjust_big[0] | adjust_big[1] || total >= (1u << 24)) {
-      AdjustSumsSerial<W, H>(qac, c, p.matrix_multiplier[c], coef[c], inverse_dequant[c], t,
-                             &sums);
+      AdjustSumsSerial<W, H>(qac, c, c == 0 ? mm0 : c == 1 ? mm1 : mm2, coef[c],
+                             inverse_dequant[c], t, &sums);
     } else {
       // The ordered sums: error terms in storage order (+0.0 on the LLF
       // leaves the never -0.0 sum unchanged), and the border terms, which
@@ -880,7 +889,7 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
 #pragma unroll 8
       for (int index = 0; index < N; ++index) error_sum += adjust_err[c][index];
       float border_sum = 0.0f;
-      const float mm = p.matrix_multiplier[c];
+      const float mm = c == 0 ? mm0 : c == 1 ? mm1 : mm2;
       for (int y = 4 * ysize; y < Sh::SH; ++y) {
         for (int x = 4 * xsize; x < Sh::SW; ++x) {
           const bool in_corner = y >= 7 * ysize && x >= 7 * xsize;
@@ -928,13 +937,12 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
     const int32_t quantized =
       fabsf(value) < thresholds[1][ti] ? 0 : static_cast<int32_t>(rintf(value));
     p.qac[p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] = quantized;
-    coef[1][j] = QuantBias(quantized, 1) * (p.dequant[N + j] * y_dequant_scale);
+    coef[1][j] = QuantBias(quantized, 1) * (dequant_y[j] * y_dequant_scale);
   }
   __syncthreads();
   // Remove the Y prediction from X and B.
-  const int tile = (a.y / 8) * p.tiles_x + (a.x / 8);
-  const float f0 = static_cast<float>(p.y_to_x[tile]) / 84.0f;
-  const float f2 = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
+  const float f0 = static_cast<float>(y_to_x) / 84.0f;
+  const float f2 = 1.0f + static_cast<float>(y_to_b) / 84.0f;
   for (int j = tid; j < N; j += kT) {
     coef[0][j] -= f0 * coef[1][j];
     coef[2][j] -= f2 * coef[1][j];
@@ -955,7 +963,7 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
     const int c = i < N ? 0 : 2, j = i % N;
     const int x = j % S::SW, y = j / S::SW;
     const int ti = (y >= S::SH / 2) * 2 + (x >= S::SW / 2);
-    const float qs = q.scale * static_cast<float>(raw) * p.matrix_multiplier[c];
+    const float qs = q.scale * static_cast<float>(raw) * (c == 0 ? mm0 : mm2);
     const float value = inverse_dequant[c][j] * qs * coef[c][j];
     const int32_t quantized = fabsf(value) < t[ti] ? 0 : static_cast<int32_t>(rintf(value));
     p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 + j % W] =

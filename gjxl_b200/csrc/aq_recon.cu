@@ -120,6 +120,7 @@ struct ReconParams {
   const float* dequant;  // family table [3][N]
   const float* matrix_multiplier;  // device, X / Y / B
   float* recon;
+  uint32_t capacity;  // entries of the family's anchor list
 };
 
 // K = 1024 / N transforms (3 channels each) per CTA of 384 threads; the
@@ -136,16 +137,47 @@ __global__ void __launch_bounds__(kReconThreads, 2) ReconstructKernel(const __gr
   extern __shared__ __align__(16) unsigned char smem[];
   double* tmp = reinterpret_cast<double*>(smem);                  // [KC] padded planes
   float* coef = reinterpret_cast<float*>(tmp + Batch::Elements);  // [KC] padded planes
+  using S = TransformShape<W, H>;
   __shared__ int2 anchor[K];
   __shared__ float scales[K][3];
   __shared__ float factors[K][2];
+  __shared__ float dc_values[K][3][S::CW * S::CH];  // the transforms' DC blocks
   const uint32_t first = blockIdx.x * K;
+  // The anchor loads do not wait for the count: the list index is clamped to
+  // the list, and anchors past the count are never used. Every later global
+  // load depends only on the anchors, so the CTA waits for two round trips.
+  constexpr int kPerThread = KC * N / kReconThreads;
+  const auto anchor_at = [&](int k) {
+    return p.anchors[min(first + static_cast<uint32_t>(k), p.capacity - 1)];
+  };
+  int2 item_anchor[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    item_anchor[q] = anchor_at((threadIdx.x + q * kReconThreads) / (3 * N));
+  }
+  const int2 own_anchor = anchor_at(threadIdx.x < K ? threadIdx.x : 0);
+  const int2 dc_anchor = anchor_at(threadIdx.x < 3 * K ? threadIdx.x / 3 : 0);
   const uint32_t n = *p.count;
   if (first >= n) return;
   const int active = min(K, static_cast<int>(n - first));
+  // Dequantize coefficient j = coefficient_index(v, u) (footprint (j % W, j / W))
+  // into (v, u). All of a thread's loads are issued before the first store.
+  int32_t qv[kPerThread];
+  float dq[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int i = threadIdx.x + q * kReconThreads;
+    const int r = i % (3 * N), c = r / N, j = r % N;
+    const bool live = i < active * 3 * N;
+    const int2 a = item_anchor[q];
+    qv[q] = live ? p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 +
+                         j % W]
+                 : 0;
+    dq[q] = p.dequant[c * N + j];
+  }
   if (threadIdx.x < active) {
     const int k = threadIdx.x;
-    const int2 a = p.anchors[first + k];
+    const int2 a = own_anchor;
     anchor[k] = a;
     const int raw = p.raw[a.y * p.blocks_x + a.x];
     for (int c = 0; c < 3; ++c) {
@@ -155,24 +187,17 @@ __global__ void __launch_bounds__(kReconThreads, 2) ReconstructKernel(const __gr
     factors[k][0] = static_cast<float>(p.y_to_x[tile]) / 84.0f;
     factors[k][1] = 1.0f + static_cast<float>(p.y_to_b[tile]) / 84.0f;
   }
-  __syncthreads();
-  // Dequantize coefficient j = coefficient_index(v, u) (footprint (j % W, j / W))
-  // into (v, u).
-  // All of a thread's loads are issued before the first store.
-  constexpr int kPerThread = KC * N / kReconThreads;
-  int32_t qv[kPerThread];
-  float dq[kPerThread];
-#pragma unroll
-  for (int q = 0; q < kPerThread; ++q) {
-    const int i = threadIdx.x + q * kReconThreads;
-    const int k = i / (3 * N), r = i % (3 * N), c = r / N, j = r % N;
-    const bool live = i < active * 3 * N;
-    const int2 a = anchor[live ? k : 0];
-    qv[q] = live ? p.qac[c * p.pitch + static_cast<size_t>(a.y * 8 + j / W) * p.stride + a.x * 8 +
-                         j % W]
-                 : 0;
-    dq[q] = p.dequant[c * N + j];
+  if (threadIdx.x < active * 3) {
+    const int k = threadIdx.x / 3, c = threadIdx.x % 3;
+    const int2 a = dc_anchor;
+    for (int y = 0; y < S::CH; ++y) {
+      for (int x = 0; x < S::CW; ++x) {
+        dc_values[k][c][y * S::CW + x] =
+          p.dc[c * p.dc_pitch + static_cast<size_t>(a.y + y) * p.blocks_x + a.x + x];
+      }
+    }
   }
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < kPerThread; ++q) {
     const int i = threadIdx.x + q * kReconThreads;
@@ -193,8 +218,8 @@ __global__ void __launch_bounds__(kReconThreads, 2) ReconstructKernel(const __gr
   // LLF from the (smoothed) DC, one thread per transform channel.
   if (threadIdx.x < active * 3) {
     const int k = threadIdx.x / 3, c = threadIdx.x % 3;
-    DcToLowFrequencies<W, H>(p.dc + c * p.dc_pitch, p.blocks_x, anchor[k].x, anchor[k].y,
-                             coef + Batch::At(k * 3 + c, 0, 0), Batch::RowPitch);
+    DcToLowFrequencies<W, H>(dc_values[k][c], S::CW, 0, 0, coef + Batch::At(k * 3 + c, 0, 0),
+                             Batch::RowPitch);
   }
   __syncthreads();
   const auto present = [&](int plane) { return plane < 3 * active; };
@@ -538,6 +563,7 @@ int LaunchReconstruct(ReconParams p, const DeviceTables& d, int family, size_t m
   if (status != GJXL_B200_OK) return status;
   const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
   if (grid == 0) return GJXL_B200_OK;
+  p.capacity = static_cast<uint32_t>(max_count);
   ReconstructKernel<W, H><<<grid, kReconThreads, smem, stream>>>(p);
   return CheckLaunch("aq reconstruct");
 }

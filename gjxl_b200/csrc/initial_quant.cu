@@ -14,7 +14,7 @@
 //   ErosionModulationKernel one thread per 8x8 block: fuzzy erosion (2x2 of
 //                          pre-erosion cells), strategy mask, gamma / HF /
 //                          blue modulations, FastPow2.
-//   Symmetric5Kernel       32x8 output tile from a mirrored halo tile in shared memory.
+//   Symmetric5Kernel       32x32 output tile from a mirrored halo tile in shared memory.
 
 #include <cmath>
 #include <cstring>
@@ -265,10 +265,12 @@ struct Symmetric5Params {
 };
 
 
-// One CTA per 32x8 output tile: the tile with a mirrored 2-pixel halo is
-// staged in shared memory (coalesced rows), then every output reads its 5x5
-// neighbourhood from there.
-constexpr int kS5W = 32, kS5H = 8;
+// One CTA of 32x8 threads per 32x32 output tile (four rows per thread): the
+// tile with a mirrored 2-pixel halo is staged in shared memory with a 2D
+// thread mapping, all of a thread's loads issued before its first store
+// (tiles whose window lies inside the image skip the mirroring); then every
+// output reads its 5x5 neighbourhood from there.
+constexpr int kS5W = 32, kS5H = 32, kS5Rows = 8;
 
 // WeightedRow (src/codec/convolution.cpp:14-30): far + (near + center), on a
 // staged row (the halo is already mirrored).
@@ -279,32 +281,59 @@ __device__ __forceinline__ float WeightedTileRow(const float* row, float c, floa
   return far + (near + center);
 }
 
-__global__ void __launch_bounds__(kS5W * kS5H)
+__global__ void __launch_bounds__(kS5W * kS5Rows)
 Symmetric5Kernel(const __grid_constant__ Symmetric5Params p) {
-  __shared__ float tile[kS5H + 4][kS5W + 4];
+  constexpr int TW = kS5W + 4, TH = kS5H + 4;
+  constexpr int kCols = (TW + kS5W - 1) / kS5W, kRows = (TH + kS5Rows - 1) / kS5Rows;
+  __shared__ float tile[TH][TW];
   const uint32_t plane = blockIdx.z;
   const int x0 = blockIdx.x * kS5W, y0 = blockIdx.y * kS5H;
   const int h = p.height, wd = p.width;
   const float* in = p.input + plane * p.in_pitch;
-  const int tid = threadIdx.y * kS5W + threadIdx.x;
-  for (int i = tid; i < (kS5H + 4) * (kS5W + 4); i += kS5W * kS5H) {
-    const int ty = i / (kS5W + 4), tx = i % (kS5W + 4);
-    tile[ty][tx] = in[static_cast<size_t>(Mirror(y0 + ty - 2, h)) * p.in_stride +
-                      Mirror(x0 + tx - 2, wd)];
+  const bool interior = x0 >= 2 && y0 >= 2 && x0 + kS5W + 2 <= wd && y0 + kS5H + 2 <= h;
+  float staged[kRows][kCols];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int ty = threadIdx.y + r * kS5Rows, tx = threadIdx.x + k * kS5W;
+      if (ty < TH && tx < TW) {
+        int gy = y0 + ty - 2, gx = x0 + tx - 2;
+        if (!interior) {
+          gy = Mirror(gy, h);
+          gx = Mirror(gx, wd);
+        }
+        staged[r][k] = in[static_cast<size_t>(gy) * p.in_stride + gx];
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+#pragma unroll
+    for (int k = 0; k < kCols; ++k) {
+      const int ty = threadIdx.y + r * kS5Rows, tx = threadIdx.x + k * kS5W;
+      if (ty < TH && tx < TW) tile[ty][tx] = staged[r][k];
+    }
   }
   __syncthreads();
-  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= wd || y >= h) return;
+  const int x = x0 + threadIdx.x;
+  if (x >= wd) return;
   const float* w = p.w[plane];
-  const int cx = threadIdx.x + 2, cy = threadIdx.y + 2;
-  float sum0 = WeightedTileRow(&tile[cy][cx], w[0], w[1], w[2]);
-  sum0 += WeightedTileRow(&tile[cy - 2][cx], w[2], w[5], w[4]);
-  float sum1 = WeightedTileRow(&tile[cy + 2][cx], w[2], w[5], w[4]);
-  sum0 += WeightedTileRow(&tile[cy - 1][cx], w[1], w[3], w[5]);
-  sum1 += WeightedTileRow(&tile[cy + 1][cx], w[1], w[3], w[5]);
-  const float v = sum0 + sum1;
-  if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
-  p.output[plane * p.out_pitch + static_cast<size_t>(y) * p.out_stride + x] = v;
+  const int cx = threadIdx.x + 2;
+#pragma unroll
+  for (int row = 0; row < kS5H / kS5Rows; ++row) {
+    const int oy = threadIdx.y + row * kS5Rows, y = y0 + oy;
+    if (y >= h) break;
+    const int cy = oy + 2;
+    float sum0 = WeightedTileRow(&tile[cy][cx], w[0], w[1], w[2]);
+    sum0 += WeightedTileRow(&tile[cy - 2][cx], w[2], w[5], w[4]);
+    float sum1 = WeightedTileRow(&tile[cy + 2][cx], w[2], w[5], w[4]);
+    sum0 += WeightedTileRow(&tile[cy - 1][cx], w[1], w[3], w[5]);
+    sum1 += WeightedTileRow(&tile[cy + 1][cx], w[1], w[3], w[5]);
+    const float v = sum0 + sum1;
+    if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
+    p.output[plane * p.out_pitch + static_cast<size_t>(y) * p.out_stride + x] = v;
+  }
 }
 
 // gaborish.cpp:11-35.
@@ -356,11 +385,11 @@ int LaunchSymmetric5(const float* input, size_t in_stride, size_t in_pitch, floa
   for (uint32_t c = 0; c < planes; ++c) std::memcpy(p.w[c], weights[c], sizeof(p.w[c]));
   p.error = error;
   if ((height + kS5H - 1) / kS5H > 65535) {
-    return SetError(GJXL_B200_UNSUPPORTED, "symmetric5: image taller than 524,280 rows");
+    return SetError(GJXL_B200_UNSUPPORTED, "symmetric5: image taller than 2,097,120 rows");
   }
   dim3 grid(static_cast<unsigned>((width + kS5W - 1) / kS5W),
             static_cast<unsigned>((height + kS5H - 1) / kS5H), planes);
-  Symmetric5Kernel<<<grid, dim3(kS5W, kS5H), 0, stream>>>(p);
+  Symmetric5Kernel<<<grid, dim3(kS5W, kS5Rows), 0, stream>>>(p);
   return CheckLaunch("symmetric5");
 }
 
