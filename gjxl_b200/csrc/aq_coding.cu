@@ -383,6 +383,7 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   // Per anchor block: covered width and height, inverse-dequant table
   // offset, and the quantization scale of its raw quant.
   __shared__ uint8_t block_cw[64], block_ch[64];
+  __shared__ uint8_t block_w_shift[64], block_sw_shift[64];  // log2 of 8 * cw, 8 * max(cw, ch)
   __shared__ int block_table[64];
   __shared__ float block_scale[64];
   const int tile = blockIdx.x;
@@ -407,19 +408,35 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
     }
     block_cw[b] = static_cast<uint8_t>(cw);
     block_ch[b] = static_cast<uint8_t>(ch);
+    block_w_shift[b] = static_cast<uint8_t>(3 + __ffs(cw) - 1);  // cw, ch are 1, 2 or 4
+    block_sw_shift[b] = static_cast<uint8_t>(3 + __ffs(cw >= ch ? cw : ch) - 1);
     block_terms[b] = n;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int running = 0;
-    for (int b = 0; b < 64; ++b) {
-      offsets[b] = running;
-      for (int g = running / 64; g < (running + block_terms[b]) / 64; ++g) {
-        group_block[g] = static_cast<uint8_t>(b);
-      }
-      running += block_terms[b];
+  // Exclusive prefix sum of the blocks' term counts (64 blocks, two warps:
+  // a shuffle scan per warp, then warp 0's total added to warp 1), and the
+  // anchor block of each 64-term group.
+  __shared__ int warp_total[2];
+  if (threadIdx.x < 64) {
+    const int b = threadIdx.x;
+    const int n = block_terms[b];
+    int inclusive = n;
+#pragma unroll
+    for (int d = 1; d < 32; d *= 2) {
+      const int v = __shfl_up_sync(0xffffffffu, inclusive, d);
+      if (lane >= d) inclusive += v;
     }
-    total_terms = running;
+    offsets[b] = inclusive - n;
+    if (lane == 31) warp_total[warp] = inclusive;
+  }
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int b = threadIdx.x;
+    const int n = block_terms[b];
+    const int offset = offsets[b] + (b >= 32 ? warp_total[0] : 0);
+    offsets[b] = offset;
+    for (int g = offset / 64; g < (offset + n) / 64; ++g) group_block[g] = static_cast<uint8_t>(b);
+    if (b == 63) total_terms = offset + n;
   }
   __syncthreads();
   // Every thread takes terms e = tid, tid + 128, ... of the tile; every
@@ -437,18 +454,19 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
       if (e >= count) continue;
       const int b = group_block[e / 64], i = e - offsets[b];
       const int cw = block_cw[b], ch = block_ch[b];
-      const int w = cw * 8;
-      // LLF extent: covered blocks with the longer side first.
+      const int w_shift = block_w_shift[b], sw_shift = block_sw_shift[b];
+      // LLF extent: covered blocks with the longer side first; the
+      // coefficient extent is 8 * max(cw, ch) wide.
       const int lfw = cw > ch ? cw : ch, lfh = cw > ch ? ch : cw;
-      const int sw = (cw >= ch ? cw : ch) * 8;  // coefficient extent width
-      const int cy = i / sw, cx = i % sw;
+      const int cy = i >> sw_shift, cx = i & ((1 << sw_shift) - 1);
       const bool llf = cy < lfh && cx < lfw;
       const float* inv = p.inverse_dequant + block_table[b];
       inv_x[j] = inv[i];
       inv_b[j] = inv[2 * cw * ch * 64 + i];
       if (!llf) {
-        const size_t at = static_cast<size_t>((by0 + b / tw) * 8 + i / w) * p.coef_stride +
-                          (bx0 + b % tw) * 8 + i % w;
+        const size_t at =
+          static_cast<size_t>((by0 + b / tw) * 8 + (i >> w_shift)) * p.coef_stride +
+          (bx0 + b % tw) * 8 + (i & ((1 << w_shift) - 1));
         luma_v[j] = p.coef[p.coef_pitch + at];
         x_v[j] = p.coef[at];
         b_v[j] = p.coef[2 * p.coef_pitch + at];
@@ -477,19 +495,32 @@ FinalCflKernel(const __grid_constant__ CflFinalParams p) {
   if (problem < 2) {
     const float* A = terms + 2 * problem * kFinalCflTerms;
     const float* B = A + kFinalCflTerms;
-    // count is a multiple of 64: batches of 8 elements per lane, loaded
-    // before the ordered multiply-adds.
+    // count is a multiple of 64: batches of 8 elements per lane; the next
+    // batch is loaded while the current one goes through the ordered
+    // multiply-adds.
+    float a[8], b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      a[j] = count > 0 ? A[slot + 4 * j] : 0.0f;
+      b[j] = count > 0 ? B[slot + 4 * j] : 0.0f;
+    }
     for (int e0 = slot; e0 < count; e0 += 32) {
-      float a[8], b[8];
+      float na[8], nb[8];
+      const int next = e0 + 32 < count ? e0 + 32 : slot;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        a[j] = A[e0 + 4 * j];
-        b[j] = B[e0 + 4 * j];
+        na[j] = A[next + 4 * j];
+        nb[j] = B[next + 4 * j];
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         quadratic = fmaf(a[j], a[j], quadratic);
         linear = fmaf(a[j], b[j], linear);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        a[j] = na[j];
+        b[j] = nb[j];
       }
     }
   }
