@@ -217,18 +217,21 @@ struct PopulationParams {
   uint32_t* present_mask;
 };
 
-// One CTA per group. The group's anchors are first listed per family; then,
-// family by family and channel by channel, each thread owns one physical
-// index (and a share of the anchors when the family has fewer than 256
-// indices) and counts zeros in a register, so shared-memory atomics happen
-// once per thread and index, not once per coefficient.
+// One CTA per group and channel (blockIdx.y). The group's anchors are first
+// listed per family, with the log2 of their footprint width; then, family by
+// family, each thread owns one physical index (and a share of the anchors
+// when the family has fewer than 256 indices) and counts zeros in a
+// register, four anchors' coefficients loaded at a time, so shared-memory
+// atomics happen once per thread and index, not once per coefficient.
 __global__ void __launch_bounds__(256) PopulationKernel(const __grid_constant__ PopulationParams p) {
-  __shared__ uint32_t counts[kPopulationCount];
+  __shared__ uint32_t counts[kPopulationStride + 64];  // this channel; then the DCT8 sample
   __shared__ short2 anchors[5][kGroupBlocks * kGroupBlocks];
+  __shared__ uint8_t anchor_shift[5][kGroupBlocks * kGroupBlocks];
   __shared__ uint8_t sampled[kGroupBlocks * kGroupBlocks];
   __shared__ int anchor_count[5];
   __shared__ uint32_t present;
-  for (int i = threadIdx.x; i < kPopulationCount; i += blockDim.x) counts[i] = 0;
+  const int c = blockIdx.y;
+  for (int i = threadIdx.x; i < kPopulationStride + 64; i += blockDim.x) counts[i] = 0;
   if (threadIdx.x < 5) anchor_count[threadIdx.x] = 0;
   if (threadIdx.x == 0) present = 0;
   __syncthreads();
@@ -242,10 +245,13 @@ __global__ void __launch_bounds__(256) PopulationKernel(const __grid_constant__ 
     const int fi = t.family == 0 ? 0 : t.family == 2 ? 1 : t.family == 3 ? 2 : t.family == 4 ? 3 : 4;
     const int slot = atomicAdd(&anchor_count[fi], 1);
     anchors[fi][slot] = make_short2(static_cast<short>(bx), static_cast<short>(by));
+    // Footprint widths are 8, 16 or 32.
+    anchor_shift[fi][slot] = static_cast<uint8_t>(__ffs(t.footprint_w) - 1);
     if (fi == 0) sampled[slot] = p.sample[by * p.blocks_x + bx];
     atomicOr(&present, 1u << t.family);
   }
   __syncthreads();
+  const int32_t* plane = p.qac + c * p.pitch;
   for (int fi = 0; fi < 5; ++fi) {
     const int count = anchor_count[fi];
     if (count == 0) continue;
@@ -253,27 +259,43 @@ __global__ void __launch_bounds__(256) PopulationKernel(const __grid_constant__ 
     const int shares = n >= static_cast<int>(blockDim.x) ? 1 : static_cast<int>(blockDim.x) / n;
     const int share = static_cast<int>(threadIdx.x) / (n >= static_cast<int>(blockDim.x) ? static_cast<int>(blockDim.x) : n);
     if (share >= shares) continue;
-    for (int c = 0; c < 3; ++c) {
-      for (int i = static_cast<int>(threadIdx.x) % n; i < n; i += blockDim.x) {
-        uint32_t zeros = 0, zeros_sampled = 0;
-        for (int a = share; a < count; a += shares) {
-          const short2 anchor = anchors[fi][a];
-          // Both orientations of a rectangular family share physical indices;
-          // the footprint width of this anchor decides where index i lies.
-          const TaskShape t = ShapeAt(p.cells, anchor.y * p.blocks_x + anchor.x);
-          const bool zero = Coefficient(p.qac, p.stride, p.pitch, c, anchor.x, anchor.y,
-                                        t.footprint_w, i) == 0;
-          zeros += zero;
-          if (fi == 0 && sampled[a]) zeros_sampled += zero;
+    for (int i = static_cast<int>(threadIdx.x) % n; i < n; i += blockDim.x) {
+      uint32_t zeros = 0, zeros_sampled = 0;
+      for (int a0 = share; a0 < count; a0 += 4 * shares) {
+        // Both orientations of a rectangular family share physical indices;
+        // the footprint width of each anchor decides where index i lies.
+        int32_t v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int a = a0 + k * shares;
+          v[k] = 1;
+          if (a < count) {
+            const short2 anchor = anchors[fi][a];
+            const int shift = anchor_shift[fi][a];
+            v[k] = plane[static_cast<size_t>(anchor.y * 8 + (i >> shift)) * p.stride +
+                         anchor.x * 8 + (i & ((1 << shift) - 1))];
+          }
         }
-        if (zeros) atomicAdd(counts + c * kPopulationStride + PopulationOffset(family) + i, zeros);
-        if (zeros_sampled) atomicAdd(counts + kPopulationFull + c * 64 + i, zeros_sampled);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int a = a0 + k * shares;
+          const bool zero = a < count && v[k] == 0;
+          zeros += zero;
+          if (fi == 0 && zero && sampled[a]) ++zeros_sampled;
+        }
       }
+      if (zeros) atomicAdd(counts + PopulationOffset(family) + i, zeros);
+      if (zeros_sampled) atomicAdd(counts + kPopulationStride + i, zeros_sampled);
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kPopulationCount; i += blockDim.x) {
-    if (counts[i]) atomicAdd(p.population + i, counts[i]);
+  for (int i = threadIdx.x; i < kPopulationStride; i += blockDim.x) {
+    if (counts[i]) atomicAdd(p.population + c * kPopulationStride + i, counts[i]);
+  }
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    if (counts[kPopulationStride + i]) {
+      atomicAdd(p.population + kPopulationFull + c * 64 + i, counts[kPopulationStride + i]);
+    }
   }
   if (threadIdx.x == 0 && present) atomicOr(p.present_mask, present);
 }
@@ -800,7 +822,7 @@ extern "C" int gjxl_b200_ac_tokenize(gjxl_b200_ac_tokens* s, const uint8_t* stra
     pp.sample = s->sample;
     pp.population = s->population;
     pp.present_mask = s->masks;
-    PopulationKernel<<<groups, 256, 0, stream>>>(pp);
+    PopulationKernel<<<dim3(groups, 3), 256, 0, stream>>>(pp);
   }
   if (order_mode != 0) {
     OrderParams op;
