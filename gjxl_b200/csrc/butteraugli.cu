@@ -116,6 +116,32 @@ Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
   }
 }
 
+// ConvolveBorderColumn's renormalized sum at position x of a line of length
+// n (samples at src[j * step]), with the taps unrolled: tap t reads sample
+// x - R + t; taps outside the line add +0.0, which leaves both sums (never
+// -0.0) unchanged, so the sums equal the reference's sums over the taps
+// inside the line, in the same order. All samples are loaded first.
+template <int R>
+__device__ __forceinline__ float ConvolveBorder(const float* src, int step, int x, int n,
+                                                const Kernel17& k) {
+  float sample[2 * R + 1];
+#pragma unroll
+  for (int t = 0; t <= 2 * R; ++t) {
+    const int j = x - R + t;
+    sample[t] = j >= 0 && j < n ? src[static_cast<ptrdiff_t>(j) * step] : 0.0f;
+  }
+  float weight = 0.0f, sum = 0.0f;
+#pragma unroll
+  for (int t = 0; t <= 2 * R; ++t) {
+    const int j = x - R + t;
+    const bool inside = j >= 0 && j < n;
+    weight += inside ? k.raw[t] : 0.0f;
+    sum += inside ? sample[t] * k.raw[t] : 0.0f;
+  }
+  const float scale = 1.0f / weight;
+  return sum * scale;
+}
+
 // One tap row of ConvolutionWithTranspose at position x of a line of length n
 // (samples at src[j * step]). Interior: pair sums folded round-robin into four
 // partial sums (ConvolveInterior7/13/15/33); border: renormalized direct sum
@@ -140,14 +166,7 @@ __device__ __forceinline__ float ConvolveLine(const float* src, int step, int x,
     for (int i = 0; i < (R < 4 ? R : 4); ++i) out = out + sums[i];
     return out;
   }
-  const int first = x < R ? 0 : x - R;
-  const int last = min(n - 1, x + R);
-  float weight = 0.0f;
-  for (int j = first; j <= last; ++j) weight += k.raw[j + R - x];
-  const float scale = 1.0f / weight;
-  float sum = 0.0f;
-  for (int j = first; j <= last; ++j) sum += src[static_cast<ptrdiff_t>(j) * step] * k.raw[j + R - x];
-  return sum * scale;
+  return ConvolveBorder<R>(src, step, x, n, k);
 }
 
 // Register-blocked blur along one axis: each thread computes kRun
@@ -266,7 +285,7 @@ BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_
     for (int r = 0; r < kBlurRows && y0 + r < h; ++r) {
       const int y = y0 + r;
       float* dst = out + plane * out_pitch + static_cast<size_t>(y) * w + first;
-      if (first >= R && first + kRowRun - 1 < w - R) {
+      {
         float v[kWindow];
         const float* s = segment[r] + threadIdx.x * kRowRun;
 #pragma unroll
@@ -282,17 +301,38 @@ BlurRowsKernel(const float* in, float* out, int w, int h, size_t in_pitch, size_
           v[kWindow - 2] = f.x;
           v[kWindow - 1] = f.y;
         }
+        // Every thread computes its four outputs from the window; only the
+        // interior ones are stored (the border CTA writes the others).
         float o4[kRowRun];
         ConvolveWindow<R, kRowRun>(v, k, o4);
 #pragma unroll
-        for (int o = 0; o < kRowRun; ++o) dst[o] = o4[o];
-        continue;
+        for (int o = 0; o < kRowRun; ++o) {
+          if (first + o >= R && first + o < w - R) dst[o] = o4[o];
+        }
       }
-      const float* row = base + static_cast<size_t>(y) * w;
-      const int count = min(kRowRun, w - first);
-      for (int o = 0; o < count; ++o) dst[o] = ConvolveLine<R>(row, 1, first + o, w, k);
     }
   }
+}
+
+// The outputs within R of either row end (ConvolveLine's renormalized border
+// sum), for the rows of the row-blur CTAs: one thread per row and border
+// position, so that the row-blur CTAs run no divergent border code. The
+// positions are x = 0..R-1 and x = w-2R+R..w-1, the latter kept only where
+// x >= R (narrow rows).
+template <int R>
+__global__ void __launch_bounds__(kThreads)
+BlurRowBordersKernel(const float* in, float* out, int w, int h, size_t in_pitch,
+                     size_t out_pitch, const __grid_constant__ Kernel17 k) {
+  constexpr int kPerRow = 2 * R;
+  constexpr int kRowsPerCta = kThreads / kPerRow;
+  const int plane = blockIdx.y;
+  const int r = threadIdx.x / kPerRow, item = threadIdx.x % kPerRow;
+  const int y = blockIdx.x * kRowsPerCta + r;
+  if (r >= kRowsPerCta || y >= h) return;
+  const int x = item < R ? item : w - kPerRow + item;
+  if (item < R ? x >= w : (x < R || x >= w)) return;
+  const float* row = in + plane * in_pitch + static_cast<size_t>(y) * w;
+  out[plane * out_pitch + static_cast<size_t>(y) * w + x] = ConvolveBorder<R>(row, 1, x, w, k);
 }
 
 template <int R>
@@ -546,6 +586,7 @@ struct MaltaParams {
   const float* scaled;  // the stage's scaled differences (MaltaPlanes)
   float* accumulate;    // block_diff_ac plane (+= stage value)
   int w, h;
+  int tiles_x, tiles_y;  // output tiles of kMaltaTileW x kMaltaTileH
 };
 
 __device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
@@ -645,70 +686,82 @@ __device__ __forceinline__ float MaltaUnit(const float (&v)[2 * kMaltaHalo + 1][
 template <bool kLowFrequency>
 __global__ void __launch_bounds__(kMaltaThreads, 3)
 MaltaKernel(const __grid_constant__ MaltaParams p) {
-  __shared__ __align__(16) float tile[kMaltaSpanH][kMaltaSpanW];
-  const int x0 = blockIdx.x * kMaltaTileW - kMaltaHalo;
-  const int y0 = blockIdx.y * kMaltaTileH - kMaltaHalo;
-  // Staging, four samples per load: x0 is a multiple of 4, so with the row
+  // Two staging buffers: the CTA walks its tiles (tile index t, t + grid,
+  // ...) and copies the next tile's window in with asynchronous copies while
+  // it computes the current one.
+  __shared__ __align__(16) float tile[2][kMaltaSpanH][kMaltaSpanW];
+  // Staging, four samples per copy: x0 is a multiple of 4, so with the row
   // length a multiple of 4 every aligned group of 4 lies wholly inside or
   // wholly outside the image, and with a 16-byte aligned plane it is 16-byte
-  // aligned; other planes take scalar loads (the half-scale planes follow the
-  // full-scale ones in the arena, so their alignment depends on the image
-  // size). All of a thread's loads are issued before its first store.
+  // aligned (outside groups are zero-filled by the copy); other planes take
+  // synchronous scalar loads (the half-scale planes follow the full-scale
+  // ones in the arena, so their alignment depends on the image size).
   constexpr int kQuads = kMaltaSpanW / 4 * kMaltaSpanH;
   constexpr int kStage = (kQuads + kMaltaThreads - 1) / kMaltaThreads;
   static_assert(kMaltaSpanW % 4 == 0 && kMaltaHalo % 4 == 0, "aligned quads");
-  float4 staged[kStage];
   const bool aligned = p.w % 4 == 0 && reinterpret_cast<uintptr_t>(p.scaled) % 16 == 0;
+  const int tiles = p.tiles_x * p.tiles_y;
+  const auto stage = [&](int t, int buffer) {
+    const int x0 = (t % p.tiles_x) * kMaltaTileW - kMaltaHalo;
+    const int y0 = (t / p.tiles_x) * kMaltaTileH - kMaltaHalo;
 #pragma unroll
-  for (int j = 0; j < kStage; ++j) {
-    const int i = threadIdx.x + j * kMaltaThreads;
-    const int ty = i / (kMaltaSpanW / 4), tx = (i % (kMaltaSpanW / 4)) * 4;
-    const int x = x0 + tx, y = y0 + ty;
-    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (i < kQuads && y >= 0 && y < p.h) {
-      const float* row = p.scaled + static_cast<size_t>(y) * p.w;
+    for (int j = 0; j < kStage; ++j) {
+      const int i = threadIdx.x + j * kMaltaThreads;
+      if (i >= kQuads) break;
+      const int ty = i / (kMaltaSpanW / 4), tx = (i % (kMaltaSpanW / 4)) * 4;
+      const int x = x0 + tx, y = y0 + ty;
+      float* dst = &tile[buffer][ty][tx];
+      const bool row_inside = y >= 0 && y < p.h;
       if (aligned) {
-        if (x >= 0 && x < p.w) v = *reinterpret_cast<const float4*>(row + x);
+        const bool inside = row_inside && x >= 0 && x < p.w;
+        const float* src = inside ? p.scaled + static_cast<size_t>(y) * p.w + x : p.scaled;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(
+                       static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                     "l"(src), "r"(inside ? 16 : 0));
       } else {
-        v.x = x >= 0 && x < p.w ? row[x] : 0.0f;
-        v.y = x + 1 >= 0 && x + 1 < p.w ? row[x + 1] : 0.0f;
-        v.z = x + 2 >= 0 && x + 2 < p.w ? row[x + 2] : 0.0f;
-        v.w = x + 3 >= 0 && x + 3 < p.w ? row[x + 3] : 0.0f;
+        const float* row = p.scaled + static_cast<size_t>(row_inside ? y : 0) * p.w;
+        float4 v;
+        v.x = row_inside && x >= 0 && x < p.w ? row[x] : 0.0f;
+        v.y = row_inside && x + 1 >= 0 && x + 1 < p.w ? row[x + 1] : 0.0f;
+        v.z = row_inside && x + 2 >= 0 && x + 2 < p.w ? row[x + 2] : 0.0f;
+        v.w = row_inside && x + 3 >= 0 && x + 3 < p.w ? row[x + 3] : 0.0f;
+        *reinterpret_cast<float4*>(dst) = v;
       }
     }
-    staged[j] = v;
-  }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  int buffer = 0;
+  if (static_cast<int>(blockIdx.x) < tiles) stage(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < tiles; t += gridDim.x, buffer ^= 1) {
+    // This tile's copies are done, and every thread is past the previous
+    // tile's reads of the other buffer.
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    if (t + static_cast<int>(gridDim.x) < tiles) stage(t + gridDim.x, buffer ^ 1);
+    const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
+    const int ly = threadIdx.x / (kMaltaTileW / kMaltaRun);
+    float v[2 * kMaltaHalo + 1][kMaltaWindowW];
 #pragma unroll
-  for (int j = 0; j < kStage; ++j) {
-    const int i = threadIdx.x + j * kMaltaThreads;
-    if (i >= kQuads) break;
-    *reinterpret_cast<float4*>(&tile[i / (kMaltaSpanW / 4)][(i % (kMaltaSpanW / 4)) * 4]) =
-      staged[j];
-  }
-  __syncthreads();
-  const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
-  const int ly = threadIdx.x / (kMaltaTileW / kMaltaRun);
-  float v[2 * kMaltaHalo + 1][kMaltaWindowW];
+    for (int dy = 0; dy < 2 * kMaltaHalo + 1; ++dy) {
 #pragma unroll
-  for (int dy = 0; dy < 2 * kMaltaHalo + 1; ++dy) {
-#pragma unroll
-    for (int q = 0; q < kMaltaWindowW / 4; ++q) {
-      const float4 f = *reinterpret_cast<const float4*>(&tile[ly + dy][lx + 4 * q]);
-      v[dy][4 * q + 0] = f.x;
-      v[dy][4 * q + 1] = f.y;
-      v[dy][4 * q + 2] = f.z;
-      v[dy][4 * q + 3] = f.w;
+      for (int q = 0; q < kMaltaWindowW / 4; ++q) {
+        const float4 f = *reinterpret_cast<const float4*>(&tile[buffer][ly + dy][lx + 4 * q]);
+        v[dy][4 * q + 0] = f.x;
+        v[dy][4 * q + 1] = f.y;
+        v[dy][4 * q + 2] = f.z;
+        v[dy][4 * q + 3] = f.w;
+      }
     }
-  }
-  const float r[kMaltaRun] = {MaltaUnit<kLowFrequency, 0>(v), MaltaUnit<kLowFrequency, 1>(v),
-                              MaltaUnit<kLowFrequency, 2>(v), MaltaUnit<kLowFrequency, 3>(v)};
-  const int x = blockIdx.x * kMaltaTileW + lx, y = blockIdx.y * kMaltaTileH + ly;
-  if (y >= p.h) return;
-  float* out = p.accumulate + static_cast<size_t>(y) * p.w + x;
+    const float r[kMaltaRun] = {MaltaUnit<kLowFrequency, 0>(v), MaltaUnit<kLowFrequency, 1>(v),
+                                MaltaUnit<kLowFrequency, 2>(v), MaltaUnit<kLowFrequency, 3>(v)};
+    const int x = (t % p.tiles_x) * kMaltaTileW + lx, y = (t / p.tiles_x) * kMaltaTileH + ly;
+    if (y >= p.h) continue;
+    float* out = p.accumulate + static_cast<size_t>(y) * p.w + x;
 #pragma unroll
-  for (int k = 0; k < kMaltaRun; ++k) {
-    // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
-    if (x + k < p.w) out[k] = out[k] + (0.0f + r[k]);
+    for (int k = 0; k < kMaltaRun; ++k) {
+      // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
+      if (x + k < p.w) out[k] = out[k] + (0.0f + r[k]);
+    }
   }
 }
 
@@ -1038,6 +1091,7 @@ struct ButteraugliState {
   uint32_t* error = nullptr;
   bool prepared = false;
   bool reference_mask_ready = false;  // reference mask planes computed
+  int sm_count = 0;                   // SMs of the device the state lives on
   Kernel17 k_opsin, k_low, k_high, k_ultra, k_mask;
 
   ~ButteraugliState() {
@@ -1054,6 +1108,9 @@ void BlurPlanes(const float* in, float* tmp, float* out, int w, int h, size_t pi
   const int row_groups = std::min((h + kBlurRows - 1) / kBlurRows, 65535);
   BlurRowsKernel<R><<<dim3((w + kRowSegment - 1) / kRowSegment, row_groups, planes), kThreads, 0,
                       stream>>>(in, tmp, w, h, pitch, pitch, k);
+  constexpr int kBorderRows = kThreads / (2 * R);
+  BlurRowBordersKernel<R><<<dim3((h + kBorderRows - 1) / kBorderRows, planes), kThreads, 0,
+                            stream>>>(in, tmp, w, h, pitch, pitch, k);
   BlurColumnsKernel<R><<<dim3(Blocks(column_runs), planes), kThreads, 0, stream>>>(
     tmp, out, w, h, pitch, pitch, k);
 }
@@ -1137,7 +1194,11 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
   // MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X.
   cudaMemsetAsync(s.ac, 0, 3 * n * sizeof(float), stream);
   const int order[6] = {4, 5, 2, 3, 0, 1};
-  dim3 tiles((s.w + kMaltaTileW - 1) / kMaltaTileW, (s.h + kMaltaTileH - 1) / kMaltaTileH);
+  const int tiles_x = (s.w + kMaltaTileW - 1) / kMaltaTileW;
+  const int tiles_y = (s.h + kMaltaTileH - 1) / kMaltaTileH;
+  // Three CTAs per SM walk the tiles.
+  const unsigned malta_grid = static_cast<unsigned>(
+    st.sm_count > 0 ? std::min(tiles_x * tiles_y, st.sm_count * 3) : tiles_x * tiles_y);
   for (int index : order) {
     MaltaParams mp;
     mp.scaled = s.malta + index * n;
@@ -1145,10 +1206,12 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
     mp.accumulate = s.ac + channel * n;
     mp.w = s.w;
     mp.h = s.h;
+    mp.tiles_x = tiles_x;
+    mp.tiles_y = tiles_y;
     if (index < 4) {
-      MaltaKernel<true><<<tiles, kMaltaThreads, 0, stream>>>(mp);
+      MaltaKernel<true><<<malta_grid, kMaltaThreads, 0, stream>>>(mp);
     } else {
-      MaltaKernel<false><<<tiles, kMaltaThreads, 0, stream>>>(mp);
+      MaltaKernel<false><<<malta_grid, kMaltaThreads, 0, stream>>>(mp);
     }
   }
   // kL2Weights (:32-36).
@@ -1231,6 +1294,12 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, Butte
     st->sub.w = static_cast<int>((width + 1) / 2);
     st->sub.h = static_cast<int>((height + 1) / 2);
     st->sub.n = static_cast<size_t>(st->sub.w) * st->sub.h;
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&st->sm_count, cudaDevAttrMultiProcessorCount, device) !=
+        cudaSuccess) {
+    st->sm_count = 0;  // the Malta grid then takes one CTA per tile
   }
   const size_t floats = ScaleFloats(st->main.n) + ScaleFloats(st->sub.n) + 64;
   int status = CheckCuda(cudaMalloc(&st->arena, floats * sizeof(float)), "butteraugli: cudaMalloc");
