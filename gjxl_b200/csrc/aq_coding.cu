@@ -817,8 +817,10 @@ __global__ void __launch_bounds__(CodingThreads<W, H>()) CodingKernel(const __gr
   __shared__ float dequant_y[N];            // the family's Y dequant weights
   static_assert(kT == 64, "two warps");
   const uint32_t anchor_index = blockIdx.x;
-  if (anchor_index >= *p.count) return;
+  // The grid is the anchor list's capacity, so the anchor load is in bounds;
+  // it is issued beside the count load instead of after it.
   const int2 a = p.anchors[anchor_index];
+  if (anchor_index >= *p.count) return;
   const int tid = threadIdx.x;
   // Every global value the CTA reads is requested here, before the first
   // barrier (loads are not moved across barriers), so that one round trip

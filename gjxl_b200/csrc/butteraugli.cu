@@ -587,6 +587,7 @@ struct MaltaParams {
   float* accumulate;    // block_diff_ac plane (+= stage value)
   int w, h;
   int tiles_x, tiles_y;  // output tiles of kMaltaTileW x kMaltaTileH
+  int first;             // first stage of its channel: the plane starts at zero
 };
 
 __device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
@@ -759,8 +760,10 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
     float* out = p.accumulate + static_cast<size_t>(y) * p.w + x;
 #pragma unroll
     for (int k = 0; k < kMaltaRun; ++k) {
-      // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0.
-      if (x + k < p.w) out[k] = out[k] + (0.0f + r[k]);
+      // The reference fills the stage with 0 and adds: 0 + r == r for r >= 0
+      // (or NaN), so the first stage of a channel stores r, and later ones
+      // add it to the plane.
+      if (x + k < p.w) out[k] = p.first ? r[k] : out[k] + (0.0f + r[k]);
     }
   }
 }
@@ -1192,7 +1195,8 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
   const float asym = st.hf_asymmetry;
   // Stage inputs (computed beside the distorted image's final planes):
   // MF_Y, MF_X, HF_Y, HF_X, UHF_Y, UHF_X.
-  cudaMemsetAsync(s.ac, 0, 3 * n * sizeof(float), stream);
+  // The first stage of each channel (4, 5) writes its plane; the B plane is
+  // written by the L2 terms.
   const int order[6] = {4, 5, 2, 3, 0, 1};
   const int tiles_x = (s.w + kMaltaTileW - 1) / kMaltaTileW;
   const int tiles_y = (s.h + kMaltaTileH - 1) / kMaltaTileH;
@@ -1208,6 +1212,7 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
     mp.h = s.h;
     mp.tiles_x = tiles_x;
     mp.tiles_y = tiles_y;
+    mp.first = index >= 4 ? 1 : 0;
     if (index < 4) {
       MaltaKernel<true><<<malta_grid, kMaltaThreads, 0, stream>>>(mp);
     } else {
