@@ -14,11 +14,18 @@ two field updates), then the coefficient-order populations and scans and the
 AC tokens with their histogram. The metric is megapixels per second (source
 pixels).
 
-`value` is measured with the input already in device memory (CUDA events on
-the launching stream around K steps). `e2e` runs the same steps through
+`value` is measured with the input already in device memory (CUDA events
+around K steps). `e2e` runs the same steps through
 gjxl_b200_session_analyze_host: host->device copy of the packed pixels from
 pinned memory, the analysis, and device->host copies of the results, all
 inside the timed region.
+
+Each GPU runs `--sessions` analysis sessions (default 3) on their own
+streams, as a serving process with several images in flight would: step i
+goes to session i mod S, so one image's latency-bound phases and host
+copies overlap another image's compute. For `e2e` every session is driven by
+its own host thread (the host-input call waits for its results). K steps
+are K images in total; the events bracket all of them.
 
 `--impl reference` times the reference's own CPU implementation of the same
 analysis (compiled from its sources into oracle/_ref) on the host cores: the
@@ -203,50 +210,92 @@ def run_gpu(args) -> dict:
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     img = make_image()
-    session = AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7)
-    stream = torch.cuda.current_stream().cuda_stream
+    count = 1 if args.launch_list else max(1, args.sessions)
+    sessions = [AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7)
+                for _ in range(count)]
+    session = sessions[0]
+    main_stream = torch.cuda.current_stream()
+    stream = main_stream.cuda_stream
+    side = [torch.cuda.Stream() for _ in range(count)]
     d_img = torch.from_numpy(img.reshape(HEIGHT, -1)).cuda()
     pinned = torch.from_numpy(img).pin_memory()
     pinned_np = pinned.numpy()
     row = WIDTH * 3
 
-    for _ in range(args.warmup):
-        session.analyze(d_img.data_ptr(), row, 3, stream)
-    torch.cuda.synchronize()
     if args.launch_list:
+        for _ in range(args.warmup):
+            session.analyze(d_img.data_ptr(), row, 3, stream)
+        torch.cuda.synchronize()
         for _ in range(args.steps):
             session.analyze(d_img.data_ptr(), row, 3, stream)
         torch.cuda.synchronize()
         session.close()
         return {}
+    # Warm-up (and each session's graph capture) one session at a time.
+    for i, sess in enumerate(sessions):
+        for _ in range(args.warmup):
+            sess.analyze(d_img.data_ptr(), row, 3, side[i].cuda_stream)
+        torch.cuda.synchronize()
 
-    # Device-resident throughput.
+    def fork(start_event):
+        for st in side:
+            st.wait_event(start_event)
+
+    def join(stop_event):
+        for st in side:
+            done = torch.cuda.Event()
+            done.record(st)
+            main_stream.wait_event(done)
+        stop_event.record(main_stream)
+
+    # Device-resident throughput: step i on session i mod S.
     barrier(world)
     sampler = ClockSampler(local) if rank == 0 else None
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    for _ in range(args.steps):
-        session.analyze(d_img.data_ptr(), row, 3, stream)
-    stop.record()
+    start.record(main_stream)
+    fork(start)
+    for i in range(args.steps):
+        sessions[i % count].analyze(d_img.data_ptr(), row, 3, side[i % count].cuda_stream)
+    join(stop)
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
     ms = max_over_ranks(start.elapsed_time(stop), world) / args.steps
     mp = WIDTH * HEIGHT / 1e6
     value = world * mp / (ms / 1e3)
 
-    # End to end through the host-input entry point.
-    for _ in range(max(1, args.warmup // 2)):
-        session.analyze_host(pinned_np, stream)
+    # End to end through the host-input entry point, one host thread per
+    # session (each call returns once its results are on the host).
+    import threading
+    for i, sess in enumerate(sessions):
+        for _ in range(max(1, args.warmup // 2)):
+            sess.analyze_host(pinned_np, side[i].cuda_stream)
     torch.cuda.synchronize()
     barrier(world)
-    start.record()
-    for _ in range(args.steps):
-        session.analyze_host(pinned_np, stream)
-    stop.record()
+    start.record(main_stream)
+    fork(start)
+    shares = [args.steps // count + (1 if i < args.steps % count else 0) for i in range(count)]
+    failures = []
+
+    def drive(i):
+        try:
+            for _ in range(shares[i]):
+                sessions[i].analyze_host(pinned_np, side[i].cuda_stream)
+        except Exception as exc:  # reported after the join
+            failures.append(exc)
+
+    threads = [threading.Thread(target=drive, args=(i,)) for i in range(count)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if failures:
+        raise failures[0]
+    join(stop)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(start.elapsed_time(stop), world) / args.steps
-    assert session.host_error() == 0, "device error word set"
+    for sess in sessions:
+        assert sess.host_error() == 0, "device error word set"
 
     # Per-stage times and the dominant kernel's roofline (separate session so
     # the timed region above carries no event records).
@@ -272,7 +321,8 @@ def run_gpu(args) -> dict:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "distance": 1.0,
-                   "effort": 7, "seed": SEED, "parallelism": f"replicas x{world}",
+                   "effort": 7, "seed": SEED,
+                   "parallelism": f"replicas x{world}, {count} concurrent sessions per GPU",
                    "l2": "working set (~0.6 GB of planes) exceeds the 126 MB L2"},
         "e2e": {"value": round(world * mp / (e2e_ms / 1e3), 3), "unit": "MP/s",
                 "ms_per_step": round(e2e_ms, 4),
@@ -298,7 +348,8 @@ def run_gpu(args) -> dict:
         },
         "clocks": clocks,
     }
-    session.close()
+    for sess in sessions:
+        sess.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -401,6 +452,8 @@ def main():
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--launch-list", action="store_true")
+    parser.add_argument("--sessions", type=int, default=3,
+                        help="analysis sessions (images in flight) per GPU")
     parser.add_argument("--size", default=None,
                         help="WxH of a smaller image of the same generator (profiling only)")
     args = parser.parse_args()
