@@ -56,7 +56,9 @@ def test_reference_corpus(cuda):
         assert s == float(GOLDEN[f"corpus{i}_ref_score"][0])
 
 
-@pytest.mark.parametrize("w,h", [(64, 64), (509, 261), (1000, 700)])
+# Narrow sizes put every blur output of the half scale (20x12, 15x9) within
+# the blur radius of a border.
+@pytest.mark.parametrize("w,h", [(64, 64), (509, 261), (1000, 700), (40, 24), (30, 17)])
 def test_reconstruction_like_distortion(cuda, w, h):
     img = generate_srgb8(w, h, 900 + w)
     r = ref.srgb8_to_linear(img)
