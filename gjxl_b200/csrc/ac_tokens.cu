@@ -157,6 +157,7 @@ struct TaskShape {
   int family = -1;   // order family, -1 for a non-anchor block
   int cw = 0, ch = 0, n = 0, covered = 0, log2_covered = 0, footprint_w = 0;
   int llf_w = 0, llf_h = 0, coef_w = 0;
+  int footprint_shift = 0, coef_shift = 0;  // log2 of footprint_w and coef_w
 };
 
 __device__ __forceinline__ TaskShape ShapeAt(const uint8_t* cells, int index) {
@@ -175,6 +176,9 @@ __device__ __forceinline__ TaskShape ShapeAt(const uint8_t* cells, int index) {
   t.llf_w = max(t.cw, t.ch);
   t.llf_h = min(t.cw, t.ch);
   t.coef_w = t.llf_w * 8;
+  // Widths are 8, 16 or 32.
+  t.footprint_shift = __ffs(t.footprint_w) - 1;
+  t.coef_shift = __ffs(t.coef_w) - 1;
   return t;
 }
 
@@ -182,6 +186,15 @@ __device__ __forceinline__ int Coefficient(const int32_t* qac, size_t stride, si
                                            int bx, int by, int footprint_w, int i) {
   return qac[c * pitch + static_cast<size_t>(by * 8 + i / footprint_w) * stride + bx * 8 +
              i % footprint_w];
+}
+
+// Coefficient() with the footprint width given as its log2 (a shift and a
+// mask instead of a division by a runtime width).
+__device__ __forceinline__ int CoefficientShift(const int32_t* qac, size_t stride, size_t pitch,
+                                                int c, int bx, int by, int footprint_shift,
+                                                int i) {
+  return qac[c * pitch + static_cast<size_t>(by * 8 + (i >> footprint_shift)) * stride + bx * 8 +
+             (i & ((1 << footprint_shift) - 1))];
 }
 
 __device__ __forceinline__ uint32_t WarpSumU(uint32_t v) {
@@ -432,8 +445,9 @@ __global__ void __launch_bounds__(256) TaskMetaKernel(const __grid_constant__ To
   int last = -1;
   for (int j = lane; j < t.n; j += 32) {
     const int physical = static_cast<int>(order[j]);
-    const int v = Coefficient(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_w, physical);
-    const int px = physical % t.coef_w, py = physical / t.coef_w;
+    const int v =
+      CoefficientShift(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_shift, physical);
+    const int px = physical & (t.coef_w - 1), py = physical >> t.coef_shift;
     const bool llf = px < t.llf_w && py < t.llf_h;
     if (v != 0 && !llf) nonzeros += 1;
     if (v != 0 && j >= t.covered) last = j;
@@ -614,7 +628,7 @@ __global__ void __launch_bounds__(256) EmitKernel(const __grid_constant__ TokenP
   for (int first = t.covered; first <= last; first += 32) {
     const int j = first + lane;
     const bool active = j <= last;
-    const int v = active ? Coefficient(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_w,
+    const int v = active ? CoefficientShift(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_shift,
                                        static_cast<int>(order[j]))
                          : 0;
     const uint32_t nz = v != 0 ? 1u : 0u;
@@ -654,7 +668,7 @@ __global__ void __launch_bounds__(256) PackKernel(const __grid_constant__ TokenP
   for (int c = 0; c < 3; ++c) {
     int32_t* dst = p.packed + p.group_coef_offsets[group] + c * per_channel + p.coef_offset[block];
     for (int i = lane; i < t.n; i += 32) {
-      dst[i] = Coefficient(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_w, i);
+      dst[i] = CoefficientShift(p.qac, p.stride, p.pitch, c, bx, by, t.footprint_shift, i);
     }
   }
 }

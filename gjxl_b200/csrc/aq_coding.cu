@@ -61,8 +61,8 @@ constexpr int kTransformThreads = 384;
 template <int W, int H>
 __global__ void __launch_bounds__(kTransformThreads)
 ForwardCoefficientsKernel(const float* opsin, size_t stride, size_t pitch, const int2* anchors,
-                          const uint32_t* count, float* coef, size_t coef_stride,
-                          size_t coef_pitch) {
+                          const uint32_t* count, uint32_t capacity, float* coef,
+                          size_t coef_stride, size_t coef_pitch) {
   using S = TransformShape<W, H>;
   constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
   using Batch = PlaneBatch<W, H, KC>;
@@ -71,18 +71,26 @@ ForwardCoefficientsKernel(const float* opsin, size_t stride, size_t pitch, const
   double* tmp = reinterpret_cast<double*>(smem);                  // [KC] padded planes
   float* px = reinterpret_cast<float*>(tmp + Batch::Elements);    // [KC] padded planes
   const uint32_t first = blockIdx.x * K;
+  // The anchor loads do not wait for the count: the list index is clamped to
+  // the list (capacity entries), and anchors past the count are never used.
+  constexpr int kPerThread = KC * N / kTransformThreads;
+  int2 item_anchor[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int k = (threadIdx.x + q * kTransformThreads) / (3 * N);
+    item_anchor[q] = anchors[min(first + static_cast<uint32_t>(k), capacity - 1)];
+  }
   const uint32_t n = *count;
   if (first >= n) return;
   const int active = min(K, static_cast<int>(n - first));
   // All of a thread's loads are issued before the first store.
-  constexpr int kPerThread = KC * N / kTransformThreads;
   float value[kPerThread];
 #pragma unroll
   for (int q = 0; q < kPerThread; ++q) {
     const int i = threadIdx.x + q * kTransformThreads;
-    const int k = i / (3 * N), r = i % (3 * N), c = r / N, yx = r % N;
+    const int r = i % (3 * N), c = r / N, yx = r % N;
     const bool live = i < active * 3 * N;
-    const int2 a = anchors[first + (live ? k : 0)];
+    const int2 a = item_anchor[q];
     value[q] = live ? opsin[c * pitch + static_cast<size_t>(a.y * 8 + yx / W) * stride + a.x * 8 +
                             yx % W]
                     : 0.0f;
@@ -1367,7 +1375,7 @@ int LaunchForward(const float* opsin, size_t stride, size_t pitch, const int2* l
   const unsigned grid = static_cast<unsigned>((max_count + K - 1) / K);
   if (grid == 0) return GJXL_B200_OK;
   ForwardCoefficientsKernel<W, H><<<grid, kTransformThreads, smem, stream>>>(
-    opsin, stride, pitch, list, count, coef, stride, pitch);
+    opsin, stride, pitch, list, count, static_cast<uint32_t>(max_count), coef, stride, pitch);
   return CheckLaunch("aq forward coefficients");
 }
 
