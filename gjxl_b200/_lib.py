@@ -52,6 +52,8 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_stage_name": None,
     "gjxl_b200_session_kernel_count": None,
     "gjxl_b200_fp64_throughput": [P, P, P],
+    "gjxl_b200_check_device_error": [P, Z, P],
+    "gjxl_b200_test_arm_failure": [I, I],
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,

@@ -748,7 +748,7 @@ extern "C" int gjxl_b200_ac_tokens_create(size_t blocks_x, size_t blocks_y,
   };
   size_t total = 0;
   for (const Item& item : items) total = (total + 255) / 256 * 256 + item.bytes;
-  int status = CheckCuda(cudaMalloc(&s->arena, total), "ac_tokens_create: cudaMalloc");
+  int status = CheckCuda(DeviceMalloc(&s->arena, total), "ac_tokens_create: cudaMalloc");
   if (status != GJXL_B200_OK) {
     delete s;
     return status;

@@ -406,9 +406,12 @@ OpsinDynamicsKernel(const float* linear, size_t linear_stride, size_t linear_pit
   const float s1 = fmaxf(GammaB(p1) / p1, 1.0e-4f);
   const float s2 = fmaxf(GammaB(p2) / p2, 1.0e-4f);
   const size_t li = static_cast<size_t>(y) * linear_stride + x;
+  const float r = linear[li], g = linear[linear_pitch + li], b = linear[2 * linear_pitch + li];
+  // A non-finite input sample would be absorbed by the clamps below (fmaxf
+  // returns the other operand for a NaN), so it is reported here.
+  if (!(IsFinite(r) && IsFinite(g) && IsFinite(b))) RaiseError(error, kErrorNonFiniteInput);
   float c0, c1, c2;
-  OpsinAbsorbance<false>(linear[li] * intensity, linear[linear_pitch + li] * intensity,
-                         linear[2 * linear_pitch + li] * intensity, c0, c1, c2);
+  OpsinAbsorbance<false>(r * intensity, g * intensity, b * intensity, c0, c1, c2);
   c0 = fmaxf(c0 * s0, 1.7557483643287353f);
   c1 = fmaxf(c1 * s1, 1.7557483643287353f);
   c2 = fmaxf(c2 * s2, 12.226454707163354f);
@@ -1307,7 +1310,7 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, Butte
     st->sm_count = 0;  // the Malta grid then takes one CTA per tile
   }
   const size_t floats = ScaleFloats(st->main.n) + ScaleFloats(st->sub.n) + 64;
-  int status = CheckCuda(cudaMalloc(&st->arena, floats * sizeof(float)), "butteraugli: cudaMalloc");
+  int status = CheckCuda(DeviceMalloc(reinterpret_cast<void**>(&st->arena), floats * sizeof(float)), "butteraugli: cudaMalloc");
   if (status != GJXL_B200_OK) {
     delete st;
     return status;

@@ -20,6 +20,22 @@ int SetError(int code, const char* message);
 int CheckLaunch(const char* what);
 int CheckCuda(cudaError_t error, const char* what);
 
+// Deterministic failure injection for tests (gjxl_b200_test_arm_failure):
+// returns true, once, when the calling thread's countdown for `kind` reaches
+// its armed check point.
+enum InjectedFailure : int {
+  kInjectAllocation = 1,
+  kInjectGraph = 2,
+  kInjectSubmission = 3,
+  kInjectKinds = 4,
+};
+bool InjectFailure(int kind);
+
+// Device / pinned host allocations of the handle constructors; both are
+// allocation check points of the failure injection.
+cudaError_t DeviceMalloc(void** ptr, size_t bytes);
+cudaError_t HostMalloc(void** ptr, size_t bytes);
+
 inline bool Aligned16(const void* p) {
   return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
 }

@@ -13,10 +13,18 @@
 // This variant takes the scratch from a fixed, statically sized device array
 // instead. It has no counterpart in the reference.
 //
-// Set-up: the first call on each device looks up the array's address there
-// with cudaGetSymbolAddress (which also loads this module's device memory on
-// that device); make that first call before any stream capture. Later calls
-// only launch the three kernels of the initial quantization field.
+// Set-up: the first call in each CUDA context (normally a device's primary
+// context) looks up the array's address there with cudaGetSymbolAddress
+// (which also loads this module's device memory in that context); make that
+// first call before any stream capture. The address belongs to that context:
+// it is cached under the context's unique id, so a call in another context,
+// or after cudaDeviceReset replaced the primary context, looks it up again
+// instead of using a stale address. Later calls only launch the three
+// kernels of the initial quantization field.
+//
+// Like every __device__ array, the 16 MiB are held on each device whose
+// context loads this library's module, whether or not this entry point is
+// ever called, until the context is destroyed.
 //
 // Every scratch element is written before it is read (the pre-erosion kernel
 // writes every pixel of the raw mask and every 4x4 cell of the grid), so
@@ -28,7 +36,10 @@
 // (on different streams, or from different host threads without ordering)
 // race on it. Callers serialize them, e.g. by using one stream.
 
+#include <cuda.h>
+
 #include <cmath>
+#include <cstdint>
 #include <mutex>
 
 #include "host_util.h"
@@ -44,9 +55,50 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
-float* g_scratch_address[kMaxDevices] = {};
+struct ScratchAddress {
+  unsigned long long context_id = 0;  // 0: not looked up yet
+  float* address = nullptr;
+};
+ScratchAddress g_scratch_address[kMaxDevices];
 
-// Address of the static scratch on the current device, looked up once.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (never reused within a
+// process, unlike the CUcontext handle), through the runtime's driver entry
+// points so the library needs no link against the driver library. Returns
+// false (and *id = 0) when no context is current.
+bool CurrentContextId(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult found;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) ==
+            cudaSuccess && found == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+        found == cudaDriverEntryPointSuccess) {
+      get_id = reinterpret_cast<CtxGetIdFn>(fn);
+    }
+    cudaGetLastError();
+  });
+  *id = 0;
+  CUcontext context = nullptr;
+  if (get_current == nullptr || get_id == nullptr || get_current(&context) != CUDA_SUCCESS ||
+      context == nullptr || get_id(context, id) != CUDA_SUCCESS) {
+    *id = 0;
+  }
+  return *id != 0;
+}
+
+// Address of the static scratch in the current context, looked up once per
+// context. With no context current yet, the lookup itself makes the device's
+// primary context current (as any runtime call does), and the address is
+// cached under that context's id.
 int NoAllocScratch(float** out) {
   int device = -1;
   int status = CheckCuda(cudaGetDevice(&device), "initial_quant_field_noalloc: cudaGetDevice");
@@ -54,16 +106,23 @@ int NoAllocScratch(float** out) {
   if (device < 0 || device >= kMaxDevices) {
     return SetError(GJXL_B200_UNSUPPORTED, "initial_quant_field_noalloc: device ordinal >= 64");
   }
+  unsigned long long context_id = 0;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (g_scratch_address[device] == nullptr) {
+  ScratchAddress& cached = g_scratch_address[device];
+  if (!CurrentContextId(&context_id) || cached.context_id != context_id) {
     float* address = nullptr;
     status = CheckCuda(cudaGetSymbolAddress(reinterpret_cast<void**>(&address),
                                             g_initial_quant_scratch),
                        "initial_quant_field_noalloc: cudaGetSymbolAddress");
     if (status != GJXL_B200_OK) return status;
-    g_scratch_address[device] = address;
+    if (!CurrentContextId(&context_id)) {
+      return SetError(GJXL_B200_UNAVAILABLE,
+                      "initial_quant_field_noalloc: no current CUDA context id");
+    }
+    cached.context_id = context_id;
+    cached.address = address;
   }
-  *out = g_scratch_address[device];
+  *out = cached.address;
   return GJXL_B200_OK;
 }
 

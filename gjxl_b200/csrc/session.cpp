@@ -165,7 +165,9 @@ struct Session {
   cudaEvent_t events[kStageCount + 1] = {};
   bool events_created = false;
   // The analysis as one CUDA graph, captured on the first analyze() call for
-  // a given input pointer / stride / channel count and replayed afterwards.
+  // a channel count and replayed afterwards. The graph reads the session's
+  // own input buffer (`pixels`, rows of width * channels bytes), so callers
+  // may pass a new input pointer per image without a recapture.
   cudaStream_t capture_stream = nullptr;
   // Side streams: the fan for the per-family stages, and one stream for the
   // Butteraugli reference preparation, which only needs the input and runs
@@ -175,8 +177,6 @@ struct Session {
   cudaStream_t prepare_stream = nullptr;
   cudaEvent_t prepare_fork = nullptr, prepare_join = nullptr;
   cudaGraphExec_t graph = nullptr;
-  const uint8_t* graph_pixels = nullptr;
-  size_t graph_stride = 0;
   int graph_channels = 0;
   bool graph_disabled = false;
 
@@ -271,7 +271,7 @@ int Allocate(Session* s) {
   };
   size_t total = 0;
   for (const Item& item : items) total = Align(total, 256) + item.bytes;
-  int status = CheckCuda(cudaMalloc(&s->arena, total), "session: cudaMalloc");
+  int status = CheckCuda(DeviceMalloc(&s->arena, total), "session: cudaMalloc");
   if (status != GJXL_B200_OK) return status;
   s->arena_bytes = total;
   size_t offset = 0;
@@ -286,7 +286,7 @@ int Allocate(Session* s) {
                             Align(3 * blocks * 4, 16) + 64 + Align(sizeof(AqQuantizer), 16) +
                             Align(3 * plane * 4, 16);
   void* host = nullptr;
-  status = CheckCuda(cudaMallocHost(&host, host_bytes), "session: cudaMallocHost");
+  status = CheckCuda(HostMalloc(&host, host_bytes), "session: cudaMallocHost");
   if (status != GJXL_B200_OK) return status;
   s->host_block = static_cast<unsigned char*>(host);
   unsigned char* h = s->host_block;
@@ -312,7 +312,7 @@ int Allocate(Session* s) {
     status = gjxl_b200_ac_tokens_create(s->bx, s->by, &s->tokens);
     if (status != GJXL_B200_OK) return status;
     void* mirror = nullptr;
-    status = CheckCuda(cudaMallocHost(&mirror, s->token_capacity * 6 + (s->groups + 1) * 4 + 64),
+    status = CheckCuda(HostMalloc(&mirror, s->token_capacity * 6 + (s->groups + 1) * 4 + 64),
                        "session: token mirrors");
     if (status != GJXL_B200_OK) return status;
     s->host_tok_values = static_cast<uint32_t*>(mirror);
@@ -489,8 +489,12 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
 }
 
 // Runs the analysis as a replay of its captured graph: one launch instead of
-// ~280, with the same kernels and arguments. Stage profiling, a caller stream
-// that is itself being captured, or a failed capture run the stages directly.
+// ~350, with the same kernels and arguments. The graph reads the session's
+// input buffer; input elsewhere on the device is first copied there (one
+// stream-ordered 2D copy, 37 MB at 12 MP), so a new input pointer per image
+// costs that copy and never a recapture. Stage profiling, a caller stream
+// that is itself being captured, or a failed capture run the stages directly
+// on the caller's pointer.
 int RunReplay(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
               cudaStream_t stream) {
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
@@ -500,8 +504,16 @@ int RunReplay(Session* s, const uint8_t* pixels, size_t row_stride, int channels
     cudaGetLastError();
     return Run(s, pixels, row_stride, channels, stream);
   }
-  if (s->graph == nullptr || s->graph_pixels != pixels || s->graph_stride != row_stride ||
-      s->graph_channels != channels) {
+  const size_t packed_row = s->width * static_cast<size_t>(channels);
+  if (pixels != s->pixels) {
+    GJXL_TRY(CheckCuda(cudaMemcpy2DAsync(s->pixels, packed_row, pixels, row_stride, packed_row,
+                                         s->height, cudaMemcpyDeviceToDevice, stream),
+                       "session: input copy"));
+  } else if (row_stride != packed_row) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT,
+                    "session_analyze: the session input buffer holds packed rows");
+  }
+  if (s->graph == nullptr || s->graph_channels != channels) {
     if (s->graph != nullptr) {
       cudaGraphExecDestroy(s->graph);
       s->graph = nullptr;
@@ -514,21 +526,20 @@ int RunReplay(Session* s, const uint8_t* pixels, size_t row_stride, int channels
     bool ok = cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeRelaxed) ==
               cudaSuccess;
     if (ok) {
-      const int run_status = Run(s, pixels, row_stride, channels, s->capture_stream);
+      const int run_status = Run(s, s->pixels, packed_row, channels, s->capture_stream);
       ok = cudaStreamEndCapture(s->capture_stream, &graph) == cudaSuccess &&
            run_status == GJXL_B200_OK;
     }
-    if (ok) ok = cudaGraphInstantiate(&s->graph, graph, 0) == cudaSuccess;
+    if (ok) ok = !InjectFailure(kInjectGraph) && cudaGraphInstantiate(&s->graph, graph, 0) ==
+                                                 cudaSuccess;
     if (graph != nullptr) cudaGraphDestroy(graph);
     if (!ok) {
       cudaGetLastError();
       ClearLastError();
       s->graph = nullptr;
       s->graph_disabled = true;
-      return Run(s, pixels, row_stride, channels, stream);
+      return Run(s, s->pixels, packed_row, channels, stream);
     }
-    s->graph_pixels = pixels;
-    s->graph_stride = row_stride;
     s->graph_channels = channels;
   }
   return CheckCuda(cudaGraphLaunch(s->graph, stream), "session: graph launch");
@@ -647,8 +658,12 @@ extern "C" void gjxl_b200_session_destroy(gjxl_b200_session* session) { delete s
 extern "C" int gjxl_b200_session_analyze(gjxl_b200_session* s, const uint8_t* pixels,
                                          size_t row_stride, int channels, void* stream) {
   ClearLastError();
-  if (s == nullptr || pixels == nullptr) {
-    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze: null argument");
+  if (s == nullptr || pixels == nullptr || (channels != 3 && channels != 4) ||
+      row_stride < s->width * static_cast<size_t>(channels)) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze: invalid arguments");
+  }
+  if (InjectFailure(kInjectSubmission)) {
+    return SetError(GJXL_B200_SUBMISSION_FAILED, "session_analyze: injected submission failure");
   }
   return RunReplay(s, pixels, row_stride, channels, static_cast<cudaStream_t>(stream));
 }
@@ -660,14 +675,18 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
       row_stride < s->width * channels) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze_host: invalid arguments");
   }
-  const size_t bytes = row_stride * (s->height - 1) + s->width * channels;
-  if (bytes > s->pixel_capacity) {
-    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_analyze_host: row stride too large");
+  if (InjectFailure(kInjectSubmission)) {
+    return SetError(GJXL_B200_SUBMISSION_FAILED,
+                    "session_analyze_host: injected submission failure");
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->pixels, host_pixels, bytes, cudaMemcpyHostToDevice, st),
+  // Packed rows in the session's input buffer (one contiguous copy when the
+  // caller's rows are packed too).
+  const size_t packed_row = s->width * static_cast<size_t>(channels);
+  GJXL_TRY(CheckCuda(cudaMemcpy2DAsync(s->pixels, packed_row, host_pixels, row_stride,
+                                       packed_row, s->height, cudaMemcpyHostToDevice, st),
                      "session: input upload"));
-  GJXL_TRY(RunReplay(s, s->pixels, row_stride, channels, st));
+  GJXL_TRY(RunReplay(s, s->pixels, packed_row, channels, st));
   GJXL_TRY(CopyOutputs(s, st));
   s->host_token_count = 0;
   if (s->tokens != nullptr) {
@@ -688,7 +707,18 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
                        "session: token contexts"));
     s->host_token_count = total;
   }
-  return CheckCuda(cudaStreamSynchronize(st), "session: analysis");
+  GJXL_TRY(CheckCuda(cudaStreamSynchronize(st), "session: analysis"));
+  // A nonzero device error word fails the call, as the reference's
+  // ReadAndCheckDeviceError does (src/gpu/cuda/cuda_aq_resident.cpp:3451).
+  for (int i = 0; i < 3; ++i) {
+    if (s->host_error[i] != 0) {
+      return SetError(GJXL_B200_DEVICE_ERROR,
+                      i == 0   ? "session_analyze_host: analysis device error word is set"
+                      : i == 1 ? "session_analyze_host: Butteraugli device error word is set"
+                               : "session_analyze_host: tokenization device error word is set");
+    }
+  }
+  return GJXL_B200_OK;
 }
 
 extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_outputs* out) {
@@ -758,6 +788,9 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   }
   out->host_token_count = s->host_token_count;
   out->device_bytes = s->arena_bytes;
+  out->input_pixels = s->pixels;
+  out->input_capacity = s->pixel_capacity;
+  out->graph_replay = s->graph != nullptr ? 1 : 0;
   return GJXL_B200_OK;
 }
 

@@ -37,7 +37,8 @@ class Outputs(Structure):
         ("groups", c_size_t)] + [(n, c_void_p) for n in (
             "token_values", "token_contexts", "group_offsets", "token_histogram", "scans",
             "order_masks", "host_token_values", "host_token_contexts", "host_group_offsets")] + [
-        ("host_token_count", c_size_t), ("device_bytes", c_size_t)]
+        ("host_token_count", c_size_t), ("device_bytes", c_size_t),
+        ("input_pixels", c_void_p), ("input_capacity", c_size_t), ("graph_replay", c_int)]
 
 
 _BOUND = False
@@ -114,9 +115,12 @@ class AnalysisSession:
             pass
 
     def analyze(self, device_pixels_ptr: int, row_stride: int, channels: int, stream: int = 0):
-        _check(_lib.load().gjxl_b200_session_analyze(self.handle, device_pixels_ptr, row_stride,
-                                                     channels, stream),
+        lib = _lib.load()
+        _check(lib.gjxl_b200_session_analyze(self.handle, device_pixels_ptr, row_stride,
+                                             channels, stream),
                "gjxl_b200_session_analyze")
+        _check(lib.gjxl_b200_session_outputs(self.handle, ctypes.byref(self.outputs)),
+               "gjxl_b200_session_outputs")
 
     def kernel_count(self, device_pixels_ptr: int, row_stride: int, channels: int) -> int:
         """Kernels one analyze() call on these arguments launches (counted

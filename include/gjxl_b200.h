@@ -394,6 +394,13 @@ typedef struct gjxl_b200_outputs {
   const uint32_t* host_group_offsets;
   size_t host_token_count;
   size_t device_bytes;
+  /* The session's own input buffer (packed rows of width * channels bytes,
+   * input_capacity bytes): a device-resident caller that writes its image
+   * here and passes this pointer to gjxl_b200_session_analyze saves the
+   * input copy. */
+  uint8_t* input_pixels;
+  size_t input_capacity;
+  int graph_replay;                 /* 1 once analyses replay a captured graph */
 } gjxl_b200_outputs;
 
 typedef struct gjxl_b200_session gjxl_b200_session;
@@ -403,7 +410,12 @@ GJXL_B200_API int gjxl_b200_session_create(size_t width, size_t height,
                                            const gjxl_b200_options* options,
                                            gjxl_b200_session** session);
 GJXL_B200_API void gjxl_b200_session_destroy(gjxl_b200_session* session);
-/* Device-resident input: packed 8-bit sRGB already in device memory. */
+/* Device-resident input: packed 8-bit sRGB already in device memory. The
+ * first call for a channel count captures the analysis into a CUDA graph
+ * over the session's input buffer; later calls replay it. Input anywhere
+ * else is first copied into that buffer on `stream` (no recapture when the
+ * pointer changes). Asynchronous: read outputs.device_error (or call
+ * gjxl_b200_check_device_error) once the stream has completed. */
 GJXL_B200_API int gjxl_b200_session_analyze(gjxl_b200_session* session,
                                             const uint8_t* pixels,
                                             size_t row_stride_bytes,
@@ -411,7 +423,8 @@ GJXL_B200_API int gjxl_b200_session_analyze(gjxl_b200_session* session,
 /* Host input: one host-to-device copy of the packed pixels, the analysis,
  * and device-to-host copies of the results into the host mirrors. Returns
  * once the stream has completed and the mirrors are filled (the token count
- * is known only then). */
+ * is known only then); returns GJXL_B200_DEVICE_ERROR when a device error
+ * word is set. */
 GJXL_B200_API int gjxl_b200_session_analyze_host(gjxl_b200_session* session,
                                                  const uint8_t* host_pixels,
                                                  size_t row_stride_bytes,
@@ -443,6 +456,32 @@ GJXL_B200_API int gjxl_b200_session_kernel_count(gjxl_b200_session* session,
  */
 GJXL_B200_API int gjxl_b200_fp64_throughput(double* device_sink, double* ops_per_second,
                                             void* stream);
+
+/*
+ * Reads `words` device error words (1..64) once `stream` has completed and
+ * returns GJXL_B200_DEVICE_ERROR if any is nonzero. Replaces the reference's
+ * ReadAndCheckDeviceError (src/gpu/cuda/cuda_aq_resident.cpp:3451).
+ */
+GJXL_B200_API int gjxl_b200_check_device_error(const uint32_t* device_error, size_t words,
+                                               void* stream);
+
+/*
+ * Deterministic failure injection for tests, per calling thread. Replaces
+ * the reference's CudaBackendOptions::test_fail_submission and
+ * ArmNextCudaSubmissionFailureForTest (src/gpu/cuda/cuda_backend.h:19-21,60).
+ * Arms the `check_point`-th (1-based) next check point of `kind` to fail
+ * (0 disarms):
+ *   1 allocation: a device or pinned host allocation in session, Butteraugli
+ *     or token-handle creation fails with GJXL_B200_OUT_OF_MEMORY, and the
+ *     handle releases what it had allocated;
+ *   2 graph: the next graph instantiation fails; the session falls back to
+ *     launching its stages directly;
+ *   3 submission: the next session analysis fails with
+ *     GJXL_B200_SUBMISSION_FAILED before anything is enqueued, leaving
+ *     every output unchanged.
+ * Failures are made on the host; nothing faults on the device.
+ */
+GJXL_B200_API int gjxl_b200_test_arm_failure(int kind, int check_point);
 
 #ifdef __cplusplus
 }  /* extern "C" */

@@ -1,0 +1,508 @@
+// The binding a maintainer adds to the gjxl encoder to run its analysis half
+// on a B200 through libgjxl_b200, with the encoder's own CPU back half
+// (block-context and coefficient-order selection, DC tokenization, entropy
+// coding, bitstream assembly) left unchanged.
+//
+// It is compiled against the reference's headers and linked with the
+// reference's own codestream and codec sources (integration/Makefile), as it
+// would be inside the reference tree. Three pieces:
+//
+//  * ResolveEncodeOptions: the workflow's option resolution for one ordinary
+//    Butteraugli-target encode attempt (EncodePreparedAttempt,
+//    src/codestream/workflow.cpp:886-921 and :1069-1076), through the
+//    reference's own policy helpers, so the frame profile and serializer
+//    options are exactly the ones the CPU path would use.
+//  * AssembleB200Frame: a VarDctEncoderFrame from a session's results
+//    (strategy cells, raw quant field, quantizer, final CfL maps, quantized DC
+//    and AC), through the reference's AssembleVarDctEncoderFrame
+//    (src/codec/vardct_frame_internal.h:59), as the reference's CUDA path
+//    does with its readbacks (src/gpu/cuda/cuda_aq_resident.cpp:2785-2830).
+//  * B200AcTokenizer: an AcTokenizationProvider
+//    (src/codestream/ac_tokenization_provider_internal.h:20-31) that
+//    tokenizes the frame's AC on the device with gjxl_b200_ac_tokenize for the
+//    block-context map and coefficient orders the serializer chose, checks the
+//    device's scans against the serializer's, and hands back split token
+//    streams and the fixed-ANS populations.
+//
+// The C entry point gjxl_b200_encode_image runs a session on packed 8-bit
+// sRGB, assembles the frame, validates it (ValidateSimpleCodestreamFrame,
+// src/codec/codestream.h:87) and writes the codestream with
+// EncodeVarDctCodestreamToBuffer (src/codestream/encoder_internal.h:168).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <span>
+#include <string>
+#include <vector>
+
+#include "codec/codestream.h"
+#include "codec/epf.h"
+#include "codec/vardct_frame.h"
+#include "codec/vardct_frame_internal.h"
+#include "codec/vardct_frame_view_internal.h"
+#include "codestream/ac_tokenization_provider_internal.h"
+#include "codestream/encoder_internal.h"
+#include "codestream/workflow.h"
+#include "codestream/workflow_internal.h"
+#include "core/ac_strategy.h"
+#include "core/frame_geometry.h"
+#include "core/quantizer.h"
+#include "gjxl_b200.h"
+
+#define GJXL_INTEGRATION_API extern "C" __attribute__((visibility("default")))
+
+namespace gjxl::b200_integration {
+namespace {
+
+thread_local std::string g_last_error;
+
+int Fail(const Status& status) {
+  g_last_error = std::string(status.message());
+  const int code = static_cast<int>(status.code());
+  return code == 0 ? 8 : code;
+}
+
+Status FromB200(int code, const char* what) {
+  if (code == GJXL_B200_OK) return Status::Ok();
+  const std::string message = std::string(what) + ": " + gjxl_b200_last_error();
+  switch (code) {
+    case GJXL_B200_INVALID_ARGUMENT: return Status::InvalidArgument(message);
+    case GJXL_B200_UNSUPPORTED: return Status::Unsupported(message);
+    case GJXL_B200_UNAVAILABLE: return Status::Unavailable(message);
+    case GJXL_B200_OUT_OF_MEMORY: return Status::OutOfMemory(message);
+    case GJXL_B200_FAILED_PRECONDITION: return Status::FailedPrecondition(message);
+    case GJXL_B200_SUBMISSION_FAILED: return Status::SubmissionFailed(message);
+    case GJXL_B200_DEVICE_ERROR: return Status::DeviceError(message);
+    default: return Status::Internal(message);
+  }
+}
+
+Status FromCuda(cudaError_t error, const char* what) {
+  if (error == cudaSuccess) return Status::Ok();
+  return Status::DeviceError(std::string(what) + ": " + cudaGetErrorString(error));
+}
+
+// The pieces of one encode attempt's options that the frame and the
+// serializer depend on.
+struct ResolvedEncode {
+  CpuQuantizationPipelineOptions pipeline;
+  VarDctCodestreamOptions codestream;
+};
+
+// EncodePreparedAttempt's resolution (src/codestream/workflow.cpp:886-921),
+// through the reference's own helpers, for a Butteraugli-target encode.
+Status ResolveEncodeOptions(const VarDctEncodingOptions& options,
+                            const codestream_internal::QuantizationMatrixScaleStats& stats,
+                            ResolvedEncode* out) {
+  ResolvedEncode r;
+  codestream_internal::ConfigureInitialQuantizationPolicy(options, &r.pipeline);
+  r.pipeline.fixed_dct8 = codestream_internal::UseFixedDct8Strategy(options);
+  r.pipeline.dense_dct32_search = codestream_internal::UseDenseDct32Search(options);
+  r.pipeline.butteraugli_target = options.butteraugli_target;
+  auto& aq = r.pipeline.adaptive_quantization;
+  aq.iterations = codestream_internal::AdaptiveQuantizationIterations(options);
+  aq.coefficient_decision_mode = codestream_internal::ResolveAcCoefficientDecision(options);
+  aq.dc_quantization = ResolveDcQuantization(options);
+  aq.dc_prediction = options.dc_prediction;
+  aq.profile.extra_dc_precision =
+    ResolveDcQuantization(options) == DcQuantizationMode::kPredictionAware ? 1 : 0;
+  aq.profile.adaptive_dc_smoothing = ResolveAdaptiveDcSmoothing(options);
+  codestream_internal::QuantizationMatrixScales scales;
+  Status status = codestream_internal::SelectQuantizationMatrixScales(
+    codestream_internal::ShouldComputeQuantizationMatrixScaleStats(options)
+      ? stats : codestream_internal::QuantizationMatrixScaleStats{},
+    options.rate_control_mode, options.butteraugli_target, &scales);
+  if (!status.ok()) return status;
+  aq.profile.x_qm_scale = scales.x;
+  aq.profile.b_qm_scale = scales.b;
+  r.codestream = VarDctCodestreamOptions{
+    .entropy_behavior = codestream_internal::ResolveEntropyBehavior(options),
+    .coefficient_order_behavior = codestream_internal::ResolveCoefficientOrderBehavior(options),
+    .dc_prediction = options.dc_prediction,
+    .dc_uint_search = codestream_internal::UseDcUintSearch(options),
+  };
+  *out = std::move(r);
+  return Status::Ok();
+}
+
+// A session's results, read back to the host.
+struct SessionResults {
+  size_t width = 0, height = 0, pw = 0, ph = 0, bx = 0, by = 0, tx = 0, ty = 0;
+  std::vector<uint8_t> cells;
+  std::vector<int32_t> raw_quant;
+  uint32_t global_scale = 0, quant_dc = 0;
+  std::vector<int8_t> y_to_x, y_to_b;
+  std::vector<int32_t> quantized_dc;  // X, Y, B planes of blocks
+  std::vector<int32_t> quantized_ac;  // 3 padded planes, footprint layout
+  std::array<int, 2> device_matrix_scales{};
+  codestream_internal::QuantizationMatrixScaleStats stats;
+};
+
+Status ReadSession(const gjxl_b200_outputs& o, size_t width, size_t height,
+                   SessionResults* out) {
+  SessionResults r;
+  r.width = width;
+  r.height = height;
+  r.pw = o.padded_width;
+  r.ph = o.padded_height;
+  r.bx = o.blocks_x;
+  r.by = o.blocks_y;
+  r.tx = o.tiles_x;
+  r.ty = o.tiles_y;
+  const size_t blocks = r.bx * r.by, tiles = r.tx * r.ty, plane = r.pw * r.ph;
+  r.cells.assign(o.host_strategy_cells, o.host_strategy_cells + blocks);
+  r.raw_quant.assign(o.host_raw_quant_field, o.host_raw_quant_field + blocks);
+  r.global_scale = o.host_quantizer_params[0];
+  r.quant_dc = o.host_quantizer_params[1];
+  r.y_to_x.assign(o.host_y_to_x, o.host_y_to_x + tiles);
+  r.y_to_b.assign(o.host_y_to_b, o.host_y_to_b + tiles);
+  r.quantized_dc.assign(o.host_quantized_dc, o.host_quantized_dc + 3 * blocks);
+  r.stats.x_edge = o.host_matrix_scale_stats[0];
+  r.stats.b_edge = o.host_matrix_scale_stats[1];
+  r.stats.exposed_blue = o.host_matrix_scale_stats[2];
+  r.quantized_ac.resize(3 * plane);
+  Status status = FromCuda(cudaMemcpy(r.quantized_ac.data(), o.quantized_ac,
+                                      3 * plane * sizeof(int32_t), cudaMemcpyDeviceToHost),
+                           "quantized AC readback");
+  if (!status.ok()) return status;
+  status = FromCuda(cudaMemcpy(r.device_matrix_scales.data(), o.matrix_scales,
+                               2 * sizeof(int), cudaMemcpyDeviceToHost),
+                    "matrix scale readback");
+  if (!status.ok()) return status;
+  *out = std::move(r);
+  return Status::Ok();
+}
+
+// VarDctEncoderFrame from the session's results: the transforms in raster
+// anchor order (AcStrategyGrid::ForEachAnchor), each channel's N coefficients
+// gathered from their footprint (coefficient i at pixel
+// (bx*8 + i % W, by*8 + i / W)) into one contiguous run.
+Status AssembleB200Frame(const SessionResults& r, const SimpleVarDctCodestreamProfile& profile,
+                         VarDctEncoderFrame* frame) {
+  FrameGeometry geometry;
+  Status status = FrameGeometry::Create({r.width, r.height}, &geometry);
+  if (!status.ok()) return status;
+  AcStrategyGrid grid;
+  status = AcStrategyGrid::CreateFromEncodedCells({r.bx, r.by}, r.cells, &grid);
+  if (!status.ok()) return status;
+  Quantizer quantizer;
+  status = Quantizer::Create({.global_scale = r.global_scale, .quant_dc = r.quant_dc},
+                             &quantizer);
+  if (!status.ok()) return status;
+  std::vector<uint8_t> sharpness(r.bx * r.by);
+  status = FillDefaultEpfSharpness({sharpness.data(), {r.bx, r.by}, r.bx});
+  if (!status.ok()) return status;
+
+  std::vector<int32_t> ac;
+  ac.reserve(3 * r.pw * r.ph);
+  std::vector<vardct_frame_internal::QuantizedAcTransformLayout> transforms;
+  const size_t plane = r.pw * r.ph;
+  status = grid.ForEachAnchor([&](size_t x, size_t y, AcStrategyType strategy) {
+    const AcStrategyInfo* info = GetAcStrategyInfo(strategy);
+    if (info == nullptr) return Status::InvalidArgument("unknown strategy in the grid");
+    const size_t w = info->covered_blocks.width * 8, h = info->covered_blocks.height * 8;
+    if ((x * 8 + w) > r.pw || (y * 8 + h) > r.ph) {
+      return Status::InvalidArgument("transform footprint leaves the padded image");
+    }
+    vardct_frame_internal::QuantizedAcTransformLayout t;
+    t.block_x = x;
+    t.block_y = y;
+    t.strategy = strategy;
+    t.coefficient_count = w * h;
+    for (size_t c = 0; c < 3; ++c) {
+      t.coefficient_offsets[c] = ac.size();
+      for (size_t row = 0; row < h; ++row) {
+        const int32_t* src = r.quantized_ac.data() + c * plane + (y * 8 + row) * r.pw + x * 8;
+        ac.insert(ac.end(), src, src + w);
+      }
+    }
+    transforms.push_back(t);
+    return Status::Ok();
+  });
+  if (!status.ok()) return status;
+
+  ConstImage3I32View dc;
+  for (size_t c = 0; c < 3; ++c) {
+    dc.plane[c] = {r.quantized_dc.data() + c * r.bx * r.by, {r.bx, r.by}, r.bx};
+  }
+  status = vardct_frame_internal::AssembleVarDctEncoderFrame(
+    vardct_frame_internal::QuantizedFrameAssemblyInput{
+      .geometry = geometry,
+      .strategies = &grid,
+      .raw_quant_field = {r.raw_quant.data(), {r.bx, r.by}, r.bx},
+      .quantizer = &quantizer,
+      .y_to_x = {r.y_to_x.data(), {r.tx, r.ty}, r.tx},
+      .y_to_b = {r.y_to_b.data(), {r.tx, r.ty}, r.tx},
+      .epf_sharpness = {sharpness.data(), {r.bx, r.by}, r.bx},
+      .profile = profile,
+      .quantized_dc = dc,
+      .quantized_ac = std::span<const int32_t>(ac.data(), ac.size()),
+      .transforms = transforms,
+      .reject_unwritten_coefficients = false,
+    },
+    frame);
+  if (!status.ok()) return status;
+  return ValidateSimpleCodestreamFrame(*frame);
+}
+
+// Scan order families of the simple codestream (coefficient_order.h) and the
+// device tokenizer's order modes.
+int OrderMode(VarDctCoefficientOrderBehavior behavior) {
+  return behavior == VarDctCoefficientOrderBehavior::kEffort7Dct8Sampled ? 2 : 1;
+}
+
+// AC tokens of the session's frame computed on the device for the block
+// context map and coefficient orders the serializer hands to Begin.
+class B200AcTokenizer final : public codestream_internal::AcTokenizationProvider {
+ public:
+  B200AcTokenizer(const gjxl_b200_outputs& outputs, VarDctCoefficientOrderBehavior behavior)
+      : o_(outputs), order_mode_(OrderMode(behavior)) {}
+
+  ~B200AcTokenizer() override {
+    if (tokens_ != nullptr) gjxl_b200_ac_tokens_destroy(tokens_);
+    if (device_ != nullptr) cudaFree(device_);
+  }
+
+  // The serializer overlaps its DC tokenization with Begin..Finish.
+  bool SupportsEarlyEntropy() const noexcept override { return false; }
+
+  Status Begin(const vardct_frame_internal::VarDctFrameView& frame,
+               const SimpleCoefficientOrders& orders,
+               const codestream_internal::SimpleAcNaturalOrders& natural,
+               const SimpleBlockContextMap& contexts, bool populations) override {
+    (void)frame;
+    (void)natural;
+    if (contexts.num_contexts == 0 || contexts.num_contexts > 16 ||
+        contexts.qf_thresholds.size() > 15 ||
+        contexts.context_map.size() != 3 * 13 * (contexts.qf_thresholds.size() + 1)) {
+      return Status::Unsupported("block-context map outside the device tokenizer's range");
+    }
+    std::memset(&map_, 0, sizeof(map_));
+    map_.threshold_count = static_cast<uint32_t>(contexts.qf_thresholds.size());
+    std::copy(contexts.qf_thresholds.begin(), contexts.qf_thresholds.end(), map_.qf_thresholds);
+    map_.num_contexts = contexts.num_contexts;
+    std::copy(contexts.context_map.begin(), contexts.context_map.end(), map_.context_map);
+    context_count_ = contexts.ac_context_count();
+    populations_ = populations;
+    // Natural scans when the serializer chose no custom order.
+    const int mode = orders.used_order_mask == 0 ? 0 : order_mode_;
+    expected_used_mask_ = orders.used_order_mask;
+    expected_orders_ = &orders;
+
+    const size_t groups = o_.groups;
+    capacity_ = gjxl_b200_ac_token_capacity(o_.blocks_x, o_.blocks_y);
+    Status status = FromB200(gjxl_b200_ac_tokens_create(o_.blocks_x, o_.blocks_y, &tokens_),
+                             "ac_tokens_create");
+    if (!status.ok()) return status;
+    const size_t histogram_words = context_count_ * 128;
+    offsets_bytes_ = Align((groups + 1) * 4);
+    const size_t bytes = capacity_ * 4 + Align(capacity_ * 2) + offsets_bytes_ +
+                         histogram_words * 4 + 13 * 3 * 1024 * 4 + 16;
+    status = FromCuda(cudaMalloc(&device_, Align(capacity_ * 4) + bytes), "token buffers");
+    if (!status.ok()) return status;
+    unsigned char* p = static_cast<unsigned char*>(device_);
+    auto take = [&](size_t n) {
+      unsigned char* r = p;
+      p += Align(n);
+      return r;
+    };
+    gjxl_b200_ac_token_outputs outs;
+    std::memset(&outs, 0, sizeof(outs));
+    outs.token_values = reinterpret_cast<uint32_t*>(take(capacity_ * 4));
+    outs.token_contexts = reinterpret_cast<uint16_t*>(take(capacity_ * 2));
+    outs.token_capacity = capacity_;
+    outs.group_offsets = reinterpret_cast<uint32_t*>(take((groups + 1) * 4));
+    outs.histogram = reinterpret_cast<uint32_t*>(take(histogram_words * 4));
+    outs.orders = reinterpret_cast<uint32_t*>(take(13 * 3 * 1024 * 4));
+    outs.used_order_mask = reinterpret_cast<uint32_t*>(take(4));
+    outs.device_error = reinterpret_cast<uint32_t*>(take(4));
+    outs_ = outs;
+    status = FromCuda(cudaMemset(outs.device_error, 0, 4), "token error word");
+    if (!status.ok()) return status;
+    return FromB200(gjxl_b200_ac_tokenize(tokens_, o_.strategy_cells, o_.raw_quant_field,
+                                          o_.quantized_ac, o_.padded_width,
+                                          o_.padded_width * o_.padded_height, &map_, mode,
+                                          &outs_, nullptr),
+                    "ac_tokenize");
+  }
+
+  Status Finish(codestream_internal::Storage<EntropyTokenStreamView>* streams,
+                codestream_internal::Storage<codestream_internal::PreparedFixedAnsCluster>*
+                  populations) override {
+    if (tokens_ == nullptr || streams == nullptr || populations == nullptr) {
+      return Status::FailedPrecondition("Finish without a device tokenization");
+    }
+    Status status = FromB200(gjxl_b200_check_device_error(outs_.device_error, 1, nullptr),
+                             "device tokenization");
+    if (!status.ok()) return status;
+    const size_t groups = o_.groups;
+    std::vector<uint32_t> offsets(groups + 1);
+    status = FromCuda(cudaMemcpy(offsets.data(), outs_.group_offsets, (groups + 1) * 4,
+                                 cudaMemcpyDeviceToHost), "group offsets");
+    if (!status.ok()) return status;
+    const size_t total = offsets[groups];
+    if (total > capacity_) return Status::Internal("device token count exceeds its capacity");
+    values_.resize(total);
+    contexts_.resize(total);
+    status = FromCuda(cudaMemcpy(values_.data(), outs_.token_values, total * 4,
+                                 cudaMemcpyDeviceToHost), "token values");
+    if (status.ok()) {
+      status = FromCuda(cudaMemcpy(contexts_.data(), outs_.token_contexts, total * 2,
+                                   cudaMemcpyDeviceToHost), "token contexts");
+    }
+    if (!status.ok()) return status;
+    // The device scans must be the serializer's (same counts, same sort).
+    uint32_t used = 0;
+    std::vector<uint32_t> scans(13 * 3 * 1024);
+    status = FromCuda(cudaMemcpy(&used, outs_.used_order_mask, 4, cudaMemcpyDeviceToHost),
+                      "used order mask");
+    if (status.ok()) {
+      status = FromCuda(cudaMemcpy(scans.data(), outs_.orders, scans.size() * 4,
+                                   cudaMemcpyDeviceToHost), "scans");
+    }
+    if (!status.ok()) return status;
+    if (used != expected_used_mask_) {
+      return Status::Internal("device coefficient orders differ from the serializer's");
+    }
+    for (size_t family = 0; family < 13; ++family) {
+      if (!(used & (1u << family))) continue;
+      for (size_t c = 0; c < 3; ++c) {
+        const auto& want = expected_orders_->orders[family][c];
+        if (!std::equal(want.begin(), want.end(), scans.begin() + (family * 3 + c) * 1024)) {
+          return Status::Internal("device coefficient scan differs from the serializer's");
+        }
+      }
+    }
+    codestream_internal::Storage<EntropyTokenStreamView> result;
+    result.reserve(groups);
+    for (size_t g = 0; g < groups; ++g) {
+      const size_t begin = offsets[g], count = offsets[g + 1] - offsets[g];
+      result.push_back(EntropyTokenStreamView::Split({values_.data() + begin, count},
+                                                     {contexts_.data() + begin, count}));
+    }
+    codestream_internal::Storage<codestream_internal::PreparedFixedAnsCluster> reduced;
+    if (populations_) {
+      std::vector<uint32_t> histogram(context_count_ * 128);
+      status = FromCuda(cudaMemcpy(histogram.data(), outs_.histogram, histogram.size() * 4,
+                                   cudaMemcpyDeviceToHost), "token histogram");
+      if (!status.ok()) return status;
+      reduced.resize(context_count_);
+      uint64_t counted = 0;
+      for (size_t context = 0; context < context_count_; ++context) {
+        auto& cluster = reduced[context];
+        for (uint32_t symbol = 0; symbol < 128; ++symbol) {
+          const uint64_t n = histogram[context * 128 + symbol];
+          cluster.counts[symbol] = n;
+          cluster.token_count += n;
+          if (n != 0) cluster.maximum_symbol = symbol;
+          // Hybrid-uint tokens from 16 up carry 2 + (token - 16) / 4 raw bits
+          // (the default 4/2/0 split of the JPEG XL entropy coder).
+          if (symbol >= 16) cluster.extra_bits += n * (2 + ((symbol - 16) >> 2));
+        }
+        counted += cluster.token_count;
+      }
+      if (counted != total) return Status::Internal("token populations differ from the count");
+    }
+    *streams = std::move(result);
+    *populations = std::move(reduced);
+    return Status::Ok();
+  }
+
+ private:
+  static size_t Align(size_t n) { return (n + 255) / 256 * 256; }
+
+  gjxl_b200_outputs o_;
+  int order_mode_;
+  gjxl_b200_block_context_map map_{};
+  size_t context_count_ = 0;
+  bool populations_ = false;
+  uint16_t expected_used_mask_ = 0;
+  const SimpleCoefficientOrders* expected_orders_ = nullptr;
+  gjxl_b200_ac_tokens* tokens_ = nullptr;
+  void* device_ = nullptr;
+  size_t capacity_ = 0, offsets_bytes_ = 0;
+  gjxl_b200_ac_token_outputs outs_{};
+  std::vector<uint32_t> values_;
+  std::vector<uint16_t> contexts_;
+};
+
+}  // namespace
+}  // namespace gjxl::b200_integration
+
+using namespace gjxl;
+using namespace gjxl::b200_integration;
+
+GJXL_INTEGRATION_API const char* gjxl_b200_integration_last_error(void) {
+  return g_last_error.c_str();
+}
+
+// Encodes packed 8-bit sRGB (3 or 4 channels) at the given distance and
+// effort: the analysis half on the B200 (one session on the current device,
+// default stream), the serializer on the CPU. device_tokens != 0 installs the
+// device AC tokenizer. Writes the codestream (size in *size, -2 when it does
+// not fit `capacity`) and the session's final Butteraugli score.
+GJXL_INTEGRATION_API int gjxl_b200_encode_image(const uint8_t* pixels, size_t width,
+                                                size_t height, size_t row_stride, int channels,
+                                                float butteraugli_target, int effort,
+                                                int device_tokens, uint8_t* out,
+                                                size_t capacity, size_t* size, double* score) {
+  g_last_error.clear();
+  VarDctEncodingOptions options;
+  options.butteraugli_target = butteraugli_target;
+  options.effort = effort;
+  gjxl_b200_options session_options;
+  gjxl_b200_default_options(&session_options);
+  session_options.butteraugli_target = butteraugli_target;
+  session_options.effort = effort;
+  session_options.tokenize = 0;  // the serializer asks for its own map's tokens
+  gjxl_b200_session* session = nullptr;
+  Status status = FromB200(gjxl_b200_session_create(width, height, &session_options, &session),
+                           "session_create");
+  if (!status.ok()) return Fail(status);
+  std::unique_ptr<gjxl_b200_session, void (*)(gjxl_b200_session*)> owner(
+    session, gjxl_b200_session_destroy);
+  status = FromB200(gjxl_b200_session_analyze_host(session, pixels, row_stride, channels,
+                                                   nullptr),
+                    "session_analyze_host");
+  if (!status.ok()) return Fail(status);
+  gjxl_b200_outputs o;
+  status = FromB200(gjxl_b200_session_outputs(session, &o), "session_outputs");
+  if (!status.ok()) return Fail(status);
+  SessionResults results;
+  status = ReadSession(o, width, height, &results);
+  if (!status.ok()) return Fail(status);
+  ResolvedEncode resolved;
+  status = ResolveEncodeOptions(options, results.stats, &resolved);
+  if (!status.ok()) return Fail(status);
+  const auto& profile = resolved.pipeline.adaptive_quantization.profile;
+  if (results.device_matrix_scales[0] != profile.x_qm_scale ||
+      results.device_matrix_scales[1] != profile.b_qm_scale) {
+    return Fail(Status::Internal("device quantization-matrix scales differ from the workflow's"));
+  }
+  VarDctEncoderFrame frame;
+  status = AssembleB200Frame(results, profile, &frame);
+  if (!status.ok()) return Fail(status);
+  std::unique_ptr<B200AcTokenizer> tokenizer;
+  if (device_tokens) {
+    tokenizer = std::make_unique<B200AcTokenizer>(o, resolved.codestream.coefficient_order_behavior);
+  }
+  codestream_internal::CodestreamBuffer buffer;
+  {
+    codestream_internal::AcTokenizationProviderScope scope(tokenizer.get());
+    status = codestream_internal::EncodeVarDctCodestreamToBuffer(
+      vardct_frame_internal::BorrowFrame(frame), resolved.codestream, &buffer);
+  }
+  if (!status.ok()) return Fail(status);
+  *size = buffer.size();
+  if (score != nullptr) *score = o.host_score_history[o.iterations];
+  if (buffer.size() > capacity) {
+    g_last_error = "codestream capacity exceeded";
+    return -2;
+  }
+  std::memcpy(out, buffer.data(), buffer.size());
+  return 0;
+}

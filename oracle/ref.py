@@ -28,6 +28,9 @@ _SIGNATURES = {
     "gjxl_ref_butteraugli": [_P, _P, _Z, _Z, _F, _P, _P],
     "gjxl_ref_quant_matrix": [_I, _I, _P, _P, _Z],
     "gjxl_ref_ac_strategy_cost_table": [_P, _Z, _Z, _P, _P, _P, _P, _F, _I, _P],
+    "gjxl_ref_matrix_scale_stats": [_P, _Z, _Z, _Z, _Z, _P],
+    "gjxl_ref_select_matrix_scales": [_P, _F, _P],
+    "gjxl_ref_encode_cpu": [_P, _Z, _Z, _F, _I, _P, _Z, _P, _P],
 }
 
 _lib = None
@@ -104,6 +107,43 @@ def opsin_to_linear(opsin: np.ndarray, intensity_target: float = 255.0) -> np.nd
     _check(lib().gjxl_ref_opsin_to_linear(_ptr(opsin), w, h, intensity_target, _ptr(out)),
            "opsin_to_linear")
     return out
+
+
+def matrix_scale_stats(opsin: np.ndarray, width: int, height: int) -> np.ndarray:
+    """ComputeQuantizationMatrixScaleStatsFromFiniteOpsin
+    (src/codestream/workflow.cpp:1318) over the unpadded region:
+    [x_edge, b_edge, exposed_blue]."""
+    opsin = np.ascontiguousarray(opsin, np.float32)
+    _, ph, pw = opsin.shape
+    out = np.empty(3, np.float32)
+    _check(lib().gjxl_ref_matrix_scale_stats(_ptr(opsin), pw, ph, width, height, _ptr(out)),
+           "matrix_scale_stats")
+    return out
+
+
+def select_matrix_scales(stats: np.ndarray, target: float) -> tuple[int, int]:
+    """SelectQuantizationMatrixScales (src/codestream/workflow.cpp:1435) for a
+    Butteraugli-target encode: (x_qm_scale, b_qm_scale)."""
+    stats = np.ascontiguousarray(stats, np.float32)
+    out = np.zeros(2, np.int32)
+    _check(lib().gjxl_ref_select_matrix_scales(_ptr(stats), target, _ptr(out)),
+           "select_matrix_scales")
+    return int(out[0]), int(out[1])
+
+
+def encode_cpu(linear: np.ndarray, target: float = 1.0, effort: int = 7) -> tuple[bytes, float]:
+    """The reference's whole CPU encode (EncodeLinearRgbVarDctCodestream,
+    src/codestream/workflow.h:281): (codestream bytes, final Butteraugli
+    score)."""
+    linear = np.ascontiguousarray(linear, np.float32)
+    _, h, w = linear.shape
+    capacity = max(1 << 16, 4 * w * h)
+    out = np.empty(capacity, np.uint8)
+    size = c_size_t(0)
+    score = c_double(0.0)
+    _check(lib().gjxl_ref_encode_cpu(_ptr(linear), w, h, target, effort, _ptr(out), capacity,
+                                     ctypes.byref(size), ctypes.byref(score)), "encode_cpu")
+    return out[:size.value].tobytes(), score.value
 
 
 def initial_quant_field(opsin: np.ndarray, target: float = 1.0, rescale: float = 1.0,

@@ -37,6 +37,8 @@
 #include "codestream/block_context_map.h"
 #include "codestream/coefficient_order.h"
 #include "codestream/encoder.h"
+#include "codestream/workflow.h"
+#include "codestream/workflow_internal.h"
 #include "codec/vardct_frame_view_internal.h"
 #include "core/ac_strategy.h"
 #include "core/image.h"
@@ -601,3 +603,70 @@ GJXL_REF_API int gjxl_ref_pipeline_tokens(
                      x_qm_scale, b_qm_scale, out, tokens);
 }
 
+
+// codestream/workflow.cpp:1318 ComputeQuantizationMatrixScaleStatsFromFiniteOpsin
+// over the unpadded width x height region of the padded opsin image, as the
+// workflow calls it (workflow.cpp:719-724, cropped_view of the frame).
+// Writes {x_edge, b_edge, exposed_blue}.
+GJXL_REF_API int gjxl_ref_matrix_scale_stats(const float* opsin, size_t padded_width,
+                                             size_t padded_height, size_t width,
+                                             size_t height, float* stats) {
+  ConstImage3FView view;
+  for (size_t c = 0; c < 3; ++c) {
+    view.plane[c] = {opsin + c * padded_width * padded_height, {width, height},
+                     padded_width};
+  }
+  codestream_internal::QuantizationMatrixScaleStats out;
+  Status status =
+    codestream_internal::ComputeQuantizationMatrixScaleStatsFromFiniteOpsin(view, &out);
+  if (!status.ok()) return Fail(status);
+  stats[0] = out.x_edge;
+  stats[1] = out.b_edge;
+  stats[2] = out.exposed_blue;
+  return 0;
+}
+
+// codestream/workflow.cpp:1435 SelectQuantizationMatrixScales for a
+// Butteraugli-target encode. Writes {x, b}.
+GJXL_REF_API int gjxl_ref_select_matrix_scales(const float* stats, float target,
+                                               int* scales) {
+  codestream_internal::QuantizationMatrixScaleStats in;
+  in.x_edge = stats[0];
+  in.b_edge = stats[1];
+  in.exposed_blue = stats[2];
+  codestream_internal::QuantizationMatrixScales out;
+  Status status = codestream_internal::SelectQuantizationMatrixScales(
+    in, VarDctRateControlMode::kButteraugliTarget, target, &out);
+  if (!status.ok()) return Fail(status);
+  scales[0] = out.x;
+  scales[1] = out.b;
+  return 0;
+}
+
+// The whole reference encode on the CPU backend
+// (codestream/workflow.h:281 EncodeLinearRgbVarDctCodestream): analysis,
+// tokenization, entropy coding and bitstream assembly. Writes the codestream
+// into `out` (capacity bytes), its size into *size and the final Butteraugli
+// score into *score. Returns -2 when the capacity is too small.
+GJXL_REF_API int gjxl_ref_encode_cpu(const float* linear, size_t width, size_t height,
+                                     float target, int effort, uint8_t* out,
+                                     size_t capacity, size_t* size, double* score) {
+  VarDctEncodingOptions options;
+  options.butteraugli_target = target;
+  options.effort = effort;
+  options.backend = VarDctBackendPreference::kCpu;
+  options.cpu_thread_count = g_threads;
+  std::vector<uint8_t> bytes;
+  VarDctEncodingSummary summary;
+  Status status = EncodeLinearRgbVarDctCodestream(ConstPlanar(linear, width, height), options,
+                                                  &bytes, &summary);
+  if (!status.ok()) return Fail(status);
+  *size = bytes.size();
+  *score = summary.score_history.empty() ? 0.0 : summary.score_history.back();
+  if (bytes.size() > capacity) {
+    g_last_error = "codestream capacity exceeded";
+    return -2;
+  }
+  std::memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}

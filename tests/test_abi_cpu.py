@@ -34,3 +34,26 @@ def test_version_and_error_string_work_without_gpu():
     lib = _lib.load()
     assert lib.gjxl_b200_version() >= 100
     assert lib.gjxl_b200_last_error() is not None
+
+
+def test_failure_injection_arming_is_validated_without_gpu():
+    """gjxl_b200_test_arm_failure is host-only: valid kinds arm and disarm,
+    unknown kinds and negative check points are rejected."""
+    lib = _lib.load()
+    for kind in (1, 2, 3):
+        assert lib.gjxl_b200_test_arm_failure(kind, 0) == 0
+    assert lib.gjxl_b200_test_arm_failure(0, 1) == 1
+    assert lib.gjxl_b200_test_arm_failure(4, 1) == 1
+    assert lib.gjxl_b200_test_arm_failure(1, -1) == 1
+
+
+def test_integration_binding_loads_without_gpu():
+    """The reference-side binding (integration/, built with the reference's
+    sources when they are present) loads and exports its entry points."""
+    import pytest
+    path = HEADER.parent.parent / "integration" / "_build" / "libgjxl_b200_encoder.so"
+    if not path.exists():
+        pytest.skip("integration binding not built (reference sources absent)")
+    lib = ctypes.CDLL(str(path))
+    assert hasattr(lib, "gjxl_b200_encode_image")
+    assert hasattr(lib, "gjxl_b200_integration_last_error")

@@ -1,0 +1,93 @@
+"""Codestreams from B200 analysis through the reference's unchanged CPU back
+half (integration/b200_encoder.cpp): the session's results are assembled into
+the reference's VarDctEncoderFrame, validated by its
+ValidateSimpleCodestreamFrame (src/codec/codestream.h:87) and serialized by
+its EncodeVarDctCodestreamToBuffer (src/codestream/encoder_internal.h:168),
+with the CPU AC tokenizer or the device one installed as the
+AcTokenizationProvider (src/codestream/ac_tokenization_provider_internal.h).
+
+Checks, against the reference's whole CPU encode of the same image
+(EncodeLinearRgbVarDctCodestream, src/codestream/workflow.h:281):
+* the device tokenizer gives the same codestream bytes as the CPU one;
+* where the analysis is bit-exact (one evaluation, effort 5) the codestream
+  is byte-identical to the reference's;
+* with field updates (effort 7) the codestream is byte-identical or its size
+  and final Butteraugli distance are within 0.2% of the reference's.
+No decoder is available here; the reference's frame validation and byte
+identity with its own CPU codestream stand in for decoding."""
+
+import ctypes
+from ctypes import c_double, c_float, c_int, c_size_t, c_void_p
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gjxl_b200.synthetic import generate_srgb8, workload_seed
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+LIBRARY = Path(__file__).resolve().parent.parent / "integration" / "_build" / \
+    "libgjxl_b200_encoder.so"
+
+
+def encoder() -> ctypes.CDLL:
+    if not LIBRARY.exists():
+        pytest.fail(f"{LIBRARY} is missing: build it with `make -C integration`")
+    lib = ctypes.CDLL(str(LIBRARY))
+    lib.gjxl_b200_encode_image.argtypes = [c_void_p, c_size_t, c_size_t, c_size_t, c_int,
+                                           c_float, c_int, c_int, c_void_p, c_size_t,
+                                           ctypes.POINTER(c_size_t), ctypes.POINTER(c_double)]
+    lib.gjxl_b200_encode_image.restype = c_int
+    lib.gjxl_b200_integration_last_error.restype = ctypes.c_char_p
+    return lib
+
+
+def b200_encode(img: np.ndarray, target: float, effort: int, device_tokens: bool):
+    import torch  # noqa: F401  (initializes the CUDA context on cuda:0)
+    lib = encoder()
+    img = np.ascontiguousarray(img)
+    h, w, ch = img.shape
+    capacity = max(1 << 16, 4 * w * h)
+    out = np.empty(capacity, np.uint8)
+    size, score = c_size_t(0), c_double(0.0)
+    rc = lib.gjxl_b200_encode_image(img.ctypes.data, w, h, w * ch, ch, target, effort,
+                                    int(device_tokens), out.ctypes.data, capacity,
+                                    ctypes.byref(size), ctypes.byref(score))
+    assert rc == 0, lib.gjxl_b200_integration_last_error().decode()
+    return out[:size.value].tobytes(), score.value
+
+
+def check_against_reference(img, target, effort, exact_required):
+    ours, score = b200_encode(img, target, effort, device_tokens=False)
+    ours_device, score_device = b200_encode(img, target, effort, device_tokens=True)
+    assert ours_device == ours, "device AC tokens changed the codestream"
+    assert score_device == score
+    want, want_score = ref.encode_cpu(ref.srgb8_to_linear(img), target, effort)
+    assert ours[:2] == b"\xff\x0a"  # JPEG XL codestream signature
+    if ours == want:
+        return "identical"
+    assert not exact_required, (f"codestream differs from the reference: {len(ours)} vs "
+                                f"{len(want)} bytes")
+    size_rel = abs(len(ours) - len(want)) / len(want)
+    assert size_rel <= 2e-3, f"size {len(ours)} vs {len(want)} bytes ({size_rel:.3%})"
+    assert abs(score - want_score) <= 2e-3 * want_score, (score, want_score)
+    return f"size within {size_rel:.3%}"
+
+
+@pytest.mark.parametrize("w,h,seed", [(256, 256, 77), (509, 261, 4509), (64, 40, 9)])
+def test_single_evaluation_codestream_is_byte_identical(cuda, w, h, seed):
+    check_against_reference(generate_srgb8(w, h, seed), 1.0, 5, exact_required=True)
+
+
+@pytest.mark.parametrize("w,h,seed", [(512, 512, workload_seed(1, 0)), (1000, 700, 5000),
+                                      (300, 200, 23)])
+def test_effort7_codestream_matches_reference(cuda, w, h, seed):
+    check_against_reference(generate_srgb8(w, h, seed), 1.0, 7, exact_required=False)
+
+
+@pytest.mark.parametrize("target,effort", [(0.5, 6), (3.0, 7), (2.0, 8)])
+def test_other_distances_and_efforts(cuda, target, effort):
+    check_against_reference(generate_srgb8(384, 256, 100 + effort), target, effort,
+                            exact_required=False)

@@ -29,3 +29,47 @@ def test_matrix_scale_selection_thresholds():
     assert restate.select_matrix_scales(np.array([0, 0, 0], np.float32), 1.0) == (3, 2)
     assert restate.select_matrix_scales(np.array([0.03, 0.4, 0.2], np.float32), 1.0) == (5, 5)
     assert restate.select_matrix_scales(np.array([0.016, 0.3, 0.0], np.float32), 3.0) == (4, 2)
+
+
+@pytest.mark.parametrize("w,h,seed,noise", [(2, 2, 5, False), (1, 9, 6, False), (9, 1, 7, False),
+                                            (509, 261, 4509, False), (256, 256, 77, True),
+                                            (333, 200, 91, True)])
+def test_restated_matrix_scale_stats_match_reference(w, h, seed, noise):
+    """The restated statistics (the CUDA path's OpsinMatrixScaleStatsKernel
+    semantics) equal the reference's own
+    ComputeQuantizationMatrixScaleStatsFromFiniteOpsin
+    (src/codestream/workflow.cpp:1318) bit for bit, over the unpadded region
+    of the padded opsin image (including 1-pixel-wide images, which have no
+    statistics)."""
+    img = generate_srgb8(max(w, 2), max(h, 2), seed, sensor_noise=noise)[:h, :w]
+    opsin = ref.linear_to_padded_opsin(ref.srgb8_to_linear(img))
+    want = ref.matrix_scale_stats(opsin, w, h)
+    got = restate.matrix_scale_stats(opsin, w, h)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (got, want)
+
+
+def test_restated_matrix_scale_selection_matches_reference():
+    """SelectQuantizationMatrixScales (src/codestream/workflow.cpp:1435) over
+    a grid that crosses every threshold (x_edge 0.015/0.022/0.026, b_edge
+    0.28/0.33/0.38, exposed blue 0.13, target 2.5/5.5/9.5), each threshold
+    probed at the float just below, at, and just above it."""
+    def around(values):
+        out = [0.0]
+        for v in values:
+            f = np.float32(v)
+            out += [np.nextafter(f, np.float32(0)), f, np.nextafter(f, np.float32(1))]
+        return out
+    xs = around([0.015, 0.022, 0.026])
+    bs = around([0.28, 0.33, 0.38])
+    es = around([0.13])
+    targets = [0.5, 1.0, 2.5, 2.6, 5.5, 6.0, 9.5, 12.0]
+    checked = 0
+    for x in xs:
+        for b in bs:
+            for e in es:
+                stats = np.array([x, b, e], np.float32)
+                for t in targets:
+                    assert restate.select_matrix_scales(stats, t) == \
+                        ref.select_matrix_scales(stats, t), (stats, t)
+                    checked += 1
+    assert checked == len(xs) * len(bs) * len(es) * len(targets)

@@ -16,16 +16,20 @@ computes the correctly rounded power; check_block_distance proves that every
 difference is such a case. With field updates (efforts 6-10) a block distance
 feeds the next field, so such a case can move single field values by an ulp:
 there the quantizer must match exactly and at most 0.1% of blocks may differ,
-and runs where nothing differs are then held to the bit-exact comparison."""
+and runs where nothing differs are then held to the bit-exact comparison.
+The same 0.1% rule covers a strategy grid that differs in a near-tie (a
+1-ulp candidate cost); the loop outputs are then compared block by block
+against the reference's own grid, never skipped."""
 
 import ctypes
+import os
 
 import numpy as np
 import pytest
 import torch
 
 from gjxl_b200.session import AnalysisSession
-from gjxl_b200.synthetic import generate_srgb8
+from gjxl_b200.synthetic import generate_srgb8, workload_seed
 from gpu_util import (STRATEGY_COVERED, assert_bitexact, device_to_host, differing_blocks,
                       footprint_to_group_order, group_order_to_footprint)
 from oracle import ref, restate
@@ -105,10 +109,12 @@ def reference(img: np.ndarray, effort: int = 7, target: float = 1.0):
     h, w, _ = img.shape
     lin = ref.srgb8_to_linear(img)
     opsin = ref.linear_to_padded_opsin(lin)
-    stats = restate.matrix_scale_stats(opsin, w, h)
-    # Below effort 7 the statistics are not gathered and select from zeros.
-    xs, bs = restate.select_matrix_scales(stats if effort >= 7 else np.zeros(3, np.float32),
-                                          target)
+    # The reference's own statistics and scale selection
+    # (src/codestream/workflow.cpp:1318,1435). Below effort 7 the statistics
+    # are not gathered and the selection starts from zeros.
+    stats = ref.matrix_scale_stats(opsin, w, h)
+    xs, bs = ref.select_matrix_scales(stats if effort >= 7 else np.zeros(3, np.float32),
+                                      target)
     return opsin, stats, ref.pipeline_tokens(lin, opsin, target, effort, xs, bs,
                                              ref.SIMPLE_BLOCK_CONTEXT_MAP,
                                              2 if effort == 7 else 1)
@@ -120,18 +126,19 @@ def device_quantized_ac(s: AnalysisSession) -> np.ndarray:
 
 
 def compare_front_half(s: AnalysisSession, got: dict, want: dict, stats: np.ndarray,
-                       effort: int) -> None:
+                       effort: int) -> bool:
+    """Initial field and matrix statistics bit for bit; the strategy grid
+    within 0.1% of blocks (a 1-ulp candidate cost can flip a near-tie).
+    Returns whether the grids are equal."""
     o = s.outputs
     assert_bitexact(got["initial_quant"], want["initial_quant"], "initial quant field")
     if effort >= 7:  # gathered from effort 7 on
         host_stats = np.ctypeslib.as_array(
             ctypes.cast(o.host_matrix_scale_stats, ctypes.POINTER(ctypes.c_float)), shape=(3,))
         assert_bitexact(host_stats.copy(), stats, "matrix scale stats")
-    # The strategy search may differ in at most 0.1% of blocks (1-ulp FP64
-    # cost differences); the evaluation loop is compared when it agrees.
-    assert (got["cells"] != want["cells"]).sum() <= 0.001 * got["cells"].size
-    if not np.array_equal(got["cells"], want["cells"]):
-        pytest.skip("strategy grid differs in a tie; loop outputs not comparable")
+    grid = differing_blocks(got["cells"], want["cells"])
+    assert grid.sum() <= 0.001 * grid.size, f"strategy grid: {grid.sum()} blocks differ"
+    return not grid.any()
 
 
 def compare_loop_exact(s: AnalysisSession, got: dict, want: dict) -> None:
@@ -162,25 +169,30 @@ def compare_loop_exact(s: AnalysisSession, got: dict, want: dict) -> None:
 
 
 def compare_loop_fed_back(s: AnalysisSession, got: dict, want: dict) -> int:
-    """Several evaluations: block distances feed the field updates, so a glibc
-    powf rounding case may move single field values by an ulp. The quantizer
-    must match exactly and at most 0.1% of blocks may differ in any output;
-    returns the number of differing blocks."""
-    by, bx = got["cells"].shape
+    """Several evaluations (or a grid that differs in a near-tie): block
+    distances feed the field updates, so a glibc powf rounding case may move
+    single field values by an ulp. The quantizer must match exactly and at
+    most 0.1% of blocks may differ in any block output (strategy, final field,
+    raw quant, quantized DC, quantized AC), each side's AC placed by its own
+    grid; the Butteraugli score history agrees within 0.2%. Returns the number
+    of differing blocks."""
     assert_bitexact(got["quantizer_params"], want["quantizer_params"], "quantizer params")
-    field_rel = np.abs(got["final_quant"].astype(np.float64) - want["final_quant"]) / want[
-        "final_quant"]
-    assert field_rel.max() <= 5e-7, f"final field differs by up to {field_rel.max():.3g}"
-    bad = (differing_blocks(got["final_quant"], want["final_quant"])
+    same_grid = np.array_equal(got["cells"], want["cells"])
+    if same_grid:
+        field_rel = np.abs(got["final_quant"].astype(np.float64) - want["final_quant"]) / want[
+            "final_quant"]
+        assert field_rel.max() <= 5e-7, f"final field differs by up to {field_rel.max():.3g}"
+    bad = (differing_blocks(got["cells"], want["cells"])
+           | differing_blocks(got["final_quant"], want["final_quant"])
            | differing_blocks(got["raw_quant"], want["raw_quant"])
            | differing_blocks(got["quantized_dc"], want["quantized_dc"])
            | differing_blocks(device_quantized_ac(s),
-                              group_order_to_footprint(want["ac"], got["cells"]), pixels=True))
+                              group_order_to_footprint(want["ac"], want["cells"]), pixels=True))
     cfl = differing_blocks(got["y_to_x"], want["y_to_x"]) | differing_blocks(got["y_to_b"],
                                                                                  want["y_to_b"])
     assert bad.sum() <= 0.001 * bad.size, f"{bad.sum()} of {bad.size} blocks differ"
     assert cfl.sum() <= max(1, 0.01 * cfl.size), f"{cfl.sum()} CfL tiles differ"
-    np.testing.assert_allclose(got["score_history"], want["score_history"], rtol=5e-3)
+    np.testing.assert_allclose(got["score_history"], want["score_history"], rtol=2e-3)
     return int(bad.sum())
 
 
@@ -197,8 +209,10 @@ def test_session_single_evaluation_bitexact(cuda, w, h, seed):
     assert s.host_error() == 0
     got = s.host_results()
     _, stats, want = reference(img, effort=5)
-    compare_front_half(s, got, want, stats, 5)
-    compare_loop_exact(s, got, want)
+    if compare_front_half(s, got, want, stats, 5):
+        compare_loop_exact(s, got, want)
+    else:
+        compare_loop_fed_back(s, got, want)
     s.close()
 
 
@@ -210,8 +224,43 @@ def test_session_matches_reference(cuda, w, h, seed):
     assert s.host_error() == 0
     got = s.host_results()
     _, stats, want = reference(img)
-    compare_front_half(s, got, want, stats, 7)
-    if compare_loop_fed_back(s, got, want) == 0:
+    same_grid = compare_front_half(s, got, want, stats, 7)
+    if compare_loop_fed_back(s, got, want) == 0 and same_grid:
+        compare_loop_exact(s, got, want)
+    s.close()
+
+
+def test_session_c1_512(cuda):
+    """The first configuration: one 512x512 image of the seeded generator
+    (configuration 1, image 0) at distance 1.0, effort 7, full analysis and
+    tokenization, against the reference CPU pipeline and tokenizer."""
+    img = generate_srgb8(512, 512, workload_seed(1, 0))
+    s = run_session(img)
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference(img)
+    same_grid = compare_front_half(s, got, want, stats, 7)
+    if compare_loop_fed_back(s, got, want) == 0 and same_grid:
+        compare_loop_exact(s, got, want)
+    s.close()
+
+
+def test_session_benchmarked_image_full_size(cuda):
+    """The benchmarked workload itself: 4032x3024 with Gaussian sensor noise
+    (configuration 2, image 0), distance 1.0, effort 7, against the
+    reference CPU pipeline on the same image (a few minutes of host time).
+    Front half bit-exact except the grid (<= 0.1% of blocks), quantizer
+    exact, every block output within 0.1% of blocks, score history within
+    0.2%, and the tokens bit-exact when the loop agrees."""
+    from oracle import ref as oracle_ref
+    oracle_ref.set_threads(os.cpu_count() or 1)
+    img = generate_srgb8(4032, 3024, workload_seed(2, 0), sensor_noise=True)
+    s = run_session(img)
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference(img)
+    same_grid = compare_front_half(s, got, want, stats, 7)
+    if compare_loop_fed_back(s, got, want) == 0 and same_grid:
         compare_loop_exact(s, got, want)
     s.close()
 
@@ -226,8 +275,8 @@ def test_session_iterations_by_effort(cuda, effort):
     got = s.host_results()
     _, stats, want = reference(img, effort=effort)
     assert got["score_history"].shape == want["score_history"].shape
-    compare_front_half(s, got, want, stats, effort)
-    if compare_loop_fed_back(s, got, want) == 0:
+    same_grid = compare_front_half(s, got, want, stats, effort)
+    if compare_loop_fed_back(s, got, want) == 0 and same_grid:
         compare_loop_exact(s, got, want)
     s.close()
 

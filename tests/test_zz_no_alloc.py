@@ -2,8 +2,9 @@
 device allocation) against gjxl_b200_initial_quant_field (caller scratch),
 called through the C ABI. Two calls in a row on different images and extents
 must each match the caller-scratch results bit for bit, so scratch left over
-from the first call cannot leak into the second; sizes beyond the static
-scratch are rejected."""
+from the first call cannot leak into the second; a call takes no device
+memory (free device memory is the same before and after it); sizes beyond
+the static scratch are rejected."""
 
 import numpy as np
 import pytest
@@ -77,3 +78,27 @@ def test_noalloc_rejects_extent_beyond_static_scratch(cuda):
                   1.0, 1.0, q.data_ptr(), m.data_ptr(), pm.data_ptr(), pw, err.data_ptr(),
                   stream_ptr())
     assert info.value.code == 1 and "16 MiB" in str(info.value)
+
+
+def test_noalloc_call_takes_no_device_memory(cuda):
+    """After a warm-up call (which loads the library's module and with it the
+    static scratch), a call on another extent leaves the device's free memory
+    exactly where it was: the entry point allocates nothing."""
+    warm = padded_opsin(128, 96, 74)
+    run(warm, 1.0, noalloc=True)
+    w, h = 700, 500
+    opsin_np = padded_opsin(w, h, 75)
+    _, ph, pw = opsin_np.shape
+    opsin = to_device(opsin_np)
+    q, m, pm, err = outputs(pw, ph)
+    torch.cuda.synchronize()
+    before = torch.cuda.mem_get_info()[0]
+    _lib.call("gjxl_b200_initial_quant_field_noalloc", opsin.data_ptr(), pw, ph * pw, pw, ph,
+              1.0, 1.0, q.data_ptr(), m.data_ptr(), pm.data_ptr(), pw, err.data_ptr(),
+              stream_ptr())
+    torch.cuda.synchronize()
+    after = torch.cuda.mem_get_info()[0]
+    assert after == before, f"free device memory changed by {before - after} bytes"
+    want = run(opsin_np, 1.0, noalloc=False)
+    assert_bitexact(host(q), want[0], "quant_field")
+    assert int(host(err)[0]) == 0
