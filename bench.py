@@ -211,8 +211,9 @@ def run_gpu(args) -> dict:
     torch.cuda.set_device(local)
     img = make_image()
     count = 1 if args.launch_list else max(1, args.sessions)
-    sessions = [AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7)
-                for _ in range(count)]
+    precision = 1 if args.precision == "fast" else 0
+    sessions = [AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7,
+                                precision=precision) for _ in range(count)]
     session = sessions[0]
     main_stream = torch.cuda.current_stream()
     stream = main_stream.cuda_stream
@@ -308,7 +309,8 @@ def run_gpu(args) -> dict:
 
     # Per-stage times and the dominant kernel's roofline (separate session so
     # the timed region above carries no event records).
-    prof = AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7, profile_stages=True)
+    prof = AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7, profile_stages=True,
+                           precision=precision)
     stage_ms = {}
     reps = max(3, min(args.steps, 10))
     for _ in range(reps):
@@ -330,7 +332,7 @@ def run_gpu(args) -> dict:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded generator, no dataset)",
         "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "distance": 1.0,
-                   "effort": 7, "seed": SEED,
+                   "effort": 7, "seed": SEED, "precision": args.precision,
                    "parallelism": f"replicas x{world}, {count} concurrent sessions per GPU",
                    "l2": "working set (~0.6 GB of planes) exceeds the 126 MB L2"},
         "e2e": {"value": round(world * mp / (e2e_ms / 1e3), 3), "unit": "MP/s",
@@ -470,6 +472,9 @@ def main():
                         help="analysis sessions (images in flight) per GPU")
     parser.add_argument("--size", default=None,
                         help="WxH of a smaller image of the same generator (profiling only)")
+    parser.add_argument("--precision", default="exact", choices=["exact", "fast"],
+                        help="candidate-cost precision: exact (FP64, the reference's CPU "
+                             "results bit for bit) or fast (tcgen05 tensor cores)")
     args = parser.parse_args()
     if args.size:
         global WIDTH, HEIGHT

@@ -31,8 +31,8 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_quant_matrix": [I, I, P, P, Z],
     "gjxl_b200_ac_strategy_cost_bytes": [Z, Z],
-    "gjxl_b200_ac_strategy_costs": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P],
-    "gjxl_b200_ac_strategy_search": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, P, P, P, P],
+    "gjxl_b200_ac_strategy_costs": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, I, P, P, P],
+    "gjxl_b200_ac_strategy_search": [P, Z, Z, Z, Z, P, P, Z, P, P, F, I, I, P, P, P, P],
     "gjxl_b200_butteraugli_create": [Z, Z, F, P],
     "gjxl_b200_butteraugli_destroy": None,
     "gjxl_b200_butteraugli_prepare": [P, P, Z, Z, P],

@@ -24,14 +24,18 @@
 // order-dependent float sums (magnitude cost, pixel loss) are done by one
 // thread per (candidate, channel) in the reference's order.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+
+#include <cuda_bf16.h>
 
 #include "common.cuh"
 #include "host_util.h"
 #include "fan.h"
 #include "line_dct.cuh"
 #include "tables.h"
+#include "umma.cuh"
 
 namespace gjxl_b200 {
 namespace {
@@ -92,7 +96,7 @@ struct Shape {
 // consecutive columns both hit distinct banks.
 constexpr int kCostThreads = 384;
 
-template <int W, int H>
+template <int W, int H, typename Acc = double>
 struct CostLayout {
   static constexpr int N = W * H, K = 1024 / N, KC = 3 * K;
   using Batch = PlaneBatch<W, H, KC>;
@@ -106,10 +110,10 @@ struct CostLayout {
   static constexpr int TermPitch = N + 4;
   // Families with a length-32 side read that pass's basis from a shared copy
   // (the forward table through the forward passes, then the inverse table).
-  static constexpr bool kStagedBasis = W == 32 || H == 32;
+  static constexpr bool kStagedBasis = (W == 32 || H == 32) && sizeof(Acc) == 8;
   static constexpr int BasisDoubles = kStagedBasis ? 32 * 32 : 0;
   static constexpr size_t SharedBytes = static_cast<size_t>(BasisDoubles) * 8 +
-                                        static_cast<size_t>(Planes) * (4 + 4 + 8) +
+                                        static_cast<size_t>(Planes) * (4 + 4 + sizeof(Acc)) +
                                         static_cast<size_t>(KC) * TermPitch * 4;
   static_assert(K * N <= Planes, "the pixel mask fits the residual buffer");
   static_assert(Batch::Items == kCostThreads, "one chunk per thread and pass");
@@ -135,16 +139,72 @@ __device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
   return v <= 1 ? 0 : 32 - __clz(v - 1);
 }
 
-template <int W, int H>
+// ComputeQuantNormUnchecked (ac_strategy.cpp:103-130) over the covered
+// blocks of the transform anchored at (ax, ay).
+template <int CW, int CH>
+__device__ __forceinline__ float QuantNorm(const CostParams& p, int ax, int ay) {
+  const float* q = p.quant_field;
+  if (CW * CH == 1) return q[ay * p.blocks_x + ax];
+  if (CW * CH == 2) {
+    return CH == 2 ? fmaxf(q[ay * p.blocks_x + ax], q[(ay + 1) * p.blocks_x + ax])
+                   : fmaxf(q[ay * p.blocks_x + ax], q[ay * p.blocks_x + ax + 1]);
+  }
+  float sum = 0.0f;
+  for (int dy = 0; dy < CH; ++dy) {
+    for (int dx = 0; dx < CW; ++dx) {
+      float v = q[(ay + dy) * p.blocks_x + ax + dx];
+      v *= v;
+      v *= v;
+      v *= v;
+      sum += v * v;
+    }
+  }
+  sum /= static_cast<float>(CW * CH);
+  return FastPow2(FastLog2(sum) * (1.0f / 16.0f));
+}
+
+// The candidate's cost from its per-channel magnitude sums, nonzero counts
+// and weighted-loss sums (EstimateAcStrategyCost, ac_strategy.cpp:960-994).
+template <int N, int kBlocks>
+__device__ __forceinline__ float CandidateCost(const CostParams& p, const float (&magnitude)[3],
+                                               const uint32_t (&nonzero)[3],
+                                               const float (&loss_sum)[3], float quant_norm) {
+  const float kChannelMultiplier[3] = {2.0441408586549744e7f, 1.0f, 1.266770081387616f};
+  float entropy = 0.0f, loss = 0.0f;
+  for (int c = 0; c < 3; ++c) {
+    loss += loss_sum[c] * kChannelMultiplier[c];
+    entropy += p.cost_delta * magnitude[c];
+    const int nonzero_bits = CeilLog2Nonzero(nonzero[c] + 1) + 1;
+    entropy += p.zeros_multiplier *
+               static_cast<float>(CeilLog2Nonzero(nonzero_bits + 17) + nonzero_bits);
+    if (c == 0 && kBlocks >= 2) {
+      const float weight = 1.0f + fminf(3.0f, static_cast<float>(kBlocks) / 8.0f);
+      entropy *= weight;
+      loss *= weight;
+    }
+  }
+  const float normalized_loss = loss / static_cast<float>(N);
+  // std::pow(float, 1/8): evaluated in double and rounded to float.
+  const float root = static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125));
+  const float loss_cost = root * static_cast<float>(N) / quant_norm;
+  return entropy * p.entropy_multiplier + p.info_loss_multiplier * loss_cost;
+}
+
+// Acc = double: the bit-exact restatement (FP64 products, separately
+// rounded, sequential sums). Acc = float: the fast mode's FP32 passes for the
+// 8-pixel families (fused multiply-adds on the bases rounded to float).
+template <int W, int H, typename Acc>
 __global__ void __launch_bounds__(kCostThreads, 3)
 CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_count) {
   using S = Shape<W, H>;
-  using Lay = CostLayout<W, H>;
+  using Lay = CostLayout<W, H, Acc>;
+  constexpr bool kExact = sizeof(Acc) == 8;
   constexpr int N = S::N, K = Lay::K, KC = Lay::KC;
   static_assert(K == S::K, "candidates per CTA");
+  static_assert(kExact || (W <= 16 && H <= 16), "FP32 passes cover lengths 8 and 16");
   extern __shared__ __align__(16) unsigned char smem[];
   double* basis = reinterpret_cast<double*>(smem);         // [32][32] staged length-32 basis
-  double* T = basis + Lay::BasisDoubles;                   // [KC][H][W+1] row-pass results
+  Acc* T = reinterpret_cast<Acc*>(basis + Lay::BasisDoubles);  // [KC][H][W+1] row-pass results
   float* A = reinterpret_cast<float*>(T + Lay::Planes);    // [KC][H][W+1] pixels, residuals
   float* B = A + Lay::Planes;                              // [KC][H][W+1] coefficients, pixels
   float* terms = B + Lay::Planes;                          // [KC][N + 4] ordered sum terms
@@ -208,27 +268,7 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     // factors, while the loads above are in flight.
     if (tid < K && anchor_x[tid] >= 0) {
       const int ax = anchor_x[tid], ay = anchor_y[tid];
-      const float* q = p.quant_field;
-      float qn;
-      if (S::CW * S::CH == 1) {
-        qn = q[ay * p.blocks_x + ax];
-      } else if (S::CW * S::CH == 2) {
-        qn = S::CH == 2 ? fmaxf(q[ay * p.blocks_x + ax], q[(ay + 1) * p.blocks_x + ax])
-                        : fmaxf(q[ay * p.blocks_x + ax], q[ay * p.blocks_x + ax + 1]);
-      } else {
-        float sum = 0.0f;
-        for (int dy = 0; dy < S::CH; ++dy) {
-          for (int dx = 0; dx < S::CW; ++dx) {
-            float v = q[(ay + dy) * p.blocks_x + ax + dx];
-            v *= v;
-            v *= v;
-            v *= v;
-            sum += v * v;
-          }
-        }
-        sum /= static_cast<float>(S::CW * S::CH);
-        qn = FastPow2(FastLog2(sum) * (1.0f / 16.0f));
-      }
+      const float qn = QuantNorm<S::CW, S::CH>(p, ax, ay);
       if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
       quant_norm[tid] = qn;
       const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
@@ -254,9 +294,15 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   // Forward DCT (ForwardDctCpu): rows into T, then columns into B.
   const auto present = [&](int plane) { return anchor_x[plane / 3] >= 0; };
   const double* staged = Lay::kStagedBasis ? basis : nullptr;
-  BatchRowPass<W, H, KC, true>(A, T, tid, kCostThreads, present, staged);
-  __syncthreads();
-  BatchColumnPass<W, H, KC, true>(T, B, tid, kCostThreads, present, staged);
+  if constexpr (kExact) {
+    BatchRowPass<W, H, KC, true>(A, T, tid, kCostThreads, present, staged);
+    __syncthreads();
+    BatchColumnPass<W, H, KC, true>(T, B, tid, kCostThreads, present, staged);
+  } else {
+    BatchRowPassF<W, H, KC, true>(A, T, tid, kCostThreads, present);
+    __syncthreads();
+    BatchColumnPassF<W, H, KC, true>(T, B, tid, kCostThreads, present);
+  }
   __syncthreads();
 
   // Quantize, coefficient j = coefficient_index(v, u) by coefficient:
@@ -328,14 +374,22 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
 
   // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
-  BatchRowPass<W, H, KC, false>(A, T, tid, kCostThreads, present, staged);
+  if constexpr (kExact) {
+    BatchRowPass<W, H, KC, false>(A, T, tid, kCostThreads, present, staged);
+  } else {
+    BatchRowPassF<W, H, KC, false>(A, T, tid, kCostThreads, present);
+  }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < kMaskLoads; ++q) {
     const int i = tid + q * kCostThreads;
     if (i < K * N && anchor_x[i / N] >= 0) mask[i] = pmask[q];
   }
-  BatchColumnPass<W, H, KC, false>(T, B, tid, kCostThreads, present, staged);
+  if constexpr (kExact) {
+    BatchColumnPass<W, H, KC, false>(T, B, tid, kCostThreads, present, staged);
+  } else {
+    BatchColumnPassF<W, H, KC, false>(T, B, tid, kCostThreads, present);
+  }
   __syncthreads();
 
   // Weighted eighth powers in pixel order.
@@ -359,30 +413,464 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   __syncthreads();
 
   if (tid < K && anchor_x[tid] >= 0) {
-    const float kChannelMultiplier[3] = {2.0441408586549744e7f, 1.0f, 1.266770081387616f};
-    float entropy = 0.0f, loss = 0.0f;
-    for (int c = 0; c < 3; ++c) {
-      loss += loss_sum[tid][c] * kChannelMultiplier[c];
-      entropy += p.cost_delta * magnitude[tid][c];
-      const int nonzero_bits = CeilLog2Nonzero(nonzero[tid][c] + 1) + 1;
-      entropy += p.zeros_multiplier *
-                 static_cast<float>(CeilLog2Nonzero(nonzero_bits + 17) + nonzero_bits);
-      constexpr int block_count = S::CW * S::CH;
-      if (c == 0 && block_count >= 2) {
-        const float weight = 1.0f + fminf(3.0f, static_cast<float>(block_count) / 8.0f);
-        entropy *= weight;
-        loss *= weight;
-      }
-    }
-    const float normalized_loss = loss / static_cast<float>(N);
-    // std::pow(float, 1/8): evaluated in double and rounded to float.
-    const float root = static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125));
-    const float loss_cost = root * static_cast<float>(N) / quant_norm[tid];
-    const float result =
-      entropy * p.entropy_multiplier + p.info_loss_multiplier * loss_cost;
+    const float mag[3] = {magnitude[tid][0], magnitude[tid][1], magnitude[tid][2]};
+    const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
+    const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
+    const float result = CandidateCost<N, S::CW * S::CH>(p, mag, nz, ls, quant_norm[tid]);
     if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
     p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core candidate costs (the fast precision mode) for the families
+// whose sides are 16 or 32 pixels.
+//
+// The same cost as CandidateCostKernel, with the four separable transform
+// passes as tcgen05 MMAs (bf16 operands, f32 accumulation in tensor memory)
+// instead of FP64 products. Every operand is split into three bf16 pieces
+// (x = hi + mid + lo, each the bf16 rounding of what remains), and every
+// product is the sum of the six piece products whose orders of magnitude
+// reach 2^-24 of the leading one (hi*hi, hi*mid, mid*hi, hi*lo, mid*mid,
+// lo*hi): the split-bf16 form of an FP32 product. The CfL subtraction is
+// applied to the pixels before the forward transform (the transform is
+// linear, so this equals the reference's subtraction of the luma
+// coefficients up to rounding), and every channel is then independent.
+//
+// Work unit: G = 128 / min(W, H) candidates, one channel at a time, so that
+// each pass is one or two M = 128 tiles. Rows and operand layouts per pass
+// (P pixels, T row-pass result, C coefficients, R quantized residual, E
+// pixel error; u/v horizontal/vertical frequency, x/y pixel):
+//   1  rows (cand, y)  K = x   N = u   A K-major    from the staged pixels
+//   2  rows (cand, u)  K = y   N = v   A MN-major   (written from pass 1)
+//   3  rows (cand, v)  K = u   N = x   A MN-major   (written from pass 2)
+//   4  rows (cand, x)  K = v   N = y   A MN-major   (written from pass 3)
+// A thread owns one accumulator row (tensor-memory lane) per tile and writes
+// its row's values as 16-byte runs of the next operand: the transposes
+// between passes are absorbed by the MN-major operand mode.
+
+constexpr int kTcThreads = 128;
+constexpr int kTcSplits = 3;
+constexpr int kTcProducts = 6;
+__device__ constexpr int kTcProductA[kTcProducts] = {0, 0, 1, 0, 1, 2};
+__device__ constexpr int kTcProductB[kTcProducts] = {0, 1, 0, 2, 1, 0};
+constexpr uint32_t kTcWaitPolls = 1u << 22;
+
+template <int W, int H>
+struct TcLayout {
+  static constexpr int N = W * H;
+  static constexpr int G = 128 / (W < H ? W : H);  // candidates per unit
+  static constexpr int R1 = G * H, R2 = G * W;      // rows of passes 1/3 and 2/4
+  static constexpr int T1 = R1 / 128, T2 = R2 / 128;
+  static constexpr int kOperandBytes = G * N * 2;   // one bf16 piece of one A operand
+  static constexpr int kSquare = W == H;
+  // Basis tables (B operands, K-major [n / 8][k / 8][8][8] bf16): forward and
+  // inverse for the width, and for the height unless the family is square.
+  static constexpr int kTableBytesW = W * W * 2, kTableBytesH = H * H * 2;
+  static constexpr int kTablesBytes =
+    kTcSplits * 2 * (kTableBytesW + (kSquare ? 0 : kTableBytesH));
+  // Quantization weights {inverse, dequant} of the family, [channel][v][u].
+  static constexpr int kWeightsBytes = 3 * N * 8;
+  // One operand buffer serves all four passes: pass k's operand is dead once
+  // its MMA completed, before the epilogue writes pass k + 1's operand.
+  static constexpr size_t SharedBytes = static_cast<size_t>(kTcSplits) * kOperandBytes +
+                                        kTablesBytes + kWeightsBytes;
+  static constexpr uint32_t kTmemColumns = 32;
+  static_assert(T1 * W <= 32 && T2 * H <= 32, "every pass accumulates within 32 columns");
+  static_assert(R1 % 128 == 0 && R2 % 128 == 0, "whole M = 128 tiles");
+};
+
+// Square root of a nonnegative float by the hardware approximation (within
+// 2 ulp); the fast mode's magnitude terms sqrt|q| of integer-valued q.
+__device__ __forceinline__ float ApproxSqrt(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Splits 8 floats into three bf16 pieces and stores each piece's 16 bytes
+// at piece_base[s] + offset.
+__device__ __forceinline__ void StoreSplit8(const float (&v)[8], unsigned char* const (&base)[3],
+                                            int offset) {
+  uint32_t hi[4], mid[4], lo[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    const float r0 = v[2 * i] - __low2float(h), r1 = v[2 * i + 1] - __high2float(h);
+    const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - __low2float(m), r1 - __high2float(m));
+    hi[i] = *reinterpret_cast<const uint32_t*>(&h);
+    mid[i] = *reinterpret_cast<const uint32_t*>(&m);
+    lo[i] = *reinterpret_cast<const uint32_t*>(&l);
+  }
+  *reinterpret_cast<uint4*>(base[0] + offset) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  *reinterpret_cast<uint4*>(base[1] + offset) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
+  *reinterpret_cast<uint4*>(base[2] + offset) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// Byte offset of element (n, k) in a K-major [n / 8][k / 8][8][8] bf16 table.
+template <int K>
+__device__ __forceinline__ int KMajorOffset(int n, int k) {
+  return (n >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
+}
+
+// One table of L x L basis values (from the exact double tables) in its three
+// bf16 pieces: element (n, k) = forward[n * L + k] (frequency n, sample k) or
+// inverse[k * L + n] (frequency k, sample n).
+template <int L, bool kForward>
+__device__ void StageBasis(unsigned char* table, int tid) {
+  for (int i = tid; i < L * L; i += kTcThreads) {
+    const int n = i / L, k = i % L;
+    const double value = kForward ? DctBasis<L, true>(n * L + k) : DctBasis<L, false>(k * L + n);
+    const __nv_bfloat16 hi = __double2bfloat16(value);
+    const double r1 = value - static_cast<double>(__bfloat162float(hi));
+    const __nv_bfloat16 mid = __double2bfloat16(r1);
+    const double r2 = r1 - static_cast<double>(__bfloat162float(mid));
+    const __nv_bfloat16 lo = __double2bfloat16(r2);
+    const int at = KMajorOffset<L>(n, k);
+    *reinterpret_cast<__nv_bfloat16*>(table + at) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(table + L * L * 2 + at) = mid;
+    *reinterpret_cast<__nv_bfloat16*>(table + 2 * L * L * 2 + at) = lo;
+  }
+}
+
+// Issues the six piece products of one pass over `tiles` M = 128 tiles and
+// `kchunks` K = 16 chunks, then commits to `barrier` (one thread).
+__device__ __forceinline__ void IssuePass(uint32_t tmem, int n_out, int tiles, int kchunks,
+                                          uint32_t a_base, int a_piece_bytes, int a_tile_bytes,
+                                          int a_kchunk_bytes, uint32_t a_lbo, uint32_t a_sbo,
+                                          bool a_mn_major, uint32_t b_base, int b_piece_bytes,
+                                          uint32_t b_sbo, uint64_t* barrier) {
+  const uint32_t instr = umma::InstrBf16F32(128, n_out, a_mn_major, false);
+  for (int tile = 0; tile < tiles; ++tile) {
+    for (int kc = 0; kc < kchunks; ++kc) {
+#pragma unroll
+      for (int q = 0; q < kTcProducts; ++q) {
+        const uint64_t a = umma::Descriptor(
+          a_base + kTcProductA[q] * a_piece_bytes + tile * a_tile_bytes + kc * a_kchunk_bytes,
+          a_lbo, a_sbo);
+        const uint64_t b =
+          umma::Descriptor(b_base + kTcProductB[q] * b_piece_bytes + kc * 256, 128, b_sbo);
+        umma::Mma(tmem + tile * n_out, a, b, instr, kc > 0 || q > 0);
+      }
+    }
+  }
+  umma::Commit(barrier);
+}
+
+template <int W, int H>
+__global__ void __launch_bounds__(kTcThreads)
+CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_count) {
+  using S = Shape<W, H>;
+  using L = TcLayout<W, H>;
+  constexpr int N = S::N, G = L::G, R1 = L::R1, R2 = L::R2, T1 = L::T1, T2 = L::T2;
+  extern __shared__ __align__(128) unsigned char tc_smem[];
+  unsigned char* operand = tc_smem;                          // A1..A4, three pieces
+  unsigned char* tables = tc_smem + kTcSplits * L::kOperandBytes;
+  float2* weights = reinterpret_cast<float2*>(tables + L::kTablesBytes);
+  unsigned char* fwdW = tables;
+  unsigned char* invW = fwdW + kTcSplits * L::kTableBytesW;
+  unsigned char* fwdH = L::kSquare ? fwdW : invW + kTcSplits * L::kTableBytesW;
+  unsigned char* invH = L::kSquare ? invW : fwdH + kTcSplits * L::kTableBytesH;
+  __shared__ __align__(8) uint64_t barrier;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int anchor_x[G], anchor_y[G];
+  __shared__ float quant_norm[G], cfl[G][3];
+  __shared__ float magnitude[G][3], loss_sum[G][3];
+  __shared__ uint32_t nonzero[G][3];
+  __shared__ int aborted;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) umma::Allocate(&tmem_slot, L::kTmemColumns);
+  if (tid == 0) {
+    umma::InitBarrier(&barrier, 1);
+    aborted = 0;
+  }
+  StageBasis<W, true>(fwdW, tid);
+  StageBasis<W, false>(invW, tid);
+  if constexpr (!L::kSquare) {
+    StageBasis<H, true>(fwdH, tid);
+    StageBasis<H, false>(invH, tid);
+  }
+  // The quantization weights, [c][v][u]: the threads of one epilogue row
+  // group (consecutive u) read consecutive words.
+  for (int i = tid; i < 3 * N; i += kTcThreads) {
+    const int c = i / N, v = (i % N) / W, u = i % W;
+    const int index = c * N + S::Index(v, u);
+    weights[i] = make_float2(__ldg(p.inverse_dequant + index), __ldg(p.dequant + index));
+  }
+  umma::FenceBeforeSync();
+  __syncthreads();
+  umma::FenceAfterSync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+  uint32_t phase = 0;
+  unsigned char* const pieces[3] = {operand, operand + L::kOperandBytes,
+                                     operand + 2 * L::kOperandBytes};
+  const uint32_t address = umma::SmemAddress(operand);
+  // Leading (K) byte offsets of the MN-major operands.
+  constexpr uint32_t kLbo2 = (R2 / 8) * 128, kLbo3 = (R1 / 8) * 128, kLbo4 = (R2 / 8) * 128;
+
+  // Waits for the pass just committed. A timeout in any thread stops the
+  // whole CTA (the decision is CTA-uniform, so no thread is left at a
+  // barrier the others skip).
+  const auto wait_pass = [&]() -> bool {
+    const bool ok = umma::WaitParity(&barrier, phase, kTcWaitPolls);
+    phase ^= 1u;
+    umma::FenceAfterSync();
+    const bool all = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!all && tid == 0) {
+      aborted = 1;
+      RaiseError(p.error, kErrorInternal);
+    }
+    return all;
+  };
+  // Makes this thread's operand writes visible to the tensor core and lines
+  // the CTA up before one thread issues the next pass.
+  const auto operands_ready = [&]() {
+    umma::FenceAsyncShared();
+    umma::FenceBeforeSync();
+    __syncthreads();
+    umma::FenceAfterSync();
+  };
+
+  const uint32_t units = (candidate_count + G - 1) / G;
+  for (uint32_t unit = blockIdx.x; unit < units && !aborted; unit += gridDim.x) {
+    if (tid < G) {
+      const uint32_t cand = unit * G + tid;
+      int ax = -1, ay = -1;
+      if (cand < candidate_count) {
+        const uint32_t per_tile = p.local_x * p.local_y;
+        const uint32_t tile = cand / per_tile, local = cand % per_tile;
+        const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+        const int lx = (local % p.local_x) * p.anchor_step;
+        const int ly = (local / p.local_x) * p.anchor_step;
+        const int tile_w = min(8, static_cast<int>(p.blocks_x) - tx * 8);
+        const int tile_h = min(8, static_cast<int>(p.blocks_y) - ty * 8);
+        if (lx + S::CW <= tile_w && ly + S::CH <= tile_h) {
+          ax = tx * 8 + lx;
+          ay = ty * 8 + ly;
+        }
+      }
+      anchor_x[tid] = ax;
+      anchor_y[tid] = ay;
+      float qn = 1.0f;
+      if (ax >= 0) {
+        qn = QuantNorm<S::CW, S::CH>(p, ax, ay);
+        if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
+        const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
+        cfl[tid][0] = static_cast<float>(p.y_to_x[tile_index]) / 84.0f;
+        cfl[tid][1] = 0.0f;
+        cfl[tid][2] = 1.0f + static_cast<float>(p.y_to_b[tile_index]) / 84.0f;
+      }
+      quant_norm[tid] = qn;
+      for (int c = 0; c < 3; ++c) {
+        magnitude[tid][c] = 0.0f;
+        loss_sum[tid][c] = 0.0f;
+        nonzero[tid][c] = 0;
+      }
+    }
+    __syncthreads();
+
+    for (int c = 0; c < 3 && !aborted; ++c) {
+      // Stage: rows (cand, y) of the decorrelated pixels, K-major.
+#pragma unroll
+      for (int i = 0; i < T1; ++i) {
+        const int r = i * 128 + tid, cand = r / H, y = r % H;
+        const int ax = anchor_x[cand], ay = anchor_y[cand];
+        float row[W];
+        if (ax >= 0) {
+          const size_t at = static_cast<size_t>(ay * 8 + y) * p.stride + ax * 8;
+          const float4* src = reinterpret_cast<const float4*>(p.opsin + c * p.pitch + at);
+#pragma unroll
+          for (int q = 0; q < W / 4; ++q) {
+            const float4 v = src[q];
+            row[4 * q] = v.x;
+            row[4 * q + 1] = v.y;
+            row[4 * q + 2] = v.z;
+            row[4 * q + 3] = v.w;
+          }
+          if (c != 1) {
+            const float4* luma = reinterpret_cast<const float4*>(p.opsin + p.pitch + at);
+            const float f = cfl[cand][c];
+#pragma unroll
+            for (int q = 0; q < W / 4; ++q) {
+              const float4 v = luma[q];
+              row[4 * q] = fmaf(-f, v.x, row[4 * q]);
+              row[4 * q + 1] = fmaf(-f, v.y, row[4 * q + 1]);
+              row[4 * q + 2] = fmaf(-f, v.z, row[4 * q + 2]);
+              row[4 * q + 3] = fmaf(-f, v.w, row[4 * q + 3]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int x = 0; x < W; ++x) row[x] = 0.0f;
+        }
+#pragma unroll
+        for (int g = 0; g < W / 8; ++g) {
+          float v[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[j] = row[g * 8 + j];
+          StoreSplit8(v, pieces, KMajorOffset<W>(r, g * 8));
+        }
+      }
+      operands_ready();
+      // Pass 1: forward row transform.
+      if (tid == 0) {
+        IssuePass(tmem, W, T1, W / 16, address, L::kOperandBytes, 16 * (W / 8) * 128, 256, 128,
+                  (W / 8) * 128, false, umma::SmemAddress(fwdW), L::kTableBytesW,
+                  (W / 8) * 128, &barrier);
+      }
+      if (!wait_pass()) break;
+      // Epilogue 1: T[(cand, y)][u] -> A2 (rows (cand, u), K = y, MN-major).
+#pragma unroll
+      for (int i = 0; i < T1; ++i) {
+        const int r = i * 128 + tid, cand = r / H, y = r % H;
+        float t[W];
+        umma::Load<W>(lane_base + i * W, t);
+#pragma unroll
+        for (int g = 0; g < W / 8; ++g) {
+          float v[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[j] = t[g * 8 + j];
+          const int m = cand * W + g * 8;
+          StoreSplit8(v, pieces, (y >> 3) * kLbo2 + (m >> 3) * 128 + (y & 7) * 16);
+        }
+      }
+      operands_ready();
+      // Pass 2: forward column transform.
+      if (tid == 0) {
+        IssuePass(tmem, H, T2, H / 16, address, L::kOperandBytes, 2048, 2 * kLbo2, kLbo2, 128,
+                  true, umma::SmemAddress(fwdH), L::kTableBytesH, (H / 8) * 128, &barrier);
+      }
+      if (!wait_pass()) break;
+      // Epilogue 2: quantize C[(cand, u)][v]; residual -> A3 (rows (cand, v),
+      // K = u, MN-major); magnitude and nonzero sums per candidate.
+      const float2* channel_weights = weights + c * N;
+#pragma unroll
+      for (int i = 0; i < T2; ++i) {
+        const int r = i * 128 + tid, cand = r / W, u = r % W;
+        float coef[H];
+        umma::Load<H>(lane_base + i * H, coef);
+        const float qn = quant_norm[cand];
+        // All of the row's weights first: the operand stores below could
+        // alias them as far as the compiler knows.
+        float2 weight[H];
+#pragma unroll
+        for (int v = 0; v < H; ++v) weight[v] = channel_weights[v * W + u];
+        float mag = 0.0f;
+        uint32_t nz = 0;
+#pragma unroll
+        for (int g = 0; g < H / 8; ++g) {
+          float res[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int v = g * 8 + j;
+            const float scaled = coef[v] * weight[v].x * qn;
+            const float rounded = roundf(scaled);
+            res[j] = weight[v].y * (scaled - rounded);
+            mag += ApproxSqrt(fabsf(rounded));
+            nz += rounded != 0.0f ? 1u : 0u;
+          }
+          const int m = cand * H + g * 8;
+          StoreSplit8(res, pieces, (u >> 3) * kLbo3 + (m >> 3) * 128 + (u & 7) * 16);
+        }
+        // The W rows of one candidate are W consecutive lanes.
+#pragma unroll
+        for (int o = W / 2; o >= 1; o >>= 1) {
+          mag += __shfl_xor_sync(0xffffffffu, mag, o);
+          nz += __shfl_xor_sync(0xffffffffu, nz, o);
+        }
+        if ((lane & (W - 1)) == 0 && anchor_x[cand] >= 0) {
+          magnitude[cand][c] += mag;
+          nonzero[cand][c] += nz;
+        }
+      }
+      operands_ready();
+      // Pass 3: inverse transform along the rows of the residual.
+      if (tid == 0) {
+        IssuePass(tmem, W, T1, W / 16, address, L::kOperandBytes, 2048, 2 * kLbo3, kLbo3, 128,
+                  true, umma::SmemAddress(invW), L::kTableBytesW, (W / 8) * 128, &barrier);
+      }
+      if (!wait_pass()) break;
+      // Epilogue 3: Z[(cand, v)][x] -> A4 (rows (cand, x), K = v, MN-major).
+#pragma unroll
+      for (int i = 0; i < T1; ++i) {
+        const int r = i * 128 + tid, cand = r / H, v = r % H;
+        float z[W];
+        umma::Load<W>(lane_base + i * W, z);
+#pragma unroll
+        for (int g = 0; g < W / 8; ++g) {
+          float e[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) e[j] = z[g * 8 + j];
+          const int m = cand * W + g * 8;
+          StoreSplit8(e, pieces, (v >> 3) * kLbo4 + (m >> 3) * 128 + (v & 7) * 16);
+        }
+      }
+      operands_ready();
+      // Pass 4: inverse transform along the columns. The pixel mask of this
+      // thread's rows is loaded while it runs.
+      if (tid == 0) {
+        IssuePass(tmem, H, T2, H / 16, address, L::kOperandBytes, 2048, 2 * kLbo4, kLbo4, 128,
+                  true, umma::SmemAddress(invH), L::kTableBytesH, (H / 8) * 128, &barrier);
+      }
+      float mask[T2][H];
+#pragma unroll
+      for (int i = 0; i < T2; ++i) {
+        const int r = i * 128 + tid, cand = r / W, x = r % W;
+        const int ax = anchor_x[cand], ay = anchor_y[cand];
+#pragma unroll
+        for (int y = 0; y < H; ++y) {
+          mask[i][y] = ax < 0 ? 1.0f
+                     : __ldg(p.pixel_mask + static_cast<size_t>(ay * 8 + y) * p.mask_stride +
+                             ax * 8 + x);
+        }
+      }
+      if (!wait_pass()) break;
+      // Epilogue 4: weighted eighth powers of E[(cand, x)][y].
+      const float offset = c == 0 ? 12.0f : c == 1 ? 0.0f : 4.0f;
+#pragma unroll
+      for (int i = 0; i < T2; ++i) {
+        const int r = i * 128 + tid, cand = r / W;
+        float e[H];
+        umma::Load<H>(lane_base + i * H, e);
+        float loss = 0.0f;
+        bool finite = true;
+#pragma unroll
+        for (int y = 0; y < H; ++y) {
+          const float m = mask[i][y];
+          finite &= IsFinite(m) && m > 0.0f;
+          float weighted = (m + offset) * e[y];
+          weighted *= weighted;
+          weighted *= weighted;
+          weighted *= weighted;
+          loss += weighted;
+        }
+        if (!finite) RaiseError(p.error, kErrorNonFiniteInput);
+#pragma unroll
+        for (int o = W / 2; o >= 1; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+        if ((lane & (W - 1)) == 0 && anchor_x[cand] >= 0) loss_sum[cand][c] += loss;
+      }
+    }
+    __syncthreads();
+    if (!aborted && tid < G && anchor_x[tid] >= 0) {
+      const float mag[3] = {magnitude[tid][0], magnitude[tid][1], magnitude[tid][2]};
+      const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
+      const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
+      const float result = CandidateCost<N, S::CW * S::CH>(p, mag, nz, ls, quant_norm[tid]);
+      if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
+      p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+    }
+    __syncthreads();
+  }
+  // A CTA that gave up on a pass waits once more (bounded) for the tensor
+  // core to finish with its tensor memory before releasing it.
+  if (aborted) umma::WaitParity(&barrier, phase ^ 1u, kTcWaitPolls);
+  umma::FenceBeforeSync();
+  __syncthreads();
+  umma::FenceAfterSync();
+  if (warp == 0) umma::Deallocate(tmem, L::kTmemColumns);
 }
 
 // ---------------------------------------------------------------------------
@@ -607,7 +1095,7 @@ __global__ void __launch_bounds__(64) SearchTileKernel(const __grid_constant__ S
       p.cells[static_cast<size_t>(t.by0 + y) * p.blocks_x + t.bx0 + x] = t.cell[y * 8 + x];
 }
 
-template <int W, int H>
+template <int W, int H, typename Acc = double>
 int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t stream) {
   using S = Shape<W, H>;
   const int table = StrategyTableFamily(kFamilyStrategy[family]);
@@ -619,15 +1107,73 @@ int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t s
   p.local_x = (8 - cw) / p.anchor_step + 1;
   p.local_y = (8 - ch) / p.anchor_step + 1;
   const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
-  const size_t smem = CostLayout<W, H>::SharedBytes;
-  int status = CheckCuda(cudaFuncSetAttribute(CandidateCostKernel<W, H>,
+  const size_t smem = CostLayout<W, H, Acc>::SharedBytes;
+  int status = CheckCuda(cudaFuncSetAttribute(CandidateCostKernel<W, H, Acc>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(smem)),
                          "ac_strategy smem attribute");
   if (status != GJXL_B200_OK) return status;
   const unsigned grid = (count + S::K - 1) / S::K;
-  CandidateCostKernel<W, H><<<grid, kCostThreads, smem, stream>>>(p, count);
+  CandidateCostKernel<W, H, Acc><<<grid, kCostThreads, smem, stream>>>(p, count);
   return CheckLaunch("ac_strategy candidate costs");
+}
+
+// The tensor-core form of a 16/32-sided family: persistent CTAs (as many as
+// fit on the device at once) walk the units of G candidates.
+template <int W, int H>
+int LaunchFamilyTc(CostParams p, const DeviceTables& d, int family, cudaStream_t stream) {
+  using Lay = TcLayout<W, H>;
+  const int table = StrategyTableFamily(kFamilyStrategy[family]);
+  const HostTables& h = GetHostTables();
+  p.dequant = d.dequant + h.layout.offset[table];
+  p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  p.entropy_multiplier = kFamilyEntropy[family];
+  const int cw = kFamilyCoveredW[family], ch = kFamilyCoveredH[family];
+  p.local_x = (8 - cw) / p.anchor_step + 1;
+  p.local_y = (8 - ch) / p.anchor_step + 1;
+  const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  const size_t smem = Lay::SharedBytes;
+  int status = CheckCuda(cudaFuncSetAttribute(CandidateCostTcKernel<W, H>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)),
+                         "ac_strategy tensor-core smem attribute");
+  if (status != GJXL_B200_OK) return status;
+  // All of the SM's unified memory for shared memory, so that the CTAs the
+  // shared memory admits are all resident.
+  status = CheckCuda(cudaFuncSetAttribute(CandidateCostTcKernel<W, H>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout, 100),
+                     "ac_strategy tensor-core carveout");
+  if (status != GJXL_B200_OK) return status;
+  int device = 0, sms = 0, smem_per_sm = 0;
+  status = CheckCuda(cudaGetDevice(&device), "ac_strategy device");
+  if (status == GJXL_B200_OK) {
+    status = CheckCuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device),
+                       "ac_strategy SM count");
+  }
+  if (status == GJXL_B200_OK) {
+    status = CheckCuda(cudaDeviceGetAttribute(&smem_per_sm,
+                                              cudaDevAttrMaxSharedMemoryPerMultiprocessor, device),
+                       "ac_strategy shared memory per SM");
+  }
+  if (status != GJXL_B200_OK) return status;
+  // Resident CTAs per SM, bounded by shared memory (with the static part and
+  // the 1 KB the runtime reserves per CTA), registers (allocated in units of
+  // 8 per thread), threads, and 16 CTAs of 32 tensor-memory columns in the
+  // SM's 512, so that no CTA of this launch ever waits for tensor memory.
+  // (The runtime's occupancy calculator reports one CTA per SM for kernels
+  // that allocate tensor memory, which the hardware does not require.)
+  cudaFuncAttributes attributes;
+  status = CheckCuda(cudaFuncGetAttributes(&attributes, CandidateCostTcKernel<W, H>),
+                     "ac_strategy attributes");
+  if (status != GJXL_B200_OK) return status;
+  const int per_cta = static_cast<int>(smem + attributes.sharedSizeBytes) + 1024;
+  const int registers = ((attributes.numRegs + 7) / 8) * 8 * kTcThreads;
+  const int per_sm = std::max(
+    1, std::min({smem_per_sm / per_cta, 65536 / std::max(registers, 1), 2048 / kTcThreads, 16}));
+  const uint32_t units = (count + Lay::G - 1) / Lay::G;
+  const unsigned grid = std::max(1u, std::min<unsigned>(units, sms * per_sm));
+  CandidateCostTcKernel<W, H><<<grid, kTcThreads, smem, stream>>>(p, count);
+  return CheckLaunch("ac_strategy tensor-core candidate costs");
 }
 
 }  // namespace
@@ -639,7 +1185,7 @@ size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y) {
 int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
                           const float* quant_field, const float* pixel_mask, size_t mask_stride,
                           const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
-                          float* costs, uint32_t* error, cudaStream_t stream,
+                          int precision, float* costs, uint32_t* error, cudaStream_t stream,
                           const StreamFan* fan) {
   DeviceTables d;
   int status = GetDeviceTables(&d);
@@ -678,14 +1224,31 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
     CostParams q = p;
     q.anchor_step = (dense && f >= 4) ? 1 : kFamilyStep[f];
     q.costs = costs + f * bx * by;
+    const bool tensor = precision == GJXL_B200_PRECISION_FAST;
     switch (f) {
-      case 0: status = LaunchFamily<8, 8>(q, d, f, fs); break;
-      case 1: status = LaunchFamily<8, 16>(q, d, f, fs); break;
-      case 2: status = LaunchFamily<16, 8>(q, d, f, fs); break;
-      case 3: status = LaunchFamily<16, 16>(q, d, f, fs); break;
-      case 4: status = LaunchFamily<16, 32>(q, d, f, fs); break;
-      case 5: status = LaunchFamily<32, 16>(q, d, f, fs); break;
-      case 6: status = LaunchFamily<32, 32>(q, d, f, fs); break;
+      case 0:
+        status = tensor ? LaunchFamily<8, 8, float>(q, d, f, fs) : LaunchFamily<8, 8>(q, d, f, fs);
+        break;
+      case 1:
+        status = tensor ? LaunchFamily<8, 16, float>(q, d, f, fs)
+                        : LaunchFamily<8, 16>(q, d, f, fs);
+        break;
+      case 2:
+        status = tensor ? LaunchFamily<16, 8, float>(q, d, f, fs)
+                        : LaunchFamily<16, 8>(q, d, f, fs);
+        break;
+      case 3:
+        status = tensor ? LaunchFamilyTc<16, 16>(q, d, f, fs) : LaunchFamily<16, 16>(q, d, f, fs);
+        break;
+      case 4:
+        status = tensor ? LaunchFamilyTc<16, 32>(q, d, f, fs) : LaunchFamily<16, 32>(q, d, f, fs);
+        break;
+      case 5:
+        status = tensor ? LaunchFamilyTc<32, 16>(q, d, f, fs) : LaunchFamily<32, 16>(q, d, f, fs);
+        break;
+      case 6:
+        status = tensor ? LaunchFamilyTc<32, 32>(q, d, f, fs) : LaunchFamily<32, 32>(q, d, f, fs);
+        break;
     }
   }
   const cudaError_t joined = FanJoin(fan);
@@ -723,34 +1286,36 @@ extern "C" int gjxl_b200_ac_strategy_costs(
   const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch, size_t padded_width,
   size_t padded_height, const float* quant_field, const float* pixel_mask,
   size_t pixel_mask_stride, const int8_t* y_to_x, const int8_t* y_to_b,
-  float butteraugli_target, int dense_dct32, float* costs, uint32_t* device_error,
-  void* stream) {
+  float butteraugli_target, int dense_dct32, int precision, float* costs,
+  uint32_t* device_error, void* stream) {
   ClearLastError();
   if (opsin == nullptr || quant_field == nullptr || pixel_mask == nullptr || y_to_x == nullptr ||
       y_to_b == nullptr || costs == nullptr || padded_width % 8 || padded_height % 8 ||
       padded_width == 0 || padded_height == 0 || opsin_stride < padded_width ||
       opsin_plane_pitch < opsin_stride * padded_height || pixel_mask_stride < padded_width ||
+      opsin_stride % 4 != 0 || opsin_plane_pitch % 4 != 0 || !Aligned16(opsin) ||
       !std::isfinite(butteraugli_target) || butteraugli_target <= 0.0f ||
+      (precision != GJXL_B200_PRECISION_EXACT && precision != GJXL_B200_PRECISION_FAST) ||
       padded_width > (1u << 30) || padded_height > (1u << 30)) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "ac_strategy_costs: invalid arguments");
   }
   return LaunchAcStrategyCosts(opsin, opsin_stride, opsin_plane_pitch, padded_width,
                                padded_height, quant_field, pixel_mask, pixel_mask_stride, y_to_x,
-                               y_to_b, butteraugli_target, dense_dct32 != 0, costs, device_error,
-                               static_cast<cudaStream_t>(stream), nullptr);
+                               y_to_b, butteraugli_target, dense_dct32 != 0, precision, costs,
+                               device_error, static_cast<cudaStream_t>(stream), nullptr);
 }
 
 extern "C" int gjxl_b200_ac_strategy_search(
   const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch, size_t padded_width,
   size_t padded_height, const float* quant_field, const float* pixel_mask,
   size_t pixel_mask_stride, const int8_t* y_to_x, const int8_t* y_to_b,
-  float butteraugli_target, int dense_dct32, float* costs, uint8_t* cells,
+  float butteraugli_target, int dense_dct32, int precision, float* costs, uint8_t* cells,
   uint32_t* device_error, void* stream) {
   int status = gjxl_b200_ac_strategy_costs(opsin, opsin_stride, opsin_plane_pitch, padded_width,
                                            padded_height, quant_field, pixel_mask,
                                            pixel_mask_stride, y_to_x, y_to_b,
-                                           butteraugli_target, dense_dct32, costs, device_error,
-                                           stream);
+                                           butteraugli_target, dense_dct32, precision, costs,
+                                           device_error, stream);
   if (status != GJXL_B200_OK) return status;
   if (cells == nullptr) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "ac_strategy_search: cells is null");

@@ -211,3 +211,80 @@ __device__ __forceinline__ void BatchColumnPass(const double* in, Out* out, int 
 }
 
 }  // namespace gjxl_b200
+
+namespace gjxl_b200 {
+
+// FP32 line passes of lengths 8 and 16 for the fast cost mode: the same
+// chunking as the FP64 passes, with the bases rounded to float and each
+// multiply-add fused (one rounding per term).
+template <int L, bool kForward>
+__device__ __forceinline__ float DctBasisF(int index) {
+  if constexpr (kForward) {
+    if constexpr (L == 8) return kDctForward8F[index];
+    if constexpr (L == 16) return kDctForward16F[index];
+  } else {
+    if constexpr (L == 8) return kDctInverse8F[index];
+    if constexpr (L == 16) return kDctInverse16F[index];
+  }
+  return 0.0f;
+}
+
+template <int L, bool kForward, int C, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunkF(const In* __restrict__ in, Out* __restrict__ out) {
+  static_assert(L == 8 || L == 16, "FP32 passes cover lengths 8 and 16");
+  float acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = 0.0f;
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    const float v = static_cast<float>(in[s * InStep]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = C * 8 + j;
+      acc[j] = fmaf(v, DctBasisF<L, kForward>(kForward ? k * L + s : s * L + k), acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) out[j * OutStep] = static_cast<Out>(acc[j]);
+}
+
+template <int L, bool kForward, int InStep, int OutStep, typename In, typename Out>
+__device__ __forceinline__ void LineChunkAtF(int chunk, const In* __restrict__ in,
+                                             Out* __restrict__ out) {
+  if (chunk == 0) {
+    LineChunkF<L, kForward, 0, InStep, OutStep>(in, out);
+  } else if constexpr (L > 8) {
+    if (chunk == 1) LineChunkF<L, kForward, 1, InStep, OutStep>(in, out);
+  }
+}
+
+// FP32 counterparts of BatchRowPass / BatchColumnPass (float intermediate).
+template <int W, int H, int KC, bool kForward, typename In, typename Valid>
+__device__ __forceinline__ void BatchRowPassF(const In* in, float* out, int tid, int threads,
+                                              Valid valid) {
+  using B = PlaneBatch<W, H, KC>;
+  constexpr int kLines = KC * H;
+  for (int item = tid; item < B::Items; item += threads) {
+    const int chunk = item / kLines, line = item % kLines;
+    if (!valid(line / H)) continue;
+    LineChunkAtF<W, kForward, 1, 1>(chunk, in + line * B::RowPitch,
+                                    out + line * B::RowPitch + chunk * 8);
+  }
+}
+
+template <int W, int H, int KC, bool kForward, typename Out, typename Valid>
+__device__ __forceinline__ void BatchColumnPassF(const float* in, Out* out, int tid, int threads,
+                                                 Valid valid) {
+  using B = PlaneBatch<W, H, KC>;
+  constexpr int kLines = KC * W;
+  for (int item = tid; item < B::Items; item += threads) {
+    const int chunk = item / kLines, line = item % kLines;
+    const int plane = line / W, u = line % W;
+    if (!valid(plane)) continue;
+    const int base = plane * B::PlanePitch + u;
+    LineChunkAtF<H, kForward, B::RowPitch, B::RowPitch>(chunk, in + base,
+                                                        out + base + chunk * 8 * B::RowPitch);
+  }
+}
+
+}  // namespace gjxl_b200

@@ -456,8 +456,8 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
   const StreamFan fan = MakeFan(s, stream);
   const bool dense = s->options.effort >= 10;
   GJXL_TRY(LaunchAcStrategyCosts(s->pre, s->pw, s->pitch, s->pw, s->ph, s->quant, s->pixel_mask,
-                                 s->pw, s->y_to_x, s->y_to_b, target, dense, s->costs, s->error,
-                                 stream, &fan));
+                                 s->pw, s->y_to_x, s->y_to_b, target, dense,
+                                 s->options.precision, s->costs, s->error, stream, &fan));
   Mark(s, kStageAcMerge, stream);
   GJXL_TRY(LaunchAcStrategySearch(s->costs, s->pw, s->ph, target, dense, s->cells, s->error,
                                   stream));
@@ -592,6 +592,7 @@ extern "C" void gjxl_b200_default_options(gjxl_b200_options* options) {
   options->profile_stages = 0;
   options->tokenize = 1;
   options->order_mode = -1;
+  options->precision = GJXL_B200_PRECISION_EXACT;
 }
 
 extern "C" int gjxl_b200_session_create(size_t width, size_t height,
@@ -616,6 +617,9 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
   }
   if (o.order_mode < -1 || o.order_mode > 2) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: order_mode is -1..2");
+  }
+  if (o.precision != GJXL_B200_PRECISION_EXACT && o.precision != GJXL_B200_PRECISION_FAST) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: precision is 0 or 1");
   }
   if (o.effort < 5 || o.effort > 10) {
     return SetError(GJXL_B200_UNSUPPORTED,

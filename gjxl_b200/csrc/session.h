@@ -30,7 +30,7 @@ size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y);
 int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
                           const float* quant_field, const float* pixel_mask, size_t mask_stride,
                           const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
-                          float* costs, uint32_t* error, cudaStream_t stream,
+                          int precision, float* costs, uint32_t* error, cudaStream_t stream,
                           const StreamFan* fan = nullptr);
 int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float target, bool dense,
                            uint8_t* cells, uint32_t* error, cudaStream_t stream);

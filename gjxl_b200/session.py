@@ -17,7 +17,7 @@ from . import _lib
 class Options(Structure):
     _fields_ = [("struct_size", c_size_t), ("butteraugli_target", c_float), ("effort", c_int),
                 ("intensity_target", c_float), ("profile_stages", c_int), ("tokenize", c_int),
-                ("order_mode", c_int)]
+                ("order_mode", c_int), ("precision", c_int)]
 
 
 class Outputs(Structure):
@@ -83,7 +83,7 @@ class AnalysisSession:
 
     def __init__(self, width: int, height: int, butteraugli_target: float = 1.0,
                  effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False,
-                 tokenize: bool = True, order_mode: int = -1):
+                 tokenize: bool = True, order_mode: int = -1, precision: int = 0):
         _bind()
         lib = _lib.load()
         opts = Options()
@@ -94,6 +94,7 @@ class AnalysisSession:
         opts.profile_stages = int(profile_stages)
         opts.tokenize = int(tokenize)
         opts.order_mode = order_mode
+        opts.precision = precision
         handle = c_void_p()
         _check(lib.gjxl_b200_session_create(width, height, ctypes.byref(opts),
                                             ctypes.byref(handle)), "gjxl_b200_session_create")

@@ -82,21 +82,24 @@ def _search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense):
             y_to_x.data_ptr(), y_to_b.data_ptr(), target, int(dense))
 
 
+PRECISION_EXACT, PRECISION_FAST = 0, 1
+
+
 def ac_strategy_costs(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, target=1.0,
-                      dense=False, device_error=None):
+                      dense=False, device_error=None, precision=PRECISION_EXACT):
     """opsin: (3, PH, PW) Gaborish-inverted XYB; costs: float tensor of
     ac_strategy_cost_bytes() bytes."""
     _lib.call("gjxl_b200_ac_strategy_costs",
               *_search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense),
-              costs.data_ptr(), None if device_error is None else device_error.data_ptr(),
-              _stream())
+              precision, costs.data_ptr(),
+              None if device_error is None else device_error.data_ptr(), _stream())
 
 
 def ac_strategy_search(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, cells,
-                       target=1.0, dense=False, device_error=None):
+                       target=1.0, dense=False, device_error=None, precision=PRECISION_EXACT):
     _lib.call("gjxl_b200_ac_strategy_search",
               *_search_args(opsin, quant_field, pixel_mask, y_to_x, y_to_b, target, dense),
-              costs.data_ptr(), cells.data_ptr(),
+              precision, costs.data_ptr(), cells.data_ptr(),
               None if device_error is None else device_error.data_ptr(), _stream())
 
 

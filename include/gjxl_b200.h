@@ -174,6 +174,22 @@ GJXL_B200_API int gjxl_b200_quant_matrix(int strategy, int channel,
                                          size_t capacity);
 
 /*
+ * Precision of the AC-strategy candidate costs.
+ *  EXACT: the reference CPU transform restated in FP64 (bit-identical costs,
+ *         hence strategy grids, to the reference's CPU path).
+ *  FAST:  the families with 16- or 32-pixel sides (DCT16x16, DCT32x16,
+ *         DCT16x32, DCT32x32) as tcgen05 tensor-core MMAs on three-piece
+ *         split-bf16 operands with f32 accumulation (FP32-class products),
+ *         like the reference's own FP32 CUDA evaluator
+ *         (src/gpu/cuda/cuda_kernels.cu:653); the 8-pixel families (DCT8,
+ *         DCT16x8, DCT8x16) with FP32 fused multiply-adds on SIMT cores.
+ *         Grids then match the exact mode except where a candidate's cost is
+ *         within rounding of a tie.
+ */
+#define GJXL_B200_PRECISION_EXACT 0
+#define GJXL_B200_PRECISION_FAST 1
+
+/*
  * AC-strategy candidate costs (rows a6, a8).
  * Replaces GpuAcStrategyEvaluation (src/gpu/ops/ac_strategy.h:118-170) as run
  * by LaunchCudaAcStrategyBatch / FusedAcStrategyKernel
@@ -194,7 +210,7 @@ GJXL_B200_API int gjxl_b200_ac_strategy_costs(
     size_t padded_width, size_t padded_height, const float* quant_field,
     const float* pixel_mask, size_t pixel_mask_stride, const int8_t* y_to_x,
     const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
-    float* costs, uint32_t* device_error, void* stream);
+    int precision, float* costs, uint32_t* device_error, void* stream);
 
 /*
  * AC-strategy search (rows a6, a7, a8): candidate costs followed by the
@@ -211,7 +227,8 @@ GJXL_B200_API int gjxl_b200_ac_strategy_search(
     size_t padded_width, size_t padded_height, const float* quant_field,
     const float* pixel_mask, size_t pixel_mask_stride, const int8_t* y_to_x,
     const int8_t* y_to_b, float butteraugli_target, int dense_dct32,
-    float* costs, uint8_t* cells, uint32_t* device_error, void* stream);
+    int precision, float* costs, uint8_t* cells, uint32_t* device_error,
+    void* stream);
 
 /*
  * Butteraugli with a prepared reference image (rows a14, a15).
@@ -323,6 +340,8 @@ typedef struct gjxl_b200_options {
   int order_mode;           /* -1 (default): by effort, as the reference resolves it
                                (effort 7: 2, else 1); or 0/1/2 as for
                                gjxl_b200_ac_tokenize */
+  int precision;            /* GJXL_B200_PRECISION_EXACT (default) or _FAST:
+                               candidate-cost precision of the strategy search */
 } gjxl_b200_options;
 
 /* Session results. The adaptive-quantization fields mirror the reference's

@@ -442,13 +442,14 @@ GJXL_INTEGRATION_API const char* gjxl_b200_integration_last_error(void) {
 
 // Encodes packed 8-bit sRGB (3 or 4 channels) at the given distance and
 // effort: the analysis half on the B200 (one session on the current device,
-// default stream), the serializer on the CPU. device_tokens != 0 installs the
-// device AC tokenizer. Writes the codestream (size in *size, -2 when it does
-// not fit `capacity`) and the session's final Butteraugli score.
+// default stream, candidate costs at `precision`), the serializer on the
+// CPU. device_tokens != 0 installs the device AC tokenizer. Writes the
+// codestream (size in *size, -2 when it does not fit `capacity`) and the
+// session's final Butteraugli score.
 GJXL_INTEGRATION_API int gjxl_b200_encode_image(const uint8_t* pixels, size_t width,
                                                 size_t height, size_t row_stride, int channels,
                                                 float butteraugli_target, int effort,
-                                                int device_tokens, uint8_t* out,
+                                                int precision, int device_tokens, uint8_t* out,
                                                 size_t capacity, size_t* size, double* score) {
   g_last_error.clear();
   VarDctEncodingOptions options;
@@ -459,6 +460,7 @@ GJXL_INTEGRATION_API int gjxl_b200_encode_image(const uint8_t* pixels, size_t wi
   session_options.butteraugli_target = butteraugli_target;
   session_options.effort = effort;
   session_options.tokenize = 0;  // the serializer asks for its own map's tokens
+  session_options.precision = precision;
   gjxl_b200_session* session = nullptr;
   Status status = FromB200(gjxl_b200_session_create(width, height, &session_options, &session),
                            "session_create");

@@ -37,14 +37,15 @@ def encoder() -> ctypes.CDLL:
         pytest.fail(f"{LIBRARY} is missing: build it with `make -C integration`")
     lib = ctypes.CDLL(str(LIBRARY))
     lib.gjxl_b200_encode_image.argtypes = [c_void_p, c_size_t, c_size_t, c_size_t, c_int,
-                                           c_float, c_int, c_int, c_void_p, c_size_t,
+                                           c_float, c_int, c_int, c_int, c_void_p, c_size_t,
                                            ctypes.POINTER(c_size_t), ctypes.POINTER(c_double)]
     lib.gjxl_b200_encode_image.restype = c_int
     lib.gjxl_b200_integration_last_error.restype = ctypes.c_char_p
     return lib
 
 
-def b200_encode(img: np.ndarray, target: float, effort: int, device_tokens: bool):
+def b200_encode(img: np.ndarray, target: float, effort: int, device_tokens: bool,
+                precision: int = 0):
     import torch  # noqa: F401  (initializes the CUDA context on cuda:0)
     lib = encoder()
     img = np.ascontiguousarray(img)
@@ -53,15 +54,16 @@ def b200_encode(img: np.ndarray, target: float, effort: int, device_tokens: bool
     out = np.empty(capacity, np.uint8)
     size, score = c_size_t(0), c_double(0.0)
     rc = lib.gjxl_b200_encode_image(img.ctypes.data, w, h, w * ch, ch, target, effort,
-                                    int(device_tokens), out.ctypes.data, capacity,
+                                    precision, int(device_tokens), out.ctypes.data, capacity,
                                     ctypes.byref(size), ctypes.byref(score))
     assert rc == 0, lib.gjxl_b200_integration_last_error().decode()
     return out[:size.value].tobytes(), score.value
 
 
-def check_against_reference(img, target, effort, exact_required):
-    ours, score = b200_encode(img, target, effort, device_tokens=False)
-    ours_device, score_device = b200_encode(img, target, effort, device_tokens=True)
+def check_against_reference(img, target, effort, exact_required, precision=0):
+    ours, score = b200_encode(img, target, effort, device_tokens=False, precision=precision)
+    ours_device, score_device = b200_encode(img, target, effort, device_tokens=True,
+                                            precision=precision)
     assert ours_device == ours, "device AC tokens changed the codestream"
     assert score_device == score
     want, want_score = ref.encode_cpu(ref.srgb8_to_linear(img), target, effort)
@@ -91,3 +93,11 @@ def test_effort7_codestream_matches_reference(cuda, w, h, seed):
 def test_other_distances_and_efforts(cuda, target, effort):
     check_against_reference(generate_srgb8(384, 256, 100 + effort), target, effort,
                             exact_required=False)
+
+
+@pytest.mark.parametrize("w,h,seed", [(512, 512, workload_seed(1, 0)), (1000, 700, 5000)])
+def test_fast_precision_codestream_within_tolerance(cuda, w, h, seed):
+    """Fast (tensor-core) candidate costs: the codestream's size and final
+    Butteraugli distance within 0.2% of the reference CPU encode."""
+    check_against_reference(generate_srgb8(w, h, seed), 1.0, 7, exact_required=False,
+                            precision=1)

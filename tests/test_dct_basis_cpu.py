@@ -23,7 +23,8 @@ def committed_tables():
     text = (CSRC / "dct_basis.inc").read_text()
     tables = {}
     for name, body in re.findall(r"kDct(\w+)\[\d+\] = \{(.*?)\};", text, re.S):
-        tables[name] = np.array([float.fromhex(v) for v in re.findall(r"-?0x[0-9a-fp.+-]+", body)])
+        values = re.findall(r"(-?0x[0-9a-f.]+p[+-]?\d+)f?", body)
+        tables[name] = np.array([float.fromhex(v) for v in values])
     return tables
 
 
@@ -53,3 +54,14 @@ def test_staged_tables_equal_constant_tables():
     tables = committed_tables()
     assert np.array_equal(tables["StagedForwardT32"], tables["ForwardT32"])
     assert np.array_equal(tables["StagedInverse32"], tables["Inverse32"])
+
+
+def test_single_precision_tables_are_rounded_double_tables():
+    """The FP32 tables of the fast cost mode are the double bases rounded to
+    nearest float."""
+    tables = committed_tables()
+    for direction in ("Forward", "Inverse"):
+        for n in (8, 16):
+            double = tables[f"{direction}{n}"]
+            single = tables[f"{direction}{n}F"]
+            assert np.array_equal(single, double.astype(np.float32).astype(np.float64))

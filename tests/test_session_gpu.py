@@ -22,6 +22,7 @@ The same 0.1% rule covers a strategy grid that differs in a near-tie (a
 against the reference's own grid, never skipped."""
 
 import ctypes
+import functools
 import os
 
 import numpy as np
@@ -118,6 +119,15 @@ def reference(img: np.ndarray, effort: int = 7, target: float = 1.0):
     return opsin, stats, ref.pipeline_tokens(lin, opsin, target, effort, xs, bs,
                                              ref.SIMPLE_BLOCK_CONTEXT_MAP,
                                              2 if effort == 7 else 1)
+
+
+@functools.lru_cache(maxsize=2)
+def reference_of_workload(w: int, h: int, seed: int, noise: bool, effort: int = 7):
+    """reference() of a generated image, cached: the 12 MP reference run
+    takes minutes and several tests compare against it."""
+    from oracle import ref as oracle_ref
+    oracle_ref.set_threads(os.cpu_count() or 1)
+    return reference(generate_srgb8(w, h, seed, sensor_noise=noise), effort)
 
 
 def device_quantized_ac(s: AnalysisSession) -> np.ndarray:
@@ -252,13 +262,11 @@ def test_session_benchmarked_image_full_size(cuda):
     Front half bit-exact except the grid (<= 0.1% of blocks), quantizer
     exact, every block output within 0.1% of blocks, score history within
     0.2%, and the tokens bit-exact when the loop agrees."""
-    from oracle import ref as oracle_ref
-    oracle_ref.set_threads(os.cpu_count() or 1)
     img = generate_srgb8(4032, 3024, workload_seed(2, 0), sensor_noise=True)
     s = run_session(img)
     assert s.host_error() == 0
     got = s.host_results()
-    _, stats, want = reference(img)
+    _, stats, want = reference_of_workload(4032, 3024, workload_seed(2, 0), True)
     same_grid = compare_front_half(s, got, want, stats, 7)
     if compare_loop_fed_back(s, got, want) == 0 and same_grid:
         compare_loop_exact(s, got, want)
@@ -332,3 +340,22 @@ def test_graph_replay_matches_direct_launches(cuda):
         assert_bitexact(got, want, name)
     replayed.close()
     direct.close()
+
+
+@pytest.mark.parametrize("w,h,seed,noise", [(512, 512, workload_seed(1, 0), False),
+                                            (4032, 3024, workload_seed(2, 0), True)])
+def test_session_fast_precision_matches_reference(cuda, w, h, seed, noise):
+    """The session with the fast (tensor-core) candidate costs, against the
+    reference CPU pipeline: every block output within 0.1% of blocks, the
+    quantizer exact, the score history within 0.2%."""
+    img = generate_srgb8(w, h, seed, sensor_noise=noise)
+    s = AnalysisSession(w, h, butteraugli_target=1.0, effort=7, precision=1)
+    s.analyze_host(img, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert s.host_error() == 0
+    got = s.host_results()
+    _, stats, want = reference_of_workload(w, h, seed, noise)
+    same_grid = compare_front_half(s, got, want, stats, 7)
+    if compare_loop_fed_back(s, got, want) == 0 and same_grid:
+        compare_loop_exact(s, got, want)
+    s.close()
