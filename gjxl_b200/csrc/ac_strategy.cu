@@ -163,6 +163,69 @@ __device__ __forceinline__ float QuantNorm(const CostParams& p, int ax, int ay) 
   return FastPow2(FastLog2(sum) * (1.0f / 16.0f));
 }
 
+// The quantities of one candidate that the transform stage needs, loaded
+// ahead of use: anchor block, the quant field over its covered blocks and
+// the tile's CfL bytes.
+template <int CW, int CH>
+struct CandidateInputs {
+  int ax = -1, ay = -1;
+  float q[CW * CH];
+  int y_to_x = 0, y_to_b = 0;
+};
+
+// Anchor of candidate `cand` of a family (the same enumeration as the FP64
+// kernel: tiles in raster order, local anchors on the family's step), or
+// ax = -1 where the candidate does not fit its tile; then the loads.
+template <int CW, int CH>
+__device__ __forceinline__ CandidateInputs<CW, CH> FetchCandidate(const CostParams& p,
+                                                                 uint32_t cand,
+                                                                 uint32_t candidate_count) {
+  CandidateInputs<CW, CH> in;
+  if (cand < candidate_count) {
+    const uint32_t per_tile = p.local_x * p.local_y;
+    const uint32_t tile = cand / per_tile, local = cand % per_tile;
+    const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
+    const int lx = (local % p.local_x) * p.anchor_step;
+    const int ly = (local / p.local_x) * p.anchor_step;
+    const int tile_w = min(8, static_cast<int>(p.blocks_x) - tx * 8);
+    const int tile_h = min(8, static_cast<int>(p.blocks_y) - ty * 8);
+    if (lx + CW <= tile_w && ly + CH <= tile_h) {
+      in.ax = tx * 8 + lx;
+      in.ay = ty * 8 + ly;
+    }
+  }
+  if (in.ax >= 0) {
+#pragma unroll
+    for (int dy = 0; dy < CH; ++dy) {
+#pragma unroll
+      for (int dx = 0; dx < CW; ++dx) {
+        in.q[dy * CW + dx] = __ldg(p.quant_field + (in.ay + dy) * p.blocks_x + in.ax + dx);
+      }
+    }
+    const int tile_index = (in.ay / 8) * p.tiles_x + (in.ax / 8);
+    in.y_to_x = p.y_to_x[tile_index];
+    in.y_to_b = p.y_to_b[tile_index];
+  }
+  return in;
+}
+
+// QuantNorm of loaded quant-field values (same arithmetic).
+template <int CW, int CH>
+__device__ __forceinline__ float QuantNormOf(const float (&q)[CW * CH]) {
+  if (CW * CH == 1) return q[0];
+  if (CW * CH == 2) return fmaxf(q[0], q[1]);
+  float sum = 0.0f;
+  for (int i = 0; i < CW * CH; ++i) {
+    float v = q[i];
+    v *= v;
+    v *= v;
+    v *= v;
+    sum += v * v;
+  }
+  sum /= static_cast<float>(CW * CH);
+  return FastPow2(FastLog2(sum) * (1.0f / 16.0f));
+}
+
 // The candidate's cost from its per-channel magnitude sums, nonzero counts
 // and weighted-loss sums (EstimateAcStrategyCost, ac_strategy.cpp:960-994).
 template <int N, int kBlocks>
@@ -635,33 +698,24 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
   };
 
   const uint32_t units = (candidate_count + G - 1) / G;
+  // The inputs of this CTA's next unit are loaded one unit ahead, so their
+  // latency overlaps a unit of transform work.
+  CandidateInputs<S::CW, S::CH> next;
+  if (tid < G) next = FetchCandidate<S::CW, S::CH>(p, blockIdx.x * G + tid, candidate_count);
   for (uint32_t unit = blockIdx.x; unit < units && !aborted; unit += gridDim.x) {
     if (tid < G) {
-      const uint32_t cand = unit * G + tid;
-      int ax = -1, ay = -1;
-      if (cand < candidate_count) {
-        const uint32_t per_tile = p.local_x * p.local_y;
-        const uint32_t tile = cand / per_tile, local = cand % per_tile;
-        const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
-        const int lx = (local % p.local_x) * p.anchor_step;
-        const int ly = (local / p.local_x) * p.anchor_step;
-        const int tile_w = min(8, static_cast<int>(p.blocks_x) - tx * 8);
-        const int tile_h = min(8, static_cast<int>(p.blocks_y) - ty * 8);
-        if (lx + S::CW <= tile_w && ly + S::CH <= tile_h) {
-          ax = tx * 8 + lx;
-          ay = ty * 8 + ly;
-        }
-      }
-      anchor_x[tid] = ax;
-      anchor_y[tid] = ay;
+      const CandidateInputs<S::CW, S::CH> in = next;
+      next = FetchCandidate<S::CW, S::CH>(p, (unit + gridDim.x) * G + tid, candidate_count);
+      anchor_x[tid] = in.ax;
+      anchor_y[tid] = in.ay;
       float qn = 1.0f;
-      if (ax >= 0) {
-        qn = QuantNorm<S::CW, S::CH>(p, ax, ay);
+      if (in.ax >= 0) {
+        qn = QuantNormOf<S::CW, S::CH>(in.q);
         if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
-        const int tile_index = (ay / 8) * p.tiles_x + (ax / 8);
-        cfl[tid][0] = static_cast<float>(p.y_to_x[tile_index]) / 84.0f;
+        // ColorCorrelationMap::AcFactors (chroma_from_luma.cpp:412-432).
+        cfl[tid][0] = static_cast<float>(in.y_to_x) / 84.0f;
         cfl[tid][1] = 0.0f;
-        cfl[tid][2] = 1.0f + static_cast<float>(p.y_to_b[tile_index]) / 84.0f;
+        cfl[tid][2] = 1.0f + static_cast<float>(in.y_to_b) / 84.0f;
       }
       quant_norm[tid] = qn;
       for (int c = 0; c < 3; ++c) {
