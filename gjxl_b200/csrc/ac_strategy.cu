@@ -135,6 +135,25 @@ __device__ __forceinline__ float OrderedSum(const float* t) {
   return sum;
 }
 
+// Sum of each plane's N terms by kThreads / KC threads per plane (a fixed
+// pairwise order, not the reference's sequential one): the fast mode's
+// magnitude and loss sums. Writes the sum of plane `tid / T` through `out`
+// from its first thread.
+template <int N, int KC, int kThreads, int kPitch, typename Out>
+__device__ __forceinline__ void ParallelPlaneSums(const float* terms, int tid, Out out) {
+  constexpr int T = kThreads / KC;
+  static_assert(T * KC == kThreads && (T & (T - 1)) == 0 && T <= 32 && N % T == 0,
+                "threads per plane: a power of two within a warp");
+  const int plane = tid / T, part = tid % T;
+  const float* t = terms + plane * kPitch + part * (N / T);
+  float sum = 0.0f;
+#pragma unroll 8
+  for (int j = 0; j < N / T; ++j) sum += t[j];
+#pragma unroll
+  for (int o = T / 2; o >= 1; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (part == 0) out(plane, sum);
+}
+
 __device__ __forceinline__ int CeilLog2Nonzero(uint32_t v) {
   return v <= 1 ? 0 : 32 - __clz(v - 1);
 }
@@ -228,7 +247,10 @@ __device__ __forceinline__ float QuantNormOf(const float (&q)[CW * CH]) {
 
 // The candidate's cost from its per-channel magnitude sums, nonzero counts
 // and weighted-loss sums (EstimateAcStrategyCost, ac_strategy.cpp:960-994).
-template <int N, int kBlocks>
+// kExactRoot: the eighth root as the reference rounds it (double pow);
+// otherwise exp2(log2(x) / 8) in single precision (within a few ulp), for the
+// fast mode.
+template <int N, int kBlocks, bool kExactRoot = true>
 __device__ __forceinline__ float CandidateCost(const CostParams& p, const float (&magnitude)[3],
                                                const uint32_t (&nonzero)[3],
                                                const float (&loss_sum)[3], float quant_norm) {
@@ -248,7 +270,9 @@ __device__ __forceinline__ float CandidateCost(const CostParams& p, const float 
   }
   const float normalized_loss = loss / static_cast<float>(N);
   // std::pow(float, 1/8): evaluated in double and rounded to float.
-  const float root = static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125));
+  const float root =
+    kExactRoot ? static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125))
+               : (normalized_loss > 0.0f ? exp2f(log2f(normalized_loss) * 0.125f) : 0.0f);
   const float loss_cost = root * static_cast<float>(N) / quant_norm;
   return entropy * p.entropy_multiplier + p.info_loss_multiplier * loss_cost;
 }
@@ -432,8 +456,14 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
 
   // Ordered magnitude sums (one thread per candidate and channel); these
   // threads then join the inverse row pass, which does not touch `terms`.
-  if (tid < KC && anchor_x[tid / 3] >= 0) {
-    magnitude[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
+  // The fast mode sums every plane with all threads instead.
+  if constexpr (kExact) {
+    if (tid < KC && anchor_x[tid / 3] >= 0) {
+      magnitude[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
+    }
+  } else {
+    ParallelPlaneSums<N, KC, kCostThreads, Lay::TermPitch>(
+      terms, tid, [&](int plane, float sum) { magnitude[plane / 3][plane % 3] = sum; });
   }
 
   // Inverse DCT (InverseDctCpu): rows of the residual into T, columns into B.
@@ -470,8 +500,13 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
-  if (tid < KC && anchor_x[tid / 3] >= 0) {
-    loss_sum[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
+  if constexpr (kExact) {
+    if (tid < KC && anchor_x[tid / 3] >= 0) {
+      loss_sum[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
+    }
+  } else {
+    ParallelPlaneSums<N, KC, kCostThreads, Lay::TermPitch>(
+      terms, tid, [&](int plane, float sum) { loss_sum[plane / 3][plane % 3] = sum; });
   }
   __syncthreads();
 
@@ -479,7 +514,7 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     const float mag[3] = {magnitude[tid][0], magnitude[tid][1], magnitude[tid][2]};
     const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
     const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
-    const float result = CandidateCost<N, S::CW * S::CH>(p, mag, nz, ls, quant_norm[tid]);
+    const float result = CandidateCost<N, S::CW * S::CH, kExact>(p, mag, nz, ls, quant_norm[tid]);
     if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
     p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
   }
@@ -698,14 +733,10 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
   };
 
   const uint32_t units = (candidate_count + G - 1) / G;
-  // The inputs of this CTA's next unit are loaded one unit ahead, so their
-  // latency overlaps a unit of transform work.
-  CandidateInputs<S::CW, S::CH> next;
-  if (tid < G) next = FetchCandidate<S::CW, S::CH>(p, blockIdx.x * G + tid, candidate_count);
   for (uint32_t unit = blockIdx.x; unit < units && !aborted; unit += gridDim.x) {
     if (tid < G) {
-      const CandidateInputs<S::CW, S::CH> in = next;
-      next = FetchCandidate<S::CW, S::CH>(p, (unit + gridDim.x) * G + tid, candidate_count);
+      const CandidateInputs<S::CW, S::CH> in =
+        FetchCandidate<S::CW, S::CH>(p, unit * G + tid, candidate_count);
       anchor_x[tid] = in.ax;
       anchor_y[tid] = in.ay;
       float qn = 1.0f;
@@ -912,7 +943,8 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
       const float mag[3] = {magnitude[tid][0], magnitude[tid][1], magnitude[tid][2]};
       const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
       const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
-      const float result = CandidateCost<N, S::CW * S::CH>(p, mag, nz, ls, quant_norm[tid]);
+      const float result =
+        CandidateCost<N, S::CW * S::CH, false>(p, mag, nz, ls, quant_norm[tid]);
       if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
       p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
     }
