@@ -450,6 +450,31 @@ def run_reference(args) -> dict:
     }
 
 
+def reference_gpu_leg(samples: int = 5, warmup: int = 2) -> dict:
+    """The reference's own CUDA path on this GPU (its gjxl_cuda sources built
+    for sm_100a into oracle/_ref/libgjxl_ref_cuda.so), as its
+    cuda_encoding_benchmark runs it: fully-resident adaptive quantization,
+    d1.0 e7, the same image. MP/s of the workflow's analysis phase
+    (quantization_pipeline), median of `samples` encodes, one image at a
+    time (the reference runs one encode per CUDA backend)."""
+    from oracle import ref
+    if not ref.cuda_available():
+        return {"unavailable": "oracle/_ref/libgjxl_ref_cuda.so not built"}
+    linear = ref.srgb8_to_linear(make_image())
+    for _ in range(warmup):
+        ref.cuda_encode(linear, 1.0, 7)
+    runs = [ref.cuda_encode(linear, 1.0, 7) for _ in range(samples)]
+    analysis = statistics.median(r["analysis_ms"] for r in runs)
+    total = statistics.median(r["total_ms"] for r in runs)
+    mp = WIDTH * HEIGHT / 1e6
+    return {"value": round(mp / (analysis / 1e3), 3), "unit": "MP/s",
+            "analysis_ms": round(analysis, 3), "encode_ms": round(total, 3),
+            "codestream_bytes": len(runs[-1]["codestream"]), "score": runs[-1]["score"],
+            "kind": "reference CUDA path (sm_100a build of its gjxl_cuda sources), "
+                    "fully-resident AQ, quantization_pipeline phase, one image at a time",
+            "samples": samples}
+
+
 def cpu_baseline_leg(pool: "ReferencePool") -> dict:
     """About 15 s of reference CPU work on all host cores (one step)."""
     pool.step()  # first step loads the library in every worker
@@ -472,6 +497,8 @@ def main():
                         help="analysis sessions (images in flight) per GPU")
     parser.add_argument("--size", default=None,
                         help="WxH of a smaller image of the same generator (profiling only)")
+    parser.add_argument("--no-reference-gpu", action="store_true",
+                        help="skip timing the reference's own CUDA path")
     parser.add_argument("--precision", default="exact", choices=["exact", "fast"],
                         help="candidate-cost precision: exact (FP64, the reference's CPU "
                              "results bit for bit) or fast (tcgen05 tensor cores)")
@@ -494,6 +521,11 @@ def main():
     if out:
         if pool is not None:
             out["cpu_baseline"] = cpu_baseline_leg(pool)
+        if world == 1 and not args.launch_list and not args.no_reference_gpu:
+            try:
+                out["reference_gpu"] = reference_gpu_leg()
+            except Exception as exc:  # reported, never fatal to our own line
+                out["reference_gpu"] = {"unavailable": str(exc)[:200]}
         print(json.dumps(out))
     if pool is not None:
         pool.close()

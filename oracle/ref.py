@@ -384,3 +384,56 @@ def pipeline_tokens(linear: np.ndarray, opsin: np.ndarray, target: float = 1.0, 
     tok["used_order_mask"] = int(tok["used_order_mask"][0])
     res.update(tok)
     return res
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA path (oracle/_ref/libgjxl_ref_cuda.so, built by
+# `make -C oracle cuda`): the reference GPU baseline.
+
+CUDA_LIBRARY_PATH = Path(__file__).resolve().parent / "_ref" / "libgjxl_ref_cuda.so"
+_cuda_lib = None
+
+
+def cuda_available() -> bool:
+    return CUDA_LIBRARY_PATH.exists()
+
+
+def cuda_lib() -> ctypes.CDLL:
+    global _cuda_lib
+    if _cuda_lib is None:
+        if not CUDA_LIBRARY_PATH.exists():
+            raise FileNotFoundError(
+                f"{CUDA_LIBRARY_PATH} is missing; build it with `make -C oracle cuda`")
+        handle = ctypes.CDLL(str(CUDA_LIBRARY_PATH))
+        handle.gjxl_ref_cuda_last_error.restype = ctypes.c_char_p
+        handle.gjxl_ref_cuda_init.restype = c_int
+        handle.gjxl_ref_cuda_encode.argtypes = [_P, _Z, _Z, _F, _I, _P, _Z, _P, _P, _P, _P]
+        handle.gjxl_ref_cuda_encode.restype = c_int
+        _cuda_lib = handle
+    return _cuda_lib
+
+
+def cuda_encode(linear: np.ndarray, target: float = 1.0, effort: int = 7) -> dict:
+    """The reference's whole encode on its CUDA backend, fully-resident AQ
+    (as its cuda_encoding_benchmark runs it): codestream bytes, final
+    Butteraugli score, and the workflow's analysis (quantization pipeline)
+    and total wall times in milliseconds."""
+    lib = cuda_lib()
+    code = lib.gjxl_ref_cuda_init()
+    if code != 0:
+        raise RuntimeError(f"gjxl_ref_cuda_init: status {code}: "
+                           f"{lib.gjxl_ref_cuda_last_error().decode()}")
+    linear = np.ascontiguousarray(linear, np.float32)
+    _, h, w = linear.shape
+    capacity = max(1 << 16, 4 * w * h)
+    out = np.empty(capacity, np.uint8)
+    size, score = c_size_t(0), c_double(0.0)
+    analysis, total = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    code = lib.gjxl_ref_cuda_encode(_ptr(linear), w, h, target, effort, _ptr(out), capacity,
+                                    ctypes.byref(size), ctypes.byref(score),
+                                    ctypes.byref(analysis), ctypes.byref(total))
+    if code != 0:
+        raise RuntimeError(f"gjxl_ref_cuda_encode: status {code}: "
+                           f"{lib.gjxl_ref_cuda_last_error().decode()}")
+    return {"codestream": out[:size.value].tobytes(), "score": score.value,
+            "analysis_ms": analysis.value / 1e6, "total_ms": total.value / 1e6}
