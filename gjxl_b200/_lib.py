@@ -53,12 +53,15 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_session_kernel_count": None,
     "gjxl_b200_fp64_throughput": [P, P, P],
     "gjxl_b200_check_device_error": [P, Z, P],
+    "gjxl_b200_butteraugli_pnorm_scratch_bytes": [],
+    "gjxl_b200_butteraugli_pnorm": [P, Z, Z, Z, c_double, P, Z, P, P],
     "gjxl_b200_test_arm_failure": [I, I],
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
              "gjxl_b200_ac_strategy_cost_bytes": c_size_t,
-             "gjxl_b200_ac_token_capacity": c_size_t}
+             "gjxl_b200_ac_token_capacity": c_size_t,
+             "gjxl_b200_butteraugli_pnorm_scratch_bytes": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

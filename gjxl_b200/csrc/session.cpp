@@ -133,6 +133,8 @@ struct Session {
   float* distance_map = nullptr;
   float* block_distance = nullptr;
   double* scores = nullptr;
+  double* pnorms = nullptr;       // FP64 p-norm (p = 3) of each evaluation's map
+  double* pnorm_scratch = nullptr;
   float* matrix_multipliers = nullptr;
   int* matrix_scales = nullptr;
   ButteraugliState* butteraugli = nullptr;
@@ -160,6 +162,7 @@ struct Session {
   int32_t* host_raw = nullptr;
   int32_t* host_qdc = nullptr;
   double* host_scores = nullptr;
+  double* host_pnorms = nullptr;
   AqQuantizer* host_quantizer = nullptr;
   int32_t* host_qac = nullptr;
   cudaEvent_t events[kStageCount + 1] = {};
@@ -260,6 +263,8 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->distance_map), image * sizeof(float)},
     {reinterpret_cast<void**>(&s->block_distance), blocks * sizeof(float)},
     {reinterpret_cast<void**>(&s->scores), 8 * sizeof(double)},
+    {reinterpret_cast<void**>(&s->pnorms), 8 * sizeof(double)},
+    {reinterpret_cast<void**>(&s->pnorm_scratch), PnormScratchBytes()},
     {reinterpret_cast<void**>(&s->matrix_multipliers), 4 * sizeof(float)},
     {reinterpret_cast<void**>(&s->matrix_scales), 4 * sizeof(int)},
     {reinterpret_cast<void**>(&s->tok_values), s->token_capacity * sizeof(uint32_t)},
@@ -283,8 +288,8 @@ int Allocate(Session* s) {
   // Pinned host mirrors.
   const size_t host_bytes = Align(blocks, 16) + Align(blocks * 4, 16) + Align(2 * tiles, 16) +
                             16 + 16 + Align(blocks * 4, 16) + Align(blocks * 4, 16) +
-                            Align(3 * blocks * 4, 16) + 64 + Align(sizeof(AqQuantizer), 16) +
-                            Align(3 * plane * 4, 16);
+                            Align(3 * blocks * 4, 16) + 64 + 64 +
+                            Align(sizeof(AqQuantizer), 16) + Align(3 * plane * 4, 16);
   void* host = nullptr;
   status = CheckCuda(HostMalloc(&host, host_bytes), "session: cudaMallocHost");
   if (status != GJXL_B200_OK) return status;
@@ -304,6 +309,7 @@ int Allocate(Session* s) {
   s->host_raw = reinterpret_cast<int32_t*>(take(blocks * 4));
   s->host_qdc = reinterpret_cast<int32_t*>(take(3 * blocks * 4));
   s->host_scores = reinterpret_cast<double*>(take(64));
+  s->host_pnorms = reinterpret_cast<double*>(take(64));
   s->host_quantizer = reinterpret_cast<AqQuantizer*>(take(sizeof(AqQuantizer)));
   s->host_qac = reinterpret_cast<int32_t*>(take(3 * plane * 4));
   status = ButteraugliCreate(s->width, s->height, 80.0f, &s->butteraugli);
@@ -400,6 +406,8 @@ int RunAq(Session* s, cudaStream_t stream) {
                              s->rec_linear, s->error, stream));
     GJXL_TRY(ButteraugliCompare(s->butteraugli, s->rec_linear, s->width, s->width * s->height,
                                 s->distance_map, s->width, s->scores + iteration, stream));
+    GJXL_TRY(LaunchPnorm(s->distance_map, s->width, s->width, s->height, 3.0,
+                         s->pnorm_scratch, s->pnorms + iteration, stream));
     GJXL_TRY(AqBlockReduce(s->cells, s->bx, s->by, s->distance_map, s->width, s->height,
                            s->block_distance, stream));
     if (iteration < s->iterations) {
@@ -562,6 +570,7 @@ int CopyOutputs(Session* s, cudaStream_t stream) {
     {s->host_raw, s->raw, blocks * sizeof(int32_t)},
     {s->host_qdc, s->qdc, 3 * blocks * sizeof(int32_t)},
     {s->host_scores, s->scores, (s->iterations + 1) * sizeof(double)},
+    {s->host_pnorms, s->pnorms, (s->iterations + 1) * sizeof(double)},
     {s->host_quantizer, s->quantizer, sizeof(AqQuantizer)},
     // Quantized AC returns to the host only without tokenization (the tokens
     // carry it otherwise).
@@ -792,6 +801,8 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   }
   out->host_token_count = s->host_token_count;
   out->device_bytes = s->arena_bytes;
+  out->pnorm_history = s->pnorms;
+  out->host_pnorm_history = s->host_pnorms;
   out->input_pixels = s->pixels;
   out->input_capacity = s->pixel_capacity;
   out->graph_replay = s->graph != nullptr ? 1 : 0;

@@ -44,4 +44,9 @@ int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride,
                        float* map, size_t map_stride, double* score, cudaStream_t stream);
 uint32_t* ButteraugliErrorWord(ButteraugliState* st);
 
+// FP64 global Butteraugli p-norm of a distance map (pnorm.cu).
+size_t PnormScratchBytes();
+int LaunchPnorm(const float* map, size_t stride, size_t width, size_t height, double p,
+                double* scratch, double* out, cudaStream_t stream);
+
 }  // namespace gjxl_b200

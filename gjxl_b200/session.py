@@ -38,7 +38,8 @@ class Outputs(Structure):
             "token_values", "token_contexts", "group_offsets", "token_histogram", "scans",
             "order_masks", "host_token_values", "host_token_contexts", "host_group_offsets")] + [
         ("host_token_count", c_size_t), ("device_bytes", c_size_t),
-        ("input_pixels", c_void_p), ("input_capacity", c_size_t), ("graph_replay", c_int)]
+        ("input_pixels", c_void_p), ("input_capacity", c_size_t), ("graph_replay", c_int),
+        ("pnorm_history", c_void_p), ("host_pnorm_history", c_void_p)]
 
 
 _BOUND = False
@@ -182,6 +183,8 @@ class AnalysisSession:
             "raw_quant": self._host("host_raw_quant_field", ctypes.c_int32, blocks),
             "quantized_dc": self._host("host_quantized_dc", ctypes.c_int32, (3,) + blocks),
             "score_history": self._host("host_score_history", ctypes.c_double,
+                                        (o.iterations + 1,)),
+            "pnorm_history": self._host("host_pnorm_history", ctypes.c_double,
                                         (o.iterations + 1,)),
             "quantizer_params": self._host("host_quantizer_params", ctypes.c_uint32, (2,)),
         } | self.host_tokens() | ({} if o.host_token_values else {

@@ -259,6 +259,22 @@ GJXL_B200_API int gjxl_b200_butteraugli_compare(
     size_t plane_pitch, float* distance_map, size_t map_stride,
     double* score, uint32_t* device_error, void* stream);
 
+/*
+ * Global Butteraugli p-norm of a distance map (width x height floats, row
+ * stride map_stride), accumulated in double precision: the mean of the p-,
+ * 2p- and 4p-norms, ((S_p/n)^(1/p) + (S_2p/n)^(1/2p) + (S_4p/n)^(1/4p)) / 3
+ * with S_q the sum of d^q over the n pixels (libjxl's published p-norm
+ * summary; the reference summarises a map by its maximum only,
+ * src/gpu/cuda/cuda_butteraugli_kernels.cu:4063-4065). Writes one device
+ * double; fixed reduction order, so repeated calls agree to the bit.
+ * `scratch`: device memory of gjxl_b200_butteraugli_pnorm_scratch_bytes().
+ */
+GJXL_B200_API size_t gjxl_b200_butteraugli_pnorm_scratch_bytes(void);
+GJXL_B200_API int gjxl_b200_butteraugli_pnorm(const float* distance_map, size_t map_stride,
+                                              size_t width, size_t height, double p,
+                                              double* scratch, size_t scratch_bytes,
+                                              double* pnorm, void* stream);
+
 /* ------------------------------------------------------------------------
  * AC group packing, coefficient-order populations and AC tokenization
  * (rows a17, a18).
@@ -420,6 +436,11 @@ typedef struct gjxl_b200_outputs {
   uint8_t* input_pixels;
   size_t input_capacity;
   int graph_replay;                 /* 1 once analyses replay a captured graph */
+  /* FP64 global Butteraugli p-norm (p = 3, gjxl_b200_butteraugli_pnorm) of
+   * each evaluation's distance map, iterations + 1 values: device, then the
+   * host mirror filled by gjxl_b200_session_analyze_host. */
+  const double* pnorm_history;
+  const double* host_pnorm_history;
 } gjxl_b200_outputs;
 
 typedef struct gjxl_b200_session gjxl_b200_session;

@@ -73,3 +73,19 @@ def select_matrix_scales(stats: np.ndarray, target: float) -> tuple[int, int]:
     out = np.zeros(2, np.int32)
     lib().restate_select_matrix_scales(_ptr(stats), target, _ptr(out))
     return int(out[0]), int(out[1])
+
+
+def butteraugli_pnorm(distance_map: np.ndarray, p: float = 3.0) -> float:
+    """Global p-norm of a distance map in double precision, restated from
+    libjxl's published p-norm summary (the mean of the p-, 2p- and 4p-norms,
+    ((S_p/n)^(1/p) + (S_2p/n)^(1/2p) + (S_4p/n)^(1/4p)) / 3, S_q = sum d^q
+    with d^p of each pixel in double, squared for 2p and again for 4p). The
+    reference itself has no p-norm (its score is the maximum). Sums in
+    numpy's pairwise order: the device's fixed tree order differs, within
+    1e-12 relative."""
+    d = np.asarray(distance_map, np.float32).astype(np.float64).ravel()
+    dp = d * d * d if p == 3.0 else np.power(d, p)
+    d2p = dp * dp
+    n = float(d.size)
+    sums = (dp.sum(), d2p.sum(), (d2p * d2p).sum())
+    return float(sum((s / n) ** (1.0 / (p * (1 << i))) for i, s in enumerate(sums)) / 3.0)

@@ -73,3 +73,16 @@ def test_restated_matrix_scale_selection_matches_reference():
                         ref.select_matrix_scales(stats, t), (stats, t)
                     checked += 1
     assert checked == len(xs) * len(bs) * len(es) * len(targets)
+
+
+def test_pnorm_restatement_properties():
+    """The FP64 p-norm restatement: a constant map is its own norm, the norm
+    is positively homogeneous, and it lies between the mean and the maximum
+    of the map for p >= 1."""
+    const = np.full((31, 17), 1.75, np.float32)
+    assert abs(restate.butteraugli_pnorm(const, 3.0) - 1.75) <= 1e-14
+    m = np.abs(np.random.default_rng(7).standard_normal((64, 48))).astype(np.float32)
+    a = restate.butteraugli_pnorm(m, 3.0)
+    b = restate.butteraugli_pnorm((2 * m).astype(np.float32), 3.0)
+    assert abs(b - 2 * a) <= 1e-13 * b
+    assert m.astype(np.float64).mean() <= a <= float(m.max())

@@ -176,6 +176,10 @@ def compare_loop_exact(s: AnalysisSession, got: dict, want: dict) -> None:
     check_block_distance(s, got, want)
     rec = device_to_host(o.reconstructed_linear, (3, h, w), np.float32)
     assert_bitexact(rec, want["reconstructed"], "reconstructed linear RGB")
+    # FP64 p-norm of the last evaluation's (bit-exact) distance map.
+    dmap = device_to_host(o.distance_map, (h, w), np.float32)
+    pn = restate.butteraugli_pnorm(dmap, 3.0)
+    assert abs(got["pnorm_history"][-1] - pn) <= 1e-12 * pn
 
 
 def compare_loop_fed_back(s: AnalysisSession, got: dict, want: dict) -> int:
