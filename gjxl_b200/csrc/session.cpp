@@ -100,6 +100,7 @@ struct Session {
   float* strategy_mask = nullptr;
   float* pixel_mask = nullptr;
   float* iq_scratch = nullptr;
+  void* cfl_scratch = nullptr;  // initial CfL (a, b) pairs, 64 KB per 64x64 tile
   int8_t* y_to_x = nullptr;
   int8_t* y_to_b = nullptr;
   float* costs = nullptr;
@@ -231,6 +232,7 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->strategy_mask), blocks * sizeof(float)},
     {reinterpret_cast<void**>(&s->pixel_mask), plane * sizeof(float)},
     {reinterpret_cast<void**>(&s->iq_scratch), InitialQuantScratchFloats(s->pw, s->ph) * 4},
+    {&s->cfl_scratch, InitialCflScratchBytes(s->pw, s->ph)},
     {reinterpret_cast<void**>(&s->y_to_x), tiles},
     {reinterpret_cast<void**>(&s->y_to_b), tiles},
     {reinterpret_cast<void**>(&s->costs), AcStrategyCostFloats(s->bx, s->by) * sizeof(float)},
@@ -459,7 +461,8 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
   GJXL_TRY(LaunchGaborishInverse(s->opsin, s->pw, s->pitch, s->pre, s->pw, s->pitch, s->pw,
                                  s->ph, multipliers, s->error, stream));
   Mark(s, kStageInitialCfl, stream);
-  GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b, stream));
+  GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b,
+                            s->cfl_scratch, s->error, stream));
   Mark(s, kStageAcCosts, stream);
   const StreamFan fan = MakeFan(s, stream);
   const bool dense = s->options.effort >= 10;
@@ -667,6 +670,24 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
 }
 
 extern "C" void gjxl_b200_session_destroy(gjxl_b200_session* session) { delete session; }
+
+extern "C" int gjxl_b200_session_set_butteraugli_target(gjxl_b200_session* s, float target) {
+  ClearLastError();
+  if (s == nullptr || !std::isfinite(target) || target <= 0.0f) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT,
+                    "session_set_butteraugli_target: invalid arguments");
+  }
+  if (s->options.butteraugli_target != target) {
+    s->options.butteraugli_target = target;
+    // The captured graph holds the old target's constants: capture again on
+    // the next analysis. Every buffer is kept.
+    if (s->graph != nullptr) {
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+  }
+  return GJXL_B200_OK;
+}
 
 extern "C" int gjxl_b200_session_analyze(gjxl_b200_session* s, const uint8_t* pixels,
                                          size_t row_stride, int channels, void* stream) {

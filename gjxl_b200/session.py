@@ -57,6 +57,8 @@ def _bind():
     lib.gjxl_b200_session_create.restype = c_int
     lib.gjxl_b200_session_destroy.argtypes = [c_void_p]
     lib.gjxl_b200_session_destroy.restype = None
+    lib.gjxl_b200_session_set_butteraugli_target.argtypes = [c_void_p, c_float]
+    lib.gjxl_b200_session_set_butteraugli_target.restype = c_int
     lib.gjxl_b200_session_analyze.argtypes = [c_void_p, c_void_p, c_size_t, c_int, c_void_p]
     lib.gjxl_b200_session_analyze.restype = c_int
     lib.gjxl_b200_session_analyze_host.argtypes = [c_void_p, c_void_p, c_size_t, c_int, c_void_p]
@@ -104,6 +106,11 @@ class AnalysisSession:
         self.outputs = Outputs()
         _check(lib.gjxl_b200_session_outputs(handle, ctypes.byref(self.outputs)),
                "gjxl_b200_session_outputs")
+
+    def set_butteraugli_target(self, target: float):
+        """Retargets later analyses; every buffer is kept."""
+        _check(_lib.load().gjxl_b200_session_set_butteraugli_target(self.handle, target),
+               "gjxl_b200_session_set_butteraugli_target")
 
     def close(self):
         if self.handle:

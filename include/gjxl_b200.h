@@ -155,13 +155,18 @@ GJXL_B200_API int gjxl_b200_gaborish_inverse(
  * PreparedQuantizationPipeline preprocessing
  * (src/codec/quantization_pipeline.cpp:155-213). Input: the Gaborish-inverted
  * padded XYB image. Outputs: int8 y_to_x and y_to_b per 64x64 tile (dense,
- * ceil(padded_width/64) x ceil(padded_height/64)).
+ * ceil(padded_width/64) x ceil(padded_height/64)). `scratch`: 16-byte aligned
+ * device memory of gjxl_b200_initial_cfl_scratch_bytes() bytes (64 KB per
+ * tile: the coefficient pairs of the Newton solve).
  */
+GJXL_B200_API size_t gjxl_b200_initial_cfl_scratch_bytes(size_t padded_width,
+                                                         size_t padded_height);
 GJXL_B200_API int gjxl_b200_initial_cfl(const float* opsin, size_t opsin_stride,
                                         size_t opsin_plane_pitch,
                                         size_t padded_width,
                                         size_t padded_height, int8_t* y_to_x,
-                                        int8_t* y_to_b, void* stream);
+                                        int8_t* y_to_b, void* scratch,
+                                        size_t scratch_bytes, void* stream);
 
 /*
  * Default AC quantization matrix of one searched strategy and channel, in the
@@ -450,6 +455,12 @@ GJXL_B200_API int gjxl_b200_session_create(size_t width, size_t height,
                                            const gjxl_b200_options* options,
                                            gjxl_b200_session** session);
 GJXL_B200_API void gjxl_b200_session_destroy(gjxl_b200_session* session);
+/* Changes the Butteraugli target of later analyses, keeping every buffer of
+ * the session (the prepared state a target-size search reuses across its
+ * attempts: src/codestream/workflow.cpp:1686-1740, rate_control.cpp:246).
+ * The next analysis captures its graph again. */
+GJXL_B200_API int gjxl_b200_session_set_butteraugli_target(gjxl_b200_session* session,
+                                                           float butteraugli_target);
 /* Device-resident input: packed 8-bit sRGB already in device memory. The
  * first call for a channel count captures the analysis into a CUDA graph
  * over the session's input buffer; later calls replay it. Input anywhere

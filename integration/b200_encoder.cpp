@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -46,6 +47,7 @@
 #include "codec/vardct_frame_view_internal.h"
 #include "codestream/ac_tokenization_provider_internal.h"
 #include "codestream/encoder_internal.h"
+#include "codestream/rate_control_internal.h"
 #include "codestream/workflow.h"
 #include "codestream/workflow_internal.h"
 #include "core/ac_strategy.h"
@@ -430,6 +432,83 @@ class B200AcTokenizer final : public codestream_internal::AcTokenizationProvider
   std::vector<uint16_t> contexts_;
 };
 
+// One complete attempt on a prepared session: the analysis at the session's
+// current target, the frame, and the unchanged serializer. Fills the summary
+// fields a target-size search reads (rate_control.cpp:140-165).
+Status EncodeWithSession(gjxl_b200_session* session, const uint8_t* pixels, size_t width,
+                         size_t height, size_t row_stride, int channels, float target,
+                         int effort, bool device_tokens, std::vector<uint8_t>* codestream,
+                         VarDctEncodingSummary* summary) {
+  VarDctEncodingOptions options;
+  options.butteraugli_target = target;
+  options.effort = effort;
+  Status status = FromB200(gjxl_b200_session_set_butteraugli_target(session, target),
+                           "session_set_butteraugli_target");
+  if (!status.ok()) return status;
+  status = FromB200(gjxl_b200_session_analyze_host(session, pixels, row_stride, channels,
+                                                   nullptr),
+                    "session_analyze_host");
+  if (!status.ok()) return status;
+  gjxl_b200_outputs o;
+  status = FromB200(gjxl_b200_session_outputs(session, &o), "session_outputs");
+  if (!status.ok()) return status;
+  SessionResults results;
+  status = ReadSession(o, width, height, &results);
+  if (!status.ok()) return status;
+  ResolvedEncode resolved;
+  status = ResolveEncodeOptions(options, results.stats, &resolved);
+  if (!status.ok()) return status;
+  const auto& profile = resolved.pipeline.adaptive_quantization.profile;
+  if (results.device_matrix_scales[0] != profile.x_qm_scale ||
+      results.device_matrix_scales[1] != profile.b_qm_scale) {
+    return Status::Internal("device quantization-matrix scales differ from the workflow's");
+  }
+  VarDctEncoderFrame frame;
+  status = AssembleB200Frame(results, profile, &frame);
+  if (!status.ok()) return status;
+  std::unique_ptr<B200AcTokenizer> tokenizer;
+  if (device_tokens) {
+    tokenizer = std::make_unique<B200AcTokenizer>(o, resolved.codestream.coefficient_order_behavior);
+  }
+  codestream_internal::CodestreamBuffer buffer;
+  {
+    codestream_internal::AcTokenizationProviderScope scope(tokenizer.get());
+    status = codestream_internal::EncodeVarDctCodestreamToBuffer(
+      vardct_frame_internal::BorrowFrame(frame), resolved.codestream, &buffer);
+  }
+  if (!status.ok()) return status;
+  codestream->assign(buffer.data(), buffer.data() + buffer.size());
+  if (summary != nullptr) {
+    *summary = VarDctEncodingSummary{};
+    summary->extent = {width, height};
+    summary->encoded_bytes = codestream->size();
+    summary->rate_control_mode = VarDctRateControlMode::kButteraugliTarget;
+    summary->selected_butteraugli_target = target;
+    summary->score_history.assign(o.host_score_history,
+                                  o.host_score_history + o.iterations + 1);
+  }
+  return Status::Ok();
+}
+
+struct SessionOwner {
+  gjxl_b200_session* session = nullptr;
+  ~SessionOwner() {
+    if (session != nullptr) gjxl_b200_session_destroy(session);
+  }
+};
+
+Status CreateSession(size_t width, size_t height, float target, int effort, int precision,
+                     SessionOwner* owner) {
+  gjxl_b200_options session_options;
+  gjxl_b200_default_options(&session_options);
+  session_options.butteraugli_target = target;
+  session_options.effort = effort;
+  session_options.tokenize = 0;  // the serializer asks for its own map's tokens
+  session_options.precision = precision;
+  return FromB200(gjxl_b200_session_create(width, height, &session_options, &owner->session),
+                  "session_create");
+}
+
 }  // namespace
 }  // namespace gjxl::b200_integration
 
@@ -452,59 +531,69 @@ GJXL_INTEGRATION_API int gjxl_b200_encode_image(const uint8_t* pixels, size_t wi
                                                 int precision, int device_tokens, uint8_t* out,
                                                 size_t capacity, size_t* size, double* score) {
   g_last_error.clear();
-  VarDctEncodingOptions options;
-  options.butteraugli_target = butteraugli_target;
-  options.effort = effort;
-  gjxl_b200_options session_options;
-  gjxl_b200_default_options(&session_options);
-  session_options.butteraugli_target = butteraugli_target;
-  session_options.effort = effort;
-  session_options.tokenize = 0;  // the serializer asks for its own map's tokens
-  session_options.precision = precision;
-  gjxl_b200_session* session = nullptr;
-  Status status = FromB200(gjxl_b200_session_create(width, height, &session_options, &session),
-                           "session_create");
+  SessionOwner owner;
+  Status status = CreateSession(width, height, butteraugli_target, effort, precision, &owner);
   if (!status.ok()) return Fail(status);
-  std::unique_ptr<gjxl_b200_session, void (*)(gjxl_b200_session*)> owner(
-    session, gjxl_b200_session_destroy);
-  status = FromB200(gjxl_b200_session_analyze_host(session, pixels, row_stride, channels,
-                                                   nullptr),
-                    "session_analyze_host");
+  std::vector<uint8_t> bytes;
+  VarDctEncodingSummary summary;
+  status = EncodeWithSession(owner.session, pixels, width, height, row_stride, channels,
+                             butteraugli_target, effort, device_tokens != 0, &bytes, &summary);
   if (!status.ok()) return Fail(status);
-  gjxl_b200_outputs o;
-  status = FromB200(gjxl_b200_session_outputs(session, &o), "session_outputs");
-  if (!status.ok()) return Fail(status);
-  SessionResults results;
-  status = ReadSession(o, width, height, &results);
-  if (!status.ok()) return Fail(status);
-  ResolvedEncode resolved;
-  status = ResolveEncodeOptions(options, results.stats, &resolved);
-  if (!status.ok()) return Fail(status);
-  const auto& profile = resolved.pipeline.adaptive_quantization.profile;
-  if (results.device_matrix_scales[0] != profile.x_qm_scale ||
-      results.device_matrix_scales[1] != profile.b_qm_scale) {
-    return Fail(Status::Internal("device quantization-matrix scales differ from the workflow's"));
-  }
-  VarDctEncoderFrame frame;
-  status = AssembleB200Frame(results, profile, &frame);
-  if (!status.ok()) return Fail(status);
-  std::unique_ptr<B200AcTokenizer> tokenizer;
-  if (device_tokens) {
-    tokenizer = std::make_unique<B200AcTokenizer>(o, resolved.codestream.coefficient_order_behavior);
-  }
-  codestream_internal::CodestreamBuffer buffer;
-  {
-    codestream_internal::AcTokenizationProviderScope scope(tokenizer.get());
-    status = codestream_internal::EncodeVarDctCodestreamToBuffer(
-      vardct_frame_internal::BorrowFrame(frame), resolved.codestream, &buffer);
-  }
-  if (!status.ok()) return Fail(status);
-  *size = buffer.size();
-  if (score != nullptr) *score = o.host_score_history[o.iterations];
-  if (buffer.size() > capacity) {
+  *size = bytes.size();
+  if (score != nullptr) *score = summary.score_history.back();
+  if (bytes.size() > capacity) {
     g_last_error = "codestream capacity exceeded";
     return -2;
   }
-  std::memcpy(out, buffer.data(), buffer.size());
+  std::memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}
+
+// Target-size rate control with the B200 analysis: the reference's own
+// bounded search over complete encodes (codestream_internal::SearchTargetSize,
+// src/codestream/rate_control.cpp:246-320, as the workflow runs it at
+// workflow.cpp:1686-1740) with an evaluator that retargets one prepared
+// session per attempt (no reallocation between attempts) and serializes with
+// the unchanged writer. tolerance is the relative byte tolerance (the
+// workflow's target_size_tolerance), selection kLargestAtOrBelow. Writes the
+// selected codestream, its Butteraugli target, the attempt count and whether
+// the size is within tolerance.
+GJXL_INTEGRATION_API int gjxl_b200_encode_target_size(
+  const uint8_t* pixels, size_t width, size_t height, size_t row_stride, int channels,
+  int effort, int precision, size_t target_bytes, double tolerance, size_t maximum_attempts,
+  uint8_t* out, size_t capacity, size_t* size, float* selected_target, size_t* attempts,
+  int* target_met) {
+  g_last_error.clear();
+  if (target_bytes == 0 || !(tolerance >= 0.0 && tolerance <= 1.0) || maximum_attempts == 0 ||
+      maximum_attempts > codestream_internal::kMaximumTargetSizeEncodeAttempts) {
+    return Fail(Status::InvalidArgument("target-size options are invalid"));
+  }
+  SessionOwner owner;
+  Status status = CreateSession(width, height, 1.0f, effort, precision, &owner);
+  if (!status.ok()) return Fail(status);
+  codestream_internal::TargetSizeSearchOptions options;
+  options.target_bytes = target_bytes;
+  options.tolerance_bytes = static_cast<size_t>(
+    std::ceil(static_cast<long double>(target_bytes) * static_cast<long double>(tolerance)));
+  options.maximum_attempts = maximum_attempts;
+  options.selection = TargetSizeSelectionPolicy::kLargestAtOrBelow;
+  codestream_internal::TargetSizeSearchResult result;
+  status = codestream_internal::SearchTargetSize(
+    options,
+    [&](float target, std::vector<uint8_t>* codestream, VarDctEncodingSummary* summary) {
+      return EncodeWithSession(owner.session, pixels, width, height, row_stride, channels,
+                               target, effort, false, codestream, summary);
+    },
+    &result);
+  if (!status.ok()) return Fail(status);
+  *size = result.codestream.size();
+  *selected_target = result.summary.selected_butteraugli_target;
+  *attempts = result.attempt_count;
+  *target_met = result.target_size_met ? 1 : 0;
+  if (result.codestream.size() > capacity) {
+    g_last_error = "codestream capacity exceeded";
+    return -2;
+  }
+  std::memcpy(out, result.codestream.data(), result.codestream.size());
   return 0;
 }

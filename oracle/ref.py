@@ -31,6 +31,8 @@ _SIGNATURES = {
     "gjxl_ref_matrix_scale_stats": [_P, _Z, _Z, _Z, _Z, _P],
     "gjxl_ref_select_matrix_scales": [_P, _F, _P],
     "gjxl_ref_encode_cpu": [_P, _Z, _Z, _F, _I, _P, _Z, _P, _P],
+    "gjxl_ref_encode_cpu_target_size": [_P, _Z, _Z, _Z, c_double, _Z, _I, _P, _Z, _P, _P,
+                                        _P, _P],
 }
 
 _lib = None
@@ -144,6 +146,24 @@ def encode_cpu(linear: np.ndarray, target: float = 1.0, effort: int = 7) -> tupl
     _check(lib().gjxl_ref_encode_cpu(_ptr(linear), w, h, target, effort, _ptr(out), capacity,
                                      ctypes.byref(size), ctypes.byref(score)), "encode_cpu")
     return out[:size.value].tobytes(), score.value
+
+
+def encode_cpu_target_size(linear: np.ndarray, target_bytes: int, tolerance: float = 0.005,
+                           maximum_attempts: int = 12, effort: int = 7) -> dict:
+    """The reference's whole CPU encode under target-size rate control
+    (kTargetBytes, its bounded search over complete encodes)."""
+    linear = np.ascontiguousarray(linear, np.float32)
+    _, h, w = linear.shape
+    capacity = max(1 << 16, 4 * w * h)
+    out = np.empty(capacity, np.uint8)
+    size, target = c_size_t(0), c_float(0.0)
+    attempts, met = c_size_t(0), c_int(0)
+    _check(lib().gjxl_ref_encode_cpu_target_size(
+        _ptr(linear), w, h, target_bytes, tolerance, maximum_attempts, effort, _ptr(out),
+        capacity, ctypes.byref(size), ctypes.byref(target), ctypes.byref(attempts),
+        ctypes.byref(met)), "encode_cpu_target_size")
+    return {"codestream": out[:size.value].tobytes(), "target": target.value,
+            "attempts": attempts.value, "met": bool(met.value)}
 
 
 def initial_quant_field(opsin: np.ndarray, target: float = 1.0, rescale: float = 1.0,

@@ -670,3 +670,39 @@ GJXL_REF_API int gjxl_ref_encode_cpu(const float* linear, size_t width, size_t h
   std::memcpy(out, bytes.data(), bytes.size());
   return 0;
 }
+
+// The reference's whole CPU encode under target-size rate control
+// (VarDctRateControlMode::kTargetBytes: the bounded search of
+// src/codestream/rate_control.cpp over complete encodes, workflow.cpp:1686).
+// Writes the selected codestream, its Butteraugli target, the attempt count
+// and whether the size met the tolerance.
+GJXL_REF_API int gjxl_ref_encode_cpu_target_size(const float* linear, size_t width,
+                                                 size_t height, size_t target_bytes,
+                                                 double tolerance, size_t maximum_attempts,
+                                                 int effort, uint8_t* out, size_t capacity,
+                                                 size_t* size, float* selected_target,
+                                                 size_t* attempts, int* target_met) {
+  VarDctEncodingOptions options;
+  options.effort = effort;
+  options.backend = VarDctBackendPreference::kCpu;
+  options.cpu_thread_count = g_threads;
+  options.rate_control_mode = VarDctRateControlMode::kTargetBytes;
+  options.target_bytes = target_bytes;
+  options.target_size_tolerance = tolerance;
+  options.target_size_maximum_attempts = maximum_attempts;
+  std::vector<uint8_t> bytes;
+  VarDctEncodingSummary summary;
+  Status status = EncodeLinearRgbVarDctCodestream(ConstPlanar(linear, width, height), options,
+                                                  &bytes, &summary);
+  if (!status.ok()) return Fail(status);
+  *size = bytes.size();
+  *selected_target = summary.selected_butteraugli_target;
+  *attempts = summary.encode_attempt_count;
+  *target_met = summary.target_size_met ? 1 : 0;
+  if (bytes.size() > capacity) {
+    g_last_error = "codestream capacity exceeded";
+    return -2;
+  }
+  std::memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}

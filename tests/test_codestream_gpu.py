@@ -125,3 +125,55 @@ def test_against_reference_cuda_path(cuda, w, h, seed):
         size_rel = abs(len(ours) - len(theirs["codestream"])) / len(theirs["codestream"])
         assert size_rel <= 2e-3, (precision, len(ours), len(theirs["codestream"]))
         assert abs(score - theirs["score"]) <= 3e-2 * theirs["score"], (score, theirs["score"])
+
+
+def b200_encode_target_size(img, target_bytes, tolerance=0.005, attempts=12, precision=0):
+    import torch  # noqa: F401
+    lib = encoder()
+    fn = lib.gjxl_b200_encode_target_size
+    fn.argtypes = [c_void_p, c_size_t, c_size_t, c_size_t, c_int, c_int, c_int, c_size_t,
+                   c_double, c_size_t, c_void_p, c_size_t, ctypes.POINTER(c_size_t),
+                   ctypes.POINTER(c_float), ctypes.POINTER(c_size_t), ctypes.POINTER(c_int)]
+    fn.restype = c_int
+    img = np.ascontiguousarray(img)
+    h, w, ch = img.shape
+    capacity = max(1 << 16, 4 * w * h)
+    out = np.empty(capacity, np.uint8)
+    size, target, n, met = c_size_t(0), c_float(0.0), c_size_t(0), c_int(0)
+    rc = fn(img.ctypes.data, w, h, w * ch, ch, 7, precision, target_bytes, tolerance, attempts,
+            out.ctypes.data, capacity, ctypes.byref(size), ctypes.byref(target), ctypes.byref(n),
+            ctypes.byref(met))
+    assert rc == 0, lib.gjxl_b200_integration_last_error().decode()
+    return {"codestream": out[:size.value].tobytes(), "target": target.value,
+            "attempts": n.value, "met": bool(met.value)}
+
+
+@pytest.mark.parametrize("fraction", [0.7, 1.3])
+def test_target_size_rate_control_matches_reference(cuda, fraction):
+    """Target-size rate control (row f4): the reference's own bounded search
+    (codestream_internal::SearchTargetSize, src/codestream/rate_control.cpp)
+    driving one prepared B200 session retargeted per attempt, against the
+    reference's CPU target-size encode of the same image. Every attempt's
+    analysis matches the CPU path (within 0.1% of blocks), so the searches take
+    the same steps: the same selected Butteraugli target and attempt count,
+    or, if one attempt's size lands on the other side of the tolerance edge,
+    selected sizes within 1% of each other."""
+    img = generate_srgb8(256, 192, 31)
+    lin = ref.srgb8_to_linear(img)
+    base, _ = ref.encode_cpu(lin, 1.0, 7)
+    target_bytes = int(len(base) * fraction)
+    want = ref.encode_cpu_target_size(lin, target_bytes)
+    got = b200_encode_target_size(img, target_bytes)
+    assert got["codestream"][:2] == b"\xff\x0a"
+    assert 1 <= got["attempts"] <= 12
+    if got["target"] == want["target"]:
+        assert got["attempts"] == want["attempts"]
+        assert got["met"] == want["met"]
+        assert abs(len(got["codestream"]) - len(want["codestream"])) <= \
+            2e-3 * len(want["codestream"])
+    else:
+        assert abs(len(got["codestream"]) - len(want["codestream"])) <= \
+            1e-2 * len(want["codestream"])
+    if got["met"]:
+        assert target_bytes - len(got["codestream"]) <= int(np.ceil(target_bytes * 0.005))
+        assert len(got["codestream"]) <= target_bytes
