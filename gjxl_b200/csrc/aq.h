@@ -53,8 +53,14 @@ int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, co
              const AqQuantizer* q, const int8_t* y_to_x, const int8_t* y_to_b,
              const float* matrix_multiplier, uint32_t* error, cudaStream_t stream,
              const StreamFan* fan = nullptr);
+// Prediction-aware DC quantization; with `tokens`, also the weighted-predictor
+// DC token stream (DcTokenOffset layout), residual range errors to `error`.
 int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, int32_t* quantized,
-                 float* reconstructed, int extra_precision, cudaStream_t stream);
+                 float* reconstructed, int extra_precision, uint2* tokens, uint32_t* error,
+                 cudaStream_t stream);
+// The weighted-predictor DC tokens of quantized DC (3 planes of `pitch`).
+int DcWeightedTokens(const int32_t* quantized, size_t pitch, size_t bx, size_t by, uint2* tokens,
+                     uint32_t* error, cudaStream_t stream);
 int AqInverseSigma(const uint8_t* cells, size_t bx, size_t by, const int32_t* raw,
                    const AqQuantizer* q, float* inverse_sigma, cudaStream_t stream);
 

@@ -26,6 +26,7 @@
 
 #include "aq.h"
 #include "common.cuh"
+#include "dc_tokens.cuh"
 #include "host_util.h"
 #include "line_dct.cuh"
 #include "tables.h"
@@ -1040,6 +1041,13 @@ struct DcQuantParams {
   size_t pitch;
   const AqQuantizer* q;
   float precision;  // 1 << extra_dc_precision
+  // Replay: `replay` holds quantized DC already (3 planes of `pitch`) and the
+  // kernel only runs the predictor over it, for its tokens.
+  const int32_t* replay;
+  // Optional DC tokens (context, packed residual) in the encoder's stream
+  // order (DcTokenOffset), and the error word for a residual outside int32.
+  uint2* tokens;
+  uint32_t* error;
 };
 
 constexpr int kDcGroup = 256;
@@ -1055,6 +1063,7 @@ struct DcRings {
   uint32_t pe[3][4][kDcRing][kDcGroup];   // sub-predictor errors (prediction_errors_)
   uint32_t row0[3][4][kDcRing];           // row 0's own errors, before row 1 adds
   uint32_t reciprocal[64];                // (1 << 24) / (i + 1)
+  uint8_t contexts[1024];                 // DC tree leaf of 512 + property
   int wide;  // set once a stored value leaves the 32-bit bounds below
 };
 
@@ -1077,14 +1086,17 @@ constexpr float kDcNarrowScaled = 2097152.0f;  // 2^21
 // neighbours' quantized values and signed errors, the four sub-predictor
 // error sums and value * inverse step in; the quantized value, its signed
 // error and the four sub-predictor errors out.
-template <typename Int, bool kWide>
+// In replay form (kReplay) the sample's quantized value comes in through
+// *quantized_out and only the prediction and the update run.
+template <typename Int, bool kWide, bool kReplay = false>
 __device__ __forceinline__ void WeightedPredictorStep(Int w, Int n, Int nw, Int ne, Int nn, Int ew,
                                                       Int en, Int enw, Int ene,
                                                       const uint32_t (&errors)[4],
                                                       const uint32_t* reciprocal,
                                                       float scaled_value, int32_t* quantized_out,
                                                       int32_t* error_out,
-                                                      uint32_t (&sub_errors)[4]) {
+                                                      uint32_t (&sub_errors)[4],
+                                                      int64_t* predicted_out) {
   // WeightedPredictorParameters defaults (prediction.h:36-40).
   constexpr int kP0 = 16, kP1 = 10, kP2 = 7, kP3 = 7, kP4 = 7, kP5 = 0, kP6 = 0;
   const uint32_t max_weights[4] = {13, 12, 12, 12};
@@ -1122,13 +1134,19 @@ __device__ __forceinline__ void WeightedPredictorStep(Int w, Int n, Int nw, Int 
     prediction = min(max(prediction, lo), hi);
   }
   const Int predicted = (prediction + 3) >> 3;
-  float residual = scaled_value;
-  residual -= static_cast<float>(predicted);
-  if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
-  float rounded = roundf(residual);
-  if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
-  const Int quantized = predicted + static_cast<Int>(rounded);
-  *quantized_out = static_cast<int32_t>(quantized);
+  *predicted_out = static_cast<int64_t>(predicted);
+  Int quantized;
+  if (kReplay) {
+    quantized = static_cast<Int>(*quantized_out);
+  } else {
+    float residual = scaled_value;
+    residual -= static_cast<float>(predicted);
+    if (residual > -0.62f && residual < 0.62f) residual = 0.0f;
+    float rounded = roundf(residual);
+    if (rounded > 2.0f || rounded < -2.0f) rounded = roundf(residual * 0.5f) * 2.0f;
+    quantized = predicted + static_cast<Int>(rounded);
+    *quantized_out = static_cast<int32_t>(quantized);
+  }
   // Update (prediction.h:121-141).
   const Int scaled = quantized * 8;
   *error_out = static_cast<int32_t>(prediction - scaled);
@@ -1139,6 +1157,7 @@ __device__ __forceinline__ void WeightedPredictorStep(Int w, Int n, Int nw, Int 
   }
 }
 
+template <bool kReplay>
 __global__ void __launch_bounds__(kDcThreads, 1)
 DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   extern __shared__ __align__(16) unsigned char dc_smem[];
@@ -1151,19 +1170,30 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
   const int y = idle ? kDcGroup : static_cast<int>(threadIdx.x) % kDcGroup;
   const int lag = c == 2 ? 1 : 0;
   for (int i = threadIdx.x; i < 64; i += blockDim.x) r.reciprocal[i] = (1u << 24) / (i + 1);
+  if (p.tokens != nullptr) {
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+      r.contexts[i] = static_cast<uint8_t>(DcContextOfIndex(i));
+  }
   if (threadIdx.x == 0) r.wide = 0;
-  const AqQuantizer q = *p.q;
-  const float inverse_step = q.inverse_dc_steps[c] * p.precision;
-  const float step_y = q.dc_steps[1] / p.precision;
-  int32_t* plane = p.quantized + c * p.pitch;
-  const float* source = p.dc + c * p.pitch;
+  const AqQuantizer q = kReplay ? AqQuantizer{} : *p.q;
+  const float inverse_step = kReplay ? 0.0f : q.inverse_dc_steps[c] * p.precision;
+  const float step_y = kReplay ? 0.0f : q.dc_steps[1] / p.precision;
+  int32_t* plane = kReplay ? nullptr : p.quantized + c * p.pitch;
+  // The samples: DC values to quantize, or quantized values to replay, read
+  // as raw 32-bit words.
+  const uint32_t* source = kReplay ? reinterpret_cast<const uint32_t*>(p.replay + c * p.pitch)
+                                   : reinterpret_cast<const uint32_t*>(p.dc + c * p.pitch);
+  uint2* tokens = p.tokens == nullptr
+                    ? nullptr
+                    : p.tokens + DcTokenOffset(blockIdx.x, blockIdx.y, p.width, p.height) +
+                        static_cast<size_t>(DcChannelRank(c)) * gw * gh;
   int32_t (*Q)[kDcGroup] = r.q[c];
   int32_t (*E)[kDcGroup] = r.e[c];
   __syncthreads();
-  // The DC sample of the next position is loaded one wave ahead, so its
+  // The sample of the next position is loaded one wave ahead, so its
   // global-memory latency overlaps this wave's work and barrier.
   const size_t row_index = static_cast<size_t>(gy0 + min(y, gh - 1)) * stride + gx0;
-  float pending = y < gh ? source[row_index] : 0.0f;  // idle threads have y >= gh
+  uint32_t pending = y < gh ? source[row_index] : 0u;  // idle threads have y >= gh
   // This row's previous quantized value and signed error (its west
   // neighbour), kept in registers.
   int32_t own_q = 0, own_e = 0;
@@ -1172,7 +1202,7 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
     const int x = t - lag - 2 * y;
     const int wide = r.wide;
     if (y < gh && x >= 0 && x < gw) {
-      const float dc_value = pending;
+      const uint32_t sample = pending;
       if (x + 1 < gw) pending = source[row_index + x + 1];
       const int s = x & 7, sw = (x - 1) & 7, sne = (x + 1 < gw ? x + 1 : x) & 7;
       const int snw = (x ? x - 1 : x) & 7;
@@ -1204,19 +1234,30 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
           errors[i] = north + northeast + northwest;
         }
       }
-      float value = dc_value;
-      if (c == 2) value = fmaf(-static_cast<float>(r.q[1][s][y]), step_y, value);
-      const float scaled_value = value * inverse_step;
-      int32_t quantized, error_value;
-      uint32_t sub[4];
-      if (!wide && fabsf(scaled_value) < kDcNarrowScaled) {
-        WeightedPredictorStep<int32_t, false>(w, n, nw, ne, nn, ew, en, enw, ene, errors,
-                                              r.reciprocal, scaled_value, &quantized,
-                                              &error_value, sub);
+      float scaled_value = 0.0f;
+      int32_t quantized = 0, error_value;
+      bool narrow;
+      if (kReplay) {
+        quantized = static_cast<int32_t>(sample);
+        narrow = quantized > -kDcNarrowQuantized && quantized < kDcNarrowQuantized;
       } else {
-        WeightedPredictorStep<int64_t, true>(w, n, nw, ne, nn, ew, en, enw, ene, errors,
-                                             r.reciprocal, scaled_value, &quantized,
-                                             &error_value, sub);
+        float value = __uint_as_float(sample);
+        if (c == 2) value = fmaf(-static_cast<float>(r.q[1][s][y]), step_y, value);
+        scaled_value = value * inverse_step;
+        narrow = fabsf(scaled_value) < kDcNarrowScaled;
+      }
+      uint32_t sub[4];
+      int64_t predicted;
+      if (!wide && narrow) {
+        WeightedPredictorStep<int32_t, false, kReplay>(w, n, nw, ne, nn, ew, en, enw, ene,
+                                                       errors, r.reciprocal, scaled_value,
+                                                       &quantized, &error_value, sub,
+                                                       &predicted);
+      } else {
+        WeightedPredictorStep<int64_t, true, kReplay>(w, n, nw, ne, nn, ew, en, enw, ene,
+                                                      errors, r.reciprocal, scaled_value,
+                                                      &quantized, &error_value, sub,
+                                                      &predicted);
       }
       // Later steps read this value: past the 32-bit bounds, every later
       // step of the CTA takes the 64-bit form.
@@ -1226,7 +1267,21 @@ DcQuantKernel(const __grid_constant__ DcQuantParams p) {
             static_cast<uint32_t>(2 * kDcNarrowError)) {
         r.wide = 1;
       }
-      plane[row_index + x] = quantized;
+      if (!kReplay) plane[row_index + x] = quantized;
+      if (tokens != nullptr) {
+        // The weighted predictor's context property: of ew, en, enw, ene the
+        // first with the largest magnitude (prediction.h:95-99); the token is
+        // the packed residual against the prediction (weighted_dc.cpp:67-80).
+        int64_t property = ew;
+        if (llabs(static_cast<int64_t>(en)) > llabs(property)) property = en;
+        if (llabs(static_cast<int64_t>(enw)) > llabs(property)) property = enw;
+        if (llabs(static_cast<int64_t>(ene)) > llabs(property)) property = ene;
+        const int64_t index = property < -512 ? 0 : property > 511 ? 1023 : 512 + property;
+        const int64_t residual = static_cast<int64_t>(quantized) - predicted;
+        if (residual < INT32_MIN || residual > INT32_MAX) RaiseError(p.error, kErrorRange);
+        tokens[y * gw + x] = make_uint2(r.contexts[index],
+                                        PackSigned(static_cast<int32_t>(residual)));
+      }
       Q[s][y] = quantized;
       E[s][y] = error_value;
       own_q = quantized;
@@ -1542,9 +1597,28 @@ int AqCoding(const int2* lists, const uint32_t* counts, size_t bx, size_t by, co
   return status;
 }
 
+namespace {
+
+template <bool kReplay>
+int LaunchDcQuant(const DcQuantParams& p, size_t bx, size_t by, cudaStream_t stream) {
+  const int smem = static_cast<int>(sizeof(DcRings));
+  int status = CheckCuda(cudaFuncSetAttribute(DcQuantKernel<kReplay>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                         "dc predictor attribute");
+  if (status != GJXL_B200_OK) return status;
+  dim3 grid(static_cast<unsigned>((bx + kDcGroup - 1) / kDcGroup),
+            static_cast<unsigned>((by + kDcGroup - 1) / kDcGroup), 2);
+  DcQuantKernel<kReplay><<<grid, kDcThreads, smem, stream>>>(p);
+  return CheckLaunch("dc predictor");
+}
+
+}  // namespace
+
 int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, int32_t* quantized,
-                 float* reconstructed, int extra_precision, cudaStream_t stream) {
+                 float* reconstructed, int extra_precision, uint2* tokens, uint32_t* error,
+                 cudaStream_t stream) {
   DcQuantParams p;
+  std::memset(&p, 0, sizeof(p));
   p.dc = dc;
   p.quantized = quantized;
   p.reconstructed = reconstructed;
@@ -1553,17 +1627,26 @@ int AqDcQuantize(const float* dc, size_t bx, size_t by, const AqQuantizer* q, in
   p.pitch = bx * by;
   p.q = q;
   p.precision = static_cast<float>(1u << extra_precision);
-  const int smem = static_cast<int>(sizeof(DcRings));
-  int status = CheckCuda(cudaFuncSetAttribute(DcQuantKernel,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                         "aq dc quantize attribute");
+  p.tokens = tokens;
+  p.error = error;
+  int status = LaunchDcQuant<false>(p, bx, by, stream);
   if (status != GJXL_B200_OK) return status;
-  dim3 grid(static_cast<unsigned>((bx + kDcGroup - 1) / kDcGroup),
-            static_cast<unsigned>((by + kDcGroup - 1) / kDcGroup), 2);
-  DcQuantKernel<<<grid, kDcThreads, smem, stream>>>(p);
   DcDequantKernel<<<Blocks(bx * by), kThreads, 0, stream>>>(
     quantized, reconstructed, static_cast<int>(bx * by), bx * by, q, p.precision);
   return CheckLaunch("aq dc quantize");
+}
+
+int DcWeightedTokens(const int32_t* quantized, size_t pitch, size_t bx, size_t by, uint2* tokens,
+                     uint32_t* error, cudaStream_t stream) {
+  DcQuantParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.width = static_cast<int>(bx);
+  p.height = static_cast<int>(by);
+  p.pitch = pitch;
+  p.replay = quantized;
+  p.tokens = tokens;
+  p.error = error;
+  return LaunchDcQuant<true>(p, bx, by, stream);
 }
 
 int AqInverseSigma(const uint8_t* cells, size_t bx, size_t by, const int32_t* raw,

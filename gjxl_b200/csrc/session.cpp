@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "aq.h"
+#include "dc_tokens.cuh"
 #include "host_util.h"
 
 namespace gjxl_b200 {
@@ -100,7 +101,6 @@ struct Session {
   float* strategy_mask = nullptr;
   float* pixel_mask = nullptr;
   float* iq_scratch = nullptr;
-  void* cfl_scratch = nullptr;  // initial CfL (a, b) pairs, 64 KB per 64x64 tile
   int8_t* y_to_x = nullptr;
   int8_t* y_to_b = nullptr;
   float* costs = nullptr;
@@ -123,6 +123,18 @@ struct Session {
   int32_t* qac = nullptr;      // quantized AC, footprint layout
   float* dc = nullptr;         // extracted DC (3 x blocks)
   int32_t* qdc = nullptr;
+  // DC-group token streams (tokenize != 0).
+  uint2* dc_tokens = nullptr;
+  uint2* meta_tokens = nullptr;
+  uint32_t* dc_group_info = nullptr;
+  uint32_t* dc_histogram = nullptr;
+  void* dc_token_scratch = nullptr;
+  size_t dc_groups = 0, meta_capacity = 0;
+  uint32_t* host_dc_tokens = nullptr;
+  uint32_t* host_meta_tokens = nullptr;
+  uint32_t* host_dc_group_info = nullptr;
+  uint32_t* host_dc_histogram = nullptr;
+  size_t host_meta_count = 0;
   float* dc_rec = nullptr;
   float* dc_smooth = nullptr;
   float* inverse_sigma = nullptr;
@@ -202,6 +214,7 @@ struct Session {
     if (butteraugli) ButteraugliDestroy(butteraugli);
     if (tokens) gjxl_b200_ac_tokens_destroy(tokens);
     if (host_tok_values) cudaFreeHost(host_tok_values);
+    if (host_dc_tokens) cudaFreeHost(host_dc_tokens);
     if (events_created) {
       for (auto& e : events) cudaEventDestroy(e);
     }
@@ -232,7 +245,6 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->strategy_mask), blocks * sizeof(float)},
     {reinterpret_cast<void**>(&s->pixel_mask), plane * sizeof(float)},
     {reinterpret_cast<void**>(&s->iq_scratch), InitialQuantScratchFloats(s->pw, s->ph) * 4},
-    {&s->cfl_scratch, InitialCflScratchBytes(s->pw, s->ph)},
     {reinterpret_cast<void**>(&s->y_to_x), tiles},
     {reinterpret_cast<void**>(&s->y_to_b), tiles},
     {reinterpret_cast<void**>(&s->costs), AcStrategyCostFloats(s->bx, s->by) * sizeof(float)},
@@ -275,6 +287,13 @@ int Allocate(Session* s) {
     {reinterpret_cast<void**>(&s->histogram), (s->token_capacity ? 4 * 495 * 128 : 0) * 4},
     {reinterpret_cast<void**>(&s->scans), 13 * 3 * 1024 * sizeof(uint32_t)},
     {reinterpret_cast<void**>(&s->order_masks), 4 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->dc_tokens), s->options.tokenize ? 3 * blocks * 8 : 0},
+    {reinterpret_cast<void**>(&s->meta_tokens), s->meta_capacity * 8},
+    {reinterpret_cast<void**>(&s->dc_group_info), s->dc_groups * 5 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->dc_histogram),
+     s->options.tokenize ? kDcContextCount * kHybridSymbols * sizeof(uint32_t) : 0},
+    {reinterpret_cast<void**>(&s->dc_token_scratch),
+     s->options.tokenize ? DcTokenScratchBytes(s->bx, s->by) : 0},
   };
   size_t total = 0;
   for (const Item& item : items) total = Align(total, 256) + item.bytes;
@@ -327,6 +346,15 @@ int Allocate(Session* s) {
     s->host_tok_contexts = reinterpret_cast<uint16_t*>(s->host_tok_values + s->token_capacity);
     s->host_group_offsets = reinterpret_cast<uint32_t*>(
       reinterpret_cast<unsigned char*>(mirror) + Align(s->token_capacity * 6, 16));
+    const size_t dc_bytes = 3 * blocks * 8 + s->meta_capacity * 8 + s->dc_groups * 5 * 4 +
+                            kDcContextCount * kHybridSymbols * 4 + 64;
+    void* dc_mirror = nullptr;
+    status = CheckCuda(HostMalloc(&dc_mirror, dc_bytes), "session: DC token mirrors");
+    if (status != GJXL_B200_OK) return status;
+    s->host_dc_tokens = static_cast<uint32_t*>(dc_mirror);
+    s->host_meta_tokens = s->host_dc_tokens + 6 * blocks;
+    s->host_dc_group_info = s->host_meta_tokens + 2 * s->meta_capacity;
+    s->host_dc_histogram = s->host_dc_group_info + 5 * s->dc_groups;
   }
   for (auto& side : s->fan_side) {
     status = CheckCuda(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking),
@@ -395,7 +423,9 @@ int RunAq(Session* s, cudaStream_t stream) {
     GJXL_TRY(AqCoding(s->anchors, s->anchor_counts, s->bx, s->by, s->coef, s->pw, s->pitch,
                       s->qac, s->dc, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
                       s->matrix_multipliers, s->error, stream, &fan));
-    GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, 1, stream));
+    GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, 1,
+                          iteration == s->iterations ? s->dc_tokens : nullptr, s->error + 2,
+                          stream));
     GJXL_TRY(AqInverseSigma(s->cells, s->bx, s->by, s->raw, s->quantizer, s->inverse_sigma,
                             stream));
     GJXL_TRY(AqSmoothDc(s->dc_rec, s->bx, s->by, s->quantizer, s->dc_smooth, stream));
@@ -462,7 +492,7 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
                                  s->ph, multipliers, s->error, stream));
   Mark(s, kStageInitialCfl, stream);
   GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b,
-                            s->cfl_scratch, s->error, stream));
+                            stream));
   Mark(s, kStageAcCosts, stream);
   const StreamFan fan = MakeFan(s, stream);
   const bool dense = s->options.effort >= 10;
@@ -490,6 +520,13 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
     outs.device_error = s->error + 2;
     GJXL_TRY(gjxl_b200_ac_tokenize(s->tokens, s->cells, s->raw, s->qac, s->pw, s->pitch, &map,
                                    OrderMode(s->options), &outs, stream));
+  }
+  if (s->dc_tokens != nullptr) {
+    // The DC tokens came with the last DC quantization; the AC metadata of
+    // the final strategy, quant field and CfL maps (default EPF sharpness 4).
+    GJXL_TRY(LaunchMetaTokens(s->cells, s->raw, nullptr, s->final_y_to_x, s->final_y_to_b, s->bx,
+                              s->by, s->dc_tokens, s->meta_tokens, s->dc_group_info,
+                              s->dc_histogram, s->dc_token_scratch, s->error + 2, stream));
   }
   Mark(s, kStageCount, stream);
   // Merge the Butteraugli error word into the session error word.
@@ -660,6 +697,10 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
   s->iterations = AqIterations(o.effort);
   s->groups = ((s->bx + 31) / 32) * ((s->by + 31) / 32);
   s->token_capacity = o.tokenize ? gjxl_b200_ac_token_capacity(s->bx, s->by) : 0;
+  if (o.tokenize) {
+    s->dc_groups = ((s->bx + 255) / 256) * ((s->by + 255) / 256);
+    s->meta_capacity = MetaTokenCapacity(s->bx, s->by);
+  }
   status = Allocate(s);
   if (status != GJXL_B200_OK) {
     delete s;
@@ -728,6 +769,17 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
                                        (s->groups + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                        st),
                        "session: group offsets"));
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_dc_group_info, s->dc_group_info,
+                                       s->dc_groups * 5 * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: DC group table"));
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_dc_tokens, s->dc_tokens, 3 * s->bx * s->by * 8,
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: DC tokens"));
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_dc_histogram, s->dc_histogram,
+                                       kDcContextCount * kHybridSymbols * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: DC histogram"));
     GJXL_TRY(CheckCuda(cudaStreamSynchronize(st), "session: analysis"));
     const size_t total = s->host_group_offsets[s->groups];
     if (total > s->token_capacity) {
@@ -740,6 +792,17 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
                                        cudaMemcpyDeviceToHost, st),
                        "session: token contexts"));
     s->host_token_count = total;
+    // DC-group streams: every DC token, the metadata tokens the group table
+    // counts, and the histogram.
+    const size_t meta = s->host_dc_group_info[5 * (s->dc_groups - 1) + 2] +
+                        s->host_dc_group_info[5 * (s->dc_groups - 1) + 3];
+    if (meta > s->meta_capacity) {
+      return SetError(GJXL_B200_INTERNAL, "session_analyze_host: metadata token overflow");
+    }
+    GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->host_meta_tokens, s->meta_tokens, meta * 8,
+                                       cudaMemcpyDeviceToHost, st),
+                       "session: metadata tokens"));
+    s->host_meta_count = meta;
   }
   GJXL_TRY(CheckCuda(cudaStreamSynchronize(st), "session: analysis"));
   // A nonzero device error word fails the call, as the reference's
@@ -821,6 +884,18 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
     out->host_group_offsets = s->host_group_offsets;
   }
   out->host_token_count = s->host_token_count;
+  out->dc_groups = s->dc_groups;
+  if (s->dc_tokens != nullptr) {
+    out->dc_tokens = reinterpret_cast<const uint32_t*>(s->dc_tokens);
+    out->meta_tokens = reinterpret_cast<const uint32_t*>(s->meta_tokens);
+    out->dc_group_info = s->dc_group_info;
+    out->dc_histogram = s->dc_histogram;
+    out->host_dc_tokens = s->host_dc_tokens;
+    out->host_meta_tokens = s->host_meta_tokens;
+    out->host_dc_group_info = s->host_dc_group_info;
+    out->host_dc_histogram = s->host_dc_histogram;
+  }
+  out->host_meta_token_count = s->host_meta_count;
   out->device_bytes = s->arena_bytes;
   out->pnorm_history = s->pnorms;
   out->host_pnorm_history = s->host_pnorms;

@@ -24,6 +24,13 @@ size_t InitialQuantScratchFloats(size_t padded_width, size_t padded_height);
 int LaunchGaborishInverse(const float* input, size_t in_stride, size_t in_pitch, float* output,
                           size_t out_stride, size_t out_pitch, size_t width, size_t height,
                           const float multipliers[3], uint32_t* error, cudaStream_t stream);
+// DC-group token streams (dc_tokens.cu).
+size_t DcTokenScratchBytes(size_t blocks_x, size_t blocks_y);
+size_t MetaTokenCapacity(size_t blocks_x, size_t blocks_y);
+int LaunchMetaTokens(const uint8_t* cells, const int32_t* raw_quant, const uint8_t* sharpness,
+                     const int8_t* y_to_x, const int8_t* y_to_b, size_t blocks_x, size_t blocks_y,
+                     const uint2* dc_tokens, uint2* meta_tokens, uint32_t* info,
+                     uint32_t* histogram, void* scratch, uint32_t* error, cudaStream_t stream);
 int LaunchInitialCfl(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
                      int8_t* y_to_x, int8_t* y_to_b, cudaStream_t stream);
 size_t AcStrategyCostFloats(size_t blocks_x, size_t blocks_y);

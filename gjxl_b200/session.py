@@ -39,7 +39,11 @@ class Outputs(Structure):
             "order_masks", "host_token_values", "host_token_contexts", "host_group_offsets")] + [
         ("host_token_count", c_size_t), ("device_bytes", c_size_t),
         ("input_pixels", c_void_p), ("input_capacity", c_size_t), ("graph_replay", c_int),
-        ("pnorm_history", c_void_p), ("host_pnorm_history", c_void_p)]
+        ("pnorm_history", c_void_p), ("host_pnorm_history", c_void_p),
+        ("dc_groups", c_size_t), ("dc_tokens", c_void_p), ("meta_tokens", c_void_p),
+        ("dc_group_info", c_void_p), ("dc_histogram", c_void_p), ("host_dc_tokens", c_void_p),
+        ("host_meta_tokens", c_void_p), ("host_dc_group_info", c_void_p),
+        ("host_dc_histogram", c_void_p), ("host_meta_token_count", c_size_t)]
 
 
 _BOUND = False
@@ -204,8 +208,15 @@ class AnalysisSession:
         if not o.host_token_values:
             return {}
         n = o.host_token_count
+        blocks = o.blocks_x * o.blocks_y
         return {
             "token_values": self._host("host_token_values", ctypes.c_uint32, (n,)),
             "token_contexts": self._host("host_token_contexts", ctypes.c_uint16, (n,)),
             "group_offsets": self._host("host_group_offsets", ctypes.c_uint32, (o.groups + 1,)),
+            # DC-group streams: (context, value) pairs and the group table.
+            "dc_tokens": self._host("host_dc_tokens", ctypes.c_uint32, (3 * blocks, 2)),
+            "meta_tokens": self._host("host_meta_tokens", ctypes.c_uint32,
+                                      (o.host_meta_token_count, 2)),
+            "dc_group_info": self._host("host_dc_group_info", ctypes.c_uint32, (o.dc_groups, 5)),
+            "dc_histogram": self._host("host_dc_histogram", ctypes.c_uint32, (45, 128)),
         }

@@ -105,9 +105,36 @@ def ac_strategy_search(opsin, quant_field, pixel_mask, y_to_x, y_to_b, costs, ce
 
 def initial_cfl(opsin: torch.Tensor, y_to_x: torch.Tensor, y_to_b: torch.Tensor):
     """opsin: (3, PH, PW) Gaborish-inverted XYB; outputs int8 per 64x64 tile."""
-    _lib.call("gjxl_b200_initial_cfl", opsin.data_ptr(), opsin.shape[2],
-              opsin.shape[1] * opsin.shape[2], opsin.shape[2], opsin.shape[1],
+    pw, ph = opsin.shape[2], opsin.shape[1]
+    _lib.call("gjxl_b200_initial_cfl", opsin.data_ptr(), pw, ph * pw, pw, ph,
               y_to_x.data_ptr(), y_to_b.data_ptr(), _stream())
+
+
+def dc_tokenize(quantized_dc: torch.Tensor, cells: torch.Tensor, raw_quant: torch.Tensor,
+                y_to_x: torch.Tensor, y_to_b: torch.Tensor, prediction: int = 1,
+                sharpness: torch.Tensor | None = None, histogram: bool = True) -> dict:
+    """DC-group token streams of a frame (gjxl_b200_dc_tokenize): quantized DC
+    (3, by, bx) int32, cells (by, bx) uint8, raw quant (by, bx) int32, CfL maps
+    per tile. Returns device tensors: dc (N, 2) and meta (M, 2) (context,
+    value) uint32 pairs, info (groups, 5), histogram (45, 128), and the
+    device error word."""
+    _, by, bx = quantized_dc.shape
+    sizes = [ctypes.c_size_t(0) for _ in range(4)]
+    _lib.call("gjxl_b200_dc_token_sizes", bx, by, *[ctypes.addressof(v) for v in sizes])
+    n_dc, n_meta, groups, scratch_bytes = (v.value for v in sizes)
+    dev = quantized_dc.device
+    dc = torch.zeros((n_dc, 2), dtype=torch.int32, device=dev)
+    meta = torch.zeros((n_meta, 2), dtype=torch.int32, device=dev)
+    info = torch.zeros((groups, 5), dtype=torch.int32, device=dev)
+    hist = torch.zeros((45, 128), dtype=torch.int32, device=dev)
+    scratch = torch.empty(scratch_bytes // 4, dtype=torch.int32, device=dev)
+    error = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call("gjxl_b200_dc_tokenize", quantized_dc.data_ptr(), bx * by, cells.data_ptr(),
+              raw_quant.data_ptr(), 0 if sharpness is None else sharpness.data_ptr(),
+              y_to_x.data_ptr(), y_to_b.data_ptr(), bx, by, prediction, dc.data_ptr(),
+              meta.data_ptr(), info.data_ptr(), hist.data_ptr() if histogram else 0,
+              scratch.data_ptr(), scratch_bytes, error.data_ptr(), _stream())
+    return {"dc": dc, "meta": meta, "info": info, "histogram": hist, "error": error}
 
 
 class Butteraugli:

@@ -155,18 +155,47 @@ GJXL_B200_API int gjxl_b200_gaborish_inverse(
  * PreparedQuantizationPipeline preprocessing
  * (src/codec/quantization_pipeline.cpp:155-213). Input: the Gaborish-inverted
  * padded XYB image. Outputs: int8 y_to_x and y_to_b per 64x64 tile (dense,
- * ceil(padded_width/64) x ceil(padded_height/64)). `scratch`: 16-byte aligned
- * device memory of gjxl_b200_initial_cfl_scratch_bytes() bytes (64 KB per
- * tile: the coefficient pairs of the Newton solve).
+ * ceil(padded_width/64) x ceil(padded_height/64)). `opsin` 8-byte aligned,
+ * stride and plane pitch even (floats).
  */
-GJXL_B200_API size_t gjxl_b200_initial_cfl_scratch_bytes(size_t padded_width,
-                                                         size_t padded_height);
 GJXL_B200_API int gjxl_b200_initial_cfl(const float* opsin, size_t opsin_stride,
                                         size_t opsin_plane_pitch,
                                         size_t padded_width,
                                         size_t padded_height, int8_t* y_to_x,
-                                        int8_t* y_to_b, void* scratch,
-                                        size_t scratch_bytes, void* stream);
+                                        int8_t* y_to_b, void* stream);
+
+/*
+ * DC-group token streams (row f1): the DC residual and AC-metadata tokens of
+ * every 256x256-block DC group, and their entropy-model histogram.
+ * Replaces the CPU path's TokenizeSimpleDcGroupsForEncoder
+ * (src/codestream/vardct/dc_group.cpp:469-546) with TokenizeWeightedDcGroup
+ * (prediction 1, weighted_dc.cpp:47) or TokenizeSimpleDcGroup (prediction
+ * 0, dc_group.cpp:291), and TokenizeSimpleAcMetadata (dc_group.cpp:349), as
+ * called by the encoder at src/codestream/vardct/encoder.cpp:1930.
+ * Inputs (device): quantized DC, 3 planes (X, Y, B) of blocks_x x blocks_y
+ * int32 dc_plane_pitch elements apart; strategy cells ((strategy << 1) |
+ * anchor); raw quant field; EPF sharpness (NULL: the default 4 everywhere);
+ * y_to_x / y_to_b per 64x64 tile (ceil(blocks/8) per side).
+ * Outputs (device): tokens as (context, value) uint32 pairs, EntropyToken's
+ * layout, in the encoder's legacy context numbering (before the DC tree
+ * layout's context map): dc_tokens (3 * blocks pairs; groups in row-major
+ * order, channels Y, X, B, raster order), meta_tokens (per group: y_to_x
+ * map, y_to_b map, anchor strategies, anchor quant fields, sharpness),
+ * group_info (per group {dc_offset, dc_count, meta_offset, meta_count,
+ * anchor_count}, in pairs), and optionally histogram: [45][128] uint32
+ * counts of (context, hybrid-uint {4,2,0} symbol) over both streams.
+ * Sizes from gjxl_b200_dc_token_sizes. A residual outside int32 or a quant /
+ * sharpness / strategy the reference rejects sets device_error bit 2.
+ */
+GJXL_B200_API int gjxl_b200_dc_token_sizes(size_t blocks_x, size_t blocks_y,
+                                           size_t* dc_tokens, size_t* meta_tokens,
+                                           size_t* groups, size_t* scratch_bytes);
+GJXL_B200_API int gjxl_b200_dc_tokenize(
+    const int32_t* quantized_dc, size_t dc_plane_pitch, const uint8_t* cells,
+    const int32_t* raw_quant, const uint8_t* epf_sharpness, const int8_t* y_to_x,
+    const int8_t* y_to_b, size_t blocks_x, size_t blocks_y, int prediction,
+    uint32_t* dc_tokens, uint32_t* meta_tokens, uint32_t* group_info, uint32_t* histogram,
+    void* scratch, size_t scratch_bytes, uint32_t* device_error, void* stream);
 
 /*
  * Default AC quantization matrix of one searched strategy and channel, in the
@@ -446,6 +475,22 @@ typedef struct gjxl_b200_outputs {
    * host mirror filled by gjxl_b200_session_analyze_host. */
   const double* pnorm_history;
   const double* host_pnorm_history;
+  /* DC-group token streams (tokenize != 0), gjxl_b200_dc_tokenize's layout
+   * with the weighted DC predictor and default EPF sharpness: DC residual
+   * tokens (3 * blocks pairs, written by the last DC quantization),
+   * AC-metadata tokens, the per-group table (5 words per group) and the
+   * [45][128] histogram. Device views, then host mirrors filled by
+   * gjxl_b200_session_analyze_host (host_meta_token_count pairs). */
+  size_t dc_groups;
+  const uint32_t* dc_tokens;
+  const uint32_t* meta_tokens;
+  const uint32_t* dc_group_info;
+  const uint32_t* dc_histogram;
+  const uint32_t* host_dc_tokens;
+  const uint32_t* host_meta_tokens;
+  const uint32_t* host_dc_group_info;
+  const uint32_t* host_dc_histogram;
+  size_t host_meta_token_count;
 } gjxl_b200_outputs;
 
 typedef struct gjxl_b200_session gjxl_b200_session;

@@ -33,6 +33,8 @@ _SIGNATURES = {
     "gjxl_ref_encode_cpu": [_P, _Z, _Z, _F, _I, _P, _Z, _P, _P],
     "gjxl_ref_encode_cpu_target_size": [_P, _Z, _Z, _Z, c_double, _Z, _I, _P, _Z, _P, _P,
                                         _P, _P],
+    "gjxl_ref_dc_group_tokens": [_P, _P, _P, _P, _P, _P, _Z, _Z, _I, _P, _Z, _P, _Z, _P],
+    "gjxl_ref_hybrid_uint": [_P, _Z, _I, _I, _I, _P],
 }
 
 _lib = None
@@ -412,6 +414,42 @@ def pipeline_tokens(linear: np.ndarray, opsin: np.ndarray, target: float = 1.0, 
 
 CUDA_LIBRARY_PATH = Path(__file__).resolve().parent / "_ref" / "libgjxl_ref_cuda.so"
 _cuda_lib = None
+
+
+def dc_group_tokens(quantized_dc: np.ndarray, cells: np.ndarray, raw_quant: np.ndarray,
+                    sharpness: np.ndarray, ytox: np.ndarray, ytob: np.ndarray,
+                    prediction: int = 1) -> dict:
+    """The encoder's DC-group token streams (dc_group.cpp:469-546): quantized
+    DC (3, by, bx) int32 in X, Y, B planes, cells (by, bx) uint8, raw quant
+    (by, bx) int32, EPF sharpness (by, bx) uint8, CfL maps per 64x64 tile.
+    Returns {"dc": (N, 2), "meta": (M, 2)} (context, value) uint32 pairs in
+    group order, and "info": per group (dc_offset, dc_count, meta_offset,
+    meta_count, anchors)."""
+    _, by, bx = quantized_dc.shape
+    groups = ((bx + 255) // 256) * ((by + 255) // 256)
+    tiles = ((bx + 7) // 8) * ((by + 7) // 8)
+    dc = np.zeros((3 * bx * by, 2), np.uint32)
+    meta = np.zeros((2 * tiles + 3 * bx * by, 2), np.uint32)
+    info = np.zeros((groups, 5), np.uint32)
+    args = [np.ascontiguousarray(quantized_dc, np.int32), np.ascontiguousarray(cells, np.uint8),
+            np.ascontiguousarray(raw_quant, np.int32), np.ascontiguousarray(sharpness, np.uint8),
+            np.ascontiguousarray(ytox, np.int8), np.ascontiguousarray(ytob, np.int8)]
+    _check(lib().gjxl_ref_dc_group_tokens(*[_ptr(a) for a in args], bx, by, int(prediction),
+                                          _ptr(dc), dc.shape[0], _ptr(meta), meta.shape[0],
+                                          _ptr(info)), "dc_group_tokens")
+    meta_used = int(info[-1, 2] + info[-1, 3])
+    return {"dc": dc, "meta": meta[:meta_used], "info": info}
+
+
+def hybrid_uint(values: np.ndarray, split_exponent: int = 4, msb_in_token: int = 2,
+                lsb_in_token: int = 0) -> np.ndarray:
+    """EncodeHybridUint of each value: (N, 3) uint32 (symbol, extra bit count,
+    extra bits)."""
+    values = np.ascontiguousarray(values, np.uint32)
+    out = np.zeros((values.size, 3), np.uint32)
+    _check(lib().gjxl_ref_hybrid_uint(_ptr(values), values.size, split_exponent, msb_in_token,
+                                      lsb_in_token, _ptr(out)), "hybrid_uint")
+    return out
 
 
 def cuda_available() -> bool:

@@ -36,6 +36,9 @@
 #include "codestream/ac_group.h"
 #include "codestream/block_context_map.h"
 #include "codestream/coefficient_order.h"
+#include "codestream/dc_group.h"
+#include "codestream/entropy.h"
+#include "codestream/weighted_dc.h"
 #include "codestream/encoder.h"
 #include "codestream/workflow.h"
 #include "codestream/workflow_internal.h"
@@ -704,5 +707,103 @@ GJXL_REF_API int gjxl_ref_encode_cpu_target_size(const float* linear, size_t wid
     return -2;
   }
   std::memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}
+
+// DC-group token streams of a frame (codestream/vardct/dc_group.cpp:469-546,
+// TokenizeSimpleDcGroupsForEncoder): every 256x256-block group in row-major
+// order, its DC residual tokens (TokenizeWeightedDcGroup for prediction 1,
+// TokenizeSimpleDcGroup for 0) and its AC-metadata tokens
+// (TokenizeSimpleAcMetadata) over the same slices the encoder takes.
+// Inputs: quantized DC as 3 planes of blocks_x x blocks_y (X, Y, B), the
+// encoded strategy cells ((strategy << 1) | anchor), raw quant field, EPF
+// sharpness, and the y_to_x / y_to_b maps (ceil(blocks/8) per side).
+// Outputs, tokens as (context, value) pairs: all groups' DC tokens in group
+// order into dc_out, all metadata tokens into meta_out, and per group
+// {dc_offset, dc_count, meta_offset, meta_count, anchor_count}.
+GJXL_REF_API int gjxl_ref_dc_group_tokens(const int32_t* quantized_dc, const uint8_t* cells,
+                                          const int32_t* raw_quant, const uint8_t* sharpness,
+                                          const int8_t* y_to_x, const int8_t* y_to_b,
+                                          size_t blocks_x, size_t blocks_y, int prediction,
+                                          uint32_t* dc_out, size_t dc_capacity,
+                                          uint32_t* meta_out, size_t meta_capacity,
+                                          uint32_t* group_info) {
+  const Extent2D blocks{blocks_x, blocks_y};
+  AcStrategyGrid grid;
+  Status status = AcStrategyGrid::CreateFromEncodedCells(
+    blocks, std::span<const uint8_t>(cells, blocks_x * blocks_y), &grid);
+  if (!status.ok()) return Fail(status);
+  const size_t tiles_x = (blocks_x + 7) / 8, tiles_y = (blocks_y + 7) / 8;
+  const size_t pitch = blocks_x * blocks_y;
+  const size_t groups_x = (blocks_x + 255) / 256, groups_y = (blocks_y + 255) / 256;
+  size_t dc_used = 0, meta_used = 0;
+  for (size_t gy = 0; gy < groups_y; ++gy) {
+    for (size_t gx = 0; gx < groups_x; ++gx) {
+      const size_t bx = gx * 256, by = gy * 256;
+      const Extent2D extent{std::min<size_t>(256, blocks_x - bx),
+                            std::min<size_t>(256, blocks_y - by)};
+      ConstImage3I32View dc;
+      for (size_t c = 0; c < 3; ++c)
+        dc.plane[c] = {quantized_dc + c * pitch + by * blocks_x + bx, extent, blocks_x};
+      codestream_internal::Storage<EntropyToken> dc_tokens, meta_tokens;
+      status = prediction == 1 ? codestream_internal::TokenizeWeightedDcGroup(dc, &dc_tokens)
+                               : TokenizeSimpleDcGroup(dc, &dc_tokens);
+      if (!status.ok()) return Fail(status);
+      const Extent2D tile_extent{(extent.width + 7) / 8, (extent.height + 7) / 8};
+      const size_t tx = bx / 8, ty = by / 8;
+      const SimpleAcMetadataInput metadata{
+        .y_to_x_map = {y_to_x + ty * tiles_x + tx, tile_extent, tiles_x},
+        .y_to_b_map = {y_to_b + ty * tiles_x + tx, tile_extent, tiles_x},
+        .strategies = &grid,
+        .block_x = bx,
+        .block_y = by,
+        .raw_quant_field = {raw_quant + by * blocks_x + bx, extent, blocks_x},
+        .epf_sharpness = {sharpness + by * blocks_x + bx, extent, blocks_x},
+      };
+      size_t anchors = 0;
+      status = TokenizeSimpleAcMetadata(metadata, &meta_tokens, &anchors);
+      if (!status.ok()) return Fail(status);
+      if (dc_used + dc_tokens.size() > dc_capacity ||
+          meta_used + meta_tokens.size() > meta_capacity) {
+        g_last_error = "token capacity exceeded";
+        return -2;
+      }
+      uint32_t* info = group_info + 5 * (gy * groups_x + gx);
+      info[0] = static_cast<uint32_t>(dc_used);
+      info[1] = static_cast<uint32_t>(dc_tokens.size());
+      info[2] = static_cast<uint32_t>(meta_used);
+      info[3] = static_cast<uint32_t>(meta_tokens.size());
+      info[4] = static_cast<uint32_t>(anchors);
+      for (const EntropyToken& t : dc_tokens) {
+        dc_out[2 * dc_used] = t.context;
+        dc_out[2 * dc_used + 1] = t.value;
+        ++dc_used;
+      }
+      for (const EntropyToken& t : meta_tokens) {
+        meta_out[2 * meta_used] = t.context;
+        meta_out[2 * meta_used + 1] = t.value;
+        ++meta_used;
+      }
+    }
+  }
+  (void)tiles_y;
+  return 0;
+}
+
+// EncodeHybridUint (codestream/entropy.cpp) with the given configuration:
+// writes {symbol, extra_bit_count, extra_bits} per value.
+GJXL_REF_API int gjxl_ref_hybrid_uint(const uint32_t* values, size_t count, int split_exponent,
+                                      int msb_in_token, int lsb_in_token, uint32_t* out) {
+  const HybridUintConfig config{static_cast<uint8_t>(split_exponent),
+                                static_cast<uint8_t>(msb_in_token),
+                                static_cast<uint8_t>(lsb_in_token)};
+  for (size_t i = 0; i < count; ++i) {
+    HybridUintToken token;
+    Status status = EncodeHybridUint(values[i], config, &token);
+    if (!status.ok()) return Fail(status);
+    out[3 * i] = token.symbol;
+    out[3 * i + 1] = token.extra_bit_count;
+    out[3 * i + 2] = token.extra_bits;
+  }
   return 0;
 }
