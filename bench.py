@@ -91,6 +91,16 @@ class ClockSampler:
         except (FileNotFoundError, OSError):
             self.proc = None
 
+    def wait_ready(self, timeout_s: float = 5.0) -> None:
+        """Blocks until nvidia-smi has written its first sample, so that the
+        timed region that follows is sampled from its start."""
+        deadline = time.monotonic() + timeout_s
+        while self.proc is not None and time.monotonic() < deadline:
+            self.file.flush()
+            if Path(self.file.name).stat().st_size > 0:
+                return
+            time.sleep(0.02)
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -261,6 +271,8 @@ def run_gpu(args) -> dict:
     # Device-resident throughput: step i on session i mod S.
     barrier(world)
     sampler = ClockSampler(local) if rank == 0 else None
+    if sampler is not None:
+        sampler.wait_ready()
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(main_stream)
@@ -269,7 +281,6 @@ def run_gpu(args) -> dict:
         sessions[i % count].analyze(resident[i % count], row, 3, side[i % count].cuda_stream)
     join(stop)
     torch.cuda.synchronize()
-    clocks = sampler.stop() if sampler else None
     ms = max_over_ranks(start.elapsed_time(stop), world) / args.steps
     mp = WIDTH * HEIGHT / 1e6
     value = world * mp / (ms / 1e3)
@@ -303,6 +314,9 @@ def run_gpu(args) -> dict:
         raise failures[0]
     join(stop)
     torch.cuda.synchronize()
+    # The clock samples span both timed regions (device-resident and end to
+    # end) and the untimed host-input warm-up between them.
+    clocks = sampler.stop() if sampler else None
     e2e_ms = max_over_ranks(start.elapsed_time(stop), world) / args.steps
     for sess in sessions:
         assert sess.host_error() == 0, "device error word set"
@@ -485,6 +499,94 @@ def cpu_baseline_leg(pool: "ReferencePool") -> dict:
             "sample": f"{pool.workers} parallel 512x512 crops of the workload image, one step"}
 
 
+# Batched form: 64 images of the seeded generator, width and height
+# log-uniform in [256, 4096] with aspect ratio in [0.5, 2], distance uniform in
+# [0.5, 3.0], effort 7 (the batched configuration, seeds workload_seed(4, i)).
+BATCH_IMAGES = 64
+
+
+def batch_specs(count: int = BATCH_IMAGES) -> list[tuple[int, int, float, int]]:
+    """(width, height, distance, seed) of each image of the batch."""
+    from gjxl_b200.synthetic import workload_seed
+    rng = np.random.default_rng(workload_seed(4, 999_999))
+    specs = []
+    for i in range(count):
+        w = int(round(np.exp(rng.uniform(np.log(256), np.log(4096)))))
+        lo, hi = max(256, w / 2), min(4096, 2 * w)
+        h = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        specs.append((w, h, float(rng.uniform(0.5, 3.0)), workload_seed(4, i)))
+    return specs
+
+
+def _batch_image(spec) -> np.ndarray:
+    from gjxl_b200.synthetic import generate_srgb8
+    w, h, _, seed = spec
+    return generate_srgb8(w, h, seed)
+
+
+class BatchImages:
+    """Generates the batch's images in host processes (spawned before any GPU
+    work) while the GPU legs run."""
+
+    def __init__(self):
+        import multiprocessing as mp
+        self.specs = batch_specs()
+        self.pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
+        self.result = self.pool.map_async(_batch_image, self.specs, chunksize=1)
+
+    def get(self) -> list[np.ndarray]:
+        images = self.result.get()
+        self.pool.close()
+        self.pool.join()
+        return images
+
+
+def batched_leg(images: "BatchImages", precision: int) -> dict:
+    """Aggregate MP/s of the whole batch through gjxl_b200_batch_analyze
+    (device-resident inputs, autotuned lanes and order), and per-image
+    latency percentiles, against the same images one after another on one
+    lane (the plain form's sequential analyses)."""
+    import torch
+    from gjxl_b200.batch import BatchAnalyzer
+    imgs = images.get()
+    specs = images.specs
+    dev = [torch.from_numpy(img.reshape(img.shape[0], -1)).cuda() for img in imgs]
+    mp = sum(w * h for w, h, _, _ in specs) / 1e6
+    b = BatchAnalyzer(precision=precision)
+    reqs = b.requests([(d.data_ptr(), w, h, t) for d, (w, h, t, _) in zip(dev, specs)])
+
+    def timed(reps: int = 3):
+        runs = [b.analyze(reqs) for _ in range(reps)]
+        results, ms = min(runs, key=lambda r: r[1])
+        assert all(r["status"] == 0 for r in results), "batch image failed"
+        service = [r["service_ms"] for r in results]
+        ready = [r["ready_ms"] for r in results]
+        return {"value": round(mp / (ms / 1e3), 3), "unit": "MP/s", "batch_ms": round(ms, 3),
+                "service_ms_p50": round(float(np.percentile(service, 50)), 3),
+                "service_ms_p99": round(float(np.percentile(service, 99)), 3),
+                "ready_ms_p50": round(float(np.percentile(ready, 50)), 3),
+                "ready_ms_p99": round(float(np.percentile(ready, 99)), 3)}
+
+    b.set_schedule(1, False)
+    b.analyze(reqs)  # plans the sequential lane (sessions, graphs)
+    sequential = timed()
+    lanes, largest_first = b.autotune(reqs, lane_counts=(2, 4, 8))
+    batched = timed()
+    device_gb = b.device_bytes() / 1e9
+    b.close()
+    del dev
+    torch.cuda.empty_cache()
+    return {"images": len(specs), "megapixels": round(mp, 3),
+            "sizes": "width, height log-uniform in [256, 4096], aspect 0.5-2, "
+                     "distance uniform in [0.5, 3.0], effort 7, seeds 4000000 + i",
+            "batched": batched | {"lanes": lanes, "largest_first": largest_first},
+            "sequential": sequential | {"lanes": 1},
+            "speedup": round(batched["value"] / sequential["value"], 3),
+            "device_gb": round(device_gb, 2),
+            "timing": "device clock (CUDA events), min of 3 runs after planning; "
+                      "service = an image's own analysis, ready = batch arrival to its end"}
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -499,6 +601,8 @@ def main():
                         help="WxH of a smaller image of the same generator (profiling only)")
     parser.add_argument("--no-reference-gpu", action="store_true",
                         help="skip timing the reference's own CUDA path")
+    parser.add_argument("--no-batched", action="store_true",
+                        help="skip the batched-form leg (64 images of uneven sizes)")
     parser.add_argument("--precision", default="exact", choices=["exact", "fast"],
                         help="candidate-cost precision: exact (FP64, the reference's CPU "
                              "results bit for bit) or fast (tcgen05 tensor cores)")
@@ -517,8 +621,13 @@ def main():
     pool = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.launch_list:
         pool = ReferencePool()
+    batch_images = None
+    if rank == 0 and world == 1 and not args.no_batched and not args.launch_list:
+        batch_images = BatchImages()
     out = run_gpu(args)
     if out:
+        if batch_images is not None:
+            out["batched_form"] = batched_leg(batch_images, 1 if args.precision == "fast" else 0)
         if pool is not None:
             out["cpu_baseline"] = cpu_baseline_leg(pool)
         if world == 1 and not args.launch_list and not args.no_reference_gpu:

@@ -30,6 +30,15 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_dc_token_sizes": [Z, Z, P, P, P, P],
+    "gjxl_b200_batch_create": [I, P, P],
+    "gjxl_b200_session_device_bytes": [Z, Z, P, P],
+    "gjxl_b200_session_create_in": [Z, Z, P, P, Z, P],
+    "gjxl_b200_batch_destroy": None,
+    "gjxl_b200_batch_set_schedule": [P, I, I],
+    "gjxl_b200_batch_analyze": [P, P, Z, I, P, P],
+    "gjxl_b200_batch_autotune": [P, P, Z, P, Z, P, P],
+    "gjxl_b200_batch_schedule": [Z, P, I, I, P, P],
+    "gjxl_b200_batch_device_bytes": [P],
     "gjxl_b200_dc_tokenize": [P, Z, P, P, P, P, P, Z, Z, I, P, P, P, P, P, Z, P, P],
     "gjxl_b200_quant_matrix": [I, I, P, P, Z],
     "gjxl_b200_ac_strategy_cost_bytes": [Z, Z],
@@ -64,7 +73,8 @@ _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
              "gjxl_b200_ac_strategy_cost_bytes": c_size_t,
              "gjxl_b200_ac_token_capacity": c_size_t,
-             "gjxl_b200_butteraugli_pnorm_scratch_bytes": c_size_t}
+             "gjxl_b200_butteraugli_pnorm_scratch_bytes": c_size_t,
+             "gjxl_b200_batch_device_bytes": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

@@ -1100,8 +1100,10 @@ struct ButteraugliState {
   int sm_count = 0;                   // SMs of the device the state lives on
   Kernel17 k_opsin, k_low, k_high, k_ultra, k_mask;
 
+  bool external_arena = false;  // planes lent by the owner (not freed)
+
   ~ButteraugliState() {
-    if (arena) cudaFree(arena);
+    if (arena && !external_arena) cudaFree(arena);
   }
 };
 
@@ -1283,7 +1285,29 @@ void TransformScales(ButteraugliState& st, const float* linear, size_t stride, s
 
 }  // namespace
 
-int ButteraugliCreate(size_t width, size_t height, float intensity_target, ButteraugliState** out) {
+namespace {
+
+struct ScaleExtents {
+  size_t main_n = 0, sub_n = 0;
+};
+
+ScaleExtents Extents(size_t width, size_t height) {
+  ScaleExtents e;
+  const bool expanded = width < 8 || height < 8;
+  e.main_n = std::max<size_t>(8, width) * std::max<size_t>(8, height);
+  if (!expanded && width >= 15 && height >= 15) e.sub_n = ((width + 1) / 2) * ((height + 1) / 2);
+  return e;
+}
+
+}  // namespace
+
+size_t ButteraugliArenaBytes(size_t width, size_t height) {
+  const ScaleExtents e = Extents(width, height);
+  return (ScaleFloats(e.main_n) + ScaleFloats(e.sub_n) + 64) * sizeof(float);
+}
+
+int ButteraugliCreate(size_t width, size_t height, float intensity_target, void* external,
+                      ButteraugliState** out) {
   auto* st = new (std::nothrow) ButteraugliState();
   if (st == nullptr) return SetError(GJXL_B200_OUT_OF_MEMORY, "butteraugli: host allocation");
   st->width = static_cast<int>(width);
@@ -1310,10 +1334,17 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, Butte
     st->sm_count = 0;  // the Malta grid then takes one CTA per tile
   }
   const size_t floats = ScaleFloats(st->main.n) + ScaleFloats(st->sub.n) + 64;
-  int status = CheckCuda(DeviceMalloc(reinterpret_cast<void**>(&st->arena), floats * sizeof(float)), "butteraugli: cudaMalloc");
-  if (status != GJXL_B200_OK) {
-    delete st;
-    return status;
+  if (external != nullptr) {
+    st->arena = static_cast<float*>(external);
+    st->external_arena = true;
+  } else {
+    const int status = CheckCuda(DeviceMalloc(reinterpret_cast<void**>(&st->arena),
+                                              floats * sizeof(float)),
+                                 "butteraugli: cudaMalloc");
+    if (status != GJXL_B200_OK) {
+      delete st;
+      return status;
+    }
   }
   AssignScale(st->main, st->arena);
   if (st->has_sub) AssignScale(st->sub, st->arena + ScaleFloats(st->main.n));
@@ -1376,7 +1407,7 @@ extern "C" int gjxl_b200_butteraugli_create(size_t width, size_t height, float i
     return SetError(GJXL_B200_INVALID_ARGUMENT, "butteraugli_create: invalid arguments");
   }
   ButteraugliState* st = nullptr;
-  const int status = ButteraugliCreate(width, height, intensity_target, &st);
+  const int status = ButteraugliCreate(width, height, intensity_target, nullptr, &st);
   if (status != GJXL_B200_OK) return status;
   // The public handle type derives from the state without adding members.
   static_assert(sizeof(gjxl_b200_butteraugli) == sizeof(ButteraugliState), "");

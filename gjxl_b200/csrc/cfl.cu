@@ -155,13 +155,26 @@ __global__ void __launch_bounds__(kCflThreads, 3) CflTileKernel(const __grid_con
     const int index0 = u * 8 + y0, index1 = index0 + 4;
     const float inv_x0 = __ldg(p.inv_x + index0), inv_x1 = __ldg(p.inv_x + index1);
     const float inv_b0 = __ldg(p.inv_b + index0), inv_b1 = __ldg(p.inv_b + index1);
-    for (int b = warp; b < blocks; b += 4) {
+    // The lane's pixels (row lane >> 2, columns 2 (lane & 3) + 0, 1) of the
+    // three channels, Y first, then X and B; the next block's are loaded
+    // while this one is transformed.
+    auto load_block = [&](int b, float2 (&pix)[3]) {
+      if (b >= blocks) return;
       const int bx = bx0 + b % tw, by = by0 + b / tw;
+      const size_t at = static_cast<size_t>(by * 8 + (lane >> 2)) * p.stride + bx * 8 +
+                        (lane & 3) * 2;
+      pix[0] = *reinterpret_cast<const float2*>(p.opsin + p.pitch + at);
+      pix[1] = *reinterpret_cast<const float2*>(p.opsin + at);
+      pix[2] = *reinterpret_cast<const float2*>(p.opsin + 2 * p.pitch + at);
+    };
+    float2 current[3], next[3];
+    load_block(warp, current);
+    for (int b = warp; b < blocks; b += 4) {
+      load_block(b + 4, next);
+#pragma unroll
       for (int c = 0; c < 3; ++c) {
         const int ch = c == 0 ? 1 : c == 1 ? 0 : 2;  // Y first, then X and B
-        const float* src = p.opsin + ch * p.pitch + static_cast<size_t>(by * 8) * p.stride + bx * 8;
-        const float2 pix = *reinterpret_cast<const float2*>(
-          src + static_cast<size_t>(lane >> 2) * p.stride + (lane & 3) * 2);
+        const float2 pix = current[c];
         __syncwarp();
         reinterpret_cast<double2*>(px)[lane] = make_double2(pix.x, pix.y);
         __syncwarp();
@@ -210,6 +223,8 @@ __global__ void __launch_bounds__(kCflThreads, 3) CflTileKernel(const __grid_con
         float2* map_pairs = pairs + (is_b ? kTileValues : 0);
         *reinterpret_cast<float4*>(map_pairs + y0 * js + b * 16 + 2 * u) = out;
       }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) current[c] = next[c];
     }
   }
   __syncthreads();
@@ -241,15 +256,34 @@ __global__ void __launch_bounds__(kCflThreads, 3) CflTileKernel(const __grid_con
         BarSync(kBarFull + buffer);
         const float4* src = reinterpret_cast<const float4*>(
           terms + (buffer * kTermRows + row) * kTermStride);
-        const int quads = min(kChunk, js - c * kChunk) / 4;
-        for (int q = 0; q < quads; ++q) {
-          const float4 t = src[q];
-          lane_sum += t.x;
-          lane_sum += t.y;
-          lane_sum += t.z;
-          lane_sum += t.w;
+        // All of the chunk's terms into registers first (the loads overlap),
+        // which also frees the buffer for the producers before the adds.
+        // A chunk holds 32 terms per chain, or 16 in a ragged tile's last.
+        float4 t[kChunk / 4];
+        const bool half = js - c * kChunk < kChunk;
+#pragma unroll
+        for (int q = 0; q < kChunk / 8; ++q) t[q] = src[q];
+        if (!half) {
+#pragma unroll
+          for (int q = kChunk / 8; q < kChunk / 4; ++q) t[q] = src[q];
         }
         BarArrive(kBarEmpty + buffer);
+#pragma unroll
+        for (int q = 0; q < kChunk / 8; ++q) {
+          lane_sum += t[q].x;
+          lane_sum += t[q].y;
+          lane_sum += t[q].z;
+          lane_sum += t[q].w;
+        }
+        if (!half) {
+#pragma unroll
+          for (int q = kChunk / 8; q < kChunk / 4; ++q) {
+            lane_sum += t[q].x;
+            lane_sum += t[q].y;
+            lane_sum += t[q].z;
+            lane_sum += t[q].w;
+          }
+        }
       }
       // Horizontal sums (l0 + l1) + (l2 + l3) for each kind, per map.
       float sums[3];

@@ -90,6 +90,8 @@ struct Session {
   gjxl_b200_options options{};
   void* arena = nullptr;
   size_t arena_bytes = 0;
+  bool external_arena = false;  // device memory lent by the caller (not freed)
+  bool host_mirrors = false;    // pinned mirrors allocated (first analyze_host)
   uint8_t* pixels = nullptr;
   size_t pixel_capacity = 0;
   float* linear = nullptr;
@@ -209,7 +211,7 @@ struct Session {
     if (prepare_stream) cudaStreamDestroy(prepare_stream);
     if (prepare_fork) cudaEventDestroy(prepare_fork);
     if (prepare_join) cudaEventDestroy(prepare_join);
-    if (arena) cudaFree(arena);
+    if (arena && !external_arena) cudaFree(arena);
     if (host_block) cudaFreeHost(host_block);
     if (butteraugli) ButteraugliDestroy(butteraugli);
     if (tokens) gjxl_b200_ac_tokens_destroy(tokens);
@@ -223,7 +225,10 @@ struct Session {
 
 namespace {
 
-int Allocate(Session* s) {
+// Device layout of a session: its own arena, then the Butteraugli planes.
+// With `external`, both are carved from caller memory of at least
+// DeviceBytes(); else allocated here.
+int Allocate(Session* s, void* external, size_t external_bytes, size_t* device_bytes) {
   const size_t plane = s->pw * s->ph;
   const size_t image = s->width * s->height;
   s->lin_stride = Align(s->width, 4);
@@ -297,16 +302,51 @@ int Allocate(Session* s) {
   };
   size_t total = 0;
   for (const Item& item : items) total = Align(total, 256) + item.bytes;
-  int status = CheckCuda(DeviceMalloc(&s->arena, total), "session: cudaMalloc");
-  if (status != GJXL_B200_OK) return status;
-  s->arena_bytes = total;
+  const size_t butteraugli_offset = Align(total, 256);
+  const size_t needed = butteraugli_offset + ButteraugliArenaBytes(s->width, s->height);
+  if (device_bytes != nullptr) {
+    *device_bytes = needed;
+    return GJXL_B200_OK;
+  }
+  int status;
+  if (external != nullptr) {
+    if (external_bytes < needed || reinterpret_cast<uintptr_t>(external) % 256) {
+      return SetError(GJXL_B200_INVALID_ARGUMENT, "session: device memory too small or unaligned");
+    }
+    s->arena = external;
+    s->external_arena = true;
+  } else {
+    status = CheckCuda(DeviceMalloc(&s->arena, total), "session: cudaMalloc");
+    if (status != GJXL_B200_OK) return status;
+  }
+  s->arena_bytes = external != nullptr ? needed : total;
   size_t offset = 0;
   for (const Item& item : items) {
     offset = Align(offset, 256);
     *item.ptr = static_cast<unsigned char*>(s->arena) + offset;
     offset += item.bytes;
   }
-  // Pinned host mirrors.
+  status = ButteraugliCreate(s->width, s->height, 80.0f,
+                             external != nullptr
+                               ? static_cast<unsigned char*>(external) + butteraugli_offset
+                               : nullptr,
+                             &s->butteraugli);
+  if (status != GJXL_B200_OK) return status;
+  if (s->options.tokenize) {
+    status = gjxl_b200_ac_tokens_create(s->bx, s->by, &s->tokens);
+    if (status != GJXL_B200_OK) return status;
+  }
+  return GJXL_B200_OK;
+}
+
+// Pinned host mirrors of the results, allocated by the first host-input
+// analysis (device-resident callers never need them).
+int AllocateHostMirrors(Session* s) {
+  if (s->host_mirrors) return GJXL_B200_OK;
+  const size_t plane = s->pw * s->ph;
+  const size_t blocks = s->bx * s->by;
+  const size_t tiles = s->tx * s->ty;
+  int status;
   const size_t host_bytes = Align(blocks, 16) + Align(blocks * 4, 16) + Align(2 * tiles, 16) +
                             16 + 16 + Align(blocks * 4, 16) + Align(blocks * 4, 16) +
                             Align(3 * blocks * 4, 16) + 64 + 64 +
@@ -333,11 +373,7 @@ int Allocate(Session* s) {
   s->host_pnorms = reinterpret_cast<double*>(take(64));
   s->host_quantizer = reinterpret_cast<AqQuantizer*>(take(sizeof(AqQuantizer)));
   s->host_qac = reinterpret_cast<int32_t*>(take(3 * plane * 4));
-  status = ButteraugliCreate(s->width, s->height, 80.0f, &s->butteraugli);
-  if (status != GJXL_B200_OK) return status;
   if (s->options.tokenize) {
-    status = gjxl_b200_ac_tokens_create(s->bx, s->by, &s->tokens);
-    if (status != GJXL_B200_OK) return status;
     void* mirror = nullptr;
     status = CheckCuda(HostMalloc(&mirror, s->token_capacity * 6 + (s->groups + 1) * 4 + 64),
                        "session: token mirrors");
@@ -356,6 +392,12 @@ int Allocate(Session* s) {
     s->host_dc_group_info = s->host_meta_tokens + 2 * s->meta_capacity;
     s->host_dc_histogram = s->host_dc_group_info + 5 * s->dc_groups;
   }
+  s->host_mirrors = true;
+  return GJXL_B200_OK;
+}
+
+int CreateStreams(Session* s) {
+  int status;
   for (auto& side : s->fan_side) {
     status = CheckCuda(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking),
                        "session: side stream");
@@ -644,14 +686,18 @@ extern "C" void gjxl_b200_default_options(gjxl_b200_options* options) {
   options->precision = GJXL_B200_PRECISION_EXACT;
 }
 
-extern "C" int gjxl_b200_session_create(size_t width, size_t height,
-                                        const gjxl_b200_options* options,
-                                        gjxl_b200_session** out) {
-  ClearLastError();
-  if (out == nullptr || width == 0 || height == 0 || width > (1u << 20) || height > (1u << 20)) {
+namespace {
+
+// Session creation proper. With `query`, only the device bytes the session
+// needs (its arena and the Butteraugli planes) are computed; with
+// `external`, those come from the caller's memory.
+int CreateSession(size_t width, size_t height, const gjxl_b200_options* options, void* external,
+                  size_t external_bytes, size_t* query, gjxl_b200_session** out) {
+  if ((out == nullptr && query == nullptr) || width == 0 || height == 0 ||
+      width > (1u << 20) || height > (1u << 20)) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: invalid extent");
   }
-  *out = nullptr;
+  if (out != nullptr) *out = nullptr;
   gjxl_b200_options o;
   gjxl_b200_default_options(&o);
   if (options != nullptr) {
@@ -701,13 +747,45 @@ extern "C" int gjxl_b200_session_create(size_t width, size_t height,
     s->dc_groups = ((s->bx + 255) / 256) * ((s->by + 255) / 256);
     s->meta_capacity = MetaTokenCapacity(s->bx, s->by);
   }
-  status = Allocate(s);
+  if (query != nullptr) {
+    status = Allocate(s, nullptr, 0, query);
+    delete s;
+    return status;
+  }
+  status = Allocate(s, external, external_bytes, nullptr);
+  if (status == GJXL_B200_OK) status = CreateStreams(s);
   if (status != GJXL_B200_OK) {
     delete s;
     return status;
   }
   *out = s;
   return GJXL_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int gjxl_b200_session_create(size_t width, size_t height,
+                                        const gjxl_b200_options* options,
+                                        gjxl_b200_session** out) {
+  ClearLastError();
+  return CreateSession(width, height, options, nullptr, 0, nullptr, out);
+}
+
+extern "C" int gjxl_b200_session_device_bytes(size_t width, size_t height,
+                                              const gjxl_b200_options* options, size_t* bytes) {
+  ClearLastError();
+  if (bytes == nullptr) return SetError(GJXL_B200_INVALID_ARGUMENT, "session_device_bytes: null");
+  return CreateSession(width, height, options, nullptr, 0, bytes, nullptr);
+}
+
+extern "C" int gjxl_b200_session_create_in(size_t width, size_t height,
+                                           const gjxl_b200_options* options, void* device_memory,
+                                           size_t device_bytes, gjxl_b200_session** out) {
+  ClearLastError();
+  if (device_memory == nullptr) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create_in: null device memory");
+  }
+  return CreateSession(width, height, options, device_memory, device_bytes, nullptr, out);
 }
 
 extern "C" void gjxl_b200_session_destroy(gjxl_b200_session* session) { delete session; }
@@ -754,6 +832,7 @@ extern "C" int gjxl_b200_session_analyze_host(gjxl_b200_session* s, const uint8_
     return SetError(GJXL_B200_SUBMISSION_FAILED,
                     "session_analyze_host: injected submission failure");
   }
+  GJXL_TRY(AllocateHostMirrors(s));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // Packed rows in the session's input buffer (one contiguous copy when the
   // caller's rows are packed too).

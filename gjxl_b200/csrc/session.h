@@ -43,7 +43,10 @@ int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float targe
                            uint8_t* cells, uint32_t* error, cudaStream_t stream);
 
 struct ButteraugliState;
-int ButteraugliCreate(size_t width, size_t height, float intensity_target, ButteraugliState** out);
+// Planes of one Butteraugli state; `external` (nullable) lends them.
+size_t ButteraugliArenaBytes(size_t width, size_t height);
+int ButteraugliCreate(size_t width, size_t height, float intensity_target, void* external,
+                      ButteraugliState** out);
 void ButteraugliDestroy(ButteraugliState* state);
 int ButteraugliPrepare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
                        cudaStream_t stream);

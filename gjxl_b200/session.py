@@ -111,6 +111,20 @@ class AnalysisSession:
         _check(lib.gjxl_b200_session_outputs(handle, ctypes.byref(self.outputs)),
                "gjxl_b200_session_outputs")
 
+    @classmethod
+    def borrow(cls, handle: int, width: int, height: int) -> "AnalysisSession":
+        """A non-owning view of a session that another object owns (a batch's
+        pooled sessions); close() leaves it alone."""
+        _bind()
+        self = cls.__new__(cls)
+        self.handle = None
+        self._borrowed = c_void_p(handle)
+        self.width, self.height = width, height
+        self.outputs = Outputs()
+        _check(_lib.load().gjxl_b200_session_outputs(self._borrowed, ctypes.byref(self.outputs)),
+               "gjxl_b200_session_outputs")
+        return self
+
     def set_butteraugli_target(self, target: float):
         """Retargets later analyses; every buffer is kept."""
         _check(_lib.load().gjxl_b200_session_set_butteraugli_target(self.handle, target),

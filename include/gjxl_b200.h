@@ -500,6 +500,20 @@ GJXL_B200_API int gjxl_b200_session_create(size_t width, size_t height,
                                            const gjxl_b200_options* options,
                                            gjxl_b200_session** session);
 GJXL_B200_API void gjxl_b200_session_destroy(gjxl_b200_session* session);
+/* Device bytes a session of this extent and options needs for its working
+ * buffers (all but a small per-session table of the AC tokenizer), and a
+ * session whose working buffers are carved from caller memory (256-byte
+ * aligned, at least that many bytes; not freed by the session). Sessions
+ * that never run at the same time, such as those of one batch lane, may
+ * share one region: nothing in it outlives an analysis. Pinned host mirrors
+ * are allocated by a session's first gjxl_b200_session_analyze_host. */
+GJXL_B200_API int gjxl_b200_session_device_bytes(size_t width, size_t height,
+                                                 const gjxl_b200_options* options,
+                                                 size_t* bytes);
+GJXL_B200_API int gjxl_b200_session_create_in(size_t width, size_t height,
+                                              const gjxl_b200_options* options,
+                                              void* device_memory, size_t device_bytes,
+                                              gjxl_b200_session** session);
 /* Changes the Butteraugli target of later analyses, keeping every buffer of
  * the session (the prepared state a target-size search reuses across its
  * attempts: src/codestream/workflow.cpp:1686-1740, rate_control.cpp:246).
@@ -541,6 +555,59 @@ GJXL_B200_API int gjxl_b200_session_kernel_count(gjxl_b200_session* session,
                                                  const uint8_t* pixels,
                                                  size_t row_stride_bytes, int channels,
                                                  size_t* kernels);
+
+/*
+ * Batched analysis (row N3). Replaces the reference's VarDctBatchEncoder
+ * (src/codestream/batch_workflow.h:74-118) for the analysis half: one call
+ * runs every request, keeps request order in the results, reports a status
+ * per image and times each image as queue / service / ready (milliseconds
+ * from the batch's arrival, device clock). Each image runs its own session
+ * (pooled per extent and reused by later calls, so a repeated batch replays
+ * captured graphs) on one of `lanes` CUDA streams; the lanes' analyses run
+ * concurrently. max_in_flight: lanes, 1..16 (0: 2 until autotuned).
+ */
+typedef struct gjxl_b200_batch gjxl_b200_batch;
+typedef struct gjxl_b200_batch_request {
+  const uint8_t* pixels;   /* packed 8-bit sRGB rows: device memory, or host
+                              memory when host_input is set */
+  size_t width, height, row_stride;
+  int channels;            /* 3 or 4 */
+  float butteraugli_target;
+} gjxl_b200_batch_request;
+typedef struct gjxl_b200_batch_result {
+  int status;                   /* StatusCode of this image */
+  gjxl_b200_session* session;   /* its results: gjxl_b200_session_outputs */
+  int lane;
+  double queue_ms, service_ms, ready_ms;
+} gjxl_b200_batch_result;
+
+GJXL_B200_API int gjxl_b200_batch_create(int max_in_flight, const gjxl_b200_options* options,
+                                         gjxl_b200_batch** batch);
+GJXL_B200_API void gjxl_b200_batch_destroy(gjxl_b200_batch* batch);
+/* Lanes and order (0: as given, 1: largest first) of later calls. */
+GJXL_B200_API int gjxl_b200_batch_set_schedule(gjxl_b200_batch* batch, int lanes,
+                                               int largest_first);
+/* Runs the batch and waits for it. host_input: pixels are host memory and
+ * each image goes through gjxl_b200_session_analyze_host (host mirrors
+ * filled), one host thread per lane; else device memory and
+ * gjxl_b200_session_analyze. batch_ms: arrival to the last image's end. */
+GJXL_B200_API int gjxl_b200_batch_analyze(gjxl_b200_batch* batch,
+                                          const gjxl_b200_batch_request* requests,
+                                          size_t count, int host_input,
+                                          gjxl_b200_batch_result* results, double* batch_ms);
+/* Autotuner: runs the (device-input) batch with each lane count of
+ * lane_counts and both orders, keeps the fastest and returns it. */
+GJXL_B200_API int gjxl_b200_batch_autotune(gjxl_b200_batch* batch,
+                                           const gjxl_b200_batch_request* requests,
+                                           size_t count, const int* lane_counts,
+                                           size_t lane_count_count, int* lanes,
+                                           int* largest_first);
+/* The placement rule (host only): order[k] = k-th request to place (as
+ * given, or by decreasing pixels, ties in request order); each goes to the
+ * lane with the fewest pixels so far (lowest index on ties). */
+GJXL_B200_API int gjxl_b200_batch_schedule(size_t count, const size_t* pixels, int lanes,
+                                           int largest_first, int* lane_of, size_t* order);
+GJXL_B200_API size_t gjxl_b200_batch_device_bytes(const gjxl_b200_batch* batch);
 
 /*
  * Measurement (no counterpart in the reference).

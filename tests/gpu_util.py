@@ -110,3 +110,18 @@ def differing_blocks(a: np.ndarray, b: np.ndarray, pixels: bool = False) -> np.n
         h, w = d.shape
         d = d.reshape(h // 8, 8, w // 8, 8).any(axis=(1, 3))
     return d
+
+
+class _CudaArray:
+    """__cuda_array_interface__ over a raw device pointer (no copy)."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def device_view(ptr: int, shape, dtype=np.uint8) -> torch.Tensor:
+    """A torch view of device memory the library owns (read it before the
+    owner reuses it)."""
+    return torch.as_tensor(_CudaArray(ptr, shape, np.dtype(dtype).str), device="cuda")

@@ -58,8 +58,8 @@ def test_device_error_word_maps_to_device_error(cuda):
 
 
 def test_every_allocation_failure_is_clean(cuda):
-    """Session creation has several allocation check points (arena, pinned
-    mirrors, Butteraugli planes, token buffers). Failing each one in turn
+    """Session creation has several allocation check points (the arena, the
+    Butteraugli planes, the AC tokenizer's tables). Failing each one in turn
     returns OUT_OF_MEMORY and leaves device memory where it was; past the
     last one, creation succeeds."""
     # One-time per-device set-up (shared tables, module loading) first.
@@ -81,8 +81,26 @@ def test_every_allocation_failure_is_clean(cuda):
         break
     else:
         pytest.fail("session creation never succeeded")
-    assert failures >= 4
+    assert failures >= 3
     assert free_bytes() == before
+
+
+def test_host_mirror_allocation_failure_is_clean(cuda):
+    """The pinned host mirrors come with the first host-input analysis: a
+    failed allocation there returns OUT_OF_MEMORY, and the next call, with
+    nothing armed, allocates them and succeeds."""
+    img = generate_srgb8(120, 96, 17)
+    s = AnalysisSession(120, 96)
+    arm(ALLOCATION, 1)
+    with pytest.raises(_lib.GjxlB200Error) as info:
+        s.analyze_host(img, stream_ptr())
+    arm(ALLOCATION, 0)
+    assert info.value.code == 4
+    s.analyze_host(img, stream_ptr())
+    torch.cuda.synchronize()
+    assert s.host_error() == 0
+    assert s.host_results()["cells"].shape == (12, 15)
+    s.close()
 
 
 def test_graph_failure_falls_back_to_direct_launches(cuda):
