@@ -31,6 +31,13 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_dc_token_sizes": [Z, Z, P, P, P, P],
     "gjxl_b200_batch_create": [I, P, P],
+    "gjxl_b200_cnn_param_count": [],
+    "gjxl_b200_cnn_workspace_bytes": [I],
+    "gjxl_b200_cnn_train_scratch_bytes": [I],
+    "gjxl_b200_cnn_gather": [P, Z, Z, Z, Z, P, I, F, P, P],
+    "gjxl_b200_cnn_forward": [P, I, P, P, P],
+    "gjxl_b200_cnn_train_step": [P, I, P, P, P, P, F, P, P, P, P],
+    "gjxl_b200_cnn_adamw": [P, P, P, P, I, F, F, F, F, F, P],
     "gjxl_b200_session_device_bytes": [Z, Z, P, P],
     "gjxl_b200_session_create_in": [Z, Z, P, P, Z, P],
     "gjxl_b200_batch_destroy": None,
@@ -74,7 +81,10 @@ _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_ac_strategy_cost_bytes": c_size_t,
              "gjxl_b200_ac_token_capacity": c_size_t,
              "gjxl_b200_butteraugli_pnorm_scratch_bytes": c_size_t,
-             "gjxl_b200_batch_device_bytes": c_size_t}
+             "gjxl_b200_batch_device_bytes": c_size_t,
+             "gjxl_b200_cnn_param_count": c_size_t,
+             "gjxl_b200_cnn_workspace_bytes": c_size_t,
+             "gjxl_b200_cnn_train_scratch_bytes": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

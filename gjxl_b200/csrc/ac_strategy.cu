@@ -77,7 +77,19 @@ struct CostParams {
   const float* inverse_dequant;  // family table [3][N]
   float* costs;           // family plane, blocks_x x blocks_y (anchor positions)
   uint32_t* error;
+  // Learned analysis mode: the tiles whose candidates of this family are
+  // scored (raster indices) and their number. Null: every tile.
+  const uint32_t* kept_tiles;
+  const uint32_t* kept_count;
 };
+
+// Candidates scored: every tile's, or those of the kept tiles.
+__device__ __forceinline__ uint32_t ScoredCandidates(const CostParams& p, uint32_t all) {
+  return p.kept_count != nullptr ? *p.kept_count * (p.local_x * p.local_y) : all;
+}
+__device__ __forceinline__ uint32_t CandidateTile(const CostParams& p, uint32_t slot) {
+  return p.kept_tiles != nullptr ? p.kept_tiles[slot] : slot;
+}
 
 template <int W, int H>
 struct Shape {
@@ -202,7 +214,7 @@ __device__ __forceinline__ CandidateInputs<CW, CH> FetchCandidate(const CostPara
   CandidateInputs<CW, CH> in;
   if (cand < candidate_count) {
     const uint32_t per_tile = p.local_x * p.local_y;
-    const uint32_t tile = cand / per_tile, local = cand % per_tile;
+    const uint32_t tile = CandidateTile(p, cand / per_tile), local = cand % per_tile;
     const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
     const int lx = (local % p.local_x) * p.anchor_step;
     const int ly = (local / p.local_x) * p.anchor_step;
@@ -304,12 +316,14 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   const int tid = threadIdx.x;
   // Anchors first (integer arithmetic only), so that the pixel loads can
   // start before the quant norms and CfL factors arrive.
+  candidate_count = ScoredCandidates(p, candidate_count);
+  if (blockIdx.x * K >= candidate_count) return;  // past the kept tiles' candidates
   if (tid < K) {
     const uint32_t cand = blockIdx.x * K + tid;
     int ax = -1, ay = -1;
     if (cand < candidate_count) {
       const uint32_t per_tile = p.local_x * p.local_y;
-      const uint32_t tile = cand / per_tile, local = cand % per_tile;
+      const uint32_t tile = CandidateTile(p, cand / per_tile), local = cand % per_tile;
       const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
       const int lx = (local % p.local_x) * p.anchor_step;
       const int ly = (local / p.local_x) * p.anchor_step;
@@ -732,6 +746,7 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
     umma::FenceAfterSync();
   };
 
+  candidate_count = ScoredCandidates(p, candidate_count);
   const uint32_t units = (candidate_count + G - 1) / G;
   for (uint32_t unit = blockIdx.x; unit < units && !aborted; unit += gridDim.x) {
     if (tid < G) {
@@ -1272,7 +1287,8 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
                           const float* quant_field, const float* pixel_mask, size_t mask_stride,
                           const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
                           int precision, float* costs, uint32_t* error, cudaStream_t stream,
-                          const StreamFan* fan) {
+                          const StreamFan* fan, const uint32_t* kept_tiles,
+                          const uint32_t* kept_counts) {
   DeviceTables d;
   int status = GetDeviceTables(&d);
   if (status != GJXL_B200_OK) return status;
@@ -1310,6 +1326,10 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
     CostParams q = p;
     q.anchor_step = (dense && f >= 4) ? 1 : kFamilyStep[f];
     q.costs = costs + f * bx * by;
+    if (kept_tiles != nullptr) {
+      q.kept_tiles = kept_tiles + static_cast<size_t>(f) * p.tiles_x * p.tiles_y;
+      q.kept_count = kept_counts + f;
+    }
     const bool tensor = precision == GJXL_B200_PRECISION_FAST;
     switch (f) {
       case 0:
@@ -1388,7 +1408,8 @@ extern "C" int gjxl_b200_ac_strategy_costs(
   return LaunchAcStrategyCosts(opsin, opsin_stride, opsin_plane_pitch, padded_width,
                                padded_height, quant_field, pixel_mask, pixel_mask_stride, y_to_x,
                                y_to_b, butteraugli_target, dense_dct32 != 0, precision, costs,
-                               device_error, static_cast<cudaStream_t>(stream), nullptr);
+                               device_error, static_cast<cudaStream_t>(stream), nullptr,
+                               nullptr, nullptr);
 }
 
 extern "C" int gjxl_b200_ac_strategy_search(

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "aq.h"
+#include "cnn.h"
 #include "dc_tokens.cuh"
 #include "host_util.h"
 
@@ -34,6 +35,7 @@ enum Stage : int {
   kStageInitialQuant,
   kStageGaborishInverse,
   kStageInitialCfl,
+  kStageProposals,
   kStageAcCosts,
   kStageAcMerge,
   kStageTransforms,
@@ -44,7 +46,7 @@ enum Stage : int {
 
 const char* const kStageNames[kStageCount] = {
   "prepare_input",   "matrix_scale_stats", "initial_quant_field", "gaborish_inverse",
-  "initial_cfl",     "ac_strategy_costs",  "ac_strategy_merge",   "forward_transforms",
+  "initial_cfl",     "proposals",          "ac_strategy_costs",  "ac_strategy_merge",   "forward_transforms",
   "adaptive_quantization", "ac_tokenize",
 };
 
@@ -125,6 +127,17 @@ struct Session {
   int32_t* qac = nullptr;      // quantized AC, footprint layout
   float* dc = nullptr;         // extracted DC (3 x blocks)
   int32_t* qdc = nullptr;
+  // Learned mode (proposal_weights set): the network's workspace over all
+  // tiles, per-block proposals, top-3 mass and log field scale, per-tile
+  // family masks.
+  void* cnn_workspace = nullptr;
+  uint8_t* proposals = nullptr;
+  float* proposal_mass = nullptr;
+  float* log_scale = nullptr;
+  uint8_t* tile_masks = nullptr;
+  uint32_t* kept_tiles = nullptr;   // per family, the tiles whose candidates are scored
+  uint32_t* kept_counts = nullptr;
+  bool learned = false;
   // DC-group token streams (tokenize != 0).
   uint2* dc_tokens = nullptr;
   uint2* meta_tokens = nullptr;
@@ -292,6 +305,14 @@ int Allocate(Session* s, void* external, size_t external_bytes, size_t* device_b
     {reinterpret_cast<void**>(&s->histogram), (s->token_capacity ? 4 * 495 * 128 : 0) * 4},
     {reinterpret_cast<void**>(&s->scans), 13 * 3 * 1024 * sizeof(uint32_t)},
     {reinterpret_cast<void**>(&s->order_masks), 4 * sizeof(uint32_t)},
+    {reinterpret_cast<void**>(&s->cnn_workspace),
+     s->learned ? CnnWorkspaceBytes(static_cast<int>(tiles)) : 0},
+    {reinterpret_cast<void**>(&s->proposals), s->learned ? 3 * blocks : 0},
+    {reinterpret_cast<void**>(&s->proposal_mass), s->learned ? blocks * sizeof(float) : 0},
+    {reinterpret_cast<void**>(&s->log_scale), s->learned ? blocks * sizeof(float) : 0},
+    {reinterpret_cast<void**>(&s->tile_masks), s->learned ? tiles : 0},
+    {reinterpret_cast<void**>(&s->kept_tiles), s->learned ? 7 * tiles * sizeof(uint32_t) : 0},
+    {reinterpret_cast<void**>(&s->kept_counts), s->learned ? 8 * sizeof(uint32_t) : 0},
     {reinterpret_cast<void**>(&s->dc_tokens), s->options.tokenize ? 3 * blocks * 8 : 0},
     {reinterpret_cast<void**>(&s->meta_tokens), s->meta_capacity * 8},
     {reinterpret_cast<void**>(&s->dc_group_info), s->dc_groups * 5 * sizeof(uint32_t)},
@@ -450,6 +471,8 @@ int RunAq(Session* s, cudaStream_t stream) {
   GJXL_TRY(AqForwardCoefficients(s->pre, s->pw, s->pitch, s->bx, s->by, s->anchors,
                                  s->anchor_counts, s->coef, stream, &fan));
   GJXL_TRY(AqAdjustField(s->cells, s->bx, s->by, s->quant, s->adjusted, target, stream));
+  // Learned mode: the refinement starts from the predicted field.
+  if (s->learned) GJXL_TRY(CnnScaleField(s->adjusted, s->log_scale, blocks, stream));
   GJXL_TRY(CheckCuda(cudaMemcpyAsync(s->field, s->adjusted, blocks * sizeof(float),
                                      cudaMemcpyDeviceToDevice, stream), "session: field"));
   GJXL_TRY(AqPolicySetup(s->adjusted, blocks, target, s->range, s->policy, s->error, stream));
@@ -466,7 +489,9 @@ int RunAq(Session* s, cudaStream_t stream) {
                       s->qac, s->dc, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
                       s->matrix_multipliers, s->error, stream, &fan));
     GJXL_TRY(AqDcQuantize(s->dc, s->bx, s->by, s->quantizer, s->qdc, s->dc_rec, 1,
-                          iteration == s->iterations ? s->dc_tokens : nullptr, s->error + 2,
+                          iteration == s->iterations && s->options.tokenize ? s->dc_tokens
+                                                                            : nullptr,
+                          s->error + 2,
                           stream));
     GJXL_TRY(AqInverseSigma(s->cells, s->bx, s->by, s->raw, s->quantizer, s->inverse_sigma,
                             stream));
@@ -535,12 +560,28 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
   Mark(s, kStageInitialCfl, stream);
   GJXL_TRY(LaunchInitialCfl(s->pre, s->pw, s->pitch, s->pw, s->ph, s->y_to_x, s->y_to_b,
                             stream));
+  Mark(s, kStageProposals, stream);
+  if (s->learned) {
+    const int tiles = static_cast<int>(s->tx * s->ty);
+    const CnnActivations a = CnnLayout(s->cnn_workspace, tiles);
+    GJXL_TRY(CnnGather(s->pre, s->pw, s->pitch, s->pw, s->ph, nullptr, tiles, target, a.act[0],
+                       stream));
+    GJXL_TRY(CnnForward(s->options.proposal_weights, a, tiles, stream));
+    GJXL_TRY(CnnPropose(a.head, tiles, s->bx, s->by, s->proposals, s->proposal_mass,
+                        s->log_scale, stream));
+    GJXL_TRY(CnnTileMasks(s->proposals, s->proposal_mass, s->bx, s->by,
+                          s->options.proposal_confidence, s->tile_masks, stream));
+    GJXL_TRY(CnnKeptTiles(s->tile_masks, s->tx * s->ty, s->kept_tiles, s->kept_counts, stream));
+  }
   Mark(s, kStageAcCosts, stream);
   const StreamFan fan = MakeFan(s, stream);
   const bool dense = s->options.effort >= 10;
   GJXL_TRY(LaunchAcStrategyCosts(s->pre, s->pw, s->pitch, s->pw, s->ph, s->quant, s->pixel_mask,
                                  s->pw, s->y_to_x, s->y_to_b, target, dense,
-                                 s->options.precision, s->costs, s->error, stream, &fan));
+                                 s->options.precision, s->costs, s->error, stream, &fan,
+                                 s->learned ? s->kept_tiles : nullptr,
+                                 s->learned ? s->kept_counts : nullptr));
+  if (s->learned) GJXL_TRY(CnnMaskCosts(s->costs, s->tile_masks, s->bx, s->by, stream));
   Mark(s, kStageAcMerge, stream);
   GJXL_TRY(LaunchAcStrategySearch(s->costs, s->pw, s->ph, target, dense, s->cells, s->error,
                                   stream));
@@ -563,7 +604,7 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
     GJXL_TRY(gjxl_b200_ac_tokenize(s->tokens, s->cells, s->raw, s->qac, s->pw, s->pitch, &map,
                                    OrderMode(s->options), &outs, stream));
   }
-  if (s->dc_tokens != nullptr) {
+  if (s->options.tokenize) {
     // The DC tokens came with the last DC quantization; the AC metadata of
     // the final strategy, quant field and CfL maps (default EPF sharpness 4).
     GJXL_TRY(LaunchMetaTokens(s->cells, s->raw, nullptr, s->final_y_to_x, s->final_y_to_b, s->bx,
@@ -684,6 +725,9 @@ extern "C" void gjxl_b200_default_options(gjxl_b200_options* options) {
   options->tokenize = 1;
   options->order_mode = -1;
   options->precision = GJXL_B200_PRECISION_EXACT;
+  options->proposal_weights = nullptr;
+  options->learned_iterations = 0;
+  options->proposal_confidence = 0.6f;
 }
 
 namespace {
@@ -716,6 +760,11 @@ int CreateSession(size_t width, size_t height, const gjxl_b200_options* options,
   if (o.precision != GJXL_B200_PRECISION_EXACT && o.precision != GJXL_B200_PRECISION_FAST) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "session_create: precision is 0 or 1");
   }
+  if (o.proposal_weights != nullptr &&
+      (o.learned_iterations > 4 || !(o.proposal_confidence >= 0.0f && o.proposal_confidence <= 1.0f))) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT,
+                    "session_create: learned_iterations <= 4, proposal_confidence in [0, 1]");
+  }
   if (o.effort < 5 || o.effort > 10) {
     return SetError(GJXL_B200_UNSUPPORTED,
                     "session_create: efforts 5-10 (mixed-transform search) are supported");
@@ -740,7 +789,9 @@ int CreateSession(size_t width, size_t height, const gjxl_b200_options* options,
   s->tx = (s->bx + 7) / 8;
   s->ty = (s->by + 7) / 8;
   s->options = o;
-  s->iterations = AqIterations(o.effort);
+  s->learned = o.proposal_weights != nullptr;
+  s->iterations = s->learned && o.learned_iterations >= 0 ? o.learned_iterations
+                                                           : AqIterations(o.effort);
   s->groups = ((s->bx + 31) / 32) * ((s->by + 31) / 32);
   s->token_capacity = o.tokenize ? gjxl_b200_ac_token_capacity(s->bx, s->by) : 0;
   if (o.tokenize) {
@@ -926,6 +977,13 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   out->matrix_scale_stats = s->stats;
   out->matrix_scales = s->matrix_scales;
   out->quant_field = s->field;
+  out->adjusted_quant_field = s->adjusted;
+  if (s->learned) {
+    out->proposals = s->proposals;
+    out->proposal_mass = s->proposal_mass;
+    out->proposal_log_scale = s->log_scale;
+    out->tile_family_masks = s->tile_masks;
+  }
   out->raw_quant_field = s->raw;
   out->y_to_x = s->final_y_to_x;
   out->y_to_b = s->final_y_to_b;
@@ -964,7 +1022,7 @@ extern "C" int gjxl_b200_session_outputs(const gjxl_b200_session* s, gjxl_b200_o
   }
   out->host_token_count = s->host_token_count;
   out->dc_groups = s->dc_groups;
-  if (s->dc_tokens != nullptr) {
+  if (s->options.tokenize) {
     out->dc_tokens = reinterpret_cast<const uint32_t*>(s->dc_tokens);
     out->meta_tokens = reinterpret_cast<const uint32_t*>(s->meta_tokens);
     out->dc_group_info = s->dc_group_info;

@@ -38,7 +38,8 @@ int LaunchAcStrategyCosts(const float* opsin, size_t stride, size_t pitch, size_
                           const float* quant_field, const float* pixel_mask, size_t mask_stride,
                           const int8_t* y_to_x, const int8_t* y_to_b, float target, bool dense,
                           int precision, float* costs, uint32_t* error, cudaStream_t stream,
-                          const StreamFan* fan = nullptr);
+                          const StreamFan* fan = nullptr, const uint32_t* kept_tiles = nullptr,
+                          const uint32_t* kept_counts = nullptr);
 int LaunchAcStrategySearch(const float* costs, size_t pw, size_t ph, float target, bool dense,
                            uint8_t* cells, uint32_t* error, cudaStream_t stream);
 

@@ -17,7 +17,8 @@ from . import _lib
 class Options(Structure):
     _fields_ = [("struct_size", c_size_t), ("butteraugli_target", c_float), ("effort", c_int),
                 ("intensity_target", c_float), ("profile_stages", c_int), ("tokenize", c_int),
-                ("order_mode", c_int), ("precision", c_int)]
+                ("order_mode", c_int), ("precision", c_int), ("proposal_weights", c_void_p),
+                ("learned_iterations", c_int), ("proposal_confidence", c_float)]
 
 
 class Outputs(Structure):
@@ -28,7 +29,9 @@ class Outputs(Structure):
         ("opsin_plane_pitch", c_size_t)] + [(n, c_void_p) for n in (
             "initial_quant_field", "strategy_mask", "pixel_mask", "initial_y_to_x",
             "initial_y_to_b", "strategy_cells", "matrix_scale_stats", "matrix_scales",
-            "quant_field", "raw_quant_field", "y_to_x", "y_to_b", "quantized_ac", "quantized_dc",
+            "quant_field", "adjusted_quant_field", "proposals", "proposal_mass",
+            "proposal_log_scale", "tile_family_masks",
+            "raw_quant_field", "y_to_x", "y_to_b", "quantized_ac", "quantized_dc",
             "dc", "block_distance", "reconstructed_linear", "distance_map", "score_history",
             "quantizer_params", "device_error", "host_strategy_cells",
             "host_initial_quant_field", "host_y_to_x", "host_y_to_b", "host_matrix_scale_stats",
@@ -90,7 +93,9 @@ class AnalysisSession:
 
     def __init__(self, width: int, height: int, butteraugli_target: float = 1.0,
                  effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False,
-                 tokenize: bool = True, order_mode: int = -1, precision: int = 0):
+                 tokenize: bool = True, order_mode: int = -1, precision: int = 0,
+                 proposal_weights: int = 0, learned_iterations: int = 0,
+                 proposal_confidence: float = 0.6):
         _bind()
         lib = _lib.load()
         opts = Options()
@@ -102,6 +107,9 @@ class AnalysisSession:
         opts.tokenize = int(tokenize)
         opts.order_mode = order_mode
         opts.precision = precision
+        opts.proposal_weights = proposal_weights or None
+        opts.learned_iterations = learned_iterations
+        opts.proposal_confidence = proposal_confidence
         handle = c_void_p()
         _check(lib.gjxl_b200_session_create(width, height, ctypes.byref(opts),
                                             ctypes.byref(handle)), "gjxl_b200_session_create")

@@ -165,6 +165,36 @@ GJXL_B200_API int gjxl_b200_initial_cfl(const float* opsin, size_t opsin_stride,
                                         int8_t* y_to_b, void* stream);
 
 /*
+ * The learned proposal network (row N4; no reference counterpart): 4
+ * convolutions of 32 channels (3x3, BF16 with FP32 accumulation) over a
+ * 64x64 tile of Gaborish-inverted XYB with an 8-px halo and log2 distance,
+ * and a 1x1 head of 27 strategy logits and a log field scale per 8x8 block.
+ * Parameters: gjxl_b200_cnn_param_count() FP32 values. The workspace holds
+ * one batch of `tiles` inputs, activations and head outputs ([tiles][64][28]
+ * FP32, copied to head_out when given). Training: one step computes the loss
+ * (mean over all tiles * 64 block slots of weight * (softmax cross-entropy
+ * against the label strategy + qf_weight * squared error of the log field
+ * scale)) and the parameter gradients; AdamW updates the parameters.
+ */
+GJXL_B200_API size_t gjxl_b200_cnn_param_count(void);
+GJXL_B200_API size_t gjxl_b200_cnn_workspace_bytes(int tiles);
+GJXL_B200_API size_t gjxl_b200_cnn_train_scratch_bytes(int tiles);
+GJXL_B200_API int gjxl_b200_cnn_gather(const float* opsin, size_t opsin_stride,
+                                       size_t opsin_plane_pitch, size_t padded_width,
+                                       size_t padded_height, const int* tile_list, int tiles,
+                                       float distance, void* workspace, void* stream);
+GJXL_B200_API int gjxl_b200_cnn_forward(const float* params, int tiles, void* workspace,
+                                        float* head_out, void* stream);
+GJXL_B200_API int gjxl_b200_cnn_train_step(const float* params, int tiles, void* workspace,
+                                           const uint8_t* labels, const float* targets,
+                                           const float* weights, float qf_weight,
+                                           float* grads, void* scratch, float* loss,
+                                           void* stream);
+GJXL_B200_API int gjxl_b200_cnn_adamw(float* params, const float* grads, float* m, float* v,
+                                      int step, float lr, float beta1, float beta2, float eps,
+                                      float weight_decay, void* stream);
+
+/*
  * DC-group token streams (row f1): the DC residual and AC-metadata tokens of
  * every 256x256-block DC group, and their entropy-model histogram.
  * Replaces the CPU path's TokenizeSimpleDcGroupsForEncoder
@@ -392,6 +422,18 @@ typedef struct gjxl_b200_options {
                                gjxl_b200_ac_tokenize */
   int precision;            /* GJXL_B200_PRECISION_EXACT (default) or _FAST:
                                candidate-cost precision of the strategy search */
+  /* Learned mode (row N4; no reference counterpart). proposal_weights: device
+   * pointer to gjxl_b200_cnn_param_count() FP32 parameters of the proposal
+   * network, NULL (default) for the plain method. The network then proposes
+   * three strategies per block: in a tile whose blocks all keep at least
+   * proposal_confidence (default 0.6) of the probability mass on their
+   * proposals, the greedy merge considers only the proposed families (and
+   * DCT8); other tiles keep the full search. The refinement starts from the
+   * adjusted field scaled by the predicted factor and runs
+   * learned_iterations field updates (default 0) instead of the effort's. */
+  const float* proposal_weights;
+  int learned_iterations;
+  float proposal_confidence;
 } gjxl_b200_options;
 
 /* Session results. The adaptive-quantization fields mirror the reference's
@@ -421,6 +463,14 @@ typedef struct gjxl_b200_outputs {
   const float* matrix_scale_stats;  /* x_edge, b_edge, exposed_blue */
   const int* matrix_scales;         /* x_qm_scale, b_qm_scale */
   const float* quant_field;         /* blocks, final field */
+  const float* adjusted_quant_field; /* blocks, the field the refinement starts from */
+  /* Learned mode: per block the 3 proposed strategy codes, their softmax
+   * mass and the predicted log field scale; per tile the searched families
+   * (bit f: family f of DCT8, 16x8, 8x16, 16x16, 32x16, 16x32, 32x32). */
+  const uint8_t* proposals;
+  const float* proposal_mass;
+  const float* proposal_log_scale;
+  const uint8_t* tile_family_masks;
   const int32_t* raw_quant_field;   /* blocks */
   const int8_t* y_to_x;             /* tiles, final CfL map */
   const int8_t* y_to_b;

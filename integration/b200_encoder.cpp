@@ -498,13 +498,17 @@ struct SessionOwner {
 };
 
 Status CreateSession(size_t width, size_t height, float target, int effort, int precision,
-                     SessionOwner* owner) {
+                     SessionOwner* owner, const float* proposal_weights = nullptr,
+                     int learned_iterations = 0, float proposal_confidence = 0.6f) {
   gjxl_b200_options session_options;
   gjxl_b200_default_options(&session_options);
   session_options.butteraugli_target = target;
   session_options.effort = effort;
   session_options.tokenize = 0;  // the serializer asks for its own map's tokens
   session_options.precision = precision;
+  session_options.proposal_weights = proposal_weights;
+  session_options.learned_iterations = learned_iterations;
+  session_options.proposal_confidence = proposal_confidence;
   return FromB200(gjxl_b200_session_create(width, height, &session_options, &owner->session),
                   "session_create");
 }
@@ -541,6 +545,40 @@ GJXL_INTEGRATION_API int gjxl_b200_encode_image(const uint8_t* pixels, size_t wi
   if (!status.ok()) return Fail(status);
   *size = bytes.size();
   if (score != nullptr) *score = summary.score_history.back();
+  if (bytes.size() > capacity) {
+    g_last_error = "codestream capacity exceeded";
+    return -2;
+  }
+  std::memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}
+
+// The same with the learned analysis mode (gjxl_b200_options.proposal_weights:
+// device pointer to the proposal network's parameters; NULL for the plain
+// method). Also writes the final evaluation's FP64 Butteraugli 3-norm.
+GJXL_INTEGRATION_API int gjxl_b200_encode_image_learned(
+  const uint8_t* pixels, size_t width, size_t height, size_t row_stride, int channels,
+  float butteraugli_target, int effort, int precision, const float* proposal_weights,
+  int learned_iterations, float proposal_confidence, uint8_t* out, size_t capacity, size_t* size,
+  double* score, double* pnorm) {
+  g_last_error.clear();
+  SessionOwner owner;
+  Status status = CreateSession(width, height, butteraugli_target, effort, precision, &owner,
+                                proposal_weights, learned_iterations, proposal_confidence);
+  if (!status.ok()) return Fail(status);
+  std::vector<uint8_t> bytes;
+  VarDctEncodingSummary summary;
+  status = EncodeWithSession(owner.session, pixels, width, height, row_stride, channels,
+                             butteraugli_target, effort, false, &bytes, &summary);
+  if (!status.ok()) return Fail(status);
+  *size = bytes.size();
+  if (score != nullptr) *score = summary.score_history.back();
+  if (pnorm != nullptr) {
+    gjxl_b200_outputs o;
+    status = FromB200(gjxl_b200_session_outputs(owner.session, &o), "session_outputs");
+    if (!status.ok()) return Fail(status);
+    *pnorm = o.host_pnorm_history[o.iterations];
+  }
   if (bytes.size() > capacity) {
     g_last_error = "codestream capacity exceeded";
     return -2;
