@@ -587,6 +587,80 @@ def batched_leg(images: "BatchImages", precision: int) -> dict:
                       "service = an image's own analysis, ready = batch arrival to its end"}
 
 
+def learned_leg(images: "BatchImages | None", precision: int, steps: int, warmup: int) -> dict:
+    """The learned form (the committed proposal network, one field update):
+    the 12 MP workload's MP/s with 3 sessions in flight, as the plain line
+    is timed; the 64-image batch through the batched analysis; and the
+    BD-rate against the plain method on 3 held-out 1024x1024 images of the
+    proposal network's configuration (seeds 5001000 + i, never trained on)
+    at distances 0.5, 1, 2, 3, through the reference's unchanged serializer."""
+    import torch
+    from gjxl_b200 import learned
+    from gjxl_b200.session import AnalysisSession
+    net = learned.ProposalNetwork.load()
+    w = net.params.data_ptr()
+    img = make_image()
+    d_img = torch.from_numpy(img.reshape(HEIGHT, -1)).cuda()
+    row = WIDTH * 3
+    sessions = [AnalysisSession(WIDTH, HEIGHT, butteraugli_target=1.0, effort=7,
+                                precision=precision, proposal_weights=w, learned_iterations=1)
+                for _ in range(3)]
+    side = [torch.cuda.Stream() for _ in sessions]
+    main = torch.cuda.current_stream()
+    for s, st in zip(sessions, side):
+        for _ in range(warmup):
+            s.analyze(d_img.data_ptr(), row, 3, st.cuda_stream)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(main)
+    for st in side:
+        st.wait_event(start)
+    for i in range(steps):
+        sessions[i % 3].analyze(d_img.data_ptr(), row, 3, side[i % 3].cuda_stream)
+    for st in side:
+        done = torch.cuda.Event()
+        done.record(st)
+        main.wait_event(done)
+    stop.record(main)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / steps
+    o = sessions[0].outputs
+    masks = learned.device_array(o.tile_family_masks, (o.tiles_y, o.tiles_x), np.uint8)
+    masks = masks.cpu().numpy()
+    kept = float(np.unpackbits(masks[..., None], axis=-1)[..., 1:].sum(-1).mean() / 7.0)
+    for s in sessions:
+        s.close()
+    out = {"iterations": 1, "value_12mp": round(WIDTH * HEIGHT / 1e6 / (ms / 1e3), 3),
+           "ms_per_step_12mp": round(ms, 4), "families_kept": round(kept, 4),
+           "fallback_tiles": round(float((masks == 0x7F).mean()), 4)}
+    if images is not None:
+        from gjxl_b200.batch import BatchAnalyzer
+        imgs = images.get() if not hasattr(images, "cached") else images.cached
+        images.cached = imgs
+        dev = [torch.from_numpy(a.reshape(a.shape[0], -1)).cuda() for a in imgs]
+        mp = sum(wd * ht for wd, ht, _, _ in images.specs) / 1e6
+        b = BatchAnalyzer(precision=precision, proposal_weights=w, learned_iterations=1)
+        reqs = b.requests([(d.data_ptr(), wd, ht, t)
+                           for d, (wd, ht, t, _) in zip(dev, images.specs)])
+        lanes, _ = b.autotune(reqs, lane_counts=(2, 4, 8))
+        runs = [b.analyze(reqs) for _ in range(3)]
+        results, bms = min(runs, key=lambda r: r[1])
+        assert all(r["status"] == 0 for r in results)
+        out["batched"] = {"value": round(mp / (bms / 1e3), 3), "batch_ms": round(bms, 3),
+                          "lanes": lanes}
+        b.close()
+        del dev
+    from gjxl_b200.synthetic import generate_srgb8, workload_seed
+    held = [generate_srgb8(1024, 1024, workload_seed(5, 1000 + i)) for i in range(3)]
+    ev = learned.evaluate(learned.WEIGHTS_PATH, held, learned_iterations=1)
+    out["bd_rate_max"] = round(ev["bd_rate_mean"], 5)
+    out["bd_rate_pnorm"] = round(ev["bd_rate_pnorm_mean"], 5)
+    out["bd_rate_images"] = "3 held-out 1024x1024 images, distances 0.5/1/2/3, plain vs learned"
+    out["analysis_speedup_1mp"] = round(ev["speedup_mean"], 3)
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -601,6 +675,8 @@ def main():
                         help="WxH of a smaller image of the same generator (profiling only)")
     parser.add_argument("--no-reference-gpu", action="store_true",
                         help="skip timing the reference's own CUDA path")
+    parser.add_argument("--no-learned", action="store_true",
+                        help="skip the learned-form leg")
     parser.add_argument("--no-batched", action="store_true",
                         help="skip the batched-form leg (64 images of uneven sizes)")
     parser.add_argument("--precision", default="exact", choices=["exact", "fast"],
@@ -626,8 +702,20 @@ def main():
         batch_images = BatchImages()
     out = run_gpu(args)
     if out:
+        precision = 1 if args.precision == "fast" else 0
         if batch_images is not None:
-            out["batched_form"] = batched_leg(batch_images, 1 if args.precision == "fast" else 0)
+            imgs = batch_images.get()
+            batch_images.cached = imgs
+            batch_images.get = lambda: imgs
+            out["batched_form"] = batched_leg(batch_images, precision)
+        if world == 1 and not args.no_learned and not args.launch_list:
+            out["learned_form"] = learned_leg(batch_images, precision, args.steps, args.warmup)
+            base = out["batched_form"]["sequential"]["value"] if batch_images else None
+            if base and "batched" in out["learned_form"]:
+                out["learned_form"]["batched_vs_plain_sequential"] = round(
+                    out["learned_form"]["batched"]["value"] / base, 3)
+            out["learned_form"]["vs_plain_12mp"] = round(
+                out["learned_form"]["value_12mp"] / out["value"], 3)
         if pool is not None:
             out["cpu_baseline"] = cpu_baseline_leg(pool)
         if world == 1 and not args.launch_list and not args.no_reference_gpu:

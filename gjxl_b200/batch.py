@@ -42,7 +42,7 @@ class BatchAnalyzer:
     """Runs many images per call over `max_in_flight` concurrent lanes."""
 
     def __init__(self, max_in_flight: int = 0, effort: int = 7, precision: int = 0,
-                 tokenize: bool = True):
+                 tokenize: bool = True, proposal_weights: int = 0, learned_iterations: int = 1):
         _bind_session()
         lib = _lib.load()
         opts = Options()
@@ -50,6 +50,8 @@ class BatchAnalyzer:
         opts.effort = effort
         opts.precision = precision
         opts.tokenize = int(tokenize)
+        opts.proposal_weights = proposal_weights or None
+        opts.learned_iterations = learned_iterations
         handle = c_void_p()
         _check(lib.gjxl_b200_batch_create(max_in_flight, ctypes.byref(opts), ctypes.byref(handle)),
                "gjxl_b200_batch_create")

@@ -726,7 +726,7 @@ extern "C" void gjxl_b200_default_options(gjxl_b200_options* options) {
   options->order_mode = -1;
   options->precision = GJXL_B200_PRECISION_EXACT;
   options->proposal_weights = nullptr;
-  options->learned_iterations = 0;
+  options->learned_iterations = 1;
   options->proposal_confidence = 0.6f;
 }
 

@@ -94,7 +94,7 @@ class AnalysisSession:
     def __init__(self, width: int, height: int, butteraugli_target: float = 1.0,
                  effort: int = 7, intensity_target: float = 255.0, profile_stages: bool = False,
                  tokenize: bool = True, order_mode: int = -1, precision: int = 0,
-                 proposal_weights: int = 0, learned_iterations: int = 0,
+                 proposal_weights: int = 0, learned_iterations: int = 1,
                  proposal_confidence: float = 0.6):
         _bind()
         lib = _lib.load()

@@ -430,7 +430,8 @@ typedef struct gjxl_b200_options {
    * proposals, the greedy merge considers only the proposed families (and
    * DCT8); other tiles keep the full search. The refinement starts from the
    * adjusted field scaled by the predicted factor and runs
-   * learned_iterations field updates (default 0) instead of the effort's. */
+   * learned_iterations field updates (default 1; -1: the effort's) instead
+   * of the effort's. */
   const float* proposal_weights;
   int learned_iterations;
   float proposal_confidence;
