@@ -35,7 +35,7 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_cnn_workspace_bytes": [I],
     "gjxl_b200_cnn_train_scratch_bytes": [I],
     "gjxl_b200_cnn_gather": [P, Z, Z, Z, Z, P, I, F, P, P],
-    "gjxl_b200_cnn_forward": [P, I, P, P, P],
+    "gjxl_b200_cnn_forward": [P, I, P, P, I, P],
     "gjxl_b200_cnn_train_step": [P, I, P, P, P, P, F, P, P, P, P],
     "gjxl_b200_cnn_adamw": [P, P, P, P, I, F, F, F, F, F, P],
     "gjxl_b200_session_device_bytes": [Z, Z, P, P],

@@ -29,12 +29,14 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
 #include "cnn.h"
 #include "common.cuh"
 #include "host_util.h"
+#include "umma.cuh"
 
 namespace gjxl_b200 {
 namespace {
@@ -150,6 +152,152 @@ ConvForwardKernel(const __nv_bfloat16* in, const float* params, int layer, int n
   uint4* dst = reinterpret_cast<uint4*>(out + pixel * kCnnC);
 #pragma unroll
   for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
+}
+
+// The same convolution as implicit GEMMs on the fifth-generation tensor
+// cores, for inference: rows are output pixels (M = 128 per MMA tile), K the
+// 3x3 x Cin patch (tap-major, padded to a multiple of 16), N the 32 output
+// channels. Each thread gathers its row's patch from the NHWC input into the
+// canonical no-swizzle K-major layout in shared memory (16-byte pieces: one
+// pixel's 8 channels, or two taps of the 4-channel input); one thread issues
+// the K / 16 MMAs into a 32-column tensor-memory accumulator; each thread
+// reads its row back (tcgen05.ld), adds the bias, applies the ReLU and
+// stores 64 bytes of BF16. Persistent CTAs walk the M tiles. The products
+// are the SIMT kernel's (BF16 x BF16); only the FP32 summation order differs.
+constexpr int kConvTcThreads = 128;
+constexpr uint32_t kConvWaitPolls = 1u << 22;
+
+template <int CIN>
+struct ConvTcShape {
+  static constexpr int K = 9 * CIN;
+  static constexpr int KP = (K + 15) / 16 * 16;  // 48 or 288
+  static constexpr int kABytes = 128 * KP * 2;
+  static constexpr int kBBytes = kCnnC * KP * 2;
+  static constexpr size_t kSmem = static_cast<size_t>(kABytes) + kBBytes;
+};
+
+template <int KP>
+__device__ __forceinline__ int KMajor(int row, int k) {
+  return (row >> 3) * (KP / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+template <int CIN>
+__global__ void __launch_bounds__(kConvTcThreads)
+ConvTcKernel(const __nv_bfloat16* in, const float* params, int layer, int n, __nv_bfloat16* out,
+             uint32_t* error) {
+  using T = ConvTcShape<CIN>;
+  constexpr int KP = T::KP;
+  const LayerShape L = Layer(layer);
+  extern __shared__ __align__(128) unsigned char conv_smem[];
+  unsigned char* a_tile = conv_smem;
+  unsigned char* b_tile = conv_smem + T::kABytes;
+  __shared__ __align__(8) uint64_t barrier;
+  __shared__ uint32_t tmem_slot;
+  __shared__ float bias[kCnnC];
+  __shared__ int aborted;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) umma::Allocate(&tmem_slot, 32);
+  if (tid == 0) {
+    umma::InitBarrier(&barrier, 1);
+    aborted = 0;
+  }
+  // B: the weights rounded to BF16, K-major [co][k], zero past K.
+  for (int i = tid; i < kCnnC * KP; i += kConvTcThreads) {
+    const int co = i / KP, k = i % KP;
+    const float wv = k < T::K ? params[L.w_offset + (co * 9 + k / CIN) * CIN + k % CIN] : 0.0f;
+    *reinterpret_cast<__nv_bfloat16*>(b_tile + KMajor<KP>(co, k)) = __float2bfloat16_rn(wv);
+  }
+  if (tid < kCnnC) bias[tid] = params[L.b_offset + tid];
+  umma::FenceAsyncShared();
+  umma::FenceBeforeSync();
+  __syncthreads();
+  umma::FenceAfterSync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+  const uint32_t a_address = umma::SmemAddress(a_tile), b_address = umma::SmemAddress(b_tile);
+  constexpr uint32_t kInstr = umma::InstrBf16F32(128, kCnnC, false, false);
+  const size_t per_tile = static_cast<size_t>(L.out_size) * L.out_size;
+  const size_t total = static_cast<size_t>(n) * per_tile;
+  const size_t m_tiles = (total + 127) / 128;
+  uint32_t phase = 0;
+  for (size_t mt = blockIdx.x; mt < m_tiles; mt += gridDim.x) {
+    const size_t m = mt * 128 + tid;
+    if (m < total) {
+      const size_t t = m / per_tile;
+      const int oy = static_cast<int>(m % per_tile) / L.out_size;
+      const int ox = static_cast<int>(m % per_tile) % L.out_size;
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) {
+        const int iy = oy * L.stride + tap / 3 - 1, ix = ox * L.stride + tap % 3 - 1;
+        const bool valid = iy >= 0 && iy < L.in_size && ix >= 0 && ix < L.in_size;
+        const __nv_bfloat16* src = in + ((t * L.in_size + (valid ? iy : 0)) * L.in_size +
+                                         (valid ? ix : 0)) * CIN;
+        if constexpr (CIN == kCnnC) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const uint4 v = valid ? *reinterpret_cast<const uint4*>(src + 8 * c)
+                                  : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(a_tile + KMajor<KP>(tid, tap * CIN + 8 * c)) = v;
+          }
+        } else {
+          const uint2 v = valid ? *reinterpret_cast<const uint2*>(src) : make_uint2(0, 0);
+          *reinterpret_cast<uint2*>(a_tile + KMajor<KP>(tid, tap * CIN)) = v;
+        }
+      }
+      if constexpr (T::K < KP) {
+        // K = 36 .. 47 of the 4-channel input.
+        *reinterpret_cast<uint2*>(a_tile + KMajor<KP>(tid, T::K)) = make_uint2(0, 0);
+        for (int k = (T::K + 8) / 8 * 8; k < KP; k += 8)
+          *reinterpret_cast<uint4*>(a_tile + KMajor<KP>(tid, k)) = make_uint4(0, 0, 0, 0);
+      }
+    }
+    umma::FenceAsyncShared();
+    umma::FenceBeforeSync();
+    __syncthreads();
+    umma::FenceAfterSync();
+    if (tid == 0) {
+#pragma unroll
+      for (int kc = 0; kc < KP / 16; ++kc) {
+        const uint64_t a = umma::Descriptor(a_address + kc * 256, 128, (KP / 8) * 128);
+        const uint64_t b = umma::Descriptor(b_address + kc * 256, 128, (KP / 8) * 128);
+        umma::Mma(tmem, a, b, kInstr, kc > 0);
+      }
+      umma::Commit(&barrier);
+    }
+    const bool ok = umma::WaitParity(&barrier, phase, kConvWaitPolls);
+    phase ^= 1u;
+    umma::FenceAfterSync();
+    if (!__syncthreads_and(ok ? 1 : 0)) {
+      if (tid == 0) {
+        aborted = 1;
+        RaiseError(error, kErrorInternal);
+      }
+      break;
+    }
+    float acc[kCnnC];
+    umma::Load<32>(lane_base, acc);
+    if (m < total) {
+      __align__(16) __nv_bfloat16 o[kCnnC];
+#pragma unroll
+      for (int co = 0; co < kCnnC; ++co)
+        o[co] = __float2bfloat16_rn(fmaxf(acc[co] + bias[co], 0.0f));
+      uint4* dst = reinterpret_cast<uint4*>(out + m * kCnnC);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
+    }
+    // The next tile's gather and MMA overwrite the operand and accumulator.
+    umma::FenceBeforeSync();
+    __syncthreads();
+    umma::FenceAfterSync();
+  }
+  // A CTA that gave up waits once more (bounded) for the tensor core to
+  // finish with its tensor memory before releasing it.
+  __syncthreads();
+  if (aborted) umma::WaitParity(&barrier, phase ^ 1u, kConvWaitPolls);
+  umma::FenceBeforeSync();
+  __syncthreads();
+  umma::FenceAfterSync();
+  if (warp == 0) umma::Deallocate(tmem, 32);
 }
 
 // Head: 28 outputs per centre cell (FP32).
@@ -501,7 +649,49 @@ int CnnGather(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t
   return CheckLaunch("cnn gather");
 }
 
-int CnnForward(const float* params, const CnnActivations& a, int n, cudaStream_t stream) {
+template <int CIN>
+int LaunchConvTc(const CnnActivations& a, const float* params, int layer, int n, uint32_t* error,
+                 cudaStream_t stream) {
+  using T = ConvTcShape<CIN>;
+  int status = CheckCuda(cudaFuncSetAttribute(ConvTcKernel<CIN>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(T::kSmem)),
+                         "cnn tensor-core smem attribute");
+  if (status != GJXL_B200_OK) return status;
+  const LayerShape L = Layer(layer);
+  const size_t tiles = (static_cast<size_t>(n) * L.out_size * L.out_size + 127) / 128;
+  // As many CTAs as fit on the device at once (shared memory with the static
+  // part and the runtime's 1 KB per CTA, threads, and 16 x 32 tensor-memory
+  // columns per SM), each walking M tiles.
+  int device = 0, sms = 148, smem_per_sm = 232448;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+  cudaFuncAttributes attributes;
+  status = CheckCuda(cudaFuncGetAttributes(&attributes, ConvTcKernel<CIN>),
+                     "cnn tensor-core attributes");
+  if (status != GJXL_B200_OK) return status;
+  const int per_cta = static_cast<int>(T::kSmem + attributes.sharedSizeBytes) + 1024;
+  const int per_sm = std::max(1, std::min({smem_per_sm / per_cta, 2048 / kConvTcThreads, 16}));
+  const unsigned grid =
+    static_cast<unsigned>(std::min<size_t>(tiles, static_cast<size_t>(sms) * per_sm));
+  ConvTcKernel<CIN><<<grid, kConvTcThreads, T::kSmem, stream>>>(a.act[layer], params, layer, n,
+                                                                a.act[layer + 1], error);
+  return CheckLaunch("cnn tensor-core convolution");
+}
+
+int CnnForward(const float* params, const CnnActivations& a, int n, cudaStream_t stream,
+               bool tensor_cores, uint32_t* error) {
+  if (tensor_cores) {
+    int status = LaunchConvTc<kCnnInChannels>(a, params, 0, n, error, stream);
+    for (int l = 1; l < 4 && status == GJXL_B200_OK; ++l)
+      status = LaunchConvTc<kCnnC>(a, params, l, n, error, stream);
+    if (status != GJXL_B200_OK) return status;
+    const size_t cells = static_cast<size_t>(n) * 64;
+    HeadForwardKernel<<<static_cast<unsigned>((cells + 127) / 128), 128, 0, stream>>>(
+      a.act[4], params, n, a.head);
+    return CheckLaunch("cnn forward");
+  }
   for (int l = 0; l < 4; ++l) {
     const LayerShape L = Layer(l);
     const size_t pixels = static_cast<size_t>(n) * L.out_size * L.out_size;
@@ -640,14 +830,14 @@ extern "C" int gjxl_b200_cnn_gather(const float* opsin, size_t opsin_stride,
 }
 
 extern "C" int gjxl_b200_cnn_forward(const float* params, int tiles, void* workspace,
-                                     float* head_out, void* stream) {
+                                     float* head_out, int tensor_cores, void* stream) {
   ClearLastError();
   if (params == nullptr || workspace == nullptr || tiles <= 0) {
     return SetError(GJXL_B200_INVALID_ARGUMENT, "cnn_forward: invalid arguments");
   }
   const CnnActivations a = CnnLayout(workspace, tiles);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int status = CnnForward(params, a, tiles, s);
+  int status = CnnForward(params, a, tiles, s, tensor_cores != 0, nullptr);
   if (status == GJXL_B200_OK && head_out != nullptr) {
     status = CheckCuda(cudaMemcpyAsync(head_out, a.head,
                                        static_cast<size_t>(tiles) * 64 * kCnnHead * 4,

@@ -40,7 +40,10 @@ CnnActivations CnnLayout(void* workspace, int tiles);
 int CnnGather(const float* opsin, size_t stride, size_t pitch, size_t pw, size_t ph,
               const int* tile_list, int n, float distance, __nv_bfloat16* out,
               cudaStream_t stream);
-int CnnForward(const float* params, const CnnActivations& a, int n, cudaStream_t stream);
+// tensor_cores: the convolutions as tcgen05 implicit GEMMs (inference);
+// otherwise the SIMT kernels the training step's backward pass pairs with.
+int CnnForward(const float* params, const CnnActivations& a, int n, cudaStream_t stream,
+               bool tensor_cores = false, uint32_t* error = nullptr);
 int CnnPropose(const float* head, int n, size_t blocks_x, size_t blocks_y, uint8_t* proposals,
                float* confidence, float* log_scale, cudaStream_t stream);
 size_t CnnTrainScratchBytes(int tiles);

@@ -566,7 +566,7 @@ int Run(Session* s, const uint8_t* pixels, size_t row_stride, int channels,
     const CnnActivations a = CnnLayout(s->cnn_workspace, tiles);
     GJXL_TRY(CnnGather(s->pre, s->pw, s->pitch, s->pw, s->ph, nullptr, tiles, target, a.act[0],
                        stream));
-    GJXL_TRY(CnnForward(s->options.proposal_weights, a, tiles, stream));
+    GJXL_TRY(CnnForward(s->options.proposal_weights, a, tiles, stream, true, s->error));
     GJXL_TRY(CnnPropose(a.head, tiles, s->bx, s->by, s->proposals, s->proposal_mass,
                         s->log_scale, stream));
     GJXL_TRY(CnnTileMasks(s->proposals, s->proposal_mass, s->bx, s->by,

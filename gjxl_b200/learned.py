@@ -108,18 +108,19 @@ class ProposalNetwork:
         _lib.call("gjxl_b200_cnn_gather", opsin_ptr, stride, pitch, pw, ph, None, tiles,
                   distance, self.workspace.data_ptr(), _stream())
 
-    def forward(self, tiles: int) -> torch.Tensor:
-        """Head outputs [tiles, 64, 28] of the inputs in the workspace."""
+    def forward(self, tiles: int, tensor_cores: bool = False) -> torch.Tensor:
+        """Head outputs [tiles, 64, 28] of the inputs in the workspace (SIMT
+        convolutions, or the tensor-core ones the learned analysis runs)."""
         head = torch.empty((tiles, 64, 28), dtype=torch.float32, device="cuda")
         _lib.call("gjxl_b200_cnn_forward", self.params.data_ptr(), tiles,
-                  self.workspace.data_ptr(), head.data_ptr(), _stream())
+                  self.workspace.data_ptr(), head.data_ptr(), int(tensor_cores), _stream())
         return head
 
     def train_step(self, tiles: int, labels: torch.Tensor, targets: torch.Tensor,
                    weights: torch.Tensor, lr: float, weight_decay: float = 1e-4) -> torch.Tensor:
         """Forward, loss, backward and one AdamW step on the workspace's inputs."""
         _lib.call("gjxl_b200_cnn_forward", self.params.data_ptr(), tiles,
-                  self.workspace.data_ptr(), None, _stream())
+                  self.workspace.data_ptr(), None, 0, _stream())
         _lib.call("gjxl_b200_cnn_train_step", self.params.data_ptr(), tiles,
                   self.workspace.data_ptr(), labels.data_ptr(), targets.data_ptr(),
                   weights.data_ptr(), QF_WEIGHT, self.grads.data_ptr(),

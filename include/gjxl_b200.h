@@ -183,8 +183,10 @@ GJXL_B200_API int gjxl_b200_cnn_gather(const float* opsin, size_t opsin_stride,
                                        size_t opsin_plane_pitch, size_t padded_width,
                                        size_t padded_height, const int* tile_list, int tiles,
                                        float distance, void* workspace, void* stream);
+/* tensor_cores != 0: the convolutions as tcgen05 implicit GEMMs (what the
+ * learned analysis runs); 0: the SIMT kernels the training step pairs with. */
 GJXL_B200_API int gjxl_b200_cnn_forward(const float* params, int tiles, void* workspace,
-                                        float* head_out, void* stream);
+                                        float* head_out, int tensor_cores, void* stream);
 GJXL_B200_API int gjxl_b200_cnn_train_step(const float* params, int tiles, void* workspace,
                                            const uint8_t* labels, const float* targets,
                                            const float* weights, float qf_weight,

@@ -46,12 +46,16 @@ def params(seed: int) -> np.ndarray:
     return flat
 
 
-def test_forward_matches_oracle(cuda):
-    x0, *_ = random_batch(6, 1)
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_forward_matches_oracle(cuda, tensor_cores):
+    """SIMT and tcgen05 convolutions against the oracle (the tensor-core form
+    over 70 tiles, several M tiles of every layer)."""
+    n = 70 if tensor_cores else 6
+    x0, *_ = random_batch(n, 1)
     flat = params(1)
     net = ProposalNetwork(flat)
     load_batch(net, x0)
-    got = host(net.forward(6))
+    got = host(net.forward(n, tensor_cores=tensor_cores))
     want = cnn_ref.forward(flat, x0)["head"]
     # FP32 sums in different orders can move a BF16-rounded activation by one
     # BF16 step; the head agrees to a small fraction of its scale.
