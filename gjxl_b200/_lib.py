@@ -30,6 +30,8 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_gaborish_inverse": [P, Z, Z, P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_initial_cfl": [P, Z, Z, Z, Z, P, P, P],
     "gjxl_b200_dc_token_sizes": [Z, Z, P, P, P, P],
+    "gjxl_b200_ac_strategy_candidate_costs": [I, P, Z, Z, P, Z, Z, Z, P, Z, P, P, P, P, F, I, P, P,
+                                              P],
     "gjxl_b200_batch_create": [I, P, P],
     "gjxl_b200_cnn_param_count": [],
     "gjxl_b200_cnn_workspace_bytes": [I],

@@ -60,6 +60,13 @@ __host__ __device__ constexpr int FamilyOfStrategy(int s) {
        : s == kDct32x16 ? 4 : s == kDct16x32 ? 5 : s == kDct32x32 ? 6 : -1;
 }
 
+// One candidate of a same-strategy batch, AcStrategyCandidate's layout
+// (src/gpu/ops/ac_strategy.h:27-42).
+struct CandidateDesc {
+  uint32_t block_x, block_y;
+  float quant_norm, entropy_multiplier, cfl_x, cfl_b;
+};
+
 struct CostParams {
   const float* opsin;  // Gaborish-inverted padded XYB
   size_t stride, pitch;
@@ -81,6 +88,14 @@ struct CostParams {
   // scored (raster indices) and their number. Null: every tile.
   const uint32_t* kept_tiles;
   const uint32_t* kept_count;
+  // Candidate-batch form: candidate i is batch[i] and its cost goes to
+  // batch_costs[i]. With batch_resident, the quant norm and CfL factors come
+  // from quant_field / y_to_x / y_to_b as in the tile enumeration; otherwise
+  // from the descriptor. A descriptor whose footprint leaves the image gets
+  // a NaN cost.
+  const CandidateDesc* batch;
+  float* batch_costs;
+  int batch_resident;
 };
 
 // Candidates scored: every tile's, or those of the kept tiles.
@@ -212,6 +227,29 @@ __device__ __forceinline__ CandidateInputs<CW, CH> FetchCandidate(const CostPara
                                                                  uint32_t cand,
                                                                  uint32_t candidate_count) {
   CandidateInputs<CW, CH> in;
+  if (p.batch != nullptr) {
+    // Candidate-batch form (the anchor only; quant norm and CfL below).
+    if (cand < candidate_count) {
+      const CandidateDesc d = p.batch[cand];
+      if (d.block_x + CW <= p.blocks_x && d.block_y + CH <= p.blocks_y) {
+        in.ax = static_cast<int>(d.block_x);
+        in.ay = static_cast<int>(d.block_y);
+      }
+    }
+    if (in.ax >= 0 && p.batch_resident) {
+#pragma unroll
+      for (int dy = 0; dy < CH; ++dy) {
+#pragma unroll
+        for (int dx = 0; dx < CW; ++dx) {
+          in.q[dy * CW + dx] = __ldg(p.quant_field + (in.ay + dy) * p.blocks_x + in.ax + dx);
+        }
+      }
+      const int tile_index = (in.ay / 8) * p.tiles_x + (in.ax / 8);
+      in.y_to_x = p.y_to_x[tile_index];
+      in.y_to_b = p.y_to_b[tile_index];
+    }
+    return in;
+  }
   if (cand < candidate_count) {
     const uint32_t per_tile = p.local_x * p.local_y;
     const uint32_t tile = CandidateTile(p, cand / per_tile), local = cand % per_tile;
@@ -265,7 +303,8 @@ __device__ __forceinline__ float QuantNormOf(const float (&q)[CW * CH]) {
 template <int N, int kBlocks, bool kExactRoot = true>
 __device__ __forceinline__ float CandidateCost(const CostParams& p, const float (&magnitude)[3],
                                                const uint32_t (&nonzero)[3],
-                                               const float (&loss_sum)[3], float quant_norm) {
+                                               const float (&loss_sum)[3], float quant_norm,
+                                               float entropy_multiplier) {
   const float kChannelMultiplier[3] = {2.0441408586549744e7f, 1.0f, 1.266770081387616f};
   float entropy = 0.0f, loss = 0.0f;
   for (int c = 0; c < 3; ++c) {
@@ -286,7 +325,7 @@ __device__ __forceinline__ float CandidateCost(const CostParams& p, const float 
     kExactRoot ? static_cast<float>(pow(static_cast<double>(normalized_loss), 0.125))
                : (normalized_loss > 0.0f ? exp2f(log2f(normalized_loss) * 0.125f) : 0.0f);
   const float loss_cost = root * static_cast<float>(N) / quant_norm;
-  return entropy * p.entropy_multiplier + p.info_loss_multiplier * loss_cost;
+  return entropy * entropy_multiplier + p.info_loss_multiplier * loss_cost;
 }
 
 // Acc = double: the bit-exact restatement (FP64 products, separately
@@ -316,12 +355,27 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   const int tid = threadIdx.x;
   // Anchors first (integer arithmetic only), so that the pixel loads can
   // start before the quant norms and CfL factors arrive.
+  __shared__ float entropy[K];
+  __shared__ int invalid[K];
   candidate_count = ScoredCandidates(p, candidate_count);
   if (blockIdx.x * K >= candidate_count) return;  // past the kept tiles' candidates
   if (tid < K) {
     const uint32_t cand = blockIdx.x * K + tid;
     int ax = -1, ay = -1;
-    if (cand < candidate_count) {
+    entropy[tid] = p.entropy_multiplier;
+    invalid[tid] = 0;
+    if (p.batch != nullptr) {
+      if (cand < candidate_count) {
+        const CandidateDesc d = p.batch[cand];
+        entropy[tid] = d.entropy_multiplier;
+        if (d.block_x + S::CW <= p.blocks_x && d.block_y + S::CH <= p.blocks_y) {
+          ax = static_cast<int>(d.block_x);
+          ay = static_cast<int>(d.block_y);
+        } else {
+          invalid[tid] = 1;
+        }
+      }
+    } else if (cand < candidate_count) {
       const uint32_t per_tile = p.local_x * p.local_y;
       const uint32_t tile = CandidateTile(p, cand / per_tile), local = cand % per_tile;
       const int tx = tile % p.tiles_x, ty = tile / p.tiles_x;
@@ -367,7 +421,13 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     }
     // ComputeQuantNormUnchecked (ac_strategy.cpp:103-130) and the CfL
     // factors, while the loads above are in flight.
-    if (tid < K && anchor_x[tid] >= 0) {
+    if (tid < K && anchor_x[tid] >= 0 && p.batch != nullptr && !p.batch_resident) {
+      const CandidateDesc d = p.batch[blockIdx.x * K + tid];
+      quant_norm[tid] = d.quant_norm;
+      cfl[tid][0] = d.cfl_x;
+      cfl[tid][1] = 0.0f;
+      cfl[tid][2] = d.cfl_b;
+    } else if (tid < K && anchor_x[tid] >= 0) {
       const int ax = anchor_x[tid], ay = anchor_y[tid];
       const float qn = QuantNorm<S::CW, S::CH>(p, ax, ay);
       if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
@@ -528,9 +588,16 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     const float mag[3] = {magnitude[tid][0], magnitude[tid][1], magnitude[tid][2]};
     const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
     const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
-    const float result = CandidateCost<N, S::CW * S::CH, kExact>(p, mag, nz, ls, quant_norm[tid]);
-    if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
-    p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+    const float result = CandidateCost<N, S::CW * S::CH, kExact>(p, mag, nz, ls, quant_norm[tid],
+                                                                  entropy[tid]);
+    if (p.batch != nullptr) {
+      p.batch_costs[blockIdx.x * K + tid] = result;
+    } else {
+      if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
+      p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+    }
+  } else if (tid < K && invalid[tid]) {
+    p.batch_costs[blockIdx.x * K + tid] = __int_as_float(0x7fc00000);
   }
 }
 
@@ -690,6 +757,8 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
   __shared__ float quant_norm[G], cfl[G][3];
   __shared__ float magnitude[G][3], loss_sum[G][3];
   __shared__ uint32_t nonzero[G][3];
+  __shared__ float entropy[G];
+  __shared__ int invalid[G];
   __shared__ int aborted;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -755,7 +824,20 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
       anchor_x[tid] = in.ax;
       anchor_y[tid] = in.ay;
       float qn = 1.0f;
-      if (in.ax >= 0) {
+      entropy[tid] = p.entropy_multiplier;
+      invalid[tid] = 0;
+      if (p.batch != nullptr && unit * G + tid < candidate_count) {
+        const CandidateDesc d = p.batch[unit * G + tid];
+        entropy[tid] = d.entropy_multiplier;
+        invalid[tid] = in.ax < 0 ? 1 : 0;
+        if (in.ax >= 0 && !p.batch_resident) {
+          qn = d.quant_norm;
+          cfl[tid][0] = d.cfl_x;
+          cfl[tid][1] = 0.0f;
+          cfl[tid][2] = d.cfl_b;
+        }
+      }
+      if (in.ax >= 0 && !(p.batch != nullptr && !p.batch_resident)) {
         qn = QuantNormOf<S::CW, S::CH>(in.q);
         if (!(IsFinite(qn) && qn > 0.0f)) RaiseError(p.error, kErrorNonFiniteInput);
         // ColorCorrelationMap::AcFactors (chroma_from_luma.cpp:412-432).
@@ -959,9 +1041,15 @@ CandidateCostTcKernel(const __grid_constant__ CostParams p, uint32_t candidate_c
       const uint32_t nz[3] = {nonzero[tid][0], nonzero[tid][1], nonzero[tid][2]};
       const float ls[3] = {loss_sum[tid][0], loss_sum[tid][1], loss_sum[tid][2]};
       const float result =
-        CandidateCost<N, S::CW * S::CH, false>(p, mag, nz, ls, quant_norm[tid]);
-      if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
-      p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+        CandidateCost<N, S::CW * S::CH, false>(p, mag, nz, ls, quant_norm[tid], entropy[tid]);
+      if (p.batch != nullptr) {
+        p.batch_costs[unit * G + tid] = result;
+      } else {
+        if (!(IsFinite(result) && result >= 0.0f)) RaiseError(p.error, kErrorNonFiniteOutput);
+        p.costs[anchor_y[tid] * p.blocks_x + anchor_x[tid]] = result;
+      }
+    } else if (!aborted && tid < G && invalid[tid]) {
+      p.batch_costs[unit * G + tid] = __int_as_float(0x7fc00000);
     }
     __syncthreads();
   }
@@ -1197,17 +1285,23 @@ __global__ void __launch_bounds__(64) SearchTileKernel(const __grid_constant__ S
 }
 
 template <int W, int H, typename Acc = double>
-int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t stream) {
+int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t stream,
+                 uint32_t batch_count = 0) {
   using S = Shape<W, H>;
   const int table = StrategyTableFamily(kFamilyStrategy[family]);
   const HostTables& h = GetHostTables();
-  p.dequant = d.dequant + h.layout.offset[table];
-  p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  if (p.dequant == nullptr) {
+    p.dequant = d.dequant + h.layout.offset[table];
+    p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  }
   p.entropy_multiplier = kFamilyEntropy[family];
   const int cw = kFamilyCoveredW[family], ch = kFamilyCoveredH[family];
   p.local_x = (8 - cw) / p.anchor_step + 1;
   p.local_y = (8 - ch) / p.anchor_step + 1;
-  const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  const uint32_t count = p.batch != nullptr
+                           ? batch_count
+                           : static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  if (count == 0) return GJXL_B200_OK;
   const size_t smem = CostLayout<W, H, Acc>::SharedBytes;
   int status = CheckCuda(cudaFuncSetAttribute(CandidateCostKernel<W, H, Acc>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1222,17 +1316,23 @@ int LaunchFamily(CostParams p, const DeviceTables& d, int family, cudaStream_t s
 // The tensor-core form of a 16/32-sided family: persistent CTAs (as many as
 // fit on the device at once) walk the units of G candidates.
 template <int W, int H>
-int LaunchFamilyTc(CostParams p, const DeviceTables& d, int family, cudaStream_t stream) {
+int LaunchFamilyTc(CostParams p, const DeviceTables& d, int family, cudaStream_t stream,
+                   uint32_t batch_count = 0) {
   using Lay = TcLayout<W, H>;
   const int table = StrategyTableFamily(kFamilyStrategy[family]);
   const HostTables& h = GetHostTables();
-  p.dequant = d.dequant + h.layout.offset[table];
-  p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  if (p.dequant == nullptr) {
+    p.dequant = d.dequant + h.layout.offset[table];
+    p.inverse_dequant = d.inverse_dequant + h.layout.offset[table];
+  }
   p.entropy_multiplier = kFamilyEntropy[family];
   const int cw = kFamilyCoveredW[family], ch = kFamilyCoveredH[family];
   p.local_x = (8 - cw) / p.anchor_step + 1;
   p.local_y = (8 - ch) / p.anchor_step + 1;
-  const uint32_t count = static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  const uint32_t count = p.batch != nullptr
+                           ? batch_count
+                           : static_cast<uint32_t>(p.tiles_x * p.tiles_y * p.local_x * p.local_y);
+  if (count == 0) return GJXL_B200_OK;
   const size_t smem = Lay::SharedBytes;
   int status = CheckCuda(cudaFuncSetAttribute(CandidateCostTcKernel<W, H>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1430,4 +1530,80 @@ extern "C" int gjxl_b200_ac_strategy_search(
   return LaunchAcStrategySearch(costs, padded_width, padded_height, butteraugli_target,
                                 dense_dct32 != 0, cells, device_error,
                                 static_cast<cudaStream_t>(stream));
+}
+
+// Candidate-batch evaluation: GpuAcStrategyEvaluation::
+// EvaluateAcStrategyCandidateBatches (src/gpu/ops/ac_strategy.h:118-170) for
+// one same-strategy batch.
+extern "C" int gjxl_b200_ac_strategy_candidate_costs(
+  int strategy, const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+  const float* pixel_mask, size_t pixel_mask_stride, size_t padded_width, size_t padded_height,
+  const void* candidates, size_t candidate_count, const float* matrices,
+  const float* quant_field, const int8_t* y_to_x, const int8_t* y_to_b, float butteraugli_target,
+  int precision, float* costs, uint32_t* device_error, void* stream) {
+  ClearLastError();
+  int family = -1;
+  for (int f = 0; f < kFamilyCount; ++f)
+    if (kFamilyStrategy[f] == strategy) family = f;
+  if (opsin == nullptr || pixel_mask == nullptr || (candidate_count > 0 && candidates == nullptr) ||
+      (candidate_count > 0 && costs == nullptr) || padded_width % 8 || padded_height % 8 ||
+      padded_width == 0 || padded_height == 0 || opsin_stride < padded_width ||
+      opsin_plane_pitch < opsin_stride * padded_height || pixel_mask_stride < padded_width ||
+      candidate_count > (1u << 30) || !(butteraugli_target > 0.0f) ||
+      (precision != GJXL_B200_PRECISION_EXACT && precision != GJXL_B200_PRECISION_FAST) ||
+      ((quant_field == nullptr) != (y_to_x == nullptr) || (y_to_x == nullptr) != (y_to_b == nullptr)) ||
+      !Aligned16(opsin)) {
+    return SetError(GJXL_B200_INVALID_ARGUMENT, "ac_strategy_candidate_costs: invalid arguments");
+  }
+  if (family < 0) {
+    return SetError(GJXL_B200_UNSUPPORTED,
+                    "ac_strategy_candidate_costs: the 7 searched strategies are supported");
+  }
+  if (candidate_count == 0) return GJXL_B200_OK;
+  DeviceTables d;
+  int status = GetDeviceTables(&d);
+  if (status != GJXL_B200_OK) return status;
+  const size_t bx = padded_width / 8, by = padded_height / 8;
+  CostParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.opsin = opsin;
+  p.stride = opsin_stride;
+  p.pitch = opsin_plane_pitch;
+  p.quant_field = quant_field;
+  p.pixel_mask = pixel_mask;
+  p.mask_stride = pixel_mask_stride;
+  p.y_to_x = y_to_x;
+  p.y_to_b = y_to_b;
+  p.blocks_x = static_cast<uint32_t>(bx);
+  p.blocks_y = static_cast<uint32_t>(by);
+  p.tiles_x = static_cast<uint32_t>((bx + 7) / 8);
+  p.tiles_y = static_cast<uint32_t>((by + 7) / 8);
+  const float kBias = 0.13731742964354549f;
+  const float ratio = (butteraugli_target + kBias) / (1.0f + kBias);
+  p.info_loss_multiplier = 1.2f * std::pow(ratio, 0.33677806662454718f);
+  p.zeros_multiplier = 9.3089059022677905f * std::pow(ratio, 0.50990926717963703f);
+  p.cost_delta = 10.833273317067883f * std::pow(ratio, 0.36702940662370243f);
+  p.error = device_error;
+  p.anchor_step = 1;
+  p.batch = static_cast<const CandidateDesc*>(candidates);
+  p.batch_costs = costs;
+  p.batch_resident = quant_field != nullptr ? 1 : 0;
+  if (matrices != nullptr) {
+    const size_t n = static_cast<size_t>(kFamilyCoveredW[family]) * kFamilyCoveredH[family] * 64;
+    p.dequant = matrices;
+    p.inverse_dequant = matrices + 3 * n;
+  }
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t count = static_cast<uint32_t>(candidate_count);
+  const bool tensor = precision == GJXL_B200_PRECISION_FAST;
+  switch (family) {
+    case 0: status = tensor ? LaunchFamily<8, 8, float>(p, d, 0, s, count) : LaunchFamily<8, 8>(p, d, 0, s, count); break;
+    case 1: status = tensor ? LaunchFamily<8, 16, float>(p, d, 1, s, count) : LaunchFamily<8, 16>(p, d, 1, s, count); break;
+    case 2: status = tensor ? LaunchFamily<16, 8, float>(p, d, 2, s, count) : LaunchFamily<16, 8>(p, d, 2, s, count); break;
+    case 3: status = tensor ? LaunchFamilyTc<16, 16>(p, d, 3, s, count) : LaunchFamily<16, 16>(p, d, 3, s, count); break;
+    case 4: status = tensor ? LaunchFamilyTc<16, 32>(p, d, 4, s, count) : LaunchFamily<16, 32>(p, d, 4, s, count); break;
+    case 5: status = tensor ? LaunchFamilyTc<32, 16>(p, d, 5, s, count) : LaunchFamily<32, 16>(p, d, 5, s, count); break;
+    default: status = tensor ? LaunchFamilyTc<32, 32>(p, d, 6, s, count) : LaunchFamily<32, 32>(p, d, 6, s, count); break;
+  }
+  return status;
 }

@@ -279,6 +279,25 @@ GJXL_B200_API int gjxl_b200_ac_strategy_costs(
     int precision, float* costs, uint32_t* device_error, void* stream);
 
 /*
+ * Candidate-batch evaluation (the reference's GpuAcStrategyEvaluation seam,
+ * src/gpu/ops/ac_strategy.h:72-170): costs of `candidate_count` candidates of
+ * one searched strategy, each an AcStrategyCandidate descriptor (24 bytes:
+ * uint32 block_x, block_y; float quant_norm, entropy_multiplier, cfl_x,
+ * cfl_b; device memory) into `costs` (device, one float per candidate).
+ * `matrices`: the strategy's dequant X/Y/B then inverse dequant X/Y/B
+ * (device; NULL: the default tables). With `quant_field` (and both CfL maps)
+ * the quant norm and CfL factors are the device's own from the field, as in
+ * the reference's resident form; otherwise the descriptors'. A descriptor
+ * whose footprint leaves the image gets a NaN cost.
+ */
+GJXL_B200_API int gjxl_b200_ac_strategy_candidate_costs(
+    int strategy, const float* opsin, size_t opsin_stride, size_t opsin_plane_pitch,
+    const float* pixel_mask, size_t pixel_mask_stride, size_t padded_width,
+    size_t padded_height, const void* candidates, size_t candidate_count,
+    const float* matrices, const float* quant_field, const int8_t* y_to_x,
+    const int8_t* y_to_b, float butteraugli_target, int precision, float* costs,
+    uint32_t* device_error, void* stream);
+/*
  * AC-strategy search (rows a6, a7, a8): candidate costs followed by the
  * greedy hierarchical merge of every 64x64 tile on the device.
  * Replaces AcStrategySearchProvider::Find (src/codec/quantization_pipeline.h:34-50)
