@@ -1102,8 +1102,16 @@ struct ButteraugliState {
 
   bool external_arena = false;  // planes lent by the owner (not freed)
 
+  // The half-resolution scale runs on its own stream beside the full one
+  // (fork / join events; inside a captured graph they become branches).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+
   ~ButteraugliState() {
     if (arena && !external_arena) cudaFree(arena);
+    if (side) cudaStreamDestroy(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
   }
 };
 
@@ -1258,8 +1266,8 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
     s.final_map, st.error);
 }
 
-void TransformScales(ButteraugliState& st, const float* linear, size_t stride, size_t pitch,
-                     bool reference, cudaStream_t stream) {
+void TransformMain(ButteraugliState& st, const float* linear, size_t stride, size_t pitch,
+                   bool reference, cudaStream_t stream) {
   const float* main_in = linear;
   size_t main_stride = stride, main_pitch = pitch;
   if (st.expanded) {
@@ -1273,14 +1281,26 @@ void TransformScales(ButteraugliState& st, const float* linear, size_t stride, s
   Psycho(st, st.main, main_in, main_stride, main_pitch,
          reference ? st.main.ref_psycho : st.main.dist_psycho,
          reference ? nullptr : st.main.ref_psycho, stream);
-  if (st.has_sub) {
-    Subsample2xKernel<<<dim3(Blocks(st.sub.n), 3), kThreads, 0, stream>>>(
-      linear, stride, pitch, st.width, st.height, st.sub.linear_tmp, st.sub.w, st.sub.h,
-      st.sub.n);
-    Psycho(st, st.sub, st.sub.linear_tmp, st.sub.w, st.sub.n,
-           reference ? st.sub.ref_psycho : st.sub.dist_psycho,
-           reference ? nullptr : st.sub.ref_psycho, stream);
-  }
+}
+
+void TransformSub(ButteraugliState& st, const float* linear, size_t stride, size_t pitch,
+                  bool reference, cudaStream_t stream) {
+  Subsample2xKernel<<<dim3(Blocks(st.sub.n), 3), kThreads, 0, stream>>>(
+    linear, stride, pitch, st.width, st.height, st.sub.linear_tmp, st.sub.w, st.sub.h,
+    st.sub.n);
+  Psycho(st, st.sub, st.sub.linear_tmp, st.sub.w, st.sub.n,
+         reference ? st.sub.ref_psycho : st.sub.dist_psycho,
+         reference ? nullptr : st.sub.ref_psycho, stream);
+}
+
+// The side stream starts after everything queued on `stream` so far.
+void Fork(ButteraugliState& st, cudaStream_t stream) {
+  cudaEventRecord(st.fork, stream);
+  cudaStreamWaitEvent(st.side, st.fork, 0);
+}
+void Join(ButteraugliState& st, cudaStream_t stream) {
+  cudaEventRecord(st.join, st.side);
+  cudaStreamWaitEvent(stream, st.join, 0);
 }
 
 }  // namespace
@@ -1350,6 +1370,15 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, void*
   if (st->has_sub) AssignScale(st->sub, st->arena + ScaleFloats(st->main.n));
   st->maximum = st->arena + ScaleFloats(st->main.n) + ScaleFloats(st->sub.n);
   st->error = reinterpret_cast<uint32_t*>(st->maximum + 32);
+  if (CheckCuda(cudaStreamCreateWithFlags(&st->side, cudaStreamNonBlocking),
+                "butteraugli: side stream") != GJXL_B200_OK ||
+      CheckCuda(cudaEventCreateWithFlags(&st->fork, cudaEventDisableTiming),
+                "butteraugli: event") != GJXL_B200_OK ||
+      CheckCuda(cudaEventCreateWithFlags(&st->join, cudaEventDisableTiming),
+                "butteraugli: event") != GJXL_B200_OK) {
+    delete st;
+    return GJXL_B200_OUT_OF_MEMORY;
+  }
   st->k_opsin = MakeKernel(kOpsinSigma);
   st->k_low = MakeKernel(kLowSigma);
   st->k_high = MakeKernel(kHighSigma);
@@ -1362,7 +1391,12 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, void*
 int ButteraugliPrepare(ButteraugliState* st, const float* linear, size_t stride, size_t pitch,
                        cudaStream_t stream) {
   cudaMemsetAsync(st->error, 0, sizeof(uint32_t), stream);
-  TransformScales(*st, linear, stride, pitch, true, stream);
+  if (st->has_sub) {
+    Fork(*st, stream);
+    TransformSub(*st, linear, stride, pitch, true, st->side);
+  }
+  TransformMain(*st, linear, stride, pitch, true, stream);
+  if (st->has_sub) Join(*st, stream);
   st->prepared = true;
   st->reference_mask_ready = false;
   return CheckLaunch("butteraugli prepare");
@@ -1373,12 +1407,17 @@ int ButteraugliCompare(ButteraugliState* st, const float* linear, size_t stride,
   if (!st->prepared) {
     return SetError(GJXL_B200_FAILED_PRECONDITION, "butteraugli: reference not prepared");
   }
-  TransformScales(*st, linear, stride, pitch, false, stream);
   // The reference's mask planes depend only on the reference image; the
   // first comparison after a prepare computes them, later ones reuse them.
   const bool reference_side = !st->reference_mask_ready;
+  if (st->has_sub) {
+    Fork(*st, stream);
+    TransformSub(*st, linear, stride, pitch, false, st->side);
+    Differences(*st, st->sub, reference_side, st->side);
+  }
+  TransformMain(*st, linear, stride, pitch, false, stream);
   Differences(*st, st->main, reference_side, stream);
-  if (st->has_sub) Differences(*st, st->sub, reference_side, stream);
+  if (st->has_sub) Join(*st, stream);
   st->reference_mask_ready = true;
   cudaMemsetAsync(st->maximum, 0, sizeof(float), stream);
   const size_t n = static_cast<size_t>(st->width) * st->height;
