@@ -19,9 +19,12 @@
 // the second pass reads columns directly (same per-output arithmetic, no
 // transposed copy). Planes are dense float32 (stride = width).
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -591,6 +594,8 @@ struct MaltaParams {
   int w, h;
   int tiles_x, tiles_y;  // output tiles of kMaltaTileW x kMaltaTileH
   int first;             // first stage of its channel: the plane starts at zero
+  int tma;               // the window arrives by a tiled bulk tensor copy of `map`
+  uint32_t* error;
 };
 
 __device__ __forceinline__ float Sum4(float a, float b, float c, float d) { return (a + b) + (c + d); }
@@ -687,14 +692,34 @@ __device__ __forceinline__ float MaltaUnit(const float (&v)[2 * kMaltaHalo + 1][
 
 // Scaled differences of the tile in shared memory, then the Malta line sums
 // of four outputs per thread, added onto the accumulator.
+// Polls the mbarrier at shared address `bar` until the phase of parity
+// `parity` has completed, at most 2^22 times; false when it gave up.
+__device__ __forceinline__ bool WaitParity(uint32_t bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (uint32_t poll = 0; poll < (1u << 22) && !done; ++poll) {
+    asm volatile(
+      "{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  }
+  return done != 0;
+}
+
 template <bool kLowFrequency>
 __global__ void __launch_bounds__(kMaltaThreads, 3)
-MaltaKernel(const __grid_constant__ MaltaParams p) {
+MaltaKernel(const __grid_constant__ MaltaParams p, const __grid_constant__ CUtensorMap map) {
   // Two staging buffers: the CTA walks its tiles (tile index t, t + grid,
-  // ...) and copies the next tile's window in with asynchronous copies while
-  // it computes the current one.
-  __shared__ __align__(16) float tile[2][kMaltaSpanH][kMaltaSpanW];
-  // Staging, four samples per copy: x0 is a multiple of 4, so with the row
+  // ...) and copies the next tile's window in while it computes the current
+  // one. With `p.tma`, one thread asks the tensor-memory-access unit for the
+  // whole 72 x 24 window of the plane (a 2D box at the tile's origin minus
+  // the 4-pixel halo; samples outside the image arrive as zeros) and the
+  // CTA waits on the buffer's mbarrier (bounded). The box's x start is a
+  // multiple of 4 floats (16 bytes), as the copy requires.
+  __shared__ __align__(128) float tile[2][kMaltaSpanH][kMaltaSpanW];
+  __shared__ __align__(8) uint64_t full[2];
+  // Otherwise, four samples per copy: x0 is a multiple of 4, so with the row
   // length a multiple of 4 every aligned group of 4 lies wholly inside or
   // wholly outside the image, and with a 16-byte aligned plane it is 16-byte
   // aligned (outside groups are zero-filled by the copy); other planes take
@@ -702,12 +727,39 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
   // ones in the arena, so their alignment depends on the image size).
   constexpr int kQuads = kMaltaSpanW / 4 * kMaltaSpanH;
   constexpr int kStage = (kQuads + kMaltaThreads - 1) / kMaltaThreads;
+  constexpr uint32_t kBoxBytes = kMaltaSpanW * kMaltaSpanH * sizeof(float);
   static_assert(kMaltaSpanW % 4 == 0 && kMaltaHalo % 4 == 0, "aligned quads");
   const bool aligned = p.w % 4 == 0 && reinterpret_cast<uintptr_t>(p.scaled) % 16 == 0;
   const int tiles = p.tiles_x * p.tiles_y;
+  if (p.tma) {
+    if (threadIdx.x == 0) {
+      for (int b = 0; b < 2; ++b) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+          static_cast<uint32_t>(__cvta_generic_to_shared(&full[b]))));
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    __syncthreads();
+  }
   const auto stage = [&](int t, int buffer) {
     const int x0 = (t % p.tiles_x) * kMaltaTileW - kMaltaHalo;
     const int y0 = (t / p.tiles_x) * kMaltaTileH - kMaltaHalo;
+    if (p.tma) {
+      if (threadIdx.x == 0) {
+        const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&full[buffer]));
+        // The buffer was last read through the generic proxy.
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(kBoxBytes));
+        asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3}], [%4];"
+          ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(&tile[buffer][0][0]))),
+            "l"(reinterpret_cast<uint64_t>(&map)), "r"(x0), "r"(y0), "r"(bar)
+          : "memory");
+      }
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < kStage; ++j) {
       const int i = threadIdx.x + j * kMaltaThreads;
@@ -735,12 +787,28 @@ MaltaKernel(const __grid_constant__ MaltaParams p) {
     asm volatile("cp.async.commit_group;\n" ::);
   };
   int buffer = 0;
+  uint32_t phases = 0;  // bit b: parity of buffer b's next completion
   if (static_cast<int>(blockIdx.x) < tiles) stage(blockIdx.x, 0);
   for (int t = blockIdx.x; t < tiles; t += gridDim.x, buffer ^= 1) {
     // This tile's copies are done, and every thread is past the previous
     // tile's reads of the other buffer.
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
+    if (p.tma) {
+      const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&full[buffer]));
+      const bool done = WaitParity(bar, (phases >> buffer) & 1u);
+      if (!__syncthreads_and(done)) {
+        // The copy did not arrive within the bound: record it, wait once
+        // more (bounded) for it before the shared memory is released, stop.
+        if (threadIdx.x == 0) {
+          RaiseError(p.error, kErrorInternal);
+          WaitParity(bar, (phases >> buffer) & 1u);
+        }
+        break;
+      }
+      phases ^= 1u << buffer;
+    } else {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      __syncthreads();
+    }
     if (t + static_cast<int>(gridDim.x) < tiles) stage(t + gridDim.x, buffer ^ 1);
     const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
     const int ly = threadIdx.x / (kMaltaTileW / kMaltaRun);
@@ -1053,6 +1121,10 @@ struct Scale {
   float* blurred1 = nullptr;
   float* final_map = nullptr;
   float* malta = nullptr;        // 6 planes: Malta stage inputs (MaltaPlanes)
+  // Tiled bulk-copy descriptors of the six Malta input planes (72 x 24
+  // boxes), when the planes allow them (EncodeMaltaMaps).
+  bool malta_tma = false;
+  CUtensorMap malta_map[6];
 };
 
 size_t ScaleFloats(size_t n) {
@@ -1226,10 +1298,12 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
     mp.tiles_x = tiles_x;
     mp.tiles_y = tiles_y;
     mp.first = index >= 4 ? 1 : 0;
+    mp.tma = s.malta_tma ? 1 : 0;
+    mp.error = st.error;
     if (index < 4) {
-      MaltaKernel<true><<<malta_grid, kMaltaThreads, 0, stream>>>(mp);
+      MaltaKernel<true><<<malta_grid, kMaltaThreads, 0, stream>>>(mp, s.malta_map[index]);
     } else {
-      MaltaKernel<false><<<malta_grid, kMaltaThreads, 0, stream>>>(mp);
+      MaltaKernel<false><<<malta_grid, kMaltaThreads, 0, stream>>>(mp, s.malta_map[index]);
     }
   }
   // kL2Weights (:32-36).
@@ -1319,6 +1393,58 @@ ScaleExtents Extents(size_t width, size_t height) {
   return e;
 }
 
+using TensorMapEncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                             const cuuint64_t*, const cuuint64_t*,
+                                             const cuuint32_t*, const cuuint32_t*,
+                                             CUtensorMapInterleave, CUtensorMapSwizzle,
+                                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tiled tensor-map encoder, looked up once through the runtime
+// (no link against the driver library); null when the driver lacks it.
+TensorMapEncodeTiledFn TensorMapEncoder() {
+  static TensorMapEncodeTiledFn encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult found;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &found) ==
+          cudaSuccess &&
+        found == cudaDriverEntryPointSuccess) {
+      encode = reinterpret_cast<TensorMapEncodeTiledFn>(fn);
+    }
+    cudaGetLastError();
+  });
+  return encode;
+}
+
+// Describes each Malta input plane of `s` as a 2D FP32 tensor (w x h, rows
+// w floats apart) read in 72 x 24 boxes with zero fill outside it. The
+// copies need a 16-byte aligned plane and a row pitch of a multiple of 16
+// bytes; other scales keep the per-thread staging.
+void EncodeMaltaMaps(Scale& s) {
+  s.malta_tma = false;
+  std::memset(s.malta_map, 0, sizeof(s.malta_map));
+  const TensorMapEncodeTiledFn encode = TensorMapEncoder();
+  if (encode == nullptr || s.malta == nullptr || s.w % 4 != 0 ||
+      reinterpret_cast<uintptr_t>(s.malta) % 16 != 0 || (s.n * sizeof(float)) % 16 != 0) {
+    return;
+  }
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(s.w), static_cast<cuuint64_t>(s.h)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(s.w) * sizeof(float)};
+  const cuuint32_t box[2] = {kMaltaSpanW, kMaltaSpanH};
+  const cuuint32_t unit[2] = {1, 1};
+  for (int i = 0; i < 6; ++i) {
+    if (encode(&s.malta_map[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s.malta + i * s.n, dims,
+               strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      std::memset(s.malta_map, 0, sizeof(s.malta_map));
+      return;
+    }
+  }
+  s.malta_tma = true;
+}
+
 }  // namespace
 
 size_t ButteraugliArenaBytes(size_t width, size_t height) {
@@ -1370,6 +1496,8 @@ int ButteraugliCreate(size_t width, size_t height, float intensity_target, void*
   if (st->has_sub) AssignScale(st->sub, st->arena + ScaleFloats(st->main.n));
   st->maximum = st->arena + ScaleFloats(st->main.n) + ScaleFloats(st->sub.n);
   st->error = reinterpret_cast<uint32_t*>(st->maximum + 32);
+  EncodeMaltaMaps(st->main);
+  if (st->has_sub) EncodeMaltaMaps(st->sub);
   if (CheckCuda(cudaStreamCreateWithFlags(&st->side, cudaStreamNonBlocking),
                 "butteraugli: side stream") != GJXL_B200_OK ||
       CheckCuda(cudaEventCreateWithFlags(&st->fork, cudaEventDisableTiming),
