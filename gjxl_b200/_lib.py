@@ -77,6 +77,9 @@ SIGNATURES: dict[str, list] = {
     "gjxl_b200_butteraugli_pnorm_scratch_bytes": [],
     "gjxl_b200_butteraugli_pnorm": [P, Z, Z, Z, c_double, P, Z, P, P],
     "gjxl_b200_test_arm_failure": [I, I],
+    "gjxl_b200_entropy_slot_words": [I, Z, Z],
+    "gjxl_b200_entropy_write_sections": [P, P, P, Z, P, P, Z, P, P, P],
+    "gjxl_b200_entropy_count_sections": [P, c_uint32, P, P, P, P],
 }
 _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_initial_quant_scratch_bytes": c_size_t,
@@ -86,7 +89,8 @@ _RESTYPES = {"gjxl_b200_last_error": c_char_p,
              "gjxl_b200_batch_device_bytes": c_size_t,
              "gjxl_b200_cnn_param_count": c_size_t,
              "gjxl_b200_cnn_workspace_bytes": c_size_t,
-             "gjxl_b200_cnn_train_scratch_bytes": c_size_t}
+             "gjxl_b200_cnn_train_scratch_bytes": c_size_t,
+             "gjxl_b200_entropy_slot_words": c_size_t}
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "UNSUPPORTED", 3: "UNAVAILABLE",

@@ -718,6 +718,100 @@ GJXL_B200_API int gjxl_b200_check_device_error(const uint32_t* device_error, siz
  */
 GJXL_B200_API int gjxl_b200_test_arm_failure(int kind, int check_point);
 
+/*
+ * Entropy-coded sections on the device: the token streams of many sections
+ * (AC groups, DC groups, ...) written with an already built entropy code,
+ * ANS or prefix, bit for bit as the reference's CPU writers write them.
+ * Replaces WriteValidatedTokenStream (src/codestream/entropy.cpp:29), which
+ * dispatches to WriteAnsTokenStream (src/codestream/ans.cpp:2305: the
+ * reverse rANS recurrence of ans.cpp:1700-1770 and the reverse-bit append of
+ * src/codestream/ans_reverse_bits_internal.h) or to the prefix
+ * WriteTokenStream (src/codestream/entropy.cpp:2294, WriteValue :1173), as
+ * WriteAcSections calls it once per AC group on its worker threads
+ * (src/codestream/vardct/encoder.cpp:721-790); and the exact token-bit
+ * counters CountAnsTokenStreamBits / MeasureAnsCodes (ans.cpp:1774,1875).
+ * Model construction (clustering, normalisation, serialisation of the
+ * histograms) stays with the caller, as in the reference.
+ *
+ * An EntropyCode (src/codestream/entropy.h:153) flattened into device tables:
+ */
+#define GJXL_B200_ENTROPY_PREFIX 0
+#define GJXL_B200_ENTROPY_ANS 1
+typedef struct gjxl_b200_entropy_code {
+  int mode;                       /* GJXL_B200_ENTROPY_PREFIX or _ANS */
+  uint32_t context_count;         /* 1..65536 */
+  uint32_t cluster_count;         /* 1..256 */
+  const uint8_t* context_map;     /* [context_count]: cluster of each context */
+  const uint8_t* uint_configs;    /* [cluster_count][3]: HybridUintConfig
+                                     {split_exponent, msb_in_token, lsb_in_token} */
+  /* Prefix codes (mode 0), PrefixCode per cluster over 128 symbols. */
+  const uint8_t* prefix_depths;   /* [cluster][128]: code length, 0 = absent */
+  const uint16_t* prefix_bits;    /* [cluster][128]: code bits, first bit in bit 0 */
+  const uint16_t* prefix_degenerate; /* [cluster]: the symbol written with no
+                                        bits (degenerate_symbol), 128 = none */
+  /* ANS (mode 1), AnsHistogram per cluster over 256 symbols of a 4096 table. */
+  const uint16_t* ans_frequencies;      /* [cluster][256]: 0 = absent */
+  const uint16_t* ans_reverse_offsets;  /* [cluster][256]: prefix sums of the frequencies */
+  const uint16_t* ans_reverse_map;      /* [cluster][4096] */
+} gjxl_b200_entropy_code;
+
+/*
+ * Token streams of `count` sections. Tokens are EntropyToken {context, value}
+ * either interleaved (`pairs`: context, value uint32 pairs, the DC-group and
+ * metadata token layout) or split (`values` uint32 + `contexts` uint16, the
+ * AC token layout of gjxl_b200_ac_tokenize), all device memory. Section s
+ * holds tokens offsets[s] .. offsets[s + 1] - 1 (device uint32[count + 1]).
+ */
+typedef struct gjxl_b200_token_sections {
+  const uint32_t* pairs;
+  const uint32_t* values;
+  const uint16_t* contexts;
+  const uint32_t* offsets;
+  uint32_t count;
+} gjxl_b200_token_sections;
+
+/*
+ * Words of the slot buffer gjxl_b200_entropy_write_sections needs for
+ * `sections` sections of `tokens` tokens in all (47 bits per ANS token plus
+ * its 32-bit final state, 46 per prefix token, two words per section).
+ * Section s's slot starts at word ceil(B * offsets[s] / 64) + 2 s
+ * (B = 47 for ANS, 46 for prefix).
+ */
+GJXL_B200_API size_t gjxl_b200_entropy_slot_words(int mode, size_t tokens, size_t sections);
+
+/*
+ * Writes every section's token stream with `code` (host struct of device
+ * tables), ANS or prefix. Each section is written from bit 0 of its slot in
+ * `slot_words` (little-endian 64-bit words, first bit in bit 0, the
+ * reference BitWriter's byte order) and its length goes to bit_counts[s]
+ * (device uint64[count]) — BitWriter::bits_written() of the reference's
+ * section. With `packed` non-NULL the sections are also concatenated, each
+ * zero-padded to a byte boundary (BitWriter::padded_bytes()), in section
+ * order, and byte_offsets (device uint64[count + 1]) receives each section's
+ * first byte and the total: the codestream's section bytes in TOC order.
+ * packed_capacity >= 8 * slot_word_capacity always suffices. A token whose
+ * context is out of range or whose symbol the code lacks sets device_error
+ * bit 2 (the reference's InvalidArgument); that section's output is then
+ * undefined.
+ */
+GJXL_B200_API int gjxl_b200_entropy_write_sections(
+  const gjxl_b200_entropy_code* code, const gjxl_b200_token_sections* sections,
+  uint64_t* slot_words, size_t slot_word_capacity, uint64_t* bit_counts, uint8_t* packed,
+  size_t packed_capacity, uint64_t* byte_offsets, uint32_t* device_error, void* stream);
+
+/*
+ * Exact token-stream bits of every section under each of `code_count`
+ * (1..8) codes (host array of structs of device tables): bit_counts[s *
+ * code_count + c] (device uint64) equals CountAnsTokenStreamBits (ANS: 32 +
+ * extra bits + 16 per renormalisation) or the prefix stream's length, the
+ * figures MeasureAnsCodes and the rate search compare (ans.cpp:1875). Errors
+ * as gjxl_b200_entropy_write_sections.
+ */
+GJXL_B200_API int gjxl_b200_entropy_count_sections(
+  const gjxl_b200_entropy_code* codes, uint32_t code_count,
+  const gjxl_b200_token_sections* sections, uint64_t* bit_counts, uint32_t* device_error,
+  void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

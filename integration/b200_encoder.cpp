@@ -24,6 +24,13 @@
 //    device's scans against the serializer's, and hands back split token
 //    streams and the fixed-ANS populations.
 //
+//  * DeviceEntropyCode / WriteAcSectionsOnDevice: an EntropyCode the
+//    serializer built, flattened into device tables, and the per-group body
+//    of WriteAcSections (src/codestream/vardct/encoder.cpp:756-775) run on the
+//    device by gjxl_b200_entropy_write_sections: every AC group's section,
+//    byte for byte as WriteValidatedTokenStream writes it, without the token
+//    streams coming back to the host.
+//
 // The C entry point gjxl_b200_encode_image runs a session on packed 8-bit
 // sRGB, assembles the frame, validates it (ValidateSimpleCodestreamFrame,
 // src/codec/codestream.h:87) and writes the codestream with
@@ -32,6 +39,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -46,6 +54,9 @@
 #include "codec/vardct_frame_internal.h"
 #include "codec/vardct_frame_view_internal.h"
 #include "codestream/ac_tokenization_provider_internal.h"
+#include "codestream/ans_internal.h"
+#include "codestream/bit_writer.h"
+#include "codestream/entropy_internal.h"
 #include "codestream/encoder_internal.h"
 #include "codestream/rate_control_internal.h"
 #include "codestream/workflow.h"
@@ -490,6 +501,187 @@ Status EncodeWithSession(gjxl_b200_session* session, const uint8_t* pixels, size
   return Status::Ok();
 }
 
+// An EntropyCode's tables on the device (gjxl_b200_entropy_code): context
+// map, HybridUint configurations and, per cluster, the prefix code (depths,
+// bits, degenerate symbol) or the ANS histogram (frequencies, reverse-map
+// offsets, reverse map) padded to 128 / 256 symbols and 4096 entries.
+class DeviceEntropyCode {
+ public:
+  ~DeviceEntropyCode() {
+    if (device_ != nullptr) cudaFree(device_);
+  }
+
+  Status Upload(const EntropyCode& code) {
+    const bool ans = code.mode == EntropyCodingMode::kAns;
+    const size_t clusters = ans ? code.ans_histograms.size() : code.prefix_codes.size();
+    if (code.context_count == 0 || clusters == 0 || clusters > 256 ||
+        code.uint_configs.size() != clusters || code.context_map.size() != code.context_count) {
+      return Status::InvalidArgument("entropy code outside the device writer's range");
+    }
+    // One host image of all tables, 16-byte aligned pieces.
+    const auto align = [](size_t n) { return (n + 15) / 16 * 16; };
+    const size_t map_at = 0, config_at = align(code.context_count);
+    const size_t a_at = config_at + align(3 * clusters);
+    const size_t a_bytes = ans ? 256 * 2 * clusters : 128 * clusters;
+    const size_t b_at = a_at + align(a_bytes);
+    const size_t b_bytes = ans ? 256 * 2 * clusters : 128 * 2 * clusters;
+    const size_t c_at = b_at + align(b_bytes);
+    const size_t c_bytes = ans ? 4096 * 2 * clusters : 2 * clusters;
+    const size_t total = c_at + align(c_bytes);
+    std::vector<uint8_t> host(total, 0);
+    std::copy(code.context_map.begin(), code.context_map.end(), host.begin() + map_at);
+    for (size_t c = 0; c < clusters; ++c) {
+      host[config_at + 3 * c] = code.uint_configs[c].split_exponent;
+      host[config_at + 3 * c + 1] = code.uint_configs[c].msb_in_token;
+      host[config_at + 3 * c + 2] = code.uint_configs[c].lsb_in_token;
+    }
+    auto* a16 = reinterpret_cast<uint16_t*>(host.data() + a_at);
+    auto* b16 = reinterpret_cast<uint16_t*>(host.data() + b_at);
+    auto* c16 = reinterpret_cast<uint16_t*>(host.data() + c_at);
+    for (size_t c = 0; c < clusters; ++c) {
+      if (ans) {
+        const AnsHistogram& h = code.ans_histograms[c];
+        if (h.frequencies.size() > 256 || h.reverse_map.size() > 4096) {
+          return Status::InvalidArgument("ANS histogram outside the device writer's range");
+        }
+        std::copy(h.frequencies.begin(), h.frequencies.end(), a16 + 256 * c);
+        std::copy(h.reverse_offsets.begin(), h.reverse_offsets.end(), b16 + 256 * c);
+        std::copy(h.reverse_map.begin(), h.reverse_map.end(), c16 + 4096 * c);
+      } else {
+        const PrefixCode& pc = code.prefix_codes[c];
+        std::copy(pc.depths.begin(), pc.depths.end(), host.begin() + a_at + 128 * c);
+        std::copy(pc.bits.begin(), pc.bits.end(), b16 + 128 * c);
+        c16[c] = pc.degenerate_symbol;
+      }
+    }
+    Status status = FromCuda(cudaMalloc(&device_, total), "entropy tables");
+    if (status.ok()) {
+      status = FromCuda(cudaMemcpy(device_, host.data(), total, cudaMemcpyHostToDevice),
+                        "entropy tables");
+    }
+    if (!status.ok()) return status;
+    auto* d = static_cast<uint8_t*>(device_);
+    std::memset(&view_, 0, sizeof(view_));
+    view_.mode = ans ? GJXL_B200_ENTROPY_ANS : GJXL_B200_ENTROPY_PREFIX;
+    view_.context_count = code.context_count;
+    view_.cluster_count = static_cast<uint32_t>(clusters);
+    view_.context_map = d + map_at;
+    view_.uint_configs = d + config_at;
+    if (ans) {
+      view_.ans_frequencies = reinterpret_cast<const uint16_t*>(d + a_at);
+      view_.ans_reverse_offsets = reinterpret_cast<const uint16_t*>(d + b_at);
+      view_.ans_reverse_map = reinterpret_cast<const uint16_t*>(d + c_at);
+    } else {
+      view_.prefix_depths = d + a_at;
+      view_.prefix_bits = reinterpret_cast<const uint16_t*>(d + b_at);
+      view_.prefix_degenerate = reinterpret_cast<const uint16_t*>(d + c_at);
+    }
+    return Status::Ok();
+  }
+
+  const gjxl_b200_entropy_code* view() const { return &view_; }
+
+ private:
+  void* device_ = nullptr;
+  gjxl_b200_entropy_code view_{};
+};
+
+// WriteAcSections' per-group writes (src/codestream/vardct/encoder.cpp:
+// 756-775) on the device: section g of `streams` (device token streams,
+// total_tokens in all) written with `code` into sections[g], the same bits
+// WriteValidatedTokenStream(streams[g], code, &sections[g]) writes.
+Status WriteAcSectionsOnDevice(const EntropyCode& code, const gjxl_b200_token_sections& streams,
+                               size_t total_tokens, std::vector<BitWriter>* sections,
+                               float* device_ms = nullptr) {
+  DeviceEntropyCode tables;
+  Status status = tables.Upload(code);
+  if (!status.ok()) return status;
+  const size_t count = streams.count;
+  const size_t words = gjxl_b200_entropy_slot_words(tables.view()->mode, total_tokens, count);
+  const size_t offsets_bytes = (count + 1) * 8, bits_bytes = count * 8;
+  void* device = nullptr;
+  const size_t bytes = words * 8 * 2 + offsets_bytes + bits_bytes + 256;
+  status = FromCuda(cudaMalloc(&device, bytes), "section buffers");
+  if (!status.ok()) return status;
+  auto* slots = static_cast<uint64_t*>(device);
+  auto* packed = reinterpret_cast<uint8_t*>(slots + words);
+  auto* byte_offsets = reinterpret_cast<uint64_t*>(packed + words * 8);
+  auto* bit_counts = byte_offsets + count + 1;
+  auto* error = reinterpret_cast<uint32_t*>(bit_counts + count);
+  cudaEvent_t begin = nullptr, end = nullptr;
+  cudaEventCreate(&begin);
+  cudaEventCreate(&end);
+  status = FromCuda(cudaMemset(error, 0, 4), "section error word");
+  if (status.ok()) {
+    cudaEventRecord(begin, nullptr);
+    status = FromB200(gjxl_b200_entropy_write_sections(tables.view(), &streams, slots, words,
+                                                       bit_counts, packed, words * 8,
+                                                       byte_offsets, error, nullptr),
+                      "entropy_write_sections");
+    cudaEventRecord(end, nullptr);
+  }
+  if (status.ok()) {
+    status = FromB200(gjxl_b200_check_device_error(error, 1, nullptr), "device sections");
+  }
+  std::vector<uint64_t> bits(count), offsets(count + 1);
+  std::vector<uint8_t> host;
+  if (status.ok()) {
+    status = FromCuda(cudaMemcpy(bits.data(), bit_counts, bits_bytes, cudaMemcpyDeviceToHost),
+                      "section bits");
+  }
+  if (status.ok()) {
+    status = FromCuda(cudaMemcpy(offsets.data(), byte_offsets, offsets_bytes,
+                                 cudaMemcpyDeviceToHost), "section offsets");
+  }
+  if (status.ok()) {
+    host.resize(offsets[count]);
+    status = FromCuda(cudaMemcpy(host.data(), packed, host.size(), cudaMemcpyDeviceToHost),
+                      "section bytes");
+  }
+  if (status.ok() && device_ms != nullptr) cudaEventElapsedTime(device_ms, begin, end);
+  cudaEventDestroy(begin);
+  cudaEventDestroy(end);
+  cudaFree(device);
+  if (!status.ok()) return status;
+  // Each section's whole bytes, then its last partial byte's bits.
+  std::vector<BitWriter> result(count);
+  for (size_t g = 0; g < count; ++g) {
+    const uint8_t* b = host.data() + offsets[g];
+    const size_t whole = bits[g] / 8, rest = bits[g] % 8;
+    for (size_t i = 0; i < whole; i += 7) {
+      const size_t n = std::min<size_t>(7, whole - i);
+      uint64_t v = 0;
+      for (size_t k = 0; k < n; ++k) v |= static_cast<uint64_t>(b[i + k]) << (8 * k);
+      status = result[g].WriteBits(8 * n, v);
+      if (!status.ok()) return status;
+    }
+    if (rest != 0) {
+      status = result[g].WriteBits(rest, b[whole] & ((1u << rest) - 1));
+      if (!status.ok()) return status;
+    }
+  }
+  *sections = std::move(result);
+  return Status::Ok();
+}
+
+// Fixed-ANS populations of a [contexts][128] device histogram (the
+// provider's Finish, above).
+std::vector<codestream_internal::PreparedFixedAnsCluster> Populations(
+  const std::vector<uint32_t>& histogram, size_t contexts) {
+  std::vector<codestream_internal::PreparedFixedAnsCluster> out(contexts);
+  for (size_t context = 0; context < contexts; ++context) {
+    auto& cluster = out[context];
+    for (uint32_t symbol = 0; symbol < 128; ++symbol) {
+      const uint64_t n = histogram[context * 128 + symbol];
+      cluster.counts[symbol] = n;
+      cluster.token_count += n;
+      if (n != 0) cluster.maximum_symbol = symbol;
+      if (symbol >= 16) cluster.extra_bits += n * (2 + ((symbol - 16) >> 2));
+    }
+  }
+  return out;
+}
+
 struct SessionOwner {
   gjxl_b200_session* session = nullptr;
   ~SessionOwner() {
@@ -633,5 +825,95 @@ GJXL_INTEGRATION_API int gjxl_b200_encode_target_size(
     return -2;
   }
   std::memcpy(out, result.codestream.data(), result.codestream.size());
+  return 0;
+}
+
+// The AC sections of one analysis written twice with the same entropy code:
+// by the reference's WriteValidatedTokenStream on host copies of the
+// session's token streams (as WriteAcSections does) and on the device by
+// WriteAcSectionsOnDevice from the session's device streams. The code is the
+// one the serializer builds from the device populations: direct ANS
+// (OptimizeDirectAnsEntropyCodeWithFixedPopulations, balanced) or, with
+// prefix != 0, the fast prefix code. Reports the section count, the bytes,
+// whether every section is identical, and both writers' times.
+GJXL_INTEGRATION_API int gjxl_b200_compare_ac_sections(
+  const uint8_t* pixels, size_t width, size_t height, size_t row_stride, int channels,
+  float butteraugli_target, int effort, int prefix, size_t* sections, size_t* bytes,
+  int* identical, double* device_ms, double* host_ms) {
+  g_last_error.clear();
+  gjxl_b200_options session_options;
+  gjxl_b200_default_options(&session_options);
+  session_options.butteraugli_target = butteraugli_target;
+  session_options.effort = effort;
+  session_options.tokenize = 1;
+  SessionOwner owner;
+  Status status = FromB200(gjxl_b200_session_create(width, height, &session_options,
+                                                    &owner.session), "session_create");
+  if (status.ok()) {
+    status = FromB200(gjxl_b200_session_analyze_host(owner.session, pixels, row_stride, channels,
+                                                     nullptr),
+                      "session_analyze_host");
+  }
+  if (status.ok()) status = FromCuda(cudaDeviceSynchronize(), "analysis");
+  gjxl_b200_outputs o;
+  if (status.ok()) {
+    status = FromB200(gjxl_b200_session_outputs(owner.session, &o), "session_outputs");
+  }
+  if (!status.ok()) return Fail(status);
+  const size_t groups = o.groups, total = o.host_token_count;
+  const size_t contexts = 4 * 495;
+  std::vector<uint32_t> histogram(contexts * 128);
+  status = FromCuda(cudaMemcpy(histogram.data(), o.token_histogram, histogram.size() * 4,
+                               cudaMemcpyDeviceToHost), "token histogram");
+  if (!status.ok()) return Fail(status);
+  std::vector<EntropyTokenStreamView> views;
+  for (size_t g = 0; g < groups; ++g) {
+    const size_t begin = o.host_group_offsets[g], n = o.host_group_offsets[g + 1] - begin;
+    views.push_back(EntropyTokenStreamView::Split({o.host_token_values + begin, n},
+                                                  {o.host_token_contexts + begin, n}));
+  }
+  EntropyCodeOptions options;
+  options.context_count = static_cast<uint32_t>(contexts);
+  options.maximum_ans_clusters =
+    codestream_internal::AcAnsClusterLimit(Extent2D{width, height});
+  EntropyCode code;
+  if (prefix != 0) {
+    status = codestream_internal::OptimizeFastPrefixEntropyCode(views, options, &code);
+  } else {
+    const auto populations = Populations(histogram, contexts);
+    status = codestream_internal::OptimizeDirectAnsEntropyCodeWithFixedPopulations(
+      views, options, populations, &code);
+  }
+  if (!status.ok()) return Fail(status);
+  // The reference's writer, one group after another on this thread.
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<BitWriter> want(groups);
+  for (size_t g = 0; g < groups && status.ok(); ++g) {
+    status = codestream_internal::WriteValidatedTokenStream(views[g], code, &want[g]);
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  if (!status.ok()) return Fail(status);
+  gjxl_b200_token_sections streams{};
+  streams.values = o.token_values;
+  streams.contexts = o.token_contexts;
+  streams.offsets = o.group_offsets;
+  streams.count = static_cast<uint32_t>(groups);
+  std::vector<BitWriter> got;
+  float ms = 0.0f;
+  status = WriteAcSectionsOnDevice(code, streams, total, &got, &ms);
+  if (!status.ok()) return Fail(status);
+  bool same = got.size() == want.size();
+  size_t written = 0;
+  for (size_t g = 0; same && g < groups; ++g) {
+    const auto a = got[g].padded_bytes(), b = want[g].padded_bytes();
+    same = got[g].bits_written() == want[g].bits_written() &&
+           std::equal(a.begin(), a.end(), b.begin(), b.end());
+    written += b.size();
+  }
+  *sections = groups;
+  *bytes = written;
+  *identical = same ? 1 : 0;
+  *device_ms = ms;
+  *host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   return 0;
 }

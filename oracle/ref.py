@@ -16,6 +16,12 @@ LIBRARY_PATH = Path(__file__).resolve().parent / "_ref" / "libgjxl_ref.so"
 
 _P, _Z, _F, _I = c_void_p, c_size_t, c_float, c_int
 _SIGNATURES = {
+    "gjxl_ref_entropy_build": [_I, _P, _P, _P, _Z, ctypes.c_uint32, ctypes.c_uint32, _P],
+    "gjxl_ref_entropy_free": [_P],
+    "gjxl_ref_entropy_info": [_P, _P, _P, _P],
+    "gjxl_ref_entropy_tables": [_P] * 9,
+    "gjxl_ref_entropy_write": [_P, _P, _P, _P, _Z, _P, _Z, _P, _P],
+    "gjxl_ref_entropy_count": [_P, _P, _P, _P, _Z, _P],
     "gjxl_ref_srgb8_to_linear": [_P, _Z, _Z, _Z, _I, _P],
     "gjxl_ref_linear_to_padded_opsin": [_P, _Z, _Z, _P, _Z, _Z, _F],
     "gjxl_ref_opsin_to_linear": [_P, _Z, _Z, _F, _P],
@@ -495,3 +501,77 @@ def cuda_encode(linear: np.ndarray, target: float = 1.0, effort: int = 7) -> dic
                            f"{lib.gjxl_ref_cuda_last_error().decode()}")
     return {"codestream": out[:size.value].tobytes(), "score": score.value,
             "analysis_ms": analysis.value / 1e6, "total_ms": total.value / 1e6}
+
+
+# ---- Entropy-coded sections: the reference's model builders, writers and
+# bit counters (ref_shim.cpp, gjxl_ref_entropy_*).
+
+ENTROPY_KINDS = {"prefix": 0, "ans": 1, "ans_high_density": 2, "ans_rate": 3}
+
+
+def _split(values: np.ndarray, contexts: np.ndarray, offsets: np.ndarray):
+    return (np.ascontiguousarray(values, np.uint32), np.ascontiguousarray(contexts, np.uint16),
+            np.ascontiguousarray(offsets, np.uint32))
+
+
+class RefEntropyCode:
+    """An EntropyCode built by the reference over split token sections
+    (values uint32, contexts uint16, offsets uint32 [count + 1])."""
+
+    def __init__(self, kind: str, values, contexts, offsets, context_count: int,
+                 max_clusters: int = 32):
+        v, c, o = _split(values, contexts, offsets)
+        handle = ctypes.c_void_p()
+        _check(lib().gjxl_ref_entropy_build(ENTROPY_KINDS[kind], _ptr(v), _ptr(c), _ptr(o),
+                                            o.size - 1, context_count, max_clusters,
+                                            ctypes.addressof(handle)), "entropy_build")
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            lib().gjxl_ref_entropy_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def tables(self) -> dict:
+        mode, ctx, clusters = c_int(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().gjxl_ref_entropy_info(self.handle, ctypes.addressof(mode),
+                                           ctypes.addressof(ctx), ctypes.addressof(clusters)),
+               "entropy_info")
+        n, k = ctx.value, clusters.value
+        t = {"mode": mode.value, "context_count": n, "cluster_count": k,
+             "context_map": np.zeros(n, np.uint8), "configs": np.zeros((k, 3), np.uint8),
+             "depths": np.zeros((k, 128), np.uint8), "bits": np.zeros((k, 128), np.uint16),
+             "degenerate": np.zeros(k, np.uint16),
+             "frequencies": np.zeros((k, 256), np.uint16),
+             "reverse_offsets": np.zeros((k, 256), np.uint16),
+             "reverse_map": np.zeros((k, 4096), np.uint16)}
+        _check(lib().gjxl_ref_entropy_tables(
+            self.handle, *[_ptr(t[name]) for name in (
+                "context_map", "configs", "depths", "bits", "degenerate", "frequencies",
+                "reverse_offsets", "reverse_map")]), "entropy_tables")
+        return t
+
+    def write(self, values, contexts, offsets) -> dict:
+        """Each section via WriteValidatedTokenStream: bit_counts, the padded
+        section bytes concatenated, byte_offsets [count + 1]."""
+        v, c, o = _split(values, contexts, offsets)
+        count = o.size - 1
+        out = np.zeros(8 * (47 * v.size // 64 + 2 * count + 2), np.uint8)
+        bits = np.zeros(count, np.uint64)
+        byte_offsets = np.zeros(count + 1, np.uint64)
+        _check(lib().gjxl_ref_entropy_write(self.handle, _ptr(v), _ptr(c), _ptr(o), count,
+                                            _ptr(out), out.size, _ptr(bits),
+                                            _ptr(byte_offsets)), "entropy_write")
+        return {"bit_counts": bits, "bytes": out[:int(byte_offsets[-1])],
+                "byte_offsets": byte_offsets}
+
+    def count(self, values, contexts, offsets) -> np.ndarray:
+        """CountAnsTokenStreamBits / CountTokenStreamBits per section."""
+        v, c, o = _split(values, contexts, offsets)
+        bits = np.zeros(o.size - 1, np.uint64)
+        _check(lib().gjxl_ref_entropy_count(self.handle, _ptr(v), _ptr(c), _ptr(o), o.size - 1,
+                                            _ptr(bits)), "entropy_count")
+        return bits

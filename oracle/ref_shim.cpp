@@ -10,7 +10,9 @@
 // stride == width) and returns 0 on success or the reference's StatusCode
 // value on failure (the message is kept for gjxl_ref_last_error()).
 
+#include <algorithm>
 #include <array>
+#include <memory>
 #include <chrono>
 #include <cmath>
 #include <cstddef>
@@ -37,7 +39,10 @@
 #include "codestream/block_context_map.h"
 #include "codestream/coefficient_order.h"
 #include "codestream/dc_group.h"
+#include "codestream/ans_internal.h"
+#include "codestream/bit_writer.h"
 #include "codestream/entropy.h"
+#include "codestream/entropy_internal.h"
 #include "codestream/weighted_dc.h"
 #include "codestream/encoder.h"
 #include "codestream/workflow.h"
@@ -804,6 +809,150 @@ GJXL_REF_API int gjxl_ref_hybrid_uint(const uint32_t* values, size_t count, int 
     out[3 * i] = token.symbol;
     out[3 * i + 1] = token.extra_bit_count;
     out[3 * i + 2] = token.extra_bits;
+  }
+  return 0;
+}
+
+// ---- Entropy-coded sections: the reference's model builders, section
+// writers and bit counters over split (value, context) token streams.
+
+namespace {
+
+std::vector<EntropyTokenStreamView> SplitSections(const uint32_t* values,
+                                                  const uint16_t* contexts,
+                                                  const uint32_t* offsets, size_t count) {
+  std::vector<EntropyTokenStreamView> views;
+  views.reserve(count);
+  for (size_t s = 0; s < count; ++s) {
+    const size_t begin = offsets[s], n = offsets[s + 1] - offsets[s];
+    views.push_back(EntropyTokenStreamView::Split({values + begin, n}, {contexts + begin, n}));
+  }
+  return views;
+}
+
+}  // namespace
+
+// Builds an EntropyCode over the sections: kind 0 the fast prefix code
+// (OptimizeFastPrefixEntropyCode), 1/2/3 direct ANS in the balanced,
+// high-density and rate-optimized modes (OptimizeDirectAnsEntropyCode) with
+// at most `max_clusters` clusters.
+GJXL_REF_API int gjxl_ref_entropy_build(int kind, const uint32_t* values,
+                                        const uint16_t* contexts, const uint32_t* offsets,
+                                        size_t count, uint32_t context_count,
+                                        uint32_t max_clusters, void** handle) {
+  if (handle == nullptr || offsets == nullptr || count == 0 || kind < 0 || kind > 3) {
+    return Fail(Status::InvalidArgument("entropy_build: invalid arguments"));
+  }
+  const auto views = SplitSections(values, contexts, offsets, count);
+  EntropyCodeOptions options;
+  options.context_count = context_count;
+  options.maximum_ans_clusters = max_clusters;
+  auto code = std::make_unique<EntropyCode>();
+  Status status = Status::Ok();
+  if (kind == 0) {
+    status = codestream_internal::OptimizeFastPrefixEntropyCode(views, options, code.get());
+  } else {
+    const auto mode = kind == 1 ? codestream_internal::DirectAnsEntropyMode::kBalanced
+                      : kind == 2 ? codestream_internal::DirectAnsEntropyMode::kHighDensity
+                                  : codestream_internal::DirectAnsEntropyMode::kRateOptimized;
+    status = codestream_internal::OptimizeDirectAnsEntropyCode(views, options, mode, code.get());
+  }
+  if (!status.ok()) return Fail(status);
+  *handle = code.release();
+  return 0;
+}
+
+GJXL_REF_API void gjxl_ref_entropy_free(void* handle) {
+  delete static_cast<EntropyCode*>(handle);
+}
+
+// mode (0 prefix, 1 ANS), context and cluster counts of a built code.
+GJXL_REF_API int gjxl_ref_entropy_info(void* handle, int* mode, uint32_t* context_count,
+                                       uint32_t* cluster_count) {
+  const auto& code = *static_cast<const EntropyCode*>(handle);
+  *mode = code.mode == EntropyCodingMode::kAns ? 1 : 0;
+  *context_count = code.context_count;
+  *cluster_count = static_cast<uint32_t>(code.mode == EntropyCodingMode::kAns
+                                           ? code.ans_histograms.size()
+                                           : code.prefix_codes.size());
+  return 0;
+}
+
+// The code flattened: context map, HybridUint configs (3 bytes per
+// cluster), prefix depths/bits [cluster][128] and degenerate symbols, ANS
+// frequencies/reverse offsets [cluster][256] and reverse maps
+// [cluster][4096] (absent entries zero).
+GJXL_REF_API int gjxl_ref_entropy_tables(void* handle, uint8_t* context_map, uint8_t* configs,
+                                         uint8_t* depths, uint16_t* bits, uint16_t* degenerate,
+                                         uint16_t* frequencies, uint16_t* reverse_offsets,
+                                         uint16_t* reverse_map) {
+  const auto& code = *static_cast<const EntropyCode*>(handle);
+  std::copy(code.context_map.begin(), code.context_map.end(), context_map);
+  for (size_t c = 0; c < code.uint_configs.size(); ++c) {
+    configs[3 * c] = code.uint_configs[c].split_exponent;
+    configs[3 * c + 1] = code.uint_configs[c].msb_in_token;
+    configs[3 * c + 2] = code.uint_configs[c].lsb_in_token;
+  }
+  if (code.mode == EntropyCodingMode::kAns) {
+    for (size_t c = 0; c < code.ans_histograms.size(); ++c) {
+      const AnsHistogram& h = code.ans_histograms[c];
+      std::fill_n(frequencies + 256 * c, 256, uint16_t{0});
+      std::fill_n(reverse_offsets + 256 * c, 256, uint16_t{0});
+      std::fill_n(reverse_map + 4096 * c, 4096, uint16_t{0});
+      std::copy(h.frequencies.begin(), h.frequencies.end(), frequencies + 256 * c);
+      std::copy(h.reverse_offsets.begin(), h.reverse_offsets.end(), reverse_offsets + 256 * c);
+      std::copy(h.reverse_map.begin(), h.reverse_map.end(), reverse_map + 4096 * c);
+    }
+  } else {
+    for (size_t c = 0; c < code.prefix_codes.size(); ++c) {
+      const PrefixCode& p = code.prefix_codes[c];
+      std::copy(p.depths.begin(), p.depths.end(), depths + 128 * c);
+      std::copy(p.bits.begin(), p.bits.end(), bits + 128 * c);
+      degenerate[c] = p.degenerate_symbol;
+    }
+  }
+  return 0;
+}
+
+// Every section written by WriteValidatedTokenStream into its own
+// BitWriter (as WriteAcSections does): bits_written per section, the padded
+// bytes concatenated into `out`, and each section's first byte.
+GJXL_REF_API int gjxl_ref_entropy_write(void* handle, const uint32_t* values,
+                                        const uint16_t* contexts, const uint32_t* offsets,
+                                        size_t count, uint8_t* out, size_t capacity,
+                                        uint64_t* bit_counts, uint64_t* byte_offsets) {
+  const auto& code = *static_cast<const EntropyCode*>(handle);
+  const auto views = SplitSections(values, contexts, offsets, count);
+  size_t at = 0;
+  for (size_t s = 0; s < count; ++s) {
+    BitWriter writer;
+    Status status = codestream_internal::WriteValidatedTokenStream(views[s], code, &writer);
+    if (!status.ok()) return Fail(status);
+    const auto bytes = writer.padded_bytes();
+    if (at + bytes.size() > capacity) {
+      return Fail(Status::InvalidArgument("entropy_write: output too small"));
+    }
+    std::copy(bytes.begin(), bytes.end(), out + at);
+    byte_offsets[s] = at;
+    bit_counts[s] = writer.bits_written();
+    at += bytes.size();
+  }
+  byte_offsets[count] = at;
+  return 0;
+}
+
+// Exact token bits per section: CountAnsTokenStreamBits for ANS,
+// CountTokenStreamBits for prefix codes.
+GJXL_REF_API int gjxl_ref_entropy_count(void* handle, const uint32_t* values,
+                                        const uint16_t* contexts, const uint32_t* offsets,
+                                        size_t count, uint64_t* bit_counts) {
+  const auto& code = *static_cast<const EntropyCode*>(handle);
+  const auto views = SplitSections(values, contexts, offsets, count);
+  for (size_t s = 0; s < count; ++s) {
+    Status status = code.mode == EntropyCodingMode::kAns
+                      ? codestream_internal::CountAnsTokenStreamBits(views[s], code, &bit_counts[s])
+                      : codestream_internal::CountTokenStreamBits(views[s], code, &bit_counts[s]);
+    if (!status.ok()) return Fail(status);
   }
   return 0;
 }

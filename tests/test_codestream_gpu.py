@@ -177,3 +177,33 @@ def test_target_size_rate_control_matches_reference(cuda, fraction):
     if got["met"]:
         assert target_bytes - len(got["codestream"]) <= int(np.ceil(target_bytes * 0.005))
         assert len(got["codestream"]) <= target_bytes
+
+
+@pytest.mark.parametrize("w,h,prefix", [(1000, 700, 0), (1000, 700, 1), (4032, 3024, 0)])
+def test_device_ac_sections_match_reference_writer(cuda, w, h, prefix):
+    """The binding's WriteAcSectionsOnDevice (device tables of the code the
+    serializer builds from the device populations, the sections written by
+    gjxl_b200_entropy_write_sections) against the reference's
+    WriteValidatedTokenStream on every AC group: identical bytes and bit
+    counts, including the 4032x3024 benchmark image."""
+    import torch  # noqa: F401  (initializes the CUDA context on cuda:0)
+    lib = encoder()
+    fn = lib.gjxl_b200_compare_ac_sections
+    fn.argtypes = [c_void_p, c_size_t, c_size_t, c_size_t, c_int, c_float, c_int, c_int,
+                   ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t), ctypes.POINTER(c_int),
+                   ctypes.POINTER(c_double), ctypes.POINTER(c_double)]
+    fn.restype = c_int
+    img = (generate_srgb8(w, h, 31) if w < 4000
+           else generate_srgb8(w, h, workload_seed(2, 0), sensor_noise=True))
+    img = np.ascontiguousarray(img)
+    sections, nbytes, same = c_size_t(0), c_size_t(0), c_int(0)
+    device_ms, host_ms = c_double(0.0), c_double(0.0)
+    rc = fn(img.ctypes.data, w, h, w * 3, 3, 1.0, 7, prefix, ctypes.byref(sections),
+            ctypes.byref(nbytes), ctypes.byref(same), ctypes.byref(device_ms),
+            ctypes.byref(host_ms))
+    assert rc == 0, lib.gjxl_b200_integration_last_error().decode()
+    print(f"\n{w}x{h} {'prefix' if prefix else 'ANS'}: {sections.value} sections, "
+          f"{nbytes.value} bytes, device {device_ms.value:.3f} ms, "
+          f"reference writer {host_ms.value:.1f} ms (one thread)")
+    assert sections.value == ((w + 255) // 256) * ((h + 255) // 256)
+    assert same.value == 1
