@@ -528,9 +528,9 @@ class RefEntropyCode:
         self.handle = handle
 
     def close(self):
-        if self.handle:
-            lib().gjxl_ref_entropy_free(self.handle)
-            self.handle = None
+        if self.handle and _lib is not None:
+            _lib.gjxl_ref_entropy_free(self.handle)
+        self.handle = None
 
     def __del__(self):
         self.close()
