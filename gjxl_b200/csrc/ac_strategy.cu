@@ -528,14 +528,11 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
                             anchor_x[k] * 8 + x];
   }
 
-  // Ordered magnitude sums (one thread per candidate and channel); these
-  // threads then join the inverse row pass, which does not touch `terms`.
-  // The fast mode sums every plane with all threads instead.
-  if constexpr (kExact) {
-    if (tid < KC && anchor_x[tid / 3] >= 0) {
-      magnitude[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
-    }
-  } else {
+  // The exact mode's ordered magnitude sums (one thread per candidate and
+  // channel) wait for the end, where they run beside the loss sums: summing
+  // here would hold back those threads' share of the inverse passes. The
+  // fast mode sums every plane with all threads now.
+  if constexpr (!kExact) {
     ParallelPlaneSums<N, KC, kCostThreads, Lay::TermPitch>(
       terms, tid, [&](int plane, float sum) { magnitude[plane / 3][plane % 3] = sum; });
   }
@@ -559,7 +556,11 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
   }
   __syncthreads();
 
-  // Weighted eighth powers in pixel order.
+  // Weighted eighth powers in pixel order; the exact mode keeps them in the
+  // row-pass buffer (free once the column pass has read it), as `terms`
+  // still holds the magnitude terms.
+  float* loss_terms = kExact ? reinterpret_cast<float*>(T) : terms;
+  static_assert(!kExact || 2 * Lay::Planes >= KC * Lay::TermPitch, "loss terms fit T");
   for (int i = tid; i < KC * N; i += kCostThreads) {
     const int kc = i / N, r = i % N, y = r / W, x = r % W, k = kc / 3, c = kc % 3;
     if (anchor_x[k] < 0) continue;
@@ -570,13 +571,19 @@ CandidateCostKernel(const __grid_constant__ CostParams p, uint32_t candidate_cou
     weighted *= weighted;
     weighted *= weighted;
     weighted *= weighted;
-    terms[kc * Lay::TermPitch + r] = weighted;
+    loss_terms[kc * Lay::TermPitch + r] = weighted;
   }
   __syncthreads();
 
   if constexpr (kExact) {
-    if (tid < KC && anchor_x[tid / 3] >= 0) {
-      loss_sum[tid / 3][tid % 3] = OrderedSum<N>(terms + tid * Lay::TermPitch);
+    // One code path for both kinds of sum, so that a warp holding threads
+    // of both runs them side by side.
+    static_assert(2 * KC <= kCostThreads, "one thread per ordered sum");
+    const bool loss = tid >= KC;
+    const int plane = loss ? tid - KC : tid;
+    if (tid < 2 * KC && anchor_x[plane / 3] >= 0) {
+      const float sum = OrderedSum<N>((loss ? loss_terms : terms) + plane * Lay::TermPitch);
+      (loss ? &loss_sum[0][0] : &magnitude[0][0])[plane] = sum;
     }
   } else {
     ParallelPlaneSums<N, KC, kCostThreads, Lay::TermPitch>(
