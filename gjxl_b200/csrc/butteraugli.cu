@@ -839,6 +839,116 @@ MaltaKernel(const __grid_constant__ MaltaParams p, const __grid_constant__ CUten
   }
 }
 
+// One channel's three Malta stages in one pass: the first stage (full
+// Malta) stores, the other two (low-frequency Malta) add, in the order of
+// the per-stage launches (stage plane order {4, 2, 0} for Y, {5, 3, 1} for
+// X): acc = r0; acc = acc + (0 + r1); acc = acc + (0 + r2), all in
+// registers, one store. Each tile's three 72 x 24 windows arrive by three
+// tiled bulk tensor copies on one mbarrier; needs planes that take tensor
+// maps (the per-stage MaltaKernel covers the others).
+struct MaltaChannelParams {
+  float* accumulate;
+  int w, h;
+  int tiles_x, tiles_y;
+  uint32_t* error;
+};
+
+__global__ void __launch_bounds__(kMaltaThreads, 2)
+MaltaChannelKernel(const __grid_constant__ MaltaChannelParams p,
+                   const __grid_constant__ CUtensorMap first,
+                   const __grid_constant__ CUtensorMap second,
+                   const __grid_constant__ CUtensorMap third) {
+  __shared__ __align__(128) float tile[2][3][kMaltaSpanH][kMaltaSpanW];
+  __shared__ __align__(8) uint64_t full[2];
+  constexpr uint32_t kBoxBytes = kMaltaSpanW * kMaltaSpanH * sizeof(float);
+  static_assert(kBoxBytes % 128 == 0, "each window starts on a 128-byte boundary");
+  const int tiles = p.tiles_x * p.tiles_y;
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+        static_cast<uint32_t>(__cvta_generic_to_shared(&full[b]))));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+  const auto stage = [&](int t, int buffer) {
+    if (threadIdx.x != 0) return;
+    const int x0 = (t % p.tiles_x) * kMaltaTileW - kMaltaHalo;
+    const int y0 = (t / p.tiles_x) * kMaltaTileH - kMaltaHalo;
+    const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&full[buffer]));
+    // The buffers were last read through the generic proxy.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(3 * kBoxBytes));
+    const auto copy = [&](const CUtensorMap& map, int k) {
+      asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(&tile[buffer][k][0][0]))),
+          "l"(reinterpret_cast<uint64_t>(&map)), "r"(x0), "r"(y0), "r"(bar)
+        : "memory");
+    };
+    copy(first, 0);
+    copy(second, 1);
+    copy(third, 2);
+  };
+  int buffer = 0;
+  uint32_t phases = 0;  // bit b: parity of buffer b's next completion
+  if (static_cast<int>(blockIdx.x) < tiles) stage(blockIdx.x, 0);
+  for (int t = blockIdx.x; t < tiles; t += gridDim.x, buffer ^= 1) {
+    const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&full[buffer]));
+    const bool done = WaitParity(bar, (phases >> buffer) & 1u);
+    if (!__syncthreads_and(done)) {
+      // The copies did not arrive within the bound: record it, wait once
+      // more (bounded) for them before the shared memory is released, stop.
+      if (threadIdx.x == 0) {
+        RaiseError(p.error, kErrorInternal);
+        WaitParity(bar, (phases >> buffer) & 1u);
+      }
+      break;
+    }
+    phases ^= 1u << buffer;
+    if (t + static_cast<int>(gridDim.x) < tiles) stage(t + gridDim.x, buffer ^ 1);
+    const int lx = (threadIdx.x % (kMaltaTileW / kMaltaRun)) * kMaltaRun;
+    const int ly = threadIdx.x / (kMaltaTileW / kMaltaRun);
+    float acc[kMaltaRun];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float v[2 * kMaltaHalo + 1][kMaltaWindowW];
+#pragma unroll
+      for (int dy = 0; dy < 2 * kMaltaHalo + 1; ++dy) {
+#pragma unroll
+        for (int q = 0; q < kMaltaWindowW / 4; ++q) {
+          const float4 f =
+            *reinterpret_cast<const float4*>(&tile[buffer][k][ly + dy][lx + 4 * q]);
+          v[dy][4 * q + 0] = f.x;
+          v[dy][4 * q + 1] = f.y;
+          v[dy][4 * q + 2] = f.z;
+          v[dy][4 * q + 3] = f.w;
+        }
+      }
+      if (k == 0) {
+        acc[0] = MaltaUnit<false, 0>(v);
+        acc[1] = MaltaUnit<false, 1>(v);
+        acc[2] = MaltaUnit<false, 2>(v);
+        acc[3] = MaltaUnit<false, 3>(v);
+      } else {
+        const float r[kMaltaRun] = {MaltaUnit<true, 0>(v), MaltaUnit<true, 1>(v),
+                                    MaltaUnit<true, 2>(v), MaltaUnit<true, 3>(v)};
+#pragma unroll
+        for (int j = 0; j < kMaltaRun; ++j) acc[j] = acc[j] + (0.0f + r[j]);
+      }
+    }
+    const int x = (t % p.tiles_x) * kMaltaTileW + lx, y = (t / p.tiles_x) * kMaltaTileH + ly;
+    if (y >= p.h) continue;
+    float* out = p.accumulate + static_cast<size_t>(y) * p.w + x;
+#pragma unroll
+    for (int j = 0; j < kMaltaRun; ++j) {
+      if (x + j < p.w) out[j] = acc[j];
+    }
+  }
+}
+
 struct L2Params {
   const float* ref;   // psycho planes of the reference
   const float* dist;  // psycho planes of the distorted image
@@ -1288,7 +1398,26 @@ void Differences(ButteraugliState& st, Scale& s, bool reference_side, cudaStream
   // Three CTAs per SM walk the tiles.
   const unsigned malta_grid = static_cast<unsigned>(
     st.sm_count > 0 ? std::min(tiles_x * tiles_y, st.sm_count * 3) : tiles_x * tiles_y);
+  if (s.malta_tma) {
+    // Channel 1 (Y) from stage planes 4, 2, 0 and channel 0 (X) from 5, 3, 1.
+    for (int channel = 1; channel >= 0; --channel) {
+      MaltaChannelParams cp;
+      cp.accumulate = s.ac + channel * n;
+      cp.w = s.w;
+      cp.h = s.h;
+      cp.tiles_x = tiles_x;
+      cp.tiles_y = tiles_y;
+      cp.error = st.error;
+      const int base = channel == 1 ? 0 : 1;
+      // Two CTAs per SM (103 registers per thread).
+      const unsigned channel_grid = static_cast<unsigned>(
+        st.sm_count > 0 ? std::min(tiles_x * tiles_y, st.sm_count * 2) : tiles_x * tiles_y);
+      MaltaChannelKernel<<<channel_grid, kMaltaThreads, 0, stream>>>(
+        cp, s.malta_map[base + 4], s.malta_map[base + 2], s.malta_map[base]);
+    }
+  }
   for (int index : order) {
+    if (s.malta_tma) break;
     MaltaParams mp;
     mp.scaled = s.malta + index * n;
     const int channel = index % 2 == 0 ? 1 : 0;
