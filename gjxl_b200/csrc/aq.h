@@ -72,9 +72,12 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
                   const int32_t* raw, const AqQuantizer* q, const int8_t* y_to_x,
                   const int8_t* y_to_b, const float* matrix_multiplier, float* recon,
                   cudaStream_t stream, const StreamFan* fan = nullptr);
+// With `linear` non-null the last pass writes OpsinToLinear of the filtered
+// image (at intensity_target) there instead of the filtered planes.
 int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, size_t width,
                   size_t height, const float* inverse_sigma, size_t bx, float* scratch_a,
-                  float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream);
+                  float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream,
+                  float* linear = nullptr, float intensity_target = 80.0f);
 int AqOpsinToLinear(const float* opsin, size_t width, size_t height, float intensity_target,
                     float* linear, uint32_t* error, cudaStream_t stream);
 int AqBlockReduce(const uint8_t* cells, size_t bx, size_t by, const float* distance_map,

@@ -336,6 +336,32 @@ GaborishForwardKernel(const __grid_constant__ GaborishParams p) {
   }
 }
 
+struct LinearParams {
+  const float* opsin;
+  float* linear;
+  size_t n;
+  float bias_cuberoot;
+  float scaled_matrix[3][3];  // scale * inverse opsin matrix
+  uint32_t* error;
+};
+
+// OpsinToLinear (color_transform.cpp:433) of one pixel (x, y, b) into
+// pixel i of the three linear planes.
+__device__ __forceinline__ void OpsinToLinearPixel(const LinearParams& p, float x, float y,
+                                                   float b, size_t i) {
+  const float kOpsinBias = 0.0037930732552754493f;
+  const float gamma[3] = {y + x + p.bias_cuberoot, y - x + p.bias_cuberoot, b + p.bias_cuberoot};
+  float mixed[3];
+  for (int c = 0; c < 3; ++c) mixed[c] = gamma[c] * gamma[c] * gamma[c] - kOpsinBias;
+  for (int r = 0; r < 3; ++r) {
+    float v = p.scaled_matrix[r][0] * mixed[0];
+    v = fmaf(p.scaled_matrix[r][1], mixed[1], v);
+    v = fmaf(p.scaled_matrix[r][2], mixed[2], v);
+    if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
+    p.linear[r * p.n + i] = v;
+  }
+}
+
 struct EpfParams {
   const float* in;  // dense planes
   float* out;
@@ -343,6 +369,10 @@ struct EpfParams {
   const float* inverse_sigma;
   int blocks_x;
   float sigma_scale;
+  // Pass 2 only: with to_linear, the filtered pixel goes through
+  // OpsinToLinear into linear.linear instead of into `out`.
+  int to_linear;
+  LinearParams linear;
 };
 
 // One EPF iteration (epf.cpp:92-160). Pass 1 compares 5-pixel plus-shaped
@@ -396,7 +426,11 @@ __global__ void __launch_bounds__(kTileW * kTileRows) EpfKernel(const __grid_con
     const int ty = oy + Halo;
     const float block_inverse_sigma = p.inverse_sigma[(y / 8) * p.blocks_x + x / 8];
     if (block_inverse_sigma < kMinInverseSigma) {
-      for (int c = 0; c < 3; ++c) p.out[c * n + i] = tile[c][ty][tx];
+      if (Pass == 2 && p.to_linear) {
+        OpsinToLinearPixel(p.linear, tile[0][ty][tx], tile[1][ty][tx], tile[2][ty][tx], i);
+      } else {
+        for (int c = 0; c < 3; ++c) p.out[c * n + i] = tile[c][ty][tx];
+      }
       continue;
     }
     const bool border = x % 8 == 0 || x % 8 == 7 || y % 8 == 0 || y % 8 == 7;
@@ -428,34 +462,19 @@ __global__ void __launch_bounds__(kTileW * kTileRows) EpfKernel(const __grid_con
 #pragma unroll
       for (int c = 0; c < 3; ++c) sum[c] = fmaf(weight, tile[c][ty + dy][tx + dx], sum[c]);
     }
-    for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
+    if (Pass == 2 && p.to_linear) {
+      OpsinToLinearPixel(p.linear, sum[0] / weight_sum, sum[1] / weight_sum,
+                         sum[2] / weight_sum, i);
+    } else {
+      for (int c = 0; c < 3; ++c) p.out[c * n + i] = sum[c] / weight_sum;
+    }
   }
 }
-
-struct LinearParams {
-  const float* opsin;
-  float* linear;
-  size_t n;
-  float bias_cuberoot;
-  float scaled_matrix[3][3];  // scale * inverse opsin matrix
-  uint32_t* error;
-};
 
 __global__ void OpsinToLinearKernel(const __grid_constant__ LinearParams p) {
   const size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
   if (i >= p.n) return;
-  const float x = p.opsin[i], y = p.opsin[p.n + i], b = p.opsin[2 * p.n + i];
-  const float kOpsinBias = 0.0037930732552754493f;
-  const float gamma[3] = {y + x + p.bias_cuberoot, y - x + p.bias_cuberoot, b + p.bias_cuberoot};
-  float mixed[3];
-  for (int c = 0; c < 3; ++c) mixed[c] = gamma[c] * gamma[c] * gamma[c] - kOpsinBias;
-  for (int r = 0; r < 3; ++r) {
-    float v = p.scaled_matrix[r][0] * mixed[0];
-    v = fmaf(p.scaled_matrix[r][1], mixed[1], v);
-    v = fmaf(p.scaled_matrix[r][2], mixed[2], v);
-    if (!IsFinite(v)) RaiseError(p.error, kErrorNonFiniteOutput);
-    p.linear[r * p.n + i] = v;
-  }
+  OpsinToLinearPixel(p, p.opsin[i], p.opsin[p.n + i], p.opsin[2 * p.n + i], i);
 }
 
 __global__ void BlockReduceKernel(const uint8_t* cells, int blocks_x, int blocks_y,
@@ -614,9 +633,28 @@ int AqReconstruct(const int2* lists, const uint32_t* counts, size_t bx, size_t b
   return status;
 }
 
+LinearParams MakeLinearParams(const float* opsin, size_t width, size_t height,
+                              float intensity_target, float* linear, uint32_t* error) {
+  LinearParams p;
+  p.opsin = opsin;
+  p.linear = linear;
+  p.n = width * height;
+  p.bias_cuberoot = std::cbrt(0.0037930732552754493f);
+  const float kInverse[3][3] = {
+    {11.031566901960783f, -9.866943921568629f, -0.16462299647058826f},
+    {-3.254147380392157f, 4.418770392156863f, -0.16462299647058826f},
+    {-3.6588512862745097f, 2.7129230470588235f, 1.9459282392156863f}};
+  const float scale = 255.0f / intensity_target;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) p.scaled_matrix[r][c] = scale * kInverse[r][c];
+  p.error = error;
+  return p;
+}
+
 int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, size_t width,
                   size_t height, const float* inverse_sigma, size_t bx, float* scratch_a,
-                  float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream) {
+                  float* scratch_b, float* filtered, uint32_t* error, cudaStream_t stream,
+                  float* linear, float intensity_target) {
   GaborishParams g;
   g.in = recon;
   g.in_stride = recon_stride;
@@ -643,9 +681,12 @@ int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, s
   e.in = scratch_a;
   e.out = scratch_b;
   e.sigma_scale = 1.65f * 1.0f;
+  e.to_linear = 0;
+  e.linear = MakeLinearParams(nullptr, width, height, intensity_target, linear, error);
   EpfKernel<1><<<tiles, threads, 0, stream>>>(e);
   e.in = scratch_b;
   e.out = filtered;
+  e.to_linear = linear != nullptr ? 1 : 0;
   e.sigma_scale = 1.65f * 6.5f;
   EpfKernel<2><<<tiles, threads, 0, stream>>>(e);
   return CheckLaunch("aq loop filters");
@@ -653,19 +694,7 @@ int AqLoopFilters(const float* recon, size_t recon_stride, size_t recon_pitch, s
 
 int AqOpsinToLinear(const float* opsin, size_t width, size_t height, float intensity_target,
                     float* linear, uint32_t* error, cudaStream_t stream) {
-  LinearParams p;
-  p.opsin = opsin;
-  p.linear = linear;
-  p.n = width * height;
-  p.bias_cuberoot = std::cbrt(0.0037930732552754493f);
-  const float kInverse[3][3] = {
-    {11.031566901960783f, -9.866943921568629f, -0.16462299647058826f},
-    {-3.254147380392157f, 4.418770392156863f, -0.16462299647058826f},
-    {-3.6588512862745097f, 2.7129230470588235f, 1.9459282392156863f}};
-  const float scale = 255.0f / intensity_target;
-  for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 3; ++c) p.scaled_matrix[r][c] = scale * kInverse[r][c];
-  p.error = error;
+  const LinearParams p = MakeLinearParams(opsin, width, height, intensity_target, linear, error);
   OpsinToLinearKernel<<<Blocks(p.n), kThreads, 0, stream>>>(p);
   return CheckLaunch("aq opsin to linear");
 }

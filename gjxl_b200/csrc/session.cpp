@@ -499,10 +499,10 @@ int RunAq(Session* s, cudaStream_t stream) {
     GJXL_TRY(AqReconstruct(s->anchors, s->anchor_counts, s->bx, s->by, s->qac, s->pw, s->pitch,
                            s->dc_smooth, s->raw, s->quantizer, s->final_y_to_x, s->final_y_to_b,
                            s->matrix_multipliers, s->recon, stream, &fan));
+    // The last loop-filter pass writes the linear image Butteraugli compares.
     GJXL_TRY(AqLoopFilters(s->recon, s->pw, s->pitch, s->width, s->height, s->inverse_sigma,
-                           s->bx, s->filter_a, s->filter_b, s->filtered, s->error, stream));
-    GJXL_TRY(AqOpsinToLinear(s->filtered, s->width, s->height, s->options.intensity_target,
-                             s->rec_linear, s->error, stream));
+                           s->bx, s->filter_a, s->filter_b, s->filtered, s->error, stream,
+                           s->rec_linear, s->options.intensity_target));
     GJXL_TRY(ButteraugliCompare(s->butteraugli, s->rec_linear, s->width, s->width * s->height,
                                 s->distance_map, s->width, s->scores + iteration, stream));
     GJXL_TRY(LaunchPnorm(s->distance_map, s->width, s->width, s->height, 3.0,
