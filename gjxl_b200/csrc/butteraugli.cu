@@ -51,73 +51,14 @@ __device__ __forceinline__ int MirrorB(int c, int size) {
   return c;
 }
 
-// Separable5 (butteraugli_internal.cpp:222-260) on a 32x32 output tile of
-// 32x8 threads (four output rows each): the mirrored input window (tile + 2
-// on each side) is staged in shared memory, all of a thread's loads issued
+// Separable5 (butteraugli_internal.cpp:222-260) runs on 32x32 output tiles
+// of 32x8 threads (four output rows each): the mirrored input window (tile +
+// 2 on each side) is staged in shared memory, all of a thread's loads issued
 // before its first store; tiles whose window lies inside the image skip the
 // mirroring. The horizontal 5-tap pass runs over the window's 36 rows, then
-// the vertical pass, with the reference's operation order for every output.
+// the vertical pass, with the reference's operation order for every output
+// (Blur5DynamicsKernel).
 constexpr int kB5W = 32, kB5H = 32, kB5Rows = 8;
-
-__global__ void __launch_bounds__(kB5W * kB5Rows)
-Blur5Kernel(const float* in, float* out, int w, int h, size_t pitch,
-            const __grid_constant__ Kernel17 k) {
-  constexpr int kSpanW = kB5W + 4, kSpanH = kB5H + 4, kSpan = kSpanW * kSpanH;
-  constexpr int kThreadsB5 = kB5W * kB5Rows;
-  constexpr int kLoads = (kSpan + kThreadsB5 - 1) / kThreadsB5;
-  __shared__ float window[kSpanH][kSpanW];
-  __shared__ float horizontal[kSpanH][kB5W];
-  const int plane = blockIdx.z;
-  const int x0 = blockIdx.x * kB5W, y0 = blockIdx.y * kB5H;
-  const float* base = in + plane * pitch;
-  const int tid = threadIdx.y * kB5W + threadIdx.x;
-  const bool interior = x0 >= 2 && y0 >= 2 && x0 + kSpanW - 2 <= w && y0 + kSpanH - 2 <= h;
-  float staged[kLoads];
-#pragma unroll
-  for (int q = 0; q < kLoads; ++q) {
-    const int i = tid + q * kThreadsB5;
-    if (i < kSpan) {
-      const int ty = i / kSpanW, tx = i - ty * kSpanW;
-      int gy = y0 + ty - 2, gx = x0 + tx - 2;
-      if (!interior) {
-        gy = MirrorB(gy, h);
-        gx = MirrorB(gx, w);
-      }
-      staged[q] = base[static_cast<size_t>(gy) * w + gx];
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < kLoads; ++q) {
-    const int i = tid + q * kThreadsB5;
-    if (i < kSpan) {
-      const int ty = i / kSpanW, tx = i - ty * kSpanW;
-      window[ty][tx] = staged[q];
-    }
-  }
-  __syncthreads();
-  const int tx = threadIdx.x;
-#pragma unroll
-  for (int ty = threadIdx.y; ty < kSpanH; ty += kB5Rows) {
-    const float* row = window[ty] + tx + 2;
-    float r = row[0] * k.w5[0];
-    r = (row[-1] + row[1]) * k.w5[1] + r;
-    r = (row[-2] + row[2]) * k.w5[2] + r;
-    horizontal[ty][tx] = r;
-  }
-  __syncthreads();
-  const int x = x0 + tx;
-  if (x >= w) return;
-#pragma unroll
-  for (int q = 0; q < kB5H / kB5Rows; ++q) {
-    const int oy = threadIdx.y + q * kB5Rows, y = y0 + oy;
-    if (y >= h) break;
-    const int ty = oy + 2;
-    float r = horizontal[ty][tx] * k.w5[0];
-    r = (horizontal[ty - 1][tx] + horizontal[ty + 1][tx]) * k.w5[1] + r;
-    r = (horizontal[ty - 2][tx] + horizontal[ty + 2][tx]) * k.w5[2] + r;
-    out[plane * pitch + static_cast<size_t>(y) * w + x] = r;
-  }
-}
 
 // ConvolveBorderColumn's renormalized sum at position x of a line of length
 // n (samples at src[j * step]), with the taps unrolled: tap t reads sample
@@ -392,24 +333,20 @@ __device__ __forceinline__ void OpsinAbsorbance(float r, float g, float b, float
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
-OpsinDynamicsKernel(const float* linear, size_t linear_stride, size_t linear_pitch,
-                    const float* blurred, float* xyb, int w, int h, size_t pitch,
-                    float intensity, uint32_t* error) {
-  const int i = blockIdx.x * kThreads + threadIdx.x;
-  if (i >= w * h) return;
-  const int x = i % w, y = i / w;
+// OpsinDynamicsImage (butteraugli_internal.cpp:624-690) of one pixel: the
+// blurred sample (b0, b1, b2) sets the sensitivity, the linear sample
+// (r, g, b) is converted; writes XYB pixel i of the three planes.
+__device__ __forceinline__ void OpsinDynamicsPixel(float b0, float b1, float b2, float r, float g,
+                                                   float b, float* xyb, size_t i, size_t pitch,
+                                                   float intensity, uint32_t* error) {
   float p0, p1, p2;
-  OpsinAbsorbance<true>(blurred[i] * intensity, blurred[pitch + i] * intensity,
-                        blurred[2 * pitch + i] * intensity, p0, p1, p2);
+  OpsinAbsorbance<true>(b0 * intensity, b1 * intensity, b2 * intensity, p0, p1, p2);
   p0 = fmaxf(p0, 1.0e-4f);
   p1 = fmaxf(p1, 1.0e-4f);
   p2 = fmaxf(p2, 1.0e-4f);
   const float s0 = fmaxf(GammaB(p0) / p0, 1.0e-4f);
   const float s1 = fmaxf(GammaB(p1) / p1, 1.0e-4f);
   const float s2 = fmaxf(GammaB(p2) / p2, 1.0e-4f);
-  const size_t li = static_cast<size_t>(y) * linear_stride + x;
-  const float r = linear[li], g = linear[linear_pitch + li], b = linear[2 * linear_pitch + li];
   // A non-finite input sample would be absorbed by the clamps below (fmaxf
   // returns the other operand for a NaN), so it is reported here.
   if (!(IsFinite(r) && IsFinite(g) && IsFinite(b))) RaiseError(error, kErrorNonFiniteInput);
@@ -423,6 +360,83 @@ OpsinDynamicsKernel(const float* linear, size_t linear_stride, size_t linear_pit
   xyb[i] = ox;
   xyb[pitch + i] = oy;
   xyb[2 * pitch + i] = c2;
+}
+
+// Separable5 of the three planes of a dense linear image with
+// OpsinDynamicsPixel applied to each output
+// pixel: the blurred planes stay in registers, the pixel's linear sample is
+// the window's centre. Writes the three XYB planes.
+__global__ void __launch_bounds__(kB5W * kB5Rows)
+Blur5DynamicsKernel(const float* in, float* xyb, int w, int h, size_t pitch,
+                    const __grid_constant__ Kernel17 k, float intensity, uint32_t* error) {
+  constexpr int kSpanW = kB5W + 4, kSpanH = kB5H + 4, kSpan = kSpanW * kSpanH;
+  constexpr int kThreadsB5 = kB5W * kB5Rows;
+  constexpr int kLoads = (kSpan + kThreadsB5 - 1) / kThreadsB5;
+  __shared__ float window[3][kSpanH][kSpanW];
+  __shared__ float horizontal[3][kSpanH][kB5W];
+  const int x0 = blockIdx.x * kB5W, y0 = blockIdx.y * kB5H;
+  const int tid = threadIdx.y * kB5W + threadIdx.x;
+  const bool interior = x0 >= 2 && y0 >= 2 && x0 + kSpanW - 2 <= w && y0 + kSpanH - 2 <= h;
+#pragma unroll
+  for (int plane = 0; plane < 3; ++plane) {
+    const float* base = in + plane * pitch;
+    float staged[kLoads];
+#pragma unroll
+    for (int q = 0; q < kLoads; ++q) {
+      const int i = tid + q * kThreadsB5;
+      if (i < kSpan) {
+        const int ty = i / kSpanW, tx = i - ty * kSpanW;
+        int gy = y0 + ty - 2, gx = x0 + tx - 2;
+        if (!interior) {
+          gy = MirrorB(gy, h);
+          gx = MirrorB(gx, w);
+        }
+        staged[q] = base[static_cast<size_t>(gy) * w + gx];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kLoads; ++q) {
+      const int i = tid + q * kThreadsB5;
+      if (i < kSpan) {
+        const int ty = i / kSpanW, tx = i - ty * kSpanW;
+        window[plane][ty][tx] = staged[q];
+      }
+    }
+  }
+  __syncthreads();
+  const int tx = threadIdx.x;
+#pragma unroll
+  for (int plane = 0; plane < 3; ++plane) {
+#pragma unroll
+    for (int ty = threadIdx.y; ty < kSpanH; ty += kB5Rows) {
+      const float* row = window[plane][ty] + tx + 2;
+      float r = row[0] * k.w5[0];
+      r = (row[-1] + row[1]) * k.w5[1] + r;
+      r = (row[-2] + row[2]) * k.w5[2] + r;
+      horizontal[plane][ty][tx] = r;
+    }
+  }
+  __syncthreads();
+  const int x = x0 + tx;
+  if (x >= w) return;
+#pragma unroll
+  for (int q = 0; q < kB5H / kB5Rows; ++q) {
+    const int oy = threadIdx.y + q * kB5Rows, y = y0 + oy;
+    if (y >= h) break;
+    const int ty = oy + 2;
+    float blurred[3];
+#pragma unroll
+    for (int plane = 0; plane < 3; ++plane) {
+      const auto& hz = horizontal[plane];
+      float r = hz[ty][tx] * k.w5[0];
+      r = (hz[ty - 1][tx] + hz[ty + 1][tx]) * k.w5[1] + r;
+      r = (hz[ty - 2][tx] + hz[ty + 2][tx]) * k.w5[2] + r;
+      blurred[plane] = r;
+    }
+    OpsinDynamicsPixel(blurred[0], blurred[1], blurred[2], window[0][ty][tx + 2],
+                       window[1][ty][tx + 2], window[2][ty][tx + 2], xyb,
+                       static_cast<size_t>(y) * w + x, pitch, intensity, error);
+  }
 }
 
 // Psycho-image plane indices (OwnedPsychoImage): LF 0-2, MF 3-5, HF 6-7,
@@ -1365,10 +1379,11 @@ void Psycho(ButteraugliState& st, Scale& s, const float* linear, size_t stride, 
                       cudaMemcpyDeviceToDevice, stream);
     dense = s.linear_tmp;
   }
-  Blur5Kernel<<<dim3((s.w + kB5W - 1) / kB5W, (s.h + kB5H - 1) / kB5H, 3), dim3(kB5W, kB5Rows),
-                0, stream>>>(dense, s.blur3, s.w, s.h, n, st.k_opsin);
-  OpsinDynamicsKernel<<<Blocks(n), kThreads, 0, stream>>>(dense, s.w, n, s.blur3, s.xyb, s.w, s.h,
-                                                          n, st.intensity_target, st.error);
+  // Opsin blur and dynamics in one pass (the blurred planes stay on chip).
+  Blur5DynamicsKernel<<<dim3((s.w + kB5W - 1) / kB5W, (s.h + kB5H - 1) / kB5H),
+                        dim3(kB5W, kB5Rows), 0, stream>>>(dense, s.xyb, s.w, s.h, n,
+                                                          st.k_opsin, st.intensity_target,
+                                                          st.error);
   // LF: 33-tap blur of the three XYB planes straight into the LF planes.
   BlurPlanes<16>(s.xyb, s.tmp, psycho + kLF * n, s.w, s.h, n, 3, st.k_low, stream);
   FrequencyLowKernel<<<Blocks(n), kThreads, 0, stream>>>(s.xyb, psycho, static_cast<int>(n), n,
