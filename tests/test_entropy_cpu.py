@@ -115,3 +115,27 @@ def test_reference_counts_match_writers_on_skewed_clusters():
         assert t["cluster_count"] > 1
         w = code.write(values, contexts, offsets)
         assert np.array_equal(code.count(values, contexts, offsets), w["bit_counts"])
+
+
+def test_slot_sizes_and_argument_checks_without_gpu():
+    """Slot layout of gjxl_b200_entropy_write_sections (host arithmetic, no
+    GPU): section s starts at ceil(B * offset / 64) + 2 s words and every
+    slot holds the section's largest stream (32 + 47 bits per ANS token, 46
+    per prefix token); invalid arguments are rejected before any launch."""
+    from gjxl_b200 import _lib
+    lib = _lib.load()
+    words = lib.gjxl_b200_entropy_slot_words
+    assert words(1, 1000, 4) == (47 * 1000 + 63) // 64 + 8
+    assert words(0, 1000, 4) == (46 * 1000 + 63) // 64 + 8
+    assert words(7, 10, 1) == 0
+    rng = np.random.default_rng(9)
+    offsets = np.concatenate([[0], np.cumsum(rng.integers(0, 5000, 300))])
+    for mode, bits in ((1, 47), (0, 46)):
+        start = [words(mode, int(o), s) for s, o in enumerate(offsets)]
+        for s in range(offsets.size - 1):
+            n = int(offsets[s + 1] - offsets[s])
+            need = (32 + bits * n + 63) // 64 if mode == 1 else (bits * n + 63) // 64
+            assert start[s + 1] - start[s] >= max(need, 1), (mode, s)
+    assert lib.gjxl_b200_entropy_write_sections(None, None, None, 0, None, None, 0, None, None,
+                                                None) == 1
+    assert lib.gjxl_b200_entropy_count_sections(None, 1, None, None, None, None) == 1
