@@ -70,6 +70,7 @@ struct Tokens {
   const uint16_t* contexts;
   const uint32_t* offsets;
   uint32_t count;
+  uint32_t capacity;  // tokens in the arrays
 };
 
 struct EmitParams {
@@ -146,8 +147,9 @@ __device__ __forceinline__ bool ClusterToken(const Code& code, uint32_t context,
   return true;
 }
 
-// Section bounds with the slot checks every kernel makes: false (and the
-// error bit) for decreasing offsets or a slot beyond the buffer.
+// Section bounds with the checks every kernel makes: false (and the error
+// bit) for decreasing offsets, tokens past the arrays' capacity or a slot
+// beyond the buffer.
 __device__ __forceinline__ bool SectionBounds(const EmitParams& p, uint32_t s, bool write,
                                               uint32_t* begin, uint32_t* end,
                                               uint64_t* slot_begin, uint64_t* slot_end,
@@ -157,7 +159,8 @@ __device__ __forceinline__ bool SectionBounds(const EmitParams& p, uint32_t s, b
   const uint32_t b = TokenBits(p.code.mode);
   *slot_begin = SlotStart(*begin, s, b);
   *slot_end = SlotStart(*end, s + 1, b);
-  const bool ok = *end >= *begin && (!write || *slot_end <= p.slot_capacity);
+  const bool ok = *end >= *begin && *end <= p.tokens.capacity &&
+                  (!write || *slot_end <= p.slot_capacity);
   if (!ok && report) {
     RaiseError(p.error, kErrorRange);
     p.bit_counts[static_cast<size_t>(s) * p.stride + p.column] = 0;
@@ -668,6 +671,7 @@ Tokens DeviceTokens(const gjxl_b200_token_sections& t) {
   d.contexts = t.contexts;
   d.offsets = t.offsets;
   d.count = t.count;
+  d.capacity = t.capacity;
   return d;
 }
 

@@ -32,7 +32,7 @@ class TokenSectionsStruct(ctypes.Structure):
     """gjxl_b200_token_sections."""
     _fields_ = [("pairs", ctypes.c_void_p), ("values", ctypes.c_void_p),
                 ("contexts", ctypes.c_void_p), ("offsets", ctypes.c_void_p),
-                ("count", ctypes.c_uint32)]
+                ("count", ctypes.c_uint32), ("capacity", ctypes.c_uint32)]
 
 
 def _device(a: np.ndarray, dtype: np.dtype, device) -> torch.Tensor:
@@ -93,9 +93,11 @@ def _sections(offsets: torch.Tensor, values=None, contexts=None, pairs=None):
     t.count = offsets.numel() - 1
     if pairs is not None:
         t.pairs = pairs.data_ptr()
+        t.capacity = pairs.shape[0]
     else:
         t.values = values.data_ptr()
         t.contexts = contexts.data_ptr()
+        t.capacity = min(values.numel(), contexts.numel())
     return t
 
 

@@ -768,6 +768,8 @@ typedef struct gjxl_b200_token_sections {
   const uint16_t* contexts;
   const uint32_t* offsets;
   uint32_t count;
+  uint32_t capacity;  /* tokens the arrays hold: a section reaching past it
+                         sets device_error bit 2 and is not read */
 } gjxl_b200_token_sections;
 
 /*

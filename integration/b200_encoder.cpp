@@ -898,6 +898,7 @@ GJXL_INTEGRATION_API int gjxl_b200_compare_ac_sections(
   streams.contexts = o.token_contexts;
   streams.offsets = o.group_offsets;
   streams.count = static_cast<uint32_t>(groups);
+  streams.capacity = static_cast<uint32_t>(total);
   std::vector<BitWriter> got;
   float ms = 0.0f;
   status = WriteAcSectionsOnDevice(code, streams, total, &got, &ms);

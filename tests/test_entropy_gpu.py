@@ -114,6 +114,21 @@ def test_invalid_tokens_raise_the_error_word(cuda):
             torch.cuda.synchronize()
 
 
+def test_sections_past_the_token_arrays_are_refused(cuda):
+    """Offsets reaching past the arrays' capacity set bit 2 of the error
+    word; the section is not read (no fault), the others are written."""
+    values, contexts = sample_tokens(14, 3000, 8)
+    offsets = np.array([0, 1000, 3000], np.uint32)
+    code_ref = ref.RefEntropyCode("ans", values, contexts, offsets, 8)
+    want = code_ref.write(values, contexts, offsets)
+    v, c, o = device_split(values, contexts, offsets)
+    got = write_sections(EntropyCode(code_ref.tables()), o, values=v[:2500],
+                         contexts=c[:2500], tokens=3000)
+    assert int(host(got["error"])[0]) & 4
+    bits = host(got["bit_counts"]).astype(np.uint64)
+    assert bits[0] == want["bit_counts"][0] and bits[1] == 0
+
+
 def session_tokens(img):
     h, w, _ = img.shape
     s = AnalysisSession(w, h, effort=7)
